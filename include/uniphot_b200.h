@@ -1,0 +1,160 @@
+/*
+ * uniphot_b200 -- C ABI of the B200-native per-island VarPro-LM forced
+ * photometry solve.
+ *
+ * The reference (uniphot / tract7dt) exposes this path as Python functions
+ * over JAX device arrays; this ABI is the boundary a maintainer binds with
+ * ctypes.  Every entry point returns an int status
+ * (UPH_OK on success) and never throws; uph_last_error() gives the text of
+ * the last failure on a context.  All pointers are plain host pointers unless
+ * the name says _device; sizes are element counts.
+ *
+ * Reference interfaces replaced (paths relative to the reference project):
+ *   uph_upload_field        <- island_stage._shard_setup device upload of the
+ *                              padded field stacks (fit/grid_gpu/island_stage.py:146-240)
+ *                              and island_fit's pad+upload (island_solver.py:3334-3344)
+ *   uph_upload_psf_poly     <- build_psf_tree (island_solver.py:1851-1871)
+ *   uph_upload_psf_mog      <- (no reference counterpart: the analytic PSF of
+ *                              the north-star render mode)
+ *   uph_upload_sersic_table <- sersic_mog.get_table_jax (sersic_mog.py:59-78)
+ *   uph_run_chunk           <- run_class_chunk (island_solver.py:2793-3131)
+ *                              for the legacy/clip/proposals step protocol
+ */
+#ifndef UNIPHOT_B200_H
+#define UNIPHOT_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define UPH_OK 0
+#define UPH_ERR_INVALID 1   /* bad argument / unsupported option            */
+#define UPH_ERR_OOM 2       /* device allocation failed (caller may halve)  */
+#define UPH_ERR_CUDA 3      /* any other CUDA runtime error                  */
+#define UPH_ERR_TIMEOUT 4   /* a bounded device wait gave up                 */
+#define UPH_ERR_STATE 5     /* call order violated (e.g. no field uploaded)  */
+
+#define UPH_RENDER_REFERENCE 0  /* pixelised polynomial PSF, Lanczos-3 shift */
+#define UPH_RENDER_ANALYTIC 1   /* Gaussian-mixture PSF (analytic convolution) */
+
+typedef struct uph_ctx uph_ctx;
+
+/* One solver class: (bbox B, nsrc N, stamp tier T) plus solver knobs.
+ * Mirrors make_class_kernels(plan, n_bands, n_terms, ...)
+ * (island_solver.py:1874-1922). */
+typedef struct uph_class_desc {
+  int32_t bbox;             /* B: island window side (pixels)              */
+  int32_t nsrc;             /* N: member slots per island                  */
+  int32_t tier;             /* T: odd stamp side                           */
+  int32_t render_mode;      /* UPH_RENDER_*                                */
+  float reg;                /* flux-solve ridge on real members (1e-9)     */
+  float pos_step_max;       /* per-step position clip (0.5 px)             */
+  float chi2_ftol_rel;      /* relative dchi2 convergence prong (1e-4)     */
+  float step_tol_pix;       /* position step prong (0.1 px)                */
+  int32_t un_freeze_steps;  /* u_n annealing budget (0 = never)            */
+  int32_t has_priors;       /* nonlinear Gaussian priors present           */
+} uph_class_desc;
+
+/* Per-island inputs of one chunk of n islands (class_host_arrays rows;
+ * island_plan.py:493-700).  Shapes: [n], [n*N], [n*N*6]. */
+typedef struct uph_chunk_in {
+  int32_t n_islands;
+  const int32_t* ox;          /* [n]   window origin in the padded stack   */
+  const int32_t* oy;          /* [n]                                        */
+  const float* x0b;           /* [n]   window origin in field coords        */
+  const float* y0b;           /* [n]                                        */
+  const int32_t* stype;       /* [n*N] SOURCE_STAR=0, EXP=1, DEV=2, SERSIC=3 */
+  const float* n_frozen;      /* [n*N] Sersic n when u_n is not free        */
+  const uint8_t* free_n;      /* [n*N]                                      */
+  const uint8_t* mmask;       /* [n*N] real member slot                     */
+  const uint8_t* keep;        /* [n*N*6] fitted parameter mask              */
+  const float* p0;            /* [n*N*6] (x, y, logre, ee1, ee2, u_n)       */
+  const float* lower;         /* [n*N*6] box bounds                         */
+  const float* upper;         /* [n*N*6]                                    */
+  const float* prior_mean;    /* [n*N*6]                                    */
+  const float* prior_inv_sigma; /* [n*N*6] 0 = no prior                     */
+  /* optional LM carry state (NULL = fresh start from p0):
+   * run_class_chunk(init_state=...) keys p, lam, chi2, consec, nrej, nst */
+  const float* init_lam;      /* [n]                                        */
+  const float* init_chi2;     /* [n]                                        */
+  const int32_t* init_consec; /* [n]                                        */
+  const int32_t* init_nrej;   /* [n]                                        */
+  const int32_t* init_nst;    /* [n]                                        */
+} uph_chunk_in;
+
+/* Per-island outputs (run_class_chunk's dict).  Shapes as noted. */
+typedef struct uph_chunk_out {
+  float* p;             /* [n*N*6]                                         */
+  float* fluxes;        /* [n*nb*N]  per-band VarPro fluxes                */
+  float* ferr;          /* [n*nb*N]  sqrt(diag inv A64)                    */
+  float* chi2;          /* [n]                                             */
+  uint8_t* conv;        /* [n]                                             */
+  uint8_t* stall;       /* [n]                                             */
+  uint8_t* diverged;    /* [n]  post-hoc frozen-proposal probe             */
+  float* stall_dchi2;   /* [n]  plateau certificate (NaN if not stalled)   */
+  int32_t* nst;         /* [n]                                             */
+  float* lam;           /* [n]                                             */
+  int32_t* consec;      /* [n]                                             */
+  int32_t* nrej;        /* [n]                                             */
+  int64_t* n_good;      /* [n]  unmasked pixels summed over bands          */
+  int32_t steps_run;    /* LM iterations executed for the chunk            */
+} uph_chunk_out;
+
+/* Context: one per device per process. */
+int uph_create(int device, uph_ctx** out);
+int uph_destroy(uph_ctx* ctx);
+const char* uph_last_error(const uph_ctx* ctx);
+/* Optional: run on a caller-owned cudaStream_t (NULL = the context's own). */
+int uph_set_stream(uph_ctx* ctx, void* stream);
+void* uph_get_stream(const uph_ctx* ctx);
+
+/* Padded field stacks (n_bands, Hp, Wp) float32: data - bg and inverse
+ * variance (masked pixels 0); ``pad`` is the border width.  Copied to HBM. */
+int uph_upload_field(uph_ctx* ctx, const float* data, const float* invvar,
+                     int32_t n_bands, int32_t Hp, int32_t Wp, int32_t pad);
+/* Same from device pointers (copied device-to-device). */
+int uph_upload_field_device(uph_ctx* ctx, const float* data_dev,
+                            const float* invvar_dev, int32_t n_bands,
+                            int32_t Hp, int32_t Wp, int32_t pad);
+
+/* Pixelised polynomial PSF zero-padded to tier T: coefs (n_bands, T, T, nt)
+ * float32, origin_scale (n_bands, 4) = (x_origin, x_scale, y_origin,
+ * y_scale).  One upload per tier. */
+int uph_upload_psf_poly(uph_ctx* ctx, int32_t tier, const float* coefs,
+                        const float* origin_scale, int32_t n_bands,
+                        int32_t nt);
+
+/* Analytic Gaussian-mixture PSF: params (n_bands, K, 4, nt) float32 holding
+ * the polynomial coefficients of (sigma, e1, e2, weight) per component;
+ * origin_scale as above. */
+int uph_upload_psf_mog(uph_ctx* ctx, const float* params,
+                       const float* origin_scale, int32_t n_bands, int32_t K,
+                       int32_t nt);
+
+/* Sersic MoG table: knots [n_knots], amps/log_vars [n_knots*kmax], core
+ * [n_knots], all float64. */
+int uph_upload_sersic_table(uph_ctx* ctx, const double* knots,
+                            const double* amps, const double* log_vars,
+                            const double* core, int32_t n_knots,
+                            int32_t kmax, double n_min, double n_max);
+
+/* Fit one chunk of one class for up to max_steps LM iterations (host
+ * buffers; the copies to and from the device are inside the call). */
+int uph_run_chunk(uph_ctx* ctx, const uph_class_desc* cls,
+                  const uph_chunk_in* in, int32_t max_steps,
+                  uph_chunk_out* out);
+
+/* Timing split of the last uph_run_chunk on the context (milliseconds of
+ * device time between events): [0] host->device inputs, [1] LM loop,
+ * [2] post-loop probes and final fluxes, [3] device->host outputs. */
+int uph_last_timing(const uph_ctx* ctx, float* ms4);
+
+/* Number of kernel launches issued by the last uph_run_chunk. */
+int64_t uph_last_launch_count(const uph_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* UNIPHOT_B200_H */

@@ -1,0 +1,66 @@
+"""Run the oracle over a solver class (test infrastructure only).
+
+``solve_chunk`` mirrors ``run_class_chunk``'s result dict for a set of
+class rows, island by island, optionally in a spawn-started process pool.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+
+from .island_oracle import (MogPsfBand, PolyPsfBand, SersicTable, SolverConfig,
+                            island_inputs_from_host, solve_island)
+
+
+def psf_bands(psfs, tier: int, mode: str):
+    """Per-band oracle PSF objects (polynomial PSFs zero-padded to tier)."""
+    out = []
+    for p in psfs:
+        if mode == "analytic":
+            out.append(MogPsfBand(np.asarray(p.sigma, np.float64),
+                                  np.asarray(p.e1, np.float64),
+                                  np.asarray(p.e2, np.float64),
+                                  np.asarray(p.weight, np.float64),
+                                  float(p.x_origin), float(p.x_scale),
+                                  float(p.y_origin), float(p.y_scale)))
+        else:
+            c = np.asarray(p.coefs, np.float32)
+            H, W = c.shape[:2]
+            if tier > H:
+                z = np.zeros((tier, tier) + c.shape[2:], np.float32)
+                y0, x0 = (tier - H) // 2, (tier - W) // 2
+                z[y0:y0 + H, x0:x0 + W] = c
+                c = z
+            out.append(PolyPsfBand(c, float(p.x_origin), float(p.x_scale),
+                                   float(p.y_origin), float(p.y_scale)))
+    return out
+
+
+def _one(args):
+    host, row, B, T, dstack, wstack, psf, table, mode, cfg, max_steps = args
+    isl = island_inputs_from_host(host, row, B=B, T=T, dstack=dstack,
+                                  wstack=wstack, psf=psf, table=table, mode=mode)
+    return solve_island(isl, cfg, max_steps)
+
+
+def solve_chunk(host, rows, *, B, T, dstack, wstack, psfs, mode, table_path=None,
+                precision="ref", max_steps=30, reg=1e-9, pos_step_max=0.5,
+                ftol_rel=1e-4, step_tol=0.1, processes: int = 1) -> dict:
+    table = SersicTable.load(table_path) if table_path is not None else None
+    psf = psf_bands(psfs, T, mode)
+    cfg = SolverConfig(reg=reg, pos_step_max=pos_step_max, ftol_rel=ftol_rel,
+                       step_tol=step_tol, precision=precision)
+    jobs = [(host, int(r), B, T, dstack, wstack, psf, table, mode, cfg, max_steps)
+            for r in rows]
+    if processes > 1 and len(jobs) > 1:
+        import multiprocessing as mp
+        with mp.get_context("spawn").Pool(processes) as pool:
+            res = pool.map(_one, jobs, chunksize=max(1, len(jobs) // (4 * processes)))
+    else:
+        res = [_one(j) for j in jobs]
+    out = {}
+    for k in ("p", "fluxes", "ferr", "chi2", "conv", "stall", "diverged",
+              "stall_dchi2", "nst", "lam", "consec", "nrej", "n_good"):
+        out[k] = np.stack([np.asarray(r[k]) for r in res])
+    out["steps_run"] = int(max(r["steps"] for r in res))
+    return out

@@ -1,0 +1,865 @@
+"""CPU restatement of uniphot's per-island VarPro-LM forced-photometry solve.
+
+TEST INFRASTRUCTURE ONLY.  Nothing in the product path (``uniphot_b200``)
+imports this module: it is the checker that the CUDA path is compared
+against (``tests/``, ``__graft_entry__.smoke()``) and the timed CPU arm of
+``bench.py`` (``cpu_baseline`` / ``--impl reference``).
+
+Parity pin: the reference solver is JAX code and JAX is not installed, so the
+reference cannot be executed here.  The host-side numpy modules it relies on
+(islands.py, island_plan.py, psf_polynomial.py, the Sersic table) ARE imported
+from the reference to generate the committed golden fixtures under
+``tests/golden/`` (``tests/golden/make_golden.py``); this restatement is pinned
+against those fixtures plus known-answer tests (noise-free star, zero shift
+identity, table knots, finite-difference Jacobians).  The solver numerics
+themselves (LM trajectory, fluxes) are therefore "parity unpinned" against
+the reference's own execution.
+
+Algorithm followed (paths relative to the reference project ``tract7dt/``):
+
+* PSF polynomial stamp ``sum_t coefs[i,j,t] X^m Y^n`` and its spatial basis:
+  ``fit/grid_gpu/psf_polynomial.py:134-197``, term order
+  ``fit/grid_gpu/bg_polynomial.py:31-100``.
+* Lanczos-3 taps (f64, normalised, cast f32) and the separable zero-border
+  correlate (x then y, fixed tap order):
+  ``fit/optimize/gpu/kernels/lanczos.py:50-181``.
+* Star stamp = PSF at (x, y) shifted by ``dx = x - x0 - rint(x - x0)``:
+  ``fit/grid_gpu/island_solver.py:441-458``; placement at
+  ``rint(x - x0) - T//2``: ``island_solver.py:469-478``.
+* Galaxy stamp ("fft" backend): Sersic MoG table lookup
+  ``fit/grid_gpu/sersic_mog.py:81-100``, ellipse covariance ``:108-150``,
+  Fourier product ``irfft2(rfft2(psf_pad) * sum_k a_k exp(v_k expo))[:T,:T]
+  + core * psf`` ``:153-194``, pad rule ``:197-207``; n <-> u logit
+  ``fit/grid_gpu/source_model.py:38-54``.
+* Per-band VarPro flux solve with ridge ``reg`` on real and 1.0 on padded
+  slots, f64 solve: ``island_solver.py:570-590``; whitened residual
+  ``:592-605``; chi2 ``:668-684``.
+* Gauss-Newton (H, g) = sum_b J_b J_b^T, J_b r_b with J the exact derivative
+  of the VarPro residual (AD through the f64 solve):
+  ``island_solver.py:812-865``.  Here J is formed explicitly per pixel from
+  the analytic stamp derivatives and the Golub-Pereyra formula.
+* LM step (keep mask, damping, f64 solve, clips, bounds, accept/reject,
+  three convergence prongs): ``island_solver.py:921-1002`` with constants
+  ``:146-152`` and ``fit/grid_gpu/island_plan.py:55-74``.
+* Post-hoc divergence probe ``island_solver.py:1335-1399``, plateau probe
+  ``:1401-1465``, final fluxes and errors ``:1467-1482``, good-pixel count
+  ``:2690-2699``.
+
+A second render mode, ``analytic``, is the north-star forward model (not in the
+reference): the PSF is a mixture of elliptical Gaussians whose sigma, e1, e2
+and weight are polynomials in the normalised position; galaxy MoG components
+are convolved analytically (covariances add), sampled at pixel centres around
+the integer-rounded position, then Lanczos-3 shifted exactly like the
+reference's stars.
+
+Two precisions:
+
+* ``"f64"``: everything float64 (the FP64 oracle for flux-error metrics).
+* ``"ref"``: the reference's arithmetic classes: f32 stamps / residuals /
+  H, g; f64 flux and step solves; f32 LM state and chi2 (per-band sums formed
+  exactly and rounded to f32, accumulated over bands in f32).
+"""
+
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+SOURCE_STAR, SOURCE_EXP, SOURCE_DEV, SOURCE_SERSIC = 0, 1, 2, 3
+SERSIC_N_MIN, SERSIC_N_MAX = 0.29, 6.3
+
+# LM constants (island_solver.py:146-152, island_plan.py:55-74)
+STALL_REJECT_K = 4
+SHAPE_STEP_MAX = 0.15
+UN_STEP_MAX = 0.5
+SHAPE_STEP_TOL = 0.01
+LM_LAMBDA0 = 1e-3
+LM_UP, LM_DOWN = 10.0, 0.1
+LAM_MIN, LAM_MAX = 1e-9, 1e6
+
+_ORDER_OF_NT = {1: 0, 3: 1, 6: 2, 10: 3, 15: 4, 21: 5}
+
+
+def poly_terms(nt: int):
+    """(m, n) exponent pairs in the low-order-first PSFEx order."""
+    if nt not in _ORDER_OF_NT:
+        raise ValueError(f"unsupported number of polynomial terms {nt}")
+    order = _ORDER_OF_NT[nt]
+    out = []
+    for deg in range(order + 1):
+        for n in range(deg + 1):
+            out.append((deg - n, n))
+    return out
+
+
+def poly_basis(X: float, Y: float, nt: int):
+    """Basis values and d/dX, d/dY (float64 arrays of length nt)."""
+    b = np.empty(nt)
+    bx = np.empty(nt)
+    by = np.empty(nt)
+    for t, (m, n) in enumerate(poly_terms(nt)):
+        b[t] = X ** m * Y ** n
+        bx[t] = m * X ** (m - 1) * Y ** n if m > 0 else 0.0
+        by[t] = n * X ** m * Y ** (n - 1) if n > 0 else 0.0
+    return b, bx, by
+
+
+# ---------------------------------------------------------------------------
+# Lanczos-3
+# ---------------------------------------------------------------------------
+
+def _l3(x: np.ndarray):
+    """Lanczos-3 window value and derivative (float64)."""
+    ax = np.abs(x)
+    zero = ax < 1e-12
+    out = ax >= 3.0
+    xs = np.where(zero, 1.0, x)
+    px = np.pi * xs
+    s1, c1 = np.sin(px), np.cos(px)
+    s3, c3 = np.sin(px / 3.0), np.cos(px / 3.0)
+    val = 3.0 * s1 * s3 / (px * px)
+    dval = 3.0 * (np.pi * c1 * s3 + (np.pi / 3.0) * s1 * c3) / (px * px) \
+        - 6.0 * s1 * s3 / (np.pi * np.pi * xs ** 3)
+    v = np.where(zero, 1.0, np.where(out, 0.0, val))
+    dv = np.where(zero | out, 0.0, dval)
+    return v, dv
+
+
+def lanczos3_taps(d: float):
+    """Normalised 7-tap weights at offsets -3..3 (+d) and d(weights)/dd."""
+    x = np.arange(-3, 4, dtype=np.float64) + float(d)
+    v, dv = _l3(x)
+    s = v.sum()
+    ds = dv.sum()
+    return v / s, (dv * s - v * ds) / (s * s)
+
+
+def correlate_x(img: np.ndarray, taps: np.ndarray) -> np.ndarray:
+    """out[:, j] = sum_k taps[k] img[:, j + k - 3], zero border, k in order."""
+    n = img.shape[1]
+    pad = np.zeros((img.shape[0], n + 6), dtype=img.dtype)
+    pad[:, 3:3 + n] = img
+    out = taps[0] * pad[:, 0:n]
+    for k in range(1, 7):
+        out = out + taps[k] * pad[:, k:k + n]
+    return out
+
+
+def correlate_y(img: np.ndarray, taps: np.ndarray) -> np.ndarray:
+    n = img.shape[0]
+    pad = np.zeros((n + 6, img.shape[1]), dtype=img.dtype)
+    pad[3:3 + n, :] = img
+    out = taps[0] * pad[0:n, :]
+    for k in range(1, 7):
+        out = out + taps[k] * pad[k:k + n, :]
+    return out
+
+
+# ---------------------------------------------------------------------------
+# Sersic MoG table and ellipse covariance
+# ---------------------------------------------------------------------------
+
+@dataclass
+class SersicTable:
+    n_knots: np.ndarray
+    amps: np.ndarray
+    log_vars: np.ndarray
+    core_amp: np.ndarray
+    n_min: float
+    n_max: float
+
+    @classmethod
+    def load(cls, path):
+        z = np.load(path)
+        return cls(np.asarray(z["n_knots"], np.float64),
+                   np.asarray(z["amps"], np.float64),
+                   np.asarray(z["log_vars"], np.float64),
+                   np.asarray(z["core_amp"], np.float64),
+                   float(z["n_min"]), float(z["n_max"]))
+
+    def lookup(self, n: float):
+        """(amps, vars, core) and their d/dn (piecewise-linear interpolant)."""
+        inside = self.n_min < n < self.n_max
+        nc = min(max(n, self.n_min), self.n_max)
+        K = self.n_knots.shape[0]
+        i = int(np.searchsorted(self.n_knots, nc, side="right")) - 1
+        i = min(max(i, 0), K - 2)
+        n0, n1 = self.n_knots[i], self.n_knots[i + 1]
+        if n1 > n0:
+            t = (nc - n0) / (n1 - n0)
+            dt = (1.0 / (n1 - n0)) if inside else 0.0
+        else:
+            t, dt = 0.0, 0.0
+        a = (1 - t) * self.amps[i] + t * self.amps[i + 1]
+        lv = (1 - t) * self.log_vars[i] + t * self.log_vars[i + 1]
+        v = np.exp(lv)
+        core = (1 - t) * self.core_amp[i] + t * self.core_amp[i + 1]
+        da = dt * (self.amps[i + 1] - self.amps[i])
+        dv = v * dt * (self.log_vars[i + 1] - self.log_vars[i])
+        dcore = dt * (self.core_amp[i + 1] - self.core_amp[i])
+        return a, v, core, da, dv, dcore
+
+
+def u_to_n(u: float):
+    """Sigmoid map u -> n and dn/du (source_model.py:50-54)."""
+    e = math.exp(-u)
+    n = SERSIC_N_MIN + (SERSIC_N_MAX - SERSIC_N_MIN) / (1.0 + e)
+    dn = (SERSIC_N_MAX - SERSIC_N_MIN) * e / (1.0 + e) ** 2
+    return n, dn
+
+
+def cov_terms(lr: float, e1: float, e2: float):
+    """(cxx, cyy, cxy) unit-variance covariance and d/d(lr, e1, e2).
+
+    Returns (c (3,), dc (3 params, 3 terms)).  Restates
+    sersic_mog._ellipse_cov_terms including the round-source nudge."""
+    ex = math.exp(lr)
+    re = min(max(ex, 0.1), 1000.0)
+    dre = re if 0.1 < ex < 1000.0 else 0.0
+    nudge = (e1 == 0.0) and (e2 == 0.0)
+    e1n = 1e-4 if nudge else e1
+    de1n = 0.0 if nudge else 1.0
+    ee = math.hypot(e1n, e2)
+    dee1 = e1n / ee * de1n
+    dee2 = e2 / ee
+    ex2 = math.exp(-ee)
+    e = 1.0 - ex2
+    de_dee = ex2
+    if 1.0 - e > 1e-4:
+        den, dden = 1.0 - e, -1.0
+    else:
+        den, dden = 1e-4, 0.0
+    ibr = (1.0 + e) / den
+    dibr = (den - (1.0 + e) * dden) / (den * den)
+    if ibr < 1000.0:
+        ib, dib = ibr, dibr
+    else:
+        ib, dib = 1000.0, 0.0
+    th = 0.5 * math.atan2(e2, e1n)
+    dth1 = -0.5 * e2 / (ee * ee) * de1n
+    dth2 = 0.5 * e1n / (ee * ee)
+    ct, st = math.cos(th), math.sin(th)
+    s2 = 1.0 / (ib * ib)
+    cxx = re * re * (ct * ct * s2 + st * st)
+    cyy = re * re * (st * st * s2 + ct * ct)
+    cxy = re * re * ct * st * (1.0 - s2)
+    # partials w.r.t. (re, ib, th)
+    d_re = np.array([2 * re * (ct * ct * s2 + st * st),
+                     2 * re * (st * st * s2 + ct * ct),
+                     2 * re * ct * st * (1.0 - s2)])
+    d_ib = np.array([re * re * ct * ct * (-2.0 / ib ** 3),
+                     re * re * st * st * (-2.0 / ib ** 3),
+                     re * re * ct * st * (2.0 / ib ** 3)])
+    d_th = np.array([2 * re * re * ct * st * (1.0 - s2),
+                     -2 * re * re * ct * st * (1.0 - s2),
+                     re * re * (ct * ct - st * st) * (1.0 - s2)])
+    dib_dee = dib * de_dee
+    dc = np.stack([
+        d_re * dre,
+        d_ib * dib_dee * dee1 + d_th * dth1,
+        d_ib * dib_dee * dee2 + d_th * dth2,
+    ])
+    return np.array([cxx, cyy, cxy]), dc
+
+
+def fft_pad_for(T: int) -> int:
+    n = 1
+    while n < T + T // 2:
+        n <<= 1
+    return n
+
+
+# ---------------------------------------------------------------------------
+# PSF models
+# ---------------------------------------------------------------------------
+
+@dataclass
+class PolyPsfBand:
+    """Pixelised polynomial PSF for one band, zero-padded to the tier T."""
+    coefs: np.ndarray         # (T, T, nt) float32
+    x_origin: float
+    x_scale: float
+    y_origin: float
+    y_scale: float
+
+    def stamp(self, x, y, dt):
+        """PSF stamp and d/dx, d/dy at image position (x, y)."""
+        f32 = np.float32
+        X = float(f32((f32(x) - f32(self.x_origin)) / f32(self.x_scale)))
+        Y = float(f32((f32(y) - f32(self.y_origin)) / f32(self.y_scale)))
+        nt = self.coefs.shape[-1]
+        b, bx, by = poly_basis(X, Y, nt)
+        c = self.coefs.astype(np.float64)
+        S = (c @ b).astype(dt)
+        Sx = (c @ (bx / self.x_scale)).astype(dt)
+        Sy = (c @ (by / self.y_scale)).astype(dt)
+        return S, Sx, Sy, nt > 1
+
+
+@dataclass
+class MogPsfBand:
+    """Analytic PSF: K elliptical Gaussians with polynomial parameters.
+
+    Component q has ``Sigma = s^2 [[1+e1, e2], [e2, 1-e1]]`` and weight
+    ``w_q / sum_q w_q``; s, e1, e2, w are polynomials (nt terms) in
+    ``X = (x - x_origin)/x_scale``, ``Y = (y - y_origin)/y_scale``."""
+    sigma: np.ndarray     # (K, nt)
+    e1: np.ndarray        # (K, nt)
+    e2: np.ndarray        # (K, nt)
+    weight: np.ndarray    # (K, nt)
+    x_origin: float
+    x_scale: float
+    y_origin: float
+    y_scale: float
+
+    def components(self, x, y):
+        """Per-component weights (K,), covariances (K, 3) = (A, C, B) with
+        A=Sxx, C=Syy, B=Sxy, and their d/dx, d/dy."""
+        X = (x - self.x_origin) / self.x_scale
+        Y = (y - self.y_origin) / self.y_scale
+        nt = self.sigma.shape[1]
+        b, bx, by = poly_basis(X, Y, nt)
+        bx = bx / self.x_scale
+        by = by / self.y_scale
+        s, sx, sy = self.sigma @ b, self.sigma @ bx, self.sigma @ by
+        a1, a1x, a1y = self.e1 @ b, self.e1 @ bx, self.e1 @ by
+        a2, a2x, a2y = self.e2 @ b, self.e2 @ bx, self.e2 @ by
+        wr, wrx, wry = self.weight @ b, self.weight @ bx, self.weight @ by
+        W, Wx, Wy = wr.sum(), wrx.sum(), wry.sum()
+        w = wr / W
+        wx = (wrx * W - wr * Wx) / (W * W)
+        wy = (wry * W - wr * Wy) / (W * W)
+        s2 = s * s
+        cov = np.stack([s2 * (1 + a1), s2 * (1 - a1), s2 * a2], axis=1)
+
+        def dcov(sd, a1d, a2d):
+            return np.stack([2 * s * sd * (1 + a1) + s2 * a1d,
+                             2 * s * sd * (1 - a1) - s2 * a1d,
+                             2 * s * sd * a2 + s2 * a2d], axis=1)
+        return w, cov, wx, wy, dcov(sx, a1x, a2x), dcov(sy, a1y, a2y)
+
+
+def _gauss_and_dlog(xx, yy, A, C, B):
+    """Normalised 2-D Gaussian at offsets and d ln N / d(A, C, B)."""
+    det = A * C - B * B
+    Q = (C * xx * xx - 2.0 * B * xx * yy + A * yy * yy) / det
+    N = np.exp(-0.5 * Q) / (2.0 * np.pi * math.sqrt(det))
+    dA = (Q * C - yy * yy - C) / (2.0 * det)
+    dC = (Q * A - xx * xx - A) / (2.0 * det)
+    dB = (xx * yy - B * Q + B) / det
+    return N, dA, dC, dB
+
+
+# ---------------------------------------------------------------------------
+# Island context
+# ---------------------------------------------------------------------------
+
+@dataclass
+class IslandInput:
+    """Everything the per-island solve reads (one island of one class)."""
+    B: int
+    T: int
+    data: np.ndarray         # (n_b, B, B) float32 window of data - bg
+    w: np.ndarray            # (n_b, B, B) float32 inverse variance
+    x0: float
+    y0: float
+    stype: np.ndarray        # (N,) int
+    n_frozen: np.ndarray     # (N,) float32
+    free_n: np.ndarray       # (N,) bool
+    mmask: np.ndarray        # (N,) bool
+    keep: np.ndarray         # (N, 6) bool
+    p0: np.ndarray           # (N*6,) float32
+    lower: np.ndarray        # (N*6,)
+    upper: np.ndarray
+    prior_mean: np.ndarray
+    prior_inv_sigma: np.ndarray
+    has_priors: bool
+    psf: list                # per band PolyPsfBand | MogPsfBand
+    table: SersicTable | None
+    mode: str                # "reference" | "analytic"
+
+
+@dataclass
+class SolverConfig:
+    reg: float = 1e-9
+    pos_step_max: float = 0.5
+    ftol_rel: float = 1e-4
+    step_tol: float = 0.1
+    un_freeze_steps: int = 0
+    precision: str = "ref"   # "ref" | "f64"
+
+
+class IslandSolver:
+    """Per-island VarPro-LM in the reference's legacy/clip/proposals mode."""
+
+    def __init__(self, isl: IslandInput, cfg: SolverConfig):
+        self.isl = isl
+        self.cfg = cfg
+        self.dt = np.float64 if cfg.precision == "f64" else np.float32
+        self.N = isl.stype.shape[0]
+        self.nP = 6 * self.N
+        self.nb = isl.data.shape[0]
+        self.clip = np.tile(np.array([cfg.pos_step_max, cfg.pos_step_max,
+                                      SHAPE_STEP_MAX, SHAPE_STEP_MAX,
+                                      SHAPE_STEP_MAX, UN_STEP_MAX]), self.N)
+        self.not_un = np.tile(np.array([1, 1, 1, 1, 1, 0], bool), self.N)
+
+    # ---------------- rendering ----------------
+    def _frac(self, x, x0):
+        f32 = np.float32
+        if self.dt == np.float32:
+            g = f32(f32(x) - f32(x0))
+            r = np.round(g)
+            return float(g - r), int(r)
+        g = float(x) - float(x0)
+        r = np.round(g)
+        return g - r, int(r)
+
+    def _star_unshifted(self, band, x, y):
+        psf = self.isl.psf[band]
+        T = self.isl.T
+        if isinstance(psf, PolyPsfBand):
+            S, Sx, Sy, var = psf.stamp(x, y, self.dt)
+            return S, (Sx if var else None), (Sy if var else None)
+        return self._analytic(band, x, y, None)[:3]
+
+    def _analytic(self, band, x, y, gal):
+        """Analytic stamp.  gal = None (star) or (amps, vars, core, da, dv,
+        dcore, dn_du, c(3), dc(3,3)).  Returns S, Sx, Sy, S_shape(3), S_u."""
+        psf = self.isl.psf[band]
+        T = self.isl.T
+        c0 = T // 2
+        yy, xx = np.mgrid[0:T, 0:T].astype(np.float64)
+        xx -= c0
+        yy -= c0
+        wq, cq, wqx, wqy, dcx, dcy = psf.components(float(x), float(y))
+        S = np.zeros((T, T))
+        Sx = np.zeros((T, T))
+        Sy = np.zeros((T, T))
+        Ssh = np.zeros((3, T, T))
+        Su = np.zeros((T, T))
+        if gal is None:
+            comps = [(1.0, 0.0, 0.0, 0.0)]
+            cgal = np.zeros(3)
+        else:
+            amps, vars_, core, da, dv, dcore, dndu, cgal, dcg = gal
+            comps = [(amps[g], vars_[g], da[g], dv[g])
+                     for g in range(amps.shape[0]) if amps[g] != 0.0 or da[g] != 0.0]
+            comps.append((core, 0.0, dcore, 0.0))
+        for q in range(wq.shape[0]):
+            for (a, v, dav, dvv) in comps:
+                A = v * cgal[0] + cq[q, 0]
+                C = v * cgal[1] + cq[q, 1]
+                Bc = v * cgal[2] + cq[q, 2]
+                N, lA, lC, lB = _gauss_and_dlog(xx, yy, A, C, Bc)
+                S += wq[q] * a * N
+                Sx += wqx[q] * a * N + wq[q] * a * N * (
+                    lA * dcx[q, 0] + lC * dcx[q, 1] + lB * dcx[q, 2])
+                Sy += wqy[q] * a * N + wq[q] * a * N * (
+                    lA * dcy[q, 0] + lC * dcy[q, 1] + lB * dcy[q, 2])
+                if gal is not None:
+                    for s in range(3):
+                        Ssh[s] += wq[q] * a * N * v * (
+                            lA * dcg[s, 0] + lC * dcg[s, 1] + lB * dcg[s, 2])
+                    Su += wq[q] * (dav * N + a * N * dvv * (
+                        lA * cgal[0] + lC * cgal[1] + lB * cgal[2])) * dndu
+        dt = self.dt
+        return (S.astype(dt), Sx.astype(dt), Sy.astype(dt),
+                Ssh.astype(dt), Su.astype(dt))
+
+    def _galaxy_fft(self, band, x, y, gal, need):
+        """Reference 'fft' backend galaxy stamp (+ derivatives if need)."""
+        T = self.isl.T
+        dt = self.dt
+        psf, psfx, psfy = self._star_unshifted(band, x, y)
+        amps, vars_, core, da, dv, dcore, dndu, cg, dcg = gal
+        pad = fft_pad_for(T)
+        cdt = np.complex64 if dt == np.float32 else np.complex128
+
+        def rf(img):
+            z = np.zeros((pad, pad), dtype=dt)
+            z[:T, :T] = img
+            return np.fft.rfft2(z).astype(cdt)
+        P = rf(psf)
+        v = np.fft.rfftfreq(pad)[None, :]
+        w = np.fft.fftfreq(pad)[:, None]
+        vv, ww, vw = v * v, w * w, v * w
+        expo = -2.0 * np.pi ** 2 * (cg[0] * vv + cg[1] * ww + 2.0 * cg[2] * vw)
+        E = np.exp(vars_[:, None, None] * expo[None])
+        F = np.tensordot(amps, E, axes=(0, 0))
+
+        def irf(Q):
+            return np.fft.irfft2(Q, s=(pad, pad))[:T, :T]
+        psf64 = psf.astype(np.float64)
+        S = (irf(P * F) + core * psf64).astype(dt)
+        if not need:
+            return S, None, None, None, None
+        F1 = np.tensordot(amps * vars_, E, axes=(0, 0))
+        Ssh = np.zeros((3, T, T))
+        for s in range(3):
+            dexpo = -2.0 * np.pi ** 2 * (dcg[s, 0] * vv + dcg[s, 1] * ww
+                                         + 2.0 * dcg[s, 2] * vw)
+            Ssh[s] = irf(P * (F1 * dexpo))
+        dF = np.tensordot(da, E, axes=(0, 0)) + \
+            np.tensordot(amps * dv, E, axes=(0, 0)) * expo
+        Su = (irf(P * dF) + dcore * psf64) * dndu
+        Sx = Sy = None
+        if psfx is not None:
+            Sx = (irf(rf(psfx) * F) + core * psfx.astype(np.float64)).astype(dt)
+            Sy = (irf(rf(psfy) * F) + core * psfy.astype(np.float64)).astype(dt)
+        return S, Sx, Sy, Ssh.astype(dt), Su.astype(dt)
+
+    def _gal_params(self, k, p):
+        isl = self.isl
+        lr, e1, e2, u = (float(p[6 * k + 2]), float(p[6 * k + 3]),
+                         float(p[6 * k + 4]), float(p[6 * k + 5]))
+        if isl.free_n[k]:
+            if self.dt == np.float32:
+                uf = np.float32(u)
+                n = float(np.float32(SERSIC_N_MIN) + np.float32(
+                    SERSIC_N_MAX - SERSIC_N_MIN) / (np.float32(1.0) + np.exp(-uf)))
+                _, dndu = u_to_n(u)
+            else:
+                n, dndu = u_to_n(u)
+        else:
+            n, dndu = float(isl.n_frozen[k]), 0.0
+        amps, vars_, core, da, dv, dcore = isl.table.lookup(n)
+        c, dc = cov_terms(lr, e1, e2)
+        return (amps, vars_, core, da, dv, dcore, dndu, c, dc)
+
+    def member_stamps(self, band, p, k, need):
+        """Unit-flux stamp of member k (T, T) and derivative stamps for its
+        live parameters (dict param_index -> (T, T)), all in self.dt."""
+        isl = self.isl
+        dt = self.dt
+        x, y = float(p[6 * k]), float(p[6 * k + 1])
+        dx, _ = self._frac(x, isl.x0)
+        dy, _ = self._frac(y, isl.y0)
+        is_star = isl.stype[k] == SOURCE_STAR
+        if is_star:
+            S, Sx, Sy = self._star_unshifted(band, x, y)
+            Ssh = Su = None
+        else:
+            gal = self._gal_params(k, p)
+            if isl.mode == "analytic":
+                S, Sx, Sy, Ssh, Su = self._analytic(band, x, y, gal)
+            else:
+                S, Sx, Sy, Ssh, Su = self._galaxy_fft(band, x, y, gal, need)
+        Lx, dLx = lanczos3_taps(dx)
+        Ly, dLy = lanczos3_taps(dy)
+        Lx, dLx, Ly, dLy = (a.astype(dt) for a in (Lx, dLx, Ly, dLy))
+        sx = correlate_x(S, Lx)
+        m = correlate_y(sx, Ly)
+        if not need:
+            return m, {}
+        keep = isl.keep[k]
+        D = {}
+        shift = lambda img: correlate_y(correlate_x(img, Lx), Ly)  # noqa: E731
+        if keep[0]:
+            d = correlate_y(correlate_x(S, dLx), Ly)
+            if Sx is not None:
+                d = d + shift(Sx)
+            D[0] = d
+        if keep[1]:
+            d = correlate_y(sx, dLy)
+            if Sy is not None:
+                d = d + shift(Sy)
+            D[1] = d
+        if not is_star:
+            for s in range(3):
+                if keep[2 + s]:
+                    D[2 + s] = shift(Ssh[s])
+            if keep[5]:
+                D[5] = shift(Su)
+        return m, D
+
+    def place(self, stamp, ix_top, iy_top):
+        B, T = self.isl.B, self.isl.T
+        out = np.zeros((B, B), dtype=stamp.dtype)
+        y0, x0 = max(iy_top, 0), max(ix_top, 0)
+        y1, x1 = min(iy_top + T, B), min(ix_top + T, B)
+        if y1 > y0 and x1 > x0:
+            out[y0:y1, x0:x1] = stamp[y0 - iy_top:y1 - iy_top,
+                                      x0 - ix_top:x1 - ix_top]
+        return out
+
+    def models_band(self, band, p, need):
+        """M (N, B, B) placed unit models and derivative list
+        [(k, j, (B,B))] for live params."""
+        isl = self.isl
+        N, B, T = self.N, isl.B, isl.T
+        M = np.zeros((N, B, B), dtype=self.dt)
+        Ds = []
+        for k in range(N):
+            if not isl.mmask[k]:
+                continue
+            x, y = float(p[6 * k]), float(p[6 * k + 1])
+            _, rx = self._frac(x, isl.x0)
+            _, ry = self._frac(y, isl.y0)
+            ixt, iyt = rx - T // 2, ry - T // 2
+            m, D = self.member_stamps(band, p, k, need)
+            M[k] = self.place(m, ixt, iyt)
+            for j in sorted(D):
+                Ds.append((k, j, self.place(D[j], ixt, iyt)))
+        return M, Ds
+
+    # ---------------- linear algebra ----------------
+    def fluxes_band(self, M, d, w):
+        mm = self.isl.mmask
+        w64 = w.astype(np.float64)
+        M64 = M.reshape(self.N, -1).astype(np.float64)
+        wm = M64 * w64.reshape(1, -1)
+        A = wm @ M64.T
+        b = wm @ d.astype(np.float64).reshape(-1)
+        if self.dt == np.float32:
+            A = A.astype(np.float32).astype(np.float64)
+            b = b.astype(np.float32).astype(np.float64)
+        A64 = A + np.diag(np.where(mm, self.cfg.reg, 1.0))
+        f64 = np.linalg.solve(A64, b)
+        f = (f64.astype(self.dt) * mm).astype(self.dt)
+        return f, f64, A64
+
+    def chi2_band(self, M, d, w, f):
+        model = np.tensordot(f.astype(self.dt), M, axes=(0, 0))
+        r = np.sqrt(w.astype(self.dt)) * (d.astype(self.dt) - model)
+        r64 = r.astype(np.float64)
+        return float((r64 * r64).sum()), r
+
+    def prior_pen(self, p):
+        isl = self.isl
+        if not isl.has_priors:
+            return 0.0
+        keep = (isl.keep & isl.mmask[:, None]).reshape(-1)
+        t = isl.prior_inv_sigma * (p - isl.prior_mean)
+        return float(np.sum(np.where(keep, t * t, 0.0)))
+
+    def chi2_of(self, p):
+        dt = self.dt
+        c = dt(0.0)
+        for b in range(self.nb):
+            M, _ = self.models_band(b, p, False)
+            f, _, _ = self.fluxes_band(M, self.isl.data[b], self.isl.w[b])
+            cb, _ = self.chi2_band(M, self.isl.data[b], self.isl.w[b], f)
+            c = dt(c + dt(cb))
+        if self.isl.has_priors:
+            c = dt(c + dt(self.prior_pen(p)))
+        return c
+
+    def hg(self, p):
+        """Un-masked, un-damped Gauss-Newton (H, g) with the explicit
+        VarPro Jacobian J_j = -sqrt(w)(f_k D_j + M^T c_j),
+        c_j = A64^{-1}(e_k s_j - f_k u_j)."""
+        dt = self.dt
+        nP, N = self.nP, self.N
+        H = np.zeros((nP, nP), dtype=dt)
+        g = np.zeros(nP, dtype=dt)
+        for b in range(self.nb):
+            d, w = self.isl.data[b], self.isl.w[b]
+            M, Ds = self.models_band(b, p, True)
+            f, f64, A64 = self.fluxes_band(M, d, w)
+            _, r = self.chi2_band(M, d, w, f)
+            if not Ds:
+                continue
+            w64 = w.astype(np.float64).reshape(-1)
+            M64 = M.reshape(N, -1).astype(np.float64)
+            rt = d.astype(np.float64).reshape(-1) - f64 @ M64
+            sw = np.sqrt(w.astype(dt).astype(np.float64)).reshape(-1)
+            Ainv = np.linalg.inv(A64)
+            rows = []
+            idx = []
+            for (k, j, Dp) in Ds:
+                D64 = Dp.astype(np.float64).reshape(-1)
+                s = np.dot(D64 * w64, rt)
+                u = M64 @ (D64 * w64)
+                rhs = -f64[k] * u
+                rhs[k] += s
+                cj = Ainv @ rhs
+                if dt == np.float32:
+                    cj = cj.astype(np.float32).astype(np.float64)
+                J = -sw * (float(f[k]) * D64 + cj @ M64)
+                if dt == np.float32:
+                    J = J.astype(np.float32).astype(np.float64)
+                rows.append(J)
+                idx.append(6 * k + j)
+            Jb = np.stack(rows)
+            Hb = Jb @ Jb.T
+            gb = Jb @ r.astype(np.float64).reshape(-1)
+            ii = np.array(idx)
+            Hf = np.zeros((nP, nP))
+            Hf[np.ix_(ii, ii)] = Hb
+            gf = np.zeros(nP)
+            gf[ii] = gb
+            H = (H + Hf.astype(dt)).astype(dt)
+            g = (g + gf.astype(dt)).astype(dt)
+        return H, g
+
+    def _keep(self, nsteps):
+        isl = self.isl
+        keep = (isl.keep & isl.mmask[:, None]).reshape(-1)
+        if self.cfg.un_freeze_steps > 0:
+            keep = keep & (self.not_un | (nsteps < self.cfg.un_freeze_steps))
+        return keep
+
+    def propose(self, p, H, g, lam, keep):
+        """Damped f64 step, clips and bounds (island_solver.py:932-967)."""
+        dt = self.dt
+        isl = self.isl
+        nP = self.nP
+        ko = keep[:, None] & keep[None, :]
+        Hm = np.where(ko, H, dt(0)).astype(dt) + np.diag(
+            np.where(keep, 0.0, 1.0)).astype(dt)
+        gm = np.where(keep, g, dt(0)).astype(dt)
+        if isl.has_priors:
+            pi2 = (isl.prior_inv_sigma * isl.prior_inv_sigma).astype(dt)
+            pdiag = np.where(keep, pi2, dt(0)).astype(dt)
+            gm = (gm + np.where(keep, pi2 * (p - isl.prior_mean).astype(dt),
+                                dt(0))).astype(dt)
+            Hd = (Hm + dt(lam) * np.diag(np.diag(Hm)) + np.diag(pdiag)
+                  + dt(1e-8) * np.eye(nP, dtype=dt)).astype(dt)
+        else:
+            Hd = (Hm + dt(lam) * np.diag(np.diag(Hm))
+                  + dt(1e-8) * np.eye(nP, dtype=dt)).astype(dt)
+        delta = -np.linalg.solve(Hd.astype(np.float64), gm.astype(np.float64))
+        delta = delta.astype(dt)
+        delta = np.where(keep, delta, dt(0)).astype(dt)
+        delta = np.clip(delta, -self.clip.astype(dt), self.clip.astype(dt))
+        p_try = np.clip((p + delta).astype(dt), isl.lower.astype(dt),
+                        isl.upper.astype(dt)).astype(dt)
+        return p_try
+
+    # ---------------- LM loop ----------------
+    def run(self, max_steps, state=None):
+        dt = self.dt
+        isl = self.isl
+        cfg = self.cfg
+        if state is None:
+            p = isl.p0.astype(dt).copy()
+            lam = dt(LM_LAMBDA0)
+            chi2 = self.chi2_of(p)
+            consec = nrej = nst = 0
+        else:
+            p = np.asarray(state["p"], dt).reshape(-1).copy()
+            lam = dt(state["lam"])
+            chi2 = dt(state["chi2"])
+            consec, nrej, nst = (int(state["consec"]), int(state["nrej"]),
+                                 int(state["nst"]))
+        conv = False
+        stall = False
+        HG = None
+        steps = 0
+        N = self.N
+        mmf = isl.mmask.astype(np.float64)
+        for _ in range(int(max_steps)):
+            if conv:
+                break
+            steps += 1
+            if HG is None:
+                HG = self.hg(p)
+            H, g = HG
+            keep = self._keep(nst)
+            p_try = self.propose(p, H, g, lam, keep)
+            chi2_try = self.chi2_of(p_try)
+            accept = bool(chi2_try < chi2)
+            p_new = p_try if accept else p
+            lam_new = dt(max(lam * dt(LM_DOWN), dt(LAM_MIN))) if accept \
+                else dt(min(lam * dt(LM_UP), dt(LAM_MAX)))
+            dchi2 = dt(chi2 - chi2_try)
+            se = (p_new - p).astype(np.float64).reshape(N, 6)
+            pos_step = float(np.max(mmf * np.hypot(se[:, 0], se[:, 1])))
+            shape_step = float(np.max(mmf[:, None] * np.abs(se[:, 2:6])))
+            small = accept and (dchi2 < dt(cfg.ftol_rel) * max(chi2, dt(1.0)))
+            consec = consec + 1 if small else (0 if accept else consec)
+            step_small = accept and pos_step < cfg.step_tol \
+                and shape_step < SHAPE_STEP_TOL
+            nrej = 0 if accept else nrej + 1
+            stall_now = nrej >= STALL_REJECT_K
+            conv = (consec >= 2) or step_small or stall_now
+            stall = stall_now
+            if accept:
+                p = p_new
+                chi2 = dt(chi2_try)
+                HG = None
+            lam = lam_new
+            nst += 1
+        return dict(p=p, lam=lam, chi2=chi2, consec=consec, nrej=nrej,
+                    nst=nst, conv=conv, stall=stall, steps=steps, HG=HG)
+
+    def diverged_probe(self, p, lam_final, nsteps_final, HG=None):
+        """True iff the K rejected proposals of a stall were identical."""
+        dt = self.dt
+        H, g = HG if HG is not None else self.hg(p)
+        props = []
+        for j in range(STALL_REJECT_K):
+            lam_j = dt(dt(lam_final) * dt(10.0 ** (j - STALL_REJECT_K)))
+            keep = self._keep(nsteps_final - STALL_REJECT_K + j) \
+                if self.cfg.un_freeze_steps > 0 else self._keep(0)
+            props.append(self.propose(p, H, g, lam_j, keep))
+        return all(np.array_equal(props[0], q) for q in props[1:])
+
+    def plateau_probe(self, p, nsteps_final, HG=None):
+        """min over the lam ladder 1e-9..1e6 of chi2(prop) - chi2(p)."""
+        dt = self.dt
+        c0 = self.chi2_of(p)
+        H, g = HG if HG is not None else self.hg(p)
+        keep = self._keep(nsteps_final)
+        best = None
+        for e in range(-9, 7):
+            lam_j = dt(10.0 ** e)
+            v = dt(self.chi2_of(self.propose(p, H, g, lam_j, keep)) - c0)
+            best = v if best is None else min(best, v)
+        return best
+
+    def final_fluxes(self, p):
+        nb, N = self.nb, self.N
+        F = np.zeros((nb, N), np.float32)
+        E = np.zeros((nb, N), np.float32)
+        for b in range(nb):
+            M, _ = self.models_band(b, p, False)
+            f, _, A64 = self.fluxes_band(M, self.isl.data[b], self.isl.w[b])
+            Ainv = np.linalg.inv(A64)
+            F[b] = f
+            E[b] = np.sqrt(np.maximum(np.diag(Ainv), 1e-30))
+        return F, E
+
+
+def solve_island(isl: IslandInput, cfg: SolverConfig, max_steps: int = 30,
+                 state=None):
+    """Full per-island result (the row of run_class_chunk's dict)."""
+    s = IslandSolver(isl, cfg)
+    out = s.run(max_steps, state)
+    div = False
+    sd = float("nan")
+    if out["stall"]:
+        div = s.diverged_probe(out["p"], out["lam"], out["nst"], out["HG"])
+        sd = float(s.plateau_probe(out["p"], out["nst"], out["HG"]))
+    F, E = s.final_fluxes(out["p"])
+    n_good = int(np.sum(isl.w > 0))
+    return dict(p=out["p"].reshape(s.N, 6).astype(np.float32),
+                fluxes=F, ferr=E, chi2=out["chi2"], conv=out["conv"],
+                stall=out["stall"], diverged=div, stall_dchi2=sd,
+                nst=out["nst"], lam=out["lam"], consec=out["consec"],
+                nrej=out["nrej"], n_good=n_good, steps=out["steps"])
+
+
+def island_inputs_from_host(host: dict, row: int, *, B: int, T: int,
+                            dstack, wstack, psf: list, table, mode: str):
+    """Slice one island out of class host arrays + the padded stacks."""
+    ox, oy = int(host["ox"][row]), int(host["oy"][row])
+    N = host["mmask"].shape[1]
+    return IslandInput(
+        B=B, T=T,
+        data=np.ascontiguousarray(dstack[:, oy:oy + B, ox:ox + B]),
+        w=np.ascontiguousarray(wstack[:, oy:oy + B, ox:ox + B]),
+        x0=float(host["x0b"][row]), y0=float(host["y0b"][row]),
+        stype=host["st"][row], n_frozen=host["sn"][row],
+        free_n=host["fn_flag"][row], mmask=host["mmask"][row],
+        keep=host["keep"][row],
+        p0=host["p0"][row].reshape(-1).astype(np.float32),
+        lower=host["lower"][row].reshape(-1).astype(np.float32),
+        upper=host["upper"][row].reshape(-1).astype(np.float32),
+        prior_mean=host["prior_mean"][row].reshape(-1).astype(np.float32),
+        prior_inv_sigma=host["prior_inv_sigma"][row].reshape(-1).astype(np.float32),
+        has_priors=bool(host["has_priors"]),
+        psf=psf, table=table, mode=mode)

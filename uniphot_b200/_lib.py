@@ -1,0 +1,230 @@
+"""ctypes binding of the C ABI in ``include/uniphot_b200.h``.
+
+The shared library is built in-tree (``uniphot_b200/libuniphot_b200.so``);
+there is no fallback: if it is missing or fails to load, every entry point
+raises.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+LIB_PATH = Path(__file__).resolve().parent / "libuniphot_b200.so"
+
+UPH_OK, UPH_ERR_INVALID, UPH_ERR_OOM, UPH_ERR_CUDA, UPH_ERR_TIMEOUT, \
+    UPH_ERR_STATE = range(6)
+RENDER_MODES = {"reference": 0, "analytic": 1}
+
+EXPORTED = ("uph_create", "uph_destroy", "uph_last_error", "uph_set_stream",
+            "uph_get_stream", "uph_upload_field", "uph_upload_field_device",
+            "uph_upload_psf_poly", "uph_upload_psf_mog",
+            "uph_upload_sersic_table", "uph_run_chunk", "uph_last_timing",
+            "uph_last_launch_count")
+
+_P = C.c_void_p
+
+
+class ClassDesc(C.Structure):
+    _fields_ = [("bbox", C.c_int32), ("nsrc", C.c_int32), ("tier", C.c_int32),
+                ("render_mode", C.c_int32), ("reg", C.c_float),
+                ("pos_step_max", C.c_float), ("chi2_ftol_rel", C.c_float),
+                ("step_tol_pix", C.c_float), ("un_freeze_steps", C.c_int32),
+                ("has_priors", C.c_int32)]
+
+
+class ChunkIn(C.Structure):
+    _fields_ = [("n_islands", C.c_int32)] + [(n, _P) for n in (
+        "ox", "oy", "x0b", "y0b", "stype", "n_frozen", "free_n", "mmask",
+        "keep", "p0", "lower", "upper", "prior_mean", "prior_inv_sigma",
+        "init_lam", "init_chi2", "init_consec", "init_nrej", "init_nst")]
+
+
+class ChunkOut(C.Structure):
+    _fields_ = [(n, _P) for n in (
+        "p", "fluxes", "ferr", "chi2", "conv", "stall", "diverged",
+        "stall_dchi2", "nst", "lam", "consec", "nrej", "n_good")] + \
+        [("steps_run", C.c_int32)]
+
+
+class UphError(RuntimeError):
+    pass
+
+
+_lib = None
+
+
+def lib():
+    """Load (once) the in-tree CUDA library; raises if absent."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise UphError(f"CUDA library not built: {LIB_PATH} (run "
+                           f"__graft_entry__.build() or "
+                           f"python -m uniphot_b200.csrc.build)")
+        L = C.CDLL(str(LIB_PATH))
+        L.uph_create.argtypes = [C.c_int, C.POINTER(_P)]
+        L.uph_destroy.argtypes = [_P]
+        L.uph_last_error.argtypes = [_P]
+        L.uph_last_error.restype = C.c_char_p
+        L.uph_set_stream.argtypes = [_P, _P]
+        L.uph_get_stream.argtypes = [_P]
+        L.uph_get_stream.restype = _P
+        L.uph_upload_field.argtypes = [_P, _P, _P, C.c_int32, C.c_int32, C.c_int32, C.c_int32]
+        L.uph_upload_field_device.argtypes = L.uph_upload_field.argtypes
+        L.uph_upload_psf_poly.argtypes = [_P, C.c_int32, _P, _P, C.c_int32, C.c_int32]
+        L.uph_upload_psf_mog.argtypes = [_P, _P, _P, C.c_int32, C.c_int32, C.c_int32]
+        L.uph_upload_sersic_table.argtypes = [_P, _P, _P, _P, _P, C.c_int32, C.c_int32,
+                                              C.c_double, C.c_double]
+        L.uph_run_chunk.argtypes = [_P, C.POINTER(ClassDesc), C.POINTER(ChunkIn),
+                                    C.c_int32, C.POINTER(ChunkOut)]
+        L.uph_last_timing.argtypes = [_P, C.POINTER(C.c_float)]
+        L.uph_last_launch_count.argtypes = [_P]
+        L.uph_last_launch_count.restype = C.c_int64
+        _lib = L
+    return _lib
+
+
+def ptr(a):
+    return None if a is None else a.ctypes.data_as(_P)
+
+
+class Context:
+    """One uph_ctx (one CUDA device)."""
+
+    def __init__(self, device: int = 0):
+        L = lib()
+        h = _P()
+        rc = L.uph_create(int(device), C.byref(h))
+        if rc != UPH_OK:
+            raise UphError(f"uph_create(device={device}) failed with status {rc}")
+        self._h = h
+        self.device = int(device)
+        self._keep = []
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().uph_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:   # noqa: BLE001 -- interpreter shutdown
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    def check(self, rc: int, what: str):
+        if rc == UPH_OK:
+            return
+        msg = lib().uph_last_error(self._h).decode(errors="replace")
+        if rc == UPH_ERR_OOM and "RESOURCE_EXHAUSTED" not in msg:
+            msg = "RESOURCE_EXHAUSTED: " + msg
+        if rc == UPH_ERR_INVALID:
+            raise ValueError(f"{what}: {msg}")
+        raise UphError(f"{what}: status {rc}: {msg}")
+
+    def set_stream(self, stream_ptr: int):
+        self.check(lib().uph_set_stream(self._h, _P(stream_ptr) if stream_ptr else None),
+                   "uph_set_stream")
+
+    def stream_ptr(self) -> int:
+        return int(lib().uph_get_stream(self._h) or 0)
+
+    def upload_field(self, data: np.ndarray, invvar: np.ndarray, pad: int):
+        d = np.ascontiguousarray(data, np.float32)
+        w = np.ascontiguousarray(invvar, np.float32)
+        nb, Hp, Wp = d.shape
+        self.check(lib().uph_upload_field(self._h, ptr(d), ptr(w), nb, Hp, Wp, int(pad)),
+                   "uph_upload_field")
+
+    def upload_field_device(self, d_ptr: int, w_ptr: int, nb, Hp, Wp, pad):
+        self.check(lib().uph_upload_field_device(self._h, _P(d_ptr), _P(w_ptr), nb, Hp,
+                                                 Wp, int(pad)), "uph_upload_field_device")
+
+    def upload_psf_poly(self, tier: int, coefs: np.ndarray, origin_scale: np.ndarray):
+        cf = np.ascontiguousarray(coefs, np.float32)
+        os_ = np.ascontiguousarray(origin_scale, np.float32)
+        self.check(lib().uph_upload_psf_poly(self._h, int(tier), ptr(cf), ptr(os_),
+                                             cf.shape[0], cf.shape[-1]),
+                   "uph_upload_psf_poly")
+
+    def upload_psf_mog(self, params: np.ndarray, origin_scale: np.ndarray):
+        pr = np.ascontiguousarray(params, np.float32)
+        os_ = np.ascontiguousarray(origin_scale, np.float32)
+        nb, K, _, nt = pr.shape
+        self.check(lib().uph_upload_psf_mog(self._h, ptr(pr), ptr(os_), nb, K, nt),
+                   "uph_upload_psf_mog")
+
+    def upload_sersic_table(self, table: dict):
+        kn = np.ascontiguousarray(table["n_knots"], np.float64)
+        am = np.ascontiguousarray(table["amps"], np.float64)
+        lv = np.ascontiguousarray(table["log_vars"], np.float64)
+        co = np.ascontiguousarray(table["core_amp"], np.float64)
+        self.check(lib().uph_upload_sersic_table(
+            self._h, ptr(kn), ptr(am), ptr(lv), ptr(co), kn.size, am.shape[1],
+            float(table["n_min"]), float(table["n_max"])), "uph_upload_sersic_table")
+
+    def run_chunk(self, desc: ClassDesc, arrays: dict, max_steps: int,
+                  nb: int, init_state: dict | None = None) -> dict:
+        n, N = arrays["mmask"].shape
+        nP = 6 * N
+
+        def f32(a, shape):
+            return np.ascontiguousarray(np.asarray(a, np.float32).reshape(shape))
+
+        def i32(a, shape):
+            return np.ascontiguousarray(np.asarray(a, np.int32).reshape(shape))
+
+        def u8(a, shape):
+            return np.ascontiguousarray(np.asarray(a).astype(np.uint8).reshape(shape))
+        keep_alive = dict(
+            ox=i32(arrays["ox"], n), oy=i32(arrays["oy"], n),
+            x0b=f32(arrays["x0b"], n), y0b=f32(arrays["y0b"], n),
+            stype=i32(arrays["st"], (n, N)), n_frozen=f32(arrays["sn"], (n, N)),
+            free_n=u8(arrays["fn_flag"], (n, N)), mmask=u8(arrays["mmask"], (n, N)),
+            keep=u8(arrays["keep"], (n, nP)), p0=f32(arrays["p0"], (n, nP)),
+            lower=f32(arrays["lower"], (n, nP)), upper=f32(arrays["upper"], (n, nP)),
+            prior_mean=f32(arrays["prior_mean"], (n, nP)),
+            prior_inv_sigma=f32(arrays["prior_inv_sigma"], (n, nP)))
+        cin = ChunkIn(n_islands=n)
+        for k, v in keep_alive.items():
+            setattr(cin, k, ptr(v))
+        if init_state is not None:
+            keep_alive["p0"] = f32(init_state["p"], (n, nP))
+            cin.p0 = ptr(keep_alive["p0"])
+            for k, conv in (("lam", f32), ("chi2", f32), ("consec", i32),
+                            ("nrej", i32), ("nst", i32)):
+                keep_alive["init_" + k] = conv(init_state[k], n)
+                setattr(cin, "init_" + k, ptr(keep_alive["init_" + k]))
+        out = dict(p=np.zeros((n, N, 6), np.float32),
+                   fluxes=np.zeros((n, nb, N), np.float32),
+                   ferr=np.zeros((n, nb, N), np.float32),
+                   chi2=np.zeros(n, np.float32), conv=np.zeros(n, np.uint8),
+                   stall=np.zeros(n, np.uint8), diverged=np.zeros(n, np.uint8),
+                   stall_dchi2=np.zeros(n, np.float32), nst=np.zeros(n, np.int32),
+                   lam=np.zeros(n, np.float32), consec=np.zeros(n, np.int32),
+                   nrej=np.zeros(n, np.int32), n_good=np.zeros(n, np.int64))
+        cout = ChunkOut()
+        for k, v in out.items():
+            setattr(cout, k, ptr(v))
+        rc = lib().uph_run_chunk(self._h, C.byref(desc), C.byref(cin), int(max_steps),
+                                 C.byref(cout))
+        self.check(rc, "uph_run_chunk")
+        for k in ("conv", "stall", "diverged"):
+            out[k] = out[k].astype(bool)
+        out["steps_run"] = int(cout.steps_run)
+        return out
+
+    def last_timing(self):
+        buf = (C.c_float * 4)()
+        lib().uph_last_timing(self._h, buf)
+        return [float(x) for x in buf]
+
+    def last_launch_count(self) -> int:
+        return int(lib().uph_last_launch_count(self._h))

@@ -1,0 +1,647 @@
+// C ABI and host engine: context, device buffers, the per-chunk LM driver.
+//
+// One LM iteration is a fixed sequence of seven kernels over every island of
+// the chunk, captured once into a CUDA graph and replayed; islands carry
+// their state and flags on the device (converged islands retire by flag, a
+// rejected step re-uses the cached Gauss-Newton blocks), so the host only
+// synchronises every UPH_CHECK_EVERY iterations to stop early.  The
+// reference syncs the host on every step (island_solver.py:2971-2977).
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/uniphot_b200.h"
+#include "uph_internal.cuh"
+
+int uph_render_setup();
+int uph_solve_setup();
+void launch_set_probe(const ClassDev& c, cudaStream_t s);
+
+#define UPH_CHECK_EVERY 4
+
+namespace {
+
+struct DevBuf {
+  void* ptr = nullptr;
+  size_t cap = 0;
+  void release() {
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    cap = 0;
+  }
+};
+
+struct PolyPsf {
+  DevBuf coefs, os;
+  int nt = 0, nb = 0;
+};
+
+}  // namespace
+
+struct uph_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  std::string err;
+  // field
+  DevBuf dstack, wstack;
+  int nb = 0, Hp = 0, Wp = 0, pad = 0;
+  // psf
+  std::map<int, PolyPsf> poly;
+  DevBuf mog, mog_os;
+  int mog_k = 0, mog_nt = 0, mog_nb = 0;
+  // table
+  DevBuf tb_knots, tb_amps, tb_lv, tb_core;
+  int tb_n = 0, tb_k = 0;
+  double tb_nmin = 0, tb_nmax = 0;
+  // chunk buffers
+  std::map<std::string, DevBuf> bufs;
+  int* h_active = nullptr;  // pinned
+  cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+  float timing[4] = {0, 0, 0, 0};
+  int64_t launches = 0;
+};
+
+namespace {
+
+int set_err(uph_ctx* c, int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  if (c) c->err = buf;
+  return code;
+}
+
+int cuda_err(uph_ctx* c, cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return UPH_OK;
+  if (e == cudaErrorMemoryAllocation) {
+    cudaGetLastError();
+    return set_err(c, UPH_ERR_OOM, "RESOURCE_EXHAUSTED: out of device memory in %s", what);
+  }
+  return set_err(c, UPH_ERR_CUDA, "CUDA error in %s: %s", what, cudaGetErrorString(e));
+}
+
+#define CK(call, what)                              \
+  do {                                              \
+    cudaError_t _e = (call);                        \
+    if (_e != cudaSuccess) return cuda_err(ctx, _e, what); \
+  } while (0)
+
+int ensure(uph_ctx* ctx, DevBuf& b, size_t bytes, const char* what) {
+  if (bytes == 0) bytes = 16;
+  if (b.cap >= bytes) return UPH_OK;
+  b.release();
+  cudaError_t e = cudaMalloc(&b.ptr, bytes);
+  if (e != cudaSuccess) return cuda_err(ctx, e, what);
+  b.cap = bytes;
+  return UPH_OK;
+}
+
+template <class T>
+T* buf(uph_ctx* ctx, const char* name, size_t count, int* rc) {
+  if (*rc != UPH_OK) return nullptr;
+  DevBuf& b = ctx->bufs[name];
+  *rc = ensure(ctx, b, count * sizeof(T), name);
+  return (T*)b.ptr;
+}
+
+int upload(uph_ctx* ctx, void* dst, const void* src, size_t bytes,
+           const char* what) {
+  if (bytes == 0) return UPH_OK;
+  if (!src) return set_err(ctx, UPH_ERR_INVALID, "null host pointer for %s", what);
+  CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, ctx->stream), what);
+  return UPH_OK;
+}
+
+int download(uph_ctx* ctx, void* dst, const void* src, size_t bytes,
+             const char* what) {
+  if (bytes == 0 || !dst) return UPH_OK;
+  CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, ctx->stream), what);
+  return UPH_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int uph_create(int device, uph_ctx** out) {
+  if (!out) return UPH_ERR_INVALID;
+  *out = nullptr;
+  int ndev = 0;
+  cudaError_t e = cudaGetDeviceCount(&ndev);
+  if (e != cudaSuccess || device < 0 || device >= ndev) return UPH_ERR_CUDA;
+  e = cudaSetDevice(device);
+  if (e != cudaSuccess) return UPH_ERR_CUDA;
+  uph_ctx* ctx = new uph_ctx();
+  ctx->device = device;
+  if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete ctx;
+    return UPH_ERR_CUDA;
+  }
+  ctx->own_stream = true;
+  if (uph_render_setup() != 0 || uph_solve_setup() != 0) {
+    cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return UPH_ERR_CUDA;
+  }
+  if (cudaMallocHost((void**)&ctx->h_active, sizeof(int)) != cudaSuccess) {
+    cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return UPH_ERR_CUDA;
+  }
+  for (auto& ev : ctx->ev) cudaEventCreate(&ev);
+  *out = ctx;
+  return UPH_OK;
+}
+
+int uph_destroy(uph_ctx* ctx) {
+  if (!ctx) return UPH_OK;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  ctx->dstack.release();
+  ctx->wstack.release();
+  for (auto& kv : ctx->poly) {
+    kv.second.coefs.release();
+    kv.second.os.release();
+  }
+  ctx->mog.release();
+  ctx->mog_os.release();
+  ctx->tb_knots.release();
+  ctx->tb_amps.release();
+  ctx->tb_lv.release();
+  ctx->tb_core.release();
+  for (auto& kv : ctx->bufs) kv.second.release();
+  for (auto& ev : ctx->ev)
+    if (ev) cudaEventDestroy(ev);
+  if (ctx->h_active) cudaFreeHost(ctx->h_active);
+  if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return UPH_OK;
+}
+
+const char* uph_last_error(const uph_ctx* ctx) {
+  return ctx ? ctx->err.c_str() : "null context";
+}
+
+int uph_set_stream(uph_ctx* ctx, void* stream) {
+  if (!ctx) return UPH_ERR_INVALID;
+  if (stream == nullptr) {
+    if (!ctx->own_stream) {
+      cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+      ctx->own_stream = true;
+    }
+    return UPH_OK;
+  }
+  if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
+  ctx->stream = (cudaStream_t)stream;
+  ctx->own_stream = false;
+  return UPH_OK;
+}
+
+void* uph_get_stream(const uph_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+static int upload_field_impl(uph_ctx* ctx, const float* d, const float* w,
+                             int nb, int Hp, int Wp, int pad,
+                             cudaMemcpyKind kind) {
+  if (!ctx) return UPH_ERR_INVALID;
+  if (!d || !w || nb <= 0 || Hp <= 0 || Wp <= 0 || pad < 0)
+    return set_err(ctx, UPH_ERR_INVALID, "invalid field arguments");
+  cudaSetDevice(ctx->device);
+  size_t bytes = sizeof(float) * (size_t)nb * Hp * Wp;
+  int rc = ensure(ctx, ctx->dstack, bytes, "field data");
+  if (rc) return rc;
+  rc = ensure(ctx, ctx->wstack, bytes, "field invvar");
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(ctx->dstack.ptr, d, bytes, kind, ctx->stream), "field copy");
+  CK(cudaMemcpyAsync(ctx->wstack.ptr, w, bytes, kind, ctx->stream), "field copy");
+  CK(cudaStreamSynchronize(ctx->stream), "field copy");
+  ctx->nb = nb;
+  ctx->Hp = Hp;
+  ctx->Wp = Wp;
+  ctx->pad = pad;
+  return UPH_OK;
+}
+
+int uph_upload_field(uph_ctx* ctx, const float* d, const float* w,
+                     int32_t nb, int32_t Hp, int32_t Wp, int32_t pad) {
+  return upload_field_impl(ctx, d, w, nb, Hp, Wp, pad, cudaMemcpyHostToDevice);
+}
+
+int uph_upload_field_device(uph_ctx* ctx, const float* d, const float* w,
+                            int32_t nb, int32_t Hp, int32_t Wp, int32_t pad) {
+  return upload_field_impl(ctx, d, w, nb, Hp, Wp, pad, cudaMemcpyDeviceToDevice);
+}
+
+int uph_upload_psf_poly(uph_ctx* ctx, int32_t tier, const float* coefs,
+                        const float* os, int32_t nb, int32_t nt) {
+  if (!ctx) return UPH_ERR_INVALID;
+  if (!coefs || !os || tier <= 0 || (tier % 2) == 0 || nb <= 0 ||
+      !(nt == 1 || nt == 3 || nt == 6 || nt == 10 || nt == 15 || nt == 21))
+    return set_err(ctx, UPH_ERR_INVALID, "invalid PSF polynomial (tier %d, nt %d)", tier, nt);
+  cudaSetDevice(ctx->device);
+  PolyPsf& p = ctx->poly[tier];
+  size_t bytes = sizeof(float) * (size_t)nb * tier * tier * nt;
+  int rc = ensure(ctx, p.coefs, bytes, "psf coefs");
+  if (rc) return rc;
+  rc = ensure(ctx, p.os, sizeof(float) * 4 * nb, "psf origin");
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(p.coefs.ptr, coefs, bytes, cudaMemcpyHostToDevice, ctx->stream), "psf");
+  CK(cudaMemcpyAsync(p.os.ptr, os, sizeof(float) * 4 * nb, cudaMemcpyHostToDevice, ctx->stream), "psf");
+  CK(cudaStreamSynchronize(ctx->stream), "psf");
+  p.nt = nt;
+  p.nb = nb;
+  return UPH_OK;
+}
+
+int uph_upload_psf_mog(uph_ctx* ctx, const float* params, const float* os,
+                       int32_t nb, int32_t K, int32_t nt) {
+  if (!ctx) return UPH_ERR_INVALID;
+  if (!params || !os || nb <= 0 || K <= 0 || K > UPH_MAXKPSF ||
+      !(nt == 1 || nt == 3 || nt == 6 || nt == 10 || nt == 15 || nt == 21))
+    return set_err(ctx, UPH_ERR_INVALID, "invalid MoG PSF (K %d, nt %d)", K, nt);
+  cudaSetDevice(ctx->device);
+  size_t bytes = sizeof(float) * (size_t)nb * K * 4 * nt;
+  int rc = ensure(ctx, ctx->mog, bytes, "mog psf");
+  if (rc) return rc;
+  rc = ensure(ctx, ctx->mog_os, sizeof(float) * 4 * nb, "mog origin");
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(ctx->mog.ptr, params, bytes, cudaMemcpyHostToDevice, ctx->stream), "mog");
+  CK(cudaMemcpyAsync(ctx->mog_os.ptr, os, sizeof(float) * 4 * nb, cudaMemcpyHostToDevice, ctx->stream), "mog");
+  CK(cudaStreamSynchronize(ctx->stream), "mog");
+  ctx->mog_k = K;
+  ctx->mog_nt = nt;
+  ctx->mog_nb = nb;
+  return UPH_OK;
+}
+
+int uph_upload_sersic_table(uph_ctx* ctx, const double* knots,
+                            const double* amps, const double* lv,
+                            const double* core, int32_t n, int32_t kmax,
+                            double nmin, double nmax) {
+  if (!ctx) return UPH_ERR_INVALID;
+  if (!knots || !amps || !lv || !core || n < 2 || kmax <= 0 || kmax > UPH_MAXGAL - 1)
+    return set_err(ctx, UPH_ERR_INVALID, "invalid Sersic table");
+  cudaSetDevice(ctx->device);
+  int rc = ensure(ctx, ctx->tb_knots, sizeof(double) * n, "table");
+  if (!rc) rc = ensure(ctx, ctx->tb_amps, sizeof(double) * n * kmax, "table");
+  if (!rc) rc = ensure(ctx, ctx->tb_lv, sizeof(double) * n * kmax, "table");
+  if (!rc) rc = ensure(ctx, ctx->tb_core, sizeof(double) * n, "table");
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(ctx->tb_knots.ptr, knots, sizeof(double) * n, cudaMemcpyHostToDevice, ctx->stream), "table");
+  CK(cudaMemcpyAsync(ctx->tb_amps.ptr, amps, sizeof(double) * n * kmax, cudaMemcpyHostToDevice, ctx->stream), "table");
+  CK(cudaMemcpyAsync(ctx->tb_lv.ptr, lv, sizeof(double) * n * kmax, cudaMemcpyHostToDevice, ctx->stream), "table");
+  CK(cudaMemcpyAsync(ctx->tb_core.ptr, core, sizeof(double) * n, cudaMemcpyHostToDevice, ctx->stream), "table");
+  CK(cudaStreamSynchronize(ctx->stream), "table");
+  ctx->tb_n = n;
+  ctx->tb_k = kmax;
+  ctx->tb_nmin = nmin;
+  ctx->tb_nmax = nmax;
+  return UPH_OK;
+}
+
+int uph_last_timing(const uph_ctx* ctx, float* ms4) {
+  if (!ctx || !ms4) return UPH_ERR_INVALID;
+  for (int i = 0; i < 4; ++i) ms4[i] = ctx->timing[i];
+  return UPH_OK;
+}
+
+int64_t uph_last_launch_count(const uph_ctx* ctx) { return ctx ? ctx->launches : -1; }
+
+int uph_run_chunk(uph_ctx* ctx, const uph_class_desc* cls,
+                  const uph_chunk_in* in, int32_t max_steps,
+                  uph_chunk_out* out) {
+  if (!ctx) return UPH_ERR_INVALID;
+  if (!cls || !in || !out) return set_err(ctx, UPH_ERR_INVALID, "null argument");
+  cudaSetDevice(ctx->device);
+  ctx->launches = 0;
+  const int n = in->n_islands, N = cls->nsrc, B = cls->bbox, T = cls->tier;
+  if (n <= 0) return set_err(ctx, UPH_ERR_INVALID, "empty chunk");
+  if (N <= 0 || N > UPH_MAXN)
+    return set_err(ctx, UPH_ERR_INVALID, "nsrc class %d outside 1..%d", N, UPH_MAXN);
+  if (B <= 0 || T <= 0 || (T % 2) == 0)
+    return set_err(ctx, UPH_ERR_INVALID, "invalid bbox %d / tier %d", B, T);
+  if (max_steps < 0) return set_err(ctx, UPH_ERR_INVALID, "max_steps < 0");
+  if (!ctx->dstack.ptr) return set_err(ctx, UPH_ERR_STATE, "no field uploaded");
+  const int nb = ctx->nb;
+  const int mode = cls->render_mode;
+  const PolyPsf* pp = nullptr;
+  if (mode == UPH_RENDER_REFERENCE) {
+    auto it = ctx->poly.find(T);
+    if (it == ctx->poly.end())
+      return set_err(ctx, UPH_ERR_STATE, "no polynomial PSF uploaded for tier %d", T);
+    pp = &it->second;
+    if (pp->nb != nb) return set_err(ctx, UPH_ERR_INVALID, "PSF band count mismatch");
+  } else if (mode == UPH_RENDER_ANALYTIC) {
+    if (!ctx->mog.ptr || ctx->mog_nb != nb)
+      return set_err(ctx, UPH_ERR_STATE, "no analytic PSF uploaded for %d bands", nb);
+  } else {
+    return set_err(ctx, UPH_ERR_INVALID, "unknown render mode %d", mode);
+  }
+  const int nP = 6 * N;
+  // ---- host-side row tables ----
+  std::vector<int> nL(n), nr(n);
+  int Kmax = 1, nLmax = 1, R = 1;
+  bool any_gal = false;
+  for (int i = 0; i < n; ++i) {
+    int cnt = 0;
+    bool seen_pad = false;
+    for (int k = 0; k < N; ++k) {
+      bool mm = in->mmask[(size_t)i * N + k] != 0;
+      if (mm && seen_pad)
+        return set_err(ctx, UPH_ERR_INVALID, "island %d: real member slots must come first", i);
+      if (!mm) seen_pad = true; else ++cnt;
+    }
+    if (cnt == 0) return set_err(ctx, UPH_ERR_INVALID, "island %d has no members", i);
+    nr[i] = cnt;
+    int live = 0;
+    for (int k = 0; k < cnt; ++k) {
+      const bool gal = in->stype[(size_t)i * N + k] != 0;
+      any_gal = any_gal || gal;
+      int lk = 0;
+      for (int j = 0; j < 6; ++j)
+        if (in->keep[((size_t)i * N + k) * 6 + j] && (j < 2 || gal)) ++lk;
+      live += lk;
+      R = std::max(R, 1 + lk);
+    }
+    nL[i] = live;
+    nLmax = std::max(nLmax, live);
+    Kmax = std::max(Kmax, live + cnt + 1);
+  }
+  if (nLmax > UPH_MAXLIVE) return set_err(ctx, UPH_ERR_INVALID, "too many live parameters");
+  if (any_gal && mode == UPH_RENDER_REFERENCE)
+    return set_err(ctx, UPH_ERR_INVALID,
+                   "reference render mode supports STAR members only in this build; "
+                   "galaxies need render_mode='analytic'");
+  if (any_gal && !ctx->tb_knots.ptr)
+    return set_err(ctx, UPH_ERR_STATE, "no Sersic table uploaded");
+  std::vector<int16_t> row_k((size_t)n * Kmax, 0), row_s((size_t)n * Kmax, -1),
+      row_p((size_t)n * Kmax, -1);
+  for (int i = 0; i < n; ++i) {
+    int r = 0;
+    for (int k = 0; k < nr[i]; ++k) {
+      const bool gal = in->stype[(size_t)i * N + k] != 0;
+      int srow = 1;
+      for (int j = 0; j < 6; ++j) {
+        if (in->keep[((size_t)i * N + k) * 6 + j] && (j < 2 || gal)) {
+          row_k[(size_t)i * Kmax + r] = (int16_t)k;
+          row_s[(size_t)i * Kmax + r] = (int16_t)srow++;
+          row_p[(size_t)i * Kmax + r] = (int16_t)(6 * k + j);
+          ++r;
+        }
+      }
+    }
+    for (int k = 0; k < nr[i]; ++k) {
+      row_k[(size_t)i * Kmax + r] = (int16_t)k;
+      row_s[(size_t)i * Kmax + r] = 0;
+      ++r;
+    }
+    row_k[(size_t)i * Kmax + r] = 0;
+    row_s[(size_t)i * Kmax + r] = -1;
+  }
+  for (int i = 0; i < n; ++i) {
+    int ox = in->ox[i], oy = in->oy[i];
+    if (ox < 0 || oy < 0 || ox + B > ctx->Wp || oy + B > ctx->Hp)
+      return set_err(ctx, UPH_ERR_INVALID, "island %d window outside the padded field", i);
+  }
+  const int Sz = std::min(T, B);
+  const int nts = (Sz + UPH_TILE - 1) / UPH_TILE;
+  // ---- device buffers ----
+  int rc = UPH_OK;
+  ClassDev c{};
+  c.n_isl = n; c.nb = nb; c.N = N; c.nP = nP; c.B = B; c.T = T; c.Sz = Sz; c.R = R;
+  c.Kmax = Kmax; c.nLmax = nLmax; c.ntile_side = nts;
+  c.mode = mode;
+  c.Hp = ctx->Hp; c.Wp = ctx->Wp;
+  c.dstack = (const float*)ctx->dstack.ptr;
+  c.wstack = (const float*)ctx->wstack.ptr;
+  if (mode == UPH_RENDER_REFERENCE) {
+    c.psf_coefs = (const float*)pp->coefs.ptr;
+    c.psf_os = (const float*)pp->os.ptr;
+    c.nt = pp->nt;
+    c.psf_varies = pp->nt > 1;
+  } else {
+    c.mog = (const float*)ctx->mog.ptr;
+    c.psf_os = (const float*)ctx->mog_os.ptr;
+    c.nt = ctx->mog_nt;
+    c.kpsf = ctx->mog_k;
+    c.psf_varies = ctx->mog_nt > 1;
+  }
+  c.tb_knots = (const double*)ctx->tb_knots.ptr;
+  c.tb_amps = (const double*)ctx->tb_amps.ptr;
+  c.tb_lv = (const double*)ctx->tb_lv.ptr;
+  c.tb_core = (const double*)ctx->tb_core.ptr;
+  c.tb_n = ctx->tb_n; c.tb_k = ctx->tb_k; c.tb_nmin = ctx->tb_nmin; c.tb_nmax = ctx->tb_nmax;
+  int* d_ox = buf<int>(ctx, "ox", n, &rc);
+  int* d_oy = buf<int>(ctx, "oy", n, &rc);
+  float* d_x0b = buf<float>(ctx, "x0b", n, &rc);
+  float* d_y0b = buf<float>(ctx, "y0b", n, &rc);
+  int* d_st = buf<int>(ctx, "stype", (size_t)n * N, &rc);
+  float* d_nf = buf<float>(ctx, "nfrozen", (size_t)n * N, &rc);
+  uint8_t* d_fn = buf<uint8_t>(ctx, "freen", (size_t)n * N, &rc);
+  uint8_t* d_mm = buf<uint8_t>(ctx, "mmask", (size_t)n * N, &rc);
+  uint8_t* d_keep = buf<uint8_t>(ctx, "keep", (size_t)n * nP, &rc);
+  float* d_lo = buf<float>(ctx, "lower", (size_t)n * nP, &rc);
+  float* d_hi = buf<float>(ctx, "upper", (size_t)n * nP, &rc);
+  float* d_pm = buf<float>(ctx, "pmean", (size_t)n * nP, &rc);
+  float* d_pi = buf<float>(ctx, "pinv", (size_t)n * nP, &rc);
+  int* d_nL = buf<int>(ctx, "nL", n, &rc);
+  int* d_nr = buf<int>(ctx, "nr", n, &rc);
+  int16_t* d_rk = buf<int16_t>(ctx, "rowk", (size_t)n * Kmax, &rc);
+  int16_t* d_rs = buf<int16_t>(ctx, "rows", (size_t)n * Kmax, &rc);
+  int16_t* d_rp = buf<int16_t>(ctx, "rowp", (size_t)n * Kmax, &rc);
+  c.p = buf<float>(ctx, "p", (size_t)n * nP, &rc);
+  c.p_try = buf<float>(ctx, "ptry", (size_t)n * nP, &rc);
+  c.lam = buf<float>(ctx, "lam", n, &rc);
+  c.chi2 = buf<float>(ctx, "chi2", n, &rc);
+  c.consec = buf<int>(ctx, "consec", n, &rc);
+  c.nrej = buf<int>(ctx, "nrej", n, &rc);
+  c.nst = buf<int>(ctx, "nst", n, &rc);
+  c.flags = buf<uint8_t>(ctx, "flags", n, &rc);
+  c.stamps = buf<float>(ctx, "stamps", (size_t)n * nb * N * R * Sz * Sz, &rc);
+  c.gram = buf<float>(ctx, "gram", (size_t)n * nb * Kmax * Kmax, &rc);
+  c.Hb = buf<float>(ctx, "Hb", (size_t)n * nb * nLmax * nLmax, &rc);
+  c.gb = buf<float>(ctx, "gb", (size_t)n * nb * nLmax, &rc);
+  c.H = buf<float>(ctx, "H", (size_t)n * nLmax * nLmax, &rc);
+  c.g = buf<float>(ctx, "g", (size_t)n * nLmax, &rc);
+  c.lu = buf<double>(ctx, "lu", nLmax > 72 ? (size_t)n * nLmax * (nLmax + 1) : 1, &rc);
+  c.chi2b = buf<double>(ctx, "chi2b", (size_t)n * nb, &rc);
+  c.flux = buf<float>(ctx, "flux", (size_t)n * nb * N, &rc);
+  c.ferr = buf<float>(ctx, "ferr", (size_t)n * nb * N, &rc);
+  c.ngood = buf<int>(ctx, "ngood", (size_t)n * nb, &rc);
+  c.probe_best = buf<float>(ctx, "pbest", n, &rc);
+  c.probe_p = buf<float>(ctx, "probep", (size_t)n * 4 * nP, &rc);
+  c.n_active = buf<int>(ctx, "nact", 1, &rc);
+  uint8_t* d_div = buf<uint8_t>(ctx, "div", n, &rc);
+  if (rc) return rc;
+  c.ox = d_ox; c.oy = d_oy; c.x0b = d_x0b; c.y0b = d_y0b; c.stype = d_st;
+  c.n_frozen = d_nf; c.free_n = d_fn; c.mmask = d_mm; c.keep = d_keep;
+  c.lower = d_lo; c.upper = d_hi; c.prior_mean = d_pm; c.prior_inv = d_pi;
+  c.has_priors = cls->has_priors ? 1 : 0;
+  c.isl_nL = d_nL; c.isl_nr = d_nr; c.row_k = d_rk; c.row_s = d_rs; c.row_p = d_rp;
+  c.reg = cls->reg; c.pos_step_max = cls->pos_step_max; c.ftol_rel = cls->chi2_ftol_rel;
+  c.step_tol = cls->step_tol_pix; c.un_freeze = cls->un_freeze_steps;
+
+  cudaStream_t s = ctx->stream;
+  CK(cudaEventRecord(ctx->ev[0], s), "event");
+  // ---- inputs ----
+  std::vector<float> h_lam(n, 1e-3f), h_chi2(n, 0.f);
+  std::vector<int> h_consec(n, 0), h_nrej(n, 0), h_nst(n, 0);
+  std::vector<uint8_t> h_flags(n, FL_NEEDLIN | FL_REAL);
+  const bool fresh = (in->init_lam == nullptr);
+  if (!fresh) {
+    if (!in->init_chi2 || !in->init_consec || !in->init_nrej || !in->init_nst)
+      return set_err(ctx, UPH_ERR_INVALID, "partial init state");
+    for (int i = 0; i < n; ++i) {
+      h_lam[i] = in->init_lam[i];
+      h_chi2[i] = in->init_chi2[i];
+      h_consec[i] = in->init_consec[i];
+      h_nrej[i] = in->init_nrej[i];
+      h_nst[i] = in->init_nst[i];
+    }
+  }
+  if ((rc = upload(ctx, d_ox, in->ox, sizeof(int) * n, "ox"))) return rc;
+  if ((rc = upload(ctx, d_oy, in->oy, sizeof(int) * n, "oy"))) return rc;
+  if ((rc = upload(ctx, d_x0b, in->x0b, sizeof(float) * n, "x0b"))) return rc;
+  if ((rc = upload(ctx, d_y0b, in->y0b, sizeof(float) * n, "y0b"))) return rc;
+  if ((rc = upload(ctx, d_st, in->stype, sizeof(int) * n * N, "stype"))) return rc;
+  if ((rc = upload(ctx, d_nf, in->n_frozen, sizeof(float) * n * N, "n_frozen"))) return rc;
+  if ((rc = upload(ctx, d_fn, in->free_n, (size_t)n * N, "free_n"))) return rc;
+  if ((rc = upload(ctx, d_mm, in->mmask, (size_t)n * N, "mmask"))) return rc;
+  if ((rc = upload(ctx, d_keep, in->keep, (size_t)n * nP, "keep"))) return rc;
+  if ((rc = upload(ctx, d_lo, in->lower, sizeof(float) * n * nP, "lower"))) return rc;
+  if ((rc = upload(ctx, d_hi, in->upper, sizeof(float) * n * nP, "upper"))) return rc;
+  if ((rc = upload(ctx, d_pm, in->prior_mean, sizeof(float) * n * nP, "prior_mean"))) return rc;
+  if ((rc = upload(ctx, d_pi, in->prior_inv_sigma, sizeof(float) * n * nP, "prior_inv"))) return rc;
+  if ((rc = upload(ctx, c.p, in->p0, sizeof(float) * n * nP, "p0"))) return rc;
+  if ((rc = upload(ctx, d_nL, nL.data(), sizeof(int) * n, "nL"))) return rc;
+  if ((rc = upload(ctx, d_nr, nr.data(), sizeof(int) * n, "nr"))) return rc;
+  if ((rc = upload(ctx, d_rk, row_k.data(), sizeof(int16_t) * n * Kmax, "rows"))) return rc;
+  if ((rc = upload(ctx, d_rs, row_s.data(), sizeof(int16_t) * n * Kmax, "rows"))) return rc;
+  if ((rc = upload(ctx, d_rp, row_p.data(), sizeof(int16_t) * n * Kmax, "rows"))) return rc;
+  if ((rc = upload(ctx, c.lam, h_lam.data(), sizeof(float) * n, "lam"))) return rc;
+  if ((rc = upload(ctx, c.chi2, h_chi2.data(), sizeof(float) * n, "chi2"))) return rc;
+  if ((rc = upload(ctx, c.consec, h_consec.data(), sizeof(int) * n, "consec"))) return rc;
+  if ((rc = upload(ctx, c.nrej, h_nrej.data(), sizeof(int) * n, "nrej"))) return rc;
+  if ((rc = upload(ctx, c.nst, h_nst.data(), sizeof(int) * n, "nst"))) return rc;
+  if ((rc = upload(ctx, c.flags, h_flags.data(), n, "flags"))) return rc;
+  CK(cudaMemsetAsync(c.stamps, 0, sizeof(float) * (size_t)n * nb * N * R * Sz * Sz, s), "memset");
+  CK(cudaEventRecord(ctx->ev[1], s), "event");
+  // ---- initial chi2 at the seeds ----
+  if (fresh) {
+    launch_render(c, c.p, PH_ALL, s);
+    launch_gram_trial(c, c.p, PH_ALL, 0, s);
+    launch_accept(c, PH_ALL, s);
+    ctx->launches += 3;
+    CK(cudaGetLastError(), "initial chi2");
+  }
+  // ---- LM loop: one iteration captured as a graph ----
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t gexec = nullptr;
+  if (max_steps > 0) {
+    CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "capture");
+    launch_render(c, c.p, PH_LIN, s);
+    launch_gram_lin(c, s);
+    launch_assemble(c, s);
+    launch_step(c, PH_TRIAL, 0, 0.f, 0, s);
+    launch_render(c, c.p_try, PH_TRIAL, s);
+    launch_gram_trial(c, c.p_try, PH_TRIAL, 0, s);
+    launch_accept(c, PH_TRIAL, s);
+    cudaError_t ce = cudaStreamEndCapture(s, &graph);
+    if (ce != cudaSuccess) return cuda_err(ctx, ce, "end capture");
+    ce = cudaGraphInstantiate(&gexec, graph, 0);
+    if (ce != cudaSuccess) {
+      cudaGraphDestroy(graph);
+      return cuda_err(ctx, ce, "graph instantiate");
+    }
+  }
+  int it = 0;
+  while (it < max_steps) {
+    const int group = std::min(UPH_CHECK_EVERY, max_steps - it);
+    for (int j = 0; j < group; ++j) {
+      cudaError_t ce = cudaGraphLaunch(gexec, s);
+      if (ce != cudaSuccess) {
+        cudaGraphExecDestroy(gexec);
+        cudaGraphDestroy(graph);
+        return cuda_err(ctx, ce, "graph launch");
+      }
+      ctx->launches += 7;
+    }
+    it += group;
+    if (it >= max_steps) break;
+    launch_count_active(c, s);
+    ctx->launches += 1;
+    CK(cudaMemcpyAsync(ctx->h_active, c.n_active, sizeof(int), cudaMemcpyDeviceToHost, s), "count");
+    CK(cudaStreamSynchronize(s), "lm loop");
+    if (*ctx->h_active == 0) break;
+  }
+  if (gexec) cudaGraphExecDestroy(gexec);
+  if (graph) cudaGraphDestroy(graph);
+  CK(cudaEventRecord(ctx->ev[2], s), "event");
+  // ---- post-hoc probes on stalled islands ----
+  launch_set_probe(c, s);
+  for (int j = 0; j < 4; ++j) launch_step(c, PH_PROBE, j, 0.f, 1, s);
+  launch_diverged_compare(c, d_div, s);
+  {
+    std::vector<float> inf(n, INFINITY);
+    if ((rc = upload(ctx, c.probe_best, inf.data(), sizeof(float) * n, "probe"))) return rc;
+    for (int e = -9; e <= 6; ++e) {
+      const float lamj = (float)std::pow(10.0, (double)e);
+      launch_step(c, PH_PROBE, 0, lamj, 2, s);
+      launch_render(c, c.p_try, PH_PROBE, s);
+      launch_gram_trial(c, c.p_try, PH_PROBE, 0, s);
+      launch_accept(c, PH_PROBE, s);
+    }
+    ctx->launches += 6 + 16 * 4;
+  }
+  // ---- final fluxes at the converged parameters ----
+  launch_render(c, c.p, PH_ALL, s);
+  launch_gram_trial(c, c.p, PH_ALL, 1, s);
+  ctx->launches += 2;
+  CK(cudaGetLastError(), "post-loop");
+  CK(cudaEventRecord(ctx->ev[3], s), "event");
+  // ---- outputs ----
+  std::vector<uint8_t> fl(n);
+  std::vector<int> ng((size_t)n * nb);
+  std::vector<float> pbest(n);
+  if ((rc = download(ctx, out->p, c.p, sizeof(float) * n * nP, "p"))) return rc;
+  if ((rc = download(ctx, out->fluxes, c.flux, sizeof(float) * n * nb * N, "flux"))) return rc;
+  if ((rc = download(ctx, out->ferr, c.ferr, sizeof(float) * n * nb * N, "ferr"))) return rc;
+  if ((rc = download(ctx, out->chi2, c.chi2, sizeof(float) * n, "chi2"))) return rc;
+  if ((rc = download(ctx, out->nst, c.nst, sizeof(int) * n, "nst"))) return rc;
+  if ((rc = download(ctx, out->lam, c.lam, sizeof(float) * n, "lam"))) return rc;
+  if ((rc = download(ctx, out->consec, c.consec, sizeof(int) * n, "consec"))) return rc;
+  if ((rc = download(ctx, out->nrej, c.nrej, sizeof(int) * n, "nrej"))) return rc;
+  if ((rc = download(ctx, out->diverged, d_div, n, "diverged"))) return rc;
+  if ((rc = download(ctx, fl.data(), c.flags, n, "flags"))) return rc;
+  if ((rc = download(ctx, ng.data(), c.ngood, sizeof(int) * n * nb, "ngood"))) return rc;
+  if ((rc = download(ctx, pbest.data(), c.probe_best, sizeof(float) * n, "probe"))) return rc;
+  CK(cudaEventRecord(ctx->ev[4], s), "event");
+  CK(cudaStreamSynchronize(s), "chunk");
+  int steps_run = 0;
+  for (int i = 0; i < n; ++i) {
+    const bool st = (fl[i] & FL_STALL) != 0;
+    if (out->conv) out->conv[i] = (fl[i] & FL_CONV) ? 1 : 0;
+    if (out->stall) out->stall[i] = st ? 1 : 0;
+    if (out->stall_dchi2) out->stall_dchi2[i] = st ? pbest[i] : NAN;
+    if (out->diverged && !st) out->diverged[i] = 0;
+    if (out->n_good) {
+      int64_t t = 0;
+      for (int b = 0; b < nb; ++b) t += ng[(size_t)i * nb + b];
+      out->n_good[i] = t;
+    }
+    const int ran = (out->nst ? out->nst[i] : 0) - h_nst[i];
+    steps_run = std::max(steps_run, ran);
+  }
+  out->steps_run = steps_run;
+  for (int i = 0; i < 4; ++i) cudaEventElapsedTime(&ctx->timing[i], ctx->ev[i], ctx->ev[i + 1]);
+  return UPH_OK;
+}
+
+}  // extern "C"

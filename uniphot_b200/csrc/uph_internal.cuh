@@ -1,0 +1,162 @@
+// Internal device-side descriptors and helpers of the uniphot_b200 solver.
+//
+// Layout in HBM (one solver class, one chunk of n_isl islands):
+//   field stacks   dstack/wstack          (nb, Hp, Wp) f32, read in place
+//   stamps         (n_isl, nb, N, R, Sz*Sz) f32 -- member m and d m/d theta
+//                  on the member's footprint box clipped to the window
+//   gram           (n_isl, nb, Kmax*Kmax) f32 -- weighted Gram of the rows
+//                  [dM/dtheta (nL); M (nr); data (1)]
+//   Hb, gb         (n_isl, nb, nLmax^2), (n_isl, nb, nLmax) f32 -- per-band
+//                  Gauss-Newton blocks of the VarPro residual
+//   H, g           (n_isl, nLmax^2), (n_isl, nLmax) f32 -- band sums
+//   chi2b          (n_isl, nb) f64, flux/ferr (n_isl, nb, N) f32
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#define UPH_MAXN 32          // member slots per island handled on the device
+#define UPH_MAXLIVE 192      // live nonlinear parameters per island
+#define UPH_MAXK (UPH_MAXLIVE + UPH_MAXN + 1)
+#define UPH_MAXKPSF 8        // Gaussian components of an analytic PSF
+#define UPH_MAXNT 21         // polynomial terms (order 5)
+#define UPH_MAXGAL 16        // Sersic table components + delta core
+#define UPH_TILE 32          // render output tile side
+#define UPH_HALO (UPH_TILE + 6)
+
+// island flag bits
+#define FL_CONV 1
+#define FL_STALL 2
+#define FL_NEEDLIN 4
+#define FL_PROBE 8
+#define FL_REAL 16           // a real island (chunk rows are all real)
+
+// kernel phases
+#define PH_LIN 0      // linearisation at p of islands that need it
+#define PH_TRIAL 1    // trial point of every non-converged island
+#define PH_PROBE 2    // post-hoc probes of stalled islands
+#define PH_ALL 3      // every island (initial chi2, final fluxes)
+
+struct ClassDev {
+  int n_isl, nb, N, nP, B, T, Sz, R, Kmax, nLmax, ntile_side;
+  int mode, nt, kpsf, psf_varies;
+  int Hp, Wp;
+  const float* dstack;
+  const float* wstack;
+  const float* psf_coefs;  // (nb, T, T, nt)
+  const float* psf_os;     // (nb, 4)
+  const float* mog;        // (nb, kpsf, 4, nt)
+  const double* tb_knots;
+  const double* tb_amps;
+  const double* tb_lv;
+  const double* tb_core;
+  int tb_n, tb_k;
+  double tb_nmin, tb_nmax;
+  const int* ox;
+  const int* oy;
+  const float* x0b;
+  const float* y0b;
+  const int* stype;
+  const float* n_frozen;
+  const uint8_t* free_n;
+  const uint8_t* mmask;
+  const uint8_t* keep;
+  const float* lower;
+  const float* upper;
+  const float* prior_mean;
+  const float* prior_inv;
+  int has_priors;
+  const int* isl_nL;       // live parameters per island
+  const int* isl_nr;       // real members per island (slots 0..nr-1)
+  const int16_t* row_k;    // (n_isl, Kmax) member slot of Gram row
+  const int16_t* row_s;    // stamp row (0 = model, >0 derivative, -1 data)
+  const int16_t* row_p;    // parameter index 6k+j of derivative rows
+  float* p;
+  float* p_try;
+  float* lam;
+  float* chi2;
+  int* consec;
+  int* nrej;
+  int* nst;
+  uint8_t* flags;
+  float* stamps;
+  float* gram;
+  float* Hb;
+  float* gb;
+  float* H;
+  float* g;
+  double* lu;
+  double* chi2b;
+  float* flux;
+  float* ferr;
+  int* ngood;
+  float* probe_best;       // (n_isl) plateau certificate
+  float* probe_p;          // (n_isl, 4, nP) diverged-probe proposals
+  int* n_active;
+  float reg, pos_step_max, ftol_rel, step_tol;
+  int un_freeze;
+};
+
+__device__ __forceinline__ bool isl_active(uint8_t fl, int phase) {
+  switch (phase) {
+    case PH_LIN: return !(fl & FL_CONV) && (fl & FL_NEEDLIN);
+    case PH_TRIAL: return !(fl & FL_CONV);
+    case PH_PROBE: return (fl & FL_PROBE) != 0;
+    default: return true;
+  }
+}
+
+// Stamp placement of member k at parameters P: the window box of its
+// footprint.  Positions are float32 as in the reference; rint is
+// round-half-to-even like jnp.round.
+struct MemberBox {
+  int ixt, iyt;      // stamp top-left in window coordinates
+  int wx0, wy0;      // clipped box origin in the window
+  int bw, bh;        // clipped box size (<= Sz), may be <= 0
+  float dx, dy;      // fractional shift
+};
+
+__device__ __forceinline__ MemberBox member_box(const ClassDev& c, int isl,
+                                                const float* P, int k) {
+  MemberBox mb;
+  const float x = P[(size_t)isl * c.nP + 6 * k];
+  const float y = P[(size_t)isl * c.nP + 6 * k + 1];
+  const float gx = __fsub_rn(x, c.x0b[isl]);
+  const float gy = __fsub_rn(y, c.y0b[isl]);
+  const float rx = rintf(gx);
+  const float ry = rintf(gy);
+  mb.dx = __fsub_rn(gx, rx);
+  mb.dy = __fsub_rn(gy, ry);
+  mb.ixt = (int)rx - c.T / 2;
+  mb.iyt = (int)ry - c.T / 2;
+  mb.wx0 = max(mb.ixt, 0);
+  mb.wy0 = max(mb.iyt, 0);
+  mb.bw = min(mb.ixt + c.T, c.B) - mb.wx0;
+  mb.bh = min(mb.iyt + c.T, c.B) - mb.wy0;
+  return mb;
+}
+
+__device__ __forceinline__ size_t stamp_slot(const ClassDev& c, int isl, int b,
+                                             int k, int row) {
+  return ((((size_t)isl * c.nb + b) * c.N + k) * c.R + row) *
+         (size_t)(c.Sz * c.Sz);
+}
+
+// Kernel launch wrappers (defined in the .cu units).
+void launch_render(const ClassDev& c, const float* P, int phase,
+                   cudaStream_t s);
+void launch_gram_lin(const ClassDev& c, cudaStream_t s);
+void launch_assemble(const ClassDev& c, cudaStream_t s);
+void launch_gram_trial(const ClassDev& c, const float* P, int phase,
+                       int final_mode, cudaStream_t s);
+void launch_step(const ClassDev& c, int phase, int probe_j, float probe_lam,
+                 int use_lam_final_scale, cudaStream_t s);
+void launch_accept(const ClassDev& c, int phase, cudaStream_t s);
+void launch_count_active(const ClassDev& c, cudaStream_t s);
+void launch_diverged_compare(const ClassDev& c, uint8_t* out,
+                             cudaStream_t s);
+size_t render_smem_bytes();
+size_t gram_lin_smem_bytes(int Kmax);
+size_t gram_trial_smem_bytes(int N);
+size_t assemble_smem_bytes(int nLmax, int N);
+size_t step_smem_bytes(int nLmax);
+int uph_kernel_setup();

@@ -1,0 +1,787 @@
+// Pixel passes and small dense algebra of the VarPro-LM step.
+//
+// k_gram_lin   -- weighted Gram G = Z W Z^T of the rows
+//                 Z = [dm/dtheta (nL) ; m (nr) ; data (1)] over the island
+//                 window of one band (FP32 CUDA cores, fixed-order
+//                 deterministic reduction).
+// k_assemble   -- from G: the f64 VarPro flux solve and the exact
+//                 Golub-Pereyra Gauss-Newton blocks
+//                   J_i = -W^1/2 (f_k D_i + M^T c_i),
+//                   c_i = A64^-1 (e_k s_i - f_k u_i),
+//                   s_i = D_i^T W (d - M^T f),  u_i = M W D_i,
+//                 i.e. H_b = J J^T and g_b = J r without materialising J
+//                 (the reference pushes tangents through jax.linearize,
+//                 island_solver.py:812-865).
+// k_gram_trial -- trial chi2: flux solve on [m; data] then the whitened
+//                 residual pass r = sqrt(w)(d - sum_k f_k m_k)
+//                 (island_solver.py:570-605, 668-684); also final fluxes and
+//                 sqrt(diag inv A64) (island_solver.py:1467-1482).
+// k_step       -- band sum, keep mask, damping, f64 LU solve, clips, box
+//                 bounds (island_solver.py:921-967).
+// k_accept     -- accept/reject, lambda update, three convergence prongs
+//                 (island_solver.py:968-1002).
+#include "uph_internal.cuh"
+
+namespace {
+
+constexpr int NT = 256;
+
+__device__ __forceinline__ void decode_upper(int idx, int nbk, int& bi,
+                                             int& bj) {
+  int row = 0;
+  while (idx >= nbk - row) {
+    idx -= nbk - row;
+    ++row;
+  }
+  bi = row;
+  bj = row + idx;
+}
+
+// Shared pixel loop: accumulates the Gram of K rows (row descriptors in
+// rk/rs, member boxes in box) over the B x B window of band b, writing the
+// full K x K result to out (pitch ld).  Used by both Gram kernels.
+struct RowSrc {
+  const int16_t* rk;
+  const int16_t* rs;
+  int K;
+};
+
+__device__ void gram_window(const ClassDev& c, int isl, int b, RowSrc rows,
+                            const int4* box, float* out, int ld, int part,
+                            float* sm) {
+  const int tid = threadIdx.x;
+  const int K = rows.K;
+  const int nbk = (K + 7) / 8;
+  const int nblk = nbk * (nbk + 1) / 2;
+  int s, my, split;
+  if (nblk <= NT) {
+    s = NT / nblk;
+    my = tid / s;
+    split = tid % s;
+    if (my >= nblk) my = -1;
+  } else {
+    s = 1;
+    my = part * NT + tid;
+    split = 0;
+    if (my >= nblk) my = -1;
+  }
+  int bi = 0, bj = 0;
+  if (my >= 0) decode_upper(my, nbk, bi, bj);
+  const int TP = (K <= 32) ? 128 : (K <= 96 ? 64 : 32);
+  const int LD = TP + 1;
+  float* Zs = sm;                        // nbk*8 x LD
+  float* swt = Zs + nbk * 8 * LD;        // TP
+  const int B = c.B, Sz = c.Sz;
+  const int npix = B * B;
+  const size_t plane = (size_t)c.Hp * c.Wp;
+  const float* dbase = c.dstack + b * plane + (size_t)c.oy[isl] * c.Wp + c.ox[isl];
+  const float* wbase = c.wstack + b * plane + (size_t)c.oy[isl] * c.Wp + c.ox[isl];
+  float acc[8][8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+#pragma unroll
+    for (int j = 0; j < 8; ++j) acc[i][j] = 0.f;
+  const int nrows = nbk * 8;
+  for (int pix0 = 0; pix0 < npix; pix0 += TP) {
+    for (int q = tid; q < TP; q += NT) {
+      const int pix = pix0 + q;
+      float sw = 0.f;
+      if (pix < npix) {
+        const int wy = pix / B, wx = pix - (pix / B) * B;
+        sw = sqrtf(wbase[(size_t)wy * c.Wp + wx]);
+      }
+      swt[q] = sw;
+    }
+    __syncthreads();
+    for (int e = tid; e < nrows * TP; e += NT) {
+      const int r = e / TP, q = e - (e / TP) * TP;
+      const int pix = pix0 + q;
+      float v = 0.f;
+      if (r < K && pix < npix) {
+        const int wy = pix / B, wx = pix - (pix / B) * B;
+        const int rs = rows.rs[r];
+        if (rs < 0) {
+          v = dbase[(size_t)wy * c.Wp + wx] * swt[q];
+        } else {
+          const int k = rows.rk[r];
+          const int4 bx = box[k];
+          const int ly = wy - bx.y, lx = wx - bx.x;
+          if (ly >= 0 && ly < bx.w && lx >= 0 && lx < bx.z)
+            v = c.stamps[stamp_slot(c, isl, b, k, rs) + (size_t)ly * Sz + lx] * swt[q];
+        }
+      }
+      Zs[r * LD + q] = v;
+    }
+    __syncthreads();
+    if (my >= 0) {
+      const float* za = Zs + bi * 8 * LD;
+      const float* zb = Zs + bj * 8 * LD;
+      for (int q = split; q < TP; q += s) {
+        float a[8], bb[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+          a[i] = za[i * LD + q];
+          bb[i] = zb[i * LD + q];
+        }
+#pragma unroll
+        for (int i = 0; i < 8; ++i)
+#pragma unroll
+          for (int j = 0; j < 8; ++j) acc[i][j] = fmaf(a[i], bb[j], acc[i][j]);
+      }
+    }
+    __syncthreads();
+  }
+  // deterministic reduction over the pixel splits
+  if (s > 1) {
+    float* red = sm;  // NT x 65
+    for (int i = 0; i < 8; ++i)
+      for (int j = 0; j < 8; ++j) red[tid * 65 + i * 8 + j] = acc[i][j];
+    __syncthreads();
+    if (my >= 0 && split == 0) {
+      for (int i = 0; i < 8; ++i)
+        for (int j = 0; j < 8; ++j) {
+          float t = 0.f;
+          for (int sp = 0; sp < s; ++sp) t += red[(tid + sp) * 65 + i * 8 + j];
+          acc[i][j] = t;
+        }
+    }
+  }
+  if (my >= 0 && split == 0) {
+    for (int i = 0; i < 8; ++i) {
+      const int gi = bi * 8 + i;
+      if (gi >= K) break;
+      for (int j = 0; j < 8; ++j) {
+        const int gj = bj * 8 + j;
+        if (gj >= K) break;
+        out[gi * ld + gj] = acc[i][j];
+        out[gj * ld + gi] = acc[i][j];
+      }
+    }
+  }
+}
+
+__device__ void load_boxes(const ClassDev& c, int isl, const float* P,
+                           int4* box) {
+  for (int k = threadIdx.x; k < c.N; k += blockDim.x) {
+    MemberBox mb = member_box(c, isl, P, k);
+    box[k] = make_int4(mb.wx0, mb.wy0, mb.bw, mb.bh);
+  }
+}
+
+__global__ void __launch_bounds__(NT) k_gram_lin(ClassDev c) {
+  extern __shared__ float sm[];
+  __shared__ int4 box[UPH_MAXN];
+  const int isl = blockIdx.x / c.nb, b = blockIdx.x % c.nb;
+  if (isl >= c.n_isl || !isl_active(c.flags[isl], PH_LIN)) return;
+  const int nL = c.isl_nL[isl], nr = c.isl_nr[isl];
+  const int K = nL + nr + 1;
+  const int nbk = (K + 7) / 8;
+  const int nblk = nbk * (nbk + 1) / 2;
+  if ((int)blockIdx.y * NT >= max(nblk, 1) && blockIdx.y > 0) return;
+  if (nblk <= NT && blockIdx.y > 0) return;
+  load_boxes(c, isl, c.p, box);
+  __syncthreads();
+  RowSrc rows{c.row_k + (size_t)isl * c.Kmax, c.row_s + (size_t)isl * c.Kmax, K};
+  gram_window(c, isl, b, rows, box,
+              c.gram + ((size_t)isl * c.nb + b) * c.Kmax * c.Kmax, c.Kmax,
+              blockIdx.y, sm);
+}
+
+// Gauss-Jordan elimination with partial pivoting on M (n x ncol, pitch ld):
+// turns the left n x n block into the identity; the remaining columns hold
+// A^-1 [rhs].  All threads of the block participate.
+__device__ void gauss_jordan(double* M, int n, int ncol, int ld, double* fac,
+                             int* piv) {
+  const int tid = threadIdx.x;
+  for (int col = 0; col < n; ++col) {
+    if (tid == 0) {
+      int p = col;
+      double best = fabs(M[col * ld + col]);
+      for (int r = col + 1; r < n; ++r) {
+        double v = fabs(M[r * ld + col]);
+        if (v > best) {
+          best = v;
+          p = r;
+        }
+      }
+      *piv = p;
+    }
+    __syncthreads();
+    const int p = *piv;
+    if (p != col)
+      for (int j = tid; j < ncol; j += blockDim.x) {
+        double t = M[col * ld + j];
+        M[col * ld + j] = M[p * ld + j];
+        M[p * ld + j] = t;
+      }
+    __syncthreads();
+    const double inv = 1.0 / M[col * ld + col];
+    __syncthreads();
+    for (int j = tid; j < ncol; j += blockDim.x) M[col * ld + j] *= inv;
+    for (int r = tid; r < n; r += blockDim.x) fac[r] = M[r * ld + col];
+    __syncthreads();
+    for (int e = tid; e < n * ncol; e += blockDim.x) {
+      const int r = e / ncol, j = e - (e / ncol) * ncol;
+      if (r != col) M[r * ld + j] -= fac[r] * M[col * ld + j];
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(NT) k_assemble(ClassDev c) {
+  extern __shared__ double dsm[];
+  __shared__ double fac[UPH_MAXN];
+  __shared__ int piv;
+  const int isl = blockIdx.x / c.nb, b = blockIdx.x % c.nb;
+  if (isl >= c.n_isl || !isl_active(c.flags[isl], PH_LIN)) return;
+  const int tid = threadIdx.x;
+  const int nL = c.isl_nL[isl], nr = c.isl_nr[isl];
+  const int K = nL + nr + 1;
+  const float* G = c.gram + ((size_t)isl * c.nb + b) * c.Kmax * c.Kmax;
+  const int ldg = c.Kmax;
+  const int16_t* rk = c.row_k + (size_t)isl * c.Kmax;
+  float* Hb = c.Hb + ((size_t)isl * c.nb + b) * c.nLmax * c.nLmax;
+  float* gb = c.gb + ((size_t)isl * c.nb + b) * c.nLmax;
+  const int ncol = 2 * nr + 1;
+  const int lda = ncol;
+  double* Aug = dsm;                       // nr x (2nr+1)
+  double* DM = Aug + UPH_MAXN * (2 * UPH_MAXN + 1);  // nL x nr
+  double* Cm = DM + (size_t)c.nLmax * UPH_MAXN;      // nL x nr
+  double* Wm = Cm + (size_t)c.nLmax * UPH_MAXN;      // nL x nr
+  double* vec = Wm + (size_t)c.nLmax * UPH_MAXN;     // f64[nr], a[nr], q[nr]
+  double* f64v = vec;
+  double* av = vec + UPH_MAXN;
+  double* qv = av + UPH_MAXN;
+  if (nL == 0) {
+    return;
+  }
+  const int m0 = nL;  // first model row
+  const int dr = nL + nr;
+  for (int e = tid; e < nr * ncol; e += NT) {
+    const int r = e / ncol, j = e - (e / ncol) * ncol;
+    double v;
+    if (j < nr) {
+      v = (double)G[(m0 + r) * ldg + m0 + j];
+      if (j == r) v += (double)c.reg;
+    } else if (j < 2 * nr) {
+      v = (j - nr == r) ? 1.0 : 0.0;
+    } else {
+      v = (double)G[(m0 + r) * ldg + dr];
+    }
+    Aug[r * lda + j] = v;
+  }
+  for (int e = tid; e < nL * nr; e += NT) {
+    const int i = e / nr, l = e - (e / nr) * nr;
+    DM[i * UPH_MAXN + l] = (double)G[i * ldg + m0 + l];
+  }
+  __syncthreads();
+  gauss_jordan(Aug, nr, ncol, lda, fac, &piv);
+  // f64 fluxes and their float32 copy (the model uses f32 fluxes)
+  for (int l = tid; l < nr; l += NT) {
+    f64v[l] = Aug[l * lda + 2 * nr];
+    av[l] = (double)(float)f64v[l];
+  }
+  __syncthreads();
+  // q = b - A a  (A without ridge)
+  for (int l = tid; l < nr; l += NT) {
+    double t = (double)G[(m0 + l) * ldg + dr];
+    for (int m = 0; m < nr; ++m) t -= (double)G[(m0 + l) * ldg + m0 + m] * av[m];
+    qv[l] = t;
+  }
+  // c_i = Ainv (e_k s_i - f_k u_i), rounded to f32
+  for (int i = tid; i < nL; i += NT) {
+    const int k = rk[i];
+    double si = (double)G[i * ldg + dr];
+    for (int m = 0; m < nr; ++m) si -= DM[i * UPH_MAXN + m] * f64v[m];
+    const double fk = f64v[k];
+    for (int l = 0; l < nr; ++l) {
+      double t = Aug[l * lda + nr + k] * si;
+      double u = 0.0;
+      for (int m = 0; m < nr; ++m) u += Aug[l * lda + nr + m] * DM[i * UPH_MAXN + m];
+      t -= fk * u;
+      Cm[i * UPH_MAXN + l] = (double)(float)t;
+    }
+  }
+  __syncthreads();
+  // W_j = A c_j + a_j DM_j
+  for (int e = tid; e < nL * nr; e += NT) {
+    const int j = e / nr, l = e - (e / nr) * nr;
+    double t = av[rk[j]] * DM[j * UPH_MAXN + l];
+    for (int m = 0; m < nr; ++m) t += (double)G[(m0 + l) * ldg + m0 + m] * Cm[j * UPH_MAXN + m];
+    Wm[j * UPH_MAXN + l] = t;
+  }
+  __syncthreads();
+  // H_ij = a_i (a_j DD_ij + DM_i . c_j) + c_i . W_j
+  const int npair = nL * (nL + 1) / 2;
+  for (int e = tid; e < npair; e += NT) {
+    int i = 0, rem = e;
+    while (rem >= nL - i) {
+      rem -= nL - i;
+      ++i;
+    }
+    const int j = i + rem;
+    const double ai = av[rk[i]], aj = av[rk[j]];
+    double t1 = aj * (double)G[i * ldg + j];
+    double t2 = 0.0;
+    for (int l = 0; l < nr; ++l) {
+      t1 += DM[i * UPH_MAXN + l] * Cm[j * UPH_MAXN + l];
+      t2 += Cm[i * UPH_MAXN + l] * Wm[j * UPH_MAXN + l];
+    }
+    const float h = (float)(ai * t1 + t2);
+    Hb[i * c.nLmax + j] = h;
+    Hb[j * c.nLmax + i] = h;
+  }
+  // g_i = -(a_i (Dd_i - DM_i . a) + c_i . q)
+  for (int i = tid; i < nL; i += NT) {
+    double t = (double)G[i * ldg + dr];
+    for (int m = 0; m < nr; ++m) t -= DM[i * UPH_MAXN + m] * av[m];
+    double u = 0.0;
+    for (int l = 0; l < nr; ++l) u += Cm[i * UPH_MAXN + l] * qv[l];
+    gb[i] = (float)(-(av[rk[i]] * t + u));
+  }
+}
+
+__global__ void __launch_bounds__(NT)
+k_gram_trial(ClassDev c, const float* __restrict__ P, int phase,
+             int final_mode) {
+  extern __shared__ float sm[];
+  __shared__ int4 box[UPH_MAXN];
+  __shared__ int16_t rk[UPH_MAXN + 1], rs[UPH_MAXN + 1];
+  __shared__ double Aug[UPH_MAXN * (2 * UPH_MAXN + 1)];
+  __shared__ double fac[UPH_MAXN];
+  __shared__ float gmm[(UPH_MAXN + 1) * (UPH_MAXN + 1)];
+  __shared__ float fl32[UPH_MAXN];
+  __shared__ double red[NT];
+  __shared__ int redi[NT];
+  __shared__ int piv;
+  const int isl = blockIdx.x / c.nb, b = blockIdx.x % c.nb;
+  if (isl >= c.n_isl || !isl_active(c.flags[isl], phase)) return;
+  const int tid = threadIdx.x;
+  const int nr = c.isl_nr[isl];
+  const int K = nr + 1;
+  load_boxes(c, isl, P, box);
+  for (int r = tid; r < K; r += NT) {
+    rk[r] = (int16_t)(r < nr ? r : 0);
+    rs[r] = (int16_t)(r < nr ? 0 : -1);
+  }
+  __syncthreads();
+  RowSrc rows{rk, rs, K};
+  gram_window(c, isl, b, rows, box, gmm, K, 0, sm);
+  __syncthreads();
+  const int ncol = 2 * nr + 1;
+  for (int e = tid; e < nr * ncol; e += NT) {
+    const int r = e / ncol, j = e - (e / ncol) * ncol;
+    double v;
+    if (j < nr) {
+      v = (double)gmm[r * K + j];
+      if (j == r) v += (double)c.reg;
+    } else if (j < 2 * nr) {
+      v = (j - nr == r) ? 1.0 : 0.0;
+    } else {
+      v = (double)gmm[r * K + nr];
+    }
+    Aug[r * ncol + j] = v;
+  }
+  __syncthreads();
+  gauss_jordan(Aug, nr, ncol, ncol, fac, &piv);
+  for (int l = tid; l < nr; l += NT) fl32[l] = (float)Aug[l * ncol + 2 * nr];
+  __syncthreads();
+  // residual pass
+  const int B = c.B, Sz = c.Sz;
+  const size_t plane = (size_t)c.Hp * c.Wp;
+  const float* dbase = c.dstack + b * plane + (size_t)c.oy[isl] * c.Wp + c.ox[isl];
+  const float* wbase = c.wstack + b * plane + (size_t)c.oy[isl] * c.Wp + c.ox[isl];
+  double acc = 0.0;
+  int good = 0;
+  for (int pix = tid; pix < B * B; pix += NT) {
+    const int wy = pix / B, wx = pix - (pix / B) * B;
+    const float w = wbase[(size_t)wy * c.Wp + wx];
+    const float d = dbase[(size_t)wy * c.Wp + wx];
+    float model = 0.f;
+    for (int k = 0; k < nr; ++k) {
+      const int4 bx = box[k];
+      const int ly = wy - bx.y, lx = wx - bx.x;
+      if (ly >= 0 && ly < bx.w && lx >= 0 && lx < bx.z)
+        model = fmaf(fl32[k], c.stamps[stamp_slot(c, isl, b, k, 0) + (size_t)ly * Sz + lx], model);
+    }
+    const float r = sqrtf(w) * (d - model);
+    acc += (double)r * (double)r;
+    good += (w > 0.f);
+  }
+  red[tid] = acc;
+  redi[tid] = good;
+  __syncthreads();
+  for (int st = NT / 2; st > 0; st >>= 1) {
+    if (tid < st) {
+      red[tid] += red[tid + st];
+      redi[tid] += redi[tid + st];
+    }
+    __syncthreads();
+  }
+  if (tid == 0) c.chi2b[(size_t)isl * c.nb + b] = red[0];
+  if (final_mode) {
+    float* fo = c.flux + ((size_t)isl * c.nb + b) * c.N;
+    float* eo = c.ferr + ((size_t)isl * c.nb + b) * c.N;
+    for (int k = tid; k < c.N; k += NT) {
+      if (k < nr) {
+        fo[k] = fl32[k];
+        eo[k] = (float)sqrt(fmax(Aug[k * ncol + nr + k], 1e-30));
+      } else {
+        fo[k] = 0.f;
+        eo[k] = 1.0f;  // padded slot: unit diagonal
+      }
+    }
+    if (tid == 0) c.ngood[(size_t)isl * c.nb + b] = redi[0];
+  }
+}
+
+// LU with partial pivoting of the n x (n+1) augmented system in M (pitch
+// n+1); the solution overwrites column n.
+__device__ void lu_solve(double* M, int n, int* piv, double* fac_g) {
+  const int tid = threadIdx.x;
+  const int ld = n + 1;
+  for (int col = 0; col < n; ++col) {
+    if (tid == 0) {
+      int p = col;
+      double best = fabs(M[col * ld + col]);
+      for (int r = col + 1; r < n; ++r) {
+        double v = fabs(M[r * ld + col]);
+        if (v > best) {
+          best = v;
+          p = r;
+        }
+      }
+      *piv = p;
+    }
+    __syncthreads();
+    const int p = *piv;
+    if (p != col)
+      for (int j = col + tid; j < ld; j += blockDim.x) {
+        double t = M[col * ld + j];
+        M[col * ld + j] = M[p * ld + j];
+        M[p * ld + j] = t;
+      }
+    __syncthreads();
+    const double pv = M[col * ld + col];
+    for (int r = col + 1 + tid; r < n; r += blockDim.x) fac_g[r] = M[r * ld + col] / pv;
+    __syncthreads();
+    const int rows = n - col - 1, cols = ld - col - 1;
+    for (int e = tid; e < rows * cols; e += blockDim.x) {
+      const int r = col + 1 + e / cols, j = col + 1 + e % cols;
+      M[r * ld + j] -= fac_g[r] * M[col * ld + j];
+    }
+    __syncthreads();
+  }
+  // back substitution (serial over rows, parallel dot)
+  __shared__ double bs[NT];
+  for (int r = n - 1; r >= 0; --r) {
+    double t = 0.0;
+    for (int j = r + 1 + tid; j < n; j += blockDim.x) t += M[r * ld + j] * M[j * ld + n];
+    bs[tid] = t;
+    __syncthreads();
+    for (int st = NT / 2; st > 0; st >>= 1) {
+      if (tid < st) bs[tid] += bs[tid + st];
+      __syncthreads();
+    }
+    if (tid == 0) M[r * ld + n] = (M[r * ld + n] - bs[0]) / M[r * ld + r];
+    __syncthreads();
+  }
+}
+
+// probe_mode: 0 normal step, 1 diverged probe j (lam_final * 10^(j-4)),
+// 2 plateau probe (lam = probe_lam)
+__global__ void __launch_bounds__(NT)
+k_step(ClassDev c, int phase, int probe_mode, int probe_j, float probe_lam) {
+  extern __shared__ double lsm[];
+  __shared__ int piv;
+  __shared__ double fac[UPH_MAXLIVE];
+  __shared__ float delta[UPH_MAXLIVE];
+  __shared__ uint8_t kp[UPH_MAXLIVE];
+  const int isl = blockIdx.x;
+  if (isl >= c.n_isl) return;
+  const uint8_t fl = c.flags[isl];
+  if (!isl_active(fl, phase)) return;
+  const int tid = threadIdx.x;
+  const int nL = c.isl_nL[isl];
+  const int nP = c.nP;
+  const int ldH = c.nLmax;
+  float* H = c.H + (size_t)isl * ldH * ldH;
+  float* g = c.g + (size_t)isl * ldH;
+  const int16_t* rp = c.row_p + (size_t)isl * c.Kmax;
+  if (probe_mode == 0 && (fl & FL_NEEDLIN)) {
+    for (int e = tid; e < nL * nL; e += NT) {
+      const int i = e / nL, j = e - (e / nL) * nL;
+      float t = 0.f;
+      for (int b = 0; b < c.nb; ++b)
+        t += c.Hb[((size_t)isl * c.nb + b) * ldH * ldH + i * ldH + j];
+      H[i * ldH + j] = t;
+    }
+    for (int i = tid; i < nL; i += NT) {
+      float t = 0.f;
+      for (int b = 0; b < c.nb; ++b) t += c.gb[((size_t)isl * c.nb + b) * ldH + i];
+      g[i] = t;
+    }
+    __syncthreads();
+    if (tid == 0) c.flags[isl] = fl & ~FL_NEEDLIN;
+  }
+  float lam;
+  int nst_eff = c.nst[isl];
+  if (probe_mode == 1) {
+    const float sc = (float)pow(10.0, (double)(probe_j - 4));
+    lam = c.lam[isl] * sc;
+    nst_eff = c.nst[isl] - 4 + probe_j;
+  } else if (probe_mode == 2) {
+    lam = probe_lam;
+  } else {
+    lam = c.lam[isl];
+  }
+  const float* p = c.p + (size_t)isl * nP;
+  const float* pm = c.prior_mean + (size_t)isl * nP;
+  const float* pinv = c.prior_inv + (size_t)isl * nP;
+  for (int i = tid; i < nL; i += NT) {
+    const int pp = rp[i];
+    bool k = true;
+    if (c.un_freeze > 0 && (pp % 6) == 5 && !(nst_eff < c.un_freeze)) k = false;
+    kp[i] = k;
+  }
+  __syncthreads();
+  const bool use_smem = (nL <= 72);
+  double* M = use_smem ? lsm : (c.lu + (size_t)isl * c.nLmax * (c.nLmax + 1));
+  const int ld = nL + 1;
+  for (int e = tid; e < nL * ld; e += NT) {
+    const int i = e / ld, j = e - (e / ld) * ld;
+    double v;
+    if (j < nL) {
+      float h;
+      if (kp[i] && kp[j]) h = H[i * ldH + j]; else h = (i == j) ? 1.f : 0.f;
+      if (i == j) {
+        float hd = __fadd_rn(h, __fmul_rn(lam, h));
+        if (c.has_priors) {
+          const int pp = rp[i];
+          const float pi2 = kp[i] ? __fmul_rn(pinv[pp], pinv[pp]) : 0.f;
+          hd = __fadd_rn(hd, pi2);
+        }
+        hd = __fadd_rn(hd, 1e-8f);
+        v = (double)hd;
+      } else {
+        v = (double)h;
+      }
+    } else {
+      float gi = kp[i] ? g[i] : 0.f;
+      if (c.has_priors && kp[i]) {
+        const int pp = rp[i];
+        gi = __fadd_rn(gi, __fmul_rn(__fmul_rn(pinv[pp], pinv[pp]),
+                                     __fsub_rn(p[pp], pm[pp])));
+      }
+      v = (double)gi;
+    }
+    M[i * ld + j] = v;
+  }
+  __syncthreads();
+  if (nL > 0) lu_solve(M, nL, &piv, fac);
+  for (int i = tid; i < nL; i += NT) {
+    const int pp = rp[i];
+    float d = -(float)M[i * ld + nL];
+    if (!kp[i]) d = 0.f;
+    const int j = pp % 6;
+    const float cl = (j < 2) ? c.pos_step_max : (j < 5 ? 0.15f : 0.5f);
+    d = fminf(fmaxf(d, -cl), cl);
+    delta[i] = d;
+  }
+  __syncthreads();
+  float* out = (probe_mode == 1)
+                   ? c.probe_p + ((size_t)isl * 4 + probe_j) * nP
+                   : c.p_try + (size_t)isl * nP;
+  const float* lo = c.lower + (size_t)isl * nP;
+  const float* hi = c.upper + (size_t)isl * nP;
+  for (int q = tid; q < nP; q += NT) out[q] = p[q];
+  __syncthreads();
+  for (int i = tid; i < nL; i += NT) out[rp[i]] = __fadd_rn(p[rp[i]], delta[i]);
+  __syncthreads();
+  for (int q = tid; q < nP; q += NT) out[q] = fminf(fmaxf(out[q], lo[q]), hi[q]);
+}
+
+__global__ void k_accept(ClassDev c, int phase) {
+  const int isl = blockIdx.x * blockDim.x + threadIdx.x;
+  if (isl >= c.n_isl) return;
+  const uint8_t fl = c.flags[isl];
+  if (!isl_active(fl, phase)) return;
+  const int nP = c.nP;
+  const float* pt = c.p_try + (size_t)isl * nP;
+  float chi2_try = 0.f;
+  for (int b = 0; b < c.nb; ++b)
+    chi2_try = __fadd_rn(chi2_try, (float)c.chi2b[(size_t)isl * c.nb + b]);
+  if (c.has_priors) {
+    float pen = 0.f;
+    const float* pm = c.prior_mean + (size_t)isl * nP;
+    const float* pinv = c.prior_inv + (size_t)isl * nP;
+    for (int q = 0; q < nP; ++q) {
+      const int k = q / 6;
+      if (!(c.keep[(size_t)isl * nP + q] && c.mmask[isl * c.N + k])) continue;
+      const float t = __fmul_rn(pinv[q], __fsub_rn(pt[q], pm[q]));
+      pen = __fadd_rn(pen, __fmul_rn(t, t));
+    }
+    chi2_try = __fadd_rn(chi2_try, pen);
+  }
+  if (phase == PH_ALL) {
+    c.chi2[isl] = chi2_try;
+    return;
+  }
+  if (phase == PH_PROBE) {
+    const float d = __fsub_rn(chi2_try, c.chi2[isl]);
+    c.probe_best[isl] = fminf(c.probe_best[isl], d);
+    return;
+  }
+  float* p = c.p + (size_t)isl * nP;
+  const float chi2 = c.chi2[isl];
+  const float lam = c.lam[isl];
+  const bool accept = chi2_try < chi2;
+  const float lam_new = accept ? fmaxf(__fmul_rn(lam, 0.1f), 1e-9f)
+                               : fminf(__fmul_rn(lam, 10.0f), 1e6f);
+  const float dchi2 = __fsub_rn(chi2, chi2_try);
+  float pos_step = 0.f, shape_step = 0.f;
+  if (accept) {
+    for (int k = 0; k < c.N; ++k) {
+      const float mm = c.mmask[isl * c.N + k] ? 1.f : 0.f;
+      const float sx = __fsub_rn(pt[6 * k], p[6 * k]);
+      const float sy = __fsub_rn(pt[6 * k + 1], p[6 * k + 1]);
+      pos_step = fmaxf(pos_step, mm * hypotf(sx, sy));
+      for (int j = 2; j < 6; ++j)
+        shape_step = fmaxf(shape_step, mm * fabsf(__fsub_rn(pt[6 * k + j], p[6 * k + j])));
+    }
+  }
+  const bool small = accept && (dchi2 < __fmul_rn(c.ftol_rel, fmaxf(chi2, 1.0f)));
+  int consec = c.consec[isl];
+  consec = small ? consec + 1 : (accept ? 0 : consec);
+  const bool step_small = accept && (pos_step < c.step_tol) && (shape_step < 0.01f);
+  const int nrej = accept ? 0 : c.nrej[isl] + 1;
+  const bool stall_now = nrej >= 4;
+  const bool conv = (consec >= 2) || step_small || stall_now;
+  uint8_t nf = fl;
+  if (accept) {
+    for (int q = 0; q < nP; ++q) p[q] = pt[q];
+    c.chi2[isl] = chi2_try;
+    nf |= FL_NEEDLIN;
+  }
+  if (conv) nf |= FL_CONV;
+  if (stall_now) nf |= FL_STALL; else nf &= ~FL_STALL;
+  c.flags[isl] = nf;
+  c.lam[isl] = lam_new;
+  c.consec[isl] = consec;
+  c.nrej[isl] = nrej;
+  c.nst[isl] = c.nst[isl] + 1;
+}
+
+__global__ void k_count_active(ClassDev c) {
+  __shared__ int s[NT];
+  int t = 0;
+  for (int i = threadIdx.x; i < c.n_isl; i += NT) t += !(c.flags[i] & FL_CONV);
+  s[threadIdx.x] = t;
+  __syncthreads();
+  for (int st = NT / 2; st > 0; st >>= 1) {
+    if (threadIdx.x < st) s[threadIdx.x] += s[threadIdx.x + st];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *c.n_active = s[0];
+}
+
+__global__ void k_diverged_compare(ClassDev c, uint8_t* out) {
+  const int isl = blockIdx.x * blockDim.x + threadIdx.x;
+  if (isl >= c.n_isl) return;
+  if (!(c.flags[isl] & FL_PROBE)) {
+    out[isl] = 0;
+    return;
+  }
+  const float* q = c.probe_p + (size_t)isl * 4 * c.nP;
+  bool same = true;
+  for (int j = 1; j < 4; ++j)
+    for (int e = 0; e < c.nP; ++e) same = same && (q[j * c.nP + e] == q[e]);
+  out[isl] = same;
+}
+
+__global__ void k_set_probe(ClassDev c) {
+  const int isl = blockIdx.x * blockDim.x + threadIdx.x;
+  if (isl >= c.n_isl) return;
+  const uint8_t fl = c.flags[isl];
+  c.flags[isl] = (fl & FL_STALL) ? (fl | FL_PROBE) : (fl & ~FL_PROBE);
+}
+
+}  // namespace
+
+void launch_set_probe(const ClassDev& c, cudaStream_t s) {
+  k_set_probe<<<(unsigned)((c.n_isl + 127) / 128), 128, 0, s>>>(c);
+}
+
+size_t gram_lin_smem_bytes(int Kmax) {
+  const int nbk = (Kmax + 7) / 8;
+  const int TP = (Kmax <= 32) ? 128 : (Kmax <= 96 ? 64 : 32);
+  size_t zs = sizeof(float) * ((size_t)nbk * 8 * (TP + 1) + TP);
+  size_t red = sizeof(float) * (size_t)NT * 65;
+  return zs > red ? zs : red;
+}
+
+size_t gram_trial_smem_bytes(int N) { return gram_lin_smem_bytes(N + 1); }
+
+size_t assemble_smem_bytes(int nLmax, int N) {
+  (void)N;
+  return sizeof(double) * ((size_t)UPH_MAXN * (2 * UPH_MAXN + 1) +
+                           3 * (size_t)nLmax * UPH_MAXN + 3 * UPH_MAXN);
+}
+
+size_t step_smem_bytes(int nLmax) {
+  const int n = nLmax < 72 ? nLmax : 72;
+  return sizeof(double) * (size_t)n * (n + 1);
+}
+
+void launch_gram_lin(const ClassDev& c, cudaStream_t s) {
+  const int nbk = (c.Kmax + 7) / 8;
+  const int nblk = nbk * (nbk + 1) / 2;
+  const int parts = nblk <= NT ? 1 : (nblk + NT - 1) / NT;
+  dim3 grid((unsigned)(c.n_isl * c.nb), (unsigned)parts);
+  k_gram_lin<<<grid, NT, gram_lin_smem_bytes(c.Kmax), s>>>(c);
+}
+
+void launch_assemble(const ClassDev& c, cudaStream_t s) {
+  k_assemble<<<(unsigned)(c.n_isl * c.nb), NT, assemble_smem_bytes(c.nLmax, c.N), s>>>(c);
+}
+
+void launch_gram_trial(const ClassDev& c, const float* P, int phase,
+                       int final_mode, cudaStream_t s) {
+  k_gram_trial<<<(unsigned)(c.n_isl * c.nb), NT, gram_trial_smem_bytes(c.N), s>>>(
+      c, P, phase, final_mode);
+}
+
+void launch_step(const ClassDev& c, int phase, int probe_j, float probe_lam,
+                 int probe_mode, cudaStream_t s) {
+  k_step<<<(unsigned)c.n_isl, NT, step_smem_bytes(c.nLmax), s>>>(
+      c, phase, probe_mode, probe_j, probe_lam);
+}
+
+void launch_accept(const ClassDev& c, int phase, cudaStream_t s) {
+  k_accept<<<(unsigned)((c.n_isl + 127) / 128), 128, 0, s>>>(c, phase);
+}
+
+void launch_count_active(const ClassDev& c, cudaStream_t s) {
+  k_count_active<<<1, NT, 0, s>>>(c);
+}
+
+void launch_diverged_compare(const ClassDev& c, uint8_t* out,
+                             cudaStream_t s) {
+  k_diverged_compare<<<(unsigned)((c.n_isl + 127) / 128), 128, 0, s>>>(c, out);
+}
+
+int uph_solve_setup() {
+  cudaError_t e;
+  e = cudaFuncSetAttribute(k_gram_lin, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)gram_lin_smem_bytes(UPH_MAXK));
+  if (e != cudaSuccess) return (int)e;
+  e = cudaFuncSetAttribute(k_gram_trial, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)gram_trial_smem_bytes(UPH_MAXN));
+  if (e != cudaSuccess) return (int)e;
+  e = cudaFuncSetAttribute(k_assemble, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)assemble_smem_bytes(UPH_MAXLIVE, UPH_MAXN));
+  if (e != cudaSuccess) return (int)e;
+  e = cudaFuncSetAttribute(k_step, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)step_smem_bytes(UPH_MAXLIVE));
+  return (int)e;
+}

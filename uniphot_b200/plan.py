@@ -1,0 +1,402 @@
+"""Class planning, per-class host arrays and result unpacking (host numpy).
+
+Same contract as the reference's ``fit/grid_gpu/island_plan.py``:
+
+* ``plan_island_classes`` (:356) -- bucket -> (B, N, kind, tier T) classes;
+  islands with any extended member are "mixed" and take the smallest tier of
+  ``(native, 111, 221)`` covering ``2 * nre(n) * Re`` of their largest
+  extended member; buckets with ``nsrc > joint_nsrc_cap`` go to the giant
+  path.
+* ``class_host_arrays`` (:493) -- window origins, seeds, keep masks, box
+  bounds, priors.
+* ``unpack_class_results`` (:702) / ``giant_seed_rows`` (:1019) -- island
+  rows -> per-source rows.
+* ``free_n_gate`` (:199), ``ladder_width`` (:96), ``IslandFitResult`` (:221).
+"""
+
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+SOURCE_STAR = 0
+SOURCE_SERSIC = 3
+SERSIC_N_MIN = 0.29
+SERSIC_N_MAX = 6.3
+
+DEFAULT_MAX_STEPS = 30
+DEFAULT_MAX_STEPS_MAIN = 8
+DEFAULT_CHI2_FTOL_REL = 1e-4
+DEFAULT_STEP_TOL_PIX = 0.1
+DEFAULT_POS_STEP_MAX = 0.5
+DEFAULT_UN_FREEZE_STEPS = 0
+HARD_CHUNK_DIV = 4
+
+
+def ladder_width(n_rows: int, cap: int) -> int:
+    """Smallest power of two >= n_rows, capped at ``cap``."""
+    n = max(1, int(n_rows))
+    return int(min(1 << (n - 1).bit_length(), max(1, int(cap))))
+
+
+def sersic_n_to_u_np(n):
+    t = (np.clip(n, SERSIC_N_MIN + 1e-4, SERSIC_N_MAX - 1e-4) - SERSIC_N_MIN) \
+        / (SERSIC_N_MAX - SERSIC_N_MIN)
+    return np.log(t / (1.0 - t))
+
+
+def free_n_gate(source_type, s1_flux, s1_flux_var, fit_sersic_n, n_fit_min_snr):
+    """Free Sersic n for SERSIC rows whose median-band S1 S/N passes."""
+    st = np.asarray(source_type)
+    out = np.zeros(st.shape[0], dtype=bool)
+    if fit_sersic_n and bool(np.any(st == SOURCE_SERSIC)):
+        with np.errstate(divide="ignore", invalid="ignore"):
+            snr_b = np.abs(s1_flux) / np.sqrt(np.maximum(s1_flux_var, 1e-30))
+        snr = np.nanmedian(snr_b, axis=1)
+        out = (st == SOURCE_SERSIC) & np.isfinite(snr) & (snr >= float(n_fit_min_snr))
+    return out
+
+
+def _propagate_shape_sigmas(ee1, ee2, re, ell_err, theta_err, re_err):
+    """Catalog-frame (Re, ELL, THETA) prior sigmas -> internal
+    (logre, ee1, ee2) sigmas through the soft-ellipse Jacobian
+    (island_plan.py:103-192).  NaN where absent/invalid."""
+    ee1 = np.asarray(ee1, np.float64)
+    ee2 = np.asarray(ee2, np.float64)
+    re = np.asarray(re, np.float64)
+    ell_err = np.asarray(ell_err, np.float64)
+    theta_err = np.asarray(theta_err, np.float64)
+    re_err = np.asarray(re_err, np.float64)
+    re_ok = np.isfinite(re_err) & (re_err > 0) & (re > 0)
+    sig_lr = np.where(re_ok, re_err / np.where(re > 0, re, 1.0), np.nan)
+    mag = np.hypot(ee1, ee2)
+    e_s = 1.0 - np.exp(-mag)
+    ab = (1.0 - e_s) / np.maximum(1.0 + e_s, 1e-12)
+    phi = -np.degrees(np.arctan2(ee2, ee1) / 2.0)
+    ell = np.clip(1.0 - ab, 0.0, 0.999)
+    ang = np.radians(-2.0 * phi)
+    ba = 1.0 - ell
+    e = (1.0 - ba) / (1.0 + ba)
+    ee = -np.log(np.maximum(1.0 - e, 1e-15))
+    ca, sa = np.cos(ang), np.sin(ang)
+    dee = 1.0 / np.maximum((2.0 - ell) * (1.0 - ell), 1e-15)
+    k = 2.0 * np.pi / 180.0
+    ok = (np.isfinite(ell_err) & (ell_err > 0) & np.isfinite(theta_err)
+          & (theta_err > 0))
+    le = np.where(ok, ell_err, 0.0)
+    te = np.where(ok, theta_err, 0.0)
+    v1 = (dee * ca * le) ** 2 + (k * ee * sa * te) ** 2
+    v2 = (dee * sa * le) ** 2 + (k * ee * ca * te) ** 2
+    s1 = np.where(ok & (v1 > 0), np.sqrt(np.where(v1 > 0, v1, 1.0)), np.nan)
+    s2 = np.where(ok & (v2 > 0), np.sqrt(np.where(v2 > 0, v2, 1.0)), np.nan)
+    return sig_lr, s1, s2
+
+
+@dataclass
+class IslandClassPlan:
+    class_idx: int
+    bbox_class: int
+    nsrc_class: int
+    kind: str
+    tier: int
+    isl_ids: np.ndarray = field(repr=False)
+    midx: np.ndarray = field(repr=False)
+    mmask: np.ndarray = field(repr=False)
+    bbox: np.ndarray = field(repr=False)
+    n_src_of: np.ndarray = field(repr=False)
+    n_gal_class: int = 0
+    tangent_chunk: int = 6
+    chunk_main: int = 1
+    chunk_hard: int = 1
+
+    @property
+    def n_islands(self) -> int:
+        return int(self.isl_ids.shape[0])
+
+    @property
+    def key(self):
+        return (self.bbox_class, self.nsrc_class, self.kind, self.tier)
+
+
+def plan_island_classes(island_set, buckets, source_type, logre, sersic_n,
+                        native, *, joint_nsrc_cap=32, nsrc_max=None,
+                        log_fn=None, crossband_rank=0, tier_ladder=(111, 221)):
+    """Occupied buckets -> solver classes and the capped giant ids.
+
+    ``tier_ladder`` are the stamp tiers above the native one (the reference
+    hard-codes 111 and 221)."""
+    todo = {k: b for k, b in buckets.buckets.items()
+            if nsrc_max is None or k[1] <= int(nsrc_max)}
+    capped = []
+    if joint_nsrc_cap is not None:
+        for k in [k for k in list(todo) if k[1] > int(joint_nsrc_cap)]:
+            capped.extend(todo.pop(k).island_ids.tolist())
+        if capped and log_fn is not None:
+            log_fn(f"joint_nsrc_cap={joint_nsrc_cap}: {len(capped)} island(s) "
+                   f"-> giant path")
+    if not todo:
+        raise ValueError("no buckets selected")
+    st = np.asarray(source_type)
+    lr = np.asarray(logre)
+    sn = np.asarray(sersic_n)
+    plans = []
+    for (bc, nc) in sorted(todo):
+        b = todo[(bc, nc)]
+        ids = b.island_ids
+        midx = np.maximum(b.member_idx.astype(np.int64), 0)
+        mm = b.member_mask.astype(bool)
+        is_gal = (st[midx] != SOURCE_STAR) & mm
+        has_ext = is_gal.any(axis=1)
+        ngal = is_gal.sum(axis=1)
+        nre = np.where(sn[midx] < 1.5, 4.0, np.where(sn[midx] < 3.0, 6.0, 8.0))
+        half = np.where(is_gal, nre * np.exp(lr[midx].astype(float)), 0.0).max(axis=1)
+        ladder = [t for t in (native, *tier_ladder) if t >= native]
+        tier = np.full(ids.size, ladder[-1], np.int64)
+        for t in reversed(ladder):
+            tier = np.where(2 * half <= t, t, tier)
+        groups = [("star", native, np.nonzero(~has_ext)[0])]
+        for t in ladder:
+            groups.append(("mixed", int(t), np.nonzero(has_ext & (tier == t))[0]))
+        for kind, T, sel in groups:
+            if sel.size == 0:
+                continue
+            plans.append(IslandClassPlan(
+                class_idx=len(plans), bbox_class=int(bc), nsrc_class=int(nc),
+                kind=kind, tier=int(T), isl_ids=ids[sel].astype(np.int64),
+                midx=midx[sel], mmask=mm[sel], bbox=island_set.bbox[ids[sel]],
+                n_src_of=island_set.n_src[ids[sel]].astype(np.int32),
+                n_gal_class=int(ngal[sel].max()) if kind == "mixed" else 0))
+    return plans, capped
+
+
+def class_host_arrays(plan, *, pos_x, pos_y, source_type, logre, ee1, ee2,
+                      sersic_n, free_n_all, pos_max_shift_pix, pad,
+                      pos_err=None, re_prior_sig=None, ell_prior_sig=None,
+                      theta_prior_sig=None, sersic_n_prior_sig=None,
+                      s1_flux=None, cb_scale=None) -> dict:
+    """Per-class seeds, bounds, keep masks, window origins and priors."""
+    B, N, T = int(plan.bbox_class), int(plan.nsrc_class), int(plan.tier)
+    midx, mmask = plan.midx, plan.mmask
+    n_isl = plan.n_islands
+    bbox = plan.bbox
+    ox = bbox[:, 0] - (B - (bbox[:, 2] - bbox[:, 0])) // 2 + pad
+    oy = bbox[:, 1] - (B - (bbox[:, 3] - bbox[:, 1])) // 2 + pad
+    x0b = (ox - pad).astype(np.float32)
+    y0b = (oy - pad).astype(np.float32)
+    sx = np.asarray(pos_x)[midx].astype(np.float32)
+    sy = np.asarray(pos_y)[midx].astype(np.float32)
+    st = np.asarray(source_type)[midx].astype(np.int32)
+    lr = np.asarray(logre)[midx].astype(np.float32)
+    e1 = np.asarray(ee1)[midx].astype(np.float32)
+    e2 = np.asarray(ee2)[midx].astype(np.float32)
+    sn = np.asarray(sersic_n)[midx].astype(np.float32)
+    u0 = sersic_n_to_u_np(sn).astype(np.float32)
+    is_ext = st != SOURCE_STAR
+    G = int(plan.n_gal_class)
+    is_gal = is_ext & mmask
+    if G > 0:
+        order = np.argsort(~is_gal, axis=1, kind="stable")
+        gsel = order[:, :G].astype(np.int32)
+        gvalid = np.take_along_axis(is_gal, order, axis=1)[:, :G]
+    else:
+        gsel = np.zeros((n_isl, 0), np.int32)
+        gvalid = np.zeros((n_isl, 0), bool)
+
+    def gat(a):
+        if a is None:
+            return np.full((n_isl, N), np.nan)
+        return np.asarray(a, np.float64)[midx]
+    pe, rps, eps, tps, nps = (gat(pos_err), gat(re_prior_sig), gat(ell_prior_sig),
+                              gat(theta_prior_sig), gat(sersic_n_prior_sig))
+    has_n_prior = (st == SOURCE_SERSIC) & np.isfinite(nps) & (nps > 0) & mmask
+    fn_flag = (np.asarray(free_n_all)[midx] | has_n_prior) & mmask
+    keep = np.zeros((n_isl, N, 6), bool)
+    keep[:, :, 0:2] = mmask[:, :, None]
+    keep[:, :, 2:5] = (is_ext & mmask)[:, :, None]
+    keep[:, :, 5] = fn_flag
+    p0 = np.stack([sx, sy, lr, e1, e2, u0], axis=2).astype(np.float32)
+    one = np.ones((n_isl, N), np.float32)
+    lower = np.stack([sx - pos_max_shift_pix, sy - pos_max_shift_pix,
+                      np.full((n_isl, N), np.log(0.1), np.float32),
+                      -100 * one, -100 * one, -12 * one], axis=2).astype(np.float32)
+    upper = np.stack([sx + pos_max_shift_pix, sy + pos_max_shift_pix,
+                      np.full((n_isl, N), np.log(0.75 * T), np.float32),
+                      100 * one, 100 * one, 12 * one], axis=2).astype(np.float32)
+    inv = np.zeros((n_isl, N, 6))
+    pos_ok = np.isfinite(pe) & (pe > 0) & mmask
+    pinv = np.where(pos_ok, 1.0 / np.where(pos_ok, pe, 1.0), 0.0)
+    inv[:, :, 0] = pinv
+    inv[:, :, 1] = pinv
+    ext_ok = is_ext & mmask
+    s_lr, s_e1, s_e2 = _propagate_shape_sigmas(e1, e2, np.exp(lr.astype(np.float64)),
+                                               eps, tps, rps)
+    ok = ext_ok & np.isfinite(s_lr) & (s_lr > 0)
+    inv[:, :, 2] = np.where(ok, 1.0 / np.where(ok, s_lr, 1.0), 0.0)
+    ok = ext_ok & np.isfinite(s_e1) & (s_e1 > 0) & np.isfinite(s_e2) & (s_e2 > 0)
+    inv[:, :, 3] = np.where(ok, 1.0 / np.where(ok, s_e1, 1.0), 0.0)
+    inv[:, :, 4] = np.where(ok, 1.0 / np.where(ok, s_e2, 1.0), 0.0)
+    sn64 = sn.astype(np.float64)
+    dndu = (sn64 - SERSIC_N_MIN) * (SERSIC_N_MAX - sn64) / (SERSIC_N_MAX - SERSIC_N_MIN)
+    inv[:, :, 5] = np.where(has_n_prior, dndu / np.where(has_n_prior, nps, 1.0), 0.0)
+    pinv32 = inv.astype(np.float32)
+    msf = None
+    if s1_flux is not None:
+        msf = (np.asarray(s1_flux, np.float32)[midx]
+               * (mmask & ~is_ext)[:, :, None]).astype(np.float32)
+    out = dict(ox=ox, oy=oy, x0b=x0b, y0b=y0b, st=st, lr=lr, e1=e1, e2=e2,
+               sn=sn, fn_flag=fn_flag, is_ext=is_ext, mmask=mmask, keep=keep,
+               gsel=gsel, gvalid=gvalid, p0=p0, lower=lower, upper=upper,
+               prior_mean=p0.copy(), prior_inv_sigma=pinv32,
+               has_priors=bool(np.any(pinv32 != 0)), member_s1_flux=msf)
+    if cb_scale is not None:
+        cs = np.asarray(cb_scale, np.float64)[midx]
+        out["cb_scale"] = (np.where(mmask, cs, 0.0).sum(axis=1)
+                           / np.maximum(mmask.sum(axis=1), 1)).astype(np.float32)
+    return out
+
+
+@dataclass
+class IslandFitResult:
+    """Per-source rows for every fitted or giant island member."""
+    bandnames: list
+    source_idx: np.ndarray
+    pos_x: np.ndarray
+    pos_y: np.ndarray
+    logre: np.ndarray
+    ee1: np.ndarray
+    ee2: np.ndarray
+    sersic_n: np.ndarray
+    fluxes: np.ndarray
+    flux_err: np.ndarray
+    chi2: np.ndarray
+    n_steps: np.ndarray
+    converged: np.ndarray
+    free_n: np.ndarray
+    stalled: np.ndarray = None
+    diverged: np.ndarray = None
+    stall_dchi2: np.ndarray = None
+    railed: np.ndarray = None
+    chi2_nu: np.ndarray = None
+    island_id: np.ndarray = None
+    island_nsrc: np.ndarray = None
+    island_giant: np.ndarray = None
+    re_upper_pix: np.ndarray = None
+    pos_x_err: np.ndarray = None
+    pos_y_err: np.ndarray = None
+    re_err: np.ndarray = None
+    re_prof_lo: np.ndarray = None
+    re_prof_hi: np.ndarray = None
+    ell_err: np.ndarray = None
+    theta_err: np.ndarray = None
+    sersic_n_err: np.ndarray = None
+    pos_x_prior_frac: np.ndarray = None
+    pos_y_prior_frac: np.ndarray = None
+    re_prior_frac: np.ndarray = None
+    ell_prior_frac: np.ndarray = None
+    theta_prior_frac: np.ndarray = None
+    sersic_n_prior_frac: np.ndarray = None
+    rchisq: np.ndarray = None
+    fracflux: np.ndarray = None
+    fracin: np.ndarray = None
+    fracmasked: np.ndarray = None
+    flux_win: np.ndarray = None
+    flux_marg_var: np.ndarray = None
+    bucket_stats: list = field(default_factory=list)
+
+    @property
+    def requeue_idx(self):
+        return self.source_idx[~self.converged]
+
+
+def _nan(n):
+    return np.full(n, np.nan, np.float32)
+
+
+def unpack_class_results(plan, host, island_set, res_p, res_f, res_fe,
+                         res_chi2, res_conv, res_stall, res_nst,
+                         res_perr=None, res_pdchi2=None, res_div=None,
+                         res_ngood=None, n_bands=0, **_unused) -> dict:
+    """Island rows -> source rows for the valid member slots.
+
+    Parameter-error, profile and metric columns are NaN here: their
+    kernels are not built (they are post-convergence options that are off by
+    default in ``island_fit``)."""
+    midx, mmask, is_ext = plan.midx, host["mmask"], host["is_ext"]
+    fn = host["fn_flag"]
+    ii, kk = np.nonzero(mmask)
+    u = res_p[:, :, 5]
+    nfree = SERSIC_N_MIN + (SERSIC_N_MAX - SERSIC_N_MIN) / (1.0 + np.exp(-u))
+    nfin = np.where(fn, nfree, host["sn"]).astype(np.float32)
+    n = ii.size
+    if res_ngood is not None and int(n_bands) > 0:
+        keep_isl = (host["keep"] & mmask[:, :, None]).reshape(mmask.shape[0], -1).sum(axis=1)
+        nfree_isl = keep_isl + float(n_bands) * mmask.sum(axis=1)
+        dof = res_ngood.astype(np.float64) - nfree_isl
+        with np.errstate(invalid="ignore", divide="ignore"):
+            cn = np.where((dof > 0) & np.isfinite(res_chi2),
+                          res_chi2 / np.maximum(dof, 1.0), np.nan)
+        chi2_nu = cn[ii].astype(np.float32)
+    else:
+        chi2_nu = _nan(n)
+    nb = max(int(n_bands), 0)
+    return dict(
+        src=midx[ii, kk],
+        pos_x=res_p[ii, kk, 0], pos_y=res_p[ii, kk, 1],
+        logre=np.where(is_ext[ii, kk], res_p[ii, kk, 2], host["lr"][ii, kk]),
+        ee1=np.where(is_ext[ii, kk], res_p[ii, kk, 3], host["e1"][ii, kk]),
+        ee2=np.where(is_ext[ii, kk], res_p[ii, kk, 4], host["e2"][ii, kk]),
+        sersic_n=nfin[ii, kk], fluxes=res_f[ii, :, kk], flux_err=res_fe[ii, :, kk],
+        chi2=res_chi2[ii], chi2_nu=chi2_nu, n_steps=res_nst[ii],
+        converged=res_conv[ii], stalled=res_stall[ii],
+        diverged=(res_div[ii] if res_div is not None else np.zeros(n, bool)),
+        stall_dchi2=(res_pdchi2[ii].astype(np.float32) if res_pdchi2 is not None
+                     else _nan(n)),
+        railed=np.zeros(n, bool), free_n=fn[ii, kk],
+        island_id=plan.isl_ids[ii].astype(np.int32),
+        island_nsrc=island_set.n_src[plan.isl_ids][ii].astype(np.int32),
+        island_giant=np.zeros(n, bool),
+        re_upper_pix=np.exp(host["upper"][ii, kk, 2].astype(np.float64)).astype(np.float32),
+        pos_x_err=_nan(n), pos_y_err=_nan(n), re_err=_nan(n), ell_err=_nan(n),
+        theta_err=_nan(n), re_prof_lo=_nan(n), re_prof_hi=_nan(n),
+        sersic_n_err=_nan(n), pos_x_prior_frac=_nan(n), pos_y_prior_frac=_nan(n),
+        re_prior_frac=_nan(n), ell_prior_frac=_nan(n), theta_prior_frac=_nan(n),
+        sersic_n_prior_frac=_nan(n), rchisq=_nan(n), fracflux=_nan(n),
+        fracin=_nan(n), fracmasked=_nan(n),
+        flux_win=np.full((n, nb), np.nan, np.float32),
+        flux_marg_var=np.full((n, nb), np.nan, np.float32))
+
+
+def giant_seed_rows(giant_ids, island_set, *, pos_x, pos_y, logre, ee1, ee2,
+                    sersic_n, n_bands) -> list:
+    """Giant islands keep the seed geometry; nothing is solved."""
+    rows = []
+    nb = max(int(n_bands), 0)
+    for g in sorted(int(i) for i in np.asarray(giant_ids).ravel()):
+        src = np.asarray(island_set.members[g], np.int64)
+        n = src.size
+        nn = lambda: _nan(n)  # noqa: E731
+        rows.append(dict(
+            src=src,
+            pos_x=np.asarray(pos_x)[src].astype(np.float32),
+            pos_y=np.asarray(pos_y)[src].astype(np.float32),
+            logre=np.asarray(logre)[src].astype(np.float32),
+            ee1=np.asarray(ee1)[src].astype(np.float32),
+            ee2=np.asarray(ee2)[src].astype(np.float32),
+            sersic_n=np.asarray(sersic_n)[src].astype(np.float32),
+            fluxes=np.full((n, nb), np.nan, np.float32),
+            flux_err=np.full((n, nb), np.nan, np.float32),
+            chi2=nn(), chi2_nu=nn(), n_steps=np.zeros(n, np.int32),
+            converged=np.ones(n, bool), stalled=np.zeros(n, bool),
+            diverged=np.zeros(n, bool), stall_dchi2=nn(),
+            railed=np.zeros(n, bool), free_n=np.zeros(n, bool),
+            island_id=np.full(n, g, np.int32), island_nsrc=np.full(n, n, np.int32),
+            island_giant=np.ones(n, bool), re_upper_pix=nn(),
+            pos_x_err=nn(), pos_y_err=nn(), re_err=nn(), ell_err=nn(),
+            re_prof_lo=nn(), re_prof_hi=nn(), theta_err=nn(), sersic_n_err=nn(),
+            pos_x_prior_frac=nn(), pos_y_prior_frac=nn(), re_prior_frac=nn(),
+            ell_prior_frac=nn(), theta_prior_frac=nn(), sersic_n_prior_frac=nn(),
+            rchisq=nn(), fracflux=nn(), fracin=nn(), fracmasked=nn(),
+            flux_win=np.full((n, nb), np.nan, np.float32),
+            flux_marg_var=np.full((n, nb), np.nan, np.float32)))
+    return rows

@@ -1,0 +1,456 @@
+"""Drop-in replacement of the reference's island solver entry points.
+
+Mirrors ``tract7dt/fit/grid_gpu/island_solver.py``:
+
+* ``build_psf_tree(psfs, tier)``           (:1851-1871)
+* ``make_class_kernels(plan, n_bands, n_terms, ...)``  (:1874-1922)
+* ``run_class_chunk(kernels, psf_tree, host, rows, width, max_steps,
+  dstack_dev, wstack_dev, pad, init_state=None, ...)``  (:2793-3131)
+* ``run_class_chunk_resilient`` (:3165-3230) -- width halving on
+  ``RESOURCE_EXHAUSTED``
+* ``island_fit(**kw)``                    (:3233-3595)
+
+with the same argument meaning, array layouts, result dict keys, flags and
+``ValueError`` on invalid option values.  All arithmetic runs in the CUDA
+library behind ``include/uniphot_b200.h``; there is no CPU path.
+
+Differences, by design:
+
+* the LM loop runs on the device for the whole step budget: the reference's
+  main pass (``max_steps_main`` steps) plus hard re-queue carrying the exact
+  LM state is the same per-island trajectory, so one pass of ``max_steps``
+  is run (``bucket_stats`` still reports the counts);
+* ``dstack_dev`` is a :class:`DeviceField` (the field stacks resident in
+  HBM inside the library context); ``wstack_dev`` is accepted and ignored;
+* options whose kernels are not built (trust-region, "changed"/"dlnp"
+  protocols, crossband GLS, scene subtract, post-convergence error / metric
+  / profile kernels) raise ``ValueError``.
+"""
+
+from __future__ import annotations
+
+import time
+from dataclasses import dataclass
+from typing import Callable, Optional
+
+import numpy as np
+
+from . import _lib
+from .plan import (DEFAULT_CHI2_FTOL_REL, DEFAULT_MAX_STEPS,
+                   DEFAULT_MAX_STEPS_MAIN, DEFAULT_POS_STEP_MAX,
+                   DEFAULT_STEP_TOL_PIX, DEFAULT_UN_FREEZE_STEPS,
+                   IslandFitResult, class_host_arrays, free_n_gate,
+                   giant_seed_rows, plan_island_classes, unpack_class_results)
+from .psf import MogPsf
+from .sersic import load_table
+
+SOURCE_STAR = 0
+DEVICE_MAX_NSRC = 32
+_CARRY_KEYS = ("p", "lam", "chi2", "consec", "nrej", "nst", "diverged",
+               "n_same", "prej")
+
+
+def _is_mog(psf) -> bool:
+    return isinstance(psf, MogPsf) or hasattr(psf, "sigma") and hasattr(psf, "weight")
+
+
+def _pad_coefs(psf, tier: int) -> np.ndarray:
+    """Zero-pad a pixelised PSF to (tier, tier), centre pixel kept at H//2
+    (island_solver.py:193-206)."""
+    coefs = np.asarray(psf.coefs, np.float32)
+    H, W = coefs.shape[:2]
+    if tier <= H and tier <= W:
+        return coefs
+    out = np.zeros((tier, tier) + coefs.shape[2:], np.float32)
+    y0, x0 = (tier - H) // 2, (tier - W) // 2
+    out[y0:y0 + H, x0:x0 + W] = coefs
+    return out
+
+
+@dataclass
+class PsfTree:
+    """Per-band PSF stack for one tier, ready for upload."""
+    mode: str                  # "reference" | "analytic"
+    tier: int
+    params: np.ndarray         # (nb, T, T, nt) or (nb, K, 4, nt)
+    origin_scale: np.ndarray   # (nb, 4)
+
+    @property
+    def n_terms(self) -> int:
+        return int(self.params.shape[-1])
+
+
+def build_psf_tree(psfs: list, tier: int):
+    """Stack the per-band PSFs (zero-padded to ``tier``) -> (tree, n_terms)."""
+    os_ = np.array([[p.x_origin, p.x_scale, p.y_origin, p.y_scale] for p in psfs],
+                   np.float32)
+    if _is_mog(psfs[0]):
+        K = max(int(np.asarray(p.sigma).shape[0]) for p in psfs)
+        nt = int(np.asarray(psfs[0].sigma).shape[1])
+        par = np.zeros((len(psfs), K, 4, nt), np.float32)
+        for b, p in enumerate(psfs):
+            k = np.asarray(p.sigma).shape[0]
+            par[b, :k, 0] = p.sigma
+            par[b, :k, 1] = p.e1
+            par[b, :k, 2] = p.e2
+            par[b, :k, 3] = p.weight
+            if k < K:       # unused components: unit sigma, zero weight
+                par[b, k:, 0, 0] = 1.0
+        tree = PsfTree("analytic", int(tier), par, os_)
+    else:
+        par = np.stack([_pad_coefs(p, int(tier)) for p in psfs]).astype(np.float32)
+        tree = PsfTree("reference", int(tier), par, os_)
+    return tree, tree.n_terms
+
+
+class DeviceField:
+    """The padded field stacks resident on one device (a library context).
+
+    Plays the role of the reference's ``dstack_dev``/``wstack_dev``."""
+
+    def __init__(self, data_pad: np.ndarray, invvar_pad: np.ndarray, pad: int,
+                 device: int = 0, context: Optional[_lib.Context] = None):
+        self.ctx = context if context is not None else _lib.Context(device)
+        self.ctx.upload_field(data_pad, invvar_pad, pad)
+        self.pad = int(pad)
+        self.n_bands = int(data_pad.shape[0])
+        self.shape = tuple(data_pad.shape)
+        self._psf_key = {}
+        self._mog_key = None
+        self._table = False
+
+    def ensure_psf(self, tree: PsfTree):
+        if tree.mode == "reference":
+            key = id(tree)
+            if self._psf_key.get(tree.tier) != key:
+                self.ctx.upload_psf_poly(tree.tier, tree.params, tree.origin_scale)
+                self._psf_key[tree.tier] = key
+        else:
+            key = id(tree)
+            if self._mog_key != key:
+                self.ctx.upload_psf_mog(tree.params, tree.origin_scale)
+                self._mog_key = key
+
+    def ensure_table(self):
+        if not self._table:
+            self.ctx.upload_sersic_table(load_table())
+            self._table = True
+
+
+@dataclass
+class ClassKernels:
+    """Opaque per-class handle (the reference returns a 16-tuple of jitted
+    programs; here it is the class descriptor of the CUDA solver)."""
+    desc: _lib.ClassDesc
+    render_mode: str
+    n_bands: int
+    kind: str
+    step_protocol: str = "proposals"
+    step_mode: str = "clip"
+
+
+def make_class_kernels(plan, n_bands: int, n_terms: int, *, render_backend: str,
+                       reg: float, pos_step_max_pix: float, chi2_ftol_rel: float,
+                       step_tol_pix: float, un_freeze_steps: int,
+                       star_render_split: bool = True, has_priors: bool = False,
+                       stall_count_mode: str = "proposals", step_mode: str = "clip",
+                       scene_subtract: bool = False, crossband: dict | None = None,
+                       convergence: str = "legacy", plateau_dlnp_tol: float = 0.5,
+                       render_mode: str = "reference") -> ClassKernels:
+    if stall_count_mode not in ("proposals", "changed"):
+        raise ValueError(f"stall_count_mode must be 'proposals' or 'changed', "
+                         f"got {stall_count_mode!r}")
+    if step_mode not in ("clip", "trust_region"):
+        raise ValueError(f"step_mode must be 'clip' or 'trust_region', got {step_mode!r}")
+    if convergence not in ("legacy", "dlnp"):
+        raise ValueError(f"convergence must be 'legacy' or 'dlnp', got {convergence!r}")
+    if convergence == "dlnp" and step_mode != "clip":
+        raise ValueError("convergence='dlnp' requires step_mode='clip' "
+                         "(trust-region support pending)")
+    if convergence == "dlnp" and stall_count_mode == "changed":
+        raise ValueError("convergence='dlnp' subsumes stall_count_mode='changed' "
+                         "(distinct-proposal counting is the dlnp behavior); "
+                         "leave stall_count_mode at 'proposals'")
+    if render_backend not in ("fft", "direct", "auto"):
+        raise ValueError(f"unknown render_backend: {render_backend!r}")
+    if render_mode not in ("reference", "analytic"):
+        raise ValueError(f"render_mode must be 'reference' or 'analytic', "
+                         f"got {render_mode!r}")
+    unsupported = []
+    if stall_count_mode != "proposals":
+        unsupported.append("stall_count_mode='changed'")
+    if step_mode == "trust_region" and plan.kind != "star":
+        unsupported.append("step_mode='trust_region'")
+    if convergence != "legacy":
+        unsupported.append("convergence='dlnp'")
+    if crossband is not None:
+        unsupported.append("crossband")
+    if scene_subtract:
+        unsupported.append("scene_subtract")
+    if unsupported:
+        raise ValueError("not supported by the B200 island solver: "
+                         + ", ".join(unsupported))
+    if int(plan.nsrc_class) > DEVICE_MAX_NSRC:
+        raise ValueError(f"nsrc class {plan.nsrc_class} exceeds the device limit "
+                         f"{DEVICE_MAX_NSRC}; lower joint_nsrc_cap")
+    desc = _lib.ClassDesc(
+        bbox=int(plan.bbox_class), nsrc=int(plan.nsrc_class), tier=int(plan.tier),
+        render_mode=_lib.RENDER_MODES[render_mode], reg=float(reg),
+        pos_step_max=float(pos_step_max_pix), chi2_ftol_rel=float(chi2_ftol_rel),
+        step_tol_pix=float(step_tol_pix), un_freeze_steps=int(un_freeze_steps),
+        has_priors=int(bool(has_priors)))
+    return ClassKernels(desc, render_mode, int(n_bands), str(plan.kind))
+
+
+def _slice_host(host: dict, rows: np.ndarray) -> dict:
+    keys = ("ox", "oy", "x0b", "y0b", "st", "sn", "fn_flag", "mmask", "keep",
+            "p0", "lower", "upper", "prior_mean", "prior_inv_sigma")
+    return {k: np.asarray(host[k])[rows] for k in keys}
+
+
+def run_class_chunk(kernels: ClassKernels, psf_tree: PsfTree, host: dict,
+                    rows: np.ndarray, width: int, max_steps: int, dstack_dev,
+                    wstack_dev, pad: int, init_state: dict | None = None,
+                    compute_param_errors: bool = False, want_residual: bool = False,
+                    compute_source_metrics: bool = False,
+                    compute_flux_marg: bool = False,
+                    compute_re_profile: bool = False) -> dict:
+    """Fit one chunk of a class; returns the reference's result dict."""
+    t0 = time.perf_counter()
+    rows = np.asarray(rows, np.int64)
+    n_c = int(rows.size)
+    if int(width) < n_c:
+        raise ValueError(f"chunk width {width} < rows {n_c}")
+    for flag, name in ((compute_param_errors, "compute_param_errors"),
+                       (want_residual, "want_residual"),
+                       (compute_source_metrics, "compute_source_metrics"),
+                       (compute_flux_marg, "compute_flux_marg"),
+                       (compute_re_profile, "compute_re_profile")):
+        if flag:
+            raise ValueError(f"{name} is not supported by the B200 island solver")
+    if not isinstance(dstack_dev, DeviceField):
+        raise ValueError("dstack_dev must be a uniphot_b200.solver.DeviceField")
+    if int(pad) != dstack_dev.pad:
+        raise ValueError(f"pad {pad} != the uploaded field's pad {dstack_dev.pad}")
+    dstack_dev.ensure_psf(psf_tree)
+    if np.any(np.asarray(host["st"])[rows] != SOURCE_STAR):
+        dstack_dev.ensure_table()
+    N = int(host["mmask"].shape[1])
+    arrays = _slice_host(host, rows)
+    init = None
+    if init_state is not None:
+        init = {k: np.asarray(init_state[k]) for k in ("p", "lam", "chi2", "consec",
+                                                       "nrej", "nst")}
+    out = dstack_dev.ctx.run_chunk(kernels.desc, arrays, int(max_steps),
+                                   kernels.n_bands, init)
+    nP = 6 * N
+    out.update(perr=None, femarg=None, reprof=None, smetrics=None, swin=None,
+               resid=None, resid_w=None, railed=np.zeros(n_c, bool),
+               n_same=np.zeros(n_c, np.int32), prej=np.zeros((n_c, nP), np.float32),
+               wall_s=time.perf_counter() - t0)
+    return out
+
+
+def run_class_chunk_resilient(kernels, psf_tree, host, rows, width, max_steps,
+                              dstack_dev, wstack_dev, pad, *, init_state=None,
+                              log_fn=None, **kw) -> dict:
+    """run_class_chunk, halving the chunk on a device-memory failure."""
+    try:
+        out = run_class_chunk(kernels, psf_tree, host, rows, width, max_steps,
+                              dstack_dev, wstack_dev, pad, init_state=init_state, **kw)
+        out["widths_ran"] = [int(width)]
+        out["halved"] = False
+        return out
+    except _lib.UphError as exc:
+        n_c = int(np.asarray(rows).size)
+        if "RESOURCE_EXHAUSTED" not in str(exc) or n_c <= 1:
+            raise
+        half = max(1, int(width) // 2)
+        msg = (f"island chunk of {n_c} at width {width} hit {exc!s:.80} -- "
+               f"retrying as chunk(s) of width {half}")
+        (log_fn or (lambda m: print("island: " + m, flush=True)))(msg)
+        parts = []
+        for lo in range(0, n_c, half):
+            sl = slice(lo, min(lo + half, n_c))
+            sub = None if init_state is None else {k: v[sl] for k, v in init_state.items()}
+            parts.append(run_class_chunk_resilient(
+                kernels, psf_tree, host, np.asarray(rows)[sl], half, max_steps,
+                dstack_dev, wstack_dev, pad, init_state=sub, log_fn=log_fn, **kw))
+        merged = dict(parts[0])
+        for k, v0 in parts[0].items():
+            if k in ("wall_s", "steps_run", "widths_ran", "halved"):
+                continue
+            if isinstance(v0, np.ndarray):
+                merged[k] = np.concatenate([p[k] for p in parts], axis=0)
+        merged["wall_s"] = float(sum(p["wall_s"] for p in parts))
+        merged["steps_run"] = int(max(p["steps_run"] for p in parts))
+        merged["widths_ran"] = sorted({w for p in parts for w in p["widths_ran"]})
+        merged["halved"] = True
+        return merged
+
+
+def _chunk_size(plan, n_bands: int, budget_bytes: float) -> int:
+    """Islands per chunk under a device scratch budget (stamps, Gram, GN
+    blocks dominate)."""
+    N, B, T = int(plan.nsrc_class), int(plan.bbox_class), int(plan.tier)
+    Sz = min(T, B)
+    R = 7 if plan.kind == "mixed" else 3
+    nL = N * (6 if plan.kind == "mixed" else 2)
+    K = nL + N + 1
+    per = 4.0 * n_bands * (N * R * Sz * Sz + K * K + nL * nL + nL) + 8.0 * nL * nL
+    return int(max(1, min(plan.n_islands, budget_bytes // max(per, 1.0))))
+
+
+def island_fit(*, bandnames: list, data_minus_bg: np.ndarray, invvar: np.ndarray,
+               psfs: list, island_set, buckets, pos_x, pos_y, source_type, logre,
+               ee1, ee2, sersic_n, s1_flux, s1_flux_var, pos_err=None,
+               re_prior_sig=None, ell_prior_sig=None, theta_prior_sig=None,
+               sersic_n_prior_sig=None, render_backend: str = "fft",
+               fit_sersic_n: bool = True, n_fit_min_snr: float = 30.0,
+               pos_max_shift_pix: float = 5.0,
+               pos_step_max_pix: float = DEFAULT_POS_STEP_MAX,
+               max_steps: int = DEFAULT_MAX_STEPS,
+               max_steps_main: int | None = DEFAULT_MAX_STEPS_MAIN,
+               chi2_ftol_rel: float = DEFAULT_CHI2_FTOL_REL,
+               step_tol_pix: float = DEFAULT_STEP_TOL_PIX,
+               un_freeze_steps: int = DEFAULT_UN_FREEZE_STEPS, reg: float = 1e-9,
+               nsrc_max: int | None = None, joint_nsrc_cap: int = 32,
+               star_render_split: bool = True, stall_count_mode: str = "proposals",
+               convergence: str = "legacy", plateau_dlnp_tol: float = 0.5,
+               include_giants: bool = True, compute_param_errors: bool = False,
+               compute_source_metrics: bool = False, compute_re_profile: bool = False,
+               return_island_residual: bool = False, free_n_override=None,
+               log_fn: Optional[Callable[[str], None]] = None,
+               render_mode: str | None = None, tier_ladder=(111, 221),
+               native_stamp: int | None = None, device: int = 0,
+               field: DeviceField | None = None,
+               chunk_budget_bytes: float = 16e9):
+    """Fit all bucketed islands (+ giants), class by class, on the GPU."""
+    def log(msg):
+        if log_fn is not None:
+            log_fn(msg)
+    for flag, name in ((compute_param_errors, "compute_param_errors"),
+                       (compute_source_metrics, "compute_source_metrics"),
+                       (compute_re_profile, "compute_re_profile"),
+                       (return_island_residual, "return_island_residual")):
+        if flag:
+            raise ValueError(f"{name} is not supported by the B200 island solver")
+    if render_mode is None:
+        render_mode = "analytic" if _is_mog(psfs[0]) else "reference"
+    n_bands = len(bandnames)
+    if native_stamp is not None:
+        native = int(native_stamp)
+    elif render_mode == "reference":
+        native = int(psfs[0].H_psf)
+    else:
+        native = _native_for_mog(psfs)
+    if free_n_override is not None:
+        free_n_all = np.asarray(free_n_override, bool)
+    else:
+        free_n_all = free_n_gate(source_type, s1_flux, s1_flux_var, fit_sersic_n,
+                                 n_fit_min_snr)
+    plans, capped = plan_island_classes(
+        island_set, buckets, source_type, logre, sersic_n, native,
+        joint_nsrc_cap=joint_nsrc_cap, nsrc_max=nsrc_max, log_fn=log_fn,
+        tier_ladder=tier_ladder)
+    occupied_B = max((p.bbox_class for p in plans), default=32)
+    PAD = int(occupied_B) + 8
+    H, W = data_minus_bg.shape[1], data_minus_bg.shape[2]
+    if field is None or field.pad != PAD or field.shape != (n_bands, H + 2 * PAD,
+                                                           W + 2 * PAD):
+        dstack = np.zeros((n_bands, H + 2 * PAD, W + 2 * PAD), np.float32)
+        wstack = np.zeros_like(dstack)
+        dstack[:, PAD:PAD + H, PAD:PAD + W] = data_minus_bg
+        wstack[:, PAD:PAD + H, PAD:PAD + W] = invvar
+        field = DeviceField(dstack, wstack, PAD, device=device,
+                            context=field.ctx if field is not None else None)
+        del dstack, wstack
+    src_kwargs = dict(pos_x=pos_x, pos_y=pos_y, source_type=source_type, logre=logre,
+                      ee1=ee1, ee2=ee2, sersic_n=sersic_n, free_n_all=free_n_all,
+                      pos_max_shift_pix=float(pos_max_shift_pix), pad=PAD,
+                      pos_err=pos_err, re_prior_sig=re_prior_sig,
+                      ell_prior_sig=ell_prior_sig, theta_prior_sig=theta_prior_sig,
+                      sersic_n_prior_sig=sersic_n_prior_sig)
+    out_rows, bucket_stats = [], []
+    trees = {}
+    for plan in plans:
+        B, N, T, kind = int(plan.bbox_class), int(plan.nsrc_class), int(plan.tier), plan.kind
+        n_isl = plan.n_islands
+        t_b = time.perf_counter()
+        host = class_host_arrays(plan, **src_kwargs)
+        if T not in trees:
+            trees[T] = build_psf_tree(psfs, T)
+        tree, n_terms = trees[T]
+        kern = make_class_kernels(
+            plan, n_bands, n_terms, render_backend=render_backend, reg=reg,
+            pos_step_max_pix=pos_step_max_pix, chi2_ftol_rel=chi2_ftol_rel,
+            step_tol_pix=step_tol_pix, un_freeze_steps=un_freeze_steps,
+            star_render_split=star_render_split, has_priors=bool(host["has_priors"]),
+            stall_count_mode=stall_count_mode, convergence=convergence,
+            plateau_dlnp_tol=plateau_dlnp_tol, render_mode=render_mode)
+        chunk = _chunk_size(plan, n_bands, chunk_budget_bytes)
+        res = {}
+        for lo in range(0, n_isl, chunk):
+            rows = np.arange(lo, min(lo + chunk, n_isl))
+            o = run_class_chunk_resilient(kern, tree, host, rows, rows.size, max_steps,
+                                          field, field, PAD, log_fn=log_fn)
+            for k, v in o.items():
+                if isinstance(v, np.ndarray):
+                    res.setdefault(k, []).append(v)
+        res = {k: np.concatenate(v, axis=0) for k, v in res.items()}
+        dt = time.perf_counter() - t_b
+        nst = res["nst"]
+        bucket_stats.append(dict(
+            bbox_class=B, nsrc_class=N, tier=T, kind=kind, n_islands=int(n_isl),
+            n_chunks=int(np.ceil(n_isl / chunk)), chunk=chunk, wall_s=dt,
+            islands_per_s=n_isl / dt if dt > 0 else float("inf"),
+            mean_steps=float(nst.mean()), max_steps_used=int(nst.max()),
+            n_unconverged=int((~res["conv"]).sum()), n_stalled=int(res["stall"].sum()),
+            n_requeued=int((nst > (max_steps_main or max_steps)).sum())))
+        log(f"bucket bbox={B} nsrc={N} kind={kind} tier={T}: {n_isl} islands, "
+            f"{dt:.2f}s ({n_isl / max(dt, 1e-9):.0f} isl/s), "
+            f"mean_steps={nst.mean():.1f}")
+        out_rows.append(unpack_class_results(
+            plan, host, island_set, res["p"], res["fluxes"], res["ferr"], res["chi2"],
+            res["conv"], res["stall"], res["nst"], res_pdchi2=res["stall_dchi2"],
+            res_div=res["diverged"], res_ngood=res["n_good"], n_bands=n_bands))
+    giant_ids = np.concatenate([np.asarray(buckets.giant_ids, np.int64).ravel(),
+                                np.asarray(capped, np.int64)])
+    if include_giants and giant_ids.size:
+        out_rows.extend(giant_seed_rows(giant_ids, island_set, pos_x=pos_x, pos_y=pos_y,
+                                        logre=logre, ee1=ee1, ee2=ee2, sersic_n=sersic_n,
+                                        n_bands=n_bands))
+    cat = {k: np.concatenate([r[k] for r in out_rows], axis=0) for k in out_rows[0]}
+    return IslandFitResult(
+        bandnames=list(bandnames), source_idx=cat["src"].astype(np.int64),
+        pos_x=cat["pos_x"], pos_y=cat["pos_y"], logre=cat["logre"], ee1=cat["ee1"],
+        ee2=cat["ee2"], sersic_n=cat["sersic_n"], fluxes=cat["fluxes"],
+        flux_err=cat["flux_err"], chi2=cat["chi2"], chi2_nu=cat["chi2_nu"],
+        n_steps=cat["n_steps"], converged=cat["converged"], stalled=cat["stalled"],
+        diverged=cat["diverged"], stall_dchi2=cat["stall_dchi2"], free_n=cat["free_n"],
+        railed=cat["railed"], island_id=cat["island_id"],
+        island_nsrc=cat["island_nsrc"], island_giant=cat["island_giant"],
+        re_upper_pix=cat["re_upper_pix"], pos_x_err=cat["pos_x_err"],
+        pos_y_err=cat["pos_y_err"], re_err=cat["re_err"], ell_err=cat["ell_err"],
+        re_prof_lo=cat["re_prof_lo"], re_prof_hi=cat["re_prof_hi"],
+        theta_err=cat["theta_err"], sersic_n_err=cat["sersic_n_err"],
+        pos_x_prior_frac=cat["pos_x_prior_frac"], pos_y_prior_frac=cat["pos_y_prior_frac"],
+        re_prior_frac=cat["re_prior_frac"], ell_prior_frac=cat["ell_prior_frac"],
+        theta_prior_frac=cat["theta_prior_frac"],
+        sersic_n_prior_frac=cat["sersic_n_prior_frac"], rchisq=cat["rchisq"],
+        fracflux=cat["fracflux"], fracin=cat["fracin"], fracmasked=cat["fracmasked"],
+        flux_win=cat["flux_win"], flux_marg_var=cat["flux_marg_var"],
+        bucket_stats=bucket_stats)
+
+
+def _native_for_mog(psfs) -> int:
+    """Native stamp for an analytic PSF: the odd side covering +-4 sigma of
+    the widest component anywhere near the field centre (>= 31)."""
+    s = max(float(np.max(np.abs(np.asarray(p.sigma)[:, 0]))) for p in psfs)
+    side = int(2 * np.ceil(4.0 * s) + 1)
+    return max(31, side | 1)
+
+
+def island_fit_singletons(**kwargs):
+    """Fit only the nsrc_class == 1 buckets."""
+    return island_fit(nsrc_max=1, include_giants=False, **kwargs)
