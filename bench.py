@@ -1,0 +1,348 @@
+"""Benchmark: islands/s of the per-island VarPro-LM forced-photometry solve.
+
+Workload (one "step"): every fitted island of the synthetic production field
+(2048x2048, 20 bands, 5000 sources: 60% STAR / 20% EXP / 12% DEV / 8% SERSIC,
+4-component elliptical Gaussian-mixture PSF varying as an order-2 polynomial,
+analytic render mode) solved to convergence (max 30 LM iterations) on one GPU.
+
+* ``value``: islands/s with the field and every chunk's inputs already
+  resident in HBM (``IslandFitJob.solve``), CUDA events on the library stream,
+  synchronize + barrier on both sides, max over ranks.  The field stacks
+  (671 MB) exceed L2, so no explicit flush is needed between steps.
+* ``e2e``: islands/s through the public API ``island_fit(...)`` from host
+  arrays: planning, field + inputs host->device, solve, results
+  device->host, unpack.
+* ``roofline``: the dominant kernel of an instrumented solve (per-launch CUDA
+  events) against the measured peaks in MEASURED_PEAKS.json.
+* ``cpu_baseline``: the CPU restatement of the reference algorithm (the
+  oracle, reference precision) on a seeded 1% sample of the same islands,
+  over all host cores.
+
+``--impl reference`` prints the reference arm: the CPU restatement timed on
+the same workload (bounded samples), since the reference's own JAX solver is
+not installable here.
+
+Multi-GPU (torchrun): weak scaling, every rank solves its own seeded field
+(islands are independent: no collective on the data path); time = max over
+ranks.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = ("islands/s at <=1e-4 rel flux err vs FP64 (plain vs batched+mixed); "
+          "p50/p99 serve latency")
+WORKLOAD = ("production field 2048x2048, 20 bands, 5000 sources "
+            "(60/20/12/8% STAR/EXP/DEV/SERSIC), 4-Gaussian order-2 PSF, "
+            "analytic render, max 30 LM steps")
+
+
+def _peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), float(d["bf16_tflops"]), "measured"
+    return 6650.0, 1590.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle sampling during the timed region."""
+
+    def __init__(self, index: int = 0):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                 "-i", str(self.index), "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+                 "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4)
+                          if len(r) > 5 + i and r[5 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.rows)}
+
+
+def make_field(seed: int, device: str):
+    from uniphot_b200.synth import make_production_field
+    return make_production_field(seed, device=device)
+
+
+def _sample_rows(classes, frac: float, seed: int, min_n: int = 8):
+    """Seeded sample of (class index, row) over all fitted islands."""
+    allr = [(ci, r) for ci, c in enumerate(classes) for r in range(c[0].n_islands)]
+    rng = np.random.default_rng(seed)
+    n = max(min_n, int(round(frac * len(allr))))
+    pick = rng.choice(len(allr), size=min(n, len(allr)), replace=False)
+    return [allr[i] for i in sorted(pick)]
+
+
+def cpu_oracle_time(classes, PAD, field, sample, precision="ref", budget_s=40.0,
+                    processes=None):
+    """Time the oracle on the sampled islands (all host cores, spawn pool)."""
+    from oracle.driver import psf_bands
+    from oracle.island_oracle import (SersicTable, SolverConfig,
+                                      island_inputs_from_host)
+    import multiprocessing as mp
+    from oracle import driver
+    procs = processes or len(os.sched_getaffinity(0))
+    nb, H, W = field.data_minus_bg.shape
+    ds = np.zeros((nb, H + 2 * PAD, W + 2 * PAD), np.float32)
+    ws = np.zeros_like(ds)
+    ds[:, PAD:PAD + H, PAD:PAD + W] = field.data_minus_bg
+    ws[:, PAD:PAD + H, PAD:PAD + W] = field.invvar
+    table = SersicTable.load(ROOT / "uniphot_b200" / "data" / "sersic_mog_table.npz")
+    cfg = SolverConfig(precision=precision)
+    jobs = []
+    for ci, r in sample:
+        plan, host = classes[ci][0], classes[ci][1]
+        psf = psf_bands(field.mog_psfs, plan.tier, "analytic")
+        isl = island_inputs_from_host(host, r, B=plan.bbox_class, T=plan.tier,
+                                      dstack=ds, wstack=ws, psf=psf, table=table,
+                                      mode="analytic")
+        jobs.append((isl, cfg))
+    t0 = time.perf_counter()
+    done = []
+    with mp.get_context("spawn").Pool(procs) as pool:
+        its = [pool.apply_async(driver.solve_one_input, j) for j in jobs]
+        for i, it in enumerate(its):
+            left = budget_s - (time.perf_counter() - t0)
+            try:
+                done.append((sample[i], it.get(timeout=max(left, 0.01))))
+            except mp.TimeoutError:
+                break
+        pool.terminate()
+    dt = time.perf_counter() - t0
+    return done, dt, procs
+
+
+def run_reference_arm(args, rank, world):
+    if rank != 0:
+        print(json.dumps({"impl": "reference", "rank": rank, "skipped": True}),
+              file=sys.stderr)
+        return
+    import torch  # noqa: F401  -- generation uses torch on whatever is present
+    dev = "cuda" if torch.cuda.is_available() else "cpu"
+    field = make_field(args.seed, dev)
+    from uniphot_b200.solver import plan_field
+    # host-side class planning only; the oracle does all the arithmetic
+    fp = plan_field(**field.fit_kwargs("analytic"))
+    n_isl = sum(p.n_islands for p, _ in fp.classes)
+    vals = []
+    ncores = len(os.sched_getaffinity(0))
+    for step in range(args.warmup + args.steps):
+        sample = _sample_rows(fp.classes, 0.01, 1000 + step)
+        done, dt, procs = cpu_oracle_time(fp.classes, fp.PAD, field, sample,
+                                          budget_s=args.ref_budget)
+        if step >= args.warmup:
+            vals.append(len(done) / dt)
+    v = float(np.mean(vals))
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "islands/s",
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "n_islands": n_isl},
+        "cpu_baseline": {"value": v, "unit": "islands/s", "cores": ncores,
+                         "kind": "port",
+                         "sample": f"seeded 1% island sample per step ({len(sample)} "
+                                   f"islands), oracle at reference precision, "
+                                   f"{args.ref_budget:.0f}s cap per step"},
+        "e2e": {"value": v, "unit": "islands/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0}}))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--cpu-budget", type=float, default=40.0)
+    ap.add_argument("--ref-budget", type=float, default=25.0)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--profile-run", action="store_true",
+                    help="one solve of the workload and exit (for ncu)")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference_arm(args, rank, world)
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    from uniphot_b200.solver import IslandFitJob, island_fit
+    field = make_field(args.seed + 7919 * rank, "cuda")
+    kw = field.fit_kwargs("analytic")
+    job = IslandFitJob(**kw, device=local)
+    n_isl = job.n_islands
+    stream = torch.cuda.ExternalStream(job.field.ctx.stream_ptr())
+    if args.profile_run:
+        job.solve()
+        torch.cuda.synchronize()
+        print(json.dumps({"profile_run": True, "n_islands": n_isl,
+                          "launches": job.field.ctx.last_launch_count(),
+                          "solve_ms": job.field.ctx.last_timing()[1]}), flush=True)
+        job.close()
+        return
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        job.solve()
+    barrier()
+    launches = 0
+    with ClockSampler(local) as clk:
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            job.solve()
+            launches += job.field.ctx.last_launch_count()
+        e1.record(stream)
+        barrier()
+    ms = e0.elapsed_time(e1)
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * n_isl * args.steps / (ms / 1e3)
+    # instrumented solve: per-kernel CUDA-event times
+    job.job.set_profile(True)
+    job.solve()
+    ktimes = job.job.kernel_times()
+    job.job.set_profile(False)
+    res = job.result()
+    # e2e through the public API (host arrays in, results out)
+    e2e_t = []
+    for _ in range(args.e2e_steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r2 = island_fit(**kw, device=local)
+        torch.cuda.synchronize()
+        e2e_t.append(time.perf_counter() - t0)
+    e2e_v = world * n_isl / float(np.median(e2e_t))
+    nb, H, W = field.data_minus_bg.shape
+    PAD = job.PAD
+    h2d = 2 * 4 * nb * (H + 2 * PAD) * (W + 2 * PAD)
+    for plan, host, _ in job.classes:
+        h2d += sum(np.asarray(host[k]).nbytes for k in (
+            "ox", "oy", "x0b", "y0b", "st", "sn", "fn_flag", "mmask", "keep", "p0",
+            "lower", "upper", "prior_mean", "prior_inv_sigma"))
+    d2h = sum(p.n_islands * (6 * p.nsrc_class * 4 + 2 * nb * p.nsrc_class * 4 + 40)
+              for p, _, _ in job.classes)
+    # roofline of the dominant kernel
+    hbm, bf16, src = _peaks()
+    dom = max(ktimes, key=lambda k: ktimes[k][0])
+    out = {
+        "metric": METRIC, "value": value, "unit": "islands/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded production field; per-rank seed)",
+        "config": {"workload": WORKLOAD, "n_islands": n_isl,
+                   "l2": "inputs (671 MB field) larger than L2",
+                   "parallelism": f"dp{world} (island partition by field)",
+                   "form": "plain FP32 Gram, device LM loop (CUDA graph)"},
+        "e2e": {"value": e2e_v, "unit": "islands/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h)},
+        "gpu_launches": int(launches),
+        "clocks": clk.summary(),
+        "kernel_ms": {k: {"ms": v[0], "launches": v[1]} for k, v in ktimes.items()},
+        "roofline": {"kernel": dom, "bound": None, "achieved": None, "peak": None,
+                     "unit": None, "frac": None, "traffic": None, "peaks": src},
+        "quality": {"converged_frac": float(np.mean(res.converged)),
+                    "mean_steps": float(np.mean(res.n_steps))},
+    }
+    if not args.no_cpu and rank == 0:
+        sample = _sample_rows(job.classes, 0.01, 1)
+        done, dt, procs = cpu_oracle_time(job.classes, job.PAD, field, sample,
+                                          budget_s=args.cpu_budget)
+        out["cpu_baseline"] = {
+            "value": len(done) / dt, "unit": "islands/s", "cores": procs,
+            "kind": "port",
+            "sample": f"seeded 1% island sample ({len(done)} of {len(sample)} "
+                      f"islands in {dt:.1f}s), oracle at reference precision"}
+        # flux error vs the FP64 oracle on the same sample
+        errs = []
+        ref64, _, _ = cpu_oracle_time(job.classes, job.PAD, field, sample[:len(done)],
+                                      precision="f64", budget_s=args.cpu_budget)
+        for (ci, r), o in ref64:
+            plan, host, ids = job.classes[ci]
+            parts = [job.job.read(i) for i in ids]
+            fl = np.concatenate([p["fluxes"] for p in parts], axis=0)[r]
+            mm = host["mmask"][r]
+            fo = o["fluxes"][:, mm]
+            fg = fl[:, mm]
+            errs.append(np.abs(fg - fo) / np.maximum(np.abs(fo), 1e-30))
+        if errs:
+            e = np.concatenate([x.ravel() for x in errs])
+            out["quality"]["flux_rel_err_vs_fp64"] = {
+                "median": float(np.median(e)), "p99": float(np.quantile(e, 0.99)),
+                "max": float(e.max()), "n": int(e.size)}
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    job.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

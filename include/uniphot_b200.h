@@ -146,13 +146,37 @@ int uph_run_chunk(uph_ctx* ctx, const uph_class_desc* cls,
                   const uph_chunk_in* in, int32_t max_steps,
                   uph_chunk_out* out);
 
-/* Timing split of the last uph_run_chunk on the context (milliseconds of
- * device time between events): [0] host->device inputs, [1] LM loop,
- * [2] post-loop probes and final fluxes, [3] device->host outputs. */
+/* Timing split of the last uph_run_chunk / uph_job_solve on the context
+ * (milliseconds of device time between events): [0] host->device inputs,
+ * [1] LM loop, [2] post-loop probes and final fluxes, [3] device->host
+ * outputs. */
 int uph_last_timing(const uph_ctx* ctx, float* ms4);
 
-/* Number of kernel launches issued by the last uph_run_chunk. */
+/* Number of kernel launches issued by the last uph_run_chunk / job solve. */
 int64_t uph_last_launch_count(const uph_ctx* ctx);
+
+/* ---- Jobs: many chunks (of any classes) resident on the device at once.
+ * This is island_fit's class loop (island_solver.py:3380-3484) with every
+ * chunk's inputs uploaded first and all chunks solved concurrently on a
+ * pool of streams.  uph_job_solve may be called again: it restarts every
+ * chunk from its uploaded inputs. */
+typedef struct uph_job uph_job;
+int uph_job_create(uph_ctx* ctx, uph_job** out);
+int uph_job_destroy(uph_job* job);
+/* Upload one chunk's inputs (host buffers); returns its index in *chunk_id. */
+int uph_job_add_chunk(uph_job* job, const uph_class_desc* cls,
+                      const uph_chunk_in* in, int32_t* chunk_id);
+/* Solve every chunk for up to max_steps LM iterations (device-resident). */
+int uph_job_solve(uph_job* job, int32_t max_steps);
+/* Copy one chunk's results to host buffers. */
+int uph_job_read(uph_job* job, int32_t chunk_id, uph_chunk_out* out);
+/* Per-kernel device time of the last instrumented solve: kind in
+ * 0 render, 1 gram, 2 assemble, 3 step, 4 trial chi2, 5 accept;
+ * returns total milliseconds and launch count.  Instrumentation is on
+ * when uph_job_set_profile(job, 1) was called before the solve. */
+int uph_job_set_profile(uph_job* job, int32_t on);
+int uph_job_kernel_time(const uph_job* job, int32_t kind, float* ms,
+                        int64_t* launches);
 
 #ifdef __cplusplus
 }

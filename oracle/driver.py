@@ -64,3 +64,8 @@ def solve_chunk(host, rows, *, B, T, dstack, wstack, psfs, mode, table_path=None
         out[k] = np.stack([np.asarray(r[k]) for r in res])
     out["steps_run"] = int(max(r["steps"] for r in res))
     return out
+
+
+def solve_one_input(isl, cfg, max_steps: int = 30):
+    """Pool entry: solve one prepared IslandInput."""
+    return solve_island(isl, cfg, max_steps)

@@ -22,7 +22,10 @@ EXPORTED = ("uph_create", "uph_destroy", "uph_last_error", "uph_set_stream",
             "uph_get_stream", "uph_upload_field", "uph_upload_field_device",
             "uph_upload_psf_poly", "uph_upload_psf_mog",
             "uph_upload_sersic_table", "uph_run_chunk", "uph_last_timing",
-            "uph_last_launch_count")
+            "uph_last_launch_count", "uph_job_create", "uph_job_destroy",
+            "uph_job_add_chunk", "uph_job_solve", "uph_job_read",
+            "uph_job_set_profile", "uph_job_kernel_time")
+KERNEL_KINDS = ("render", "gram", "assemble", "step", "trial_chi2", "accept")
 
 _P = C.c_void_p
 
@@ -83,6 +86,15 @@ def lib():
         L.uph_last_timing.argtypes = [_P, C.POINTER(C.c_float)]
         L.uph_last_launch_count.argtypes = [_P]
         L.uph_last_launch_count.restype = C.c_int64
+        L.uph_job_create.argtypes = [_P, C.POINTER(_P)]
+        L.uph_job_destroy.argtypes = [_P]
+        L.uph_job_add_chunk.argtypes = [_P, C.POINTER(ClassDesc), C.POINTER(ChunkIn),
+                                        C.POINTER(C.c_int32)]
+        L.uph_job_solve.argtypes = [_P, C.c_int32]
+        L.uph_job_read.argtypes = [_P, C.c_int32, C.POINTER(ChunkOut)]
+        L.uph_job_set_profile.argtypes = [_P, C.c_int32]
+        L.uph_job_kernel_time.argtypes = [_P, C.c_int32, C.POINTER(C.c_float),
+                                          C.POINTER(C.c_int64)]
         _lib = L
     return _lib
 
@@ -172,54 +184,14 @@ class Context:
 
     def run_chunk(self, desc: ClassDesc, arrays: dict, max_steps: int,
                   nb: int, init_state: dict | None = None) -> dict:
+        """One chunk through uph_run_chunk (upload, solve, read)."""
+        cin, keep_alive = chunk_in(arrays, init_state)
         n, N = arrays["mmask"].shape
-        nP = 6 * N
-
-        def f32(a, shape):
-            return np.ascontiguousarray(np.asarray(a, np.float32).reshape(shape))
-
-        def i32(a, shape):
-            return np.ascontiguousarray(np.asarray(a, np.int32).reshape(shape))
-
-        def u8(a, shape):
-            return np.ascontiguousarray(np.asarray(a).astype(np.uint8).reshape(shape))
-        keep_alive = dict(
-            ox=i32(arrays["ox"], n), oy=i32(arrays["oy"], n),
-            x0b=f32(arrays["x0b"], n), y0b=f32(arrays["y0b"], n),
-            stype=i32(arrays["st"], (n, N)), n_frozen=f32(arrays["sn"], (n, N)),
-            free_n=u8(arrays["fn_flag"], (n, N)), mmask=u8(arrays["mmask"], (n, N)),
-            keep=u8(arrays["keep"], (n, nP)), p0=f32(arrays["p0"], (n, nP)),
-            lower=f32(arrays["lower"], (n, nP)), upper=f32(arrays["upper"], (n, nP)),
-            prior_mean=f32(arrays["prior_mean"], (n, nP)),
-            prior_inv_sigma=f32(arrays["prior_inv_sigma"], (n, nP)))
-        cin = ChunkIn(n_islands=n)
-        for k, v in keep_alive.items():
-            setattr(cin, k, ptr(v))
-        if init_state is not None:
-            keep_alive["p0"] = f32(init_state["p"], (n, nP))
-            cin.p0 = ptr(keep_alive["p0"])
-            for k, conv in (("lam", f32), ("chi2", f32), ("consec", i32),
-                            ("nrej", i32), ("nst", i32)):
-                keep_alive["init_" + k] = conv(init_state[k], n)
-                setattr(cin, "init_" + k, ptr(keep_alive["init_" + k]))
-        out = dict(p=np.zeros((n, N, 6), np.float32),
-                   fluxes=np.zeros((n, nb, N), np.float32),
-                   ferr=np.zeros((n, nb, N), np.float32),
-                   chi2=np.zeros(n, np.float32), conv=np.zeros(n, np.uint8),
-                   stall=np.zeros(n, np.uint8), diverged=np.zeros(n, np.uint8),
-                   stall_dchi2=np.zeros(n, np.float32), nst=np.zeros(n, np.int32),
-                   lam=np.zeros(n, np.float32), consec=np.zeros(n, np.int32),
-                   nrej=np.zeros(n, np.int32), n_good=np.zeros(n, np.int64))
-        cout = ChunkOut()
-        for k, v in out.items():
-            setattr(cout, k, ptr(v))
+        out, cout = chunk_out(n, N, nb)
         rc = lib().uph_run_chunk(self._h, C.byref(desc), C.byref(cin), int(max_steps),
                                  C.byref(cout))
         self.check(rc, "uph_run_chunk")
-        for k in ("conv", "stall", "diverged"):
-            out[k] = out[k].astype(bool)
-        out["steps_run"] = int(cout.steps_run)
-        return out
+        return finish_out(out, cout)
 
     def last_timing(self):
         buf = (C.c_float * 4)()
@@ -228,3 +200,114 @@ class Context:
 
     def last_launch_count(self) -> int:
         return int(lib().uph_last_launch_count(self._h))
+
+
+def chunk_in(arrays: dict, init_state: dict | None = None):
+    """ChunkIn over contiguous copies of class host arrays (kept alive by the
+    returned dict)."""
+    n, N = arrays["mmask"].shape
+    nP = 6 * N
+
+    def f32(a, shape):
+        return np.ascontiguousarray(np.asarray(a, np.float32).reshape(shape))
+
+    def i32(a, shape):
+        return np.ascontiguousarray(np.asarray(a, np.int32).reshape(shape))
+
+    def u8(a, shape):
+        return np.ascontiguousarray(np.asarray(a).astype(np.uint8).reshape(shape))
+    keep = dict(
+        ox=i32(arrays["ox"], n), oy=i32(arrays["oy"], n),
+        x0b=f32(arrays["x0b"], n), y0b=f32(arrays["y0b"], n),
+        stype=i32(arrays["st"], (n, N)), n_frozen=f32(arrays["sn"], (n, N)),
+        free_n=u8(arrays["fn_flag"], (n, N)), mmask=u8(arrays["mmask"], (n, N)),
+        keep=u8(arrays["keep"], (n, nP)), p0=f32(arrays["p0"], (n, nP)),
+        lower=f32(arrays["lower"], (n, nP)), upper=f32(arrays["upper"], (n, nP)),
+        prior_mean=f32(arrays["prior_mean"], (n, nP)),
+        prior_inv_sigma=f32(arrays["prior_inv_sigma"], (n, nP)))
+    if init_state is not None:
+        keep["p0"] = f32(init_state["p"], (n, nP))
+        for k, conv in (("lam", f32), ("chi2", f32), ("consec", i32), ("nrej", i32),
+                        ("nst", i32)):
+            keep["init_" + k] = conv(init_state[k], n)
+    cin = ChunkIn(n_islands=n)
+    for k, v in keep.items():
+        setattr(cin, k, ptr(v))
+    return cin, keep
+
+
+def chunk_out(n: int, N: int, nb: int):
+    out = dict(p=np.zeros((n, N, 6), np.float32),
+               fluxes=np.zeros((n, nb, N), np.float32),
+               ferr=np.zeros((n, nb, N), np.float32),
+               chi2=np.zeros(n, np.float32), conv=np.zeros(n, np.uint8),
+               stall=np.zeros(n, np.uint8), diverged=np.zeros(n, np.uint8),
+               stall_dchi2=np.zeros(n, np.float32), nst=np.zeros(n, np.int32),
+               lam=np.zeros(n, np.float32), consec=np.zeros(n, np.int32),
+               nrej=np.zeros(n, np.int32), n_good=np.zeros(n, np.int64))
+    cout = ChunkOut()
+    for k, v in out.items():
+        setattr(cout, k, ptr(v))
+    return out, cout
+
+
+def finish_out(out: dict, cout: ChunkOut) -> dict:
+    for k in ("conv", "stall", "diverged"):
+        out[k] = out[k].astype(bool)
+    out["steps_run"] = int(cout.steps_run)
+    return out
+
+
+class Job:
+    """Many chunks resident on the device, solved concurrently."""
+
+    def __init__(self, ctx: Context):
+        self.ctx = ctx
+        h = _P()
+        ctx.check(lib().uph_job_create(ctx.handle, C.byref(h)), "uph_job_create")
+        self._h = h
+        self.shapes = []
+
+    def add_chunk(self, desc: ClassDesc, arrays: dict, nb: int,
+                  init_state: dict | None = None) -> int:
+        cin, _keep = chunk_in(arrays, init_state)
+        cid = C.c_int32(-1)
+        self.ctx.check(lib().uph_job_add_chunk(self._h, C.byref(desc), C.byref(cin),
+                                               C.byref(cid)), "uph_job_add_chunk")
+        n, N = arrays["mmask"].shape
+        self.shapes.append((n, N, nb))
+        return int(cid.value)
+
+    def solve(self, max_steps: int):
+        self.ctx.check(lib().uph_job_solve(self._h, int(max_steps)), "uph_job_solve")
+
+    def read(self, cid: int) -> dict:
+        n, N, nb = self.shapes[cid]
+        out, cout = chunk_out(n, N, nb)
+        self.ctx.check(lib().uph_job_read(self._h, int(cid), C.byref(cout)),
+                       "uph_job_read")
+        return finish_out(out, cout)
+
+    def set_profile(self, on: bool):
+        self.ctx.check(lib().uph_job_set_profile(self._h, int(bool(on))),
+                       "uph_job_set_profile")
+
+    def kernel_times(self) -> dict:
+        res = {}
+        for i, name in enumerate(KERNEL_KINDS):
+            ms = C.c_float(0)
+            cnt = C.c_int64(0)
+            lib().uph_job_kernel_time(self._h, i, C.byref(ms), C.byref(cnt))
+            res[name] = (float(ms.value), int(cnt.value))
+        return res
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().uph_job_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # noqa: BLE001
+            pass

@@ -21,6 +21,7 @@
 int uph_render_setup();
 int uph_solve_setup();
 void launch_set_probe(const ClassDev& c, cudaStream_t s);
+void launch_fill_float(float* p, float v, int n, cudaStream_t s);
 
 #define UPH_CHECK_EVERY 4
 
@@ -59,8 +60,6 @@ struct uph_ctx {
   DevBuf tb_knots, tb_amps, tb_lv, tb_core;
   int tb_n = 0, tb_k = 0;
   double tb_nmin = 0, tb_nmax = 0;
-  // chunk buffers
-  std::map<std::string, DevBuf> bufs;
   int* h_active = nullptr;  // pinned
   cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
   float timing[4] = {0, 0, 0, 0};
@@ -102,14 +101,6 @@ int ensure(uph_ctx* ctx, DevBuf& b, size_t bytes, const char* what) {
   if (e != cudaSuccess) return cuda_err(ctx, e, what);
   b.cap = bytes;
   return UPH_OK;
-}
-
-template <class T>
-T* buf(uph_ctx* ctx, const char* name, size_t count, int* rc) {
-  if (*rc != UPH_OK) return nullptr;
-  DevBuf& b = ctx->bufs[name];
-  *rc = ensure(ctx, b, count * sizeof(T), name);
-  return (T*)b.ptr;
 }
 
 int upload(uph_ctx* ctx, void* dst, const void* src, size_t bytes,
@@ -177,7 +168,6 @@ int uph_destroy(uph_ctx* ctx) {
   ctx->tb_amps.release();
   ctx->tb_lv.release();
   ctx->tb_core.release();
-  for (auto& kv : ctx->bufs) kv.second.release();
   for (auto& ev : ctx->ev)
     if (ev) cudaEventDestroy(ev);
   if (ctx->h_active) cudaFreeHost(ctx->h_active);
@@ -314,21 +304,113 @@ int uph_last_timing(const uph_ctx* ctx, float* ms4) {
 
 int64_t uph_last_launch_count(const uph_ctx* ctx) { return ctx ? ctx->launches : -1; }
 
-int uph_run_chunk(uph_ctx* ctx, const uph_class_desc* cls,
-                  const uph_chunk_in* in, int32_t max_steps,
-                  uph_chunk_out* out) {
-  if (!ctx) return UPH_ERR_INVALID;
-  if (!cls || !in || !out) return set_err(ctx, UPH_ERR_INVALID, "null argument");
-  cudaSetDevice(ctx->device);
-  ctx->launches = 0;
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Chunks and jobs
+// ---------------------------------------------------------------------------
+
+struct Chunk {
+  ClassDev c{};
+  std::map<std::string, DevBuf> bufs;
+  int n = 0, N = 0, nb = 0, nP = 0;
+  bool fresh = true;
+  std::vector<int> h_nst0;
+  std::vector<uint8_t> h_flags0;
+  float* d_lam0 = nullptr;
+  float* d_chi20 = nullptr;
+  int* d_consec0 = nullptr;
+  int* d_nrej0 = nullptr;
+  int* d_nst0 = nullptr;
+  uint8_t* d_flags0 = nullptr;
+  float* d_p0 = nullptr;
+  uint8_t* d_div = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t gexec = nullptr;
+  cudaEvent_t ev_group = nullptr;
+  bool done = false;
+  int iters = 0;
+  int slot = 0;
+  ~Chunk() {
+    if (gexec) cudaGraphExecDestroy(gexec);
+    if (graph) cudaGraphDestroy(graph);
+    if (ev_group) cudaEventDestroy(ev_group);
+    for (auto& kv : bufs) kv.second.release();
+  }
+};
+
+struct uph_job {
+  uph_ctx* ctx = nullptr;
+  std::vector<Chunk*> chunks;
+  std::vector<cudaStream_t> streams;
+  int* h_active = nullptr;  // pinned, one slot per chunk
+  int h_active_cap = 0;
+  bool profile = false;
+  float ktime[6] = {0, 0, 0, 0, 0, 0};
+  int64_t kcount[6] = {0, 0, 0, 0, 0, 0};
+  ~uph_job() {
+    for (auto* c : chunks) delete c;
+    for (auto s : streams) cudaStreamDestroy(s);
+    if (h_active) cudaFreeHost(h_active);
+  }
+};
+
+namespace {
+
+template <class T>
+T* cbuf(uph_ctx* ctx, Chunk* ch, const char* name, size_t count, int* rc) {
+  if (*rc != UPH_OK) return nullptr;
+  DevBuf& b = ch->bufs[name];
+  *rc = ensure(ctx, b, count * sizeof(T), name);
+  return (T*)b.ptr;
+}
+
+// Kernel launcher that optionally brackets each launch with events.
+struct Launcher {
+  uph_job* job;
+  cudaStream_t s;
+  std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>>* rec;
+  template <class F>
+  void operator()(int kind, F&& fn) {
+    if (rec) {
+      cudaEvent_t a, b;
+      cudaEventCreate(&a);
+      cudaEventCreate(&b);
+      cudaEventRecord(a, s);
+      fn();
+      cudaEventRecord(b, s);
+      rec->push_back({kind, {a, b}});
+    } else {
+      fn();
+    }
+    job->ctx->launches += 1;
+  }
+};
+
+void iteration(const ClassDev& c, Launcher& L) {
+  cudaStream_t s = L.s;
+  L(0, [&] { launch_render(c, c.p, PH_LIN, s); });
+  L(1, [&] { launch_gram_lin(c, s); });
+  L(2, [&] { launch_assemble(c, s); });
+  L(3, [&] { launch_step(c, PH_TRIAL, 0, 0.f, 0, s); });
+  L(0, [&] { launch_render(c, c.p_try, PH_TRIAL, s); });
+  L(4, [&] { launch_gram_trial(c, c.p_try, PH_TRIAL, 0, s); });
+  L(5, [&] { launch_accept(c, PH_TRIAL, s); });
+}
+
+int add_chunk(uph_ctx* ctx, Chunk* ch, const uph_class_desc* cls,
+              const uph_chunk_in* in) {
   const int n = in->n_islands, N = cls->nsrc, B = cls->bbox, T = cls->tier;
   if (n <= 0) return set_err(ctx, UPH_ERR_INVALID, "empty chunk");
   if (N <= 0 || N > UPH_MAXN)
     return set_err(ctx, UPH_ERR_INVALID, "nsrc class %d outside 1..%d", N, UPH_MAXN);
   if (B <= 0 || T <= 0 || (T % 2) == 0)
     return set_err(ctx, UPH_ERR_INVALID, "invalid bbox %d / tier %d", B, T);
-  if (max_steps < 0) return set_err(ctx, UPH_ERR_INVALID, "max_steps < 0");
   if (!ctx->dstack.ptr) return set_err(ctx, UPH_ERR_STATE, "no field uploaded");
+  if (!in->ox || !in->oy || !in->x0b || !in->y0b || !in->stype || !in->n_frozen ||
+      !in->free_n || !in->mmask || !in->keep || !in->p0 || !in->lower ||
+      !in->upper || !in->prior_mean || !in->prior_inv_sigma)
+    return set_err(ctx, UPH_ERR_INVALID, "null input array");
   const int nb = ctx->nb;
   const int mode = cls->render_mode;
   const PolyPsf* pp = nullptr;
@@ -345,7 +427,6 @@ int uph_run_chunk(uph_ctx* ctx, const uph_class_desc* cls,
     return set_err(ctx, UPH_ERR_INVALID, "unknown render mode %d", mode);
   }
   const int nP = 6 * N;
-  // ---- host-side row tables ----
   std::vector<int> nL(n), nr(n);
   int Kmax = 1, nLmax = 1, R = 1;
   bool any_gal = false;
@@ -362,7 +443,9 @@ int uph_run_chunk(uph_ctx* ctx, const uph_class_desc* cls,
     nr[i] = cnt;
     int live = 0;
     for (int k = 0; k < cnt; ++k) {
-      const bool gal = in->stype[(size_t)i * N + k] != 0;
+      const int st = in->stype[(size_t)i * N + k];
+      if (st < 0 || st > 3) return set_err(ctx, UPH_ERR_INVALID, "bad source type %d", st);
+      const bool gal = st != 0;
       any_gal = any_gal || gal;
       int lk = 0;
       for (int j = 0; j < 6; ++j)
@@ -373,6 +456,9 @@ int uph_run_chunk(uph_ctx* ctx, const uph_class_desc* cls,
     nL[i] = live;
     nLmax = std::max(nLmax, live);
     Kmax = std::max(Kmax, live + cnt + 1);
+    const int ox = in->ox[i], oy = in->oy[i];
+    if (ox < 0 || oy < 0 || ox + B > ctx->Wp || oy + B > ctx->Hp)
+      return set_err(ctx, UPH_ERR_INVALID, "island %d window outside the padded field", i);
   }
   if (nLmax > UPH_MAXLIVE) return set_err(ctx, UPH_ERR_INVALID, "too many live parameters");
   if (any_gal && mode == UPH_RENDER_REFERENCE)
@@ -405,18 +491,11 @@ int uph_run_chunk(uph_ctx* ctx, const uph_class_desc* cls,
     row_k[(size_t)i * Kmax + r] = 0;
     row_s[(size_t)i * Kmax + r] = -1;
   }
-  for (int i = 0; i < n; ++i) {
-    int ox = in->ox[i], oy = in->oy[i];
-    if (ox < 0 || oy < 0 || ox + B > ctx->Wp || oy + B > ctx->Hp)
-      return set_err(ctx, UPH_ERR_INVALID, "island %d window outside the padded field", i);
-  }
   const int Sz = std::min(T, B);
-  const int nts = (Sz + UPH_TILE - 1) / UPH_TILE;
-  // ---- device buffers ----
-  int rc = UPH_OK;
-  ClassDev c{};
+  ch->n = n; ch->N = N; ch->nb = nb; ch->nP = nP;
+  ClassDev& c = ch->c;
   c.n_isl = n; c.nb = nb; c.N = N; c.nP = nP; c.B = B; c.T = T; c.Sz = Sz; c.R = R;
-  c.Kmax = Kmax; c.nLmax = nLmax; c.ntile_side = nts;
+  c.Kmax = Kmax; c.nLmax = nLmax; c.ntile_side = (Sz + UPH_TILE - 1) / UPH_TILE;
   c.mode = mode;
   c.Hp = ctx->Hp; c.Wp = ctx->Wp;
   c.dstack = (const float*)ctx->dstack.ptr;
@@ -438,47 +517,55 @@ int uph_run_chunk(uph_ctx* ctx, const uph_class_desc* cls,
   c.tb_lv = (const double*)ctx->tb_lv.ptr;
   c.tb_core = (const double*)ctx->tb_core.ptr;
   c.tb_n = ctx->tb_n; c.tb_k = ctx->tb_k; c.tb_nmin = ctx->tb_nmin; c.tb_nmax = ctx->tb_nmax;
-  int* d_ox = buf<int>(ctx, "ox", n, &rc);
-  int* d_oy = buf<int>(ctx, "oy", n, &rc);
-  float* d_x0b = buf<float>(ctx, "x0b", n, &rc);
-  float* d_y0b = buf<float>(ctx, "y0b", n, &rc);
-  int* d_st = buf<int>(ctx, "stype", (size_t)n * N, &rc);
-  float* d_nf = buf<float>(ctx, "nfrozen", (size_t)n * N, &rc);
-  uint8_t* d_fn = buf<uint8_t>(ctx, "freen", (size_t)n * N, &rc);
-  uint8_t* d_mm = buf<uint8_t>(ctx, "mmask", (size_t)n * N, &rc);
-  uint8_t* d_keep = buf<uint8_t>(ctx, "keep", (size_t)n * nP, &rc);
-  float* d_lo = buf<float>(ctx, "lower", (size_t)n * nP, &rc);
-  float* d_hi = buf<float>(ctx, "upper", (size_t)n * nP, &rc);
-  float* d_pm = buf<float>(ctx, "pmean", (size_t)n * nP, &rc);
-  float* d_pi = buf<float>(ctx, "pinv", (size_t)n * nP, &rc);
-  int* d_nL = buf<int>(ctx, "nL", n, &rc);
-  int* d_nr = buf<int>(ctx, "nr", n, &rc);
-  int16_t* d_rk = buf<int16_t>(ctx, "rowk", (size_t)n * Kmax, &rc);
-  int16_t* d_rs = buf<int16_t>(ctx, "rows", (size_t)n * Kmax, &rc);
-  int16_t* d_rp = buf<int16_t>(ctx, "rowp", (size_t)n * Kmax, &rc);
-  c.p = buf<float>(ctx, "p", (size_t)n * nP, &rc);
-  c.p_try = buf<float>(ctx, "ptry", (size_t)n * nP, &rc);
-  c.lam = buf<float>(ctx, "lam", n, &rc);
-  c.chi2 = buf<float>(ctx, "chi2", n, &rc);
-  c.consec = buf<int>(ctx, "consec", n, &rc);
-  c.nrej = buf<int>(ctx, "nrej", n, &rc);
-  c.nst = buf<int>(ctx, "nst", n, &rc);
-  c.flags = buf<uint8_t>(ctx, "flags", n, &rc);
-  c.stamps = buf<float>(ctx, "stamps", (size_t)n * nb * N * R * Sz * Sz, &rc);
-  c.gram = buf<float>(ctx, "gram", (size_t)n * nb * Kmax * Kmax, &rc);
-  c.Hb = buf<float>(ctx, "Hb", (size_t)n * nb * nLmax * nLmax, &rc);
-  c.gb = buf<float>(ctx, "gb", (size_t)n * nb * nLmax, &rc);
-  c.H = buf<float>(ctx, "H", (size_t)n * nLmax * nLmax, &rc);
-  c.g = buf<float>(ctx, "g", (size_t)n * nLmax, &rc);
-  c.lu = buf<double>(ctx, "lu", nLmax > 72 ? (size_t)n * nLmax * (nLmax + 1) : 1, &rc);
-  c.chi2b = buf<double>(ctx, "chi2b", (size_t)n * nb, &rc);
-  c.flux = buf<float>(ctx, "flux", (size_t)n * nb * N, &rc);
-  c.ferr = buf<float>(ctx, "ferr", (size_t)n * nb * N, &rc);
-  c.ngood = buf<int>(ctx, "ngood", (size_t)n * nb, &rc);
-  c.probe_best = buf<float>(ctx, "pbest", n, &rc);
-  c.probe_p = buf<float>(ctx, "probep", (size_t)n * 4 * nP, &rc);
-  c.n_active = buf<int>(ctx, "nact", 1, &rc);
-  uint8_t* d_div = buf<uint8_t>(ctx, "div", n, &rc);
+  int rc = UPH_OK;
+  int* d_ox = cbuf<int>(ctx, ch, "ox", n, &rc);
+  int* d_oy = cbuf<int>(ctx, ch, "oy", n, &rc);
+  float* d_x0b = cbuf<float>(ctx, ch, "x0b", n, &rc);
+  float* d_y0b = cbuf<float>(ctx, ch, "y0b", n, &rc);
+  int* d_st = cbuf<int>(ctx, ch, "stype", (size_t)n * N, &rc);
+  float* d_nf = cbuf<float>(ctx, ch, "nfrozen", (size_t)n * N, &rc);
+  uint8_t* d_fn = cbuf<uint8_t>(ctx, ch, "freen", (size_t)n * N, &rc);
+  uint8_t* d_mm = cbuf<uint8_t>(ctx, ch, "mmask", (size_t)n * N, &rc);
+  uint8_t* d_keep = cbuf<uint8_t>(ctx, ch, "keep", (size_t)n * nP, &rc);
+  float* d_lo = cbuf<float>(ctx, ch, "lower", (size_t)n * nP, &rc);
+  float* d_hi = cbuf<float>(ctx, ch, "upper", (size_t)n * nP, &rc);
+  float* d_pm = cbuf<float>(ctx, ch, "pmean", (size_t)n * nP, &rc);
+  float* d_pi = cbuf<float>(ctx, ch, "pinv", (size_t)n * nP, &rc);
+  int* d_nL = cbuf<int>(ctx, ch, "nL", n, &rc);
+  int* d_nr = cbuf<int>(ctx, ch, "nr", n, &rc);
+  int16_t* d_rk = cbuf<int16_t>(ctx, ch, "rowk", (size_t)n * Kmax, &rc);
+  int16_t* d_rs = cbuf<int16_t>(ctx, ch, "rows", (size_t)n * Kmax, &rc);
+  int16_t* d_rp = cbuf<int16_t>(ctx, ch, "rowp", (size_t)n * Kmax, &rc);
+  ch->d_p0 = cbuf<float>(ctx, ch, "p0", (size_t)n * nP, &rc);
+  ch->d_lam0 = cbuf<float>(ctx, ch, "lam0", n, &rc);
+  ch->d_chi20 = cbuf<float>(ctx, ch, "chi20", n, &rc);
+  ch->d_consec0 = cbuf<int>(ctx, ch, "consec0", n, &rc);
+  ch->d_nrej0 = cbuf<int>(ctx, ch, "nrej0", n, &rc);
+  ch->d_nst0 = cbuf<int>(ctx, ch, "nst0", n, &rc);
+  ch->d_flags0 = cbuf<uint8_t>(ctx, ch, "flags0", n, &rc);
+  c.p = cbuf<float>(ctx, ch, "p", (size_t)n * nP, &rc);
+  c.p_try = cbuf<float>(ctx, ch, "ptry", (size_t)n * nP, &rc);
+  c.lam = cbuf<float>(ctx, ch, "lam", n, &rc);
+  c.chi2 = cbuf<float>(ctx, ch, "chi2", n, &rc);
+  c.consec = cbuf<int>(ctx, ch, "consec", n, &rc);
+  c.nrej = cbuf<int>(ctx, ch, "nrej", n, &rc);
+  c.nst = cbuf<int>(ctx, ch, "nst", n, &rc);
+  c.flags = cbuf<uint8_t>(ctx, ch, "flags", n, &rc);
+  c.stamps = cbuf<float>(ctx, ch, "stamps", (size_t)n * nb * N * R * Sz * Sz, &rc);
+  c.gram = cbuf<float>(ctx, ch, "gram", (size_t)n * nb * Kmax * Kmax, &rc);
+  c.Hb = cbuf<float>(ctx, ch, "Hb", (size_t)n * nb * nLmax * nLmax, &rc);
+  c.gb = cbuf<float>(ctx, ch, "gb", (size_t)n * nb * nLmax, &rc);
+  c.H = cbuf<float>(ctx, ch, "H", (size_t)n * nLmax * nLmax, &rc);
+  c.g = cbuf<float>(ctx, ch, "g", (size_t)n * nLmax, &rc);
+  c.lu = cbuf<double>(ctx, ch, "lu", nLmax > 72 ? (size_t)n * nLmax * (nLmax + 1) : 1, &rc);
+  c.chi2b = cbuf<double>(ctx, ch, "chi2b", (size_t)n * nb, &rc);
+  c.flux = cbuf<float>(ctx, ch, "flux", (size_t)n * nb * N, &rc);
+  c.ferr = cbuf<float>(ctx, ch, "ferr", (size_t)n * nb * N, &rc);
+  c.ngood = cbuf<int>(ctx, ch, "ngood", (size_t)n * nb, &rc);
+  c.probe_best = cbuf<float>(ctx, ch, "pbest", n, &rc);
+  c.probe_p = cbuf<float>(ctx, ch, "probep", (size_t)n * 4 * nP, &rc);
+  c.n_active = cbuf<int>(ctx, ch, "nact", 1, &rc);
+  ch->d_div = cbuf<uint8_t>(ctx, ch, "div", n, &rc);
   if (rc) return rc;
   c.ox = d_ox; c.oy = d_oy; c.x0b = d_x0b; c.y0b = d_y0b; c.stype = d_st;
   c.n_frozen = d_nf; c.free_n = d_fn; c.mmask = d_mm; c.keep = d_keep;
@@ -487,15 +574,12 @@ int uph_run_chunk(uph_ctx* ctx, const uph_class_desc* cls,
   c.isl_nL = d_nL; c.isl_nr = d_nr; c.row_k = d_rk; c.row_s = d_rs; c.row_p = d_rp;
   c.reg = cls->reg; c.pos_step_max = cls->pos_step_max; c.ftol_rel = cls->chi2_ftol_rel;
   c.step_tol = cls->step_tol_pix; c.un_freeze = cls->un_freeze_steps;
-
-  cudaStream_t s = ctx->stream;
-  CK(cudaEventRecord(ctx->ev[0], s), "event");
-  // ---- inputs ----
   std::vector<float> h_lam(n, 1e-3f), h_chi2(n, 0.f);
-  std::vector<int> h_consec(n, 0), h_nrej(n, 0), h_nst(n, 0);
-  std::vector<uint8_t> h_flags(n, FL_NEEDLIN | FL_REAL);
-  const bool fresh = (in->init_lam == nullptr);
-  if (!fresh) {
+  std::vector<int> h_consec(n, 0), h_nrej(n, 0);
+  ch->h_nst0.assign(n, 0);
+  ch->h_flags0.assign(n, FL_NEEDLIN | FL_REAL);
+  ch->fresh = (in->init_lam == nullptr);
+  if (!ch->fresh) {
     if (!in->init_chi2 || !in->init_consec || !in->init_nrej || !in->init_nst)
       return set_err(ctx, UPH_ERR_INVALID, "partial init state");
     for (int i = 0; i < n; ++i) {
@@ -503,7 +587,7 @@ int uph_run_chunk(uph_ctx* ctx, const uph_class_desc* cls,
       h_chi2[i] = in->init_chi2[i];
       h_consec[i] = in->init_consec[i];
       h_nrej[i] = in->init_nrej[i];
-      h_nst[i] = in->init_nst[i];
+      ch->h_nst0[i] = in->init_nst[i];
     }
   }
   if ((rc = upload(ctx, d_ox, in->ox, sizeof(int) * n, "ox"))) return rc;
@@ -519,114 +603,206 @@ int uph_run_chunk(uph_ctx* ctx, const uph_class_desc* cls,
   if ((rc = upload(ctx, d_hi, in->upper, sizeof(float) * n * nP, "upper"))) return rc;
   if ((rc = upload(ctx, d_pm, in->prior_mean, sizeof(float) * n * nP, "prior_mean"))) return rc;
   if ((rc = upload(ctx, d_pi, in->prior_inv_sigma, sizeof(float) * n * nP, "prior_inv"))) return rc;
-  if ((rc = upload(ctx, c.p, in->p0, sizeof(float) * n * nP, "p0"))) return rc;
+  if ((rc = upload(ctx, ch->d_p0, in->p0, sizeof(float) * n * nP, "p0"))) return rc;
   if ((rc = upload(ctx, d_nL, nL.data(), sizeof(int) * n, "nL"))) return rc;
   if ((rc = upload(ctx, d_nr, nr.data(), sizeof(int) * n, "nr"))) return rc;
   if ((rc = upload(ctx, d_rk, row_k.data(), sizeof(int16_t) * n * Kmax, "rows"))) return rc;
   if ((rc = upload(ctx, d_rs, row_s.data(), sizeof(int16_t) * n * Kmax, "rows"))) return rc;
   if ((rc = upload(ctx, d_rp, row_p.data(), sizeof(int16_t) * n * Kmax, "rows"))) return rc;
-  if ((rc = upload(ctx, c.lam, h_lam.data(), sizeof(float) * n, "lam"))) return rc;
-  if ((rc = upload(ctx, c.chi2, h_chi2.data(), sizeof(float) * n, "chi2"))) return rc;
-  if ((rc = upload(ctx, c.consec, h_consec.data(), sizeof(int) * n, "consec"))) return rc;
-  if ((rc = upload(ctx, c.nrej, h_nrej.data(), sizeof(int) * n, "nrej"))) return rc;
-  if ((rc = upload(ctx, c.nst, h_nst.data(), sizeof(int) * n, "nst"))) return rc;
-  if ((rc = upload(ctx, c.flags, h_flags.data(), n, "flags"))) return rc;
-  CK(cudaMemsetAsync(c.stamps, 0, sizeof(float) * (size_t)n * nb * N * R * Sz * Sz, s), "memset");
-  CK(cudaEventRecord(ctx->ev[1], s), "event");
-  // ---- initial chi2 at the seeds ----
-  if (fresh) {
-    launch_render(c, c.p, PH_ALL, s);
-    launch_gram_trial(c, c.p, PH_ALL, 0, s);
-    launch_accept(c, PH_ALL, s);
-    ctx->launches += 3;
-    CK(cudaGetLastError(), "initial chi2");
-  }
-  // ---- LM loop: one iteration captured as a graph ----
-  cudaGraph_t graph = nullptr;
-  cudaGraphExec_t gexec = nullptr;
-  if (max_steps > 0) {
-    CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "capture");
-    launch_render(c, c.p, PH_LIN, s);
-    launch_gram_lin(c, s);
-    launch_assemble(c, s);
-    launch_step(c, PH_TRIAL, 0, 0.f, 0, s);
-    launch_render(c, c.p_try, PH_TRIAL, s);
-    launch_gram_trial(c, c.p_try, PH_TRIAL, 0, s);
-    launch_accept(c, PH_TRIAL, s);
-    cudaError_t ce = cudaStreamEndCapture(s, &graph);
-    if (ce != cudaSuccess) return cuda_err(ctx, ce, "end capture");
-    ce = cudaGraphInstantiate(&gexec, graph, 0);
-    if (ce != cudaSuccess) {
-      cudaGraphDestroy(graph);
-      return cuda_err(ctx, ce, "graph instantiate");
-    }
-  }
-  int it = 0;
-  while (it < max_steps) {
-    const int group = std::min(UPH_CHECK_EVERY, max_steps - it);
-    for (int j = 0; j < group; ++j) {
-      cudaError_t ce = cudaGraphLaunch(gexec, s);
-      if (ce != cudaSuccess) {
-        cudaGraphExecDestroy(gexec);
-        cudaGraphDestroy(graph);
-        return cuda_err(ctx, ce, "graph launch");
-      }
-      ctx->launches += 7;
-    }
-    it += group;
-    if (it >= max_steps) break;
-    launch_count_active(c, s);
-    ctx->launches += 1;
-    CK(cudaMemcpyAsync(ctx->h_active, c.n_active, sizeof(int), cudaMemcpyDeviceToHost, s), "count");
-    CK(cudaStreamSynchronize(s), "lm loop");
-    if (*ctx->h_active == 0) break;
-  }
-  if (gexec) cudaGraphExecDestroy(gexec);
-  if (graph) cudaGraphDestroy(graph);
-  CK(cudaEventRecord(ctx->ev[2], s), "event");
-  // ---- post-hoc probes on stalled islands ----
+  if ((rc = upload(ctx, ch->d_lam0, h_lam.data(), sizeof(float) * n, "lam"))) return rc;
+  if ((rc = upload(ctx, ch->d_chi20, h_chi2.data(), sizeof(float) * n, "chi2"))) return rc;
+  if ((rc = upload(ctx, ch->d_consec0, h_consec.data(), sizeof(int) * n, "consec"))) return rc;
+  if ((rc = upload(ctx, ch->d_nrej0, h_nrej.data(), sizeof(int) * n, "nrej"))) return rc;
+  if ((rc = upload(ctx, ch->d_nst0, ch->h_nst0.data(), sizeof(int) * n, "nst"))) return rc;
+  if ((rc = upload(ctx, ch->d_flags0, ch->h_flags0.data(), n, "flags"))) return rc;
+  CK(cudaMemsetAsync(c.stamps, 0, sizeof(float) * (size_t)n * nb * N * R * Sz * Sz,
+                     ctx->stream), "memset");
+  CK(cudaEventCreateWithFlags(&ch->ev_group, cudaEventDisableTiming), "event");
+  return UPH_OK;
+}
+
+// Reset a chunk's LM state from its uploaded inputs (stream s).
+int reset_chunk(uph_ctx* ctx, Chunk* ch, cudaStream_t s) {
+  const ClassDev& c = ch->c;
+  const int n = ch->n;
+  CK(cudaMemcpyAsync(c.p, ch->d_p0, sizeof(float) * n * ch->nP, cudaMemcpyDeviceToDevice, s), "reset");
+  CK(cudaMemcpyAsync(c.lam, ch->d_lam0, sizeof(float) * n, cudaMemcpyDeviceToDevice, s), "reset");
+  CK(cudaMemcpyAsync(c.chi2, ch->d_chi20, sizeof(float) * n, cudaMemcpyDeviceToDevice, s), "reset");
+  CK(cudaMemcpyAsync(c.consec, ch->d_consec0, sizeof(int) * n, cudaMemcpyDeviceToDevice, s), "reset");
+  CK(cudaMemcpyAsync(c.nrej, ch->d_nrej0, sizeof(int) * n, cudaMemcpyDeviceToDevice, s), "reset");
+  CK(cudaMemcpyAsync(c.nst, ch->d_nst0, sizeof(int) * n, cudaMemcpyDeviceToDevice, s), "reset");
+  CK(cudaMemcpyAsync(c.flags, ch->d_flags0, n, cudaMemcpyDeviceToDevice, s), "reset");
+  ch->done = false;
+  ch->iters = 0;
+  return UPH_OK;
+}
+
+void post_loop(Chunk* ch, Launcher& L) {
+  const ClassDev& c = ch->c;
+  cudaStream_t s = L.s;
   launch_set_probe(c, s);
-  for (int j = 0; j < 4; ++j) launch_step(c, PH_PROBE, j, 0.f, 1, s);
-  launch_diverged_compare(c, d_div, s);
-  {
-    std::vector<float> inf(n, INFINITY);
-    if ((rc = upload(ctx, c.probe_best, inf.data(), sizeof(float) * n, "probe"))) return rc;
-    for (int e = -9; e <= 6; ++e) {
-      const float lamj = (float)std::pow(10.0, (double)e);
-      launch_step(c, PH_PROBE, 0, lamj, 2, s);
-      launch_render(c, c.p_try, PH_PROBE, s);
-      launch_gram_trial(c, c.p_try, PH_PROBE, 0, s);
-      launch_accept(c, PH_PROBE, s);
-    }
-    ctx->launches += 6 + 16 * 4;
+  for (int j = 0; j < 4; ++j) L(3, [&] { launch_step(c, PH_PROBE, j, 0.f, 1, s); });
+  launch_diverged_compare(c, ch->d_div, s);
+  launch_fill_float(c.probe_best, INFINITY, c.n_isl, s);
+  L.job->ctx->launches += 3;
+  for (int e = -9; e <= 6; ++e) {
+    const float lamj = (float)std::pow(10.0, (double)e);
+    L(3, [&] { launch_step(c, PH_PROBE, 0, lamj, 2, s); });
+    L(0, [&] { launch_render(c, c.p_try, PH_PROBE, s); });
+    L(4, [&] { launch_gram_trial(c, c.p_try, PH_PROBE, 0, s); });
+    L(5, [&] { launch_accept(c, PH_PROBE, s); });
   }
-  // ---- final fluxes at the converged parameters ----
-  launch_render(c, c.p, PH_ALL, s);
-  launch_gram_trial(c, c.p, PH_ALL, 1, s);
-  ctx->launches += 2;
+  L(0, [&] { launch_render(c, c.p, PH_ALL, s); });
+  L(4, [&] { launch_gram_trial(c, c.p, PH_ALL, 1, s); });
+}
+
+int job_solve(uph_job* job, int max_steps) {
+  uph_ctx* ctx = job->ctx;
+  cudaSetDevice(ctx->device);
+  if (max_steps < 0) return set_err(ctx, UPH_ERR_INVALID, "max_steps < 0");
+  const int nch = (int)job->chunks.size();
+  if (nch == 0) return UPH_OK;
+  ctx->launches = 0;
+  // instrumented solves run on one stream so that per-launch event times
+  // are not inflated by other streams' kernels
+  const int nstreams = job->profile ? 1 : std::min(nch, 16);
+  while ((int)job->streams.size() < nstreams) {
+    cudaStream_t st;
+    CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "stream");
+    job->streams.push_back(st);
+  }
+  if (job->h_active_cap < nch) {
+    if (job->h_active) cudaFreeHost(job->h_active);
+    CK(cudaMallocHost((void**)&job->h_active, sizeof(int) * nch), "pinned");
+    job->h_active_cap = nch;
+  }
+  std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> rec;
+  auto* recp = job->profile ? &rec : nullptr;
+  CK(cudaEventRecord(ctx->ev[0], ctx->stream), "event");
+  for (auto st : job->streams) CK(cudaStreamWaitEvent(st, ctx->ev[0], 0), "wait");
+  for (int i = 0; i < nch; ++i) {
+    Chunk* ch = job->chunks[i];
+    ch->slot = i % nstreams;
+    cudaStream_t s = job->streams[ch->slot];
+    int rc = reset_chunk(ctx, ch, s);
+    if (rc) return rc;
+    Launcher L{job, s, recp};
+    if (ch->fresh) {
+      L(0, [&] { launch_render(ch->c, ch->c.p, PH_ALL, s); });
+      L(4, [&] { launch_gram_trial(ch->c, ch->c.p, PH_ALL, 0, s); });
+      L(5, [&] { launch_accept(ch->c, PH_ALL, s); });
+    }
+    if (max_steps > 0 && !job->profile && !ch->gexec) {
+      Launcher Lc{job, s, nullptr};
+      CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "capture");
+      iteration(ch->c, Lc);
+      ctx->launches -= 7;
+      cudaError_t ce = cudaStreamEndCapture(s, &ch->graph);
+      if (ce != cudaSuccess) return cuda_err(ctx, ce, "end capture");
+      CK(cudaGraphInstantiate(&ch->gexec, ch->graph, 0), "graph instantiate");
+    }
+    if (max_steps == 0) ch->done = true;
+  }
+  CK(cudaGetLastError(), "launch");
+  // LM loop: every unfinished chunk advances UPH_CHECK_EVERY iterations, then
+  // one host check of the active counts.
+  for (;;) {
+    bool any = false;
+    for (int i = 0; i < nch; ++i) {
+      Chunk* ch = job->chunks[i];
+      if (ch->done) continue;
+      any = true;
+      cudaStream_t s = job->streams[ch->slot];
+      const int group = std::min(UPH_CHECK_EVERY, max_steps - ch->iters);
+      for (int j = 0; j < group; ++j) {
+        if (job->profile) {
+          Launcher L{job, s, recp};
+          iteration(ch->c, L);
+        } else {
+          CK(cudaGraphLaunch(ch->gexec, s), "graph launch");
+          ctx->launches += 7;
+        }
+      }
+      ch->iters += group;
+      launch_count_active(ch->c, s);
+      ctx->launches += 1;
+      CK(cudaMemcpyAsync(job->h_active + i, ch->c.n_active, sizeof(int),
+                         cudaMemcpyDeviceToHost, s), "count");
+      CK(cudaEventRecord(ch->ev_group, s), "event");
+    }
+    if (!any) break;
+    for (int i = 0; i < nch; ++i) {
+      Chunk* ch = job->chunks[i];
+      if (ch->done) continue;
+      CK(cudaEventSynchronize(ch->ev_group), "lm loop");
+      if (job->h_active[i] == 0 || ch->iters >= max_steps) ch->done = true;
+    }
+  }
+  CK(cudaEventRecord(ctx->ev[1], ctx->stream), "event");
+  for (int i = 0; i < nch; ++i) {
+    Chunk* ch = job->chunks[i];
+    Launcher L{job, job->streams[ch->slot], recp};
+    post_loop(ch, L);
+  }
   CK(cudaGetLastError(), "post-loop");
-  CK(cudaEventRecord(ctx->ev[3], s), "event");
-  // ---- outputs ----
+  for (auto st : job->streams) {
+    cudaEvent_t e;
+    CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
+    CK(cudaEventRecord(e, st), "event");
+    CK(cudaStreamWaitEvent(ctx->stream, e, 0), "join");
+    cudaEventDestroy(e);
+  }
+  CK(cudaEventRecord(ctx->ev[2], ctx->stream), "event");
+  CK(cudaStreamSynchronize(ctx->stream), "solve");
+  cudaEventElapsedTime(&ctx->timing[1], ctx->ev[0], ctx->ev[2]);
+  ctx->timing[2] = 0.f;
+  if (job->profile) {
+    for (int k = 0; k < 6; ++k) {
+      job->ktime[k] = 0.f;
+      job->kcount[k] = 0;
+    }
+    for (auto& r : rec) {
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, r.second.first, r.second.second);
+      job->ktime[r.first] += ms;
+      job->kcount[r.first] += 1;
+      cudaEventDestroy(r.second.first);
+      cudaEventDestroy(r.second.second);
+    }
+  }
+  return UPH_OK;
+}
+
+int job_read(uph_job* job, int id, uph_chunk_out* out) {
+  uph_ctx* ctx = job->ctx;
+  if (id < 0 || id >= (int)job->chunks.size())
+    return set_err(ctx, UPH_ERR_INVALID, "bad chunk id %d", id);
+  if (!out) return set_err(ctx, UPH_ERR_INVALID, "null output");
+  Chunk* ch = job->chunks[id];
+  const ClassDev& c = ch->c;
+  const int n = ch->n, N = ch->N, nb = ch->nb, nP = ch->nP;
   std::vector<uint8_t> fl(n);
   std::vector<int> ng((size_t)n * nb);
   std::vector<float> pbest(n);
+  std::vector<int> nst(n);
+  int rc;
   if ((rc = download(ctx, out->p, c.p, sizeof(float) * n * nP, "p"))) return rc;
   if ((rc = download(ctx, out->fluxes, c.flux, sizeof(float) * n * nb * N, "flux"))) return rc;
   if ((rc = download(ctx, out->ferr, c.ferr, sizeof(float) * n * nb * N, "ferr"))) return rc;
   if ((rc = download(ctx, out->chi2, c.chi2, sizeof(float) * n, "chi2"))) return rc;
-  if ((rc = download(ctx, out->nst, c.nst, sizeof(int) * n, "nst"))) return rc;
+  if ((rc = download(ctx, nst.data(), c.nst, sizeof(int) * n, "nst"))) return rc;
   if ((rc = download(ctx, out->lam, c.lam, sizeof(float) * n, "lam"))) return rc;
   if ((rc = download(ctx, out->consec, c.consec, sizeof(int) * n, "consec"))) return rc;
   if ((rc = download(ctx, out->nrej, c.nrej, sizeof(int) * n, "nrej"))) return rc;
-  if ((rc = download(ctx, out->diverged, d_div, n, "diverged"))) return rc;
+  if ((rc = download(ctx, out->diverged, ch->d_div, n, "diverged"))) return rc;
   if ((rc = download(ctx, fl.data(), c.flags, n, "flags"))) return rc;
   if ((rc = download(ctx, ng.data(), c.ngood, sizeof(int) * n * nb, "ngood"))) return rc;
   if ((rc = download(ctx, pbest.data(), c.probe_best, sizeof(float) * n, "probe"))) return rc;
-  CK(cudaEventRecord(ctx->ev[4], s), "event");
-  CK(cudaStreamSynchronize(s), "chunk");
+  CK(cudaStreamSynchronize(ctx->stream), "read");
   int steps_run = 0;
   for (int i = 0; i < n; ++i) {
     const bool st = (fl[i] & FL_STALL) != 0;
+    if (out->nst) out->nst[i] = nst[i];
     if (out->conv) out->conv[i] = (fl[i] & FL_CONV) ? 1 : 0;
     if (out->stall) out->stall[i] = st ? 1 : 0;
     if (out->stall_dchi2) out->stall_dchi2[i] = st ? pbest[i] : NAN;
@@ -636,12 +812,111 @@ int uph_run_chunk(uph_ctx* ctx, const uph_class_desc* cls,
       for (int b = 0; b < nb; ++b) t += ng[(size_t)i * nb + b];
       out->n_good[i] = t;
     }
-    const int ran = (out->nst ? out->nst[i] : 0) - h_nst[i];
-    steps_run = std::max(steps_run, ran);
+    steps_run = std::max(steps_run, nst[i] - ch->h_nst0[i]);
   }
   out->steps_run = steps_run;
-  for (int i = 0; i < 4; ++i) cudaEventElapsedTime(&ctx->timing[i], ctx->ev[i], ctx->ev[i + 1]);
   return UPH_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int uph_job_create(uph_ctx* ctx, uph_job** out) {
+  if (!ctx || !out) return UPH_ERR_INVALID;
+  uph_job* j = new uph_job();
+  j->ctx = ctx;
+  *out = j;
+  return UPH_OK;
+}
+
+int uph_job_destroy(uph_job* job) {
+  if (!job) return UPH_OK;
+  cudaSetDevice(job->ctx->device);
+  cudaStreamSynchronize(job->ctx->stream);
+  for (auto s : job->streams) cudaStreamSynchronize(s);
+  delete job;
+  return UPH_OK;
+}
+
+int uph_job_add_chunk(uph_job* job, const uph_class_desc* cls,
+                      const uph_chunk_in* in, int32_t* chunk_id) {
+  if (!job) return UPH_ERR_INVALID;
+  uph_ctx* ctx = job->ctx;
+  if (!cls || !in) return set_err(ctx, UPH_ERR_INVALID, "null argument");
+  cudaSetDevice(ctx->device);
+  Chunk* ch = new Chunk();
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  cudaEventRecord(a, ctx->stream);
+  int rc = add_chunk(ctx, ch, cls, in);
+  if (rc) {
+    cudaStreamSynchronize(ctx->stream);
+    delete ch;
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    return rc;
+  }
+  cudaEventRecord(b, ctx->stream);
+  cudaEventSynchronize(b);
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, a, b);
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  if (job->chunks.empty()) ctx->timing[0] = 0.f;
+  ctx->timing[0] += ms;
+  job->chunks.push_back(ch);
+  if (chunk_id) *chunk_id = (int32_t)job->chunks.size() - 1;
+  return UPH_OK;
+}
+
+int uph_job_solve(uph_job* job, int32_t max_steps) {
+  if (!job) return UPH_ERR_INVALID;
+  return job_solve(job, max_steps);
+}
+
+int uph_job_read(uph_job* job, int32_t chunk_id, uph_chunk_out* out) {
+  if (!job) return UPH_ERR_INVALID;
+  cudaSetDevice(job->ctx->device);
+  cudaEvent_t a = job->ctx->ev[3], b = job->ctx->ev[4];
+  cudaEventRecord(a, job->ctx->stream);
+  int rc = job_read(job, chunk_id, out);
+  cudaEventRecord(b, job->ctx->stream);
+  cudaEventSynchronize(b);
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, a, b);
+  job->ctx->timing[3] = (chunk_id == 0 ? 0.f : job->ctx->timing[3]) + ms;
+  return rc;
+}
+
+int uph_job_set_profile(uph_job* job, int32_t on) {
+  if (!job) return UPH_ERR_INVALID;
+  job->profile = on != 0;
+  return UPH_OK;
+}
+
+int uph_job_kernel_time(const uph_job* job, int32_t kind, float* ms,
+                        int64_t* launches) {
+  if (!job || kind < 0 || kind >= 6) return UPH_ERR_INVALID;
+  if (ms) *ms = job->ktime[kind];
+  if (launches) *launches = job->kcount[kind];
+  return UPH_OK;
+}
+
+int uph_run_chunk(uph_ctx* ctx, const uph_class_desc* cls,
+                  const uph_chunk_in* in, int32_t max_steps,
+                  uph_chunk_out* out) {
+  if (!ctx) return UPH_ERR_INVALID;
+  if (!out) return set_err(ctx, UPH_ERR_INVALID, "null output");
+  uph_job* job = nullptr;
+  int rc = uph_job_create(ctx, &job);
+  if (rc) return rc;
+  rc = uph_job_add_chunk(job, cls, in, nullptr);
+  if (!rc) rc = uph_job_solve(job, max_steps);
+  if (!rc) rc = uph_job_read(job, 0, out);
+  uph_job_destroy(job);
+  return rc;
 }
 
 }  // extern "C"

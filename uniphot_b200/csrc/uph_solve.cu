@@ -46,11 +46,89 @@ struct RowSrc {
   int K;
 };
 
+// Value of Gram row r at window pixel (wy, wx), already scaled by sqrt(w).
+__device__ __forceinline__ float row_value(const ClassDev& c, int isl, int b,
+                                           const RowSrc& rows, const int4* box,
+                                           int r, int wy, int wx, float sw,
+                                           const float* dbase) {
+  const int rs = rows.rs[r];
+  if (rs < 0) return dbase[(size_t)wy * c.Wp + wx] * sw;
+  const int k = rows.rk[r];
+  const int4 bx = box[k];
+  const int ly = wy - bx.y, lx = wx - bx.x;
+  if (ly >= 0 && ly < bx.w && lx >= 0 && lx < bx.z)
+    return c.stamps[stamp_slot(c, isl, b, k, rs) + (size_t)ly * c.Sz + lx] * sw;
+  return 0.f;
+}
+
+// Small-K path (K <= 8): every thread accumulates the packed upper triangle
+// of its own pixels in registers; warp-shuffle + fixed-order block reduction.
+__device__ void gram_window_small(const ClassDev& c, int isl, int b,
+                                  const RowSrc& rows, const int4* box,
+                                  float* out, int ld, float* sm) {
+  const int tid = threadIdx.x;
+  const int K = rows.K;
+  const int B = c.B;
+  const int npix = B * B;
+  const size_t plane = (size_t)c.Hp * c.Wp;
+  const float* dbase = c.dstack + b * plane + (size_t)c.oy[isl] * c.Wp + c.ox[isl];
+  const float* wbase = c.wstack + b * plane + (size_t)c.oy[isl] * c.Wp + c.ox[isl];
+  float acc[36];
+#pragma unroll
+  for (int e = 0; e < 36; ++e) acc[e] = 0.f;
+  for (int pix = tid; pix < npix; pix += NT) {
+    const int wy = pix / B, wx = pix - (pix / B) * B;
+    const float sw = sqrtf(wbase[(size_t)wy * c.Wp + wx]);
+    float z[8];
+#pragma unroll
+    for (int r = 0; r < 8; ++r)
+      z[r] = (r < K) ? row_value(c, isl, b, rows, box, r, wy, wx, sw, dbase) : 0.f;
+    int e = 0;
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+      for (int j = i; j < 8; ++j) {
+        acc[e] = fmaf(z[i], z[j], acc[e]);
+        ++e;
+      }
+  }
+  const int lane = tid & 31, warp = tid >> 5;
+#pragma unroll
+  for (int e = 0; e < 36; ++e) {
+    float v = acc[e];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    acc[e] = v;
+  }
+  if (lane == 0)
+    for (int e = 0; e < 36; ++e) sm[warp * 36 + e] = acc[e];
+  __syncthreads();
+  if (tid < 36) {
+    float t = 0.f;
+    for (int w = 0; w < NT / 32; ++w) t += sm[w * 36 + tid];
+    int i = 0, rem = tid;
+    while (rem >= 8 - i) {
+      rem -= 8 - i;
+      ++i;
+    }
+    const int j = i + rem;
+    if (i < K && j < K) {
+      out[i * ld + j] = t;
+      out[j * ld + i] = t;
+    }
+  }
+  __syncthreads();
+}
+
 __device__ void gram_window(const ClassDev& c, int isl, int b, RowSrc rows,
                             const int4* box, float* out, int ld, int part,
                             float* sm) {
   const int tid = threadIdx.x;
   const int K = rows.K;
+  if (K <= 8) {
+    if (part == 0) gram_window_small(c, isl, b, rows, box, out, ld, sm);
+    return;
+  }
   const int nbk = (K + 7) / 8;
   const int nblk = nbk * (nbk + 1) / 2;
   int s, my, split;
@@ -71,7 +149,7 @@ __device__ void gram_window(const ClassDev& c, int isl, int b, RowSrc rows,
   const int LD = TP + 1;
   float* Zs = sm;                        // nbk*8 x LD
   float* swt = Zs + nbk * 8 * LD;        // TP
-  const int B = c.B, Sz = c.Sz;
+  const int B = c.B;
   const int npix = B * B;
   const size_t plane = (size_t)c.Hp * c.Wp;
   const float* dbase = c.dstack + b * plane + (size_t)c.oy[isl] * c.Wp + c.ox[isl];
@@ -99,16 +177,7 @@ __device__ void gram_window(const ClassDev& c, int isl, int b, RowSrc rows,
       float v = 0.f;
       if (r < K && pix < npix) {
         const int wy = pix / B, wx = pix - (pix / B) * B;
-        const int rs = rows.rs[r];
-        if (rs < 0) {
-          v = dbase[(size_t)wy * c.Wp + wx] * swt[q];
-        } else {
-          const int k = rows.rk[r];
-          const int4 bx = box[k];
-          const int ly = wy - bx.y, lx = wx - bx.x;
-          if (ly >= 0 && ly < bx.w && lx >= 0 && lx < bx.z)
-            v = c.stamps[stamp_slot(c, isl, b, k, rs) + (size_t)ly * Sz + lx] * swt[q];
-        }
+        v = row_value(c, isl, b, rows, box, r, wy, wx, swt[q], dbase);
       }
       Zs[r * LD + q] = v;
     }
@@ -131,20 +200,23 @@ __device__ void gram_window(const ClassDev& c, int isl, int b, RowSrc rows,
     }
     __syncthreads();
   }
-  // deterministic reduction over the pixel splits
+  // deterministic tree reduction over the pixel splits of each block
   if (s > 1) {
     float* red = sm;  // NT x 65
     for (int i = 0; i < 8; ++i)
       for (int j = 0; j < 8; ++j) red[tid * 65 + i * 8 + j] = acc[i][j];
     __syncthreads();
-    if (my >= 0 && split == 0) {
-      for (int i = 0; i < 8; ++i)
-        for (int j = 0; j < 8; ++j) {
-          float t = 0.f;
-          for (int sp = 0; sp < s; ++sp) t += red[(tid + sp) * 65 + i * 8 + j];
-          acc[i][j] = t;
-        }
+    int cur = s;
+    while (cur > 1) {
+      const int half = (cur + 1) >> 1;
+      if (my >= 0 && split + half < cur)
+        for (int e = 0; e < 64; ++e) red[tid * 65 + e] += red[(tid + half) * 65 + e];
+      __syncthreads();
+      cur = half;
     }
+    if (my >= 0 && split == 0)
+      for (int i = 0; i < 8; ++i)
+        for (int j = 0; j < 8; ++j) acc[i][j] = red[tid * 65 + i * 8 + j];
   }
   if (my >= 0 && split == 0) {
     for (int i = 0; i < 8; ++i) {
@@ -158,6 +230,7 @@ __device__ void gram_window(const ClassDev& c, int isl, int b, RowSrc rows,
       }
     }
   }
+  __syncthreads();
 }
 
 __device__ void load_boxes(const ClassDev& c, int isl, const float* P,
@@ -707,6 +780,15 @@ __global__ void k_set_probe(ClassDev c) {
 }
 
 }  // namespace
+
+__global__ void k_fill_float(float* p, float v, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) p[i] = v;
+}
+
+void launch_fill_float(float* p, float v, int n, cudaStream_t s) {
+  if (n > 0) k_fill_float<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(p, v, n);
+}
 
 void launch_set_probe(const ClassDev& c, cudaStream_t s) {
   k_set_probe<<<(unsigned)((c.n_isl + 127) / 128), 128, 0, s>>>(c);

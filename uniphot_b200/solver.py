@@ -301,43 +301,37 @@ def _chunk_size(plan, n_bands: int, budget_bytes: float) -> int:
     return int(max(1, min(plan.n_islands, budget_bytes // max(per, 1.0))))
 
 
-def island_fit(*, bandnames: list, data_minus_bg: np.ndarray, invvar: np.ndarray,
-               psfs: list, island_set, buckets, pos_x, pos_y, source_type, logre,
-               ee1, ee2, sersic_n, s1_flux, s1_flux_var, pos_err=None,
-               re_prior_sig=None, ell_prior_sig=None, theta_prior_sig=None,
-               sersic_n_prior_sig=None, render_backend: str = "fft",
-               fit_sersic_n: bool = True, n_fit_min_snr: float = 30.0,
-               pos_max_shift_pix: float = 5.0,
-               pos_step_max_pix: float = DEFAULT_POS_STEP_MAX,
-               max_steps: int = DEFAULT_MAX_STEPS,
-               max_steps_main: int | None = DEFAULT_MAX_STEPS_MAIN,
-               chi2_ftol_rel: float = DEFAULT_CHI2_FTOL_REL,
-               step_tol_pix: float = DEFAULT_STEP_TOL_PIX,
-               un_freeze_steps: int = DEFAULT_UN_FREEZE_STEPS, reg: float = 1e-9,
-               nsrc_max: int | None = None, joint_nsrc_cap: int = 32,
-               star_render_split: bool = True, stall_count_mode: str = "proposals",
-               convergence: str = "legacy", plateau_dlnp_tol: float = 0.5,
-               include_giants: bool = True, compute_param_errors: bool = False,
-               compute_source_metrics: bool = False, compute_re_profile: bool = False,
-               return_island_residual: bool = False, free_n_override=None,
-               log_fn: Optional[Callable[[str], None]] = None,
-               render_mode: str | None = None, tier_ladder=(111, 221),
-               native_stamp: int | None = None, device: int = 0,
-               field: DeviceField | None = None,
-               chunk_budget_bytes: float = 16e9):
-    """Fit all bucketed islands (+ giants), class by class, on the GPU."""
-    def log(msg):
-        if log_fn is not None:
-            log_fn(msg)
-    for flag, name in ((compute_param_errors, "compute_param_errors"),
-                       (compute_source_metrics, "compute_source_metrics"),
-                       (compute_re_profile, "compute_re_profile"),
-                       (return_island_residual, "return_island_residual")):
-        if flag:
-            raise ValueError(f"{name} is not supported by the B200 island solver")
+def pad_stacks(data_minus_bg, invvar, PAD: int):
+    """Zero-padded (n_bands, H + 2 PAD, W + 2 PAD) float32 field stacks
+    (island_solver.py:3334-3344)."""
+    nb, H, W = data_minus_bg.shape
+    dstack = np.zeros((nb, H + 2 * PAD, W + 2 * PAD), np.float32)
+    wstack = np.zeros_like(dstack)
+    dstack[:, PAD:PAD + H, PAD:PAD + W] = data_minus_bg
+    wstack[:, PAD:PAD + H, PAD:PAD + W] = invvar
+    return dstack, wstack
+
+
+@dataclass
+class FieldPlan:
+    """Host-side plan of a field: classes with their host arrays."""
+    classes: list          # [(IslandClassPlan, host dict)]
+    capped: list
+    PAD: int
+    native: int
+    render_mode: str
+
+
+def plan_field(*, psfs, island_set, buckets, pos_x, pos_y, source_type, logre, ee1,
+               ee2, sersic_n, s1_flux, s1_flux_var, pos_err=None, re_prior_sig=None,
+               ell_prior_sig=None, theta_prior_sig=None, sersic_n_prior_sig=None,
+               fit_sersic_n=True, n_fit_min_snr=30.0, pos_max_shift_pix=5.0,
+               nsrc_max=None, joint_nsrc_cap=32, free_n_override=None, log_fn=None,
+               render_mode=None, tier_ladder=(111, 221), native_stamp=None,
+               **_ignored) -> FieldPlan:
+    """Class planning and per-class host arrays (no device work)."""
     if render_mode is None:
         render_mode = "analytic" if _is_mog(psfs[0]) else "reference"
-    n_bands = len(bandnames)
     if native_stamp is not None:
         native = int(native_stamp)
     elif render_mode == "reference":
@@ -353,94 +347,189 @@ def island_fit(*, bandnames: list, data_minus_bg: np.ndarray, invvar: np.ndarray
         island_set, buckets, source_type, logre, sersic_n, native,
         joint_nsrc_cap=joint_nsrc_cap, nsrc_max=nsrc_max, log_fn=log_fn,
         tier_ladder=tier_ladder)
-    occupied_B = max((p.bbox_class for p in plans), default=32)
-    PAD = int(occupied_B) + 8
-    H, W = data_minus_bg.shape[1], data_minus_bg.shape[2]
-    if field is None or field.pad != PAD or field.shape != (n_bands, H + 2 * PAD,
-                                                           W + 2 * PAD):
-        dstack = np.zeros((n_bands, H + 2 * PAD, W + 2 * PAD), np.float32)
-        wstack = np.zeros_like(dstack)
-        dstack[:, PAD:PAD + H, PAD:PAD + W] = data_minus_bg
-        wstack[:, PAD:PAD + H, PAD:PAD + W] = invvar
-        field = DeviceField(dstack, wstack, PAD, device=device,
-                            context=field.ctx if field is not None else None)
-        del dstack, wstack
-    src_kwargs = dict(pos_x=pos_x, pos_y=pos_y, source_type=source_type, logre=logre,
-                      ee1=ee1, ee2=ee2, sersic_n=sersic_n, free_n_all=free_n_all,
-                      pos_max_shift_pix=float(pos_max_shift_pix), pad=PAD,
-                      pos_err=pos_err, re_prior_sig=re_prior_sig,
-                      ell_prior_sig=ell_prior_sig, theta_prior_sig=theta_prior_sig,
-                      sersic_n_prior_sig=sersic_n_prior_sig)
-    out_rows, bucket_stats = [], []
-    trees = {}
-    for plan in plans:
-        B, N, T, kind = int(plan.bbox_class), int(plan.nsrc_class), int(plan.tier), plan.kind
-        n_isl = plan.n_islands
-        t_b = time.perf_counter()
-        host = class_host_arrays(plan, **src_kwargs)
-        if T not in trees:
-            trees[T] = build_psf_tree(psfs, T)
-        tree, n_terms = trees[T]
-        kern = make_class_kernels(
-            plan, n_bands, n_terms, render_backend=render_backend, reg=reg,
-            pos_step_max_pix=pos_step_max_pix, chi2_ftol_rel=chi2_ftol_rel,
-            step_tol_pix=step_tol_pix, un_freeze_steps=un_freeze_steps,
-            star_render_split=star_render_split, has_priors=bool(host["has_priors"]),
-            stall_count_mode=stall_count_mode, convergence=convergence,
-            plateau_dlnp_tol=plateau_dlnp_tol, render_mode=render_mode)
-        chunk = _chunk_size(plan, n_bands, chunk_budget_bytes)
-        res = {}
-        for lo in range(0, n_isl, chunk):
-            rows = np.arange(lo, min(lo + chunk, n_isl))
-            o = run_class_chunk_resilient(kern, tree, host, rows, rows.size, max_steps,
-                                          field, field, PAD, log_fn=log_fn)
-            for k, v in o.items():
-                if isinstance(v, np.ndarray):
-                    res.setdefault(k, []).append(v)
-        res = {k: np.concatenate(v, axis=0) for k, v in res.items()}
-        dt = time.perf_counter() - t_b
-        nst = res["nst"]
-        bucket_stats.append(dict(
-            bbox_class=B, nsrc_class=N, tier=T, kind=kind, n_islands=int(n_isl),
-            n_chunks=int(np.ceil(n_isl / chunk)), chunk=chunk, wall_s=dt,
-            islands_per_s=n_isl / dt if dt > 0 else float("inf"),
-            mean_steps=float(nst.mean()), max_steps_used=int(nst.max()),
-            n_unconverged=int((~res["conv"]).sum()), n_stalled=int(res["stall"].sum()),
-            n_requeued=int((nst > (max_steps_main or max_steps)).sum())))
-        log(f"bucket bbox={B} nsrc={N} kind={kind} tier={T}: {n_isl} islands, "
-            f"{dt:.2f}s ({n_isl / max(dt, 1e-9):.0f} isl/s), "
-            f"mean_steps={nst.mean():.1f}")
-        out_rows.append(unpack_class_results(
-            plan, host, island_set, res["p"], res["fluxes"], res["ferr"], res["chi2"],
-            res["conv"], res["stall"], res["nst"], res_pdchi2=res["stall_dchi2"],
-            res_div=res["diverged"], res_ngood=res["n_good"], n_bands=n_bands))
-    giant_ids = np.concatenate([np.asarray(buckets.giant_ids, np.int64).ravel(),
-                                np.asarray(capped, np.int64)])
-    if include_giants and giant_ids.size:
-        out_rows.extend(giant_seed_rows(giant_ids, island_set, pos_x=pos_x, pos_y=pos_y,
-                                        logre=logre, ee1=ee1, ee2=ee2, sersic_n=sersic_n,
-                                        n_bands=n_bands))
-    cat = {k: np.concatenate([r[k] for r in out_rows], axis=0) for k in out_rows[0]}
-    return IslandFitResult(
-        bandnames=list(bandnames), source_idx=cat["src"].astype(np.int64),
-        pos_x=cat["pos_x"], pos_y=cat["pos_y"], logre=cat["logre"], ee1=cat["ee1"],
-        ee2=cat["ee2"], sersic_n=cat["sersic_n"], fluxes=cat["fluxes"],
-        flux_err=cat["flux_err"], chi2=cat["chi2"], chi2_nu=cat["chi2_nu"],
-        n_steps=cat["n_steps"], converged=cat["converged"], stalled=cat["stalled"],
-        diverged=cat["diverged"], stall_dchi2=cat["stall_dchi2"], free_n=cat["free_n"],
-        railed=cat["railed"], island_id=cat["island_id"],
-        island_nsrc=cat["island_nsrc"], island_giant=cat["island_giant"],
-        re_upper_pix=cat["re_upper_pix"], pos_x_err=cat["pos_x_err"],
-        pos_y_err=cat["pos_y_err"], re_err=cat["re_err"], ell_err=cat["ell_err"],
-        re_prof_lo=cat["re_prof_lo"], re_prof_hi=cat["re_prof_hi"],
-        theta_err=cat["theta_err"], sersic_n_err=cat["sersic_n_err"],
-        pos_x_prior_frac=cat["pos_x_prior_frac"], pos_y_prior_frac=cat["pos_y_prior_frac"],
-        re_prior_frac=cat["re_prior_frac"], ell_prior_frac=cat["ell_prior_frac"],
-        theta_prior_frac=cat["theta_prior_frac"],
-        sersic_n_prior_frac=cat["sersic_n_prior_frac"], rchisq=cat["rchisq"],
-        fracflux=cat["fracflux"], fracin=cat["fracin"], fracmasked=cat["fracmasked"],
-        flux_win=cat["flux_win"], flux_marg_var=cat["flux_marg_var"],
-        bucket_stats=bucket_stats)
+    PAD = int(max((p.bbox_class for p in plans), default=32)) + 8
+    kw = dict(pos_x=pos_x, pos_y=pos_y, source_type=source_type, logre=logre,
+              ee1=ee1, ee2=ee2, sersic_n=sersic_n, free_n_all=free_n_all,
+              pos_max_shift_pix=float(pos_max_shift_pix), pad=PAD, pos_err=pos_err,
+              re_prior_sig=re_prior_sig, ell_prior_sig=ell_prior_sig,
+              theta_prior_sig=theta_prior_sig, sersic_n_prior_sig=sersic_n_prior_sig)
+    classes = [(p, class_host_arrays(p, **kw)) for p in plans]
+    return FieldPlan(classes, capped, PAD, native, render_mode)
+
+
+class IslandFitJob:
+    """``island_fit`` split into its three phases: construction plans the
+    classes and uploads the field and every chunk's inputs to the device,
+    :meth:`solve` runs all chunks (device-resident, concurrent), and
+    :meth:`result` reads them back and unpacks the per-source rows."""
+
+    def __init__(self, *, bandnames: list, data_minus_bg: np.ndarray,
+                 invvar: np.ndarray, psfs: list, island_set, buckets, pos_x, pos_y,
+                 source_type, logre, ee1, ee2, sersic_n, s1_flux, s1_flux_var,
+                 pos_err=None, re_prior_sig=None, ell_prior_sig=None,
+                 theta_prior_sig=None, sersic_n_prior_sig=None,
+                 render_backend: str = "fft", fit_sersic_n: bool = True,
+                 n_fit_min_snr: float = 30.0, pos_max_shift_pix: float = 5.0,
+                 pos_step_max_pix: float = DEFAULT_POS_STEP_MAX,
+                 max_steps: int = DEFAULT_MAX_STEPS,
+                 max_steps_main: int | None = DEFAULT_MAX_STEPS_MAIN,
+                 chi2_ftol_rel: float = DEFAULT_CHI2_FTOL_REL,
+                 step_tol_pix: float = DEFAULT_STEP_TOL_PIX,
+                 un_freeze_steps: int = DEFAULT_UN_FREEZE_STEPS, reg: float = 1e-9,
+                 nsrc_max: int | None = None, joint_nsrc_cap: int = 32,
+                 star_render_split: bool = True,
+                 stall_count_mode: str = "proposals", convergence: str = "legacy",
+                 plateau_dlnp_tol: float = 0.5, include_giants: bool = True,
+                 compute_param_errors: bool = False,
+                 compute_source_metrics: bool = False,
+                 compute_re_profile: bool = False,
+                 return_island_residual: bool = False, free_n_override=None,
+                 log_fn: Optional[Callable[[str], None]] = None,
+                 render_mode: str | None = None, tier_ladder=(111, 221),
+                 native_stamp: int | None = None, device: int = 0,
+                 field: DeviceField | None = None,
+                 chunk_budget_bytes: float = 16e9):
+        for flag, name in ((compute_param_errors, "compute_param_errors"),
+                           (compute_source_metrics, "compute_source_metrics"),
+                           (compute_re_profile, "compute_re_profile"),
+                           (return_island_residual, "return_island_residual")):
+            if flag:
+                raise ValueError(f"{name} is not supported by the B200 island solver")
+        self.log_fn = log_fn
+        if render_mode is None:
+            render_mode = "analytic" if _is_mog(psfs[0]) else "reference"
+        self.render_mode = render_mode
+        n_bands = len(bandnames)
+        self.bandnames, self.n_bands = list(bandnames), n_bands
+        fp = plan_field(
+            psfs=psfs, island_set=island_set, buckets=buckets, pos_x=pos_x,
+            pos_y=pos_y, source_type=source_type, logre=logre, ee1=ee1, ee2=ee2,
+            sersic_n=sersic_n, s1_flux=s1_flux, s1_flux_var=s1_flux_var,
+            pos_err=pos_err, re_prior_sig=re_prior_sig, ell_prior_sig=ell_prior_sig,
+            theta_prior_sig=theta_prior_sig, sersic_n_prior_sig=sersic_n_prior_sig,
+            fit_sersic_n=fit_sersic_n, n_fit_min_snr=n_fit_min_snr,
+            pos_max_shift_pix=pos_max_shift_pix, nsrc_max=nsrc_max,
+            joint_nsrc_cap=joint_nsrc_cap, free_n_override=free_n_override,
+            log_fn=log_fn, render_mode=render_mode, tier_ladder=tier_ladder,
+            native_stamp=native_stamp)
+        PAD = fp.PAD
+        H, W = data_minus_bg.shape[1], data_minus_bg.shape[2]
+        if field is None or field.pad != PAD or field.shape != (
+                n_bands, H + 2 * PAD, W + 2 * PAD):
+            dstack, wstack = pad_stacks(data_minus_bg, invvar, PAD)
+            field = DeviceField(dstack, wstack, PAD, device=device,
+                                context=field.ctx if field is not None else None)
+            del dstack, wstack
+        self.field, self.PAD = field, PAD
+        plans = [p for p, _ in fp.classes]
+        capped = fp.capped
+        self.job = _lib.Job(field.ctx)
+        self.classes = []
+        trees = {}
+        for plan, host in fp.classes:
+            T = int(plan.tier)
+            if T not in trees:
+                trees[T] = build_psf_tree(psfs, T)
+            tree, n_terms = trees[T]
+            field.ensure_psf(tree)
+            if np.any(np.asarray(host["st"]) != SOURCE_STAR):
+                field.ensure_table()
+            kern = make_class_kernels(
+                plan, n_bands, n_terms, render_backend=render_backend, reg=reg,
+                pos_step_max_pix=pos_step_max_pix, chi2_ftol_rel=chi2_ftol_rel,
+                step_tol_pix=step_tol_pix, un_freeze_steps=un_freeze_steps,
+                star_render_split=star_render_split,
+                has_priors=bool(host["has_priors"]),
+                stall_count_mode=stall_count_mode, convergence=convergence,
+                plateau_dlnp_tol=plateau_dlnp_tol, render_mode=render_mode)
+            chunk = _chunk_size(plan, n_bands, chunk_budget_bytes)
+            ids = []
+            for lo in range(0, plan.n_islands, chunk):
+                rows = np.arange(lo, min(lo + chunk, plan.n_islands))
+                ids.append(self.job.add_chunk(kern.desc, _slice_host(host, rows),
+                                              n_bands))
+            self.classes.append((plan, host, ids))
+        self.max_steps = int(max_steps)
+        self.max_steps_main = max_steps_main
+        self.island_set, self.buckets, self.capped = island_set, buckets, capped
+        self.include_giants = include_giants
+        self.src = dict(pos_x=pos_x, pos_y=pos_y, logre=logre, ee1=ee1, ee2=ee2,
+                        sersic_n=sersic_n)
+        self.n_islands = sum(p.n_islands for p, _, _ in self.classes)
+
+    def solve(self):
+        t0 = time.perf_counter()
+        self.job.solve(self.max_steps)
+        self.solve_wall_s = time.perf_counter() - t0
+
+    def result(self) -> IslandFitResult:
+        out_rows, bucket_stats = [], []
+        n_bands = self.n_bands
+        for plan, host, ids in self.classes:
+            parts = [self.job.read(i) for i in ids]
+            res = {k: np.concatenate([p[k] for p in parts], axis=0)
+                   for k in parts[0] if isinstance(parts[0][k], np.ndarray)}
+            nst = res["nst"]
+            bucket_stats.append(dict(
+                bbox_class=int(plan.bbox_class), nsrc_class=int(plan.nsrc_class),
+                tier=int(plan.tier), kind=plan.kind, n_islands=int(plan.n_islands),
+                n_chunks=len(ids), mean_steps=float(nst.mean()),
+                max_steps_used=int(nst.max()),
+                n_unconverged=int((~res["conv"]).sum()),
+                n_stalled=int(res["stall"].sum()),
+                n_requeued=int((nst > (self.max_steps_main or self.max_steps)).sum())))
+            if self.log_fn is not None:
+                self.log_fn(f"bucket bbox={plan.bbox_class} nsrc={plan.nsrc_class} "
+                            f"kind={plan.kind} tier={plan.tier}: {plan.n_islands} "
+                            f"islands, mean_steps={nst.mean():.1f}")
+            out_rows.append(unpack_class_results(
+                plan, host, self.island_set, res["p"], res["fluxes"], res["ferr"],
+                res["chi2"], res["conv"], res["stall"], res["nst"],
+                res_pdchi2=res["stall_dchi2"], res_div=res["diverged"],
+                res_ngood=res["n_good"], n_bands=n_bands))
+        giant_ids = np.concatenate([np.asarray(self.buckets.giant_ids, np.int64).ravel(),
+                                    np.asarray(self.capped, np.int64)])
+        if self.include_giants and giant_ids.size:
+            out_rows.extend(giant_seed_rows(giant_ids, self.island_set,
+                                            n_bands=n_bands, **self.src))
+        cat = {k: np.concatenate([r[k] for r in out_rows], axis=0) for k in out_rows[0]}
+        return IslandFitResult(
+            bandnames=list(self.bandnames), source_idx=cat["src"].astype(np.int64),
+            pos_x=cat["pos_x"], pos_y=cat["pos_y"], logre=cat["logre"],
+            ee1=cat["ee1"], ee2=cat["ee2"], sersic_n=cat["sersic_n"],
+            fluxes=cat["fluxes"], flux_err=cat["flux_err"], chi2=cat["chi2"],
+            chi2_nu=cat["chi2_nu"], n_steps=cat["n_steps"],
+            converged=cat["converged"], stalled=cat["stalled"],
+            diverged=cat["diverged"], stall_dchi2=cat["stall_dchi2"],
+            free_n=cat["free_n"], railed=cat["railed"], island_id=cat["island_id"],
+            island_nsrc=cat["island_nsrc"], island_giant=cat["island_giant"],
+            re_upper_pix=cat["re_upper_pix"], pos_x_err=cat["pos_x_err"],
+            pos_y_err=cat["pos_y_err"], re_err=cat["re_err"], ell_err=cat["ell_err"],
+            re_prof_lo=cat["re_prof_lo"], re_prof_hi=cat["re_prof_hi"],
+            theta_err=cat["theta_err"], sersic_n_err=cat["sersic_n_err"],
+            pos_x_prior_frac=cat["pos_x_prior_frac"],
+            pos_y_prior_frac=cat["pos_y_prior_frac"],
+            re_prior_frac=cat["re_prior_frac"], ell_prior_frac=cat["ell_prior_frac"],
+            theta_prior_frac=cat["theta_prior_frac"],
+            sersic_n_prior_frac=cat["sersic_n_prior_frac"], rchisq=cat["rchisq"],
+            fracflux=cat["fracflux"], fracin=cat["fracin"],
+            fracmasked=cat["fracmasked"], flux_win=cat["flux_win"],
+            flux_marg_var=cat["flux_marg_var"], bucket_stats=bucket_stats)
+
+    def close(self):
+        self.job.close()
+
+
+def island_fit(**kwargs) -> IslandFitResult:
+    """Fit all bucketed islands (+ giants) on the GPU; same keywords and
+    result as the reference's ``island_fit`` (plus ``render_mode``,
+    ``tier_ladder``, ``native_stamp``, ``device``, ``field``)."""
+    job = IslandFitJob(**kwargs)
+    try:
+        job.solve()
+        return job.result()
+    finally:
+        job.close()
 
 
 def _native_for_mog(psfs) -> int:
