@@ -143,7 +143,7 @@ def cpu_oracle_time(classes, PAD, field, sample, precision="ref", budget_s=40.0,
         psf = psf_bands(field.mog_psfs, plan.tier, "analytic")
         isl = island_inputs_from_host(host, r, B=plan.bbox_class, T=plan.tier,
                                       dstack=ds, wstack=ws, psf=psf, table=table,
-                                      mode="analytic")
+                                      mode="analytic", native=field.native)
         jobs.append((isl, cfg))
     t0 = time.perf_counter()
     done = []

@@ -55,6 +55,9 @@ typedef struct uph_class_desc {
   float step_tol_pix;       /* position step prong (0.1 px)                */
   int32_t un_freeze_steps;  /* u_n annealing budget (0 = never)            */
   int32_t has_priors;       /* nonlinear Gaussian priors present           */
+  int32_t native_stamp;     /* odd native PSF stamp side: a star's model is
+                               zero outside it (the reference zero-pads its
+                               native PSF to the tier); 0 = tier            */
 } uph_class_desc;
 
 /* Per-island inputs of one chunk of n islands (class_host_arrays rows;

@@ -345,7 +345,7 @@ def _gauss_and_dlog(xx, yy, A, C, B):
     """Normalised 2-D Gaussian at offsets and d ln N / d(A, C, B)."""
     det = A * C - B * B
     Q = (C * xx * xx - 2.0 * B * xx * yy + A * yy * yy) / det
-    N = np.exp(-0.5 * Q) / (2.0 * np.pi * math.sqrt(det))
+    N = np.exp(-0.5 * Q) / (2.0 * np.pi * np.sqrt(det))
     dA = (Q * C - yy * yy - C) / (2.0 * det)
     dC = (Q * A - xx * xx - A) / (2.0 * det)
     dB = (xx * yy - B * Q + B) / det
@@ -379,6 +379,7 @@ class IslandInput:
     psf: list                # per band PolyPsfBand | MogPsfBand
     table: SersicTable | None
     mode: str                # "reference" | "analytic"
+    native: int = 0          # star support side (0 = the tier)
 
 
 @dataclass
@@ -423,48 +424,74 @@ class IslandSolver:
         if isinstance(psf, PolyPsfBand):
             S, Sx, Sy, var = psf.stamp(x, y, self.dt)
             return S, (Sx if var else None), (Sy if var else None)
-        return self._analytic(band, x, y, None)[:3]
+        return self._analytic(band, x, y, None, True)[:3]
 
-    def _analytic(self, band, x, y, gal):
+    def _analytic(self, band, x, y, gal, need=True):
         """Analytic stamp.  gal = None (star) or (amps, vars, core, da, dv,
-        dcore, dn_du, c(3), dc(3,3)).  Returns S, Sx, Sy, S_shape(3), S_u."""
+        dcore, dn_du, c(3), dc(3,3)).  Returns S, Sx, Sy, S_shape(3), S_u.
+
+        Components (PSF q x galaxy g) are evaluated together; a star is the
+        PSF on its native stamp, zero beyond it (the reference zero-pads the
+        native PSF to the tier)."""
         psf = self.isl.psf[band]
         T = self.isl.T
         c0 = T // 2
-        yy, xx = np.mgrid[0:T, 0:T].astype(np.float64)
-        xx -= c0
-        yy -= c0
+        hs = c0 if gal is not None else min((self.isl.native or T) // 2, c0)
+        n = 2 * hs + 1
+        off = np.arange(-hs, hs + 1, dtype=np.float64)
+        xx = off[None, None, :]
+        yy = off[None, :, None]
         wq, cq, wqx, wqy, dcx, dcy = psf.components(float(x), float(y))
+        if gal is None:
+            ga = np.array([1.0]); gv = np.zeros(1); gda = np.zeros(1); gdv = np.zeros(1)
+            cgal = np.zeros(3)
+            dcg = np.zeros((3, 3))
+            dndu = 0.0
+        else:
+            amps, vars_, core, da, dv, dcore, dndu, cgal, dcg = gal
+            sel = (amps != 0.0) | (da != 0.0)
+            ga = np.concatenate([amps[sel], [core]])
+            gv = np.concatenate([vars_[sel], [0.0]])
+            gda = np.concatenate([da[sel], [dcore]])
+            gdv = np.concatenate([dv[sel], [0.0]])
+        K = wq.shape[0]
+        G = ga.shape[0]
+        A = (gv[None, :] * cgal[0] + cq[:, 0, None]).reshape(-1)[:, None, None]
+        C = (gv[None, :] * cgal[1] + cq[:, 1, None]).reshape(-1)[:, None, None]
+        Bc = (gv[None, :] * cgal[2] + cq[:, 2, None]).reshape(-1)[:, None, None]
+        wa = (wq[:, None] * ga[None, :]).reshape(-1)[:, None, None]
+        N, lA, lC, lB = _gauss_and_dlog(xx, yy, A, C, Bc)
+        Nw = wa * N
+        Sfull = np.zeros((6, T, T))
+        sub = (slice(c0 - hs, c0 + hs + 1), slice(c0 - hs, c0 + hs + 1))
         S = np.zeros((T, T))
+        S[sub] = Nw.sum(0)
         Sx = np.zeros((T, T))
         Sy = np.zeros((T, T))
         Ssh = np.zeros((3, T, T))
         Su = np.zeros((T, T))
-        if gal is None:
-            comps = [(1.0, 0.0, 0.0, 0.0)]
-            cgal = np.zeros(3)
-        else:
-            amps, vars_, core, da, dv, dcore, dndu, cgal, dcg = gal
-            comps = [(amps[g], vars_[g], da[g], dv[g])
-                     for g in range(amps.shape[0]) if amps[g] != 0.0 or da[g] != 0.0]
-            comps.append((core, 0.0, dcore, 0.0))
-        for q in range(wq.shape[0]):
-            for (a, v, dav, dvv) in comps:
-                A = v * cgal[0] + cq[q, 0]
-                C = v * cgal[1] + cq[q, 1]
-                Bc = v * cgal[2] + cq[q, 2]
-                N, lA, lC, lB = _gauss_and_dlog(xx, yy, A, C, Bc)
-                S += wq[q] * a * N
-                Sx += wqx[q] * a * N + wq[q] * a * N * (
-                    lA * dcx[q, 0] + lC * dcx[q, 1] + lB * dcx[q, 2])
-                Sy += wqy[q] * a * N + wq[q] * a * N * (
-                    lA * dcy[q, 0] + lC * dcy[q, 1] + lB * dcy[q, 2])
-                if gal is not None:
-                    for s in range(3):
-                        Ssh[s] += wq[q] * a * N * v * (
-                            lA * dcg[s, 0] + lC * dcg[s, 1] + lB * dcg[s, 2])
-                    Su += wq[q] * (dav * N + a * N * dvv * (
-                        lA * cgal[0] + lC * cgal[1] + lB * cgal[2])) * dndu
+        if need:
+            rep = lambda a: np.repeat(a, G, axis=0)  # noqa: E731  per (q, g)
+            wxa = (wqx[:, None] * ga[None, :]).reshape(-1)[:, None, None]
+            wya = (wqy[:, None] * ga[None, :]).reshape(-1)[:, None, None]
+            dx_ = rep(dcx)[:, :, None, None]
+            dy_ = rep(dcy)[:, :, None, None]
+            Sx[sub] = (wxa * N + Nw * (lA * dx_[:, 0] + lC * dx_[:, 1]
+                                       + lB * dx_[:, 2])).sum(0)
+            Sy[sub] = (wya * N + Nw * (lA * dy_[:, 0] + lC * dy_[:, 1]
+                                       + lB * dy_[:, 2])).sum(0)
+            if gal is not None:
+                v = np.tile(gv, K)[:, None, None]
+                dvv = np.tile(gdv, K)[:, None, None]
+                wda = (wq[:, None] * gda[None, :]).reshape(-1)[:, None, None]
+                gA = (Nw * v * lA).sum(0)
+                gC = (Nw * v * lC).sum(0)
+                gB = (Nw * v * lB).sum(0)
+                for s_ in range(3):
+                    Ssh[s_][sub] = gA * dcg[s_, 0] + gC * dcg[s_, 1] + gB * dcg[s_, 2]
+                Su[sub] = ((wda * N).sum(0) + (Nw * dvv * (
+                    lA * cgal[0] + lC * cgal[1] + lB * cgal[2])).sum(0)) * dndu
+        del Sfull
         dt = self.dt
         return (S.astype(dt), Sx.astype(dt), Sy.astype(dt),
                 Ssh.astype(dt), Su.astype(dt))
@@ -544,7 +571,7 @@ class IslandSolver:
         else:
             gal = self._gal_params(k, p)
             if isl.mode == "analytic":
-                S, Sx, Sy, Ssh, Su = self._analytic(band, x, y, gal)
+                S, Sx, Sy, Ssh, Su = self._analytic(band, x, y, gal, need)
             else:
                 S, Sx, Sy, Ssh, Su = self._galaxy_fft(band, x, y, gal, need)
         Lx, dLx = lanczos3_taps(dx)
@@ -844,7 +871,8 @@ def solve_island(isl: IslandInput, cfg: SolverConfig, max_steps: int = 30,
 
 
 def island_inputs_from_host(host: dict, row: int, *, B: int, T: int,
-                            dstack, wstack, psf: list, table, mode: str):
+                            dstack, wstack, psf: list, table, mode: str,
+                            native: int = 0):
     """Slice one island out of class host arrays + the padded stacks."""
     ox, oy = int(host["ox"][row]), int(host["oy"][row])
     N = host["mmask"].shape[1]
@@ -862,4 +890,4 @@ def island_inputs_from_host(host: dict, row: int, *, B: int, T: int,
         prior_mean=host["prior_mean"][row].reshape(-1).astype(np.float32),
         prior_inv_sigma=host["prior_inv_sigma"][row].reshape(-1).astype(np.float32),
         has_priors=bool(host["has_priors"]),
-        psf=psf, table=table, mode=mode)
+        psf=psf, table=table, mode=mode, native=int(native))

@@ -32,7 +32,8 @@ def field_classes(f, mode: str, kinds=("star", "mixed")):
     return plans, hosts, PAD, ds, ws, psfs
 
 
-def run_gpu(plans, hosts, PAD, ds, ws, psfs, mode, max_steps=30, field=None):
+def run_gpu(plans, hosts, PAD, ds, ws, psfs, mode, max_steps=30, field=None,
+            native=0):
     from uniphot_b200 import solver
     if field is None:
         field = solver.DeviceField(ds, ws, PAD)
@@ -42,7 +43,8 @@ def run_gpu(plans, hosts, PAD, ds, ws, psfs, mode, max_steps=30, field=None):
         kern = solver.make_class_kernels(
             plan, ds.shape[0], nt, render_backend="fft", reg=1e-9,
             pos_step_max_pix=0.5, chi2_ftol_rel=1e-4, step_tol_pix=0.1,
-            un_freeze_steps=0, has_priors=bool(host["has_priors"]), render_mode=mode)
+            un_freeze_steps=0, has_priors=bool(host["has_priors"]), render_mode=mode,
+            native_stamp=native)
         rows = np.arange(plan.n_islands)
         outs.append(solver.run_class_chunk(kern, tree, host, rows, rows.size,
                                            max_steps, field, field, PAD))
@@ -50,11 +52,12 @@ def run_gpu(plans, hosts, PAD, ds, ws, psfs, mode, max_steps=30, field=None):
 
 
 def run_oracle(plans, hosts, PAD, ds, ws, psfs, mode, precision="ref",
-               max_steps=30, processes=1):
+               max_steps=30, processes=1, native=0):
     from oracle.driver import solve_chunk
     return [solve_chunk(h, np.arange(p.n_islands), B=p.bbox_class, T=p.tier,
                         dstack=ds, wstack=ws, psfs=psfs, mode=mode, table_path=TABLE,
-                        precision=precision, max_steps=max_steps, processes=processes)
+                        precision=precision, max_steps=max_steps, processes=processes,
+                        native=native)
             for p, h in zip(plans, hosts)]
 
 

@@ -35,7 +35,7 @@ class ClassDesc(C.Structure):
                 ("render_mode", C.c_int32), ("reg", C.c_float),
                 ("pos_step_max", C.c_float), ("chi2_ftol_rel", C.c_float),
                 ("step_tol_pix", C.c_float), ("un_freeze_steps", C.c_int32),
-                ("has_priors", C.c_int32)]
+                ("has_priors", C.c_int32), ("native_stamp", C.c_int32)]
 
 
 class ChunkIn(C.Structure):

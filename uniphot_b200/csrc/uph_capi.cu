@@ -497,6 +497,8 @@ int add_chunk(uph_ctx* ctx, Chunk* ch, const uph_class_desc* cls,
   c.n_isl = n; c.nb = nb; c.N = N; c.nP = nP; c.B = B; c.T = T; c.Sz = Sz; c.R = R;
   c.Kmax = Kmax; c.nLmax = nLmax; c.ntile_side = (Sz + UPH_TILE - 1) / UPH_TILE;
   c.mode = mode;
+  c.native = (cls->native_stamp > 0 && cls->native_stamp < T) ? (cls->native_stamp | 1) : T;
+  c.has_gal = any_gal ? 1 : 0;
   c.Hp = ctx->Hp; c.Wp = ctx->Wp;
   c.dstack = (const float*)ctx->dstack.ptr;
   c.wstack = (const float*)ctx->wstack.ptr;

@@ -39,6 +39,8 @@
 struct ClassDev {
   int n_isl, nb, N, nP, B, T, Sz, R, Kmax, nLmax, ntile_side;
   int mode, nt, kpsf, psf_varies;
+  int native;              // star support side (odd, <= T)
+  int has_gal;             // some member of the chunk is extended
   int Hp, Wp;
   const float* dstack;
   const float* wstack;

@@ -42,7 +42,32 @@ struct MemberSetup {
   int is_gal;
   int need[NS];
   int live_row[6];           // stamp row of parameter j (0 = not live)
+  int support_half;          // S is zero beyond this offset from the centre
+  int nact;                  // components active on this tile
+  uint8_t act[UPH_MAXKPSF * UPH_MAXGAL];
 };
+
+// Pruning threshold: a Gaussian term whose Mahalanobis distance Q exceeds
+// this everywhere on a tile contributes < exp(-69) ~ 1e-30 of its norm there.
+constexpr float QCUT = 138.f;
+
+// Minimum over the rectangle [x0,x1] x [y0,y1] of
+// Q = ia x^2 + 2 ib x y + ic y^2 (positive definite).
+__device__ float qmin_box(float ia, float ib, float ic, float x0, float x1,
+                          float y0, float y1) {
+  if (x0 <= 0.f && x1 >= 0.f && y0 <= 0.f && y1 >= 0.f) return 0.f;
+  float best = INFINITY;
+  const float xs[2] = {x0, x1}, ys[2] = {y0, y1};
+  for (int e = 0; e < 2; ++e) {
+    const float xe = xs[e];
+    const float y = fminf(fmaxf(-ib * xe / ic, y0), y1);
+    best = fminf(best, ia * xe * xe + 2.f * ib * xe * y + ic * y * y);
+    const float ye = ys[e];
+    const float x = fminf(fmaxf(-ib * ye / ia, x0), x1);
+    best = fminf(best, ia * x * x + 2.f * ib * x * ye + ic * ye * ye);
+  }
+  return best;
+}
 
 __device__ void lanczos_taps(double d, float* L, float* dL) {
   double v[7], dv[7], s = 0.0, ds = 0.0;
@@ -143,173 +168,57 @@ __device__ void cov_terms(double lr, double e1, double e2, float* cg,
   }
 }
 
-__device__ void sersic_lookup(const ClassDev& c, double n, double* a,
-                              double* v, double& core, double* da, double* dv,
-                              double& dcore) {
-  bool inside = (n > c.tb_nmin) && (n < c.tb_nmax);
-  double nc = fmin(fmax(n, c.tb_nmin), c.tb_nmax);
-  // searchsorted(side='right') - 1
-  int lo = 0, hi = c.tb_n;
-  while (lo < hi) {
-    int mid = (lo + hi) >> 1;
-    if (c.tb_knots[mid] <= nc) lo = mid + 1; else hi = mid;
-  }
-  int i = lo - 1;
-  i = max(0, min(i, c.tb_n - 2));
-  double n0 = c.tb_knots[i], n1 = c.tb_knots[i + 1];
-  double t = 0.0, dt = 0.0;
-  if (n1 > n0) {
-    t = (nc - n0) / (n1 - n0);
-    dt = inside ? 1.0 / (n1 - n0) : 0.0;
-  }
-  for (int g = 0; g < c.tb_k; ++g) {
-    double a0 = c.tb_amps[i * c.tb_k + g], a1 = c.tb_amps[(i + 1) * c.tb_k + g];
-    double l0 = c.tb_lv[i * c.tb_k + g], l1 = c.tb_lv[(i + 1) * c.tb_k + g];
-    a[g] = (1 - t) * a0 + t * a1;
-    v[g] = exp((1 - t) * l0 + t * l1);
-    da[g] = dt * (a1 - a0);
-    dv[g] = v[g] * dt * (l1 - l0);
-  }
-  core = (1 - t) * c.tb_core[i] + t * c.tb_core[i + 1];
-  dcore = dt * (c.tb_core[i + 1] - c.tb_core[i]);
-}
+// Per-member scratch of the parallel setup (analytic mode).
+struct PsfComp {
+  double w, wx, wy;          // raw weight and its d/dx, d/dy
+  double cov[3], cx[3], cy[3];
+};
+struct GalComp {
+  double a, v, da, dv;
+};
+struct SetupScratch {
+  PsfComp pq[UPH_MAXKPSF];
+  GalComp gg[UPH_MAXGAL];
+  int ng;
+  int seg;                   // Sersic table segment
+  double t, dt;              // interpolation weight and d t / d n
+  double W, Wx, Wy;          // weight sums
+};
 
-// Analytic-mode member setup: PSF components at (x, y) and the galaxy
-// mixture, combined into Gaussian components (covariances add).
-__device__ void setup_analytic(const ClassDev& c, int b, int isl, int k,
-                               const float* P, MemberSetup& ms, GComp* comps,
-                               bool lin) {
-  const float* os = c.psf_os + 4 * b;
-  double X = ((double)P[(size_t)isl * c.nP + 6 * k] - os[0]) / os[1];
-  double Y = ((double)P[(size_t)isl * c.nP + 6 * k + 1] - os[2]) / os[3];
-  double bt[UPH_MAXNT], bx[UPH_MAXNT], by[UPH_MAXNT];
+// PSF component q at the member position (one thread per component).
+__device__ void psf_component(const ClassDev& c, int b, double X, double Y,
+                              double ixs, double iys, int q, PsfComp& o) {
+  double val[4] = {0, 0, 0, 0}, vx[4] = {0, 0, 0, 0}, vy[4] = {0, 0, 0, 0};
   for (int t = 0; t < c.nt; ++t) {
     int m, n;
     term_mn(t, m, n);
-    bt[t] = ipow(X, m) * ipow(Y, n);
-    bx[t] = m > 0 ? m * ipow(X, m - 1) * ipow(Y, n) / os[1] : 0.0;
-    by[t] = n > 0 ? n * ipow(X, m) * ipow(Y, n - 1) / os[3] : 0.0;
-  }
-  double w[UPH_MAXKPSF], wx[UPH_MAXKPSF], wy[UPH_MAXKPSF];
-  double cq[UPH_MAXKPSF][3], cx[UPH_MAXKPSF][3], cy[UPH_MAXKPSF][3];
-  double W = 0, Wx = 0, Wy = 0;
-  for (int q = 0; q < c.kpsf; ++q) {
-    double val[4] = {0, 0, 0, 0}, vx[4] = {0, 0, 0, 0}, vy[4] = {0, 0, 0, 0};
+    const double bt = ipow(X, m) * ipow(Y, n);
+    const double bx = m > 0 ? m * ipow(X, m - 1) * ipow(Y, n) * ixs : 0.0;
+    const double by = n > 0 ? n * ipow(X, m) * ipow(Y, n - 1) * iys : 0.0;
     for (int f = 0; f < 4; ++f) {
-      const float* cf = c.mog + (((size_t)b * c.kpsf + q) * 4 + f) * c.nt;
-      for (int t = 0; t < c.nt; ++t) {
-        val[f] += cf[t] * bt[t];
-        vx[f] += cf[t] * bx[t];
-        vy[f] += cf[t] * by[t];
-      }
-    }
-    double s = val[0], a1 = val[1], a2 = val[2];
-    double s2 = s * s;
-    cq[q][0] = s2 * (1 + a1);
-    cq[q][1] = s2 * (1 - a1);
-    cq[q][2] = s2 * a2;
-    cx[q][0] = 2 * s * vx[0] * (1 + a1) + s2 * vx[1];
-    cx[q][1] = 2 * s * vx[0] * (1 - a1) - s2 * vx[1];
-    cx[q][2] = 2 * s * vx[0] * a2 + s2 * vx[2];
-    cy[q][0] = 2 * s * vy[0] * (1 + a1) + s2 * vy[1];
-    cy[q][1] = 2 * s * vy[0] * (1 - a1) - s2 * vy[1];
-    cy[q][2] = 2 * s * vy[0] * a2 + s2 * vy[2];
-    w[q] = val[3];
-    wx[q] = vx[3];
-    wy[q] = vy[3];
-    W += val[3];
-    Wx += vx[3];
-    Wy += vy[3];
-  }
-  for (int q = 0; q < c.kpsf; ++q) {
-    double wn = w[q] / W;
-    double wnx = (wx[q] * W - w[q] * Wx) / (W * W);
-    double wny = (wy[q] * W - w[q] * Wy) / (W * W);
-    w[q] = wn;
-    wx[q] = wnx;
-    wy[q] = wny;
-  }
-  // galaxy mixture
-  double ga[UPH_MAXGAL], gv[UPH_MAXGAL], gda[UPH_MAXGAL], gdv[UPH_MAXGAL];
-  int ng = 0;
-  ms.cg[0] = ms.cg[1] = ms.cg[2] = 0.f;
-  ms.dndu = 0.f;
-  if (ms.is_gal) {
-    const float* pk = P + (size_t)isl * c.nP + 6 * k;
-    double n, dndu = 0.0;
-    if (c.free_n[isl * c.N + k]) {
-      float u = pk[5];
-      float nf = 0.29f + 6.01f / (1.0f + expf(-u));
-      n = (double)nf;
-      double eu = exp(-(double)u);
-      dndu = 6.01 * eu / ((1.0 + eu) * (1.0 + eu));
-    } else {
-      n = (double)c.n_frozen[isl * c.N + k];
-    }
-    double a[UPH_MAXGAL], v[UPH_MAXGAL], da[UPH_MAXGAL], dv[UPH_MAXGAL];
-    double core, dcore;
-    sersic_lookup(c, n, a, v, core, da, dv, dcore);
-    for (int g = 0; g < c.tb_k; ++g) {
-      if (a[g] != 0.0 || da[g] != 0.0) {
-        ga[ng] = a[g];
-        gv[ng] = v[g];
-        gda[ng] = da[g];
-        gdv[ng] = dv[g];
-        ++ng;
-      }
-    }
-    if (core != 0.0 || dcore != 0.0) {
-      ga[ng] = core;
-      gv[ng] = 0.0;
-      gda[ng] = dcore;
-      gdv[ng] = 0.0;
-      ++ng;
-    }
-    cov_terms((double)pk[2], (double)pk[3], (double)pk[4], ms.cg, ms.dcov);
-    ms.dndu = (float)dndu;
-  } else {
-    ga[0] = 1.0;
-    gv[0] = 0.0;
-    gda[0] = 0.0;
-    gdv[0] = 0.0;
-    ng = 1;
-  }
-  int nc = 0;
-  const double inv2pi = 0.15915494309189535;
-  for (int q = 0; q < c.kpsf; ++q) {
-    for (int g = 0; g < ng; ++g) {
-      GComp& o = comps[nc++];
-      double A = gv[g] * ms.cg[0] + cq[q][0];
-      double C = gv[g] * ms.cg[1] + cq[q][1];
-      double B = gv[g] * ms.cg[2] + cq[q][2];
-      double det = A * C - B * B;
-      double rs = inv2pi / sqrt(det);
-      o.ia = (float)(C / det);
-      o.ib = (float)(-B / det);
-      o.ic = (float)(A / det);
-      o.A = (float)A;
-      o.B = (float)B;
-      o.C = (float)C;
-      o.det = (float)det;
-      o.nrm = (float)(w[q] * ga[g] * rs);
-      o.nx = (float)(wx[q] * ga[g] * rs);
-      o.ny = (float)(wy[q] * ga[g] * rs);
-      o.nu = (float)(w[q] * gda[g] * rs);
-      o.v = (float)gv[g];
-      o.dv = (float)gdv[g];
-      o.dAx = (float)cx[q][0];
-      o.dCx = (float)cx[q][1];
-      o.dBx = (float)cx[q][2];
-      o.dAy = (float)cy[q][0];
-      o.dCy = (float)cy[q][1];
-      o.dBy = (float)cy[q][2];
+      const double cf = c.mog[(((size_t)b * c.kpsf + q) * 4 + f) * c.nt + t];
+      val[f] += cf * bt;
+      vx[f] += cf * bx;
+      vy[f] += cf * by;
     }
   }
-  ms.ncomp = nc;
+  const double s = val[0], a1 = val[1], a2 = val[2], s2 = s * s;
+  o.cov[0] = s2 * (1 + a1);
+  o.cov[1] = s2 * (1 - a1);
+  o.cov[2] = s2 * a2;
+  o.cx[0] = 2 * s * vx[0] * (1 + a1) + s2 * vx[1];
+  o.cx[1] = 2 * s * vx[0] * (1 - a1) - s2 * vx[1];
+  o.cx[2] = 2 * s * vx[0] * a2 + s2 * vx[2];
+  o.cy[0] = 2 * s * vy[0] * (1 + a1) + s2 * vy[1];
+  o.cy[1] = 2 * s * vy[0] * (1 - a1) - s2 * vy[1];
+  o.cy[2] = 2 * s * vy[0] * a2 + s2 * vy[2];
+  o.w = val[3];
+  o.wx = vx[3];
+  o.wy = vy[3];
 }
 
 __global__ void __launch_bounds__(256)
-k_render(ClassDev c, const float* __restrict__ P, int phase) {
+k_render(ClassDev c, const float* __restrict__ P, int phase, int nsa) {
   extern __shared__ float smem[];
   __shared__ MemberSetup ms;
   __shared__ GComp comps[UPH_MAXKPSF * UPH_MAXGAL];
@@ -328,9 +237,14 @@ k_render(ClassDev c, const float* __restrict__ P, int phase) {
   const bool lin = (phase == PH_LIN);
   const int tid = threadIdx.x;
 
+  __shared__ SetupScratch sc;
+  const float px = P[(size_t)isl * c.nP + 6 * k];
+  const float py = P[(size_t)isl * c.nP + 6 * k + 1];
+  // ---- setup stage 1: box, flags, taps, PSF components, table segment ----
   if (tid == 0) {
     mb = member_box(c, isl, P, k);
     ms.is_gal = c.stype[isl * c.N + k] != 0;
+    ms.support_half = ms.is_gal ? c.T / 2 : c.native / 2;
     const uint8_t* kp = c.keep + ((size_t)isl * c.N + k) * 6;
     int row = 1;
     for (int j = 0; j < 6; ++j) {
@@ -343,30 +257,155 @@ k_render(ClassDev c, const float* __restrict__ P, int phase) {
     ms.need[2] = ms.live_row[1] && c.psf_varies;
     for (int s = 0; s < 3; ++s) ms.need[3 + s] = ms.live_row[2 + s] != 0;
     ms.need[6] = ms.live_row[5] != 0;
-    lanczos_taps((double)mb.dx, ms.Lx, ms.dLx);
-    lanczos_taps((double)mb.dy, ms.Ly, ms.dLy);
-    if (c.mode == 0) {
+    for (int a = 0; a < 3; ++a) {
+      ms.cg[a] = 0.f;
+      for (int q = 0; q < 3; ++q) ms.dcov[a][q] = 0.f;
+    }
+    ms.dndu = 0.f;
+    if (c.mode == 1 && ms.is_gal) {
+      const float* pk = P + (size_t)isl * c.nP + 6 * k;
+      double n;
+      if (c.free_n[isl * c.N + k]) {
+        const float u = pk[5];
+        n = (double)(0.29f + 6.01f / (1.0f + expf(-u)));
+        const double eu = exp(-(double)u);
+        ms.dndu = (float)(6.01 * eu / ((1.0 + eu) * (1.0 + eu)));
+      } else {
+        n = (double)c.n_frozen[isl * c.N + k];
+      }
+      const bool inside = (n > c.tb_nmin) && (n < c.tb_nmax);
+      const double nc = fmin(fmax(n, c.tb_nmin), c.tb_nmax);
+      int lo = 0, hi = c.tb_n;
+      while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (c.tb_knots[mid] <= nc) lo = mid + 1; else hi = mid;
+      }
+      const int seg = max(0, min(lo - 1, c.tb_n - 2));
+      const double n0 = c.tb_knots[seg], n1 = c.tb_knots[seg + 1];
+      sc.seg = seg;
+      sc.t = (n1 > n0) ? (nc - n0) / (n1 - n0) : 0.0;
+      sc.dt = (n1 > n0 && inside) ? 1.0 / (n1 - n0) : 0.0;
+      cov_terms((double)pk[2], (double)pk[3], (double)pk[4], ms.cg, ms.dcov);
+    }
+  } else if (tid == 32) {
+    const float gx = __fsub_rn(px, c.x0b[isl]);
+    lanczos_taps((double)__fsub_rn(gx, rintf(gx)), ms.Lx, ms.dLx);
+  } else if (tid == 64) {
+    const float gy = __fsub_rn(py, c.y0b[isl]);
+    lanczos_taps((double)__fsub_rn(gy, rintf(gy)), ms.Ly, ms.dLy);
+  } else if (tid >= 96 && tid < 96 + UPH_MAXNT && c.mode == 0) {
+    const int tt = tid - 96;
+    if (tt < c.nt) {
       const float* os = c.psf_os + 4 * b;
-      const float x = P[(size_t)isl * c.nP + 6 * k];
-      const float y = P[(size_t)isl * c.nP + 6 * k + 1];
-      const float X = __fdiv_rn(__fsub_rn(x, os[0]), os[1]);
-      const float Y = __fdiv_rn(__fsub_rn(y, os[2]), os[3]);
+      const float X = __fdiv_rn(__fsub_rn(px, os[0]), os[1]);
+      const float Y = __fdiv_rn(__fsub_rn(py, os[2]), os[3]);
       const float ix = __fdiv_rn(1.0f, os[1]);
       const float iy = __fdiv_rn(1.0f, os[3]);
-      for (int tt = 0; tt < c.nt; ++tt) {
-        int m, n;
-        term_mn(tt, m, n);
-        float xm = 1.f, yn = 1.f, xm1 = 1.f, yn1 = 1.f;
-        for (int i = 0; i < m; ++i) xm *= X;
-        for (int i = 0; i < n; ++i) yn *= Y;
-        for (int i = 0; i + 1 < m; ++i) xm1 *= X;
-        for (int i = 0; i + 1 < n; ++i) yn1 *= Y;
-        ms.beta[tt] = xm * yn;
-        ms.betax[tt] = m > 0 ? (float)m * xm1 * yn * ix : 0.f;
-        ms.betay[tt] = n > 0 ? (float)n * xm * yn1 * iy : 0.f;
+      int m, n;
+      term_mn(tt, m, n);
+      float xm = 1.f, yn = 1.f, xm1 = 1.f, yn1 = 1.f;
+      for (int i = 0; i < m; ++i) xm *= X;
+      for (int i = 0; i < n; ++i) yn *= Y;
+      for (int i = 0; i + 1 < m; ++i) xm1 *= X;
+      for (int i = 0; i + 1 < n; ++i) yn1 *= Y;
+      ms.beta[tt] = xm * yn;
+      ms.betax[tt] = m > 0 ? (float)m * xm1 * yn * ix : 0.f;
+      ms.betay[tt] = n > 0 ? (float)n * xm * yn1 * iy : 0.f;
+    }
+  } else if (tid >= 128 && tid < 128 + UPH_MAXKPSF && c.mode == 1) {
+    const int q = tid - 128;
+    if (q < c.kpsf) {
+      const float* os = c.psf_os + 4 * b;
+      const double X = ((double)px - os[0]) / os[1];
+      const double Y = ((double)py - os[2]) / os[3];
+      psf_component(c, b, X, Y, 1.0 / os[1], 1.0 / os[3], q, sc.pq[q]);
+    }
+  }
+  __syncthreads();
+  if (c.mode == 1) {
+    // ---- stage 2: normalised PSF weights, galaxy table components ----
+    if (tid == 0) {
+      double W = 0, Wx = 0, Wy = 0;
+      for (int q = 0; q < c.kpsf; ++q) {
+        W += sc.pq[q].w;
+        Wx += sc.pq[q].wx;
+        Wy += sc.pq[q].wy;
       }
-    } else {
-      setup_analytic(c, b, isl, k, P, ms, comps, lin);
+      sc.W = W;
+      sc.Wx = Wx;
+      sc.Wy = Wy;
+    } else if (tid >= 32 && tid < 32 + UPH_MAXGAL && ms.is_gal) {
+      const int g = tid - 32;
+      const int seg = sc.seg;
+      const double t = sc.t, dt = sc.dt;
+      GalComp& o = sc.gg[g];
+      if (g < c.tb_k) {
+        const double a0 = c.tb_amps[seg * c.tb_k + g], a1 = c.tb_amps[(seg + 1) * c.tb_k + g];
+        const double l0 = c.tb_lv[seg * c.tb_k + g], l1 = c.tb_lv[(seg + 1) * c.tb_k + g];
+        o.a = (1 - t) * a0 + t * a1;
+        o.v = exp((1 - t) * l0 + t * l1);
+        o.da = dt * (a1 - a0);
+        o.dv = o.v * dt * (l1 - l0);
+      } else if (g == c.tb_k) {          // delta core: zero-variance component
+        o.a = (1 - t) * c.tb_core[seg] + t * c.tb_core[seg + 1];
+        o.v = 0.0;
+        o.da = dt * (c.tb_core[seg + 1] - c.tb_core[seg]);
+        o.dv = 0.0;
+      }
+    }
+    __syncthreads();
+    if (tid == 0) {
+      // compact the galaxy components that contribute (non-zero amplitude
+      // or amplitude derivative); a star is a single unit delta
+      int ng = 0;
+      if (ms.is_gal) {
+        for (int g = 0; g <= c.tb_k; ++g)
+          if (sc.gg[g].a != 0.0 || sc.gg[g].da != 0.0) sc.gg[ng++] = sc.gg[g];
+      } else {
+        sc.gg[0].a = 1.0;
+        sc.gg[0].v = 0.0;
+        sc.gg[0].da = 0.0;
+        sc.gg[0].dv = 0.0;
+        ng = 1;
+      }
+      sc.ng = ng;
+      ms.ncomp = c.kpsf * ng;
+    }
+    __syncthreads();
+    // ---- stage 3: combined Gaussian components (covariances add) ----
+    for (int e = tid; e < ms.ncomp; e += blockDim.x) {
+      const int q = e / sc.ng, g = e - (e / sc.ng) * sc.ng;
+      const PsfComp& pq = sc.pq[q];
+      const GalComp& gq = sc.gg[g];
+      const double W = sc.W;
+      const double wn = pq.w / W;
+      const double wnx = (pq.wx * W - pq.w * sc.Wx) / (W * W);
+      const double wny = (pq.wy * W - pq.w * sc.Wy) / (W * W);
+      const double A = gq.v * ms.cg[0] + pq.cov[0];
+      const double C = gq.v * ms.cg[1] + pq.cov[1];
+      const double Bc = gq.v * ms.cg[2] + pq.cov[2];
+      const double det = A * C - Bc * Bc;
+      const double rs = 0.15915494309189535 / sqrt(det);
+      GComp& o = comps[e];
+      o.ia = (float)(C / det);
+      o.ib = (float)(-Bc / det);
+      o.ic = (float)(A / det);
+      o.A = (float)A;
+      o.B = (float)Bc;
+      o.C = (float)C;
+      o.det = (float)det;
+      o.nrm = (float)(wn * gq.a * rs);
+      o.nx = (float)(wnx * gq.a * rs);
+      o.ny = (float)(wny * gq.a * rs);
+      o.nu = (float)(wn * gq.da * rs);
+      o.v = (float)gq.v;
+      o.dv = (float)gq.dv;
+      o.dAx = (float)pq.cx[0];
+      o.dCx = (float)pq.cx[1];
+      o.dBx = (float)pq.cx[2];
+      o.dAy = (float)pq.cy[0];
+      o.dCy = (float)pq.cy[1];
+      o.dBy = (float)pq.cy[2];
     }
   }
   __syncthreads();
@@ -379,15 +418,53 @@ k_render(ClassDev c, const float* __restrict__ P, int phase) {
   const int si0 = oy0 - mb.iyt, sj0 = ox0 - mb.ixt;  // stamp coords of tile
   const int hr = oh + 6, hc = ow + 6;
   float* S = smem;                           // NS * UPH_HALO * HP
-  float* X = smem + NS * UPH_HALO * HP;      // NS * UPH_HALO * XP
+  float* X = smem + nsa * UPH_HALO * HP;     // nsa * UPH_HALO * XP
   const int T = c.T, c0 = c.T / 2;
+  const int hs = ms.support_half;
+  // halo rectangle intersected with the support box (offsets from centre)
+  const int ylo = max(si0 - 3, max(0, c0 - hs)) - c0;
+  const int yhi = min(si0 + oh + 2, min(T - 1, c0 + hs)) - c0;
+  const int xlo = max(sj0 - 3, max(0, c0 - hs)) - c0;
+  const int xhi = min(sj0 + ow + 2, min(T - 1, c0 + hs)) - c0;
+  bool empty = (ylo > yhi) || (xlo > xhi);
+  if (!empty && c.mode == 1) {
+    if (tid == 0) ms.nact = 0;
+    __syncthreads();
+    for (int q = tid; q < ms.ncomp; q += blockDim.x) {
+      const GComp& o = comps[q];
+      ms.act[q] = qmin_box(o.ia, o.ib, o.ic, (float)xlo, (float)xhi, (float)ylo,
+                           (float)yhi) <= QCUT;
+    }
+    __syncthreads();
+    if (tid == 0) {
+      int na = 0;
+      for (int q = 0; q < ms.ncomp; ++q)
+        if (ms.act[q]) ms.act[na++] = (uint8_t)q;
+      ms.nact = na;
+    }
+    __syncthreads();
+    empty = (ms.nact == 0);
+  }
+  if (empty) {
+    // every value on this tile is zero: write the zeros and stop
+    for (int e = tid; e < oh * ow; e += blockDim.x) {
+      const int rr = e / ow, cc = e % ow;
+      const size_t off = (size_t)(oy0 + rr - mb.wy0) * c.Sz + (ox0 + cc - mb.wx0);
+      c.stamps[stamp_slot(c, isl, b, k, 0) + off] = 0.f;
+      if (lin)
+        for (int j = 0; j < 6; ++j)
+          if (ms.live_row[j]) c.stamps[stamp_slot(c, isl, b, k, ms.live_row[j]) + off] = 0.f;
+    }
+    return;
+  }
 
   // ---- un-shifted stamp (and partials) on the halo region ----
   for (int e = tid; e < hr * hc; e += blockDim.x) {
     const int r = e / hc, cc = e % hc;
     const int si = si0 - 3 + r, sj = sj0 - 3 + cc;
     float v[NS] = {0, 0, 0, 0, 0, 0, 0};
-    if (si >= 0 && si < T && sj >= 0 && sj < T) {
+    if (si >= 0 && si < T && sj >= 0 && sj < T && abs(si - c0) <= hs &&
+        abs(sj - c0) <= hs) {
       if (c.mode == 0) {
         const float* cf = c.psf_coefs + (((size_t)b * T + si) * T + sj) * c.nt;
         float s0 = 0.f, sx = 0.f, sy = 0.f;
@@ -404,8 +481,8 @@ k_render(ClassDev c, const float* __restrict__ P, int phase) {
         const float xo = (float)(sj - c0), yo = (float)(si - c0);
         float s0 = 0.f, sx = 0.f, sy = 0.f, gA = 0.f, gB = 0.f, gC = 0.f,
               u1 = 0.f, u2 = 0.f;
-        for (int q = 0; q < ms.ncomp; ++q) {
-          const GComp& o = comps[q];
+        for (int a = 0; a < ms.nact; ++a) {
+          const GComp& o = comps[ms.act[a]];
           const float Q = fmaf(o.ia * xo, xo, fmaf(2.f * o.ib * xo, yo, o.ic * yo * yo));
           const float ex = expf(-0.5f * Q);
           const float nw = o.nrm * ex;
@@ -515,11 +592,20 @@ size_t render_smem_bytes() {
   return sizeof(float) * (size_t)NS * UPH_HALO * (HP + XP);
 }
 
+// Shared arrays a launch needs: every S/X slot index used by the phase is
+// below this count (trial renders use S only; star classes S, Sx, Sy).
+static int render_arrays(const ClassDev& c, int phase) {
+  if (phase != PH_LIN) return 1;
+  return c.has_gal ? NS : 3;
+}
+
 void launch_render(const ClassDev& c, const float* P, int phase,
                    cudaStream_t s) {
   const long long nblk = (long long)c.n_isl * c.nb * c.N * c.ntile_side * c.ntile_side;
   if (nblk <= 0) return;
-  k_render<<<(unsigned)nblk, 256, render_smem_bytes(), s>>>(c, P, phase);
+  const int nsa = render_arrays(c, phase);
+  const size_t bytes = sizeof(float) * (size_t)nsa * UPH_HALO * (HP + XP);
+  k_render<<<(unsigned)nblk, 256, bytes, s>>>(c, P, phase, nsa);
 }
 
 int uph_render_setup() {

@@ -156,7 +156,8 @@ def make_class_kernels(plan, n_bands: int, n_terms: int, *, render_backend: str,
                        stall_count_mode: str = "proposals", step_mode: str = "clip",
                        scene_subtract: bool = False, crossband: dict | None = None,
                        convergence: str = "legacy", plateau_dlnp_tol: float = 0.5,
-                       render_mode: str = "reference") -> ClassKernels:
+                       render_mode: str = "reference",
+                       native_stamp: int = 0) -> ClassKernels:
     if stall_count_mode not in ("proposals", "changed"):
         raise ValueError(f"stall_count_mode must be 'proposals' or 'changed', "
                          f"got {stall_count_mode!r}")
@@ -198,7 +199,7 @@ def make_class_kernels(plan, n_bands: int, n_terms: int, *, render_backend: str,
         render_mode=_lib.RENDER_MODES[render_mode], reg=float(reg),
         pos_step_max=float(pos_step_max_pix), chi2_ftol_rel=float(chi2_ftol_rel),
         step_tol_pix=float(step_tol_pix), un_freeze_steps=int(un_freeze_steps),
-        has_priors=int(bool(has_priors)))
+        has_priors=int(bool(has_priors)), native_stamp=int(native_stamp))
     return ClassKernels(desc, render_mode, int(n_bands), str(plan.kind))
 
 
@@ -441,7 +442,8 @@ class IslandFitJob:
                 star_render_split=star_render_split,
                 has_priors=bool(host["has_priors"]),
                 stall_count_mode=stall_count_mode, convergence=convergence,
-                plateau_dlnp_tol=plateau_dlnp_tol, render_mode=render_mode)
+                plateau_dlnp_tol=plateau_dlnp_tol, render_mode=render_mode,
+                native_stamp=fp.native)
             chunk = _chunk_size(plan, n_bands, chunk_budget_bytes)
             ids = []
             for lo in range(0, plan.n_islands, chunk):
