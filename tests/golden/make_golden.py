@@ -119,8 +119,18 @@ def psf_fixture(ref):
 
 
 def table_fixture(ref):
+    """Sampled rows plus SHA-256 digests of the reference table arrays."""
+    import hashlib
     t = ref["sersic_mog"].load_table_np()
-    return {k: np.asarray(t[k]) for k in ("n_knots", "amps", "log_vars", "core_amp")}
+    rows = np.array([0, 43, 148, 348, 600, 748, 1148, 1208])
+    out = {"rows": rows}
+    for k in ("n_knots", "amps", "log_vars", "core_amp"):
+        a = np.ascontiguousarray(np.asarray(t[k], np.float64))
+        out[f"{k}_sha256"] = np.array(hashlib.sha256(a.tobytes()).hexdigest())
+        out[f"{k}_rows"] = a[rows]
+    out["n_min"] = np.asarray(t["n_min"])
+    out["n_max"] = np.asarray(t["n_max"])
+    return out
 
 
 def main(ref_root):

@@ -1,0 +1,56 @@
+"""Host-side API behaviour that needs no GPU: option validation mirrors the
+reference's ValueErrors; unsupported options fail loudly."""
+import numpy as np
+import pytest
+
+from uniphot_b200 import solver
+from uniphot_b200.plan import IslandClassPlan
+
+
+def _plan(kind="star"):
+    return IslandClassPlan(0, 32, 1, kind, 31, np.zeros(1, np.int64),
+                           np.zeros((1, 1), np.int64), np.ones((1, 1), bool),
+                           np.zeros((1, 4), np.int64), np.ones(1, np.int32))
+
+
+KW = dict(render_backend="fft", reg=1e-9, pos_step_max_pix=0.5, chi2_ftol_rel=1e-4,
+          step_tol_pix=0.1, un_freeze_steps=0)
+
+
+@pytest.mark.parametrize("bad", [dict(stall_count_mode="x"), dict(step_mode="x"),
+                                 dict(convergence="x"),
+                                 dict(convergence="dlnp", step_mode="trust_region"),
+                                 dict(convergence="dlnp", stall_count_mode="changed"),
+                                 dict(render_mode="x")])
+def test_invalid_options_raise_valueerror(bad):
+    with pytest.raises(ValueError):
+        solver.make_class_kernels(_plan(), 3, 1, **KW, **bad)
+
+
+@pytest.mark.parametrize("opt", [dict(stall_count_mode="changed"), dict(convergence="dlnp"),
+                                 dict(crossband={"rank": 1}), dict(scene_subtract=True)])
+def test_unbuilt_options_raise(opt):
+    with pytest.raises(ValueError, match="not supported"):
+        solver.make_class_kernels(_plan("mixed"), 3, 1, **KW, **opt)
+
+
+def test_class_descriptor_fields():
+    k = solver.make_class_kernels(_plan(), 3, 1, **KW, native_stamp=31)
+    assert (k.desc.bbox, k.desc.nsrc, k.desc.tier, k.desc.native_stamp) == (32, 1, 31, 31)
+    assert k.desc.render_mode == 0
+
+
+def test_run_class_chunk_rejects_post_convergence_options():
+    k = solver.make_class_kernels(_plan(), 3, 1, **KW)
+    with pytest.raises(ValueError):
+        solver.run_class_chunk(k, None, {}, np.arange(1), 1, 30, None, None, 10,
+                               compute_param_errors=True)
+
+
+def test_psf_tree_padding_keeps_centre():
+    from uniphot_b200.psf import PsfPolynomial
+    c = np.zeros((5, 5, 1), np.float32)
+    c[2, 2, 0] = 1.0
+    tree, nt = solver.build_psf_tree([PsfPolynomial(c, 0, 1, 0, 1, 5, 5)], 9)
+    assert nt == 1 and tree.params.shape == (1, 9, 9, 1)
+    assert tree.params[0, 4, 4, 0] == 1.0 and tree.params.sum() == 1.0

@@ -1,0 +1,124 @@
+"""CUDA path vs the CPU oracle (parity tests proper, through the C ABI).
+
+Bar: identical LM iteration counts and converged/stalled flags; fluxes within
+1e-4 relative or 0.01 sigma; positions within 1e-3 px (SURVEY parity bar).
+"""
+import numpy as np
+import pytest
+
+from _common import compare, field_classes, run_gpu, run_oracle
+
+pytestmark = pytest.mark.gpu
+
+
+def _assert_parity(plans, hosts, g, o, label):
+    for p, h, gg, oo in zip(plans, hosts, g, o):
+        r = compare(gg, oo, h["mmask"])
+        msg = f"{label} {p.key}: {r['max_rel']:.2e} {r['max_dpos']:.2e} " \
+              f"gpu nst {gg['nst'].tolist()} oracle nst {oo['nst'].tolist()}"
+        assert r["same_nst"].all(), msg
+        assert r["same_flags"].all(), msg
+        assert r["flux_ok"].all(), msg
+        assert r["pos_ok"].all(), msg
+        np.testing.assert_array_equal(gg["n_good"], oo["n_good"])
+        st = gg["stall"]
+        np.testing.assert_array_equal(gg["diverged"][st], oo["diverged"][st])
+
+
+@pytest.fixture(scope="module")
+def small():
+    from uniphot_b200.synth import make_small_field
+    return make_small_field(0)
+
+
+@pytest.mark.parametrize("mode,kinds", [("reference", ("star",)),
+                                        ("analytic", ("star", "mixed"))])
+def test_small_field_parity(small, mode, kinds):
+    plans, hosts, PAD, ds, ws, psfs = field_classes(small, mode, kinds)
+    g, _ = run_gpu(plans, hosts, PAD, ds, ws, psfs, mode, native=small.native)
+    o = run_oracle(plans, hosts, PAD, ds, ws, psfs, mode, native=small.native)
+    _assert_parity(plans, hosts, g, o, mode)
+
+
+def test_production_like_field_parity():
+    """Reduced production field (512^2, 3 bands, 300 sources): polynomial
+    Gaussian-mixture PSF, EXP/DEV/SERSIC with free n, tiers 31/63/127."""
+    from uniphot_b200.synth import make_production_field
+    f = make_production_field(3, side=512, n_bands=3, n_src=300)
+    plans, hosts, PAD, ds, ws, psfs = field_classes(f, "analytic")
+    keep = [i for i, p in enumerate(plans) if p.nsrc_class <= 2]
+    plans = [plans[i] for i in keep]
+    hosts = [hosts[i] for i in keep]
+    g, _ = run_gpu(plans, hosts, PAD, ds, ws, psfs, "analytic", native=f.native)
+    o = run_oracle(plans, hosts, PAD, ds, ws, psfs, "analytic", native=f.native,
+                   processes=8)
+    _assert_parity(plans, hosts, g, o, "production")
+
+
+def test_continuation_equals_single_pass(small):
+    """Main pass of 8 steps + a re-queued pass carrying the LM state equals
+    one 30-step pass (island_solver.py:3419-3484)."""
+    from uniphot_b200 import solver
+    plans, hosts, PAD, ds, ws, psfs = field_classes(small, "analytic", ("mixed",))
+    p, h = plans[0], hosts[0]
+    full, fld = run_gpu([p], [h], PAD, ds, ws, psfs, "analytic", native=small.native)
+    a, _ = run_gpu([p], [h], PAD, ds, ws, psfs, "analytic", max_steps=2, field=fld,
+                   native=small.native)
+    a = a[0]
+    tree, nt = solver.build_psf_tree(psfs, p.tier)
+    kern = solver.make_class_kernels(p, ds.shape[0], nt, render_backend="fft",
+                                     reg=1e-9, pos_step_max_pix=0.5,
+                                     chi2_ftol_rel=1e-4, step_tol_pix=0.1,
+                                     un_freeze_steps=0, render_mode="analytic",
+                                     native_stamp=small.native)
+    rows = np.nonzero(~a["conv"])[0]
+    assert rows.size > 0
+    init = {k: a[k][rows] for k in ("p", "lam", "chi2", "consec", "nrej", "nst")}
+    b = solver.run_class_chunk(kern, tree, h, rows, rows.size, 28, fld, fld, PAD,
+                               init_state=init)
+    f = full[0]
+    np.testing.assert_array_equal(b["nst"], f["nst"][rows])
+    np.testing.assert_array_equal(b["p"], f["p"][rows])
+    np.testing.assert_array_equal(b["fluxes"], f["fluxes"][rows])
+
+
+def test_solve_is_deterministic(small):
+    plans, hosts, PAD, ds, ws, psfs = field_classes(small, "analytic")
+    g1, fld = run_gpu(plans, hosts, PAD, ds, ws, psfs, "analytic", native=small.native)
+    g2, _ = run_gpu(plans, hosts, PAD, ds, ws, psfs, "analytic", field=fld,
+                    native=small.native)
+    for a, b in zip(g1, g2):
+        for k in ("p", "fluxes", "ferr", "chi2", "nst"):
+            np.testing.assert_array_equal(a[k], b[k])
+
+
+def test_island_fit_end_to_end(small):
+    from uniphot_b200.solver import island_fit
+    res = island_fit(**small.fit_kwargs("analytic"))
+    n = small.pos_x.size
+    assert sorted(res.source_idx.tolist()) == list(range(n))
+    assert res.fluxes.shape == (n, 3)
+    assert np.all(np.isfinite(res.fluxes)) and res.converged.all()
+    order = np.argsort(res.source_idx)
+    rel = np.abs(res.fluxes[order] / small.true_flux - 1)
+    assert np.median(rel) < 0.05
+    assert len(res.bucket_stats) >= 2
+
+
+def test_zero_weight_island_stalls_like_oracle(small):
+    plans, hosts, PAD, ds, ws, psfs = field_classes(small, "analytic", ("star",))
+    p, h = plans[0], hosts[0]
+    ws2 = ws.copy()
+    oy, ox = int(h["oy"][0]), int(h["ox"][0])
+    ws2[:, oy:oy + p.bbox_class, ox:ox + p.bbox_class] = 0.0
+    g, _ = run_gpu([p], [h], PAD, ds, ws2, psfs, "analytic", native=small.native)
+    o = run_oracle([p], [h], PAD, ds, ws2, psfs, "analytic", native=small.native)
+    assert g[0]["stall"][0] and g[0]["nst"][0] == 4 and g[0]["n_good"][0] == 0
+    _assert_parity([p], [h], g, o, "zero-weight")
+
+
+def test_reference_mode_galaxy_is_rejected(small):
+    plans, hosts, PAD, ds, ws, psfs = field_classes(small, "reference", ("mixed",))
+    with pytest.raises(ValueError):
+        run_gpu(plans[:1], hosts[:1], PAD, ds, ws, psfs, "reference",
+                native=small.native)

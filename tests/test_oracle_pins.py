@@ -1,0 +1,200 @@
+"""Pins of the CPU oracle: the reference's numpy PSF evaluation, the Sersic
+table, Lanczos taps, ellipse covariance and the VarPro Jacobian (finite
+differences), plus known-answer fits."""
+import hashlib
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from oracle import island_oracle as O
+from uniphot_b200.sersic import load_table
+
+GOLD = Path(__file__).resolve().parent / "golden"
+ROOT = Path(__file__).resolve().parents[1]
+TABLE = ROOT / "uniphot_b200" / "data" / "sersic_mog_table.npz"
+
+
+@pytest.mark.parametrize("nt", [1, 3, 6, 10, 15])
+def test_poly_psf_matches_reference_numpy_eval(nt):
+    z = np.load(GOLD / "psf_poly_eval.npz")
+    coefs, xy, stamps = z[f"nt{nt}_coefs"], z[f"nt{nt}_xy"], z[f"nt{nt}_stamps"]
+    psf = O.PolyPsfBand(coefs, 1000.0, 900.0, 700.0, 650.0)
+    for (x, y), ref in zip(xy, stamps):
+        S, _, _, _ = psf.stamp(x, y, np.float64)
+        np.testing.assert_allclose(S, ref, rtol=2e-5, atol=2e-5 * np.abs(ref).max())
+
+
+def test_sersic_table_identical_to_reference():
+    z = np.load(GOLD / "sersic_table_ref.npz")
+    t = load_table()
+    for k in ("n_knots", "amps", "log_vars", "core_amp"):
+        a = np.ascontiguousarray(np.asarray(t[k], np.float64))
+        assert hashlib.sha256(a.tobytes()).hexdigest() == str(z[f"{k}_sha256"])
+        np.testing.assert_array_equal(a[z["rows"]], z[f"{k}_rows"])
+    assert float(t["n_min"]) == float(z["n_min"]) and float(t["n_max"]) == float(z["n_max"])
+
+
+def test_table_lookup_at_knots_returns_stored_rows():
+    tb = O.SersicTable.load(TABLE)
+    for i in (10, 148, 600, 1100):
+        n = tb.n_knots[i]
+        if tb.n_knots[i + 1] == n:       # duplicated boundary knot
+            continue
+        a, v, core, *_ = tb.lookup(n)
+        j = int(np.searchsorted(tb.n_knots, n, side="right")) - 1
+        np.testing.assert_allclose(a, tb.amps[j], rtol=1e-12)
+        np.testing.assert_allclose(v, np.exp(tb.log_vars[j]), rtol=1e-12)
+
+
+def test_lanczos_zero_shift_is_identity():
+    L, dL = O.lanczos3_taps(0.0)
+    np.testing.assert_allclose(L, [0, 0, 0, 1, 0, 0, 0], atol=1e-15)
+    img = np.random.default_rng(0).normal(size=(9, 11))
+    np.testing.assert_allclose(O.correlate_y(O.correlate_x(img, L), L), img, atol=1e-14)
+
+
+@pytest.mark.parametrize("d", [-0.49, -0.2, 0.13, 0.37])
+def test_lanczos_taps_normalised_and_derivative(d):
+    L, dL = O.lanczos3_taps(d)
+    assert abs(L.sum() - 1.0) < 1e-14 and abs(dL.sum()) < 1e-12
+    h = 1e-6
+    num = (O.lanczos3_taps(d + h)[0] - O.lanczos3_taps(d - h)[0]) / (2 * h)
+    np.testing.assert_allclose(dL, num, atol=1e-7)
+
+
+@pytest.mark.parametrize("p", [(0.3, 0.2, -0.1), (1.2, -0.5, 0.4), (-0.7, 1e-3, 2.0)])
+def test_cov_terms_derivative(p):
+    c, dc = O.cov_terms(*p)
+    h = 1e-6
+    for s in range(3):
+        q1 = list(p)
+        q2 = list(p)
+        q1[s] += h
+        q2[s] -= h
+        num = (O.cov_terms(*q1)[0] - O.cov_terms(*q2)[0]) / (2 * h)
+        np.testing.assert_allclose(dc[s], num, rtol=1e-5, atol=1e-8)
+
+
+def test_cov_terms_round_source_nudge():
+    """ee1 = ee2 = 0 is evaluated at ee1 = 1e-4 with a zero ee1 derivative
+    (sersic_mog.py:135-136): finite, and identical to the nudged point."""
+    c0, dc0 = O.cov_terms(0.5, 0.0, 0.0)
+    c1, _ = O.cov_terms(0.5, 1e-4, 0.0)
+    np.testing.assert_array_equal(c0, c1)
+    np.testing.assert_array_equal(dc0[1], 0.0)
+    assert np.all(np.isfinite(dc0))
+
+
+def _mini_island(mode, n_src=2, seed=0, gal=True, B=32, T=31, nb=2, noise=True):
+    """A small synthetic island for known-answer and Jacobian tests."""
+    from uniphot_b200.psf import MogPsf, rasterize_mog_psf
+    rng = np.random.default_rng(seed)
+    mog = MogPsf(np.array([[1.3, 0.05, 0.0], [2.4, 0.0, 0.1]]),
+                 np.array([[0.05, 0.01, 0.0], [-0.02, 0.0, 0.01]]),
+                 np.array([[0.02, 0.0, 0.0], [0.0, 0.01, 0.0]]),
+                 np.array([[0.8, 0.0, 0.0], [0.2, 0.0, 0.0]]), 100.0, 100.0, 100.0, 100.0)
+    if mode == "analytic":
+        psf = [O.MogPsfBand(mog.sigma, mog.e1, mog.e2, mog.weight, 100.0, 100.0,
+                            100.0, 100.0) for _ in range(nb)]
+    else:
+        p = rasterize_mog_psf(mog, T, 100.0, 100.0)
+        psf = [O.PolyPsfBand(p.coefs, 100.0, 100.0, 100.0, 100.0) for _ in range(nb)]
+    N = n_src
+    x0 = y0 = 84.0
+    xs = x0 + B / 2 + rng.uniform(-4, 4, N)
+    ys = y0 + B / 2 + rng.uniform(-4, 4, N)
+    stype = np.zeros(N, np.int32)
+    if gal and mode == "analytic":
+        stype[-1] = 3
+    keep = np.zeros((N, 6), bool)
+    keep[:, :2] = True
+    keep[stype != 0, 2:5] = True
+    keep[stype == 3, 5] = True
+    p0 = np.zeros((N, 6), np.float32)
+    p0[:, 0], p0[:, 1] = xs, ys
+    p0[:, 2] = 0.6
+    p0[:, 3], p0[:, 4] = 0.2, -0.1
+    p0[:, 5] = -0.5
+    isl = O.IslandInput(
+        B=B, T=T, data=np.zeros((nb, B, B), np.float32),
+        w=np.full((nb, B, B), 0.01, np.float32), x0=x0, y0=y0, stype=stype,
+        n_frozen=np.ones(N, np.float32), free_n=(stype == 3), mmask=np.ones(N, bool),
+        keep=keep, p0=p0.reshape(-1), lower=(p0 - 5).reshape(-1),
+        upper=(p0 + 5).reshape(-1), prior_mean=p0.reshape(-1),
+        prior_inv_sigma=np.zeros(6 * N, np.float32), has_priors=False, psf=psf,
+        table=O.SersicTable.load(TABLE), mode=mode, native=T)
+    cfg = O.SolverConfig(precision="f64")
+    s = O.IslandSolver(isl, cfg)
+    flux = rng.uniform(2e3, 2e4, (nb, N))
+    for b in range(nb):
+        M, _ = s.models_band(b, isl.p0.astype(np.float64), False)
+        isl.data[b] = np.tensordot(flux[b], M, axes=(0, 0)).astype(np.float32)
+        if noise:
+            isl.data[b] += rng.normal(0, 10.0, (B, B)).astype(np.float32)
+    return isl, flux
+
+
+@pytest.mark.parametrize("mode", ["reference", "analytic"])
+def test_noise_free_fit_recovers_truth(mode):
+    isl, flux = _mini_island(mode, n_src=2, noise=False)
+    truth = isl.p0.copy()
+    isl.p0 = truth + np.tile(np.array([0.2, -0.15, 0, 0, 0, 0], np.float32), 2)
+    out = O.solve_island(isl, O.SolverConfig(precision="f64"), max_steps=30)
+    np.testing.assert_allclose(out["p"].reshape(-1)[[0, 1, 6, 7]],
+                               truth[[0, 1, 6, 7]], atol=2e-3)
+    np.testing.assert_allclose(out["fluxes"], flux, rtol=2e-3)
+
+
+@pytest.mark.parametrize("mode", ["reference", "analytic"])
+def test_varpro_jacobian_matches_finite_differences(mode):
+    isl, _ = _mini_island(mode, n_src=2)
+    s = O.IslandSolver(isl, O.SolverConfig(precision="f64"))
+    p = isl.p0.astype(np.float64)
+
+    def resid(q, b):
+        M, _ = s.models_band(b, q, False)
+        f, _, _ = s.fluxes_band(M, isl.data[b], isl.w[b])
+        _, r = s.chi2_band(M, isl.data[b], isl.w[b], f)
+        return r.reshape(-1)
+    live = [j for j in range(p.size) if isl.keep.reshape(-1)[j]]
+    H, g = s.hg(p)
+    Jn = []
+    for j in live:
+        h = 1e-5 if (j % 6) < 2 else 1e-5
+        q1, q2 = p.copy(), p.copy()
+        q1[j] += h
+        q2[j] -= h
+        Jn.append(np.concatenate([(resid(q1, b) - resid(q2, b)) / (2 * h)
+                                  for b in range(isl.data.shape[0])]))
+    Jn = np.array(Jn)
+    r = np.concatenate([resid(p, b) for b in range(isl.data.shape[0])])
+    Hn = Jn @ Jn.T
+    gn = Jn @ r
+    idx = np.array(live)
+    np.testing.assert_allclose(H[np.ix_(idx, idx)], Hn, rtol=2e-4,
+                               atol=2e-4 * np.abs(Hn).max())
+    np.testing.assert_allclose(g[idx], gn, rtol=2e-3, atol=2e-4 * np.abs(gn).max())
+
+
+def test_two_source_blend_flux_solve_is_normal_equations():
+    isl, flux = _mini_island("analytic", n_src=2, gal=False, noise=False)
+    s = O.IslandSolver(isl, O.SolverConfig(precision="f64"))
+    M, _ = s.models_band(0, isl.p0.astype(np.float64), False)
+    f, f64, A64 = s.fluxes_band(M, isl.data[0], isl.w[0])
+    Mm = M.reshape(2, -1).astype(np.float64)
+    w = isl.w[0].reshape(-1).astype(np.float64)
+    A = (Mm * w) @ Mm.T + 1e-9 * np.eye(2)
+    b = (Mm * w) @ isl.data[0].reshape(-1).astype(np.float64)
+    np.testing.assert_allclose(f64, np.linalg.solve(A, b), rtol=1e-10)
+    np.testing.assert_allclose(f64, flux[0], rtol=1e-5)
+
+
+def test_stall_sets_probes():
+    """A zero-weight island never improves: 4 rejects -> stalled, and the
+    frozen proposals are identical (diverged)."""
+    isl, _ = _mini_island("analytic", n_src=1, gal=False, noise=False)
+    isl.w[:] = 0.0
+    out = O.solve_island(isl, O.SolverConfig(precision="ref"), max_steps=30)
+    assert out["stall"] and out["conv"] and out["nst"] == 4
+    assert np.isfinite(out["stall_dchi2"])
