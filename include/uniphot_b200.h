@@ -181,6 +181,47 @@ int uph_job_set_profile(uph_job* job, int32_t on);
 int uph_job_kernel_time(const uph_job* job, int32_t kind, float* ms,
                         int64_t* launches);
 
+/* ---- Allocation-free final-flux pass.  No counterpart in the reference:
+ * it exists for callers that cannot call cudaMalloc (a host inside a
+ * framework that owns the device memory pool, or a serving process that
+ * must not allocate after start-up).  Every buffer is a caller-owned DEVICE
+ * pointer; the intermediates live in one fixed device array of
+ * UPH_NOALLOC_SCRATCH_BYTES inside the library (held by every GPU that
+ * loads it, until exit).  Star members, reference render mode: renders each
+ * member at parameters p, solves the per-band VarPro fluxes and returns
+ * fluxes, sqrt(diag inv A64) and the island chi2 -- the same numbers as
+ * uph_run_chunk with max_steps = 0.  Real members must occupy the first
+ * slots of each island.  Calls share the array: calls that overlap on the
+ * GPU race and must be serialised by the caller.  The first call on a
+ * device does a one-time set-up (symbol address, kernel limits) and should
+ * come before any stream capture.  Work that does not fit the array is
+ * rejected with UPH_ERR_INVALID and a message in err_buf; the call never
+ * allocates and does not synchronise (results are ready when `stream`
+ * is). */
+#define UPH_NOALLOC_SCRATCH_BYTES (32u << 20)
+typedef struct uph_noalloc_args {
+  const float* data;             /* (n_bands, Hp, Wp) padded field, data - bg */
+  const float* invvar;           /* (n_bands, Hp, Wp)                       */
+  const float* psf_coefs;        /* (n_bands, tier, tier, nt)               */
+  const float* psf_origin_scale; /* (n_bands, 4)                            */
+  const int32_t* ox;             /* [n] window origins in the padded field  */
+  const int32_t* oy;             /* [n]                                     */
+  const float* x0b;              /* [n] window origins in field coords      */
+  const float* y0b;              /* [n]                                     */
+  const int32_t* stype;          /* [n*N] all SOURCE_STAR (0)               */
+  const uint8_t* mmask;          /* [n*N]                                   */
+  const float* p;                /* [n*N*6] parameters (x, y used)          */
+  float* fluxes;                 /* [n*n_bands*N] out                       */
+  float* ferr;                   /* [n*n_bands*N] out                       */
+  float* chi2;                   /* [n] out                                 */
+  int32_t n_islands, nsrc, bbox, tier, native_stamp, n_bands, Hp, Wp, nt;
+  float reg;                     /* ridge on real members (1e-9)            */
+  void* stream;                  /* cudaStream_t (NULL = legacy default)    */
+  char* err_buf;                 /* optional message buffer                 */
+  int32_t err_len;
+} uph_noalloc_args;
+int uph_fluxes_noalloc(const uph_noalloc_args* args);
+
 #ifdef __cplusplus
 }
 #endif

@@ -311,3 +311,49 @@ class Job:
             self.close()
         except Exception:  # noqa: BLE001
             pass
+
+
+# ---------------------------------------------------------------------------
+# Allocation-free final-flux pass (uph_fluxes_noalloc): for callers that own
+# all device memory and cannot allocate (see include/uniphot_b200.h).
+# ---------------------------------------------------------------------------
+
+class NoallocArgs(C.Structure):
+    _fields_ = [(n, _P) for n in (
+        "data", "invvar", "psf_coefs", "psf_origin_scale", "ox", "oy", "x0b",
+        "y0b", "stype", "mmask", "p", "fluxes", "ferr", "chi2")] + \
+        [(n, C.c_int32) for n in ("n_islands", "nsrc", "bbox", "tier",
+                                  "native_stamp", "n_bands", "Hp", "Wp", "nt")] + \
+        [("reg", C.c_float), ("stream", _P), ("err_buf", C.c_char_p),
+         ("err_len", C.c_int32)]
+
+
+NOALLOC_SCRATCH_BYTES = 32 << 20
+
+
+def fluxes_noalloc(ptrs: dict, *, n_islands: int, nsrc: int, bbox: int, tier: int,
+                   native_stamp: int, n_bands: int, Hp: int, Wp: int, nt: int,
+                   reg: float = 1e-9, stream: int = 0) -> None:
+    """Call uph_fluxes_noalloc with caller-owned device pointers
+    (``ptrs[name]`` = integer device address for every pointer field)."""
+    L = lib()
+    fn = L.uph_fluxes_noalloc
+    fn.argtypes = [C.POINTER(NoallocArgs)]
+    fn.restype = C.c_int
+    err = C.create_string_buffer(256)
+    a = NoallocArgs()
+    for name, _t in NoallocArgs._fields_[:14]:
+        setattr(a, name, _P(int(ptrs[name])))
+    a.n_islands, a.nsrc, a.bbox, a.tier = int(n_islands), int(nsrc), int(bbox), int(tier)
+    a.native_stamp, a.n_bands, a.Hp, a.Wp, a.nt = (int(native_stamp), int(n_bands),
+                                                   int(Hp), int(Wp), int(nt))
+    a.reg = float(reg)
+    a.stream = _P(int(stream)) if stream else None
+    a.err_buf = C.cast(err, C.c_char_p)
+    a.err_len = 256
+    rc = fn(C.byref(a))
+    if rc != UPH_OK:
+        msg = err.value.decode(errors="replace")
+        if rc == UPH_ERR_INVALID:
+            raise ValueError(msg)
+        raise UphError(f"uph_fluxes_noalloc: status {rc}: {msg}")
