@@ -371,7 +371,7 @@ struct Launcher {
   cudaStream_t s;
   std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>>* rec;
   template <class F>
-  void operator()(int kind, F&& fn) {
+  void operator()(int kind, F&& fn, int kernels = 1) {
     if (rec) {
       cudaEvent_t a, b;
       cudaEventCreate(&a);
@@ -383,17 +383,17 @@ struct Launcher {
     } else {
       fn();
     }
-    job->ctx->launches += 1;
+    job->ctx->launches += kernels;
   }
 };
 
 void iteration(const ClassDev& c, Launcher& L) {
   cudaStream_t s = L.s;
-  L(0, [&] { launch_render(c, c.p, PH_LIN, s); });
+  L(0, [&] { launch_render(c, c.p, PH_LIN, s); }, 2);
   L(1, [&] { launch_gram_lin(c, s); });
   L(2, [&] { launch_assemble(c, s); });
   L(3, [&] { launch_step(c, PH_TRIAL, 0, 0.f, 0, s); });
-  L(0, [&] { launch_render(c, c.p_try, PH_TRIAL, s); });
+  L(0, [&] { launch_render(c, c.p_try, PH_TRIAL, s); }, 2);
   L(4, [&] { launch_gram_trial(c, c.p_try, PH_TRIAL, 0, s); });
   L(5, [&] { launch_accept(c, PH_TRIAL, s); });
 }
@@ -554,6 +554,7 @@ int add_chunk(uph_ctx* ctx, Chunk* ch, const uph_class_desc* cls,
   c.nst = cbuf<int>(ctx, ch, "nst", n, &rc);
   c.flags = cbuf<uint8_t>(ctx, ch, "flags", n, &rc);
   c.stamps = cbuf<float>(ctx, ch, "stamps", (size_t)n * nb * N * R * Sz * Sz, &rc);
+  c.mrec = cbuf<MemberRecord>(ctx, ch, "mrec", (size_t)n * nb * N, &rc);
   c.gram = cbuf<float>(ctx, ch, "gram", (size_t)n * nb * Kmax * Kmax, &rc);
   c.Hb = cbuf<float>(ctx, ch, "Hb", (size_t)n * nb * nLmax * nLmax, &rc);
   c.gb = cbuf<float>(ctx, ch, "gb", (size_t)n * nb * nLmax, &rc);
@@ -650,11 +651,11 @@ void post_loop(Chunk* ch, Launcher& L) {
   for (int e = -9; e <= 6; ++e) {
     const float lamj = (float)std::pow(10.0, (double)e);
     L(3, [&] { launch_step(c, PH_PROBE, 0, lamj, 2, s); });
-    L(0, [&] { launch_render(c, c.p_try, PH_PROBE, s); });
+    L(0, [&] { launch_render(c, c.p_try, PH_PROBE, s); }, 2);
     L(4, [&] { launch_gram_trial(c, c.p_try, PH_PROBE, 0, s); });
     L(5, [&] { launch_accept(c, PH_PROBE, s); });
   }
-  L(0, [&] { launch_render(c, c.p, PH_ALL, s); });
+  L(0, [&] { launch_render(c, c.p, PH_ALL, s); }, 2);
   L(4, [&] { launch_gram_trial(c, c.p, PH_ALL, 1, s); });
 }
 
@@ -690,7 +691,7 @@ int job_solve(uph_job* job, int max_steps) {
     if (rc) return rc;
     Launcher L{job, s, recp};
     if (ch->fresh) {
-      L(0, [&] { launch_render(ch->c, ch->c.p, PH_ALL, s); });
+      L(0, [&] { launch_render(ch->c, ch->c.p, PH_ALL, s); }, 2);
       L(4, [&] { launch_gram_trial(ch->c, ch->c.p, PH_ALL, 0, s); });
       L(5, [&] { launch_accept(ch->c, PH_ALL, s); });
     }
@@ -698,7 +699,7 @@ int job_solve(uph_job* job, int max_steps) {
       Launcher Lc{job, s, nullptr};
       CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "capture");
       iteration(ch->c, Lc);
-      ctx->launches -= 7;
+      ctx->launches -= 9;
       cudaError_t ce = cudaStreamEndCapture(s, &ch->graph);
       if (ce != cudaSuccess) return cuda_err(ctx, ce, "end capture");
       CK(cudaGraphInstantiate(&ch->gexec, ch->graph, 0), "graph instantiate");
@@ -722,7 +723,7 @@ int job_solve(uph_job* job, int max_steps) {
           iteration(ch->c, L);
         } else {
           CK(cudaGraphLaunch(ch->gexec, s), "graph launch");
-          ctx->launches += 7;
+          ctx->launches += 9;
         }
       }
       ch->iters += group;

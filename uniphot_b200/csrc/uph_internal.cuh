@@ -36,6 +36,29 @@
 #define PH_PROBE 2    // post-hoc probes of stalled islands
 #define PH_ALL 3      // every island (initial chi2, final fluxes)
 
+// One Gaussian term of an analytic member stamp: PSF component q convolved
+// with galaxy component g (covariances add), with what the derivative
+// stamps need.
+struct GComp {
+  float ia, ib, ic;          // inverse covariance
+  float A, B, C, det;        // covariance xx, xy, yy; det holds 0.5/det
+  float nrm, nx, ny, nu;     // weight * amplitude / (2 pi sqrt det) (+ d/dx, d/dy, d/dn)
+  float v, dv;               // galaxy variance scale and d v / d n
+  float dAx, dBx, dCx, dAy, dBy, dCy;
+};
+
+// Per (island, band, member) render set-up at the current parameters,
+// computed once by k_member_setup and read by every render tile.
+struct MemberRecord {
+  float Lx[7], dLx[7], Ly[7], dLy[7];            // Lanczos taps, d/d shift
+  float beta[UPH_MAXNT], betax[UPH_MAXNT], betay[UPH_MAXNT];  // PSF basis
+  float dcov[3][3];                              // d(cxx,cyy,cxy)/d(lr,e1,e2)
+  float cg[3];                                   // unit galaxy covariance
+  float dndu;
+  int ncomp;
+  GComp comps[UPH_MAXKPSF * UPH_MAXGAL];
+};
+
 struct ClassDev {
   int n_isl, nb, N, nP, B, T, Sz, R, Kmax, nLmax, ntile_side;
   int mode, nt, kpsf, psf_varies;
@@ -81,6 +104,7 @@ struct ClassDev {
   int* nst;
   uint8_t* flags;
   float* stamps;
+  MemberRecord* mrec;      // (n_isl, nb, N)
   float* gram;
   float* Hb;
   float* gb;

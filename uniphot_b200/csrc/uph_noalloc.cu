@@ -10,7 +10,8 @@
 // pass -- render every member at fixed parameters (reference render mode),
 // solve the per-band VarPro fluxes and compute the island chi2 -- using the
 // same kernels as the solver, with every intermediate (stamps, per-band
-// chi2, good-pixel counts, island flags) in the file-scope device array
+// chi2, good-pixel counts, island flags, per-member render set-up records)
+// in the file-scope device array
 // below instead of memory allocated per call.
 //
 // Limits and sharing rules:
@@ -105,6 +106,8 @@ extern "C" int uph_fluxes_noalloc(const uph_noalloc_args* a) {
   off = align256(off + sizeof(int) * (size_t)n * nb);
   const size_t o_stamps = off;
   off = align256(off + sizeof(float) * (size_t)n * nb * N * Sz * Sz);
+  const size_t o_mrec = off;
+  off = align256(off + sizeof(MemberRecord) * (size_t)n * nb * N);
   if (off > (size_t)UPH_NOALLOC_SCRATCH_BYTES) {
     char msg[256];
     std::snprintf(msg, sizeof msg,
@@ -156,6 +159,7 @@ extern "C" int uph_fluxes_noalloc(const uph_noalloc_args* a) {
   c.chi2b = (double*)(base + o_chi2b);
   c.ngood = (int*)(base + o_ngood);
   c.stamps = (float*)(base + o_stamps);
+  c.mrec = (MemberRecord*)(base + o_mrec);
   c.flux = a->fluxes;
   c.ferr = a->ferr;
   c.reg = a->reg;

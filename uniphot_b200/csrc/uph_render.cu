@@ -24,14 +24,6 @@ constexpr int NS = 7;            // S arrays: S, Sx, Sy, Slr, Se1, Se2, Su
 constexpr int HP = UPH_HALO + 1; // padded halo pitch
 constexpr int XP = UPH_TILE + 1;
 
-struct GComp {
-  float ia, ib, ic;          // inverse covariance
-  float A, B, C, det;        // covariance xx, xy, yy
-  float nrm, nx, ny, nu;     // weight * amplitude / (2 pi sqrt det) (+ d/dx, d/dy, d/dn)
-  float v, dv;               // galaxy variance scale and d v / d n
-  float dAx, dBx, dCx, dAy, dBy, dCy;
-};
-
 struct MemberSetup {
   float Lx[7], dLx[7], Ly[7], dLy[7];
   float beta[UPH_MAXNT], betax[UPH_MAXNT], betay[UPH_MAXNT];
@@ -217,6 +209,181 @@ __device__ void psf_component(const ClassDev& c, int b, double X, double Y,
   o.wy = vy[3];
 }
 
+// Per (island, band, member) setup at parameters P: Lanczos taps, PSF basis
+// (reference mode) or the combined Gaussian components (analytic mode),
+// written once to the member record that every render tile of the member
+// reads.
+__global__ void __launch_bounds__(128)
+k_member_setup(ClassDev c, const float* __restrict__ P, int phase) {
+  __shared__ SetupScratch sc;
+  __shared__ int is_gal;
+  __shared__ int ncomp;
+  const int k = blockIdx.x % c.N;
+  const int b = (blockIdx.x / c.N) % c.nb;
+  const int isl = blockIdx.x / (c.N * c.nb);
+  if (isl >= c.n_isl) return;
+  if (!isl_active(c.flags[isl], phase)) return;
+  if (!c.mmask[isl * c.N + k]) return;
+  const int tid = threadIdx.x;
+  MemberRecord* rec = c.mrec + ((size_t)isl * c.nb + b) * c.N + k;
+  const float px = P[(size_t)isl * c.nP + 6 * k];
+  const float py = P[(size_t)isl * c.nP + 6 * k + 1];
+  if (tid == 0) {
+    is_gal = c.stype[isl * c.N + k] != 0;
+    for (int a = 0; a < 3; ++a) {
+      rec->cg[a] = 0.f;
+      for (int q = 0; q < 3; ++q) rec->dcov[a][q] = 0.f;
+    }
+    rec->dndu = 0.f;
+    rec->ncomp = 0;
+    if (c.mode == 1 && is_gal) {
+      const float* pk = P + (size_t)isl * c.nP + 6 * k;
+      double n;
+      if (c.free_n[isl * c.N + k]) {
+        const float u = pk[5];
+        n = (double)(0.29f + 6.01f / (1.0f + expf(-u)));
+        const double eu = exp(-(double)u);
+        rec->dndu = (float)(6.01 * eu / ((1.0 + eu) * (1.0 + eu)));
+      } else {
+        n = (double)c.n_frozen[isl * c.N + k];
+      }
+      const bool inside = (n > c.tb_nmin) && (n < c.tb_nmax);
+      const double nc = fmin(fmax(n, c.tb_nmin), c.tb_nmax);
+      int lo = 0, hi = c.tb_n;
+      while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (c.tb_knots[mid] <= nc) lo = mid + 1; else hi = mid;
+      }
+      const int seg = max(0, min(lo - 1, c.tb_n - 2));
+      const double n0 = c.tb_knots[seg], n1 = c.tb_knots[seg + 1];
+      sc.seg = seg;
+      sc.t = (n1 > n0) ? (nc - n0) / (n1 - n0) : 0.0;
+      sc.dt = (n1 > n0 && inside) ? 1.0 / (n1 - n0) : 0.0;
+      cov_terms((double)pk[2], (double)pk[3], (double)pk[4], rec->cg, rec->dcov);
+    }
+  } else if (tid == 32) {
+    const float gx = __fsub_rn(px, c.x0b[isl]);
+    lanczos_taps((double)__fsub_rn(gx, rintf(gx)), rec->Lx, rec->dLx);
+  } else if (tid == 64) {
+    const float gy = __fsub_rn(py, c.y0b[isl]);
+    lanczos_taps((double)__fsub_rn(gy, rintf(gy)), rec->Ly, rec->dLy);
+  } else if (tid >= 96 && tid < 96 + UPH_MAXNT && c.mode == 0) {
+    const int tt = tid - 96;
+    if (tt < c.nt) {
+      const float* os = c.psf_os + 4 * b;
+      const float X = __fdiv_rn(__fsub_rn(px, os[0]), os[1]);
+      const float Y = __fdiv_rn(__fsub_rn(py, os[2]), os[3]);
+      const float ix = __fdiv_rn(1.0f, os[1]);
+      const float iy = __fdiv_rn(1.0f, os[3]);
+      int m, n;
+      term_mn(tt, m, n);
+      float xm = 1.f, yn = 1.f, xm1 = 1.f, yn1 = 1.f;
+      for (int i = 0; i < m; ++i) xm *= X;
+      for (int i = 0; i < n; ++i) yn *= Y;
+      for (int i = 0; i + 1 < m; ++i) xm1 *= X;
+      for (int i = 0; i + 1 < n; ++i) yn1 *= Y;
+      rec->beta[tt] = xm * yn;
+      rec->betax[tt] = m > 0 ? (float)m * xm1 * yn * ix : 0.f;
+      rec->betay[tt] = n > 0 ? (float)n * xm * yn1 * iy : 0.f;
+    }
+  } else if (tid >= 96 && tid < 96 + UPH_MAXKPSF && c.mode == 1) {
+    const int q = tid - 96;
+    if (q < c.kpsf) {
+      const float* os = c.psf_os + 4 * b;
+      const double X = ((double)px - os[0]) / os[1];
+      const double Y = ((double)py - os[2]) / os[3];
+      psf_component(c, b, X, Y, 1.0 / os[1], 1.0 / os[3], q, sc.pq[q]);
+    }
+  }
+  __syncthreads();
+  if (c.mode != 1) return;
+  if (tid == 0) {
+    double W = 0, Wx = 0, Wy = 0;
+    for (int q = 0; q < c.kpsf; ++q) {
+      W += sc.pq[q].w;
+      Wx += sc.pq[q].wx;
+      Wy += sc.pq[q].wy;
+    }
+    sc.W = W;
+    sc.Wx = Wx;
+    sc.Wy = Wy;
+  } else if (tid >= 32 && tid < 32 + UPH_MAXGAL && is_gal) {
+    const int g = tid - 32;
+    const int seg = sc.seg;
+    const double t = sc.t, dt = sc.dt;
+    GalComp& o = sc.gg[g];
+    if (g < c.tb_k) {
+      const double a0 = c.tb_amps[seg * c.tb_k + g], a1 = c.tb_amps[(seg + 1) * c.tb_k + g];
+      const double l0 = c.tb_lv[seg * c.tb_k + g], l1 = c.tb_lv[(seg + 1) * c.tb_k + g];
+      o.a = (1 - t) * a0 + t * a1;
+      o.v = exp((1 - t) * l0 + t * l1);
+      o.da = dt * (a1 - a0);
+      o.dv = o.v * dt * (l1 - l0);
+    } else if (g == c.tb_k) {          // delta core: zero-variance component
+      o.a = (1 - t) * c.tb_core[seg] + t * c.tb_core[seg + 1];
+      o.v = 0.0;
+      o.da = dt * (c.tb_core[seg + 1] - c.tb_core[seg]);
+      o.dv = 0.0;
+    }
+  }
+  __syncthreads();
+  if (tid == 0) {
+    // compact the galaxy components that contribute (non-zero amplitude or
+    // amplitude derivative); a star is a single unit delta
+    int ng = 0;
+    if (is_gal) {
+      for (int g = 0; g <= c.tb_k; ++g)
+        if (sc.gg[g].a != 0.0 || sc.gg[g].da != 0.0) sc.gg[ng++] = sc.gg[g];
+    } else {
+      sc.gg[0].a = 1.0;
+      sc.gg[0].v = 0.0;
+      sc.gg[0].da = 0.0;
+      sc.gg[0].dv = 0.0;
+      ng = 1;
+    }
+    sc.ng = ng;
+    ncomp = c.kpsf * ng;
+    rec->ncomp = ncomp;
+  }
+  __syncthreads();
+  const float* cg = rec->cg;
+  for (int e = tid; e < ncomp; e += blockDim.x) {
+    const int q = e / sc.ng, g = e - (e / sc.ng) * sc.ng;
+    const PsfComp& pq = sc.pq[q];
+    const GalComp& gq = sc.gg[g];
+    const double W = sc.W;
+    const double wn = pq.w / W;
+    const double wnx = (pq.wx * W - pq.w * sc.Wx) / (W * W);
+    const double wny = (pq.wy * W - pq.w * sc.Wy) / (W * W);
+    const double A = gq.v * cg[0] + pq.cov[0];
+    const double C = gq.v * cg[1] + pq.cov[1];
+    const double Bc = gq.v * cg[2] + pq.cov[2];
+    const double det = A * C - Bc * Bc;
+    const double rs = 0.15915494309189535 / sqrt(det);
+    GComp o;
+    o.ia = (float)(C / det);
+    o.ib = (float)(-Bc / det);
+    o.ic = (float)(A / det);
+    o.A = (float)A;
+    o.B = (float)Bc;
+    o.C = (float)C;
+    o.det = (float)(0.5 / det);
+    o.nrm = (float)(wn * gq.a * rs);
+    o.nx = (float)(wnx * gq.a * rs);
+    o.ny = (float)(wny * gq.a * rs);
+    o.nu = (float)(wn * gq.da * rs);
+    o.v = (float)gq.v;
+    o.dv = (float)gq.dv;
+    o.dAx = (float)pq.cx[0];
+    o.dCx = (float)pq.cx[1];
+    o.dBx = (float)pq.cx[2];
+    o.dAy = (float)pq.cy[0];
+    o.dCy = (float)pq.cy[1];
+    o.dBy = (float)pq.cy[2];
+    rec->comps[e] = o;
+  }
+}
+
 __global__ void __launch_bounds__(256)
 k_render(ClassDev c, const float* __restrict__ P, int phase, int nsa) {
   extern __shared__ float smem[];
@@ -237,10 +404,7 @@ k_render(ClassDev c, const float* __restrict__ P, int phase, int nsa) {
   const bool lin = (phase == PH_LIN);
   const int tid = threadIdx.x;
 
-  __shared__ SetupScratch sc;
-  const float px = P[(size_t)isl * c.nP + 6 * k];
-  const float py = P[(size_t)isl * c.nP + 6 * k + 1];
-  // ---- setup stage 1: box, flags, taps, PSF components, table segment ----
+  const MemberRecord* rec = c.mrec + ((size_t)isl * c.nb + b) * c.N + k;
   if (tid == 0) {
     mb = member_box(c, isl, P, k);
     ms.is_gal = c.stype[isl * c.N + k] != 0;
@@ -257,156 +421,30 @@ k_render(ClassDev c, const float* __restrict__ P, int phase, int nsa) {
     ms.need[2] = ms.live_row[1] && c.psf_varies;
     for (int s = 0; s < 3; ++s) ms.need[3 + s] = ms.live_row[2 + s] != 0;
     ms.need[6] = ms.live_row[5] != 0;
+    ms.ncomp = rec->ncomp;
+    ms.dndu = rec->dndu;
     for (int a = 0; a < 3; ++a) {
-      ms.cg[a] = 0.f;
-      for (int q = 0; q < 3; ++q) ms.dcov[a][q] = 0.f;
-    }
-    ms.dndu = 0.f;
-    if (c.mode == 1 && ms.is_gal) {
-      const float* pk = P + (size_t)isl * c.nP + 6 * k;
-      double n;
-      if (c.free_n[isl * c.N + k]) {
-        const float u = pk[5];
-        n = (double)(0.29f + 6.01f / (1.0f + expf(-u)));
-        const double eu = exp(-(double)u);
-        ms.dndu = (float)(6.01 * eu / ((1.0 + eu) * (1.0 + eu)));
-      } else {
-        n = (double)c.n_frozen[isl * c.N + k];
-      }
-      const bool inside = (n > c.tb_nmin) && (n < c.tb_nmax);
-      const double nc = fmin(fmax(n, c.tb_nmin), c.tb_nmax);
-      int lo = 0, hi = c.tb_n;
-      while (lo < hi) {
-        const int mid = (lo + hi) >> 1;
-        if (c.tb_knots[mid] <= nc) lo = mid + 1; else hi = mid;
-      }
-      const int seg = max(0, min(lo - 1, c.tb_n - 2));
-      const double n0 = c.tb_knots[seg], n1 = c.tb_knots[seg + 1];
-      sc.seg = seg;
-      sc.t = (n1 > n0) ? (nc - n0) / (n1 - n0) : 0.0;
-      sc.dt = (n1 > n0 && inside) ? 1.0 / (n1 - n0) : 0.0;
-      cov_terms((double)pk[2], (double)pk[3], (double)pk[4], ms.cg, ms.dcov);
-    }
-  } else if (tid == 32) {
-    const float gx = __fsub_rn(px, c.x0b[isl]);
-    lanczos_taps((double)__fsub_rn(gx, rintf(gx)), ms.Lx, ms.dLx);
-  } else if (tid == 64) {
-    const float gy = __fsub_rn(py, c.y0b[isl]);
-    lanczos_taps((double)__fsub_rn(gy, rintf(gy)), ms.Ly, ms.dLy);
-  } else if (tid >= 96 && tid < 96 + UPH_MAXNT && c.mode == 0) {
-    const int tt = tid - 96;
-    if (tt < c.nt) {
-      const float* os = c.psf_os + 4 * b;
-      const float X = __fdiv_rn(__fsub_rn(px, os[0]), os[1]);
-      const float Y = __fdiv_rn(__fsub_rn(py, os[2]), os[3]);
-      const float ix = __fdiv_rn(1.0f, os[1]);
-      const float iy = __fdiv_rn(1.0f, os[3]);
-      int m, n;
-      term_mn(tt, m, n);
-      float xm = 1.f, yn = 1.f, xm1 = 1.f, yn1 = 1.f;
-      for (int i = 0; i < m; ++i) xm *= X;
-      for (int i = 0; i < n; ++i) yn *= Y;
-      for (int i = 0; i + 1 < m; ++i) xm1 *= X;
-      for (int i = 0; i + 1 < n; ++i) yn1 *= Y;
-      ms.beta[tt] = xm * yn;
-      ms.betax[tt] = m > 0 ? (float)m * xm1 * yn * ix : 0.f;
-      ms.betay[tt] = n > 0 ? (float)n * xm * yn1 * iy : 0.f;
-    }
-  } else if (tid >= 128 && tid < 128 + UPH_MAXKPSF && c.mode == 1) {
-    const int q = tid - 128;
-    if (q < c.kpsf) {
-      const float* os = c.psf_os + 4 * b;
-      const double X = ((double)px - os[0]) / os[1];
-      const double Y = ((double)py - os[2]) / os[3];
-      psf_component(c, b, X, Y, 1.0 / os[1], 1.0 / os[3], q, sc.pq[q]);
+      ms.cg[a] = rec->cg[a];
+      for (int q = 0; q < 3; ++q) ms.dcov[a][q] = rec->dcov[a][q];
     }
   }
-  __syncthreads();
-  if (c.mode == 1) {
-    // ---- stage 2: normalised PSF weights, galaxy table components ----
-    if (tid == 0) {
-      double W = 0, Wx = 0, Wy = 0;
-      for (int q = 0; q < c.kpsf; ++q) {
-        W += sc.pq[q].w;
-        Wx += sc.pq[q].wx;
-        Wy += sc.pq[q].wy;
-      }
-      sc.W = W;
-      sc.Wx = Wx;
-      sc.Wy = Wy;
-    } else if (tid >= 32 && tid < 32 + UPH_MAXGAL && ms.is_gal) {
-      const int g = tid - 32;
-      const int seg = sc.seg;
-      const double t = sc.t, dt = sc.dt;
-      GalComp& o = sc.gg[g];
-      if (g < c.tb_k) {
-        const double a0 = c.tb_amps[seg * c.tb_k + g], a1 = c.tb_amps[(seg + 1) * c.tb_k + g];
-        const double l0 = c.tb_lv[seg * c.tb_k + g], l1 = c.tb_lv[(seg + 1) * c.tb_k + g];
-        o.a = (1 - t) * a0 + t * a1;
-        o.v = exp((1 - t) * l0 + t * l1);
-        o.da = dt * (a1 - a0);
-        o.dv = o.v * dt * (l1 - l0);
-      } else if (g == c.tb_k) {          // delta core: zero-variance component
-        o.a = (1 - t) * c.tb_core[seg] + t * c.tb_core[seg + 1];
-        o.v = 0.0;
-        o.da = dt * (c.tb_core[seg + 1] - c.tb_core[seg]);
-        o.dv = 0.0;
-      }
+  if (tid < 7) {
+    ms.Lx[tid] = rec->Lx[tid];
+    ms.dLx[tid] = rec->dLx[tid];
+    ms.Ly[tid] = rec->Ly[tid];
+    ms.dLy[tid] = rec->dLy[tid];
+  }
+  if (c.mode == 0) {
+    for (int tt = tid; tt < c.nt; tt += blockDim.x) {
+      ms.beta[tt] = rec->beta[tt];
+      ms.betax[tt] = rec->betax[tt];
+      ms.betay[tt] = rec->betay[tt];
     }
-    __syncthreads();
-    if (tid == 0) {
-      // compact the galaxy components that contribute (non-zero amplitude
-      // or amplitude derivative); a star is a single unit delta
-      int ng = 0;
-      if (ms.is_gal) {
-        for (int g = 0; g <= c.tb_k; ++g)
-          if (sc.gg[g].a != 0.0 || sc.gg[g].da != 0.0) sc.gg[ng++] = sc.gg[g];
-      } else {
-        sc.gg[0].a = 1.0;
-        sc.gg[0].v = 0.0;
-        sc.gg[0].da = 0.0;
-        sc.gg[0].dv = 0.0;
-        ng = 1;
-      }
-      sc.ng = ng;
-      ms.ncomp = c.kpsf * ng;
-    }
-    __syncthreads();
-    // ---- stage 3: combined Gaussian components (covariances add) ----
-    for (int e = tid; e < ms.ncomp; e += blockDim.x) {
-      const int q = e / sc.ng, g = e - (e / sc.ng) * sc.ng;
-      const PsfComp& pq = sc.pq[q];
-      const GalComp& gq = sc.gg[g];
-      const double W = sc.W;
-      const double wn = pq.w / W;
-      const double wnx = (pq.wx * W - pq.w * sc.Wx) / (W * W);
-      const double wny = (pq.wy * W - pq.w * sc.Wy) / (W * W);
-      const double A = gq.v * ms.cg[0] + pq.cov[0];
-      const double C = gq.v * ms.cg[1] + pq.cov[1];
-      const double Bc = gq.v * ms.cg[2] + pq.cov[2];
-      const double det = A * C - Bc * Bc;
-      const double rs = 0.15915494309189535 / sqrt(det);
-      GComp& o = comps[e];
-      o.ia = (float)(C / det);
-      o.ib = (float)(-Bc / det);
-      o.ic = (float)(A / det);
-      o.A = (float)A;
-      o.B = (float)Bc;
-      o.C = (float)C;
-      o.det = (float)det;
-      o.nrm = (float)(wn * gq.a * rs);
-      o.nx = (float)(wnx * gq.a * rs);
-      o.ny = (float)(wny * gq.a * rs);
-      o.nu = (float)(wn * gq.da * rs);
-      o.v = (float)gq.v;
-      o.dv = (float)gq.dv;
-      o.dAx = (float)pq.cx[0];
-      o.dCx = (float)pq.cx[1];
-      o.dBx = (float)pq.cx[2];
-      o.dAy = (float)pq.cy[0];
-      o.dCy = (float)pq.cy[1];
-      o.dBy = (float)pq.cy[2];
-    }
+  } else {
+    const int nf = rec->ncomp * (int)(sizeof(GComp) / sizeof(float));
+    const float* src = reinterpret_cast<const float*>(rec->comps);
+    float* dst = reinterpret_cast<float*>(comps);
+    for (int e = tid; e < nf; e += blockDim.x) dst[e] = src[e];
   }
   __syncthreads();
   if (mb.bw <= 0 || mb.bh <= 0) return;
@@ -484,11 +522,12 @@ k_render(ClassDev c, const float* __restrict__ P, int phase, int nsa) {
         for (int a = 0; a < ms.nact; ++a) {
           const GComp& o = comps[ms.act[a]];
           const float Q = fmaf(o.ia * xo, xo, fmaf(2.f * o.ib * xo, yo, o.ic * yo * yo));
-          const float ex = expf(-0.5f * Q);
+          // exp(-Q/2) as one base-2 exponential
+          const float ex = exp2f(Q * -0.72134752044448170f);
           const float nw = o.nrm * ex;
           s0 += nw;
           if (lin) {
-            const float i2d = 0.5f / o.det;
+            const float i2d = o.det;   // holds 0.5 / det
             const float dA = (Q * o.C - yo * yo - o.C) * i2d;
             const float dC = (Q * o.A - xo * xo - o.A) * i2d;
             const float dB = (xo * yo - o.B * Q + o.B) * (2.f * i2d);
@@ -605,6 +644,7 @@ void launch_render(const ClassDev& c, const float* P, int phase,
   if (nblk <= 0) return;
   const int nsa = render_arrays(c, phase);
   const size_t bytes = sizeof(float) * (size_t)nsa * UPH_HALO * (HP + XP);
+  k_member_setup<<<(unsigned)((long long)c.n_isl * c.nb * c.N), 128, 0, s>>>(c, P, phase);
   k_render<<<(unsigned)nblk, 256, bytes, s>>>(c, P, phase, nsa);
 }
 
