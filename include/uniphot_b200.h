@@ -58,7 +58,20 @@ typedef struct uph_class_desc {
   int32_t native_stamp;     /* odd native PSF stamp side: a star's model is
                                zero outside it (the reference zero-pads its
                                native PSF to the tier); 0 = tier            */
+  int32_t precision;        /* UPH_PRECISION_PLAIN: FP32 Gram on CUDA cores;
+                               UPH_PRECISION_MIXED: islands with more than
+                               tc_min_rows Gram rows form it on the tensor
+                               cores from BF16 hi/lo pairs with FP32
+                               accumulation, in residual form             */
+  int32_t tc_min_rows;      /* mixed form: Gram-row threshold of the
+                               tensor-core path; < 0 selects the default
+                               (UPH_TC_MIN_ROWS_DEFAULT)                   */
 } uph_class_desc;
+
+#define UPH_TC_MIN_ROWS_DEFAULT 24
+
+#define UPH_PRECISION_PLAIN 0
+#define UPH_PRECISION_MIXED 1
 
 /* Per-island inputs of one chunk of n islands (class_host_arrays rows;
  * island_plan.py:493-700).  Shapes: [n], [n*N], [n*N*6]. */

@@ -17,6 +17,7 @@ LIB_PATH = Path(__file__).resolve().parent / "libuniphot_b200.so"
 UPH_OK, UPH_ERR_INVALID, UPH_ERR_OOM, UPH_ERR_CUDA, UPH_ERR_TIMEOUT, \
     UPH_ERR_STATE = range(6)
 RENDER_MODES = {"reference": 0, "analytic": 1}
+PRECISIONS = {"plain": 0, "mixed": 1}
 
 EXPORTED = ("uph_create", "uph_destroy", "uph_last_error", "uph_set_stream",
             "uph_get_stream", "uph_upload_field", "uph_upload_field_device",
@@ -35,7 +36,8 @@ class ClassDesc(C.Structure):
                 ("render_mode", C.c_int32), ("reg", C.c_float),
                 ("pos_step_max", C.c_float), ("chi2_ftol_rel", C.c_float),
                 ("step_tol_pix", C.c_float), ("un_freeze_steps", C.c_int32),
-                ("has_priors", C.c_int32), ("native_stamp", C.c_int32)]
+                ("has_priors", C.c_int32), ("native_stamp", C.c_int32),
+                ("precision", C.c_int32), ("tc_min_rows", C.c_int32)]
 
 
 class ChunkIn(C.Structure):

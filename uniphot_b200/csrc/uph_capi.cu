@@ -20,6 +20,7 @@
 
 int uph_render_setup();
 int uph_solve_setup();
+int uph_gram_tc_setup();
 void launch_set_probe(const ClassDev& c, cudaStream_t s);
 void launch_fill_float(float* p, float v, int n, cudaStream_t s);
 
@@ -137,7 +138,7 @@ int uph_create(int device, uph_ctx** out) {
     return UPH_ERR_CUDA;
   }
   ctx->own_stream = true;
-  if (uph_render_setup() != 0 || uph_solve_setup() != 0) {
+  if (uph_render_setup() != 0 || uph_solve_setup() != 0 || uph_gram_tc_setup() != 0) {
     cudaStreamDestroy(ctx->stream);
     delete ctx;
     return UPH_ERR_CUDA;
@@ -331,6 +332,7 @@ struct Chunk {
   bool done = false;
   int iters = 0;
   int slot = 0;
+  int graph_kernels = 0;
   ~Chunk() {
     if (gexec) cudaGraphExecDestroy(gexec);
     if (graph) cudaGraphDestroy(graph);
@@ -391,10 +393,11 @@ void iteration(const ClassDev& c, Launcher& L) {
   cudaStream_t s = L.s;
   L(0, [&] { launch_render(c, c.p, PH_LIN, s); }, 2);
   L(1, [&] { launch_gram_lin(c, s); });
+  if (c.tc_min_rows < (1 << 30)) L(1, [&] { launch_gram_tc(c, s); });
   L(2, [&] { launch_assemble(c, s); });
   L(3, [&] { launch_step(c, PH_TRIAL, 0, 0.f, 0, s); });
   L(0, [&] { launch_render(c, c.p_try, PH_TRIAL, s); }, 2);
-  L(4, [&] { launch_gram_trial(c, c.p_try, PH_TRIAL, 0, s); });
+  L(4, [&] { launch_gram_trial(c, c.p_try, PH_TRIAL, 0, c.ftry, s); });
   L(5, [&] { launch_accept(c, PH_TRIAL, s); });
 }
 
@@ -499,6 +502,11 @@ int add_chunk(uph_ctx* ctx, Chunk* ch, const uph_class_desc* cls,
   c.mode = mode;
   c.native = (cls->native_stamp > 0 && cls->native_stamp < T) ? (cls->native_stamp | 1) : T;
   c.has_gal = any_gal ? 1 : 0;
+  if (cls->precision != UPH_PRECISION_PLAIN && cls->precision != UPH_PRECISION_MIXED)
+    return set_err(ctx, UPH_ERR_INVALID, "unknown precision %d", cls->precision);
+  c.tc_min_rows = (cls->precision == UPH_PRECISION_MIXED)
+                      ? (cls->tc_min_rows < 0 ? UPH_TC_MIN_ROWS_DEFAULT : cls->tc_min_rows)
+                      : (1 << 30);
   c.Hp = ctx->Hp; c.Wp = ctx->Wp;
   c.dstack = (const float*)ctx->dstack.ptr;
   c.wstack = (const float*)ctx->wstack.ptr;
@@ -568,6 +576,11 @@ int add_chunk(uph_ctx* ctx, Chunk* ch, const uph_class_desc* cls,
   c.probe_best = cbuf<float>(ctx, ch, "pbest", n, &rc);
   c.probe_p = cbuf<float>(ctx, ch, "probep", (size_t)n * 4 * nP, &rc);
   c.n_active = cbuf<int>(ctx, ch, "nact", 1, &rc);
+  c.err = cbuf<int>(ctx, ch, "err", 1, &rc);
+  if (c.tc_min_rows < (1 << 30)) {
+    c.fcur = cbuf<float>(ctx, ch, "fcur", (size_t)n * nb * N, &rc);
+    c.ftry = cbuf<float>(ctx, ch, "ftry", (size_t)n * nb * N, &rc);
+  }
   ch->d_div = cbuf<uint8_t>(ctx, ch, "div", n, &rc);
   if (rc) return rc;
   c.ox = d_ox; c.oy = d_oy; c.x0b = d_x0b; c.y0b = d_y0b; c.stype = d_st;
@@ -635,6 +648,7 @@ int reset_chunk(uph_ctx* ctx, Chunk* ch, cudaStream_t s) {
   CK(cudaMemcpyAsync(c.nrej, ch->d_nrej0, sizeof(int) * n, cudaMemcpyDeviceToDevice, s), "reset");
   CK(cudaMemcpyAsync(c.nst, ch->d_nst0, sizeof(int) * n, cudaMemcpyDeviceToDevice, s), "reset");
   CK(cudaMemcpyAsync(c.flags, ch->d_flags0, n, cudaMemcpyDeviceToDevice, s), "reset");
+  CK(cudaMemsetAsync(c.err, 0, sizeof(int), s), "reset");
   ch->done = false;
   ch->iters = 0;
   return UPH_OK;
@@ -652,11 +666,11 @@ void post_loop(Chunk* ch, Launcher& L) {
     const float lamj = (float)std::pow(10.0, (double)e);
     L(3, [&] { launch_step(c, PH_PROBE, 0, lamj, 2, s); });
     L(0, [&] { launch_render(c, c.p_try, PH_PROBE, s); }, 2);
-    L(4, [&] { launch_gram_trial(c, c.p_try, PH_PROBE, 0, s); });
+    L(4, [&] { launch_gram_trial(c, c.p_try, PH_PROBE, 0, nullptr, s); });
     L(5, [&] { launch_accept(c, PH_PROBE, s); });
   }
   L(0, [&] { launch_render(c, c.p, PH_ALL, s); }, 2);
-  L(4, [&] { launch_gram_trial(c, c.p, PH_ALL, 1, s); });
+  L(4, [&] { launch_gram_trial(c, c.p, PH_ALL, 1, nullptr, s); });
 }
 
 int job_solve(uph_job* job, int max_steps) {
@@ -690,16 +704,20 @@ int job_solve(uph_job* job, int max_steps) {
     int rc = reset_chunk(ctx, ch, s);
     if (rc) return rc;
     Launcher L{job, s, recp};
-    if (ch->fresh) {
+    // initial chi2 (fresh chunks) and, for the tensor-core Gram, the fluxes
+    // at the starting parameters that its residual row needs
+    if (ch->fresh || ch->c.fcur) {
       L(0, [&] { launch_render(ch->c, ch->c.p, PH_ALL, s); }, 2);
-      L(4, [&] { launch_gram_trial(ch->c, ch->c.p, PH_ALL, 0, s); });
-      L(5, [&] { launch_accept(ch->c, PH_ALL, s); });
+      L(4, [&] { launch_gram_trial(ch->c, ch->c.p, PH_ALL, 0, ch->c.fcur, s); });
+      if (ch->fresh) L(5, [&] { launch_accept(ch->c, PH_ALL, s); });
     }
     if (max_steps > 0 && !job->profile && !ch->gexec) {
       Launcher Lc{job, s, nullptr};
       CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "capture");
+      const int64_t before = ctx->launches;
       iteration(ch->c, Lc);
-      ctx->launches -= 9;
+      ch->graph_kernels = (int)(ctx->launches - before);
+      ctx->launches = before;
       cudaError_t ce = cudaStreamEndCapture(s, &ch->graph);
       if (ce != cudaSuccess) return cuda_err(ctx, ce, "end capture");
       CK(cudaGraphInstantiate(&ch->gexec, ch->graph, 0), "graph instantiate");
@@ -723,7 +741,7 @@ int job_solve(uph_job* job, int max_steps) {
           iteration(ch->c, L);
         } else {
           CK(cudaGraphLaunch(ch->gexec, s), "graph launch");
-          ctx->launches += 9;
+          ctx->launches += ch->graph_kernels;
         }
       }
       ch->iters += group;
@@ -757,6 +775,12 @@ int job_solve(uph_job* job, int max_steps) {
   }
   CK(cudaEventRecord(ctx->ev[2], ctx->stream), "event");
   CK(cudaStreamSynchronize(ctx->stream), "solve");
+  for (int i = 0; i < nch; ++i) {
+    int e = 0;
+    CK(cudaMemcpy(&e, job->chunks[i]->c.err, sizeof(int), cudaMemcpyDeviceToHost), "err");
+    if (e) return set_err(ctx, UPH_ERR_TIMEOUT,
+                          "a bounded device wait expired in chunk %d (tensor-core Gram)", i);
+  }
   cudaEventElapsedTime(&ctx->timing[1], ctx->ev[0], ctx->ev[2]);
   ctx->timing[2] = 0.f;
   if (job->profile) {

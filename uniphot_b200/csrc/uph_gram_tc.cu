@@ -1,0 +1,294 @@
+// Weighted Gram of the VarPro rows on the 5th-generation tensor cores.
+//
+// G = Z W Z^T for Z = [dm/dtheta (nL); m (nr); r (1)] over the island
+// window of one band, computed with tcgen05.mma.  The last row is the
+// residual r = d - M^T fc at the fluxes fc solved at the same parameters (the
+// FP32 Gram of k_gram_lin uses the data row instead): at high signal to noise
+// the gradient D W (d - M^T f) is a small difference of large Gram entries,
+// which a BF16-split Gram cannot resolve, while D W r is formed directly
+// (k_assemble works in the corresponding residual form).  Z is split per
+// element into a BF16 pair
+// Z = Zh + Zl (Zl = bf16(Z - Zh)), and
+//     G ~= Zh Zh^T + Zh Zl^T + Zl Zh^T
+// is accumulated in FP32 in tensor memory (the dropped Zl Zl^T term and the
+// pair's representation error are ~2^-16 relative per product).
+//
+// One CTA per (island, band) with K = nL + nr + 1 rows (stored padded to R =
+// 128 * ceil(K / 128) rows); pixels stream through shared memory in chunks
+// of 64, double-buffered: all threads convert chunk c + 1 while the tensor
+// core consumes chunk c.  Operands are K-major (pixels contiguous) in the
+// no-swizzle canonical layout: 8-row x 16-byte core matrices, consecutive
+// 8-row groups 128 B apart (SBO), the two 8-pixel halves of a 16-pixel MMA
+// step R * 16 B apart (LBO).  One elected thread issues M = 128, N = ceil16
+// (K) <= 256, K-step = 16 MMAs; tcgen05.commit arrives on the stage's
+// mbarrier.  Waits are bounded: on expiry the kernel raises the chunk's error
+// flag, drains, frees its tensor memory and returns.
+#include <cuda_bf16.h>
+
+#include "uph_internal.cuh"
+
+namespace {
+
+constexpr int NT = 256;
+constexpr int KC = 64;                  // pixels per chunk
+constexpr int RMAX = 256;               // rows per CTA (two M = 128 halves)
+constexpr int STAGE_BYTES = 2 * RMAX * KC * 2;   // Zh + Zl, bf16
+constexpr unsigned SPIN_LIMIT = 1u << 24;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+// UMMA shared-memory descriptor, K-major, no swizzle (sm100 version 1).
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo,
+                                              uint32_t sbo) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
+  d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+  d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+  d |= (uint64_t)1 << 46;               // descriptor version (Blackwell)
+  return d;                             // base offset 0, layout SWIZZLE_NONE
+}
+
+// Instruction descriptor: kind::f16, A = B = BF16, D = F32, K-major both,
+// M = 128, N = n.
+__device__ __forceinline__ uint32_t umma_idesc(int n) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) |
+         ((uint32_t)(128 >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_bf16(uint32_t dtmem, uint64_t adesc,
+                                         uint64_t bdesc, uint32_t idesc,
+                                         uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n"
+      :
+      : "r"(dtmem), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(acc));
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t* bar) {
+  asm volatile(
+      "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+      :
+      : "r"(smem_u32(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t phase) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred P1;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+      "selp.b32 %0, 1, 0, P1;\n\t}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(phase)
+      : "memory");
+  return ok != 0;
+}
+
+// Bounded wait on an mbarrier phase; false on expiry.
+__device__ bool mbar_wait(uint64_t* bar, uint32_t phase) {
+  for (unsigned i = 0; i < SPIN_LIMIT; ++i)
+    if (mbar_try(bar, phase)) return true;
+  return false;
+}
+
+__device__ __forceinline__ int gram_rows(const ClassDev& c, int isl) {
+  return c.isl_nL[isl] + c.isl_nr[isl] + 1;
+}
+
+__global__ void __launch_bounds__(NT, 1) k_gram_tc(ClassDev c) {
+  extern __shared__ __align__(1024) uint8_t tsm[];
+  __shared__ __align__(8) uint64_t mbar[2];
+  __shared__ uint32_t tmem_base;
+  __shared__ int4 box[UPH_MAXN];
+  __shared__ float swt[2][KC];
+  __shared__ float rsd[2][KC];
+  __shared__ float fcs[UPH_MAXN];
+  __shared__ int abort_flag;
+  const int isl = blockIdx.x / c.nb, b = blockIdx.x % c.nb;
+  if (isl >= c.n_isl || !isl_active(c.flags[isl], PH_LIN)) return;
+  const int K = gram_rows(c, isl);
+  if (K <= c.tc_min_rows) return;            // handled by k_gram_lin
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int Mh = (K + 127) / 128;            // M = 128 halves
+  const int R = Mh * 128;                    // stored rows
+  const int N = (K + 15) & ~15;              // MMA N (<= 256)
+  int ncols = 32;
+  while (ncols < Mh * N) ncols <<= 1;        // power of two >= 32
+  const int16_t* rk = c.row_k + (size_t)isl * c.Kmax;
+  const int16_t* rs = c.row_s + (size_t)isl * c.Kmax;
+  const int nr = c.isl_nr[isl];
+  for (int k = tid; k < c.N; k += NT) {
+    MemberBox mb = member_box(c, isl, c.p, k);
+    box[k] = make_int4(mb.wx0, mb.wy0, mb.bw, mb.bh);
+    fcs[k] = c.fcur[((size_t)isl * c.nb + b) * c.N + k];
+  }
+  if (tid == 0) {
+    abort_flag = 0;
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[0])) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[1])) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                 ::"r"(smem_u32(&tmem_base)), "r"(ncols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    asm volatile("tcgen05.fence::before_thread_sync;");
+  }
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  const uint32_t tbase = tmem_base;
+  const int B = c.B, Sz = c.Sz, npix = B * B;
+  const size_t plane = (size_t)c.Hp * c.Wp;
+  const float* dbase = c.dstack + b * plane + (size_t)c.oy[isl] * c.Wp + c.ox[isl];
+  const float* wbase = c.wstack + b * plane + (size_t)c.oy[isl] * c.Wp + c.ox[isl];
+  const int nchunk = (npix + KC - 1) / KC;
+  const uint32_t idesc = umma_idesc(N);
+  const uint32_t lbo = (uint32_t)R * 16u;    // between the two 8-pixel halves
+  const uint32_t sbo = 128u;                 // between 8-row groups
+  uint32_t phase[2] = {0u, 0u};   // next parity to wait for, per stage
+  int issued[2] = {0, 0}, waited[2] = {0, 0};
+  for (int ch = 0; ch < nchunk; ++ch) {
+    const int st = ch & 1;
+    uint8_t* zh = tsm + st * STAGE_BYTES;
+    uint8_t* zl = zh + RMAX * KC * 2;
+    if (ch >= 2) {
+      // the MMAs of chunk ch - 2 read this stage: wait for their commit
+      if (tid == 0) {
+        if (!mbar_wait(&mbar[st], phase[st])) abort_flag = 1;
+        phase[st] ^= 1u;
+        ++waited[st];
+      }
+      __syncthreads();
+      if (abort_flag) break;
+    }
+    const int pix0 = ch * KC;
+    if (tid < KC) {
+      // weights and the weighted residual sqrt(w) (d - sum_k fc_k m_k)
+      const int pix = pix0 + tid;
+      float sw = 0.f, rv = 0.f;
+      if (pix < npix) {
+        const int wy = pix / B, wx = pix - (pix / B) * B;
+        sw = sqrtf(wbase[(size_t)wy * c.Wp + wx]);
+        float model = 0.f;
+        for (int k = 0; k < nr; ++k) {
+          const int4 bx = box[k];
+          const int ly = wy - bx.y, lx = wx - bx.x;
+          if (ly >= 0 && ly < bx.w && lx >= 0 && lx < bx.z)
+            model = fmaf(fcs[k], c.stamps[stamp_slot(c, isl, b, k, 0) + (size_t)ly * Sz + lx],
+                         model);
+        }
+        rv = sw * (dbase[(size_t)wy * c.Wp + wx] - model);
+      }
+      swt[st][tid] = sw;
+      rsd[st][tid] = rv;
+    }
+    __syncthreads();
+    for (int e = tid; e < R * KC; e += NT) {
+      const int r = e / KC, q = e - (e / KC) * KC;
+      const int pix = pix0 + q;
+      float v = 0.f;
+      if (r < K && pix < npix) {
+        const int wy = pix / B, wx = pix - (pix / B) * B;
+        const int s = rs[r];
+        if (s < 0) {
+          v = rsd[st][q];
+        } else {
+          const int k = rk[r];
+          const int4 bx = box[k];
+          const int ly = wy - bx.y, lx = wx - bx.x;
+          if (ly >= 0 && ly < bx.w && lx >= 0 && lx < bx.z)
+            v = c.stamps[stamp_slot(c, isl, b, k, s) + (size_t)ly * Sz + lx] * swt[st][q];
+        }
+      }
+      const __nv_bfloat16 h = __float2bfloat16_rn(v);
+      const __nv_bfloat16 l = __float2bfloat16_rn(v - __bfloat162float(h));
+      const uint32_t off = (uint32_t)(((q >> 3) * (R >> 3) + (r >> 3)) * 128 +
+                                      (r & 7) * 16 + (q & 7) * 2);
+      *reinterpret_cast<__nv_bfloat16*>(zh + off) = h;
+      *reinterpret_cast<__nv_bfloat16*>(zl + off) = l;
+    }
+    // make the generic-proxy stores visible to the tensor core (async proxy)
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    if (tid == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;");
+      const uint32_t ah = smem_u32(zh), al = smem_u32(zl);
+      for (int s = 0; s < KC / 16; ++s) {
+        const uint32_t koff = (uint32_t)(2 * s * (R >> 3)) * 128u;
+        for (int h = 0; h < Mh; ++h) {
+          const uint32_t moff = (uint32_t)(h * 16) * 128u;
+          const uint32_t dt = tbase + (uint32_t)(h * N);
+          const uint32_t acc0 = (ch > 0 || s > 0) ? 1u : 0u;
+          mma_bf16(dt, umma_desc(ah + koff + moff, lbo, sbo),
+                   umma_desc(ah + koff, lbo, sbo), idesc, acc0);
+          mma_bf16(dt, umma_desc(ah + koff + moff, lbo, sbo),
+                   umma_desc(al + koff, lbo, sbo), idesc, 1u);
+          mma_bf16(dt, umma_desc(al + koff + moff, lbo, sbo),
+                   umma_desc(ah + koff, lbo, sbo), idesc, 1u);
+        }
+      }
+      mma_commit(&mbar[st]);
+      ++issued[st];
+    }
+  }
+  // drain: wait for every commit not yet observed (bounded, also on abort)
+  if (tid == 0) {
+    for (int st = 0; st < 2; ++st) {
+      while (waited[st] < issued[st]) {
+        if (!mbar_wait(&mbar[st], phase[st])) {
+          abort_flag = 1;
+          break;
+        }
+        phase[st] ^= 1u;
+        ++waited[st];
+      }
+    }
+  }
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  if (abort_flag) {
+    if (tid == 0) atomicExch(c.err, 1);
+  } else if (warp < 4) {
+    float* out = c.gram + ((size_t)isl * c.nb + b) * c.Kmax * c.Kmax;
+    const int ld = c.Kmax;
+    for (int h = 0; h < Mh; ++h) {
+      const int row = h * 128 + warp * 32 + lane;
+      for (int c0 = 0; c0 < N; c0 += 16) {
+        uint32_t v[16];
+        const uint32_t ta = tbase + ((uint32_t)(warp * 32) << 16) + (uint32_t)(h * N + c0);
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+            "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+            : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]),
+              "=r"(v[6]), "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]),
+              "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+            : "r"(ta));
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        if (row < K)
+          for (int j = 0; j < 16; ++j)
+            if (c0 + j < K) out[row * ld + c0 + j] = __uint_as_float(v[j]);
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase), "r"(ncols));
+}
+
+}  // namespace
+
+size_t gram_tc_smem_bytes() { return (size_t)2 * STAGE_BYTES; }
+
+void launch_gram_tc(const ClassDev& c, cudaStream_t s) {
+  k_gram_tc<<<(unsigned)(c.n_isl * c.nb), NT, gram_tc_smem_bytes(), s>>>(c);
+}
+
+int uph_gram_tc_setup() {
+  return (int)cudaFuncSetAttribute(k_gram_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)gram_tc_smem_bytes());
+}

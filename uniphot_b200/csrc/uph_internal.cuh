@@ -115,9 +115,16 @@ struct ClassDev {
   float* flux;
   float* ferr;
   int* ngood;
+  // Fluxes solved at p (fcur) and at p_try (ftry), (n_isl, nb, N); only
+  // allocated when some island uses the tensor-core Gram, whose last row is
+  // the residual d - M^T fcur instead of the data.
+  float* fcur;
+  float* ftry;
   float* probe_best;       // (n_isl) plateau certificate
   float* probe_p;          // (n_isl, 4, nP) diverged-probe proposals
   int* n_active;
+  int* err;                // device error flag (bounded waits that expired)
+  int tc_min_rows;         // islands with more Gram rows use the tensor-core Gram
   float reg, pos_step_max, ftol_rel, step_tol;
   int un_freeze;
 };
@@ -173,7 +180,7 @@ void launch_render(const ClassDev& c, const float* P, int phase,
 void launch_gram_lin(const ClassDev& c, cudaStream_t s);
 void launch_assemble(const ClassDev& c, cudaStream_t s);
 void launch_gram_trial(const ClassDev& c, const float* P, int phase,
-                       int final_mode, cudaStream_t s);
+                       int final_mode, float* fout, cudaStream_t s);
 void launch_step(const ClassDev& c, int phase, int probe_j, float probe_lam,
                  int use_lam_final_scale, cudaStream_t s);
 void launch_accept(const ClassDev& c, int phase, cudaStream_t s);
@@ -185,4 +192,6 @@ size_t gram_lin_smem_bytes(int Kmax);
 size_t gram_trial_smem_bytes(int N);
 size_t assemble_smem_bytes(int nLmax, int N);
 size_t step_smem_bytes(int nLmax);
+void launch_gram_tc(const ClassDev& c, cudaStream_t s);
+size_t gram_tc_smem_bytes();
 int uph_kernel_setup();

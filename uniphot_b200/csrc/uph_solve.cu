@@ -248,6 +248,7 @@ __global__ void __launch_bounds__(NT) k_gram_lin(ClassDev c) {
   if (isl >= c.n_isl || !isl_active(c.flags[isl], PH_LIN)) return;
   const int nL = c.isl_nL[isl], nr = c.isl_nr[isl];
   const int K = nL + nr + 1;
+  if (K > c.tc_min_rows) return;     // the tensor-core Gram handles this island
   const int nbk = (K + 7) / 8;
   const int nblk = nbk * (nbk + 1) / 2;
   if ((int)blockIdx.y * NT >= max(nblk, 1) && blockIdx.y > 0) return;
@@ -330,6 +331,16 @@ __global__ void __launch_bounds__(NT) k_assemble(ClassDev c) {
   }
   const int m0 = nL;  // first model row
   const int dr = nL + nr;
+  // Residual form (tensor-core Gram): the last Gram row is r = d - M^T fc
+  // with fc the fluxes solved at the same parameters, so G holds M W r and
+  // D W r instead of M W d and D W d.  Every quantity below is rewritten in
+  // terms of the small differences fc - f, which avoids the cancellation of
+  // D W d - D W M^T f at high signal to noise:
+  //   f = fc + (A + reg I)^-1 (M W r - reg fc),
+  //   D W (d - M^T x) = D W r + D W M^T (fc - x),
+  //   M W d - A x     = M W r + A (fc - x).
+  const bool resid = K > c.tc_min_rows;
+  const float* fc = resid ? c.fcur + ((size_t)isl * c.nb + b) * c.N : nullptr;
   for (int e = tid; e < nr * ncol; e += NT) {
     const int r = e / ncol, j = e - (e / ncol) * ncol;
     double v;
@@ -340,6 +351,7 @@ __global__ void __launch_bounds__(NT) k_assemble(ClassDev c) {
       v = (j - nr == r) ? 1.0 : 0.0;
     } else {
       v = (double)G[(m0 + r) * ldg + dr];
+      if (resid) v -= (double)c.reg * (double)fc[r];
     }
     Aug[r * lda + j] = v;
   }
@@ -351,21 +363,28 @@ __global__ void __launch_bounds__(NT) k_assemble(ClassDev c) {
   gauss_jordan(Aug, nr, ncol, lda, fac, &piv);
   // f64 fluxes and their float32 copy (the model uses f32 fluxes)
   for (int l = tid; l < nr; l += NT) {
-    f64v[l] = Aug[l * lda + 2 * nr];
+    f64v[l] = Aug[l * lda + 2 * nr] + (resid ? (double)fc[l] : 0.0);
     av[l] = (double)(float)f64v[l];
   }
   __syncthreads();
   // q = b - A a  (A without ridge)
   for (int l = tid; l < nr; l += NT) {
     double t = (double)G[(m0 + l) * ldg + dr];
-    for (int m = 0; m < nr; ++m) t -= (double)G[(m0 + l) * ldg + m0 + m] * av[m];
+    if (resid)
+      for (int m = 0; m < nr; ++m)
+        t += (double)G[(m0 + l) * ldg + m0 + m] * ((double)fc[m] - av[m]);
+    else
+      for (int m = 0; m < nr; ++m) t -= (double)G[(m0 + l) * ldg + m0 + m] * av[m];
     qv[l] = t;
   }
   // c_i = Ainv (e_k s_i - f_k u_i), rounded to f32
   for (int i = tid; i < nL; i += NT) {
     const int k = rk[i];
     double si = (double)G[i * ldg + dr];
-    for (int m = 0; m < nr; ++m) si -= DM[i * UPH_MAXN + m] * f64v[m];
+    if (resid)
+      for (int m = 0; m < nr; ++m) si += DM[i * UPH_MAXN + m] * ((double)fc[m] - f64v[m]);
+    else
+      for (int m = 0; m < nr; ++m) si -= DM[i * UPH_MAXN + m] * f64v[m];
     const double fk = f64v[k];
     for (int l = 0; l < nr; ++l) {
       double t = Aug[l * lda + nr + k] * si;
@@ -407,7 +426,10 @@ __global__ void __launch_bounds__(NT) k_assemble(ClassDev c) {
   // g_i = -(a_i (Dd_i - DM_i . a) + c_i . q)
   for (int i = tid; i < nL; i += NT) {
     double t = (double)G[i * ldg + dr];
-    for (int m = 0; m < nr; ++m) t -= DM[i * UPH_MAXN + m] * av[m];
+    if (resid)
+      for (int m = 0; m < nr; ++m) t += DM[i * UPH_MAXN + m] * ((double)fc[m] - av[m]);
+    else
+      for (int m = 0; m < nr; ++m) t -= DM[i * UPH_MAXN + m] * av[m];
     double u = 0.0;
     for (int l = 0; l < nr; ++l) u += Cm[i * UPH_MAXN + l] * qv[l];
     gb[i] = (float)(-(av[rk[i]] * t + u));
@@ -416,7 +438,7 @@ __global__ void __launch_bounds__(NT) k_assemble(ClassDev c) {
 
 __global__ void __launch_bounds__(NT)
 k_gram_trial(ClassDev c, const float* __restrict__ P, int phase,
-             int final_mode) {
+             int final_mode, float* __restrict__ fout) {
   extern __shared__ float sm[];
   __shared__ int4 box[UPH_MAXN];
   __shared__ int16_t rk[UPH_MAXN + 1], rs[UPH_MAXN + 1];
@@ -458,6 +480,10 @@ k_gram_trial(ClassDev c, const float* __restrict__ P, int phase,
   __syncthreads();
   gauss_jordan(Aug, nr, ncol, ncol, fac, &piv);
   for (int l = tid; l < nr; l += NT) fl32[l] = (float)Aug[l * ncol + 2 * nr];
+  if (fout) {
+    float* fo = fout + ((size_t)isl * c.nb + b) * c.N;
+    for (int k = tid; k < c.N; k += NT) fo[k] = k < nr ? (float)Aug[k * ncol + 2 * nr] : 0.f;
+  }
   __syncthreads();
   // residual pass
   const int B = c.B, Sz = c.Sz;
@@ -733,6 +759,10 @@ __global__ void k_accept(ClassDev c, int phase) {
   uint8_t nf = fl;
   if (accept) {
     for (int q = 0; q < nP; ++q) p[q] = pt[q];
+    if (c.fcur) {
+      const size_t o = (size_t)isl * c.nb * c.N;
+      for (int e = 0; e < c.nb * c.N; ++e) c.fcur[o + e] = c.ftry[o + e];
+    }
     c.chi2[isl] = chi2_try;
     nf |= FL_NEEDLIN;
   }
@@ -828,9 +858,9 @@ void launch_assemble(const ClassDev& c, cudaStream_t s) {
 }
 
 void launch_gram_trial(const ClassDev& c, const float* P, int phase,
-                       int final_mode, cudaStream_t s) {
+                       int final_mode, float* fout, cudaStream_t s) {
   k_gram_trial<<<(unsigned)(c.n_isl * c.nb), NT, gram_trial_smem_bytes(c.N), s>>>(
-      c, P, phase, final_mode);
+      c, P, phase, final_mode, fout);
 }
 
 void launch_step(const ClassDev& c, int phase, int probe_j, float probe_lam,

@@ -157,7 +157,8 @@ def make_class_kernels(plan, n_bands: int, n_terms: int, *, render_backend: str,
                        scene_subtract: bool = False, crossband: dict | None = None,
                        convergence: str = "legacy", plateau_dlnp_tol: float = 0.5,
                        render_mode: str = "reference",
-                       native_stamp: int = 0) -> ClassKernels:
+                       native_stamp: int = 0, precision: str = "plain",
+                       tc_min_rows: int = -1) -> ClassKernels:
     if stall_count_mode not in ("proposals", "changed"):
         raise ValueError(f"stall_count_mode must be 'proposals' or 'changed', "
                          f"got {stall_count_mode!r}")
@@ -177,6 +178,8 @@ def make_class_kernels(plan, n_bands: int, n_terms: int, *, render_backend: str,
     if render_mode not in ("reference", "analytic"):
         raise ValueError(f"render_mode must be 'reference' or 'analytic', "
                          f"got {render_mode!r}")
+    if precision not in _lib.PRECISIONS:
+        raise ValueError(f"precision must be 'plain' or 'mixed', got {precision!r}")
     unsupported = []
     if stall_count_mode != "proposals":
         unsupported.append("stall_count_mode='changed'")
@@ -199,7 +202,8 @@ def make_class_kernels(plan, n_bands: int, n_terms: int, *, render_backend: str,
         render_mode=_lib.RENDER_MODES[render_mode], reg=float(reg),
         pos_step_max=float(pos_step_max_pix), chi2_ftol_rel=float(chi2_ftol_rel),
         step_tol_pix=float(step_tol_pix), un_freeze_steps=int(un_freeze_steps),
-        has_priors=int(bool(has_priors)), native_stamp=int(native_stamp))
+        has_priors=int(bool(has_priors)), native_stamp=int(native_stamp),
+        precision=_lib.PRECISIONS[precision], tc_min_rows=int(tc_min_rows))
     return ClassKernels(desc, render_mode, int(n_bands), str(plan.kind))
 
 
@@ -389,7 +393,7 @@ class IslandFitJob:
                  render_mode: str | None = None, tier_ladder=(111, 221),
                  native_stamp: int | None = None, device: int = 0,
                  field: DeviceField | None = None,
-                 chunk_budget_bytes: float = 16e9):
+                 chunk_budget_bytes: float = 16e9, precision: str = "plain"):
         for flag, name in ((compute_param_errors, "compute_param_errors"),
                            (compute_source_metrics, "compute_source_metrics"),
                            (compute_re_profile, "compute_re_profile"),
@@ -443,7 +447,7 @@ class IslandFitJob:
                 has_priors=bool(host["has_priors"]),
                 stall_count_mode=stall_count_mode, convergence=convergence,
                 plateau_dlnp_tol=plateau_dlnp_tol, render_mode=render_mode,
-                native_stamp=fp.native)
+                native_stamp=fp.native, precision=precision)
             chunk = _chunk_size(plan, n_bands, chunk_budget_bytes)
             ids = []
             for lo in range(0, plan.n_islands, chunk):
