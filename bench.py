@@ -42,6 +42,9 @@ import numpy as np
 
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
+# chunks run on up to 32 streams: give them as many hardware queues (read at
+# CUDA context creation, so before torch touches the device)
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 
 METRIC = ("islands/s at <=1e-4 rel flux err vs FP64 (plain vs batched+mixed); "
           "p50/p99 serve latency")
@@ -51,11 +54,13 @@ WORKLOAD = ("production field 2048x2048, 20 bands, 5000 sources "
 
 
 def _peaks():
+    """(HBM GB/s, bf16 TFLOP/s burst, bf16 TFLOP/s sustained, source)."""
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
         d = json.loads(p.read_text())
-        return float(d["hbm_gbs"]), float(d["bf16_tflops"]), "measured"
-    return 6650.0, 1590.0, "fallback"
+        return (float(d["hbm_gbs"]), float(d["bf16_tflops"]),
+                float(d.get("bf16_tflops_sustained", d["bf16_tflops"])), "measured")
+    return 6650.0, 1590.0, 1400.0, "fallback"
 
 
 class ClockSampler:
@@ -196,6 +201,97 @@ def run_reference_arm(args, rank, world):
                 "d2h_bytes_per_step": 0}}))
 
 
+def _timed_solves(job, steps, stream, barrier, dist):
+    """Device time (ms) of `steps` solves, max over ranks, and launches."""
+    import torch
+    launches = 0
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    barrier()
+    e0.record(stream)
+    for _ in range(steps):
+        job.solve()
+        launches += job.field.ctx.last_launch_count()
+    e1.record(stream)
+    barrier()
+    ms = e0.elapsed_time(e1)
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    return ms, launches
+
+
+def _kernel_table(job):
+    """Instrumented solve: per kind device ms, launches and algorithmic work."""
+    job.job.set_profile(True)
+    job.solve()
+    kt = job.job.kernel_times()
+    kw = job.job.kernel_work()
+    job.job.set_profile(False)
+    out = {}
+    for k, (ms, n) in kt.items():
+        if n == 0:
+            continue
+        by, fl = kw[k]
+        out[k] = {"ms": ms, "launches": n, "alg_bytes": by, "alg_flops": fl,
+                  "gbs": by / (ms * 1e6) if ms > 0 else None,
+                  "tflops": fl / (ms * 1e9) if ms > 0 and fl > 0 else None}
+    return out
+
+
+def _traffic(kernel):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary,
+    scaled to this workload's algorithmic bytes per launch (the summary
+    records both for its capture), or None."""
+    p = ROOT / "profiles" / f"{kernel}_launch_traffic.md"
+    if not p.exists():
+        return None
+    vals = {}
+    for line in p.read_text().splitlines():
+        if line.startswith("- ") and ":" in line:
+            k, v = line[2:].split(":", 1)
+            try:
+                vals[k.strip()] = float(v.split()[0])
+            except (ValueError, IndexError):
+                pass
+    if "dram_bytes_per_launch" in vals and "alg_bytes_per_launch" in vals:
+        return vals
+    return None
+
+
+def _class_results(job):
+    cache = {}
+
+    def get(ci):
+        if ci not in cache:
+            plan, host, ids = job.classes[ci]
+            parts = [job.job.read(i) for i in ids]
+            cache[ci] = {k: np.concatenate([q[k] for q in parts], axis=0)
+                         for k in ("fluxes", "p")}
+        return cache[ci]
+    return get
+
+
+def _flux_quality(get, classes, ref64):
+    """Per-flux error against the float64 oracle on the sampled islands."""
+    rel, ok = [], []
+    for (ci, r), o in ref64:
+        mm = classes[ci][1]["mmask"][r]
+        fg = get(ci)["fluxes"][r][:, mm]
+        fo = o["fluxes"][:, mm]
+        so = o["ferr"][:, mm]
+        d = np.abs(fg - fo)
+        rel.append((d / np.maximum(np.abs(fo), 1e-30)).ravel())
+        ok.append(((d <= 1e-4 * np.abs(fo)) | (d <= 0.01 * so)).ravel())
+    if not rel:
+        return None
+    e = np.concatenate(rel)
+    return {"frac_within_1e-4_rel_or_0.01sigma": float(np.mean(np.concatenate(ok))),
+            "rel_median": float(np.median(e)), "rel_p99": float(np.quantile(e, 0.99)),
+            "n_fluxes": int(e.size)}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -207,8 +303,15 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=40.0)
     ap.add_argument("--ref-budget", type=float, default=25.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--precision", default="mixed", choices=["plain", "mixed"],
+                    help="Gram form of the headline number (the other form is "
+                         "timed too and reported beside it)")
     ap.add_argument("--profile-run", action="store_true",
-                    help="one solve of the workload and exit (for ncu)")
+                    help="one instrumented solve and exit (for ncu)")
+    ap.add_argument("--side", type=int, default=2048,
+                    help="field side (the workload is 2048; smaller sides "
+                         "are for profiler captures)")
+    ap.add_argument("--n-src", type=int, default=5000)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -225,17 +328,19 @@ def main():
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))
     from uniphot_b200.solver import IslandFitJob, island_fit
-    field = make_field(args.seed + 7919 * rank, "cuda")
+    from uniphot_b200.synth import make_production_field
+    field = make_production_field(args.seed + 7919 * rank, device="cuda",
+                                  side=args.side, n_src=args.n_src)
     kw = field.fit_kwargs("analytic")
+    kw["precision"] = args.precision
     job = IslandFitJob(**kw, device=local)
     n_isl = job.n_islands
     stream = torch.cuda.ExternalStream(job.field.ctx.stream_ptr())
     if args.profile_run:
-        job.solve()
+        kt = _kernel_table(job)
         torch.cuda.synchronize()
         print(json.dumps({"profile_run": True, "n_islands": n_isl,
-                          "launches": job.field.ctx.last_launch_count(),
-                          "solve_ms": job.field.ctx.last_timing()[1]}), flush=True)
+                          "precision": args.precision, "kernels": kt}), flush=True)
         job.close()
         return
 
@@ -246,35 +351,25 @@ def main():
 
     for _ in range(args.warmup):
         job.solve()
-    barrier()
-    launches = 0
     with ClockSampler(local) as clk:
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for _ in range(args.steps):
-            job.solve()
-            launches += job.field.ctx.last_launch_count()
-        e1.record(stream)
-        barrier()
-    ms = e0.elapsed_time(e1)
-    if dist is not None:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+        ms, launches = _timed_solves(job, args.steps, stream, barrier, dist)
     value = world * n_isl * args.steps / (ms / 1e3)
-    # instrumented solve: per-kernel CUDA-event times
-    job.job.set_profile(True)
-    job.solve()
-    ktimes = job.job.kernel_times()
-    job.job.set_profile(False)
+    # the other Gram form on the same resident field
+    other = "plain" if args.precision == "mixed" else "mixed"
+    job_o = IslandFitJob(**dict(kw, precision=other), device=local, field=job.field)
+    for _ in range(args.warmup):
+        job_o.solve()
+    ms_o, _ = _timed_solves(job_o, args.steps, stream, barrier, dist)
+    value_o = world * n_isl * args.steps / (ms_o / 1e3)
+    ktab = _kernel_table(job)
+    ktab_o = _kernel_table(job_o)
     res = job.result()
     # e2e through the public API (host arrays in, results out)
     e2e_t = []
     for _ in range(args.e2e_steps):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        r2 = island_fit(**kw, device=local)
+        island_fit(**kw, device=local)
         torch.cuda.synchronize()
         e2e_t.append(time.perf_counter() - t0)
     e2e_v = world * n_isl / float(np.median(e2e_t))
@@ -287,9 +382,27 @@ def main():
             "lower", "upper", "prior_mean", "prior_inv_sigma"))
     d2h = sum(p.n_islands * (6 * p.nsrc_class * 4 + 2 * nb * p.nsrc_class * 4 + 40)
               for p, _, _ in job.classes)
-    # roofline of the dominant kernel
-    hbm, bf16, src = _peaks()
-    dom = max(ktimes, key=lambda k: ktimes[k][0])
+    # roofline of the dominant kernel (largest device time)
+    hbm, bf16, bf16_sus, src = _peaks()
+    dom = max(ktab, key=lambda k: ktab[k]["ms"])
+    d = ktab[dom]
+    if dom == "gram_tc":
+        roof = {"kernel": dom, "bound": "tensor", "achieved": d["tflops"],
+                "peak": bf16_sus, "unit": "TFLOP/s", "frac": d["tflops"] / bf16_sus}
+    else:
+        roof = {"kernel": dom, "bound": "hbm", "achieved": d["gbs"], "peak": hbm,
+                "unit": "GB/s", "frac": d["gbs"] / hbm}
+    tr = _traffic(dom)
+    roof["traffic"] = None
+    if tr is not None:
+        per_launch = d["alg_bytes"] / d["launches"]
+        roof["traffic"] = tr["dram_bytes_per_launch"] * per_launch / tr["alg_bytes_per_launch"]
+        roof["alg_bytes_per_launch"] = per_launch
+    roof["peaks"] = f"{src} (MEASURED_PEAKS.json)" if src == "measured" else src
+    forms = {
+        "mixed": "batched+mixed: LM loop as CUDA graphs on 16 streams; tcgen05 "
+                 "BF16 hi/lo Gram (residual form) for islands with > 24 Gram rows",
+        "plain": "plain: same engine, FP32 Gram on CUDA cores for every island"}
     out = {
         "metric": METRIC, "value": value, "unit": "islands/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup,
@@ -299,14 +412,16 @@ def main():
         "config": {"workload": WORKLOAD, "n_islands": n_isl,
                    "l2": "inputs (671 MB field) larger than L2",
                    "parallelism": f"dp{world} (island partition by field)",
-                   "form": "plain FP32 Gram, device LM loop (CUDA graph)"},
+                   "form": forms[args.precision]},
+        "forms": {args.precision: {"value": value, "ms_per_step": ms / args.steps,
+                                   "kernels": ktab},
+                  other: {"value": value_o, "ms_per_step": ms_o / args.steps,
+                          "kernels": ktab_o, "form": forms[other]}},
         "e2e": {"value": e2e_v, "unit": "islands/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},
         "gpu_launches": int(launches),
         "clocks": clk.summary(),
-        "kernel_ms": {k: {"ms": v[0], "launches": v[1]} for k, v in ktimes.items()},
-        "roofline": {"kernel": dom, "bound": None, "achieved": None, "peak": None,
-                     "unit": None, "frac": None, "traffic": None, "peaks": src},
+        "roofline": roof,
         "quality": {"converged_frac": float(np.mean(res.converged)),
                     "mean_steps": float(np.mean(res.n_steps))},
     }
@@ -319,25 +434,15 @@ def main():
             "kind": "port",
             "sample": f"seeded 1% island sample ({len(done)} of {len(sample)} "
                       f"islands in {dt:.1f}s), oracle at reference precision"}
-        # flux error vs the FP64 oracle on the same sample
-        errs = []
         ref64, _, _ = cpu_oracle_time(job.classes, job.PAD, field, sample[:len(done)],
                                       precision="f64", budget_s=args.cpu_budget)
-        for (ci, r), o in ref64:
-            plan, host, ids = job.classes[ci]
-            parts = [job.job.read(i) for i in ids]
-            fl = np.concatenate([p["fluxes"] for p in parts], axis=0)[r]
-            mm = host["mmask"][r]
-            fo = o["fluxes"][:, mm]
-            fg = fl[:, mm]
-            errs.append(np.abs(fg - fo) / np.maximum(np.abs(fo), 1e-30))
-        if errs:
-            e = np.concatenate([x.ravel() for x in errs])
-            out["quality"]["flux_rel_err_vs_fp64"] = {
-                "median": float(np.median(e)), "p99": float(np.quantile(e, 0.99)),
-                "max": float(e.max()), "n": int(e.size)}
+        out["quality"]["flux_vs_fp64"] = {
+            args.precision: _flux_quality(_class_results(job), job.classes, ref64),
+            other: _flux_quality(_class_results(job_o), job.classes, ref64),
+            "sample_islands": len(ref64)}
     if rank == 0:
         print(json.dumps(out), flush=True)
+    job_o.close()
     job.close()
     if dist is not None:
         dist.barrier()

@@ -187,12 +187,22 @@ int uph_job_solve(uph_job* job, int32_t max_steps);
 /* Copy one chunk's results to host buffers. */
 int uph_job_read(uph_job* job, int32_t chunk_id, uph_chunk_out* out);
 /* Per-kernel device time of the last instrumented solve: kind in
- * 0 render, 1 gram, 2 assemble, 3 step, 4 trial chi2, 5 accept;
- * returns total milliseconds and launch count.  Instrumentation is on
- * when uph_job_set_profile(job, 1) was called before the solve. */
+ * 0 render, 1 gram (FP32), 2 assemble, 3 step, 4 trial chi2, 5 accept,
+ * 6 gram on the tensor cores; returns total milliseconds and launch count.
+ * Instrumentation is on when uph_job_set_profile(job, 1) was called before
+ * the solve.  An instrumented solve runs every chunk on one stream with
+ * CUDA events around each launch (no graphs); its results are identical. */
+#define UPH_KERNEL_KINDS 7
 int uph_job_set_profile(uph_job* job, int32_t on);
 int uph_job_kernel_time(const uph_job* job, int32_t kind, float* ms,
                         int64_t* launches);
+/* Algorithmic work of the same kernels over the last instrumented solve, as
+ * counted by every working CTA: bytes (stamps written by the render; stamp
+ * rows over their member boxes, data, weights and the result for the Gram
+ * and the trial chi2; small per-island arrays for the rest) and flops (the
+ * Gram's K (K + 1) per window pixel; the step's 2/3 nL^3 LU). */
+int uph_job_kernel_work(const uph_job* job, int32_t kind, double* bytes,
+                        double* flops);
 
 /* ---- Allocation-free final-flux pass.  No counterpart in the reference:
  * it exists for callers that cannot call cudaMalloc (a host inside a

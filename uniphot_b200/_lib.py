@@ -25,8 +25,9 @@ EXPORTED = ("uph_create", "uph_destroy", "uph_last_error", "uph_set_stream",
             "uph_upload_sersic_table", "uph_run_chunk", "uph_last_timing",
             "uph_last_launch_count", "uph_job_create", "uph_job_destroy",
             "uph_job_add_chunk", "uph_job_solve", "uph_job_read",
-            "uph_job_set_profile", "uph_job_kernel_time")
-KERNEL_KINDS = ("render", "gram", "assemble", "step", "trial_chi2", "accept")
+            "uph_job_set_profile", "uph_job_kernel_time", "uph_job_kernel_work")
+KERNEL_KINDS = ("render", "gram", "assemble", "step", "trial_chi2", "accept",
+                "gram_tc")
 
 _P = C.c_void_p
 
@@ -97,6 +98,8 @@ def lib():
         L.uph_job_set_profile.argtypes = [_P, C.c_int32]
         L.uph_job_kernel_time.argtypes = [_P, C.c_int32, C.POINTER(C.c_float),
                                           C.POINTER(C.c_int64)]
+        L.uph_job_kernel_work.argtypes = [_P, C.c_int32, C.POINTER(C.c_double),
+                                          C.POINTER(C.c_double)]
         _lib = L
     return _lib
 
@@ -301,6 +304,17 @@ class Job:
             cnt = C.c_int64(0)
             lib().uph_job_kernel_time(self._h, i, C.byref(ms), C.byref(cnt))
             res[name] = (float(ms.value), int(cnt.value))
+        return res
+
+    def kernel_work(self) -> dict:
+        """Algorithmic (bytes, flops) per kernel kind of the last
+        instrumented solve."""
+        res = {}
+        for i, name in enumerate(KERNEL_KINDS):
+            by = C.c_double(0)
+            fl = C.c_double(0)
+            lib().uph_job_kernel_work(self._h, i, C.byref(by), C.byref(fl))
+            res[name] = (float(by.value), float(fl.value))
         return res
 
     def close(self):

@@ -13,6 +13,7 @@
 #include <cstring>
 #include <map>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/uniphot_b200.h"
@@ -25,6 +26,8 @@ void launch_set_probe(const ClassDev& c, cudaStream_t s);
 void launch_fill_float(float* p, float v, int n, cudaStream_t s);
 
 #define UPH_CHECK_EVERY 4
+#define UPH_MAX_STREAMS 32
+#define UPH_HIGH_PRIORITY_STREAMS 4
 
 namespace {
 
@@ -348,12 +351,16 @@ struct uph_job {
   int* h_active = nullptr;  // pinned, one slot per chunk
   int h_active_cap = 0;
   bool profile = false;
-  float ktime[6] = {0, 0, 0, 0, 0, 0};
-  int64_t kcount[6] = {0, 0, 0, 0, 0, 0};
+  float ktime[WK_KINDS] = {};
+  int64_t kcount[WK_KINDS] = {};
+  double kbytes[WK_KINDS] = {};
+  double kflops[WK_KINDS] = {};
+  unsigned long long* d_work = nullptr;   // (WK_KINDS, 2) device counters
   ~uph_job() {
     for (auto* c : chunks) delete c;
     for (auto s : streams) cudaStreamDestroy(s);
     if (h_active) cudaFreeHost(h_active);
+    if (d_work) cudaFree(d_work);
   }
 };
 
@@ -393,7 +400,7 @@ void iteration(const ClassDev& c, Launcher& L) {
   cudaStream_t s = L.s;
   L(0, [&] { launch_render(c, c.p, PH_LIN, s); }, 2);
   L(1, [&] { launch_gram_lin(c, s); });
-  if (c.tc_min_rows < (1 << 30)) L(1, [&] { launch_gram_tc(c, s); });
+  if (c.tc_min_rows < (1 << 30)) L(WK_GRAM_TC, [&] { launch_gram_tc(c, s); });
   L(2, [&] { launch_assemble(c, s); });
   L(3, [&] { launch_step(c, PH_TRIAL, 0, 0.f, 0, s); });
   L(0, [&] { launch_render(c, c.p_try, PH_TRIAL, s); }, 2);
@@ -682,11 +689,37 @@ int job_solve(uph_job* job, int max_steps) {
   ctx->launches = 0;
   // instrumented solves run on one stream so that per-launch event times
   // are not inflated by other streams' kernels
-  const int nstreams = job->profile ? 1 : std::min(nch, 16);
-  while ((int)job->streams.size() < nstreams) {
-    cudaStream_t st;
-    CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "stream");
-    job->streams.push_back(st);
+  const int nstreams = job->profile ? 1 : std::min(nch, UPH_MAX_STREAMS);
+  if ((int)job->streams.size() < nstreams) {
+    int prio_lo = 0, prio_hi = 0;
+    CK(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi), "stream priorities");
+    while ((int)job->streams.size() < nstreams) {
+      // the first streams take the heaviest chunks (the critical path) and
+      // get the highest priority
+      const int prio = (int)job->streams.size() < UPH_HIGH_PRIORITY_STREAMS ? prio_hi : prio_lo;
+      cudaStream_t st;
+      CK(cudaStreamCreateWithPriority(&st, cudaStreamNonBlocking, prio), "stream");
+      job->streams.push_back(st);
+    }
+  }
+  // heaviest chunks first, each onto the least-loaded stream (longest
+  // processing time first); cost ~ one iteration's Gram and render work
+  std::vector<int> order(nch);
+  std::vector<double> cost(nch);
+  for (int i = 0; i < nch; ++i) {
+    const ClassDev& c = job->chunks[i]->c;
+    order[i] = i;
+    cost[i] = (double)c.n_isl * c.nb *
+              ((double)c.B * c.B * c.Kmax + (double)c.N * c.T * c.T * c.R);
+  }
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost[a] > cost[b]; });
+  {
+    std::vector<double> load(nstreams, 0.0);
+    for (int i : order) {
+      const int j = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+      job->chunks[i]->slot = j;
+      load[j] += cost[i];
+    }
   }
   if (job->h_active_cap < nch) {
     if (job->h_active) cudaFreeHost(job->h_active);
@@ -695,11 +728,17 @@ int job_solve(uph_job* job, int max_steps) {
   }
   std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> rec;
   auto* recp = job->profile ? &rec : nullptr;
+  if (job->profile) {
+    if (!job->d_work)
+      CK(cudaMalloc((void**)&job->d_work, sizeof(unsigned long long) * 2 * WK_KINDS), "work");
+    CK(cudaMemsetAsync(job->d_work, 0, sizeof(unsigned long long) * 2 * WK_KINDS,
+                       ctx->stream), "work");
+  }
+  for (auto* ch : job->chunks) ch->c.work = job->profile ? job->d_work : nullptr;
   CK(cudaEventRecord(ctx->ev[0], ctx->stream), "event");
   for (auto st : job->streams) CK(cudaStreamWaitEvent(st, ctx->ev[0], 0), "wait");
-  for (int i = 0; i < nch; ++i) {
+  for (int i : order) {
     Chunk* ch = job->chunks[i];
-    ch->slot = i % nstreams;
     cudaStream_t s = job->streams[ch->slot];
     int rc = reset_chunk(ctx, ch, s);
     if (rc) return rc;
@@ -725,45 +764,68 @@ int job_solve(uph_job* job, int max_steps) {
     if (max_steps == 0) ch->done = true;
   }
   CK(cudaGetLastError(), "launch");
-  // LM loop: every unfinished chunk advances UPH_CHECK_EVERY iterations, then
-  // one host check of the active counts.
-  for (;;) {
-    bool any = false;
-    for (int i = 0; i < nch; ++i) {
-      Chunk* ch = job->chunks[i];
-      if (ch->done) continue;
-      any = true;
-      cudaStream_t s = job->streams[ch->slot];
-      const int group = std::min(UPH_CHECK_EVERY, max_steps - ch->iters);
-      for (int j = 0; j < group; ++j) {
-        if (job->profile) {
-          Launcher L{job, s, recp};
-          iteration(ch->c, L);
-        } else {
-          CK(cudaGraphLaunch(ch->gexec, s), "graph launch");
-          ctx->launches += ch->graph_kernels;
-        }
-      }
-      ch->iters += group;
-      launch_count_active(ch->c, s);
-      ctx->launches += 1;
-      CK(cudaMemcpyAsync(job->h_active + i, ch->c.n_active, sizeof(int),
-                         cudaMemcpyDeviceToHost, s), "count");
-      CK(cudaEventRecord(ch->ev_group, s), "event");
-    }
-    if (!any) break;
-    for (int i = 0; i < nch; ++i) {
-      Chunk* ch = job->chunks[i];
-      if (ch->done) continue;
-      CK(cudaEventSynchronize(ch->ev_group), "lm loop");
-      if (job->h_active[i] == 0 || ch->iters >= max_steps) ch->done = true;
-    }
-  }
-  CK(cudaEventRecord(ctx->ev[1], ctx->stream), "event");
-  for (int i = 0; i < nch; ++i) {
+  // LM loop: every chunk advances in groups of UPH_CHECK_EVERY iterations;
+  // as soon as a group's active count reaches the host, that chunk's next
+  // group -- or, once it has finished, its post-loop probes and final pass --
+  // is enqueued, so no chunk waits for another.
+  std::vector<char> inflight(nch, 0);
+  auto enqueue_group = [&](int i) -> int {
     Chunk* ch = job->chunks[i];
+    cudaStream_t s = job->streams[ch->slot];
+    const int group = std::min(UPH_CHECK_EVERY, max_steps - ch->iters);
+    for (int j = 0; j < group; ++j) {
+      if (job->profile) {
+        Launcher L{job, s, recp};
+        iteration(ch->c, L);
+      } else {
+        CK(cudaGraphLaunch(ch->gexec, s), "graph launch");
+        ctx->launches += ch->graph_kernels;
+      }
+    }
+    ch->iters += group;
+    launch_count_active(ch->c, s);
+    ctx->launches += 1;
+    CK(cudaMemcpyAsync(job->h_active + i, ch->c.n_active, sizeof(int),
+                       cudaMemcpyDeviceToHost, s), "count");
+    CK(cudaEventRecord(ch->ev_group, s), "event");
+    inflight[i] = 1;
+    return UPH_OK;
+  };
+  auto finish = [&](int i) {
+    Chunk* ch = job->chunks[i];
+    ch->done = true;
     Launcher L{job, job->streams[ch->slot], recp};
     post_loop(ch, L);
+  };
+  int live = 0;
+  for (int i : order) {
+    if (job->chunks[i]->done) {
+      finish(i);
+      continue;
+    }
+    int rc = enqueue_group(i);
+    if (rc) return rc;
+    ++live;
+  }
+  while (live > 0) {
+    bool progress = false;
+    for (int i : order) {
+      if (!inflight[i]) continue;
+      Chunk* ch = job->chunks[i];
+      const cudaError_t q = cudaEventQuery(ch->ev_group);
+      if (q == cudaErrorNotReady) continue;
+      if (q != cudaSuccess) return cuda_err(ctx, q, "lm loop");
+      inflight[i] = 0;
+      progress = true;
+      if (job->h_active[i] == 0 || ch->iters >= max_steps) {
+        finish(i);
+        --live;
+      } else {
+        int rc = enqueue_group(i);
+        if (rc) return rc;
+      }
+    }
+    if (!progress) std::this_thread::yield();
   }
   CK(cudaGetLastError(), "post-loop");
   for (auto st : job->streams) {
@@ -783,10 +845,15 @@ int job_solve(uph_job* job, int max_steps) {
   }
   cudaEventElapsedTime(&ctx->timing[1], ctx->ev[0], ctx->ev[2]);
   ctx->timing[2] = 0.f;
+  for (auto* ch : job->chunks) ch->c.work = nullptr;
   if (job->profile) {
-    for (int k = 0; k < 6; ++k) {
+    unsigned long long w[2 * WK_KINDS];
+    CK(cudaMemcpy(w, job->d_work, sizeof w, cudaMemcpyDeviceToHost), "work");
+    for (int k = 0; k < WK_KINDS; ++k) {
       job->ktime[k] = 0.f;
       job->kcount[k] = 0;
+      job->kbytes[k] = (double)w[2 * k];
+      job->kflops[k] = (double)w[2 * k + 1];
     }
     for (auto& r : rec) {
       float ms = 0.f;
@@ -925,9 +992,17 @@ int uph_job_set_profile(uph_job* job, int32_t on) {
 
 int uph_job_kernel_time(const uph_job* job, int32_t kind, float* ms,
                         int64_t* launches) {
-  if (!job || kind < 0 || kind >= 6) return UPH_ERR_INVALID;
+  if (!job || kind < 0 || kind >= WK_KINDS) return UPH_ERR_INVALID;
   if (ms) *ms = job->ktime[kind];
   if (launches) *launches = job->kcount[kind];
+  return UPH_OK;
+}
+
+int uph_job_kernel_work(const uph_job* job, int32_t kind, double* bytes,
+                        double* flops) {
+  if (!job || kind < 0 || kind >= WK_KINDS) return UPH_ERR_INVALID;
+  if (bytes) *bytes = job->kbytes[kind];
+  if (flops) *flops = job->kflops[kind];
   return UPH_OK;
 }
 

@@ -14,12 +14,18 @@
 // pair's representation error are ~2^-16 relative per product).
 //
 // One CTA per (island, band) with K = nL + nr + 1 rows (stored padded to R =
-// 128 * ceil(K / 128) rows); pixels stream through shared memory in chunks
-// of 64, double-buffered: all threads convert chunk c + 1 while the tensor
-// core consumes chunk c.  Operands are K-major (pixels contiguous) in the
-// no-swizzle canonical layout: 8-row x 16-byte core matrices, consecutive
-// 8-row groups 128 B apart (SBO), the two 8-pixel halves of a 16-pixel MMA
-// step R * 16 B apart (LBO).  One elected thread issues M = 128, N = ceil16
+// 128 * ceil(K / 128) rows; the padding rows are zeroed once and never
+// rewritten); pixels stream through shared memory in chunks of 64,
+// double-buffered: all threads convert chunk c + 1 while the tensor core
+// consumes chunk c.  A chunk's window coordinates, weights and residuals are
+// decoded once into shared memory; each lane then converts 8 pixels of one
+// row (8 independent loads) into one 16-byte store per half of the pair,
+// consecutive lanes taking consecutive rows so that a warp fills whole core
+// matrices without bank conflicts.  Shared memory is sized by the class's
+// largest row count, so classes with at most 128 rows fit three CTAs per SM.
+// Operands are K-major (pixels contiguous) in the no-swizzle canonical
+// layout: 8-row x 16-byte core matrices, consecutive 8-row groups 128 B apart
+// (SBO), the two 8-pixel halves of a 16-pixel MMA step R * 16 B apart (LBO).  One elected thread issues M = 128, N = ceil16
 // (K) <= 256, K-step = 16 MMAs; tcgen05.commit arrives on the stage's
 // mbarrier.  Waits are bounded: on expiry the kernel raises the chunk's error
 // flag, drains, frees its tensor memory and returns.
@@ -31,9 +37,17 @@ namespace {
 
 constexpr int NT = 256;
 constexpr int KC = 64;                  // pixels per chunk
-constexpr int RMAX = 256;               // rows per CTA (two M = 128 halves)
-constexpr int STAGE_BYTES = 2 * RMAX * KC * 2;   // Zh + Zl, bf16
+constexpr int NG = KC / 8;              // 8-pixel groups per chunk
 constexpr unsigned SPIN_LIMIT = 1u << 24;
+
+// Stored rows for at most kmax Gram rows (one or two M = 128 halves), and
+// the bytes of one stage (Zh and Zl, bf16).
+__host__ __device__ constexpr int rows_cap(int kmax) { return ((kmax + 127) / 128) * 128; }
+__host__ __device__ constexpr size_t stage_bytes(int rcap) { return (size_t)2 * rcap * KC * 2; }
+
+__device__ __forceinline__ uint32_t pack_bf16(__nv_bfloat16 lo, __nv_bfloat16 hi) {
+  return (uint32_t)__bfloat16_as_ushort(lo) | ((uint32_t)__bfloat16_as_ushort(hi) << 16);
+}
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return (uint32_t)__cvta_generic_to_shared(p);
@@ -99,14 +113,16 @@ __device__ __forceinline__ int gram_rows(const ClassDev& c, int isl) {
   return c.isl_nL[isl] + c.isl_nr[isl] + 1;
 }
 
-__global__ void __launch_bounds__(NT, 1) k_gram_tc(ClassDev c) {
+__global__ void __launch_bounds__(NT) k_gram_tc(ClassDev c, int rcap) {
   extern __shared__ __align__(1024) uint8_t tsm[];
   __shared__ __align__(8) uint64_t mbar[2];
   __shared__ uint32_t tmem_base;
   __shared__ int4 box[UPH_MAXN];
+  __shared__ float fcs[UPH_MAXN];
+  __shared__ int16_t srk[UPH_MAXK], srs[UPH_MAXK];
   __shared__ float swt[2][KC];
   __shared__ float rsd[2][KC];
-  __shared__ float fcs[UPH_MAXN];
+  __shared__ int pwy[2][KC], pwx[2][KC];   // window pixel of each chunk slot
   __shared__ int abort_flag;
   const int isl = blockIdx.x / c.nb, b = blockIdx.x % c.nb;
   if (isl >= c.n_isl || !isl_active(c.flags[isl], PH_LIN)) return;
@@ -126,6 +142,17 @@ __global__ void __launch_bounds__(NT, 1) k_gram_tc(ClassDev c) {
     box[k] = make_int4(mb.wx0, mb.wy0, mb.bw, mb.bh);
     fcs[k] = c.fcur[((size_t)isl * c.nb + b) * c.N + k];
   }
+  for (int r = tid; r < K; r += NT) {
+    srk[r] = rk[r];
+    srs[r] = rs[r];
+  }
+  const size_t sbytes = stage_bytes(rcap);
+  {
+    // rows K..R-1 of both stages stay zero for the whole kernel
+    uint4* z = reinterpret_cast<uint4*>(tsm);
+    const int n16 = (int)(2 * sbytes / 16);
+    for (int i = tid; i < n16; i += NT) z[i] = make_uint4(0u, 0u, 0u, 0u);
+  }
   if (tid == 0) {
     abort_flag = 0;
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[0])) : "memory");
@@ -141,6 +168,7 @@ __global__ void __launch_bounds__(NT, 1) k_gram_tc(ClassDev c) {
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;");
   const uint32_t tbase = tmem_base;
+  if (tid == 0) gram_work(c, WK_GRAM_TC, rk, rs, K, box);
   const int B = c.B, Sz = c.Sz, npix = B * B;
   const size_t plane = (size_t)c.Hp * c.Wp;
   const float* dbase = c.dstack + b * plane + (size_t)c.oy[isl] * c.Wp + c.ox[isl];
@@ -153,8 +181,8 @@ __global__ void __launch_bounds__(NT, 1) k_gram_tc(ClassDev c) {
   int issued[2] = {0, 0}, waited[2] = {0, 0};
   for (int ch = 0; ch < nchunk; ++ch) {
     const int st = ch & 1;
-    uint8_t* zh = tsm + st * STAGE_BYTES;
-    uint8_t* zl = zh + RMAX * KC * 2;
+    uint8_t* zh = tsm + st * sbytes;
+    uint8_t* zl = zh + (size_t)rcap * KC * 2;
     if (ch >= 2) {
       // the MMAs of chunk ch - 2 read this stage: wait for their commit
       if (tid == 0) {
@@ -167,11 +195,13 @@ __global__ void __launch_bounds__(NT, 1) k_gram_tc(ClassDev c) {
     }
     const int pix0 = ch * KC;
     if (tid < KC) {
-      // weights and the weighted residual sqrt(w) (d - sum_k fc_k m_k)
+      // window pixel, sqrt(w) and the weighted residual sqrt(w) (d - sum_k fc_k m_k)
       const int pix = pix0 + tid;
+      int wy = -1, wx = 0;
       float sw = 0.f, rv = 0.f;
       if (pix < npix) {
-        const int wy = pix / B, wx = pix - (pix / B) * B;
+        wy = pix / B;
+        wx = pix - wy * B;
         sw = sqrtf(wbase[(size_t)wy * c.Wp + wx]);
         float model = 0.f;
         for (int k = 0; k < nr; ++k) {
@@ -183,33 +213,50 @@ __global__ void __launch_bounds__(NT, 1) k_gram_tc(ClassDev c) {
         }
         rv = sw * (dbase[(size_t)wy * c.Wp + wx] - model);
       }
+      pwy[st][tid] = wy;
+      pwx[st][tid] = wx;
       swt[st][tid] = sw;
       rsd[st][tid] = rv;
     }
     __syncthreads();
-    for (int e = tid; e < R * KC; e += NT) {
-      const int r = e / KC, q = e - (e / KC) * KC;
-      const int pix = pix0 + q;
-      float v = 0.f;
-      if (r < K && pix < npix) {
-        const int wy = pix / B, wx = pix - (pix / B) * B;
-        const int s = rs[r];
-        if (s < 0) {
-          v = rsd[st][q];
-        } else {
-          const int k = rk[r];
-          const int4 bx = box[k];
-          const int ly = wy - bx.y, lx = wx - bx.x;
-          if (ly >= 0 && ly < bx.w && lx >= 0 && lx < bx.z)
-            v = c.stamps[stamp_slot(c, isl, b, k, s) + (size_t)ly * Sz + lx] * swt[st][q];
+    // warp tiles of (8-pixel group g, 32 consecutive rows); lane = row
+    const int ntile = NG * ((K + 31) >> 5);
+    for (int t = warp; t < ntile; t += NT / 32) {
+      const int g = t & (NG - 1);
+      const int r = (t >> 3) * 32 + lane;
+      if (r >= K) continue;
+      float v[8];
+      const int s = srs[r];
+      if (s < 0) {
+#pragma unroll
+        for (int j = 0; j < 8; ++j) v[j] = rsd[st][g * 8 + j];
+      } else {
+        const int k = srk[r];
+        const int4 bx = box[k];
+        const float* sp = c.stamps + stamp_slot(c, isl, b, k, s);
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          const int q = g * 8 + j;
+          const int ly = pwy[st][q] - bx.y, lx = pwx[st][q] - bx.x;
+          float val = 0.f;
+          if (pwy[st][q] >= 0 && ly >= 0 && ly < bx.w && lx >= 0 && lx < bx.z)
+            val = sp[(size_t)ly * Sz + lx] * swt[st][q];
+          v[j] = val;
         }
       }
-      const __nv_bfloat16 h = __float2bfloat16_rn(v);
-      const __nv_bfloat16 l = __float2bfloat16_rn(v - __bfloat162float(h));
-      const uint32_t off = (uint32_t)(((q >> 3) * (R >> 3) + (r >> 3)) * 128 +
-                                      (r & 7) * 16 + (q & 7) * 2);
-      *reinterpret_cast<__nv_bfloat16*>(zh + off) = h;
-      *reinterpret_cast<__nv_bfloat16*>(zl + off) = l;
+      uint32_t hw[4], lw[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const __nv_bfloat16 h0 = __float2bfloat16_rn(v[2 * j]);
+        const __nv_bfloat16 h1 = __float2bfloat16_rn(v[2 * j + 1]);
+        const __nv_bfloat16 l0 = __float2bfloat16_rn(v[2 * j] - __bfloat162float(h0));
+        const __nv_bfloat16 l1 = __float2bfloat16_rn(v[2 * j + 1] - __bfloat162float(h1));
+        hw[j] = pack_bf16(h0, h1);
+        lw[j] = pack_bf16(l0, l1);
+      }
+      const uint32_t off = (uint32_t)((g * (R >> 3) + (r >> 3)) * 128 + (r & 7) * 16);
+      *reinterpret_cast<uint4*>(zh + off) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
+      *reinterpret_cast<uint4*>(zl + off) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
     }
     // make the generic-proxy stores visible to the tensor core (async proxy)
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -282,13 +329,15 @@ __global__ void __launch_bounds__(NT, 1) k_gram_tc(ClassDev c) {
 
 }  // namespace
 
-size_t gram_tc_smem_bytes() { return (size_t)2 * STAGE_BYTES; }
+size_t gram_tc_smem_bytes(int kmax) { return 2 * stage_bytes(rows_cap(kmax)); }
 
 void launch_gram_tc(const ClassDev& c, cudaStream_t s) {
-  k_gram_tc<<<(unsigned)(c.n_isl * c.nb), NT, gram_tc_smem_bytes(), s>>>(c);
+  const int kmax = c.Kmax < UPH_MAXK ? c.Kmax : UPH_MAXK;
+  k_gram_tc<<<(unsigned)(c.n_isl * c.nb), NT, gram_tc_smem_bytes(kmax), s>>>(
+      c, rows_cap(kmax));
 }
 
 int uph_gram_tc_setup() {
   return (int)cudaFuncSetAttribute(k_gram_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   (int)gram_tc_smem_bytes());
+                                   (int)gram_tc_smem_bytes(UPH_MAXK));
 }

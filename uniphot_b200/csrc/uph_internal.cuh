@@ -124,10 +124,44 @@ struct ClassDev {
   float* probe_p;          // (n_isl, 4, nP) diverged-probe proposals
   int* n_active;
   int* err;                // device error flag (bounded waits that expired)
+  // (WK_KINDS, 2) algorithmic bytes and flops per kernel kind, added by every
+  // working CTA; non-null only during instrumented solves
+  unsigned long long* work;
   int tc_min_rows;         // islands with more Gram rows use the tensor-core Gram
   float reg, pos_step_max, ftol_rel, step_tol;
   int un_freeze;
 };
+
+// Kernel kinds of the instrumented solve (uph_job_kernel_time numbering).
+enum { WK_RENDER = 0, WK_GRAM = 1, WK_ASSEMBLE = 2, WK_STEP = 3, WK_TRIAL = 4,
+       WK_ACCEPT = 5, WK_GRAM_TC = 6, WK_KINDS = 7 };
+
+__device__ __forceinline__ void work_add(const ClassDev& c, int kind,
+                                         unsigned long long bytes,
+                                         unsigned long long flops) {
+  if (c.work) {
+    atomicAdd(c.work + 2 * kind, bytes);
+    if (flops) atomicAdd(c.work + 2 * kind + 1, flops);
+  }
+}
+
+// Algorithmic work of one (island, band) Gram of K rows: every stamp row
+// read over its member's box, data and weights over the window, the K x K
+// result written; K (K + 1) flops per pixel (upper triangle, multiply-add).
+__device__ __forceinline__ void gram_work(const ClassDev& c, int kind,
+                                          const int16_t* rk, const int16_t* rs,
+                                          int K, const int4* box) {
+  if (!c.work) return;
+  unsigned long long px = 0;
+  for (int r = 0; r < K; ++r) {
+    if (rs[r] < 0) continue;
+    const int4 bx = box[rk[r]];
+    px += (unsigned long long)max(bx.z, 0) * (unsigned long long)max(bx.w, 0);
+  }
+  const unsigned long long npix = (unsigned long long)c.B * c.B;
+  work_add(c, kind, 4ull * (px + 2 * npix + (unsigned long long)K * K),
+           (unsigned long long)K * (K + 1) * npix);
+}
 
 __device__ __forceinline__ bool isl_active(uint8_t fl, int phase) {
   switch (phase) {
@@ -193,5 +227,5 @@ size_t gram_trial_smem_bytes(int N);
 size_t assemble_smem_bytes(int nLmax, int N);
 size_t step_smem_bytes(int nLmax);
 void launch_gram_tc(const ClassDev& c, cudaStream_t s);
-size_t gram_tc_smem_bytes();
+size_t gram_tc_smem_bytes(int kmax);
 int uph_kernel_setup();

@@ -453,6 +453,12 @@ k_render(ClassDev c, const float* __restrict__ P, int phase, int nsa) {
   if (oy0 >= mb.wy0 + mb.bh || ox0 >= mb.wx0 + mb.bw) return;
   const int oh = min(UPH_TILE, mb.wy0 + mb.bh - oy0);
   const int ow = min(UPH_TILE, mb.wx0 + mb.bw - ox0);
+  if (tid == 0 && c.work) {
+    int rows = 1;
+    if (lin)
+      for (int j = 0; j < 6; ++j) rows += ms.live_row[j] != 0;
+    work_add(c, WK_RENDER, 4ull * (unsigned long long)(oh * ow * rows), 0);
+  }
   const int si0 = oy0 - mb.iyt, sj0 = ox0 - mb.ixt;  // stamp coords of tile
   const int hr = oh + 6, hc = ow + 6;
   float* S = smem;                           // NS * UPH_HALO * HP

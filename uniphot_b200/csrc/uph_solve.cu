@@ -255,6 +255,9 @@ __global__ void __launch_bounds__(NT) k_gram_lin(ClassDev c) {
   if (nblk <= NT && blockIdx.y > 0) return;
   load_boxes(c, isl, c.p, box);
   __syncthreads();
+  if (threadIdx.x == 0 && blockIdx.y == 0)
+    gram_work(c, WK_GRAM, c.row_k + (size_t)isl * c.Kmax, c.row_s + (size_t)isl * c.Kmax,
+              K, box);
   RowSrc rows{c.row_k + (size_t)isl * c.Kmax, c.row_s + (size_t)isl * c.Kmax, K};
   gram_window(c, isl, b, rows, box,
               c.gram + ((size_t)isl * c.nb + b) * c.Kmax * c.Kmax, c.Kmax,
@@ -339,6 +342,8 @@ __global__ void __launch_bounds__(NT) k_assemble(ClassDev c) {
   //   f = fc + (A + reg I)^-1 (M W r - reg fc),
   //   D W (d - M^T x) = D W r + D W M^T (fc - x),
   //   M W d - A x     = M W r + A (fc - x).
+  if (tid == 0)
+    work_add(c, WK_ASSEMBLE, 4ull * (unsigned long long)(K * K + nL * nL + nL), 0);
   const bool resid = K > c.tc_min_rows;
   const float* fc = resid ? c.fcur + ((size_t)isl * c.nb + b) * c.N : nullptr;
   for (int e = tid; e < nr * ncol; e += NT) {
@@ -460,6 +465,12 @@ k_gram_trial(ClassDev c, const float* __restrict__ P, int phase,
     rs[r] = (int16_t)(r < nr ? 0 : -1);
   }
   __syncthreads();
+  if (tid == 0 && c.work) {
+    unsigned long long px = 0;
+    for (int k = 0; k < nr; ++k)
+      px += (unsigned long long)max(box[k].z, 0) * (unsigned long long)max(box[k].w, 0);
+    work_add(c, WK_TRIAL, 4ull * (px + 2ull * c.B * c.B) + 8ull, 0);
+  }
   RowSrc rows{rk, rs, K};
   gram_window(c, isl, b, rows, box, gmm, K, 0, sm);
   __syncthreads();
@@ -607,6 +618,12 @@ k_step(ClassDev c, int phase, int probe_mode, int probe_j, float probe_lam) {
   float* H = c.H + (size_t)isl * ldH * ldH;
   float* g = c.g + (size_t)isl * ldH;
   const int16_t* rp = c.row_p + (size_t)isl * c.Kmax;
+  if (tid == 0 && c.work) {
+    const unsigned long long hl = (unsigned long long)(nL * nL + nL);
+    const bool sum = probe_mode == 0 && (fl & FL_NEEDLIN);
+    work_add(c, WK_STEP, 4ull * ((sum ? c.nb + 1 : 1) * hl + 2ull * nP),
+             (unsigned long long)(2.0 * nL * nL * nL / 3.0));
+  }
   if (probe_mode == 0 && (fl & FL_NEEDLIN)) {
     for (int e = tid; e < nL * nL; e += NT) {
       const int i = e / nL, j = e - (e / nL) * nL;
@@ -707,6 +724,7 @@ __global__ void k_accept(ClassDev c, int phase) {
   if (!isl_active(fl, phase)) return;
   const int nP = c.nP;
   const float* pt = c.p_try + (size_t)isl * nP;
+  work_add(c, WK_ACCEPT, 8ull * c.nb + 8ull * nP, 0);
   float chi2_try = 0.f;
   for (int b = 0; b < c.nb; ++b)
     chi2_try = __fadd_rn(chi2_try, (float)c.chi2b[(size_t)isl * c.nb + b]);
