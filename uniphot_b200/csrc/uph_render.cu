@@ -40,8 +40,51 @@ struct MemberSetup {
 };
 
 // Pruning threshold: a Gaussian term whose Mahalanobis distance Q exceeds
-// this everywhere on a tile contributes < exp(-69) ~ 1e-30 of its norm there.
-constexpr float QCUT = 138.f;
+// this everywhere on a tile contributes < exp(-23) ~ 1e-10 of its norm there
+// (its derivative rows at most a factor ~Q more), far below the float32
+// resolution of the pixels it would touch relative to the member's peak.
+constexpr float QCUT = 46.f;
+
+// Per-tile record of one active analytic component: the exponent
+// coefficients (Q' = qa x^2 + qb x y + qc y^2, value = nrm 2^Q') and, for the
+// linearisation, one quadratic form per derivative row so that
+//   row_o = sum_comp 2^Q' (a_o x^2 + b_o x y + c_o y^2 + d_o).
+// Rows o = 0..5 are S arrays 1..6 (x, y, log r_e, e1, e2, Sersic n): the
+// covariance derivatives dQ/dA, dQ/dC, dQ/dB of the exponential are quadratic
+// forms, and the member's d(cov)/d(shape) and d n / d u are folded in.
+constexpr int MAXCOMP = UPH_MAXKPSF * UPH_MAXGAL;
+constexpr float KEXP = -0.72134752044448170f;   // -1 / (2 ln 2)
+
+template <int NOUT>
+__device__ __forceinline__ void mog_pair(const float4* __restrict__ rec, int na,
+                                         float x2a, float xya, float y2a,
+                                         float x2b, float xyb, float y2b,
+                                         float* va, float* vb) {
+  float s0a = 0.f, s0b = 0.f;
+  float aa[NOUT > 0 ? NOUT : 1], ab[NOUT > 0 ? NOUT : 1];
+#pragma unroll
+  for (int o = 0; o < NOUT; ++o) aa[o] = ab[o] = 0.f;
+  for (int a = 0; a < na; ++a) {
+    const float4 q = rec[a * (NOUT + 1)];
+    const float ea = exp2f(fmaf(q.x, x2a, fmaf(q.y, xya, q.z * y2a)));
+    const float eb = exp2f(fmaf(q.x, x2b, fmaf(q.y, xyb, q.z * y2b)));
+    s0a = fmaf(q.w, ea, s0a);
+    s0b = fmaf(q.w, eb, s0b);
+#pragma unroll
+    for (int o = 0; o < NOUT; ++o) {
+      const float4 k = rec[a * (NOUT + 1) + 1 + o];
+      aa[o] = fmaf(ea, fmaf(k.x, x2a, fmaf(k.y, xya, fmaf(k.z, y2a, k.w))), aa[o]);
+      ab[o] = fmaf(eb, fmaf(k.x, x2b, fmaf(k.y, xyb, fmaf(k.z, y2b, k.w))), ab[o]);
+    }
+  }
+  va[0] = s0a;
+  vb[0] = s0b;
+#pragma unroll
+  for (int o = 0; o < NOUT; ++o) {
+    va[1 + o] = aa[o];
+    vb[1 + o] = ab[o];
+  }
+}
 
 // Minimum over the rectangle [x0,x1] x [y0,y1] of
 // Q = ia x^2 + 2 ib x y + ic y^2 (positive definite).
@@ -389,6 +432,7 @@ k_render(ClassDev c, const float* __restrict__ P, int phase, int nsa) {
   extern __shared__ float smem[];
   __shared__ MemberSetup ms;
   __shared__ GComp comps[UPH_MAXKPSF * UPH_MAXGAL];
+  __shared__ float4 trec[MAXCOMP * 7];   // per-tile component records
   __shared__ MemberBox mb;
   const int ntile = c.ntile_side * c.ntile_side;
   int t = blockIdx.x;
@@ -489,6 +533,42 @@ k_render(ClassDev c, const float* __restrict__ P, int phase, int nsa) {
     __syncthreads();
     empty = (ms.nact == 0);
   }
+  // analytic records: 0 derivative rows (trial), 2 (star: x, y) or 6
+  int nout = 0;
+  if (lin) nout = ms.is_gal ? 6 : ((ms.need[1] || ms.need[2]) ? 2 : 0);
+  if (!empty && c.mode == 1) {
+    for (int a = tid; a < ms.nact; a += blockDim.x) {
+      const GComp& o = comps[ms.act[a]];
+      float4* r = trec + a * (nout + 1);
+      r[0] = make_float4(KEXP * o.ia, 2.f * KEXP * o.ib, KEXP * o.ic, o.nrm);
+      if (nout == 0) continue;
+      const float i2d = o.det;   // holds 0.5 / det
+      // dA, dC, dB of the covariance-derivative chain as quadratic forms
+      const float4 PA = make_float4(i2d * o.C * o.ia, i2d * 2.f * o.C * o.ib,
+                                    i2d * (o.C * o.ic - 1.f), -i2d * o.C);
+      const float4 PC = make_float4(i2d * (o.A * o.ia - 1.f), i2d * 2.f * o.A * o.ib,
+                                    i2d * o.A * o.ic, -i2d * o.A);
+      const float t2 = 2.f * i2d;
+      const float4 PB = make_float4(-t2 * o.B * o.ia, t2 * (1.f - 2.f * o.B * o.ib),
+                                    -t2 * o.B * o.ic, t2 * o.B);
+      auto comb = [&](float wa, float wc, float wb, float s, float add) {
+        return make_float4(s * (wa * PA.x + wc * PC.x + wb * PB.x),
+                           s * (wa * PA.y + wc * PC.y + wb * PB.y),
+                           s * (wa * PA.z + wc * PC.z + wb * PB.z),
+                           s * (wa * PA.w + wc * PC.w + wb * PB.w) + add);
+      };
+      r[1] = comb(o.dAx, o.dCx, o.dBx, o.nrm, o.nx);
+      r[2] = comb(o.dAy, o.dCy, o.dBy, o.nrm, o.ny);
+      if (nout == 6) {
+        const float nv = o.nrm * o.v;
+        for (int q = 0; q < 3; ++q)
+          r[3 + q] = comb(ms.dcov[q][0], ms.dcov[q][1], ms.dcov[q][2], nv, 0.f);
+        const float4 u = comb(ms.cg[0], ms.cg[1], ms.cg[2], o.nrm * o.dv, o.nu);
+        r[6] = make_float4(ms.dndu * u.x, ms.dndu * u.y, ms.dndu * u.z, ms.dndu * u.w);
+      }
+    }
+    __syncthreads();
+  }
   if (empty) {
     // every value on this tile is zero: write the zeros and stop
     for (int e = tid; e < oh * ow; e += blockDim.x) {
@@ -503,62 +583,64 @@ k_render(ClassDev c, const float* __restrict__ P, int phase, int nsa) {
   }
 
   // ---- un-shifted stamp (and partials) on the halo region ----
-  for (int e = tid; e < hr * hc; e += blockDim.x) {
-    const int r = e / hc, cc = e % hc;
-    const int si = si0 - 3 + r, sj = sj0 - 3 + cc;
-    float v[NS] = {0, 0, 0, 0, 0, 0, 0};
-    if (si >= 0 && si < T && sj >= 0 && sj < T && abs(si - c0) <= hs &&
-        abs(sj - c0) <= hs) {
-      if (c.mode == 0) {
+  const int nh = hr * hc;
+  if (c.mode == 0) {
+    for (int e = tid; e < nh; e += blockDim.x) {
+      const int r = e / hc, cc = e % hc;
+      const int si = si0 - 3 + r, sj = sj0 - 3 + cc;
+      float v0 = 0.f, v1 = 0.f, v2 = 0.f;
+      if (si >= 0 && si < T && sj >= 0 && sj < T && abs(si - c0) <= hs &&
+          abs(sj - c0) <= hs) {
         const float* cf = c.psf_coefs + (((size_t)b * T + si) * T + sj) * c.nt;
-        float s0 = 0.f, sx = 0.f, sy = 0.f;
         for (int tt = 0; tt < c.nt; ++tt) {
           const float cv = cf[tt];
-          s0 = fmaf(cv, ms.beta[tt], s0);
-          sx = fmaf(cv, ms.betax[tt], sx);
-          sy = fmaf(cv, ms.betay[tt], sy);
+          v0 = fmaf(cv, ms.beta[tt], v0);
+          v1 = fmaf(cv, ms.betax[tt], v1);
+          v2 = fmaf(cv, ms.betay[tt], v2);
         }
-        v[0] = s0;
-        v[1] = sx;
-        v[2] = sy;
-      } else {
+      }
+      S[(0 * UPH_HALO + r) * HP + cc] = v0;
+      if (ms.need[1]) S[(1 * UPH_HALO + r) * HP + cc] = v1;
+      if (ms.need[2]) S[(2 * UPH_HALO + r) * HP + cc] = v2;
+    }
+  } else {
+    // two halo pixels per thread share every component record
+    const int step = 2 * blockDim.x;
+    for (int e0 = tid; e0 < nh; e0 += step) {
+      const int e1 = e0 + blockDim.x;
+      bool ok[2];
+      float x2[2], xy[2], y2[2];
+      int rr[2], cs[2];
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int e = h ? e1 : e0;
+        rr[h] = e / hc;
+        cs[h] = e - rr[h] * hc;
+        const int si = si0 - 3 + rr[h], sj = sj0 - 3 + cs[h];
+        ok[h] = e < nh && si >= 0 && si < T && sj >= 0 && sj < T && abs(si - c0) <= hs &&
+                abs(sj - c0) <= hs;
         const float xo = (float)(sj - c0), yo = (float)(si - c0);
-        float s0 = 0.f, sx = 0.f, sy = 0.f, gA = 0.f, gB = 0.f, gC = 0.f,
-              u1 = 0.f, u2 = 0.f;
-        for (int a = 0; a < ms.nact; ++a) {
-          const GComp& o = comps[ms.act[a]];
-          const float Q = fmaf(o.ia * xo, xo, fmaf(2.f * o.ib * xo, yo, o.ic * yo * yo));
-          // exp(-Q/2) as one base-2 exponential
-          const float ex = exp2f(Q * -0.72134752044448170f);
-          const float nw = o.nrm * ex;
-          s0 += nw;
-          if (lin) {
-            const float i2d = o.det;   // holds 0.5 / det
-            const float dA = (Q * o.C - yo * yo - o.C) * i2d;
-            const float dC = (Q * o.A - xo * xo - o.A) * i2d;
-            const float dB = (xo * yo - o.B * Q + o.B) * (2.f * i2d);
-            if (ms.need[1]) sx += o.nx * ex + nw * (dA * o.dAx + dC * o.dCx + dB * o.dBx);
-            if (ms.need[2]) sy += o.ny * ex + nw * (dA * o.dAy + dC * o.dCy + dB * o.dBy);
-            if (ms.is_gal) {
-              const float nv = nw * o.v;
-              gA = fmaf(nv, dA, gA);
-              gC = fmaf(nv, dC, gC);
-              gB = fmaf(nv, dB, gB);
-              u1 = fmaf(o.nu, ex, u1);
-              u2 += nw * o.dv * (dA * ms.cg[0] + dC * ms.cg[1] + dB * ms.cg[2]);
-            }
-          }
-        }
-        v[0] = s0;
-        v[1] = sx;
-        v[2] = sy;
-        for (int s = 0; s < 3; ++s)
-          v[3 + s] = gA * ms.dcov[s][0] + gC * ms.dcov[s][1] + gB * ms.dcov[s][2];
-        v[6] = ms.dndu * (u1 + u2);
+        x2[h] = xo * xo;
+        xy[h] = xo * yo;
+        y2[h] = yo * yo;
+      }
+      float va[NS], vb[NS];
+      if (nout == 6)
+        mog_pair<6>(trec, ms.nact, x2[0], xy[0], y2[0], x2[1], xy[1], y2[1], va, vb);
+      else if (nout == 2)
+        mog_pair<2>(trec, ms.nact, x2[0], xy[0], y2[0], x2[1], xy[1], y2[1], va, vb);
+      else
+        mog_pair<0>(trec, ms.nact, x2[0], xy[0], y2[0], x2[1], xy[1], y2[1], va, vb);
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        if ((h ? e1 : e0) >= nh) continue;
+        const float* v = h ? vb : va;
+        const int r = rr[h], cc = cs[h];
+        S[(0 * UPH_HALO + r) * HP + cc] = ok[h] ? v[0] : 0.f;
+        for (int q = 1; q <= nout; ++q)
+          if (ms.need[q]) S[(q * UPH_HALO + r) * HP + cc] = ok[h] ? v[q] : 0.f;
       }
     }
-    for (int s = 0; s < NS; ++s)
-      if (ms.need[s]) S[(s * UPH_HALO + r) * HP + cc] = v[s];
   }
   __syncthreads();
 
