@@ -203,6 +203,9 @@ int uph_job_kernel_time(const uph_job* job, int32_t kind, float* ms,
  * Gram's K (K + 1) per window pixel; the step's 2/3 nL^3 LU). */
 int uph_job_kernel_work(const uph_job* job, int32_t kind, double* bytes,
                         double* flops);
+/* Device time from the start of the last uph_job_solve to the end of one
+ * chunk's work (its LM iterations, probes and final pass), in ms. */
+int uph_job_chunk_time(const uph_job* job, int32_t chunk_id, float* ms);
 
 /* ---- Allocation-free final-flux pass.  No counterpart in the reference:
  * it exists for callers that cannot call cudaMalloc (a host inside a

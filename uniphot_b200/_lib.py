@@ -25,7 +25,8 @@ EXPORTED = ("uph_create", "uph_destroy", "uph_last_error", "uph_set_stream",
             "uph_upload_sersic_table", "uph_run_chunk", "uph_last_timing",
             "uph_last_launch_count", "uph_job_create", "uph_job_destroy",
             "uph_job_add_chunk", "uph_job_solve", "uph_job_read",
-            "uph_job_set_profile", "uph_job_kernel_time", "uph_job_kernel_work")
+            "uph_job_set_profile", "uph_job_kernel_time", "uph_job_kernel_work",
+            "uph_job_chunk_time")
 KERNEL_KINDS = ("render", "gram", "assemble", "step", "trial_chi2", "accept",
                 "gram_tc")
 
@@ -100,6 +101,7 @@ def lib():
                                           C.POINTER(C.c_int64)]
         L.uph_job_kernel_work.argtypes = [_P, C.c_int32, C.POINTER(C.c_double),
                                           C.POINTER(C.c_double)]
+        L.uph_job_chunk_time.argtypes = [_P, C.c_int32, C.POINTER(C.c_float)]
         _lib = L
     return _lib
 
@@ -305,6 +307,13 @@ class Job:
             lib().uph_job_kernel_time(self._h, i, C.byref(ms), C.byref(cnt))
             res[name] = (float(ms.value), int(cnt.value))
         return res
+
+    def chunk_time(self, chunk_id: int) -> float:
+        """ms from the start of the last solve to the end of one chunk."""
+        ms = C.c_float(0)
+        self.ctx.check(lib().uph_job_chunk_time(self._h, int(chunk_id), C.byref(ms)),
+                       "uph_job_chunk_time")
+        return float(ms.value)
 
     def kernel_work(self) -> dict:
         """Algorithmic (bytes, flops) per kernel kind of the last

@@ -68,6 +68,7 @@ struct uph_ctx {
   cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
   float timing[4] = {0, 0, 0, 0};
   int64_t launches = 0;
+  int sm_count = 148;
 };
 
 namespace {
@@ -136,6 +137,8 @@ int uph_create(int device, uph_ctx** out) {
   if (e != cudaSuccess) return UPH_ERR_CUDA;
   uph_ctx* ctx = new uph_ctx();
   ctx->device = device;
+  cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, device);
+  if (ctx->sm_count <= 0) ctx->sm_count = 148;
   if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
     delete ctx;
     return UPH_ERR_CUDA;
@@ -332,6 +335,8 @@ struct Chunk {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t gexec = nullptr;
   cudaEvent_t ev_group = nullptr;
+  cudaEvent_t ev_done = nullptr;   // end of the chunk's last solve (timed)
+  float done_ms = 0.f;             // its time from the solve's start
   bool done = false;
   int iters = 0;
   int slot = 0;
@@ -340,6 +345,7 @@ struct Chunk {
     if (gexec) cudaGraphExecDestroy(gexec);
     if (graph) cudaGraphDestroy(graph);
     if (ev_group) cudaEventDestroy(ev_group);
+    if (ev_done) cudaEventDestroy(ev_done);
     for (auto& kv : bufs) kv.second.release();
   }
 };
@@ -400,7 +406,8 @@ void iteration(const ClassDev& c, Launcher& L) {
   cudaStream_t s = L.s;
   L(0, [&] { launch_render(c, c.p, PH_LIN, s); }, 2);
   L(1, [&] { launch_gram_lin(c, s); });
-  if (c.tc_min_rows < (1 << 30)) L(WK_GRAM_TC, [&] { launch_gram_tc(c, s); });
+  if (c.tc_min_rows < (1 << 30))
+    L(WK_GRAM_TC, [&] { launch_gram_tc(c, s); }, c.tc_split > 1 ? 2 : 1);
   L(2, [&] { launch_assemble(c, s); });
   L(3, [&] { launch_step(c, PH_TRIAL, 0, 0.f, 0, s); });
   L(0, [&] { launch_render(c, c.p_try, PH_TRIAL, s); }, 2);
@@ -575,7 +582,7 @@ int add_chunk(uph_ctx* ctx, Chunk* ch, const uph_class_desc* cls,
   c.gb = cbuf<float>(ctx, ch, "gb", (size_t)n * nb * nLmax, &rc);
   c.H = cbuf<float>(ctx, ch, "H", (size_t)n * nLmax * nLmax, &rc);
   c.g = cbuf<float>(ctx, ch, "g", (size_t)n * nLmax, &rc);
-  c.lu = cbuf<double>(ctx, ch, "lu", nLmax > 72 ? (size_t)n * nLmax * (nLmax + 1) : 1, &rc);
+  c.lu = cbuf<double>(ctx, ch, "lu", nLmax > UPH_LU_SMEM_N ? (size_t)n * nLmax * (nLmax + 1) : 1, &rc);
   c.chi2b = cbuf<double>(ctx, ch, "chi2b", (size_t)n * nb, &rc);
   c.flux = cbuf<float>(ctx, ch, "flux", (size_t)n * nb * N, &rc);
   c.ferr = cbuf<float>(ctx, ch, "ferr", (size_t)n * nb * N, &rc);
@@ -584,9 +591,13 @@ int add_chunk(uph_ctx* ctx, Chunk* ch, const uph_class_desc* cls,
   c.probe_p = cbuf<float>(ctx, ch, "probep", (size_t)n * 4 * nP, &rc);
   c.n_active = cbuf<int>(ctx, ch, "nact", 1, &rc);
   c.err = cbuf<int>(ctx, ch, "err", 1, &rc);
+  c.tc_split = 1;
   if (c.tc_min_rows < (1 << 30)) {
     c.fcur = cbuf<float>(ctx, ch, "fcur", (size_t)n * nb * N, &rc);
     c.ftry = cbuf<float>(ctx, ch, "ftry", (size_t)n * nb * N, &rc);
+    c.tc_split = gram_tc_splits(n, nb, B, ctx->sm_count);
+    if (c.tc_split > 1)
+      c.gpart = cbuf<float>(ctx, ch, "gpart", (size_t)c.tc_split * n * nb * Kmax * Kmax, &rc);
   }
   ch->d_div = cbuf<uint8_t>(ctx, ch, "div", n, &rc);
   if (rc) return rc;
@@ -641,6 +652,7 @@ int add_chunk(uph_ctx* ctx, Chunk* ch, const uph_class_desc* cls,
   CK(cudaMemsetAsync(c.stamps, 0, sizeof(float) * (size_t)n * nb * N * R * Sz * Sz,
                      ctx->stream), "memset");
   CK(cudaEventCreateWithFlags(&ch->ev_group, cudaEventDisableTiming), "event");
+  CK(cudaEventCreate(&ch->ev_done), "event");
   return UPH_OK;
 }
 
@@ -796,6 +808,7 @@ int job_solve(uph_job* job, int max_steps) {
     ch->done = true;
     Launcher L{job, job->streams[ch->slot], recp};
     post_loop(ch, L);
+    cudaEventRecord(ch->ev_done, job->streams[ch->slot]);
   };
   int live = 0;
   for (int i : order) {
@@ -844,6 +857,7 @@ int job_solve(uph_job* job, int max_steps) {
                           "a bounded device wait expired in chunk %d (tensor-core Gram)", i);
   }
   cudaEventElapsedTime(&ctx->timing[1], ctx->ev[0], ctx->ev[2]);
+  for (auto* ch : job->chunks) cudaEventElapsedTime(&ch->done_ms, ctx->ev[0], ch->ev_done);
   ctx->timing[2] = 0.f;
   for (auto* ch : job->chunks) ch->c.work = nullptr;
   if (job->profile) {
@@ -995,6 +1009,13 @@ int uph_job_kernel_time(const uph_job* job, int32_t kind, float* ms,
   if (!job || kind < 0 || kind >= WK_KINDS) return UPH_ERR_INVALID;
   if (ms) *ms = job->ktime[kind];
   if (launches) *launches = job->kcount[kind];
+  return UPH_OK;
+}
+
+int uph_job_chunk_time(const uph_job* job, int32_t chunk_id, float* ms) {
+  if (!job || !ms || chunk_id < 0 || chunk_id >= (int)job->chunks.size())
+    return UPH_ERR_INVALID;
+  *ms = job->chunks[chunk_id]->done_ms;
   return UPH_OK;
 }
 

@@ -31,6 +31,8 @@
 // flag, drains, frees its tensor memory and returns.
 #include <cuda_bf16.h>
 
+#include <algorithm>
+
 #include "uph_internal.cuh"
 
 namespace {
@@ -124,7 +126,9 @@ __global__ void __launch_bounds__(NT) k_gram_tc(ClassDev c, int rcap) {
   __shared__ float rsd[2][KC];
   __shared__ int pwy[2][KC], pwx[2][KC];   // window pixel of each chunk slot
   __shared__ int abort_flag;
-  const int isl = blockIdx.x / c.nb, b = blockIdx.x % c.nb;
+  const int split = blockIdx.x % c.tc_split;
+  const int ib = blockIdx.x / c.tc_split;
+  const int isl = ib / c.nb, b = ib % c.nb;
   if (isl >= c.n_isl || !isl_active(c.flags[isl], PH_LIN)) return;
   const int K = gram_rows(c, isl);
   if (K <= c.tc_min_rows) return;            // handled by k_gram_lin
@@ -168,23 +172,26 @@ __global__ void __launch_bounds__(NT) k_gram_tc(ClassDev c, int rcap) {
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;");
   const uint32_t tbase = tmem_base;
-  if (tid == 0) gram_work(c, WK_GRAM_TC, rk, rs, K, box);
+  if (tid == 0 && split == 0) gram_work(c, WK_GRAM_TC, rk, rs, K, box);
   const int B = c.B, Sz = c.Sz, npix = B * B;
   const size_t plane = (size_t)c.Hp * c.Wp;
   const float* dbase = c.dstack + b * plane + (size_t)c.oy[isl] * c.Wp + c.ox[isl];
   const float* wbase = c.wstack + b * plane + (size_t)c.oy[isl] * c.Wp + c.ox[isl];
   const int nchunk = (npix + KC - 1) / KC;
+  const int cps = (nchunk + c.tc_split - 1) / c.tc_split;   // chunks per split
+  const int ch0 = split * cps, ch1 = min(nchunk, ch0 + cps);
   const uint32_t idesc = umma_idesc(N);
   const uint32_t lbo = (uint32_t)R * 16u;    // between the two 8-pixel halves
   const uint32_t sbo = 128u;                 // between 8-row groups
   uint32_t phase[2] = {0u, 0u};   // next parity to wait for, per stage
   int issued[2] = {0, 0}, waited[2] = {0, 0};
-  for (int ch = 0; ch < nchunk; ++ch) {
-    const int st = ch & 1;
+  for (int ch = ch0; ch < ch1; ++ch) {
+    const int lc = ch - ch0;   // chunk index within this split
+    const int st = lc & 1;
     uint8_t* zh = tsm + st * sbytes;
     uint8_t* zl = zh + (size_t)rcap * KC * 2;
-    if (ch >= 2) {
-      // the MMAs of chunk ch - 2 read this stage: wait for their commit
+    if (lc >= 2) {
+      // the MMAs of chunk lc - 2 read this stage: wait for their commit
       if (tid == 0) {
         if (!mbar_wait(&mbar[st], phase[st])) abort_flag = 1;
         phase[st] ^= 1u;
@@ -269,7 +276,7 @@ __global__ void __launch_bounds__(NT) k_gram_tc(ClassDev c, int rcap) {
         for (int h = 0; h < Mh; ++h) {
           const uint32_t moff = (uint32_t)(h * 16) * 128u;
           const uint32_t dt = tbase + (uint32_t)(h * N);
-          const uint32_t acc0 = (ch > 0 || s > 0) ? 1u : 0u;
+          const uint32_t acc0 = (lc > 0 || s > 0) ? 1u : 0u;
           mma_bf16(dt, umma_desc(ah + koff + moff, lbo, sbo),
                    umma_desc(ah + koff, lbo, sbo), idesc, acc0);
           mma_bf16(dt, umma_desc(ah + koff + moff, lbo, sbo),
@@ -300,7 +307,9 @@ __global__ void __launch_bounds__(NT) k_gram_tc(ClassDev c, int rcap) {
   if (abort_flag) {
     if (tid == 0) atomicExch(c.err, 1);
   } else if (warp < 4) {
-    float* out = c.gram + ((size_t)isl * c.nb + b) * c.Kmax * c.Kmax;
+    float* out = (c.tc_split > 1 ? c.gpart + (size_t)split * c.n_isl * c.nb * c.Kmax * c.Kmax
+                                  : c.gram) +
+                 ((size_t)isl * c.nb + b) * c.Kmax * c.Kmax;
     const int ld = c.Kmax;
     for (int h = 0; h < Mh; ++h) {
       const int row = h * 128 + warp * 32 + lane;
@@ -317,7 +326,7 @@ __global__ void __launch_bounds__(NT) k_gram_tc(ClassDev c, int rcap) {
         asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
         if (row < K)
           for (int j = 0; j < 16; ++j)
-            if (c0 + j < K) out[row * ld + c0 + j] = __uint_as_float(v[j]);
+            if (c0 + j < K) out[row * ld + c0 + j] = ch1 > ch0 ? __uint_as_float(v[j]) : 0.f;
       }
     }
   }
@@ -327,14 +336,43 @@ __global__ void __launch_bounds__(NT) k_gram_tc(ClassDev c, int rcap) {
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase), "r"(ncols));
 }
 
+// Sum of the tc_split partial Grams of every tensor-core island, in split
+// order (deterministic), into the chunk's Gram.
+__global__ void __launch_bounds__(NT) k_gram_tc_reduce(ClassDev c) {
+  const int isl = blockIdx.x / c.nb, b = blockIdx.x % c.nb;
+  if (isl >= c.n_isl || !isl_active(c.flags[isl], PH_LIN)) return;
+  const int K = gram_rows(c, isl);
+  if (K <= c.tc_min_rows) return;
+  const size_t mat = (size_t)c.Kmax * c.Kmax;
+  const size_t stride = (size_t)c.n_isl * c.nb * mat;
+  const float* src = c.gpart + ((size_t)isl * c.nb + b) * mat;
+  float* dst = c.gram + ((size_t)isl * c.nb + b) * mat;
+  for (int e = threadIdx.x; e < K * K; e += NT) {
+    const int r = e / K, q = e - (e / K) * K;
+    const size_t o = (size_t)r * c.Kmax + q;
+    float t = src[o];
+    for (int sp = 1; sp < c.tc_split; ++sp) t += src[sp * stride + o];
+    dst[o] = t;
+  }
+}
+
 }  // namespace
+
+int gram_tc_splits(int n_isl, int nb, int B, int sm_count) {
+  // enough CTAs for about four per SM, each over at least 8 pixel chunks
+  const int nchunk = (B * B + KC - 1) / KC;
+  const int cap = std::max(1, std::min(16, nchunk / 8));
+  const int want = (4 * sm_count + n_isl * nb - 1) / (n_isl * nb);
+  return std::max(1, std::min(cap, want));
+}
 
 size_t gram_tc_smem_bytes(int kmax) { return 2 * stage_bytes(rows_cap(kmax)); }
 
 void launch_gram_tc(const ClassDev& c, cudaStream_t s) {
   const int kmax = c.Kmax < UPH_MAXK ? c.Kmax : UPH_MAXK;
-  k_gram_tc<<<(unsigned)(c.n_isl * c.nb), NT, gram_tc_smem_bytes(kmax), s>>>(
+  k_gram_tc<<<(unsigned)(c.n_isl * c.nb * c.tc_split), NT, gram_tc_smem_bytes(kmax), s>>>(
       c, rows_cap(kmax));
+  if (c.tc_split > 1) k_gram_tc_reduce<<<(unsigned)(c.n_isl * c.nb), NT, 0, s>>>(c);
 }
 
 int uph_gram_tc_setup() {

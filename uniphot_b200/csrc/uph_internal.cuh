@@ -17,6 +17,7 @@
 #define UPH_MAXN 32          // member slots per island handled on the device
 #define UPH_MAXLIVE 192      // live nonlinear parameters per island
 #define UPH_MAXK (UPH_MAXLIVE + UPH_MAXN + 1)
+#define UPH_LU_SMEM_N 160    // damped systems up to this size factor in shared memory
 #define UPH_MAXKPSF 8        // Gaussian components of an analytic PSF
 #define UPH_MAXNT 21         // polynomial terms (order 5)
 #define UPH_MAXGAL 16        // Sersic table components + delta core
@@ -128,6 +129,10 @@ struct ClassDev {
   // working CTA; non-null only during instrumented solves
   unsigned long long* work;
   int tc_min_rows;         // islands with more Gram rows use the tensor-core Gram
+  int tc_split;            // CTAs per (island, band) of the tensor-core Gram,
+                           // each over a contiguous range of pixel chunks
+  float* gpart;            // (tc_split, n_isl, nb, Kmax, Kmax) partial Grams
+                           // (tc_split > 1), summed in split order
   float reg, pos_step_max, ftol_rel, step_tol;
   int un_freeze;
 };
@@ -228,4 +233,5 @@ size_t assemble_smem_bytes(int nLmax, int N);
 size_t step_smem_bytes(int nLmax);
 void launch_gram_tc(const ClassDev& c, cudaStream_t s);
 size_t gram_tc_smem_bytes(int kmax);
+int gram_tc_splits(int n_isl, int nb, int B, int sm_count);
 int uph_kernel_setup();

@@ -547,21 +547,31 @@ k_gram_trial(ClassDev c, const float* __restrict__ P, int phase,
 
 // LU with partial pivoting of the n x (n+1) augmented system in M (pitch
 // n+1); the solution overwrites column n.
-__device__ void lu_solve(double* M, int n, int* piv, double* fac_g) {
-  const int tid = threadIdx.x;
+__device__ void lu_solve(double* M, int n, int* piv, double* x) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int nw = blockDim.x >> 5;
   const int ld = n + 1;
   for (int col = 0; col < n; ++col) {
-    if (tid == 0) {
+    // pivot: the first row (in row order) of largest |M[r][col]|, r >= col
+    if (warp == 0) {
+      double best = -1.0;
       int p = col;
-      double best = fabs(M[col * ld + col]);
-      for (int r = col + 1; r < n; ++r) {
-        double v = fabs(M[r * ld + col]);
+      for (int r = col + lane; r < n; r += 32) {
+        const double v = fabs(M[r * ld + col]);
         if (v > best) {
           best = v;
           p = r;
         }
       }
-      *piv = p;
+      for (int off = 16; off > 0; off >>= 1) {
+        const double ob = __shfl_down_sync(0xffffffffu, best, off);
+        const int op = __shfl_down_sync(0xffffffffu, p, off);
+        if (ob > best || (ob == best && op < p)) {
+          best = ob;
+          p = op;
+        }
+      }
+      if (lane == 0) *piv = p;
     }
     __syncthreads();
     const int p = *piv;
@@ -572,30 +582,24 @@ __device__ void lu_solve(double* M, int n, int* piv, double* fac_g) {
         M[p * ld + j] = t;
       }
     __syncthreads();
+    // eliminate below the pivot: one row per warp, columns across lanes
     const double pv = M[col * ld + col];
-    for (int r = col + 1 + tid; r < n; r += blockDim.x) fac_g[r] = M[r * ld + col] / pv;
-    __syncthreads();
-    const int rows = n - col - 1, cols = ld - col - 1;
-    for (int e = tid; e < rows * cols; e += blockDim.x) {
-      const int r = col + 1 + e / cols, j = col + 1 + e % cols;
-      M[r * ld + j] -= fac_g[r] * M[col * ld + j];
+    for (int r = col + 1 + warp; r < n; r += nw) {
+      const double f = M[r * ld + col] / pv;
+      for (int j = col + 1 + lane; j < ld; j += 32) M[r * ld + j] -= f * M[col * ld + j];
     }
     __syncthreads();
   }
-  // back substitution (serial over rows, parallel dot)
-  __shared__ double bs[NT];
+  // back substitution, column oriented: x_r is final once the rows below
+  // have been folded into the right-hand side
   for (int r = n - 1; r >= 0; --r) {
-    double t = 0.0;
-    for (int j = r + 1 + tid; j < n; j += blockDim.x) t += M[r * ld + j] * M[j * ld + n];
-    bs[tid] = t;
-    __syncthreads();
-    for (int st = NT / 2; st > 0; st >>= 1) {
-      if (tid < st) bs[tid] += bs[tid + st];
-      __syncthreads();
-    }
-    if (tid == 0) M[r * ld + n] = (M[r * ld + n] - bs[0]) / M[r * ld + r];
+    const double xr = M[r * ld + n] / M[r * ld + r];
+    if (tid == 0) x[r] = xr;
+    for (int i = tid; i < r; i += blockDim.x) M[i * ld + n] -= M[i * ld + r] * xr;
     __syncthreads();
   }
+  for (int i = tid; i < n; i += blockDim.x) M[i * ld + n] = x[i];
+  __syncthreads();
 }
 
 // probe_mode: 0 normal step, 1 diverged probe j (lam_final * 10^(j-4)),
@@ -661,7 +665,7 @@ k_step(ClassDev c, int phase, int probe_mode, int probe_j, float probe_lam) {
     kp[i] = k;
   }
   __syncthreads();
-  const bool use_smem = (nL <= 72);
+  const bool use_smem = (nL <= UPH_LU_SMEM_N);
   double* M = use_smem ? lsm : (c.lu + (size_t)isl * c.nLmax * (c.nLmax + 1));
   const int ld = nL + 1;
   for (int e = tid; e < nL * ld; e += NT) {
@@ -859,7 +863,7 @@ size_t assemble_smem_bytes(int nLmax, int N) {
 }
 
 size_t step_smem_bytes(int nLmax) {
-  const int n = nLmax < 72 ? nLmax : 72;
+  const int n = nLmax < UPH_LU_SMEM_N ? nLmax : UPH_LU_SMEM_N;
   return sizeof(double) * (size_t)n * (n + 1);
 }
 
