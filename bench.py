@@ -222,6 +222,40 @@ def _timed_solves(job, steps, stream, barrier, dist):
     return ms, launches
 
 
+class _ClassRun:
+    """One class (its first n islands) of a planned field as its own job."""
+
+    def __init__(self, job, field, kw, args):
+        import inspect
+        from uniphot_b200 import _lib
+        from uniphot_b200.solver import (IslandFitJob, _slice_host, build_psf_tree,
+                                         make_class_kernels)
+        b, n, kind, t = args.only_class.split(",")
+        key = (int(b), int(n), kind, int(t))
+        plan, host = next((p, h) for p, h, _ in job.classes if p.key == key)
+        d = {k: v.default for k, v in inspect.signature(IslandFitJob).parameters.items()}
+        tree, nt = build_psf_tree(kw["psfs"], plan.tier)
+        nb = len(kw["bandnames"])
+        kern = make_class_kernels(
+            plan, nb, nt, render_backend=d["render_backend"], reg=d["reg"],
+            pos_step_max_pix=d["pos_step_max_pix"], chi2_ftol_rel=d["chi2_ftol_rel"],
+            step_tol_pix=d["step_tol_pix"], un_freeze_steps=d["un_freeze_steps"],
+            has_priors=bool(host["has_priors"]), render_mode="analytic",
+            native_stamp=field.native, precision=args.precision)
+        rows = np.arange(min(args.class_islands, plan.n_islands))
+        self.job = _lib.Job(job.field.ctx)
+        self.job.add_chunk(kern.desc, _slice_host(host, rows), nb)
+        self.n_islands = int(rows.size)
+        self.max_steps = int(d["max_steps"])
+
+    def solve(self):
+        self.job.solve(self.max_steps)
+
+
+def _class_job(job, field, kw, args):
+    return _ClassRun(job, field, kw, args)
+
+
 def _kernel_table(job):
     """Instrumented solve: per kind device ms, launches and algorithmic work."""
     job.job.set_profile(True)
@@ -244,7 +278,7 @@ def _traffic(kernel):
     """DRAM bytes per launch of `kernel` from the committed ncu summary,
     scaled to this workload's algorithmic bytes per launch (the summary
     records both for its capture), or None."""
-    p = ROOT / "profiles" / f"{kernel}_launch_traffic.md"
+    p = ROOT / "profiles" / f"{kernel}_quarter_field_traffic.md"
     if not p.exists():
         return None
     vals = {}
@@ -312,6 +346,11 @@ def main():
                     help="field side (the workload is 2048; smaller sides "
                          "are for profiler captures)")
     ap.add_argument("--n-src", type=int, default=5000)
+    ap.add_argument("--only-class", default=None,
+                    help="with --profile-run: solve only the class 'B,N,kind,T' "
+                         "(e.g. 96,32,mixed,127), for kernel captures")
+    ap.add_argument("--class-islands", type=int, default=3,
+                    help="with --only-class: its first n islands")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -337,10 +376,15 @@ def main():
     n_isl = job.n_islands
     stream = torch.cuda.ExternalStream(job.field.ctx.stream_ptr())
     if args.profile_run:
-        kt = _kernel_table(job)
+        if args.only_class:
+            run = _class_job(job, field, kw, args)
+        else:
+            run = job
+        kt = _kernel_table(run)
         torch.cuda.synchronize()
-        print(json.dumps({"profile_run": True, "n_islands": n_isl,
-                          "precision": args.precision, "kernels": kt}), flush=True)
+        print(json.dumps({"profile_run": True, "n_islands": run.n_islands,
+                          "only_class": args.only_class, "precision": args.precision,
+                          "kernels": kt}), flush=True)
         job.close()
         return
 
