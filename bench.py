@@ -256,6 +256,46 @@ def _class_job(job, field, kw, args):
     return _ClassRun(job, field, kw, args)
 
 
+def _serve_measure(args, rates, device):
+    """Serving: the same seeded request pool streamed with Poisson arrivals
+    through the batched+mixed server and through one plain FP32 worker (one
+    request at a time)."""
+    from uniphot_b200.serve import Server, latency_summary, poisson_stream
+    from uniphot_b200.synth import make_serving_request
+    pool = [make_serving_request(i, device="cuda").fit_kwargs("analytic")
+            for i in range(args.serve_requests)]
+    out = {"requests": len(pool), "workers": args.serve_workers,
+           "hbm_budget_bytes": 160e9,
+           "request_shapes": "cutout side log-normal 64-1024 px, bands U{1..40}, "
+                             "sources 5-2000 at the production density, PSF "
+                             "polynomial coefficients drawn per request",
+           "rates": []}
+    forms = (("batched_mixed", "mixed", args.serve_workers),
+             ("one_at_a_time_plain", "plain", 1))
+    for name, prec, workers in forms:
+        with Server(device=device, workers=workers, hbm_budget_bytes=160e9,
+                    precision=prec) as srv:
+            # warm-up: every worker's context, allocations and graphs
+            for f in [srv.submit(dict(pool[i % len(pool)], precision=prec))
+                      for i in range(workers)]:
+                f.result()
+        for rate in rates:
+            with Server(device=device, workers=workers, hbm_budget_bytes=160e9,
+                        precision=prec) as srv:
+                futs = poisson_stream(srv, [dict(kw, precision=prec) for kw in pool],
+                                      rate, seed=7)
+                for f in futs:
+                    f.result()
+            summ = latency_summary(srv.stats)
+            summ["peak_admitted_bytes"] = srv.peak_in_use
+            row = next((r for r in out["rates"] if r["rate_hz"] == rate), None)
+            if row is None:
+                row = {"rate_hz": rate}
+                out["rates"].append(row)
+            row[name] = summ
+    return out
+
+
 def _kernel_table(job):
     """Instrumented solve: per kind device ms, launches and algorithmic work."""
     job.job.set_profile(True)
@@ -346,6 +386,15 @@ def main():
                     help="field side (the workload is 2048; smaller sides "
                          "are for profiler captures)")
     ap.add_argument("--n-src", type=int, default=5000)
+    ap.add_argument("--serve-rate", type=float, default=20.0,
+                    help="Poisson arrival rate (requests/s) of the serving run")
+    ap.add_argument("--serve-requests", type=int, default=40)
+    ap.add_argument("--serve-workers", type=int, default=4)
+    ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--serve-only", action="store_true",
+                    help="run only the serving measurement (rates from "
+                         "--serve-rates) and print its JSON line")
+    ap.add_argument("--serve-rates", default="10,50,200,2000")
     ap.add_argument("--only-class", default=None,
                     help="with --profile-run: solve only the class 'B,N,kind,T' "
                          "(e.g. 96,32,mixed,127), for kernel captures")
@@ -361,6 +410,11 @@ def main():
         return run_reference_arm(args, rank, world)
     import torch
     torch.cuda.set_device(local)
+    if args.serve_only:
+        if rank == 0:
+            rates = [float(r) for r in args.serve_rates.split(",")]
+            print(json.dumps({"serve": _serve_measure(args, rates, local)}), flush=True)
+        return
     dist = None
     if world > 1:
         import torch.distributed as dist
@@ -484,10 +538,16 @@ def main():
             args.precision: _flux_quality(_class_results(job), job.classes, ref64),
             other: _flux_quality(_class_results(job_o), job.classes, ref64),
             "sample_islands": len(ref64)}
-    if rank == 0:
-        print(json.dumps(out), flush=True)
     job_o.close()
     job.close()
+    if rank == 0 and world == 1 and not args.no_serve:
+        sv = _serve_measure(args, [args.serve_rate], local)
+        r = sv["rates"][0]
+        out["serve"] = sv
+        out["serve_latency_ms"] = {k: r["batched_mixed"][k]
+                                   for k in ("p50_ms", "p95_ms", "p99_ms")}
+    if rank == 0:
+        print(json.dumps(out), flush=True)
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()

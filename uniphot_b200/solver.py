@@ -29,6 +29,8 @@ Differences, by design:
 
 from __future__ import annotations
 
+import hashlib
+
 import time
 from dataclasses import dataclass
 from typing import Callable, Optional
@@ -103,6 +105,15 @@ def build_psf_tree(psfs: list, tier: int):
     return tree, tree.n_terms
 
 
+def _fingerprint(*arrays) -> str:
+    h = hashlib.sha1()
+    for a in arrays:
+        a = np.ascontiguousarray(a)
+        h.update(str((a.dtype.str, a.shape)).encode())
+        h.update(a.tobytes())
+    return h.hexdigest()
+
+
 class DeviceField:
     """The padded field stacks resident on one device (a library context).
 
@@ -120,13 +131,13 @@ class DeviceField:
         self._table = False
 
     def ensure_psf(self, tree: PsfTree):
+        # keyed by content: object ids can be reused once a tree is freed
+        key = _fingerprint(tree.params, tree.origin_scale)
         if tree.mode == "reference":
-            key = id(tree)
             if self._psf_key.get(tree.tier) != key:
                 self.ctx.upload_psf_poly(tree.tier, tree.params, tree.origin_scale)
                 self._psf_key[tree.tier] = key
         else:
-            key = id(tree)
             if self._mog_key != key:
                 self.ctx.upload_psf_mog(tree.params, tree.origin_scale)
                 self._mog_key = key
@@ -306,6 +317,30 @@ def _chunk_size(plan, n_bands: int, budget_bytes: float) -> int:
     return int(max(1, min(plan.n_islands, budget_bytes // max(per, 1.0))))
 
 
+def estimate_device_bytes(fp: "FieldPlan", n_bands: int, H: int, W: int,
+                          chunk_budget_bytes: float = 16e9,
+                          precision: str = "plain") -> int:
+    """Device memory a solve of the planned field holds: the padded field
+    stacks plus every class's chunk buffers (stamps, Grams, GN blocks, with
+    the same per-island estimate that sizes the chunks; the mixed form adds
+    up to 16 partial Grams per island-band)."""
+    PAD = int(fp.PAD)
+    total = 8.0 * n_bands * (H + 2 * PAD) * (W + 2 * PAD)
+    for plan, _ in fp.classes:
+        n = int(plan.n_islands)
+        per_chunk = _chunk_size(plan, n_bands, chunk_budget_bytes)
+        N, B, T = int(plan.nsrc_class), int(plan.bbox_class), int(plan.tier)
+        Sz = min(T, B)
+        R = 7 if plan.kind == "mixed" else 3
+        nL = N * (6 if plan.kind == "mixed" else 2)
+        K = nL + N + 1
+        per = 4.0 * n_bands * (N * R * Sz * Sz + K * K + nL * nL + nL) + 8.0 * nL * nL
+        if precision == "mixed":
+            per += 16 * 4.0 * n_bands * K * K
+        total += per * n + 64 * 1024 * -(-n // max(per_chunk, 1))
+    return int(total)
+
+
 def pad_stacks(data_minus_bg, invvar, PAD: int):
     """Zero-padded (n_bands, H + 2 PAD, W + 2 PAD) float32 field stacks
     (island_solver.py:3334-3344)."""
@@ -393,7 +428,8 @@ class IslandFitJob:
                  render_mode: str | None = None, tier_ladder=(111, 221),
                  native_stamp: int | None = None, device: int = 0,
                  field: DeviceField | None = None,
-                 chunk_budget_bytes: float = 16e9, precision: str = "plain"):
+                 chunk_budget_bytes: float = 16e9, precision: str = "plain",
+                 plan: "FieldPlan | None" = None):
         for flag, name in ((compute_param_errors, "compute_param_errors"),
                            (compute_source_metrics, "compute_source_metrics"),
                            (compute_re_profile, "compute_re_profile"),
@@ -406,7 +442,7 @@ class IslandFitJob:
         self.render_mode = render_mode
         n_bands = len(bandnames)
         self.bandnames, self.n_bands = list(bandnames), n_bands
-        fp = plan_field(
+        fp = plan if plan is not None else plan_field(
             psfs=psfs, island_set=island_set, buckets=buckets, pos_x=pos_x,
             pos_y=pos_y, source_type=source_type, logre=logre, ee1=ee1, ee2=ee2,
             sersic_n=sersic_n, s1_flux=s1_flux, s1_flux_var=s1_flux_var,
@@ -498,32 +534,52 @@ class IslandFitJob:
         if self.include_giants and giant_ids.size:
             out_rows.extend(giant_seed_rows(giant_ids, self.island_set,
                                             n_bands=n_bands, **self.src))
-        cat = {k: np.concatenate([r[k] for r in out_rows], axis=0) for k in out_rows[0]}
-        return IslandFitResult(
-            bandnames=list(self.bandnames), source_idx=cat["src"].astype(np.int64),
-            pos_x=cat["pos_x"], pos_y=cat["pos_y"], logre=cat["logre"],
-            ee1=cat["ee1"], ee2=cat["ee2"], sersic_n=cat["sersic_n"],
-            fluxes=cat["fluxes"], flux_err=cat["flux_err"], chi2=cat["chi2"],
-            chi2_nu=cat["chi2_nu"], n_steps=cat["n_steps"],
-            converged=cat["converged"], stalled=cat["stalled"],
-            diverged=cat["diverged"], stall_dchi2=cat["stall_dchi2"],
-            free_n=cat["free_n"], railed=cat["railed"], island_id=cat["island_id"],
-            island_nsrc=cat["island_nsrc"], island_giant=cat["island_giant"],
-            re_upper_pix=cat["re_upper_pix"], pos_x_err=cat["pos_x_err"],
-            pos_y_err=cat["pos_y_err"], re_err=cat["re_err"], ell_err=cat["ell_err"],
-            re_prof_lo=cat["re_prof_lo"], re_prof_hi=cat["re_prof_hi"],
-            theta_err=cat["theta_err"], sersic_n_err=cat["sersic_n_err"],
-            pos_x_prior_frac=cat["pos_x_prior_frac"],
-            pos_y_prior_frac=cat["pos_y_prior_frac"],
-            re_prior_frac=cat["re_prior_frac"], ell_prior_frac=cat["ell_prior_frac"],
-            theta_prior_frac=cat["theta_prior_frac"],
-            sersic_n_prior_frac=cat["sersic_n_prior_frac"], rchisq=cat["rchisq"],
-            fracflux=cat["fracflux"], fracin=cat["fracin"],
-            fracmasked=cat["fracmasked"], flux_win=cat["flux_win"],
-            flux_marg_var=cat["flux_marg_var"], bucket_stats=bucket_stats)
+        return _assemble_result(self.bandnames, out_rows, bucket_stats)
 
     def close(self):
         self.job.close()
+
+
+def _assemble_result(bandnames, out_rows, bucket_stats) -> IslandFitResult:
+    """IslandFitResult from per-class (and giant) row dicts."""
+    cat = {k: np.concatenate([r[k] for r in out_rows], axis=0) for k in out_rows[0]}
+    return IslandFitResult(
+        bandnames=list(bandnames), source_idx=cat["src"].astype(np.int64),
+        pos_x=cat["pos_x"], pos_y=cat["pos_y"], logre=cat["logre"],
+        ee1=cat["ee1"], ee2=cat["ee2"], sersic_n=cat["sersic_n"],
+        fluxes=cat["fluxes"], flux_err=cat["flux_err"], chi2=cat["chi2"],
+        chi2_nu=cat["chi2_nu"], n_steps=cat["n_steps"],
+        converged=cat["converged"], stalled=cat["stalled"],
+        diverged=cat["diverged"], stall_dchi2=cat["stall_dchi2"],
+        free_n=cat["free_n"], railed=cat["railed"], island_id=cat["island_id"],
+        island_nsrc=cat["island_nsrc"], island_giant=cat["island_giant"],
+        re_upper_pix=cat["re_upper_pix"], pos_x_err=cat["pos_x_err"],
+        pos_y_err=cat["pos_y_err"], re_err=cat["re_err"], ell_err=cat["ell_err"],
+        re_prof_lo=cat["re_prof_lo"], re_prof_hi=cat["re_prof_hi"],
+        theta_err=cat["theta_err"], sersic_n_err=cat["sersic_n_err"],
+        pos_x_prior_frac=cat["pos_x_prior_frac"],
+        pos_y_prior_frac=cat["pos_y_prior_frac"],
+        re_prior_frac=cat["re_prior_frac"], ell_prior_frac=cat["ell_prior_frac"],
+        theta_prior_frac=cat["theta_prior_frac"],
+        sersic_n_prior_frac=cat["sersic_n_prior_frac"], rchisq=cat["rchisq"],
+        fracflux=cat["fracflux"], fracin=cat["fracin"],
+        fracmasked=cat["fracmasked"], flux_win=cat["flux_win"],
+        flux_marg_var=cat["flux_marg_var"], bucket_stats=bucket_stats)
+
+
+def giant_only_result(*, bandnames, island_set, buckets, pos_x, pos_y, logre, ee1,
+                      ee2, sersic_n, joint_nsrc_cap=32, **_ignored) -> IslandFitResult:
+    """Result of a field whose islands all take the giant path (no bucket
+    left to fit): every member keeps its seed, flagged as a giant -- the rows
+    ``island_fit`` appends for giants."""
+    ids = [np.asarray(buckets.giant_ids, np.int64).ravel()]
+    for (bc, nc), b in buckets.buckets.items():
+        if joint_nsrc_cap is None or nc > int(joint_nsrc_cap):
+            ids.append(np.asarray(b.island_ids, np.int64))
+    giant_ids = np.concatenate(ids)
+    rows = giant_seed_rows(giant_ids, island_set, n_bands=len(bandnames), pos_x=pos_x,
+                           pos_y=pos_y, logre=logre, ee1=ee1, ee2=ee2, sersic_n=sersic_n)
+    return _assemble_result(bandnames, rows, [])
 
 
 def island_fit(**kwargs) -> IslandFitResult:

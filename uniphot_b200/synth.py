@@ -234,8 +234,9 @@ def make_small_field(seed: int = 0, n_star: int = 30, n_exp: int = 10,
 
 def make_production_field(seed: int = 0, side: int = 2048, n_bands: int = 20,
                           n_src: int = 5000, device="cpu",
-                          tier_ladder=(63, 127)) -> Field:
-    """Production field (see module docstring)."""
+                          tier_ladder=(63, 127), margin: float = 40.0) -> Field:
+    """Production field (see module docstring); cluster centres keep
+    ``margin`` px from the edges."""
     rng = np.random.default_rng(seed)
     nb, H, W = n_bands, side, side
     native = 31
@@ -264,7 +265,7 @@ def make_production_field(seed: int = 0, side: int = 2048, n_bands: int = 20,
     xs, ys = [], []
     while sum(len(a) for a in xs) < n_src:
         size = int(min(64, max(1, np.floor(rng.pareto(1.2) + 1))))
-        cx, cy = rng.uniform(40, W - 40), rng.uniform(40, H - 40)
+        cx, cy = rng.uniform(margin, W - margin), rng.uniform(margin, H - margin)
         spread = 3.0 + 1.5 * math.sqrt(size)
         xs.append(np.clip(cx + rng.normal(0, spread, size), 8, W - 8))
         ys.append(np.clip(cy + rng.normal(0, spread, size), 8, H - 8))
@@ -310,3 +311,24 @@ def make_production_field(seed: int = 0, side: int = 2048, n_bands: int = 20,
                         psf_stamp=stamp)
     return Field(dmb, iv, mogs, polys, px, py, st, lr, e1s, e2s, sn, s1, s1v,
                  tx, ty, flux, iset, bk, native, tuple(tier_ladder))
+
+
+def serving_request_shape(rng) -> tuple:
+    """(side, n_bands, n_sources) of one serving request: cutout side
+    log-normal clipped to 64-1024 px, bands uniform in 1..40, sources at the
+    production field's density (x U(0.5, 2)) clipped to 5-2000."""
+    side = int(np.clip(np.exp(rng.normal(np.log(256.0), 0.6)), 64, 1024))
+    n_bands = int(rng.integers(1, 41))
+    dens = 5000.0 / 2048.0 ** 2
+    n_src = int(np.clip(round(dens * side * side * rng.uniform(0.5, 2.0)), 5, 2000))
+    return side, n_bands, n_src
+
+
+def make_serving_request(seed: int, device="cpu") -> Field:
+    """One serving request: a field cutout drawn like the production field
+    (its own PSF polynomial coefficients, sources, noise) with the shape of
+    ``serving_request_shape``."""
+    rng = np.random.default_rng(10_000 + seed)
+    side, nb, n_src = serving_request_shape(rng)
+    return make_production_field(seed, side=side, n_bands=nb, n_src=n_src,
+                                 device=device, margin=min(40.0, side / 4.0))
