@@ -134,6 +134,12 @@ int uph_upload_field(uph_ctx* ctx, const float* data, const float* invvar,
 int uph_upload_field_device(uph_ctx* ctx, const float* data_dev,
                             const float* invvar_dev, int32_t n_bands,
                             int32_t Hp, int32_t Wp, int32_t pad);
+/* Same stacks from the UNPADDED host field (nb, H, W): the padded
+ * (nb, H + 2 pad, W + 2 pad) stacks are zeroed and filled on the device, so
+ * the caller builds no padded host copy (the reference pads on the host,
+ * island_solver.py:3334-3344). */
+int uph_upload_field_unpadded(uph_ctx* ctx, const float* data, const float* invvar,
+                              int32_t nb, int32_t H, int32_t W, int32_t pad);
 
 /* Pixelised polynomial PSF zero-padded to tier T: coefs (n_bands, T, T, nt)
  * float32, origin_scale (n_bands, 4) = (x_origin, x_scale, y_origin,

@@ -122,3 +122,17 @@ def test_reference_mode_galaxy_is_rejected(small):
     with pytest.raises(ValueError):
         run_gpu(plans[:1], hosts[:1], PAD, ds, ws, psfs, "reference",
                 native=small.native)
+
+
+def test_unpadded_upload_matches_padded(small):
+    """Stacks padded on the device give bitwise the results of stacks padded
+    on the host."""
+    from uniphot_b200.solver import DeviceField
+    plans, hosts, PAD, ds, ws, psfs = field_classes(small, "analytic")
+    a, _ = run_gpu(plans, hosts, PAD, ds, ws, psfs, "analytic", native=small.native)
+    fld = DeviceField.from_unpadded(small.data_minus_bg, small.invvar, PAD)
+    b, _ = run_gpu(plans, hosts, PAD, ds, ws, psfs, "analytic", native=small.native,
+                   field=fld)
+    for x, y in zip(a, b):
+        for k in ("p", "fluxes", "ferr", "chi2", "nst", "n_good"):
+            np.testing.assert_array_equal(x[k], y[k])

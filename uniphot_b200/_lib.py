@@ -20,7 +20,7 @@ RENDER_MODES = {"reference": 0, "analytic": 1}
 PRECISIONS = {"plain": 0, "mixed": 1}
 
 EXPORTED = ("uph_create", "uph_destroy", "uph_last_error", "uph_set_stream",
-            "uph_get_stream", "uph_upload_field", "uph_upload_field_device",
+            "uph_get_stream", "uph_upload_field", "uph_upload_field_device", "uph_upload_field_unpadded",
             "uph_upload_psf_poly", "uph_upload_psf_mog",
             "uph_upload_sersic_table", "uph_run_chunk", "uph_last_timing",
             "uph_last_launch_count", "uph_job_create", "uph_job_destroy",
@@ -81,6 +81,7 @@ def lib():
         L.uph_get_stream.restype = _P
         L.uph_upload_field.argtypes = [_P, _P, _P, C.c_int32, C.c_int32, C.c_int32, C.c_int32]
         L.uph_upload_field_device.argtypes = L.uph_upload_field.argtypes
+        L.uph_upload_field_unpadded.argtypes = L.uph_upload_field.argtypes
         L.uph_upload_psf_poly.argtypes = [_P, C.c_int32, _P, _P, C.c_int32, C.c_int32]
         L.uph_upload_psf_mog.argtypes = [_P, _P, _P, C.c_int32, C.c_int32, C.c_int32]
         L.uph_upload_sersic_table.argtypes = [_P, _P, _P, _P, _P, C.c_int32, C.c_int32,
@@ -161,6 +162,13 @@ class Context:
         nb, Hp, Wp = d.shape
         self.check(lib().uph_upload_field(self._h, ptr(d), ptr(w), nb, Hp, Wp, int(pad)),
                    "uph_upload_field")
+
+    def upload_field_unpadded(self, data: np.ndarray, invvar: np.ndarray, pad: int):
+        d = np.ascontiguousarray(data, np.float32)
+        w = np.ascontiguousarray(invvar, np.float32)
+        nb, H, W = d.shape
+        self.check(lib().uph_upload_field_unpadded(self._h, ptr(d), ptr(w), nb, H, W,
+                                                   int(pad)), "uph_upload_field_unpadded")
 
     def upload_field_device(self, d_ptr: int, w_ptr: int, nb, Hp, Wp, pad):
         self.check(lib().uph_upload_field_device(self._h, _P(d_ptr), _P(w_ptr), nb, Hp,

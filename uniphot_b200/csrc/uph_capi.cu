@@ -31,11 +31,18 @@ void launch_fill_float(float* p, float v, int n, cudaStream_t s);
 
 namespace {
 
+// Device buffer from the device's stream-ordered memory pool: allocated on
+// the owning context's stream, released without synchronising the device;
+// freed memory stays in the pool (its release threshold is raised at context
+// creation) for the next job to reuse.  Every release follows a
+// synchronisation of all streams that used the buffer (job and context
+// teardown synchronise first), so the free is issued on the legacy stream,
+// whose handle stays valid whatever the owner's stream has become.
 struct DevBuf {
   void* ptr = nullptr;
   size_t cap = 0;
   void release() {
-    if (ptr) cudaFree(ptr);
+    if (ptr) cudaFreeAsync(ptr, 0);
     ptr = nullptr;
     cap = 0;
   }
@@ -102,8 +109,11 @@ int ensure(uph_ctx* ctx, DevBuf& b, size_t bytes, const char* what) {
   if (bytes == 0) bytes = 16;
   if (b.cap >= bytes) return UPH_OK;
   b.release();
-  cudaError_t e = cudaMalloc(&b.ptr, bytes);
-  if (e != cudaSuccess) return cuda_err(ctx, e, what);
+  cudaError_t e = cudaMallocAsync(&b.ptr, bytes, ctx->stream);
+  if (e != cudaSuccess) {
+    b.ptr = nullptr;
+    return cuda_err(ctx, e, what);
+  }
   b.cap = bytes;
   return UPH_OK;
 }
@@ -139,6 +149,16 @@ int uph_create(int device, uph_ctx** out) {
   ctx->device = device;
   cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, device);
   if (ctx->sm_count <= 0) ctx->sm_count = 148;
+  {
+    // keep freed chunk buffers cached in the device's default pool: a job's
+    // teardown then returns memory without synchronising the device and the
+    // next job reuses it (the pool is trimmed when a context is destroyed)
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+      uint64_t thr = ~0ull;
+      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    }
+  }
   if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
     delete ctx;
     return UPH_ERR_CUDA;
@@ -179,6 +199,12 @@ int uph_destroy(uph_ctx* ctx) {
     if (ev) cudaEventDestroy(ev);
   if (ctx->h_active) cudaFreeHost(ctx->h_active);
   if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
+  ctx->stream = nullptr;
+  {
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, ctx->device) == cudaSuccess)
+      cudaMemPoolTrimTo(pool, 0);
+  }
   delete ctx;
   return UPH_OK;
 }
@@ -229,6 +255,38 @@ static int upload_field_impl(uph_ctx* ctx, const float* d, const float* w,
 int uph_upload_field(uph_ctx* ctx, const float* d, const float* w,
                      int32_t nb, int32_t Hp, int32_t Wp, int32_t pad) {
   return upload_field_impl(ctx, d, w, nb, Hp, Wp, pad, cudaMemcpyHostToDevice);
+}
+
+int uph_upload_field_unpadded(uph_ctx* ctx, const float* d, const float* w,
+                              int32_t nb, int32_t H, int32_t W, int32_t pad) {
+  if (!ctx) return UPH_ERR_INVALID;
+  if (!d || !w || nb <= 0 || H <= 0 || W <= 0 || pad < 0)
+    return set_err(ctx, UPH_ERR_INVALID, "invalid field arguments");
+  cudaSetDevice(ctx->device);
+  const int Hp = H + 2 * pad, Wp = W + 2 * pad;
+  const size_t bytes = sizeof(float) * (size_t)nb * Hp * Wp;
+  int rc = ensure(ctx, ctx->dstack, bytes, "field data");
+  if (rc) return rc;
+  rc = ensure(ctx, ctx->wstack, bytes, "field invvar");
+  if (rc) return rc;
+  CK(cudaMemsetAsync(ctx->dstack.ptr, 0, bytes, ctx->stream), "field pad");
+  CK(cudaMemsetAsync(ctx->wstack.ptr, 0, bytes, ctx->stream), "field pad");
+  for (int b = 0; b < nb; ++b) {
+    const size_t o = ((size_t)b * Hp + pad) * Wp + pad;
+    const size_t so = (size_t)b * H * W;
+    CK(cudaMemcpy2DAsync((float*)ctx->dstack.ptr + o, sizeof(float) * Wp, d + so,
+                         sizeof(float) * W, sizeof(float) * W, H,
+                         cudaMemcpyHostToDevice, ctx->stream), "field copy");
+    CK(cudaMemcpy2DAsync((float*)ctx->wstack.ptr + o, sizeof(float) * Wp, w + so,
+                         sizeof(float) * W, sizeof(float) * W, H,
+                         cudaMemcpyHostToDevice, ctx->stream), "field copy");
+  }
+  CK(cudaStreamSynchronize(ctx->stream), "field copy");
+  ctx->nb = nb;
+  ctx->Hp = Hp;
+  ctx->Wp = Wp;
+  ctx->pad = pad;
+  return UPH_OK;
 }
 
 int uph_upload_field_device(uph_ctx* ctx, const float* d, const float* w,

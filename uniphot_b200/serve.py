@@ -189,17 +189,15 @@ def default_solve(state: dict, kwargs: dict, plan):
     """Solve one request on the worker's context (created on first use and
     kept: its field and PSF buffers are reused and regrown as needed)."""
     from . import _lib
-    from .solver import DeviceField, IslandFitJob, giant_only_result, pad_stacks
+    from .solver import DeviceField, IslandFitJob, giant_only_result
     if plan is None:
         return giant_only_result(**kwargs)
     if "ctx" not in state:
         state["ctx"] = _lib.Context(state["device"])
     kw = dict(kwargs)
     kw.setdefault("precision", state["precision"])
-    dstack, wstack = pad_stacks(kw["data_minus_bg"], kw["invvar"], plan.PAD)
-    fld = DeviceField(dstack, wstack, plan.PAD, device=state["device"],
-                      context=state["ctx"])
-    del dstack, wstack
+    fld = DeviceField.from_unpadded(kw["data_minus_bg"], kw["invvar"], plan.PAD,
+                                    device=state["device"], context=state["ctx"])
     job = IslandFitJob(**kw, device=state["device"], field=fld, plan=plan)
     try:
         job.solve()

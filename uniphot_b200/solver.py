@@ -130,6 +130,23 @@ class DeviceField:
         self._mog_key = None
         self._table = False
 
+    @classmethod
+    def from_unpadded(cls, data_minus_bg: np.ndarray, invvar: np.ndarray, pad: int,
+                      device: int = 0, context: Optional[_lib.Context] = None):
+        """Upload the unpadded (n_bands, H, W) field; the zero-padded stacks
+        are built on the device."""
+        self = cls.__new__(cls)
+        self.ctx = context if context is not None else _lib.Context(device)
+        self.ctx.upload_field_unpadded(data_minus_bg, invvar, pad)
+        nb, H, W = np.shape(data_minus_bg)
+        self.pad = int(pad)
+        self.n_bands = int(nb)
+        self.shape = (int(nb), int(H) + 2 * int(pad), int(W) + 2 * int(pad))
+        self._psf_key = {}
+        self._mog_key = None
+        self._table = False
+        return self
+
     def ensure_psf(self, tree: PsfTree):
         # keyed by content: object ids can be reused once a tree is freed
         key = _fingerprint(tree.params, tree.origin_scale)
@@ -457,10 +474,9 @@ class IslandFitJob:
         H, W = data_minus_bg.shape[1], data_minus_bg.shape[2]
         if field is None or field.pad != PAD or field.shape != (
                 n_bands, H + 2 * PAD, W + 2 * PAD):
-            dstack, wstack = pad_stacks(data_minus_bg, invvar, PAD)
-            field = DeviceField(dstack, wstack, PAD, device=device,
-                                context=field.ctx if field is not None else None)
-            del dstack, wstack
+            field = DeviceField.from_unpadded(
+                data_minus_bg, invvar, PAD, device=device,
+                context=field.ctx if field is not None else None)
         self.field, self.PAD = field, PAD
         plans = [p for p, _ in fp.classes]
         capped = fp.capped
