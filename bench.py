@@ -256,6 +256,53 @@ def _class_job(job, field, kw, args):
     return _ClassRun(job, field, kw, args)
 
 
+def _stress_measure(args, device):
+    """Crowded blends vs the float64 oracle, plain and mixed forms: per-flux
+    relative error, pass fraction at 1e-4 relative or 0.01 sigma, position
+    error, and islands/s of each form on the whole field."""
+    import torch
+    from uniphot_b200.solver import IslandFitJob
+    from uniphot_b200.synth import make_blend_field
+    field = make_blend_field(args.seed, n_islands=args.stress_islands, n_bands=40,
+                             device="cuda")
+    kw = field.fit_kwargs("analytic")
+    out = {"workload": f"{args.stress_islands} blends of 2-12 point sources 0.3-1.5 "
+                       f"FWHM apart, flux ratios log-U up to 1e4, 40 bands (a quarter "
+                       f"at SNR 3-10 for faint members), production PSF",
+           "refinement_iterations_per_linearisation": {"plain": 0, "mixed": 1}}
+    jobs = {}
+    for prec in ("plain", "mixed"):
+        job = IslandFitJob(**dict(kw, precision=prec), device=device)
+        for _ in range(2):
+            job.solve()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        job.solve()
+        torch.cuda.synchronize()
+        out.setdefault("islands_per_s", {})[prec] = job.n_islands / (time.perf_counter() - t0)
+        jobs[prec] = job
+    out["n_islands"] = jobs["plain"].n_islands
+    sample = _sample_rows(jobs["plain"].classes, 0.0, 3, min_n=args.stress_sample)
+    nb, H, W = field.data_minus_bg.shape
+    ref64, dt, procs = cpu_oracle_time(jobs["plain"].classes, jobs["plain"].PAD, field,
+                                       sample, precision="f64", budget_s=240.0)
+    out["fp64_sample_islands"] = len(ref64)
+    for prec, job in jobs.items():
+        get = _class_results(job)
+        q = _flux_quality(get, job.classes, ref64)
+        dpos = []
+        for (ci, r), o in ref64:
+            mm = job.classes[ci][1]["mmask"][r]
+            dpos.append(np.abs(get(ci)["p"][r][mm, :2] - o["p"][mm, :2]).max(axis=1))
+        dp = np.concatenate(dpos) if dpos else np.zeros(0)
+        q["pos_err_px_median"] = float(np.median(dp)) if dp.size else None
+        q["pos_err_px_max"] = float(dp.max()) if dp.size else None
+        q["frac_pos_within_1e-3_px"] = float(np.mean(dp <= 1e-3)) if dp.size else None
+        out[prec] = q
+        job.close()
+    return out
+
+
 def _serve_measure(args, rates, device):
     """Serving: the same seeded request pool streamed with Poisson arrivals
     through the batched+mixed server and through one plain FP32 worker (one
@@ -395,6 +442,11 @@ def main():
                     help="run only the serving measurement (rates from "
                          "--serve-rates) and print its JSON line")
     ap.add_argument("--serve-rates", default="10,50,200,2000")
+    ap.add_argument("--precision-stress", action="store_true",
+                    help="run only the precision-stress measurement (crowded "
+                         "blends, 40 bands) and print its JSON line")
+    ap.add_argument("--stress-islands", type=int, default=2000)
+    ap.add_argument("--stress-sample", type=int, default=120)
     ap.add_argument("--only-class", default=None,
                     help="with --profile-run: solve only the class 'B,N,kind,T' "
                          "(e.g. 96,32,mixed,127), for kernel captures")
@@ -410,6 +462,11 @@ def main():
         return run_reference_arm(args, rank, world)
     import torch
     torch.cuda.set_device(local)
+    if args.precision_stress:
+        if rank == 0:
+            print(json.dumps({"precision_stress": _stress_measure(args, local)}),
+                  flush=True)
+        return
     if args.serve_only:
         if rank == 0:
             rates = [float(r) for r in args.serve_rates.split(",")]

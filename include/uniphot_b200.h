@@ -66,9 +66,14 @@ typedef struct uph_class_desc {
   int32_t tc_min_rows;      /* mixed form: Gram-row threshold of the
                                tensor-core path; < 0 selects the default
                                (UPH_TC_MIN_ROWS_DEFAULT)                   */
+  float tc_cond_max;        /* mixed form: islands whose members' scaled
+                               normal matrix has a conditioning indicator
+                               above this (in any band) form the Gram in
+                               FP32; < 0 selects UPH_TC_COND_MAX_DEFAULT  */
 } uph_class_desc;
 
 #define UPH_TC_MIN_ROWS_DEFAULT 24
+#define UPH_TC_COND_MAX_DEFAULT 10.0f
 
 #define UPH_PRECISION_PLAIN 0
 #define UPH_PRECISION_MIXED 1

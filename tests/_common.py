@@ -33,7 +33,7 @@ def field_classes(f, mode: str, kinds=("star", "mixed")):
 
 
 def run_gpu(plans, hosts, PAD, ds, ws, psfs, mode, max_steps=30, field=None,
-            native=0, precision="plain", tc_min_rows=-1):
+            native=0, precision="plain", tc_min_rows=-1, tc_cond_max=-1.0):
     from uniphot_b200 import solver
     if field is None:
         field = solver.DeviceField(ds, ws, PAD)
@@ -44,7 +44,8 @@ def run_gpu(plans, hosts, PAD, ds, ws, psfs, mode, max_steps=30, field=None,
             plan, ds.shape[0], nt, render_backend="fft", reg=1e-9,
             pos_step_max_pix=0.5, chi2_ftol_rel=1e-4, step_tol_pix=0.1,
             un_freeze_steps=0, has_priors=bool(host["has_priors"]), render_mode=mode,
-            native_stamp=native, precision=precision, tc_min_rows=tc_min_rows)
+            native_stamp=native, precision=precision, tc_min_rows=tc_min_rows,
+            tc_cond_max=tc_cond_max)
         rows = np.arange(plan.n_islands)
         outs.append(solver.run_class_chunk(kern, tree, host, rows, rows.size,
                                            max_steps, field, field, PAD))

@@ -28,13 +28,14 @@ def _pos_ok(g, o, mmask):
     return (dp <= POS)[mmask]
 
 
-def _check(plans, hosts, gp, gm, o64, label):
+def _check(plans, hosts, gp, gm, o64, label, same_path=True, margin=0.0):
     fp, fm, pp, pm = [], [], [], []
     for p, h, a, b, o in zip(plans, hosts, gp, gm, o64):
         msg = f"{label} {p.key}"
-        np.testing.assert_array_equal(b["nst"], a["nst"], err_msg=msg)
-        np.testing.assert_array_equal(b["conv"], a["conv"], err_msg=msg)
-        np.testing.assert_array_equal(b["stall"], a["stall"], err_msg=msg)
+        if same_path:
+            np.testing.assert_array_equal(b["nst"], a["nst"], err_msg=msg)
+            np.testing.assert_array_equal(b["conv"], a["conv"], err_msg=msg)
+            np.testing.assert_array_equal(b["stall"], a["stall"], err_msg=msg)
         assert np.isfinite(b["fluxes"]).all() and np.isfinite(b["p"]).all(), msg
         fp.append(_flux_ok(a, o, h["mmask"]))
         fm.append(_flux_ok(b, o, h["mmask"]))
@@ -42,8 +43,10 @@ def _check(plans, hosts, gp, gm, o64, label):
         pm.append(_pos_ok(b, o, h["mmask"]))
     fp, fm = np.concatenate(fp), np.concatenate(fm)
     pp, pm = np.concatenate(pp), np.concatenate(pm)
-    assert fm.mean() >= fp.mean(), f"{label}: flux pass {fm.mean():.4f} < plain {fp.mean():.4f}"
-    assert pm.mean() >= pp.mean(), f"{label}: pos pass {pm.mean():.4f} < plain {pp.mean():.4f}"
+    assert fm.mean() >= fp.mean() - margin, \
+        f"{label}: flux pass {fm.mean():.4f} < plain {fp.mean():.4f}"
+    assert pm.mean() >= pp.mean() - margin, \
+        f"{label}: pos pass {pm.mean():.4f} < plain {pp.mean():.4f}"
     return fp.mean(), fm.mean()
 
 
@@ -56,12 +59,12 @@ def small():
 @pytest.mark.parametrize("mode,kinds", [("reference", ("star",)),
                                         ("analytic", ("star", "mixed"))])
 def test_every_island_on_tensor_cores(small, mode, kinds):
-    """tc_min_rows = 0 routes every island (Gram rows 3..) through the
-    tensor-core kernel."""
+    """tc_min_rows = 0 and no conditioning limit route every island (Gram
+    rows 3..) through the tensor-core kernel."""
     plans, hosts, PAD, ds, ws, psfs = field_classes(small, mode, kinds)
     gp, fld = run_gpu(plans, hosts, PAD, ds, ws, psfs, mode, native=small.native)
     gm, _ = run_gpu(plans, hosts, PAD, ds, ws, psfs, mode, native=small.native,
-                    precision="mixed", tc_min_rows=0, field=fld)
+                    precision="mixed", tc_min_rows=0, tc_cond_max=1e30, field=fld)
     o64 = run_oracle(plans, hosts, PAD, ds, ws, psfs, mode, precision="f64",
                      native=small.native, processes=8)
     fp, fm = _check(plans, hosts, gp, gm, o64, mode)
@@ -97,3 +100,21 @@ def test_mixed_deterministic(small):
     for x, y in zip(a, b):
         for k in ("p", "fluxes", "ferr", "chi2", "nst"):
             np.testing.assert_array_equal(x[k], y[k])
+
+
+def test_precision_stress_blends():
+    """Crowded blends (2-12 sources 0.3-1.5 FWHM apart, flux ratios up to
+    1e4, a quarter of the bands at low SNR): the mixed form stays as close to
+    float64 as the plain form (within 2 points of its pass fraction).  The
+    two forms may take different LM paths on these ill-conditioned
+    problems, so iteration counts are not compared."""
+    from uniphot_b200.synth import make_blend_field
+    f = make_blend_field(0, n_islands=30, n_bands=8)
+    plans, hosts, PAD, ds, ws, psfs = field_classes(f, "analytic")
+    gp, fld = run_gpu(plans, hosts, PAD, ds, ws, psfs, "analytic", native=f.native)
+    gm, _ = run_gpu(plans, hosts, PAD, ds, ws, psfs, "analytic", native=f.native,
+                    precision="mixed", field=fld)
+    o64 = run_oracle(plans, hosts, PAD, ds, ws, psfs, "analytic", precision="f64",
+                     native=f.native, processes=8)
+    fp, fm = _check(plans, hosts, gp, gm, o64, "stress", same_path=False, margin=0.02)
+    print(f"stress: flux pass plain {fp:.4f} mixed {fm:.4f}")

@@ -39,7 +39,8 @@ class ClassDesc(C.Structure):
                 ("pos_step_max", C.c_float), ("chi2_ftol_rel", C.c_float),
                 ("step_tol_pix", C.c_float), ("un_freeze_steps", C.c_int32),
                 ("has_priors", C.c_int32), ("native_stamp", C.c_int32),
-                ("precision", C.c_int32), ("tc_min_rows", C.c_int32)]
+                ("precision", C.c_int32), ("tc_min_rows", C.c_int32),
+                ("tc_cond_max", C.c_float)]
 
 
 class ChunkIn(C.Structure):

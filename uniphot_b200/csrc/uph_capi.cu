@@ -469,7 +469,7 @@ void iteration(const ClassDev& c, Launcher& L) {
   L(2, [&] { launch_assemble(c, s); });
   L(3, [&] { launch_step(c, PH_TRIAL, 0, 0.f, 0, s); });
   L(0, [&] { launch_render(c, c.p_try, PH_TRIAL, s); }, 2);
-  L(4, [&] { launch_gram_trial(c, c.p_try, PH_TRIAL, 0, c.ftry, s); });
+  L(4, [&] { launch_gram_trial(c, c.p_try, PH_TRIAL, 0, c.ftry, c.acond_try, s); });
   L(5, [&] { launch_accept(c, PH_TRIAL, s); });
 }
 
@@ -653,6 +653,9 @@ int add_chunk(uph_ctx* ctx, Chunk* ch, const uph_class_desc* cls,
   if (c.tc_min_rows < (1 << 30)) {
     c.fcur = cbuf<float>(ctx, ch, "fcur", (size_t)n * nb * N, &rc);
     c.ftry = cbuf<float>(ctx, ch, "ftry", (size_t)n * nb * N, &rc);
+    c.acond_cur = cbuf<float>(ctx, ch, "acondc", (size_t)n * nb, &rc);
+    c.acond_try = cbuf<float>(ctx, ch, "acondt", (size_t)n * nb, &rc);
+    c.tc_cond_max = cls->tc_cond_max < 0.f ? UPH_TC_COND_MAX_DEFAULT : cls->tc_cond_max;
     c.tc_split = gram_tc_splits(n, nb, B, ctx->sm_count);
     if (c.tc_split > 1)
       c.gpart = cbuf<float>(ctx, ch, "gpart", (size_t)c.tc_split * n * nb * Kmax * Kmax, &rc);
@@ -743,11 +746,11 @@ void post_loop(Chunk* ch, Launcher& L) {
     const float lamj = (float)std::pow(10.0, (double)e);
     L(3, [&] { launch_step(c, PH_PROBE, 0, lamj, 2, s); });
     L(0, [&] { launch_render(c, c.p_try, PH_PROBE, s); }, 2);
-    L(4, [&] { launch_gram_trial(c, c.p_try, PH_PROBE, 0, nullptr, s); });
+    L(4, [&] { launch_gram_trial(c, c.p_try, PH_PROBE, 0, nullptr, nullptr, s); });
     L(5, [&] { launch_accept(c, PH_PROBE, s); });
   }
   L(0, [&] { launch_render(c, c.p, PH_ALL, s); }, 2);
-  L(4, [&] { launch_gram_trial(c, c.p, PH_ALL, 1, nullptr, s); });
+  L(4, [&] { launch_gram_trial(c, c.p, PH_ALL, 1, nullptr, nullptr, s); });
 }
 
 int job_solve(uph_job* job, int max_steps) {
@@ -817,7 +820,8 @@ int job_solve(uph_job* job, int max_steps) {
     // at the starting parameters that its residual row needs
     if (ch->fresh || ch->c.fcur) {
       L(0, [&] { launch_render(ch->c, ch->c.p, PH_ALL, s); }, 2);
-      L(4, [&] { launch_gram_trial(ch->c, ch->c.p, PH_ALL, 0, ch->c.fcur, s); });
+      L(4, [&] { launch_gram_trial(ch->c, ch->c.p, PH_ALL, 0, ch->c.fcur, ch->c.acond_cur,
+                                   s); });
       if (ch->fresh) L(5, [&] { launch_accept(ch->c, PH_ALL, s); });
     }
     if (max_steps > 0 && !job->profile && !ch->gexec) {

@@ -131,7 +131,7 @@ __global__ void __launch_bounds__(NT) k_gram_tc(ClassDev c, int rcap) {
   const int isl = ib / c.nb, b = ib % c.nb;
   if (isl >= c.n_isl || !isl_active(c.flags[isl], PH_LIN)) return;
   const int K = gram_rows(c, isl);
-  if (K <= c.tc_min_rows) return;            // handled by k_gram_lin
+  if (!tc_island(c, isl, K)) return;         // handled by k_gram_lin
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int Mh = (K + 127) / 128;            // M = 128 halves
   const int R = Mh * 128;                    // stored rows
@@ -342,7 +342,7 @@ __global__ void __launch_bounds__(NT) k_gram_tc_reduce(ClassDev c) {
   const int isl = blockIdx.x / c.nb, b = blockIdx.x % c.nb;
   if (isl >= c.n_isl || !isl_active(c.flags[isl], PH_LIN)) return;
   const int K = gram_rows(c, isl);
-  if (K <= c.tc_min_rows) return;
+  if (!tc_island(c, isl, K)) return;
   const size_t mat = (size_t)c.Kmax * c.Kmax;
   const size_t stride = (size_t)c.n_isl * c.nb * mat;
   const float* src = c.gpart + ((size_t)isl * c.nb + b) * mat;

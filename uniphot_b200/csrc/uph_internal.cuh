@@ -121,6 +121,13 @@ struct ClassDev {
   // the residual d - M^T fcur instead of the data.
   float* fcur;
   float* ftry;
+  // (n_isl, nb) conditioning indicator of the members' scaled normal matrix
+  // at p (acond_cur) and p_try (acond_try), from the trial pass's f64
+  // elimination; an island whose indicator exceeds tc_cond_max in any band
+  // forms its Gram in FP32
+  float* acond_cur;
+  float* acond_try;
+  float tc_cond_max;
   float* probe_best;       // (n_isl) plateau certificate
   float* probe_p;          // (n_isl, 4, nP) diverged-probe proposals
   int* n_active;
@@ -136,6 +143,18 @@ struct ClassDev {
   float reg, pos_step_max, ftol_rel, step_tol;
   int un_freeze;
 };
+
+// Whether island isl forms its next Gram on the tensor cores (mixed form):
+// more than tc_min_rows rows and a well-conditioned normal matrix of its
+// members in every band.  k_gram_lin, k_gram_tc and k_assemble take the same
+// decision from the same data.
+__device__ __forceinline__ bool tc_island(const ClassDev& c, int isl, int K) {
+  if (K <= c.tc_min_rows) return false;
+  const float* a = c.acond_cur + (size_t)isl * c.nb;
+  for (int b = 0; b < c.nb; ++b)
+    if (!(a[b] <= c.tc_cond_max)) return false;
+  return true;
+}
 
 // Kernel kinds of the instrumented solve (uph_job_kernel_time numbering).
 enum { WK_RENDER = 0, WK_GRAM = 1, WK_ASSEMBLE = 2, WK_STEP = 3, WK_TRIAL = 4,
@@ -219,7 +238,7 @@ void launch_render(const ClassDev& c, const float* P, int phase,
 void launch_gram_lin(const ClassDev& c, cudaStream_t s);
 void launch_assemble(const ClassDev& c, cudaStream_t s);
 void launch_gram_trial(const ClassDev& c, const float* P, int phase,
-                       int final_mode, float* fout, cudaStream_t s);
+                       int final_mode, float* fout, float* cout, cudaStream_t s);
 void launch_step(const ClassDev& c, int phase, int probe_j, float probe_lam,
                  int use_lam_final_scale, cudaStream_t s);
 void launch_accept(const ClassDev& c, int phase, cudaStream_t s);

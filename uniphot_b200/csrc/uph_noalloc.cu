@@ -166,7 +166,7 @@ extern "C" int uph_fluxes_noalloc(const uph_noalloc_args* a) {
   k_noalloc_prepare<<<(n + 127) / 128, 128, 0, s>>>(n, N, a->mmask, c.flags,
                                                    (int*)(base + o_nr));
   launch_render(c, c.p, PH_ALL, s);
-  launch_gram_trial(c, c.p, PH_ALL, 1, nullptr, s);
+  launch_gram_trial(c, c.p, PH_ALL, 1, nullptr, nullptr, s);
   k_noalloc_chi2<<<(n + 127) / 128, 128, 0, s>>>(n, nb, c.chi2b, a->chi2);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {

@@ -44,15 +44,31 @@ struct RowSrc {
   const int16_t* rk;
   const int16_t* rs;
   int K;
+  const float* fc = nullptr;   // residual form: fluxes of the nr model rows
+  int nr = 0;
 };
 
 // Value of Gram row r at window pixel (wy, wx), already scaled by sqrt(w).
+// The last row is the data, or in residual form (fc set) the residual
+// d - sum_k fc_k m_k, summed in member order as the trial pass does.
 __device__ __forceinline__ float row_value(const ClassDev& c, int isl, int b,
                                            const RowSrc& rows, const int4* box,
                                            int r, int wy, int wx, float sw,
                                            const float* dbase) {
   const int rs = rows.rs[r];
-  if (rs < 0) return dbase[(size_t)wy * c.Wp + wx] * sw;
+  if (rs < 0) {
+    const float d = dbase[(size_t)wy * c.Wp + wx];
+    if (!rows.fc) return d * sw;
+    float model = 0.f;
+    for (int k = 0; k < rows.nr; ++k) {
+      const int4 bx = box[k];
+      const int ly = wy - bx.y, lx = wx - bx.x;
+      if (ly >= 0 && ly < bx.w && lx >= 0 && lx < bx.z)
+        model = fmaf(rows.fc[k], c.stamps[stamp_slot(c, isl, b, k, 0) + (size_t)ly * c.Sz + lx],
+                     model);
+    }
+    return sw * (d - model);
+  }
   const int k = rows.rk[r];
   const int4 bx = box[k];
   const int ly = wy - bx.y, lx = wx - bx.x;
@@ -248,7 +264,7 @@ __global__ void __launch_bounds__(NT) k_gram_lin(ClassDev c) {
   if (isl >= c.n_isl || !isl_active(c.flags[isl], PH_LIN)) return;
   const int nL = c.isl_nL[isl], nr = c.isl_nr[isl];
   const int K = nL + nr + 1;
-  if (K > c.tc_min_rows) return;     // the tensor-core Gram handles this island
+  if (tc_island(c, isl, K)) return;  // the tensor-core Gram handles this island
   const int nbk = (K + 7) / 8;
   const int nblk = nbk * (nbk + 1) / 2;
   if ((int)blockIdx.y * NT >= max(nblk, 1) && blockIdx.y > 0) return;
@@ -258,7 +274,9 @@ __global__ void __launch_bounds__(NT) k_gram_lin(ClassDev c) {
   if (threadIdx.x == 0 && blockIdx.y == 0)
     gram_work(c, WK_GRAM, c.row_k + (size_t)isl * c.Kmax, c.row_s + (size_t)isl * c.Kmax,
               K, box);
-  RowSrc rows{c.row_k + (size_t)isl * c.Kmax, c.row_s + (size_t)isl * c.Kmax, K};
+  // the mixed form forms every Gram in residual form (k_assemble matches)
+  RowSrc rows{c.row_k + (size_t)isl * c.Kmax, c.row_s + (size_t)isl * c.Kmax, K,
+              c.fcur ? c.fcur + ((size_t)isl * c.nb + b) * c.N : nullptr, nr};
   gram_window(c, isl, b, rows, box,
               c.gram + ((size_t)isl * c.nb + b) * c.Kmax * c.Kmax, c.Kmax,
               blockIdx.y, sm);
@@ -267,9 +285,20 @@ __global__ void __launch_bounds__(NT) k_gram_lin(ClassDev c) {
 // Gauss-Jordan elimination with partial pivoting on M (n x ncol, pitch ld):
 // turns the left n x n block into the identity; the remaining columns hold
 // A^-1 [rhs].  All threads of the block participate.
+//
+// With diag (the matrix's original diagonal) and cond non-null, thread 0
+// also writes a conditioning indicator of the diagonally scaled matrix
+// D^-1/2 A D^-1/2: the spread max/min of the pivots in that scaling (each
+// pivot |M[p][col]| divided by sqrt(diag[row of p] diag[col])), 1 for a
+// diagonal matrix and 1 / (1 - rho^2) for two members of correlation rho.
 __device__ void gauss_jordan(double* M, int n, int ncol, int ld, double* fac,
-                             int* piv) {
+                             int* piv, const double* diag = nullptr,
+                             float* cond = nullptr) {
   const int tid = threadIdx.x;
+  int perm[UPH_MAXN];
+  double rmin = INFINITY, rmax = 0.0;
+  if (tid == 0 && cond)
+    for (int r = 0; r < n; ++r) perm[r] = r;
   for (int col = 0; col < n; ++col) {
     if (tid == 0) {
       int p = col;
@@ -282,6 +311,15 @@ __device__ void gauss_jordan(double* M, int n, int ncol, int ld, double* fac,
         }
       }
       *piv = p;
+      if (cond) {
+        const double sc = sqrt(fabs(diag[perm[p]] * diag[col]));
+        const double rr = sc > 0.0 ? best / sc : 0.0;
+        rmin = fmin(rmin, rr);
+        rmax = fmax(rmax, rr);
+        const int t = perm[p];
+        perm[p] = perm[col];
+        perm[col] = t;
+      }
     }
     __syncthreads();
     const int p = *piv;
@@ -303,6 +341,7 @@ __device__ void gauss_jordan(double* M, int n, int ncol, int ld, double* fac,
     }
     __syncthreads();
   }
+  if (tid == 0 && cond) *cond = rmin > 0.0 ? (float)(rmax / rmin) : INFINITY;
 }
 
 __global__ void __launch_bounds__(NT) k_assemble(ClassDev c) {
@@ -344,7 +383,7 @@ __global__ void __launch_bounds__(NT) k_assemble(ClassDev c) {
   //   M W d - A x     = M W r + A (fc - x).
   if (tid == 0)
     work_add(c, WK_ASSEMBLE, 4ull * (unsigned long long)(K * K + nL * nL + nL), 0);
-  const bool resid = K > c.tc_min_rows;
+  const bool resid = c.fcur != nullptr;   // mixed form: every Gram in residual form
   const float* fc = resid ? c.fcur + ((size_t)isl * c.nb + b) * c.N : nullptr;
   for (int e = tid; e < nr * ncol; e += NT) {
     const int r = e / ncol, j = e - (e / ncol) * ncol;
@@ -443,12 +482,13 @@ __global__ void __launch_bounds__(NT) k_assemble(ClassDev c) {
 
 __global__ void __launch_bounds__(NT)
 k_gram_trial(ClassDev c, const float* __restrict__ P, int phase,
-             int final_mode, float* __restrict__ fout) {
+             int final_mode, float* __restrict__ fout, float* __restrict__ cout) {
   extern __shared__ float sm[];
   __shared__ int4 box[UPH_MAXN];
   __shared__ int16_t rk[UPH_MAXN + 1], rs[UPH_MAXN + 1];
   __shared__ double Aug[UPH_MAXN * (2 * UPH_MAXN + 1)];
   __shared__ double fac[UPH_MAXN];
+  __shared__ double dg[UPH_MAXN];
   __shared__ float gmm[(UPH_MAXN + 1) * (UPH_MAXN + 1)];
   __shared__ float fl32[UPH_MAXN];
   __shared__ double red[NT];
@@ -488,8 +528,12 @@ k_gram_trial(ClassDev c, const float* __restrict__ P, int phase,
     }
     Aug[r * ncol + j] = v;
   }
+  // the diagonal Aug receives, read from the finished Gram (not from Aug,
+  // which other threads are still filling)
+  for (int r = tid; r < nr; r += NT) dg[r] = (double)gmm[r * K + r] + (double)c.reg;
   __syncthreads();
-  gauss_jordan(Aug, nr, ncol, ncol, fac, &piv);
+  gauss_jordan(Aug, nr, ncol, ncol, fac, &piv, dg,
+               cout ? cout + (size_t)isl * c.nb + b : nullptr);
   for (int l = tid; l < nr; l += NT) fl32[l] = (float)Aug[l * ncol + 2 * nr];
   if (fout) {
     float* fo = fout + ((size_t)isl * c.nb + b) * c.N;
@@ -784,6 +828,8 @@ __global__ void k_accept(ClassDev c, int phase) {
     if (c.fcur) {
       const size_t o = (size_t)isl * c.nb * c.N;
       for (int e = 0; e < c.nb * c.N; ++e) c.fcur[o + e] = c.ftry[o + e];
+      for (int b = 0; b < c.nb; ++b)
+        c.acond_cur[(size_t)isl * c.nb + b] = c.acond_try[(size_t)isl * c.nb + b];
     }
     c.chi2[isl] = chi2_try;
     nf |= FL_NEEDLIN;
@@ -880,9 +926,9 @@ void launch_assemble(const ClassDev& c, cudaStream_t s) {
 }
 
 void launch_gram_trial(const ClassDev& c, const float* P, int phase,
-                       int final_mode, float* fout, cudaStream_t s) {
+                       int final_mode, float* fout, float* cout, cudaStream_t s) {
   k_gram_trial<<<(unsigned)(c.n_isl * c.nb), NT, gram_trial_smem_bytes(c.N), s>>>(
-      c, P, phase, final_mode, fout);
+      c, P, phase, final_mode, fout, cout);
 }
 
 void launch_step(const ClassDev& c, int phase, int probe_j, float probe_lam,

@@ -186,7 +186,7 @@ def make_class_kernels(plan, n_bands: int, n_terms: int, *, render_backend: str,
                        convergence: str = "legacy", plateau_dlnp_tol: float = 0.5,
                        render_mode: str = "reference",
                        native_stamp: int = 0, precision: str = "plain",
-                       tc_min_rows: int = -1) -> ClassKernels:
+                       tc_min_rows: int = -1, tc_cond_max: float = -1.0) -> ClassKernels:
     if stall_count_mode not in ("proposals", "changed"):
         raise ValueError(f"stall_count_mode must be 'proposals' or 'changed', "
                          f"got {stall_count_mode!r}")
@@ -231,7 +231,8 @@ def make_class_kernels(plan, n_bands: int, n_terms: int, *, render_backend: str,
         pos_step_max=float(pos_step_max_pix), chi2_ftol_rel=float(chi2_ftol_rel),
         step_tol_pix=float(step_tol_pix), un_freeze_steps=int(un_freeze_steps),
         has_priors=int(bool(has_priors)), native_stamp=int(native_stamp),
-        precision=_lib.PRECISIONS[precision], tc_min_rows=int(tc_min_rows))
+        precision=_lib.PRECISIONS[precision], tc_min_rows=int(tc_min_rows),
+        tc_cond_max=float(tc_cond_max))
     return ClassKernels(desc, render_mode, int(n_bands), str(plan.kind))
 
 

@@ -332,3 +332,64 @@ def make_serving_request(seed: int, device="cpu") -> Field:
     side, nb, n_src = serving_request_shape(rng)
     return make_production_field(seed, side=side, n_bands=nb, n_src=n_src,
                                  device=device, margin=min(40.0, side / 4.0))
+
+
+def make_blend_field(seed: int = 0, n_islands: int = 400, n_bands: int = 40,
+                     device="cpu", spacing: int = 64) -> Field:
+    """Precision-stress field: ``n_islands`` crowded blends of 2-12 point
+    sources on a grid ``spacing`` px apart.  Within a blend each new source
+    sits U(0.3, 1.5) FWHM from a random earlier member; the brightest has a
+    flux log-U(1e3, 1e6) and the others fainter by a ratio log-U(1, 1e4).  A
+    quarter of the bands scale every flux down to SNR ~3-10 for the faint
+    members.  PSF as in the production field (4-Gaussian, order-2
+    polynomial); islands by the production field's flux-aware radii."""
+    rng = np.random.default_rng(20_000 + seed)
+    g = int(math.ceil(math.sqrt(n_islands)))
+    side = g * spacing + spacing
+    nb, H, W = n_bands, side, side
+    native = 31
+    base = make_production_field(seed, side=64, n_bands=nb, n_src=5, margin=16)
+    mogs = [type(m)(m.sigma, m.e1, m.e2, m.weight, W / 2, W / 2, H / 2, H / 2)
+            for m in base.mog_psfs]
+    fwhm = 2.355 * float(np.mean([m.sigma[1, 0] for m in mogs]))
+    xs, ys, fl = [], [], []
+    for i in range(n_islands):
+        cx = spacing + (i % g) * spacing + rng.uniform(-2, 2)
+        cy = spacing + (i // g) * spacing + rng.uniform(-2, 2)
+        k = int(rng.integers(2, 13))
+        px, py = [cx], [cy]
+        for _ in range(k - 1):
+            j = int(rng.integers(0, len(px)))
+            r = rng.uniform(0.3, 1.5) * fwhm
+            a = rng.uniform(0, 2 * math.pi)
+            px.append(px[j] + r * math.cos(a))
+            py.append(py[j] + r * math.sin(a))
+        f0 = math.exp(rng.uniform(math.log(1e3), math.log(1e6)))
+        ratios = np.exp(rng.uniform(0, math.log(1e4), k))
+        ratios[0] = 1.0
+        xs.extend(px)
+        ys.extend(py)
+        fl.extend(f0 / ratios)
+    tx, ty = np.asarray(xs), np.asarray(ys)
+    n = tx.size
+    flux = np.asarray(fl)[:, None] * np.exp(rng.normal(0, 0.3, (n, nb)))
+    faint = rng.uniform(size=nb) < 0.25
+    flux[:, faint] *= np.exp(rng.uniform(np.log(1e-3), np.log(1e-2), faint.sum()))
+    st = np.full(n, SOURCE_STAR, np.int32)
+    zero = np.zeros(n, np.float32)
+    sn = np.ones(n, np.float32)
+    half = np.full(n, native // 2)
+    model = render_truth((nb, H, W), mogs, tx, ty, st, zero, zero, zero, sn, flux,
+                         half, device)
+    bg = np.full((nb, H, W), 100.0)
+    dmb, iv = _noise(model, bg, rng)
+    px = (tx + rng.normal(0, 0.3, n)).astype(np.float32)
+    py = (ty + rng.normal(0, 0.3, n)).astype(np.float32)
+    s1 = (flux * (1 + 0.05 * rng.normal(size=flux.shape))).astype(np.float32)
+    s1v = ((0.05 * flux) ** 2 + 25.0).astype(np.float32)
+    polys = [mog_to_poly_psf(m, native, W, H) for m in mogs]
+    stamp = polys[0].stamp_at(W / 2, H / 2)
+    iset, bk = _islands(px, py, st, zero, sn, native, s1_flux=s1, invvar=iv,
+                        psf_stamp=stamp)
+    return Field(dmb, iv, mogs, polys, px, py, st, zero, zero.copy(), zero.copy(),
+                 sn, s1, s1v, tx, ty, flux, iset, bk, native, (63, 127))
