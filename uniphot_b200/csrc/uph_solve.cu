@@ -136,10 +136,39 @@ __device__ void gram_window_small(const ClassDev& c, int isl, int b,
   __syncthreads();
 }
 
+__device__ __forceinline__ void cp_async4(float* dst, const float* src, bool valid) {
+  const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;"
+               :
+               : "r"(d), "l"(src), "r"(valid ? 4 : 0)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;" ::: "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.wait_group 0;" ::: "memory");
+}
+
+// Pixel-tile geometry of the tiled Gram path for K rows.
+__host__ __device__ __forceinline__ int gram_tile_pixels(int K) {
+  return (K <= 32) ? 128 : (K <= 96 ? 64 : 32);
+}
+
+// Tiled path (K > 8): the rows are staged UNWEIGHTED -- stamp values, data
+// (zero outside a member's box) and the raw weights -- by 4-byte cp.async
+// into double-buffered shared tiles, so the copies of tile t + 1 are in
+// flight while tile t is consumed; the weight enters the product
+// (sum_pix w z_i z_j).  In residual form the last row is rebuilt from the
+// staged model rows once a tile has landed (d - sum_k fc_k m_k in member
+// order, the trial pass's order).  Each thread accumulates one 8 x 8 block
+// of the upper triangle over its share of the pixels; the s threads sharing
+// a block are s consecutive lanes (s a power of two), reduced by shuffles in
+// a fixed order, and through a small shared buffer when s > 32.
 __device__ void gram_window(const ClassDev& c, int isl, int b, RowSrc rows,
                             const int4* box, float* out, int ld, int part,
                             float* sm) {
-  const int tid = threadIdx.x;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int K = rows.K;
   if (K <= 8) {
     if (part == 0) gram_window_small(c, isl, b, rows, box, out, ld, sm);
@@ -149,9 +178,10 @@ __device__ void gram_window(const ClassDev& c, int isl, int b, RowSrc rows,
   const int nblk = nbk * (nbk + 1) / 2;
   int s, my, split;
   if (nblk <= NT) {
-    s = NT / nblk;
+    s = 1;
+    while (2 * s * nblk <= NT) s *= 2;
     my = tid / s;
-    split = tid % s;
+    split = tid - my * s;
     if (my >= nblk) my = -1;
   } else {
     s = 1;
@@ -161,52 +191,94 @@ __device__ void gram_window(const ClassDev& c, int isl, int b, RowSrc rows,
   }
   int bi = 0, bj = 0;
   if (my >= 0) decode_upper(my, nbk, bi, bj);
-  const int TP = (K <= 32) ? 128 : (K <= 96 ? 64 : 32);
+  const int TP = gram_tile_pixels(K);
+  const int lgTP = (TP == 128) ? 7 : (TP == 64 ? 6 : 5);
   const int LD = TP + 1;
-  float* Zs = sm;                        // nbk*8 x LD
-  float* swt = Zs + nbk * 8 * LD;        // TP
+  const int nrows = nbk * 8;
+  // buffers: Z0 Z1 (nrows x LD each), W0 W1 (TP each), red ((NT / 32) x 64)
+  float* red = sm + 2 * nrows * LD + 2 * TP;
   const int B = c.B;
   const int npix = B * B;
+  const float invB = 1.0f / (float)B;
   const size_t plane = (size_t)c.Hp * c.Wp;
   const float* dbase = c.dstack + b * plane + (size_t)c.oy[isl] * c.Wp + c.ox[isl];
   const float* wbase = c.wstack + b * plane + (size_t)c.oy[isl] * c.Wp + c.ox[isl];
+  const int m0 = K - 1 - rows.nr;   // first model row (residual form)
+
+  auto stage = [&](int pix0, int bufi) {
+    float* Z = sm + bufi * nrows * LD;
+    float* Wt = sm + 2 * nrows * LD + bufi * TP;
+    for (int e = tid; e < nrows * TP; e += NT) {
+      const int r = e >> lgTP, q = e & (TP - 1);
+      const int pix = pix0 + q;
+      const float* src = dbase;
+      bool ok = false;
+      if (r < K && pix < npix) {
+        const int wy = (int)(((float)pix + 0.5f) * invB);
+        const int wx = pix - wy * B;
+        const int rs = rows.rs[r];
+        if (rs < 0) {
+          src = dbase + (size_t)wy * c.Wp + wx;
+          ok = true;
+        } else {
+          const int k = rows.rk[r];
+          const int4 bx = box[k];
+          const int ly = wy - bx.y, lx = wx - bx.x;
+          if (ly >= 0 && ly < bx.w && lx >= 0 && lx < bx.z) {
+            src = c.stamps + stamp_slot(c, isl, b, k, rs) + (size_t)ly * c.Sz + lx;
+            ok = true;
+          }
+        }
+      }
+      cp_async4(Z + r * LD + q, src, ok);
+    }
+    for (int q = tid; q < TP; q += NT) {
+      const int pix = pix0 + q;
+      const float* src = wbase;
+      bool ok = false;
+      if (pix < npix) {
+        const int wy = (int)(((float)pix + 0.5f) * invB);
+        src = wbase + (size_t)wy * c.Wp + (pix - wy * B);
+        ok = true;
+      }
+      cp_async4(Wt + q, src, ok);
+    }
+    cp_async_commit();
+  };
+
   float acc[8][8];
 #pragma unroll
   for (int i = 0; i < 8; ++i)
 #pragma unroll
     for (int j = 0; j < 8; ++j) acc[i][j] = 0.f;
-  const int nrows = nbk * 8;
-  for (int pix0 = 0; pix0 < npix; pix0 += TP) {
-    for (int q = tid; q < TP; q += NT) {
-      const int pix = pix0 + q;
-      float sw = 0.f;
-      if (pix < npix) {
-        const int wy = pix / B, wx = pix - (pix / B) * B;
-        sw = sqrtf(wbase[(size_t)wy * c.Wp + wx]);
-      }
-      swt[q] = sw;
-    }
+  const int ntile = (npix + TP - 1) / TP;
+  stage(0, 0);
+  for (int t = 0; t < ntile; ++t) {
+    const int cur = t & 1;
+    cp_async_wait_all();
     __syncthreads();
-    for (int e = tid; e < nrows * TP; e += NT) {
-      const int r = e / TP, q = e - (e / TP) * TP;
-      const int pix = pix0 + q;
-      float v = 0.f;
-      if (r < K && pix < npix) {
-        const int wy = pix / B, wx = pix - (pix / B) * B;
-        v = row_value(c, isl, b, rows, box, r, wy, wx, swt[q], dbase);
+    float* Z = sm + cur * nrows * LD;
+    const float* Wt = sm + 2 * nrows * LD + cur * TP;
+    if (rows.fc) {
+      // residual row from the staged model rows
+      for (int q = tid; q < TP; q += NT) {
+        float model = 0.f;
+        for (int k = 0; k < rows.nr; ++k) model = fmaf(rows.fc[k], Z[(m0 + k) * LD + q], model);
+        Z[(K - 1) * LD + q] = Z[(K - 1) * LD + q] - model;
       }
-      Zs[r * LD + q] = v;
+      __syncthreads();
     }
-    __syncthreads();
+    if (t + 1 < ntile) stage((t + 1) * TP, cur ^ 1);
     if (my >= 0) {
-      const float* za = Zs + bi * 8 * LD;
-      const float* zb = Zs + bj * 8 * LD;
+      const float* za = Z + bi * 8 * LD;
+      const float* zb = Z + bj * 8 * LD;
       for (int q = split; q < TP; q += s) {
+        const float w = Wt[q];
         float a[8], bb[8];
 #pragma unroll
         for (int i = 0; i < 8; ++i) {
           a[i] = za[i * LD + q];
-          bb[i] = zb[i * LD + q];
+          bb[i] = zb[i * LD + q] * w;
         }
 #pragma unroll
         for (int i = 0; i < 8; ++i)
@@ -214,35 +286,46 @@ __device__ void gram_window(const ClassDev& c, int isl, int b, RowSrc rows,
           for (int j = 0; j < 8; ++j) acc[i][j] = fmaf(a[i], bb[j], acc[i][j]);
       }
     }
-    __syncthreads();
   }
-  // deterministic tree reduction over the pixel splits of each block
-  if (s > 1) {
-    float* red = sm;  // NT x 65
-    for (int i = 0; i < 8; ++i)
-      for (int j = 0; j < 8; ++j) red[tid * 65 + i * 8 + j] = acc[i][j];
-    __syncthreads();
-    int cur = s;
-    while (cur > 1) {
-      const int half = (cur + 1) >> 1;
-      if (my >= 0 && split + half < cur)
-        for (int e = 0; e < 64; ++e) red[tid * 65 + e] += red[(tid + half) * 65 + e];
-      __syncthreads();
-      cur = half;
+  // fixed-order reduction over the s pixel splits of each block
+  const int sw = s < 32 ? s : 32;
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      float v = acc[i][j];
+      for (int o = 1; o < sw; o <<= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+      acc[i][j] = v;
     }
-    if (my >= 0 && split == 0)
-      for (int i = 0; i < 8; ++i)
-        for (int j = 0; j < 8; ++j) acc[i][j] = red[tid * 65 + i * 8 + j];
+  if (s > 32) {
+    // one partial per warp; warps of a block are consecutive
+    __syncthreads();
+    if (lane == 0) {
+#pragma unroll
+      for (int e = 0; e < 64; ++e) red[warp * 64 + e] = acc[e >> 3][e & 7];
+    }
+    __syncthreads();
+    if (my >= 0 && split == 0) {
+      const int w0 = (my * s) >> 5, nw = s >> 5;
+#pragma unroll
+      for (int e = 0; e < 64; ++e) {
+        float t = red[w0 * 64 + e];
+        for (int w = 1; w < nw; ++w) t += red[(w0 + w) * 64 + e];
+        acc[e >> 3][e & 7] = t;
+      }
+    }
   }
   if (my >= 0 && split == 0) {
+#pragma unroll
     for (int i = 0; i < 8; ++i) {
       const int gi = bi * 8 + i;
-      if (gi >= K) break;
+#pragma unroll
       for (int j = 0; j < 8; ++j) {
         const int gj = bj * 8 + j;
-        if (gj >= K) break;
-        out[gi * ld + gj] = acc[i][j];
-        out[gj * ld + gi] = acc[i][j];
+        if (gi < K && gj < K) {
+          out[gi * ld + gj] = acc[i][j];
+          out[gj * ld + gi] = acc[i][j];
+        }
       }
     }
   }
@@ -893,11 +976,16 @@ void launch_set_probe(const ClassDev& c, cudaStream_t s) {
 }
 
 size_t gram_lin_smem_bytes(int Kmax) {
-  const int nbk = (Kmax + 7) / 8;
-  const int TP = (Kmax <= 32) ? 128 : (Kmax <= 96 ? 64 : 32);
-  size_t zs = sizeof(float) * ((size_t)nbk * 8 * (TP + 1) + TP);
-  size_t red = sizeof(float) * (size_t)NT * 65;
-  return zs > red ? zs : red;
+  // the largest tiled-path footprint over K <= Kmax (the tile width shrinks
+  // as K grows), and the small path's per-warp partials
+  size_t best = sizeof(float) * (size_t)(NT / 32) * 36;
+  for (int K = 9; K <= Kmax; ++K) {
+    const int nrows = ((K + 7) / 8) * 8;
+    const int TP = gram_tile_pixels(K);
+    const size_t b = sizeof(float) * ((size_t)2 * nrows * (TP + 1) + 2 * TP + (NT / 32) * 64);
+    if (b > best) best = b;
+  }
+  return best;
 }
 
 size_t gram_trial_smem_bytes(int N) { return gram_lin_smem_bytes(N + 1); }
