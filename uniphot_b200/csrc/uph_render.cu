@@ -22,7 +22,6 @@ namespace {
 
 constexpr int NS = 7;            // S arrays: S, Sx, Sy, Slr, Se1, Se2, Su
 constexpr int HP = UPH_HALO + 1; // padded halo pitch
-constexpr int XP = UPH_TILE + 1;
 
 struct MemberSetup {
   float Lx[7], dLx[7], Ly[7], dLy[7];
@@ -431,7 +430,6 @@ __global__ void __launch_bounds__(256)
 k_render(ClassDev c, const float* __restrict__ P, int phase, int nsa) {
   extern __shared__ float smem[];
   __shared__ MemberSetup ms;
-  __shared__ GComp comps[UPH_MAXKPSF * UPH_MAXGAL];
   __shared__ float4 trec[MAXCOMP * 7];   // per-tile component records
   __shared__ MemberBox mb;
   const int ntile = c.ntile_side * c.ntile_side;
@@ -484,11 +482,6 @@ k_render(ClassDev c, const float* __restrict__ P, int phase, int nsa) {
       ms.betax[tt] = rec->betax[tt];
       ms.betay[tt] = rec->betay[tt];
     }
-  } else {
-    const int nf = rec->ncomp * (int)(sizeof(GComp) / sizeof(float));
-    const float* src = reinterpret_cast<const float*>(rec->comps);
-    float* dst = reinterpret_cast<float*>(comps);
-    for (int e = tid; e < nf; e += blockDim.x) dst[e] = src[e];
   }
   __syncthreads();
   if (mb.bw <= 0 || mb.bh <= 0) return;
@@ -505,8 +498,7 @@ k_render(ClassDev c, const float* __restrict__ P, int phase, int nsa) {
   }
   const int si0 = oy0 - mb.iyt, sj0 = ox0 - mb.ixt;  // stamp coords of tile
   const int hr = oh + 6, hc = ow + 6;
-  float* S = smem;                           // NS * UPH_HALO * HP
-  float* X = smem + nsa * UPH_HALO * HP;     // nsa * UPH_HALO * XP
+  float* S = smem;   // nsa * UPH_HALO * HP; the x pass overwrites it in place
   const int T = c.T, c0 = c.T / 2;
   const int hs = ms.support_half;
   // halo rectangle intersected with the support box (offsets from centre)
@@ -519,7 +511,7 @@ k_render(ClassDev c, const float* __restrict__ P, int phase, int nsa) {
     if (tid == 0) ms.nact = 0;
     __syncthreads();
     for (int q = tid; q < ms.ncomp; q += blockDim.x) {
-      const GComp& o = comps[q];
+      const GComp& o = rec->comps[q];
       ms.act[q] = qmin_box(o.ia, o.ib, o.ic, (float)xlo, (float)xhi, (float)ylo,
                            (float)yhi) <= QCUT;
     }
@@ -538,7 +530,7 @@ k_render(ClassDev c, const float* __restrict__ P, int phase, int nsa) {
   if (lin) nout = ms.is_gal ? 6 : ((ms.need[1] || ms.need[2]) ? 2 : 0);
   if (!empty && c.mode == 1) {
     for (int a = tid; a < ms.nact; a += blockDim.x) {
-      const GComp& o = comps[ms.act[a]];
+      const GComp& o = rec->comps[ms.act[a]];
       float4* r = trec + a * (nout + 1);
       r[0] = make_float4(KEXP * o.ia, 2.f * KEXP * o.ib, KEXP * o.ic, o.nrm);
       if (nout == 0) continue;
@@ -644,32 +636,50 @@ k_render(ClassDev c, const float* __restrict__ P, int phase, int nsa) {
   }
   __syncthreads();
 
-  // ---- x pass: X0 = cx(S,L), X1 = cx(S,dL) + cx(Sx,L), X2 = cx(Sy,L),
-  //      X3..5 = cx(S_shape,L), X6 = cx(Su,L) ----
-  const bool dox = ms.live_row[0] != 0;
-  for (int e = tid; e < hr * ow; e += blockDim.x) {
-    const int r = e / ow, cc = e % ow;
-    const float* s0 = S + (0 * UPH_HALO + r) * HP + cc;
-    float a0 = ms.Lx[0] * s0[0];
-    for (int q = 1; q < 7; ++q) a0 = fmaf(ms.Lx[q], s0[q], a0);
-    X[(0 * UPH_HALO + r) * XP + cc] = a0;
-    if (dox) {
-      float a1 = ms.dLx[0] * s0[0];
-      for (int q = 1; q < 7; ++q) a1 = fmaf(ms.dLx[q], s0[q], a1);
-      if (ms.need[1]) {
-        const float* s1 = S + (1 * UPH_HALO + r) * HP + cc;
-        float b1 = ms.Lx[0] * s1[0];
-        for (int q = 1; q < 7; ++q) b1 = fmaf(ms.Lx[q], s1[q], b1);
-        a1 += b1;
+  // ---- x pass, in place: X0 = cx(S,L), X1 = cx(S,dL) + cx(Sx,L),
+  //      X2 = cx(Sy,L), X3..5 = cx(S_shape,L), X6 = cx(Su,L).  One warp per
+  //      halo row (lane = output column): a row's outputs depend only on that
+  //      row, so the warp reads all of it, syncs, then overwrites it ----
+  {
+    const bool dox = ms.live_row[0] != 0;
+    const int lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+    for (int r = warp; r < hr; r += nw) {
+      float xv[NS];
+      const int cc = lane;
+      if (cc < ow) {
+        const float* s0 = S + (0 * UPH_HALO + r) * HP + cc;
+        float a0 = ms.Lx[0] * s0[0];
+        for (int q = 1; q < 7; ++q) a0 = fmaf(ms.Lx[q], s0[q], a0);
+        xv[0] = a0;
+        if (dox) {
+          float a1 = ms.dLx[0] * s0[0];
+          for (int q = 1; q < 7; ++q) a1 = fmaf(ms.dLx[q], s0[q], a1);
+          if (ms.need[1]) {
+            const float* s1 = S + (1 * UPH_HALO + r) * HP + cc;
+            float b1 = ms.Lx[0] * s1[0];
+            for (int q = 1; q < 7; ++q) b1 = fmaf(ms.Lx[q], s1[q], b1);
+            a1 += b1;
+          }
+          xv[1] = a1;
+        }
+#pragma unroll
+        for (int sa = 2; sa < NS; ++sa) {
+          if (!ms.need[sa]) continue;
+          const float* sp = S + (sa * UPH_HALO + r) * HP + cc;
+          float a = ms.Lx[0] * sp[0];
+          for (int q = 1; q < 7; ++q) a = fmaf(ms.Lx[q], sp[q], a);
+          xv[sa] = a;
+        }
       }
-      X[(1 * UPH_HALO + r) * XP + cc] = a1;
-    }
-    for (int s = 2; s < NS; ++s) {
-      if (!ms.need[s]) continue;
-      const float* sp = S + (s * UPH_HALO + r) * HP + cc;
-      float a = ms.Lx[0] * sp[0];
-      for (int q = 1; q < 7; ++q) a = fmaf(ms.Lx[q], sp[q], a);
-      X[(s * UPH_HALO + r) * XP + cc] = a;
+      __syncwarp();
+      if (cc < ow) {
+        S[(0 * UPH_HALO + r) * HP + cc] = xv[0];
+        if (dox) S[(1 * UPH_HALO + r) * HP + cc] = xv[1];
+#pragma unroll
+        for (int sa = 2; sa < NS; ++sa)
+          if (ms.need[sa]) S[(sa * UPH_HALO + r) * HP + cc] = xv[sa];
+      }
+      __syncwarp();
     }
   }
   __syncthreads();
@@ -680,24 +690,24 @@ k_render(ClassDev c, const float* __restrict__ P, int phase, int nsa) {
     const int rr = e / ow, cc = e % ow;
     const int wy = oy0 + rr, wx = ox0 + cc;
     const size_t off = (size_t)(wy - mb.wy0) * Sz + (wx - mb.wx0);
-    const float* x0 = X + (0 * UPH_HALO + rr) * XP + cc;
+    const float* x0 = S + (0 * UPH_HALO + rr) * HP + cc;
     float m = ms.Ly[0] * x0[0];
-    for (int q = 1; q < 7; ++q) m = fmaf(ms.Ly[q], x0[q * XP], m);
+    for (int q = 1; q < 7; ++q) m = fmaf(ms.Ly[q], x0[q * HP], m);
     c.stamps[stamp_slot(c, isl, b, k, 0) + off] = m;
     if (!lin) continue;
     if (ms.live_row[0]) {
-      const float* x1 = X + (1 * UPH_HALO + rr) * XP + cc;
+      const float* x1 = S + (1 * UPH_HALO + rr) * HP + cc;
       float d = ms.Ly[0] * x1[0];
-      for (int q = 1; q < 7; ++q) d = fmaf(ms.Ly[q], x1[q * XP], d);
+      for (int q = 1; q < 7; ++q) d = fmaf(ms.Ly[q], x1[q * HP], d);
       c.stamps[stamp_slot(c, isl, b, k, ms.live_row[0]) + off] = d;
     }
     if (ms.live_row[1]) {
       float d = ms.dLy[0] * x0[0];
-      for (int q = 1; q < 7; ++q) d = fmaf(ms.dLy[q], x0[q * XP], d);
+      for (int q = 1; q < 7; ++q) d = fmaf(ms.dLy[q], x0[q * HP], d);
       if (ms.need[2]) {
-        const float* x2 = X + (2 * UPH_HALO + rr) * XP + cc;
+        const float* x2 = S + (2 * UPH_HALO + rr) * HP + cc;
         float d2 = ms.Ly[0] * x2[0];
-        for (int q = 1; q < 7; ++q) d2 = fmaf(ms.Ly[q], x2[q * XP], d2);
+        for (int q = 1; q < 7; ++q) d2 = fmaf(ms.Ly[q], x2[q * HP], d2);
         d += d2;
       }
       c.stamps[stamp_slot(c, isl, b, k, ms.live_row[1]) + off] = d;
@@ -705,9 +715,9 @@ k_render(ClassDev c, const float* __restrict__ P, int phase, int nsa) {
     for (int j = 2; j < 6; ++j) {
       if (!ms.live_row[j]) continue;
       const int s = j + 1;  // S arrays 3..6 hold lr, e1, e2, u
-      const float* xs = X + (s * UPH_HALO + rr) * XP + cc;
+      const float* xs = S + (s * UPH_HALO + rr) * HP + cc;
       float d = ms.Ly[0] * xs[0];
-      for (int q = 1; q < 7; ++q) d = fmaf(ms.Ly[q], xs[q * XP], d);
+      for (int q = 1; q < 7; ++q) d = fmaf(ms.Ly[q], xs[q * HP], d);
       c.stamps[stamp_slot(c, isl, b, k, ms.live_row[j]) + off] = d;
     }
   }
@@ -716,7 +726,7 @@ k_render(ClassDev c, const float* __restrict__ P, int phase, int nsa) {
 }  // namespace
 
 size_t render_smem_bytes() {
-  return sizeof(float) * (size_t)NS * UPH_HALO * (HP + XP);
+  return sizeof(float) * (size_t)NS * UPH_HALO * HP;
 }
 
 // Shared arrays a launch needs: every S/X slot index used by the phase is
@@ -731,7 +741,7 @@ void launch_render(const ClassDev& c, const float* P, int phase,
   const long long nblk = (long long)c.n_isl * c.nb * c.N * c.ntile_side * c.ntile_side;
   if (nblk <= 0) return;
   const int nsa = render_arrays(c, phase);
-  const size_t bytes = sizeof(float) * (size_t)nsa * UPH_HALO * (HP + XP);
+  const size_t bytes = sizeof(float) * (size_t)nsa * UPH_HALO * HP;
   k_member_setup<<<(unsigned)((long long)c.n_isl * c.nb * c.N), 128, 0, s>>>(c, P, phase);
   k_render<<<(unsigned)nblk, 256, bytes, s>>>(c, P, phase, nsa);
 }
