@@ -915,8 +915,13 @@ int job_solve(uph_job* job, int max_steps) {
   for (int i = 0; i < nch; ++i) {
     int e = 0;
     CK(cudaMemcpy(&e, job->chunks[i]->c.err, sizeof(int), cudaMemcpyDeviceToHost), "err");
-    if (e) return set_err(ctx, UPH_ERR_TIMEOUT,
-                          "a bounded device wait expired in chunk %d (tensor-core Gram)", i);
+    if (e == 1)
+      return set_err(ctx, UPH_ERR_TIMEOUT,
+                     "a bounded device wait expired in chunk %d (tensor-core Gram)", i);
+    if (e)
+      return set_err(ctx, UPH_ERR_CUDA,
+                     "chunk %d: a kernel was launched with less shared memory than its "
+                     "tiles need (device check %d)", i, e);
   }
   cudaEventElapsedTime(&ctx->timing[1], ctx->ev[0], ctx->ev[2]);
   for (auto* ch : job->chunks) cudaEventElapsedTime(&ch->done_ms, ctx->ev[0], ch->ev_done);

@@ -131,7 +131,8 @@ struct ClassDev {
   float* probe_best;       // (n_isl) plateau certificate
   float* probe_p;          // (n_isl, 4, nP) diverged-probe proposals
   int* n_active;
-  int* err;                // device error flag (bounded waits that expired)
+  int* err;                // device error flag: 1 a bounded wait expired,
+                           // 2 a launch had too little shared memory
   // (WK_KINDS, 2) algorithmic bytes and flops per kernel kind, added by every
   // working CTA; non-null only during instrumented solves
   unsigned long long* work;

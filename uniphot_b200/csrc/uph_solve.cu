@@ -155,6 +155,76 @@ __host__ __device__ __forceinline__ int gram_tile_pixels(int K) {
   return (K <= 32) ? 128 : (K <= 96 ? 64 : 32);
 }
 
+// Stage pixels [pix0, pix0 + TP) of rows 0..K-1 UNWEIGHTED (stamp values,
+// data; zero outside a member's box) into Z (pitch LD) and the raw weights
+// into Wt, by 4-byte cp.async (one commit group).  Rows K..nrows-1 are not
+// touched: the caller zeroes them once.
+__device__ __forceinline__ void stage_rows(const ClassDev& c, int isl, int b,
+                                           const RowSrc& rows, const int4* box,
+                                           float* Z, float* Wt, int pix0, int TP,
+                                           int lgTP, int LD, int nrows) {
+  const int tid = threadIdx.x;
+  const int K = rows.K, B = c.B, npix = B * B;
+  const float invB = 1.0f / (float)B;
+  const size_t plane = (size_t)c.Hp * c.Wp;
+  const float* dbase = c.dstack + b * plane + (size_t)c.oy[isl] * c.Wp + c.ox[isl];
+  const float* wbase = c.wstack + b * plane + (size_t)c.oy[isl] * c.Wp + c.ox[isl];
+  for (int e = tid; e < K * TP; e += blockDim.x) {
+    const int r = e >> lgTP, q = e & (TP - 1);
+    const int pix = pix0 + q;
+    const float* src = dbase;
+    bool ok = false;
+    if (pix < npix) {
+      const int wy = (int)(((float)pix + 0.5f) * invB);
+      const int wx = pix - wy * B;
+      const int rs = rows.rs[r];
+      if (rs < 0) {
+        src = dbase + (size_t)wy * c.Wp + wx;
+        ok = true;
+      } else {
+        const int k = rows.rk[r];
+        const int4 bx = box[k];
+        const int ly = wy - bx.y, lx = wx - bx.x;
+        if (ly >= 0 && ly < bx.w && lx >= 0 && lx < bx.z) {
+          src = c.stamps + stamp_slot(c, isl, b, k, rs) + (size_t)ly * c.Sz + lx;
+          ok = true;
+        }
+      }
+    }
+    cp_async4(Z + r * LD + q, src, ok);
+  }
+  for (int q = tid; q < TP; q += blockDim.x) {
+    const int pix = pix0 + q;
+    const float* src = wbase;
+    bool ok = false;
+    if (pix < npix) {
+      const int wy = (int)(((float)pix + 0.5f) * invB);
+      src = wbase + (size_t)wy * c.Wp + (pix - wy * B);
+      ok = true;
+    }
+    cp_async4(Wt + q, src, ok);
+  }
+  cp_async_commit();
+}
+
+__host__ __device__ __forceinline__ int log2_tile(int TP) {
+  return (TP == 128) ? 7 : (TP == 64 ? 6 : 5);
+}
+
+// Dynamic shared floats the staged tiles of K rows use: two tiles of
+// ceil8(K) rows x (TP + 1), two weight rows, the cross-warp partials.
+__host__ __device__ __forceinline__ int tile_floats(int K) {
+  const int nrows = ((K + 7) / 8) * 8;
+  const int TP = gram_tile_pixels(K);
+  return 2 * nrows * (TP + 1) + 2 * TP + (NT / 32) * 64;
+}
+
+__device__ __forceinline__ unsigned dynamic_smem_bytes() {
+  unsigned v;
+  asm volatile("mov.u32 %0, %%dynamic_smem_size;" : "=r"(v));
+  return v;
+}
+
 // Tiled path (K > 8): the rows are staged UNWEIGHTED -- stamp values, data
 // (zero outside a member's box) and the raw weights -- by 4-byte cp.async
 // into double-buffered shared tiles, so the copies of tile t + 1 are in
@@ -172,6 +242,11 @@ __device__ void gram_window(const ClassDev& c, int isl, int b, RowSrc rows,
   const int K = rows.K;
   if (K <= 8) {
     if (part == 0) gram_window_small(c, isl, b, rows, box, out, ld, sm);
+    return;
+  }
+  if (sizeof(float) * (size_t)tile_floats(K) > dynamic_smem_bytes()) {
+    // launched with too little shared memory for these tiles: report, skip
+    if (threadIdx.x == 0 && c.err) atomicExch(c.err, 2);
     return;
   }
   const int nbk = (K + 7) / 8;
@@ -192,58 +267,16 @@ __device__ void gram_window(const ClassDev& c, int isl, int b, RowSrc rows,
   int bi = 0, bj = 0;
   if (my >= 0) decode_upper(my, nbk, bi, bj);
   const int TP = gram_tile_pixels(K);
-  const int lgTP = (TP == 128) ? 7 : (TP == 64 ? 6 : 5);
+  const int lgTP = log2_tile(TP);
   const int LD = TP + 1;
   const int nrows = nbk * 8;
   // buffers: Z0 Z1 (nrows x LD each), W0 W1 (TP each), red ((NT / 32) x 64)
   float* red = sm + 2 * nrows * LD + 2 * TP;
-  const int B = c.B;
-  const int npix = B * B;
-  const float invB = 1.0f / (float)B;
-  const size_t plane = (size_t)c.Hp * c.Wp;
-  const float* dbase = c.dstack + b * plane + (size_t)c.oy[isl] * c.Wp + c.ox[isl];
-  const float* wbase = c.wstack + b * plane + (size_t)c.oy[isl] * c.Wp + c.ox[isl];
+  const int npix = c.B * c.B;
   const int m0 = K - 1 - rows.nr;   // first model row (residual form)
-
   auto stage = [&](int pix0, int bufi) {
-    float* Z = sm + bufi * nrows * LD;
-    float* Wt = sm + 2 * nrows * LD + bufi * TP;
-    for (int e = tid; e < nrows * TP; e += NT) {
-      const int r = e >> lgTP, q = e & (TP - 1);
-      const int pix = pix0 + q;
-      const float* src = dbase;
-      bool ok = false;
-      if (r < K && pix < npix) {
-        const int wy = (int)(((float)pix + 0.5f) * invB);
-        const int wx = pix - wy * B;
-        const int rs = rows.rs[r];
-        if (rs < 0) {
-          src = dbase + (size_t)wy * c.Wp + wx;
-          ok = true;
-        } else {
-          const int k = rows.rk[r];
-          const int4 bx = box[k];
-          const int ly = wy - bx.y, lx = wx - bx.x;
-          if (ly >= 0 && ly < bx.w && lx >= 0 && lx < bx.z) {
-            src = c.stamps + stamp_slot(c, isl, b, k, rs) + (size_t)ly * c.Sz + lx;
-            ok = true;
-          }
-        }
-      }
-      cp_async4(Z + r * LD + q, src, ok);
-    }
-    for (int q = tid; q < TP; q += NT) {
-      const int pix = pix0 + q;
-      const float* src = wbase;
-      bool ok = false;
-      if (pix < npix) {
-        const int wy = (int)(((float)pix + 0.5f) * invB);
-        src = wbase + (size_t)wy * c.Wp + (pix - wy * B);
-        ok = true;
-      }
-      cp_async4(Wt + q, src, ok);
-    }
-    cp_async_commit();
+    stage_rows(c, isl, b, rows, box, sm + bufi * nrows * LD,
+               sm + 2 * nrows * LD + bufi * TP, pix0, TP, lgTP, LD, nrows);
   };
 
   float acc[8][8];
@@ -252,6 +285,12 @@ __device__ void gram_window(const ClassDev& c, int isl, int b, RowSrc rows,
 #pragma unroll
     for (int j = 0; j < 8; ++j) acc[i][j] = 0.f;
   const int ntile = (npix + TP - 1) / TP;
+  // padding rows K..nrows-1 of both tiles stay zero for the whole pass
+  for (int e = tid; e < (nrows - K) * LD; e += NT) {
+    sm[K * LD + e] = 0.f;
+    sm[nrows * LD + K * LD + e] = 0.f;
+  }
+  __syncthreads();
   stage(0, 0);
   for (int t = 0; t < ntile; ++t) {
     const int cur = t & 1;
@@ -976,13 +1015,12 @@ void launch_set_probe(const ClassDev& c, cudaStream_t s) {
 }
 
 size_t gram_lin_smem_bytes(int Kmax) {
-  // the largest tiled-path footprint over K <= Kmax (the tile width shrinks
-  // as K grows), and the small path's per-warp partials
+  // the largest staged-tile footprint over every K <= Kmax (the tile width
+  // shrinks as K grows; the trial pass stages tiles for its residual even
+  // when its Gram takes the small path), and the small path's partials
   size_t best = sizeof(float) * (size_t)(NT / 32) * 36;
-  for (int K = 9; K <= Kmax; ++K) {
-    const int nrows = ((K + 7) / 8) * 8;
-    const int TP = gram_tile_pixels(K);
-    const size_t b = sizeof(float) * ((size_t)2 * nrows * (TP + 1) + 2 * TP + (NT / 32) * 64);
+  for (int K = 1; K <= Kmax; ++K) {
+    const size_t b = sizeof(float) * (size_t)tile_floats(K);
     if (b > best) best = b;
   }
   return best;
