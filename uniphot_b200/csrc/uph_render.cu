@@ -426,11 +426,15 @@ k_member_setup(ClassDev c, const float* __restrict__ P, int phase) {
   }
 }
 
+template <bool LIN>
 __global__ void __launch_bounds__(256)
 k_render(ClassDev c, const float* __restrict__ P, int phase, int nsa) {
+  // LIN: linearisation render (model and derivative rows); the trial and
+  // probe renders (model row only) are a separate instantiation that needs
+  // far fewer registers, hence more CTAs per SM
   extern __shared__ float smem[];
   __shared__ MemberSetup ms;
-  __shared__ float4 trec[MAXCOMP * 7];   // per-tile component records
+  __shared__ float4 trec[MAXCOMP * (LIN ? 7 : 1)];   // per-tile component records
   __shared__ MemberBox mb;
   const int ntile = c.ntile_side * c.ntile_side;
   int t = blockIdx.x;
@@ -443,7 +447,7 @@ k_render(ClassDev c, const float* __restrict__ P, int phase, int nsa) {
   if (isl >= c.n_isl) return;
   if (!isl_active(c.flags[isl], phase)) return;
   if (!c.mmask[isl * c.N + k]) return;
-  const bool lin = (phase == PH_LIN);
+  constexpr bool lin = LIN;
   const int tid = threadIdx.x;
 
   const MemberRecord* rec = c.mrec + ((size_t)isl * c.nb + b) * c.N + k;
@@ -743,11 +747,18 @@ void launch_render(const ClassDev& c, const float* P, int phase,
   const int nsa = render_arrays(c, phase);
   const size_t bytes = sizeof(float) * (size_t)nsa * UPH_HALO * HP;
   k_member_setup<<<(unsigned)((long long)c.n_isl * c.nb * c.N), 128, 0, s>>>(c, P, phase);
-  k_render<<<(unsigned)nblk, 256, bytes, s>>>(c, P, phase, nsa);
+  if (phase == PH_LIN)
+    k_render<true><<<(unsigned)nblk, 256, bytes, s>>>(c, P, phase, nsa);
+  else
+    k_render<false><<<(unsigned)nblk, 256, bytes, s>>>(c, P, phase, nsa);
 }
 
 int uph_render_setup() {
-  return (int)cudaFuncSetAttribute(k_render,
+  cudaError_t e = cudaFuncSetAttribute(k_render<true>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)render_smem_bytes());
+  if (e != cudaSuccess) return (int)e;
+  return (int)cudaFuncSetAttribute(k_render<false>,
                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)render_smem_bytes());
 }
