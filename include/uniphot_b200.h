@@ -66,6 +66,11 @@ typedef struct uph_class_desc {
   int32_t tc_min_rows;      /* mixed form: Gram-row threshold of the
                                tensor-core path; < 0 selects the default
                                (UPH_TC_MIN_ROWS_DEFAULT)                   */
+  int32_t bg_joint;         /* 1: each band's planar background (1, X, Y
+                               over the island window) is solved with the
+                               fluxes in the inner linear step; 0: the data
+                               are background-subtracted (the reference's
+                               island mode)                                */
   float tc_cond_max;        /* mixed form: islands whose members' scaled
                                normal matrix has a conditioning indicator
                                above this (in any band) form the Gram in
@@ -121,6 +126,9 @@ typedef struct uph_chunk_out {
   int32_t* nrej;        /* [n]                                             */
   int64_t* n_good;      /* [n]  unmasked pixels summed over bands          */
   int32_t steps_run;    /* LM iterations executed for the chunk            */
+  float* bg;            /* [n*nb*3] planar background (1, X, Y) per band
+                           when bg_joint; may be NULL                      */
+  float* bg_err;        /* [n*nb*3] its sqrt(diag inv A64); may be NULL    */
 } uph_chunk_out;
 
 /* Context: one per device per process. */

@@ -37,23 +37,23 @@ def psf_bands(psfs, tier: int, mode: str):
 
 
 def _one(args):
-    host, row, B, T, dstack, wstack, psf, table, mode, cfg, max_steps, native = args
+    host, row, B, T, dstack, wstack, psf, table, mode, cfg, max_steps, native, bg = args
     isl = island_inputs_from_host(host, row, B=B, T=T, dstack=dstack,
                                   wstack=wstack, psf=psf, table=table, mode=mode,
-                                  native=native)
+                                  native=native, bg_joint=bg)
     return solve_island(isl, cfg, max_steps)
 
 
 def solve_chunk(host, rows, *, B, T, dstack, wstack, psfs, mode, table_path=None,
                 precision="ref", max_steps=30, reg=1e-9, pos_step_max=0.5,
                 ftol_rel=1e-4, step_tol=0.1, processes: int = 1,
-                native: int = 0) -> dict:
+                native: int = 0, bg_joint: bool = False) -> dict:
     table = SersicTable.load(table_path) if table_path is not None else None
     psf = psf_bands(psfs, T, mode)
     cfg = SolverConfig(reg=reg, pos_step_max=pos_step_max, ftol_rel=ftol_rel,
                        step_tol=step_tol, precision=precision)
     jobs = [(host, int(r), B, T, dstack, wstack, psf, table, mode, cfg, max_steps,
-             native) for r in rows]
+             native, bg_joint) for r in rows]
     if processes > 1 and len(jobs) > 1:
         import multiprocessing as mp
         with mp.get_context("spawn").Pool(processes) as pool:
@@ -61,7 +61,7 @@ def solve_chunk(host, rows, *, B, T, dstack, wstack, psfs, mode, table_path=None
     else:
         res = [_one(j) for j in jobs]
     out = {}
-    for k in ("p", "fluxes", "ferr", "chi2", "conv", "stall", "diverged",
+    for k in ("p", "fluxes", "ferr", "bg", "bg_err", "chi2", "conv", "stall", "diverged",
               "stall_dchi2", "nst", "lam", "consec", "nrej", "n_good"):
         out[k] = np.stack([np.asarray(r[k]) for r in res])
     out["steps_run"] = int(max(r["steps"] for r in res))

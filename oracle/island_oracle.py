@@ -380,6 +380,7 @@ class IslandInput:
     table: SersicTable | None
     mode: str                # "reference" | "analytic"
     native: int = 0          # star support side (0 = the tier)
+    bg_joint: bool = False   # planar background (1, X, Y) solved with the fluxes
 
 
 @dataclass
@@ -612,12 +613,33 @@ class IslandSolver:
                                       x0 - ix_top:x1 - ix_top]
         return out
 
+    def bg_basis(self):
+        """(3, B, B) planar background basis over the island window:
+        1, X = (x - c) / s, Y = (y - c) / s with c = (B - 1) / 2, s = B / 2
+        (the per-tile plane of forced_phot_sparse.py:417-497 /
+        bg_polynomial.py:125-178 at order 1, the island window as its
+        tile), in the working precision."""
+        B = self.isl.B
+        c, sc = (B - 1) / 2.0, B / 2.0
+        X = ((np.arange(B, dtype=np.float64) - c) / sc).astype(np.float32)
+        P = np.zeros((3, B, B), dtype=self.dt)
+        P[0] = 1.0
+        P[1] = X[None, :]
+        P[2] = X[:, None]
+        return P
+
+    @property
+    def n_lin(self):
+        return self.N + (3 if self.isl.bg_joint else 0)
+
     def models_band(self, band, p, need):
-        """M (N, B, B) placed unit models and derivative list
-        [(k, j, (B,B))] for live params."""
+        """M (n_lin, B, B) placed unit models (+ the background basis when
+        bg_joint) and derivative list [(k, j, (B,B))] for live params."""
         isl = self.isl
         N, B, T = self.N, isl.B, isl.T
-        M = np.zeros((N, B, B), dtype=self.dt)
+        M = np.zeros((self.n_lin, B, B), dtype=self.dt)
+        if isl.bg_joint:
+            M[N:] = self.bg_basis()
         Ds = []
         for k in range(N):
             if not isl.mmask[k]:
@@ -634,16 +656,23 @@ class IslandSolver:
 
     # ---------------- linear algebra ----------------
     def fluxes_band(self, M, d, w):
-        mm = self.isl.mmask
+        """Linear solve of one band: fluxes (and background coefficients).
+        Ridge: reg on real members, 1.0 on padded slots
+        (island_solver.py:570-590); reg * |diag| on background rows (the
+        element-wise ridge of forced_phot_sparse.py:474-489)."""
+        nl = self.n_lin
+        mm = np.concatenate([self.isl.mmask, np.ones(nl - self.N, bool)])
         w64 = w.astype(np.float64)
-        M64 = M.reshape(self.N, -1).astype(np.float64)
+        M64 = M.reshape(nl, -1).astype(np.float64)
         wm = M64 * w64.reshape(1, -1)
         A = wm @ M64.T
         b = wm @ d.astype(np.float64).reshape(-1)
         if self.dt == np.float32:
             A = A.astype(np.float32).astype(np.float64)
             b = b.astype(np.float32).astype(np.float64)
-        A64 = A + np.diag(np.where(mm, self.cfg.reg, 1.0))
+        ridge = np.where(mm, self.cfg.reg, 1.0)
+        ridge[self.N:] = self.cfg.reg * np.maximum(np.abs(np.diag(A)[self.N:]), 1e-30)
+        A64 = A + np.diag(ridge)
         f64 = np.linalg.solve(A64, b)
         f = (f64.astype(self.dt) * mm).astype(self.dt)
         return f, f64, A64
@@ -690,7 +719,7 @@ class IslandSolver:
             if not Ds:
                 continue
             w64 = w.astype(np.float64).reshape(-1)
-            M64 = M.reshape(N, -1).astype(np.float64)
+            M64 = M.reshape(self.n_lin, -1).astype(np.float64)
             rt = d.astype(np.float64).reshape(-1) - f64 @ M64
             sw = np.sqrt(w.astype(dt).astype(np.float64)).reshape(-1)
             Ainv = np.linalg.inv(A64)
@@ -839,16 +868,24 @@ class IslandSolver:
         return best
 
     def final_fluxes(self, p):
+        """Fluxes and errors (n_b, N), and background coefficients and
+        errors (n_b, 3; zero without bg_joint)."""
         nb, N = self.nb, self.N
         F = np.zeros((nb, N), np.float32)
         E = np.zeros((nb, N), np.float32)
+        G = np.zeros((nb, 3), np.float32)
+        GE = np.zeros((nb, 3), np.float32)
         for b in range(nb):
             M, _ = self.models_band(b, p, False)
             f, _, A64 = self.fluxes_band(M, self.isl.data[b], self.isl.w[b])
             Ainv = np.linalg.inv(A64)
-            F[b] = f
-            E[b] = np.sqrt(np.maximum(np.diag(Ainv), 1e-30))
-        return F, E
+            e = np.sqrt(np.maximum(np.diag(Ainv), 1e-30))
+            F[b] = f[:N]
+            E[b] = e[:N]
+            if self.isl.bg_joint:
+                G[b] = f[N:]
+                GE[b] = e[N:]
+        return F, E, G, GE
 
 
 def solve_island(isl: IslandInput, cfg: SolverConfig, max_steps: int = 30,
@@ -861,10 +898,10 @@ def solve_island(isl: IslandInput, cfg: SolverConfig, max_steps: int = 30,
     if out["stall"]:
         div = s.diverged_probe(out["p"], out["lam"], out["nst"], out["HG"])
         sd = float(s.plateau_probe(out["p"], out["nst"], out["HG"]))
-    F, E = s.final_fluxes(out["p"])
+    F, E, G, GE = s.final_fluxes(out["p"])
     n_good = int(np.sum(isl.w > 0))
     return dict(p=out["p"].reshape(s.N, 6).astype(np.float32),
-                fluxes=F, ferr=E, chi2=out["chi2"], conv=out["conv"],
+                fluxes=F, ferr=E, bg=G, bg_err=GE, chi2=out["chi2"], conv=out["conv"],
                 stall=out["stall"], diverged=div, stall_dchi2=sd,
                 nst=out["nst"], lam=out["lam"], consec=out["consec"],
                 nrej=out["nrej"], n_good=n_good, steps=out["steps"])
@@ -872,7 +909,7 @@ def solve_island(isl: IslandInput, cfg: SolverConfig, max_steps: int = 30,
 
 def island_inputs_from_host(host: dict, row: int, *, B: int, T: int,
                             dstack, wstack, psf: list, table, mode: str,
-                            native: int = 0):
+                            native: int = 0, bg_joint: bool = False):
     """Slice one island out of class host arrays + the padded stacks."""
     ox, oy = int(host["ox"][row]), int(host["oy"][row])
     N = host["mmask"].shape[1]
@@ -890,4 +927,4 @@ def island_inputs_from_host(host: dict, row: int, *, B: int, T: int,
         prior_mean=host["prior_mean"][row].reshape(-1).astype(np.float32),
         prior_inv_sigma=host["prior_inv_sigma"][row].reshape(-1).astype(np.float32),
         has_priors=bool(host["has_priors"]),
-        psf=psf, table=table, mode=mode, native=int(native))
+        psf=psf, table=table, mode=mode, native=int(native), bg_joint=bool(bg_joint))

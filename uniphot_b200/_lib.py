@@ -40,7 +40,7 @@ class ClassDesc(C.Structure):
                 ("step_tol_pix", C.c_float), ("un_freeze_steps", C.c_int32),
                 ("has_priors", C.c_int32), ("native_stamp", C.c_int32),
                 ("precision", C.c_int32), ("tc_min_rows", C.c_int32),
-                ("tc_cond_max", C.c_float)]
+                ("bg_joint", C.c_int32), ("tc_cond_max", C.c_float)]
 
 
 class ChunkIn(C.Structure):
@@ -54,7 +54,7 @@ class ChunkOut(C.Structure):
     _fields_ = [(n, _P) for n in (
         "p", "fluxes", "ferr", "chi2", "conv", "stall", "diverged",
         "stall_dchi2", "nst", "lam", "consec", "nrej", "n_good")] + \
-        [("steps_run", C.c_int32)]
+        [("steps_run", C.c_int32), ("bg", _P), ("bg_err", _P)]
 
 
 class UphError(RuntimeError):
@@ -260,7 +260,8 @@ def chunk_out(n: int, N: int, nb: int):
                stall=np.zeros(n, np.uint8), diverged=np.zeros(n, np.uint8),
                stall_dchi2=np.zeros(n, np.float32), nst=np.zeros(n, np.int32),
                lam=np.zeros(n, np.float32), consec=np.zeros(n, np.int32),
-               nrej=np.zeros(n, np.int32), n_good=np.zeros(n, np.int64))
+               nrej=np.zeros(n, np.int32), n_good=np.zeros(n, np.int64),
+               bg=np.zeros((n, nb, 3), np.float32), bg_err=np.zeros((n, nb, 3), np.float32))
     cout = ChunkOut()
     for k, v in out.items():
         setattr(cout, k, ptr(v))

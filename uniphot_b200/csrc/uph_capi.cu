@@ -502,6 +502,7 @@ int add_chunk(uph_ctx* ctx, Chunk* ch, const uph_class_desc* cls,
     return set_err(ctx, UPH_ERR_INVALID, "unknown render mode %d", mode);
   }
   const int nP = 6 * N;
+  const int nbg = cls->bg_joint ? UPH_MAXBG : 0;
   std::vector<int> nL(n), nr(n);
   int Kmax = 1, nLmax = 1, R = 1;
   bool any_gal = false;
@@ -530,7 +531,7 @@ int add_chunk(uph_ctx* ctx, Chunk* ch, const uph_class_desc* cls,
     }
     nL[i] = live;
     nLmax = std::max(nLmax, live);
-    Kmax = std::max(Kmax, live + cnt + 1);
+    Kmax = std::max(Kmax, live + cnt + nbg + 1);
     const int ox = in->ox[i], oy = in->oy[i];
     if (ox < 0 || oy < 0 || ox + B > ctx->Wp || oy + B > ctx->Hp)
       return set_err(ctx, UPH_ERR_INVALID, "island %d window outside the padded field", i);
@@ -563,6 +564,11 @@ int add_chunk(uph_ctx* ctx, Chunk* ch, const uph_class_desc* cls,
       row_s[(size_t)i * Kmax + r] = 0;
       ++r;
     }
+    for (int j = 0; j < nbg; ++j) {   // background basis rows: sources -2, -3, -4
+      row_k[(size_t)i * Kmax + r] = 0;
+      row_s[(size_t)i * Kmax + r] = (int16_t)(-2 - j);
+      ++r;
+    }
     row_k[(size_t)i * Kmax + r] = 0;
     row_s[(size_t)i * Kmax + r] = -1;
   }
@@ -570,6 +576,7 @@ int add_chunk(uph_ctx* ctx, Chunk* ch, const uph_class_desc* cls,
   ch->n = n; ch->N = N; ch->nb = nb; ch->nP = nP;
   ClassDev& c = ch->c;
   c.n_isl = n; c.nb = nb; c.N = N; c.nP = nP; c.B = B; c.T = T; c.Sz = Sz; c.R = R;
+  c.nbg = nbg; c.NL = N + nbg;
   c.Kmax = Kmax; c.nLmax = nLmax; c.ntile_side = (Sz + UPH_TILE - 1) / UPH_TILE;
   c.mode = mode;
   c.native = (cls->native_stamp > 0 && cls->native_stamp < T) ? (cls->native_stamp | 1) : T;
@@ -644,6 +651,10 @@ int add_chunk(uph_ctx* ctx, Chunk* ch, const uph_class_desc* cls,
   c.chi2b = cbuf<double>(ctx, ch, "chi2b", (size_t)n * nb, &rc);
   c.flux = cbuf<float>(ctx, ch, "flux", (size_t)n * nb * N, &rc);
   c.ferr = cbuf<float>(ctx, ch, "ferr", (size_t)n * nb * N, &rc);
+  if (nbg) {
+    c.bgout = cbuf<float>(ctx, ch, "bgout", (size_t)n * nb * UPH_MAXBG, &rc);
+    c.bgerr = cbuf<float>(ctx, ch, "bgerr", (size_t)n * nb * UPH_MAXBG, &rc);
+  }
   c.ngood = cbuf<int>(ctx, ch, "ngood", (size_t)n * nb, &rc);
   c.probe_best = cbuf<float>(ctx, ch, "pbest", n, &rc);
   c.probe_p = cbuf<float>(ctx, ch, "probep", (size_t)n * 4 * nP, &rc);
@@ -651,8 +662,8 @@ int add_chunk(uph_ctx* ctx, Chunk* ch, const uph_class_desc* cls,
   c.err = cbuf<int>(ctx, ch, "err", 1, &rc);
   c.tc_split = 1;
   if (c.tc_min_rows < (1 << 30)) {
-    c.fcur = cbuf<float>(ctx, ch, "fcur", (size_t)n * nb * N, &rc);
-    c.ftry = cbuf<float>(ctx, ch, "ftry", (size_t)n * nb * N, &rc);
+    c.fcur = cbuf<float>(ctx, ch, "fcur", (size_t)n * nb * c.NL, &rc);
+    c.ftry = cbuf<float>(ctx, ch, "ftry", (size_t)n * nb * c.NL, &rc);
     c.acond_cur = cbuf<float>(ctx, ch, "acondc", (size_t)n * nb, &rc);
     c.acond_try = cbuf<float>(ctx, ch, "acondt", (size_t)n * nb, &rc);
     c.tc_cond_max = cls->tc_cond_max < 0.f ? UPH_TC_COND_MAX_DEFAULT : cls->tc_cond_max;
@@ -964,6 +975,14 @@ int job_read(uph_job* job, int id, uph_chunk_out* out) {
   if ((rc = download(ctx, out->p, c.p, sizeof(float) * n * nP, "p"))) return rc;
   if ((rc = download(ctx, out->fluxes, c.flux, sizeof(float) * n * nb * N, "flux"))) return rc;
   if ((rc = download(ctx, out->ferr, c.ferr, sizeof(float) * n * nb * N, "ferr"))) return rc;
+  if (c.nbg) {
+    if ((rc = download(ctx, out->bg, c.bgout, sizeof(float) * n * nb * UPH_MAXBG, "bg"))) return rc;
+    if ((rc = download(ctx, out->bg_err, c.bgerr, sizeof(float) * n * nb * UPH_MAXBG, "bg")))
+      return rc;
+  } else {
+    if (out->bg) std::memset(out->bg, 0, sizeof(float) * n * nb * UPH_MAXBG);
+    if (out->bg_err) std::memset(out->bg_err, 0, sizeof(float) * n * nb * UPH_MAXBG);
+  }
   if ((rc = download(ctx, out->chi2, c.chi2, sizeof(float) * n, "chi2"))) return rc;
   if ((rc = download(ctx, nst.data(), c.nst, sizeof(int) * n, "nst"))) return rc;
   if ((rc = download(ctx, out->lam, c.lam, sizeof(float) * n, "lam"))) return rc;

@@ -112,7 +112,7 @@ __device__ bool mbar_wait(uint64_t* bar, uint32_t phase) {
 }
 
 __device__ __forceinline__ int gram_rows(const ClassDev& c, int isl) {
-  return c.isl_nL[isl] + c.isl_nr[isl] + 1;
+  return gram_K(c, isl);
 }
 
 __global__ void __launch_bounds__(NT) k_gram_tc(ClassDev c, int rcap) {
@@ -121,6 +121,7 @@ __global__ void __launch_bounds__(NT) k_gram_tc(ClassDev c, int rcap) {
   __shared__ uint32_t tmem_base;
   __shared__ int4 box[UPH_MAXN];
   __shared__ float fcs[UPH_MAXN];
+  __shared__ float bgs[UPH_MAXBG];    // background coefficients of the residual
   __shared__ int16_t srk[UPH_MAXK], srs[UPH_MAXK];
   __shared__ float swt[2][KC];
   __shared__ float rsd[2][KC];
@@ -144,8 +145,10 @@ __global__ void __launch_bounds__(NT) k_gram_tc(ClassDev c, int rcap) {
   for (int k = tid; k < c.N; k += NT) {
     MemberBox mb = member_box(c, isl, c.p, k);
     box[k] = make_int4(mb.wx0, mb.wy0, mb.bw, mb.bh);
-    fcs[k] = c.fcur[((size_t)isl * c.nb + b) * c.N + k];
+    fcs[k] = c.fcur[((size_t)isl * c.nb + b) * c.NL + k];
   }
+  for (int j = tid; j < c.nbg; j += NT)
+    bgs[j] = c.fcur[((size_t)isl * c.nb + b) * c.NL + c.N + j];
   for (int r = tid; r < K; r += NT) {
     srk[r] = rk[r];
     srs[r] = rs[r];
@@ -218,6 +221,7 @@ __global__ void __launch_bounds__(NT) k_gram_tc(ClassDev c, int rcap) {
             model = fmaf(fcs[k], c.stamps[stamp_slot(c, isl, b, k, 0) + (size_t)ly * Sz + lx],
                          model);
         }
+        for (int j = 0; j < c.nbg; ++j) model = fmaf(bgs[j], bg_basis(j, wy, wx, B), model);
         rv = sw * (dbase[(size_t)wy * c.Wp + wx] - model);
       }
       pwy[st][tid] = wy;
@@ -234,7 +238,14 @@ __global__ void __launch_bounds__(NT) k_gram_tc(ClassDev c, int rcap) {
       if (r >= K) continue;
       float v[8];
       const int s = srs[r];
-      if (s < 0) {
+      if (s <= -2) {
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          const int q = g * 8 + j;
+          v[j] = pwy[st][q] >= 0 ? bg_basis(-2 - s, pwy[st][q], pwx[st][q], B) * swt[st][q]
+                                 : 0.f;
+        }
+      } else if (s < 0) {
 #pragma unroll
         for (int j = 0; j < 8; ++j) v[j] = rsd[st][g * 8 + j];
       } else {

@@ -16,7 +16,9 @@
 
 #define UPH_MAXN 32          // member slots per island handled on the device
 #define UPH_MAXLIVE 192      // live nonlinear parameters per island
-#define UPH_MAXK (UPH_MAXLIVE + UPH_MAXN + 1)
+#define UPH_MAXBG 3           // planar background rows (1, X, Y) per band
+#define UPH_MAXLIN (UPH_MAXN + UPH_MAXBG)   // linear unknowns per band
+#define UPH_MAXK (UPH_MAXLIVE + UPH_MAXLIN + 1)
 #define UPH_LU_SMEM_N 160    // damped systems up to this size factor in shared memory
 #define UPH_MAXKPSF 8        // Gaussian components of an analytic PSF
 #define UPH_MAXNT 21         // polynomial terms (order 5)
@@ -119,6 +121,13 @@ struct ClassDev {
   // Fluxes solved at p (fcur) and at p_try (ftry), (n_isl, nb, N); only
   // allocated when some island uses the tensor-core Gram, whose last row is
   // the residual d - M^T fcur instead of the data.
+  // Linear solution per band: nr member fluxes, then nbg background
+  // coefficients (nbg = 3 when the planar background is solved jointly,
+  // else 0); arrays of it have stride NL = N + nbg.
+  int nbg;
+  int NL;
+  float* bgout;            // (n_isl, nb, 3) final background coefficients
+  float* bgerr;            // (n_isl, nb, 3) and their errors
   float* fcur;
   float* ftry;
   // (n_isl, nb) conditioning indicator of the members' scaled normal matrix
@@ -144,6 +153,21 @@ struct ClassDev {
   float reg, pos_step_max, ftol_rel, step_tol;
   int un_freeze;
 };
+
+// Gram rows of island isl: live derivative rows, member model rows,
+// background rows, the data (or residual) row.
+__device__ __forceinline__ int gram_K(const ClassDev& c, int isl) {
+  return c.isl_nL[isl] + c.isl_nr[isl] + c.nbg + 1;
+}
+
+// Planar background basis j (0: 1, 1: X, 2: Y) at window pixel (wy, wx):
+// X = (wx - c) / s, Y = (wy - c) / s with c = (B - 1) / 2 and s = B / 2,
+// evaluated in double and rounded once.
+__device__ __forceinline__ float bg_basis(int j, int wy, int wx, int B) {
+  if (j == 0) return 1.0f;
+  const double cen = 0.5 * (B - 1), sc = 0.5 * B;
+  return (float)(((double)(j == 1 ? wx : wy) - cen) / sc);
+}
 
 // Whether island isl forms its next Gram on the tensor cores (mixed form):
 // more than tc_min_rows rows and a well-conditioned normal matrix of its

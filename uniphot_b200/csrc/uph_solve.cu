@@ -44,18 +44,22 @@ struct RowSrc {
   const int16_t* rk;
   const int16_t* rs;
   int K;
-  const float* fc = nullptr;   // residual form: fluxes of the nr model rows
-  int nr = 0;
+  const float* fc = nullptr;   // residual form: linear solution (stride-NL layout)
+  int nr = 0;                  // member model rows
+  int nbg = 0;                 // background rows after them
+  int N = 0;                   // slot of background coefficient j in fc: N + j
 };
 
 // Value of Gram row r at window pixel (wy, wx), already scaled by sqrt(w).
 // The last row is the data, or in residual form (fc set) the residual
 // d - sum_k fc_k m_k, summed in member order as the trial pass does.
+template <bool BG>
 __device__ __forceinline__ float row_value(const ClassDev& c, int isl, int b,
                                            const RowSrc& rows, const int4* box,
                                            int r, int wy, int wx, float sw,
                                            const float* dbase) {
   const int rs = rows.rs[r];
+  if (BG && rs <= -2) return bg_basis(-2 - rs, wy, wx, c.B) * sw;
   if (rs < 0) {
     const float d = dbase[(size_t)wy * c.Wp + wx];
     if (!rows.fc) return d * sw;
@@ -67,6 +71,9 @@ __device__ __forceinline__ float row_value(const ClassDev& c, int isl, int b,
         model = fmaf(rows.fc[k], c.stamps[stamp_slot(c, isl, b, k, 0) + (size_t)ly * c.Sz + lx],
                      model);
     }
+    if (BG)
+      for (int j = 0; j < rows.nbg; ++j)
+        model = fmaf(rows.fc[rows.N + j], bg_basis(j, wy, wx, c.B), model);
     return sw * (d - model);
   }
   const int k = rows.rk[r];
@@ -79,6 +86,7 @@ __device__ __forceinline__ float row_value(const ClassDev& c, int isl, int b,
 
 // Small-K path (K <= 8): every thread accumulates the packed upper triangle
 // of its own pixels in registers; warp-shuffle + fixed-order block reduction.
+template <bool BG>
 __device__ void gram_window_small(const ClassDev& c, int isl, int b,
                                   const RowSrc& rows, const int4* box,
                                   float* out, int ld, float* sm) {
@@ -98,7 +106,7 @@ __device__ void gram_window_small(const ClassDev& c, int isl, int b,
     float z[8];
 #pragma unroll
     for (int r = 0; r < 8; ++r)
-      z[r] = (r < K) ? row_value(c, isl, b, rows, box, r, wy, wx, sw, dbase) : 0.f;
+      z[r] = (r < K) ? row_value<BG>(c, isl, b, rows, box, r, wy, wx, sw, dbase) : 0.f;
     int e = 0;
 #pragma unroll
     for (int i = 0; i < 8; ++i)
@@ -159,6 +167,7 @@ __host__ __device__ __forceinline__ int gram_tile_pixels(int K) {
 // data; zero outside a member's box) into Z (pitch LD) and the raw weights
 // into Wt, by 4-byte cp.async (one commit group).  Rows K..nrows-1 are not
 // touched: the caller zeroes them once.
+template <bool BG>
 __device__ __forceinline__ void stage_rows(const ClassDev& c, int isl, int b,
                                            const RowSrc& rows, const int4* box,
                                            float* Z, float* Wt, int pix0, int TP,
@@ -178,7 +187,11 @@ __device__ __forceinline__ void stage_rows(const ClassDev& c, int isl, int b,
       const int wy = (int)(((float)pix + 0.5f) * invB);
       const int wx = pix - wy * B;
       const int rs = rows.rs[r];
-      if (rs < 0) {
+      if (BG && rs <= -2) {
+        // background basis: computed, not copied
+        Z[r * LD + q] = bg_basis(-2 - rs, wy, wx, B);
+        continue;
+      } else if (rs < 0) {
         src = dbase + (size_t)wy * c.Wp + wx;
         ok = true;
       } else {
@@ -235,13 +248,14 @@ __device__ __forceinline__ unsigned dynamic_smem_bytes() {
 // of the upper triangle over its share of the pixels; the s threads sharing
 // a block are s consecutive lanes (s a power of two), reduced by shuffles in
 // a fixed order, and through a small shared buffer when s > 32.
+template <bool BG>
 __device__ void gram_window(const ClassDev& c, int isl, int b, RowSrc rows,
                             const int4* box, float* out, int ld, int part,
                             float* sm) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int K = rows.K;
   if (K <= 8) {
-    if (part == 0) gram_window_small(c, isl, b, rows, box, out, ld, sm);
+    if (part == 0) gram_window_small<BG>(c, isl, b, rows, box, out, ld, sm);
     return;
   }
   if (sizeof(float) * (size_t)tile_floats(K) > dynamic_smem_bytes()) {
@@ -273,9 +287,10 @@ __device__ void gram_window(const ClassDev& c, int isl, int b, RowSrc rows,
   // buffers: Z0 Z1 (nrows x LD each), W0 W1 (TP each), red ((NT / 32) x 64)
   float* red = sm + 2 * nrows * LD + 2 * TP;
   const int npix = c.B * c.B;
-  const int m0 = K - 1 - rows.nr;   // first model row (residual form)
+  const int nlin = rows.nr + rows.nbg;
+  const int m0 = K - 1 - nlin;      // first linear row (residual form)
   auto stage = [&](int pix0, int bufi) {
-    stage_rows(c, isl, b, rows, box, sm + bufi * nrows * LD,
+    stage_rows<BG>(c, isl, b, rows, box, sm + bufi * nrows * LD,
                sm + 2 * nrows * LD + bufi * TP, pix0, TP, lgTP, LD, nrows);
   };
 
@@ -303,6 +318,9 @@ __device__ void gram_window(const ClassDev& c, int isl, int b, RowSrc rows,
       for (int q = tid; q < TP; q += NT) {
         float model = 0.f;
         for (int k = 0; k < rows.nr; ++k) model = fmaf(rows.fc[k], Z[(m0 + k) * LD + q], model);
+        if (BG)
+          for (int j = 0; j < rows.nbg; ++j)
+            model = fmaf(rows.fc[rows.N + j], Z[(m0 + rows.nr + j) * LD + q], model);
         Z[(K - 1) * LD + q] = Z[(K - 1) * LD + q] - model;
       }
       __syncthreads();
@@ -379,13 +397,14 @@ __device__ void load_boxes(const ClassDev& c, int isl, const float* P,
   }
 }
 
+template <bool BG>
 __global__ void __launch_bounds__(NT) k_gram_lin(ClassDev c) {
   extern __shared__ float sm[];
   __shared__ int4 box[UPH_MAXN];
   const int isl = blockIdx.x / c.nb, b = blockIdx.x % c.nb;
   if (isl >= c.n_isl || !isl_active(c.flags[isl], PH_LIN)) return;
-  const int nL = c.isl_nL[isl], nr = c.isl_nr[isl];
-  const int K = nL + nr + 1;
+  const int nr = c.isl_nr[isl];
+  const int K = gram_K(c, isl);
   if (tc_island(c, isl, K)) return;  // the tensor-core Gram handles this island
   const int nbk = (K + 7) / 8;
   const int nblk = nbk * (nbk + 1) / 2;
@@ -398,8 +417,8 @@ __global__ void __launch_bounds__(NT) k_gram_lin(ClassDev c) {
               K, box);
   // the mixed form forms every Gram in residual form (k_assemble matches)
   RowSrc rows{c.row_k + (size_t)isl * c.Kmax, c.row_s + (size_t)isl * c.Kmax, K,
-              c.fcur ? c.fcur + ((size_t)isl * c.nb + b) * c.N : nullptr, nr};
-  gram_window(c, isl, b, rows, box,
+              c.fcur ? c.fcur + ((size_t)isl * c.nb + b) * c.NL : nullptr, nr, c.nbg, c.N};
+  gram_window<BG>(c, isl, b, rows, box,
               c.gram + ((size_t)isl * c.nb + b) * c.Kmax * c.Kmax, c.Kmax,
               blockIdx.y, sm);
 }
@@ -408,17 +427,18 @@ __global__ void __launch_bounds__(NT) k_gram_lin(ClassDev c) {
 // turns the left n x n block into the identity; the remaining columns hold
 // A^-1 [rhs].  All threads of the block participate.
 //
-// With diag (the matrix's original diagonal) and cond non-null, thread 0
+// With diag (the matrix's original diagonal), cond and perm (n ints of
+// shared scratch for the row order) non-null, thread 0
 // also writes a conditioning indicator of the diagonally scaled matrix
 // D^-1/2 A D^-1/2: the spread max/min of the pivots in that scaling (each
 // pivot |M[p][col]| divided by sqrt(diag[row of p] diag[col])), 1 for a
 // diagonal matrix and 1 / (1 - rho^2) for two members of correlation rho.
 __device__ void gauss_jordan(double* M, int n, int ncol, int ld, double* fac,
                              int* piv, const double* diag = nullptr,
-                             float* cond = nullptr) {
+                             float* cond = nullptr, int* perm = nullptr) {
   const int tid = threadIdx.x;
-  int perm[UPH_MAXN];
   double rmin = INFINITY, rmax = 0.0;
+  if (!perm) cond = nullptr;   // the indicator needs the caller's row-order scratch
   if (tid == 0 && cond)
     for (int r = 0; r < n; ++r) perm[r] = r;
   for (int col = 0; col < n; ++col) {
@@ -468,33 +488,36 @@ __device__ void gauss_jordan(double* M, int n, int ncol, int ld, double* fac,
 
 __global__ void __launch_bounds__(NT) k_assemble(ClassDev c) {
   extern __shared__ double dsm[];
-  __shared__ double fac[UPH_MAXN];
+  __shared__ double fac[UPH_MAXLIN];
+  __shared__ double ridge[UPH_MAXLIN];
   __shared__ int piv;
   const int isl = blockIdx.x / c.nb, b = blockIdx.x % c.nb;
   if (isl >= c.n_isl || !isl_active(c.flags[isl], PH_LIN)) return;
   const int tid = threadIdx.x;
   const int nL = c.isl_nL[isl], nr = c.isl_nr[isl];
-  const int K = nL + nr + 1;
+  const int nl = nr + c.nbg;   // linear rows: member models, then background
+  const int K = gram_K(c, isl);
   const float* G = c.gram + ((size_t)isl * c.nb + b) * c.Kmax * c.Kmax;
   const int ldg = c.Kmax;
   const int16_t* rk = c.row_k + (size_t)isl * c.Kmax;
   float* Hb = c.Hb + ((size_t)isl * c.nb + b) * c.nLmax * c.nLmax;
   float* gb = c.gb + ((size_t)isl * c.nb + b) * c.nLmax;
-  const int ncol = 2 * nr + 1;
+  const int ncol = 2 * nl + 1;
   const int lda = ncol;
-  double* Aug = dsm;                       // nr x (2nr+1)
-  double* DM = Aug + UPH_MAXN * (2 * UPH_MAXN + 1);  // nL x nr
-  double* Cm = DM + (size_t)c.nLmax * UPH_MAXN;      // nL x nr
-  double* Wm = Cm + (size_t)c.nLmax * UPH_MAXN;      // nL x nr
-  double* vec = Wm + (size_t)c.nLmax * UPH_MAXN;     // f64[nr], a[nr], q[nr]
+  constexpr int LS = UPH_MAXLIN;           // row stride of the nL x nl blocks
+  double* Aug = dsm;                       // nl x (2 nl + 1)
+  double* DM = Aug + LS * (2 * LS + 1);    // nL x nl
+  double* Cm = DM + (size_t)c.nLmax * LS;  // nL x nl
+  double* Wm = Cm + (size_t)c.nLmax * LS;  // nL x nl
+  double* vec = Wm + (size_t)c.nLmax * LS; // f64[nl], a[nl], q[nl]
   double* f64v = vec;
-  double* av = vec + UPH_MAXN;
-  double* qv = av + UPH_MAXN;
+  double* av = vec + LS;
+  double* qv = av + LS;
   if (nL == 0) {
     return;
   }
-  const int m0 = nL;  // first model row
-  const int dr = nL + nr;
+  const int m0 = nL;  // first linear row
+  const int dr = nL + nl;
   // Residual form (tensor-core Gram): the last Gram row is r = d - M^T fc
   // with fc the fluxes solved at the same parameters, so G holds M W r and
   // D W r instead of M W d and D W d.  Every quantity below is rewritten in
@@ -506,41 +529,49 @@ __global__ void __launch_bounds__(NT) k_assemble(ClassDev c) {
   if (tid == 0)
     work_add(c, WK_ASSEMBLE, 4ull * (unsigned long long)(K * K + nL * nL + nL), 0);
   const bool resid = c.fcur != nullptr;   // mixed form: every Gram in residual form
-  const float* fc = resid ? c.fcur + ((size_t)isl * c.nb + b) * c.N : nullptr;
-  for (int e = tid; e < nr * ncol; e += NT) {
+  const float* fcb = resid ? c.fcur + ((size_t)isl * c.nb + b) * c.NL : nullptr;
+  // linear slot l in the stride-NL arrays: members at l, background j at N + j
+  auto fcl = [&](int l) -> double { return (double)fcb[l < nr ? l : c.N + (l - nr)]; };
+  // ridge: reg on members (island_solver.py:570-590), reg * |diag| on the
+  // background rows (forced_phot_sparse.py:474-489)
+  for (int l = tid; l < nl; l += NT)
+    ridge[l] = l < nr ? (double)c.reg
+                      : (double)c.reg * fmax(fabs((double)G[(m0 + l) * ldg + m0 + l]), 1e-30);
+  __syncthreads();
+  for (int e = tid; e < nl * ncol; e += NT) {
     const int r = e / ncol, j = e - (e / ncol) * ncol;
     double v;
-    if (j < nr) {
+    if (j < nl) {
       v = (double)G[(m0 + r) * ldg + m0 + j];
-      if (j == r) v += (double)c.reg;
-    } else if (j < 2 * nr) {
-      v = (j - nr == r) ? 1.0 : 0.0;
+      if (j == r) v += ridge[r];
+    } else if (j < 2 * nl) {
+      v = (j - nl == r) ? 1.0 : 0.0;
     } else {
       v = (double)G[(m0 + r) * ldg + dr];
-      if (resid) v -= (double)c.reg * (double)fc[r];
+      if (resid) v -= ridge[r] * fcl(r);
     }
     Aug[r * lda + j] = v;
   }
-  for (int e = tid; e < nL * nr; e += NT) {
-    const int i = e / nr, l = e - (e / nr) * nr;
-    DM[i * UPH_MAXN + l] = (double)G[i * ldg + m0 + l];
+  for (int e = tid; e < nL * nl; e += NT) {
+    const int i = e / nl, l = e - (e / nl) * nl;
+    DM[i * LS + l] = (double)G[i * ldg + m0 + l];
   }
   __syncthreads();
-  gauss_jordan(Aug, nr, ncol, lda, fac, &piv);
+  gauss_jordan(Aug, nl, ncol, lda, fac, &piv);
   // f64 fluxes and their float32 copy (the model uses f32 fluxes)
-  for (int l = tid; l < nr; l += NT) {
-    f64v[l] = Aug[l * lda + 2 * nr] + (resid ? (double)fc[l] : 0.0);
+  for (int l = tid; l < nl; l += NT) {
+    f64v[l] = Aug[l * lda + 2 * nl] + (resid ? fcl(l) : 0.0);
     av[l] = (double)(float)f64v[l];
   }
   __syncthreads();
   // q = b - A a  (A without ridge)
-  for (int l = tid; l < nr; l += NT) {
+  for (int l = tid; l < nl; l += NT) {
     double t = (double)G[(m0 + l) * ldg + dr];
     if (resid)
-      for (int m = 0; m < nr; ++m)
-        t += (double)G[(m0 + l) * ldg + m0 + m] * ((double)fc[m] - av[m]);
+      for (int m = 0; m < nl; ++m)
+        t += (double)G[(m0 + l) * ldg + m0 + m] * (fcl(m) - av[m]);
     else
-      for (int m = 0; m < nr; ++m) t -= (double)G[(m0 + l) * ldg + m0 + m] * av[m];
+      for (int m = 0; m < nl; ++m) t -= (double)G[(m0 + l) * ldg + m0 + m] * av[m];
     qv[l] = t;
   }
   // c_i = Ainv (e_k s_i - f_k u_i), rounded to f32
@@ -548,25 +579,25 @@ __global__ void __launch_bounds__(NT) k_assemble(ClassDev c) {
     const int k = rk[i];
     double si = (double)G[i * ldg + dr];
     if (resid)
-      for (int m = 0; m < nr; ++m) si += DM[i * UPH_MAXN + m] * ((double)fc[m] - f64v[m]);
+      for (int m = 0; m < nl; ++m) si += DM[i * LS + m] * (fcl(m) - f64v[m]);
     else
-      for (int m = 0; m < nr; ++m) si -= DM[i * UPH_MAXN + m] * f64v[m];
+      for (int m = 0; m < nl; ++m) si -= DM[i * LS + m] * f64v[m];
     const double fk = f64v[k];
-    for (int l = 0; l < nr; ++l) {
-      double t = Aug[l * lda + nr + k] * si;
+    for (int l = 0; l < nl; ++l) {
+      double t = Aug[l * lda + nl + k] * si;
       double u = 0.0;
-      for (int m = 0; m < nr; ++m) u += Aug[l * lda + nr + m] * DM[i * UPH_MAXN + m];
+      for (int m = 0; m < nl; ++m) u += Aug[l * lda + nl + m] * DM[i * LS + m];
       t -= fk * u;
-      Cm[i * UPH_MAXN + l] = (double)(float)t;
+      Cm[i * LS + l] = (double)(float)t;
     }
   }
   __syncthreads();
   // W_j = A c_j + a_j DM_j
-  for (int e = tid; e < nL * nr; e += NT) {
-    const int j = e / nr, l = e - (e / nr) * nr;
-    double t = av[rk[j]] * DM[j * UPH_MAXN + l];
-    for (int m = 0; m < nr; ++m) t += (double)G[(m0 + l) * ldg + m0 + m] * Cm[j * UPH_MAXN + m];
-    Wm[j * UPH_MAXN + l] = t;
+  for (int e = tid; e < nL * nl; e += NT) {
+    const int j = e / nl, l = e - (e / nl) * nl;
+    double t = av[rk[j]] * DM[j * LS + l];
+    for (int m = 0; m < nl; ++m) t += (double)G[(m0 + l) * ldg + m0 + m] * Cm[j * LS + m];
+    Wm[j * LS + l] = t;
   }
   __syncthreads();
   // H_ij = a_i (a_j DD_ij + DM_i . c_j) + c_i . W_j
@@ -581,9 +612,9 @@ __global__ void __launch_bounds__(NT) k_assemble(ClassDev c) {
     const double ai = av[rk[i]], aj = av[rk[j]];
     double t1 = aj * (double)G[i * ldg + j];
     double t2 = 0.0;
-    for (int l = 0; l < nr; ++l) {
-      t1 += DM[i * UPH_MAXN + l] * Cm[j * UPH_MAXN + l];
-      t2 += Cm[i * UPH_MAXN + l] * Wm[j * UPH_MAXN + l];
+    for (int l = 0; l < nl; ++l) {
+      t1 += DM[i * LS + l] * Cm[j * LS + l];
+      t2 += Cm[i * LS + l] * Wm[j * LS + l];
     }
     const float h = (float)(ai * t1 + t2);
     Hb[i * c.nLmax + j] = h;
@@ -593,26 +624,28 @@ __global__ void __launch_bounds__(NT) k_assemble(ClassDev c) {
   for (int i = tid; i < nL; i += NT) {
     double t = (double)G[i * ldg + dr];
     if (resid)
-      for (int m = 0; m < nr; ++m) t += DM[i * UPH_MAXN + m] * ((double)fc[m] - av[m]);
+      for (int m = 0; m < nl; ++m) t += DM[i * LS + m] * (fcl(m) - av[m]);
     else
-      for (int m = 0; m < nr; ++m) t -= DM[i * UPH_MAXN + m] * av[m];
+      for (int m = 0; m < nl; ++m) t -= DM[i * LS + m] * av[m];
     double u = 0.0;
-    for (int l = 0; l < nr; ++l) u += Cm[i * UPH_MAXN + l] * qv[l];
+    for (int l = 0; l < nl; ++l) u += Cm[i * LS + l] * qv[l];
     gb[i] = (float)(-(av[rk[i]] * t + u));
   }
 }
 
+template <bool BG>
 __global__ void __launch_bounds__(NT)
 k_gram_trial(ClassDev c, const float* __restrict__ P, int phase,
              int final_mode, float* __restrict__ fout, float* __restrict__ cout) {
   extern __shared__ float sm[];
   __shared__ int4 box[UPH_MAXN];
-  __shared__ int16_t rk[UPH_MAXN + 1], rs[UPH_MAXN + 1];
-  __shared__ double Aug[UPH_MAXN * (2 * UPH_MAXN + 1)];
-  __shared__ double fac[UPH_MAXN];
-  __shared__ double dg[UPH_MAXN];
-  __shared__ float gmm[(UPH_MAXN + 1) * (UPH_MAXN + 1)];
-  __shared__ float fl32[UPH_MAXN];
+  __shared__ int16_t rk[UPH_MAXLIN + 1], rs[UPH_MAXLIN + 1];
+  __shared__ double Aug[UPH_MAXLIN * (2 * UPH_MAXLIN + 1)];
+  __shared__ double fac[UPH_MAXLIN];
+  __shared__ double dg[UPH_MAXLIN];
+  __shared__ float gmm[(UPH_MAXLIN + 1) * (UPH_MAXLIN + 1)];
+  __shared__ float fl32[UPH_MAXLIN];
+  __shared__ int permsh[UPH_MAXLIN];
   __shared__ double red[NT];
   __shared__ int redi[NT];
   __shared__ int piv;
@@ -620,11 +653,12 @@ k_gram_trial(ClassDev c, const float* __restrict__ P, int phase,
   if (isl >= c.n_isl || !isl_active(c.flags[isl], phase)) return;
   const int tid = threadIdx.x;
   const int nr = c.isl_nr[isl];
-  const int K = nr + 1;
+  const int nl = nr + c.nbg;   // linear rows: member models, then background
+  const int K = nl + 1;
   load_boxes(c, isl, P, box);
   for (int r = tid; r < K; r += NT) {
     rk[r] = (int16_t)(r < nr ? r : 0);
-    rs[r] = (int16_t)(r < nr ? 0 : -1);
+    rs[r] = (int16_t)(r < nr ? 0 : (r < nl ? -2 - (r - nr) : -1));
   }
   __syncthreads();
   if (tid == 0 && c.work) {
@@ -634,32 +668,41 @@ k_gram_trial(ClassDev c, const float* __restrict__ P, int phase,
     work_add(c, WK_TRIAL, 4ull * (px + 2ull * c.B * c.B) + 8ull, 0);
   }
   RowSrc rows{rk, rs, K};
-  gram_window(c, isl, b, rows, box, gmm, K, 0, sm);
+  gram_window<BG>(c, isl, b, rows, box, gmm, K, 0, sm);
   __syncthreads();
-  const int ncol = 2 * nr + 1;
-  for (int e = tid; e < nr * ncol; e += NT) {
+  const int ncol = 2 * nl + 1;
+  // ridge: reg on members (island_solver.py:570-590), reg * |diag| on the
+  // background rows (forced_phot_sparse.py:474-489); dg holds the diagonal
+  // Aug receives, read from the finished Gram (not from Aug, which other
+  // threads are still filling)
+  for (int r = tid; r < nl; r += NT) {
+    const double a = (double)gmm[r * K + r];
+    dg[r] = a + (r < nr ? (double)c.reg : (double)c.reg * fmax(fabs(a), 1e-30));
+  }
+  __syncthreads();
+  for (int e = tid; e < nl * ncol; e += NT) {
     const int r = e / ncol, j = e - (e / ncol) * ncol;
     double v;
-    if (j < nr) {
-      v = (double)gmm[r * K + j];
-      if (j == r) v += (double)c.reg;
-    } else if (j < 2 * nr) {
-      v = (j - nr == r) ? 1.0 : 0.0;
+    if (j < nl) {
+      v = (j == r) ? dg[r] : (double)gmm[r * K + j];
+    } else if (j < 2 * nl) {
+      v = (j - nl == r) ? 1.0 : 0.0;
     } else {
-      v = (double)gmm[r * K + nr];
+      v = (double)gmm[r * K + nl];
     }
     Aug[r * ncol + j] = v;
   }
-  // the diagonal Aug receives, read from the finished Gram (not from Aug,
-  // which other threads are still filling)
-  for (int r = tid; r < nr; r += NT) dg[r] = (double)gmm[r * K + r] + (double)c.reg;
   __syncthreads();
-  gauss_jordan(Aug, nr, ncol, ncol, fac, &piv, dg,
-               cout ? cout + (size_t)isl * c.nb + b : nullptr);
-  for (int l = tid; l < nr; l += NT) fl32[l] = (float)Aug[l * ncol + 2 * nr];
+  gauss_jordan(Aug, nl, ncol, ncol, fac, &piv, dg,
+               cout ? cout + (size_t)isl * c.nb + b : nullptr, permsh);
+  for (int l = tid; l < nl; l += NT) fl32[l] = (float)Aug[l * ncol + 2 * nl];
   if (fout) {
-    float* fo = fout + ((size_t)isl * c.nb + b) * c.N;
-    for (int k = tid; k < c.N; k += NT) fo[k] = k < nr ? (float)Aug[k * ncol + 2 * nr] : 0.f;
+    // stride-NL layout: members at k, background coefficient j at N + j
+    float* fo = fout + ((size_t)isl * c.nb + b) * c.NL;
+    for (int k = tid; k < c.NL; k += NT) {
+      const int l = k < c.N ? (k < nr ? k : -1) : nr + (k - c.N);
+      fo[k] = l >= 0 ? (float)Aug[l * ncol + 2 * nl] : 0.f;
+    }
   }
   __syncthreads();
   // residual pass
@@ -680,6 +723,8 @@ k_gram_trial(ClassDev c, const float* __restrict__ P, int phase,
       if (ly >= 0 && ly < bx.w && lx >= 0 && lx < bx.z)
         model = fmaf(fl32[k], c.stamps[stamp_slot(c, isl, b, k, 0) + (size_t)ly * Sz + lx], model);
     }
+    if (BG)
+      for (int j = 0; j < c.nbg; ++j) model = fmaf(fl32[nr + j], bg_basis(j, wy, wx, B), model);
     const float r = sqrtf(w) * (d - model);
     acc += (double)r * (double)r;
     good += (w > 0.f);
@@ -701,12 +746,19 @@ k_gram_trial(ClassDev c, const float* __restrict__ P, int phase,
     for (int k = tid; k < c.N; k += NT) {
       if (k < nr) {
         fo[k] = fl32[k];
-        eo[k] = (float)sqrt(fmax(Aug[k * ncol + nr + k], 1e-30));
+        eo[k] = (float)sqrt(fmax(Aug[k * ncol + nl + k], 1e-30));
       } else {
         fo[k] = 0.f;
         eo[k] = 1.0f;  // padded slot: unit diagonal
       }
     }
+    if (c.nbg)
+      for (int j = tid; j < c.nbg; j += NT) {
+        const int l = nr + j;
+        c.bgout[((size_t)isl * c.nb + b) * UPH_MAXBG + j] = fl32[l];
+        c.bgerr[((size_t)isl * c.nb + b) * UPH_MAXBG + j] =
+            (float)sqrt(fmax(Aug[l * ncol + nl + l], 1e-30));
+      }
     if (tid == 0) c.ngood[(size_t)isl * c.nb + b] = redi[0];
   }
 }
@@ -948,8 +1000,8 @@ __global__ void k_accept(ClassDev c, int phase) {
   if (accept) {
     for (int q = 0; q < nP; ++q) p[q] = pt[q];
     if (c.fcur) {
-      const size_t o = (size_t)isl * c.nb * c.N;
-      for (int e = 0; e < c.nb * c.N; ++e) c.fcur[o + e] = c.ftry[o + e];
+      const size_t o = (size_t)isl * c.nb * c.NL;
+      for (int e = 0; e < c.nb * c.NL; ++e) c.fcur[o + e] = c.ftry[o + e];
       for (int b = 0; b < c.nb; ++b)
         c.acond_cur[(size_t)isl * c.nb + b] = c.acond_try[(size_t)isl * c.nb + b];
     }
@@ -1026,12 +1078,12 @@ size_t gram_lin_smem_bytes(int Kmax) {
   return best;
 }
 
-size_t gram_trial_smem_bytes(int N) { return gram_lin_smem_bytes(N + 1); }
+size_t gram_trial_smem_bytes(int N) { return gram_lin_smem_bytes(N + UPH_MAXBG + 1); }
 
 size_t assemble_smem_bytes(int nLmax, int N) {
   (void)N;
-  return sizeof(double) * ((size_t)UPH_MAXN * (2 * UPH_MAXN + 1) +
-                           3 * (size_t)nLmax * UPH_MAXN + 3 * UPH_MAXN);
+  return sizeof(double) * ((size_t)UPH_MAXLIN * (2 * UPH_MAXLIN + 1) +
+                           3 * (size_t)nLmax * UPH_MAXLIN + 3 * UPH_MAXLIN);
 }
 
 size_t step_smem_bytes(int nLmax) {
@@ -1044,7 +1096,10 @@ void launch_gram_lin(const ClassDev& c, cudaStream_t s) {
   const int nblk = nbk * (nbk + 1) / 2;
   const int parts = nblk <= NT ? 1 : (nblk + NT - 1) / NT;
   dim3 grid((unsigned)(c.n_isl * c.nb), (unsigned)parts);
-  k_gram_lin<<<grid, NT, gram_lin_smem_bytes(c.Kmax), s>>>(c);
+  if (c.nbg)
+    k_gram_lin<true><<<grid, NT, gram_lin_smem_bytes(c.Kmax), s>>>(c);
+  else
+    k_gram_lin<false><<<grid, NT, gram_lin_smem_bytes(c.Kmax), s>>>(c);
 }
 
 void launch_assemble(const ClassDev& c, cudaStream_t s) {
@@ -1053,7 +1108,11 @@ void launch_assemble(const ClassDev& c, cudaStream_t s) {
 
 void launch_gram_trial(const ClassDev& c, const float* P, int phase,
                        int final_mode, float* fout, float* cout, cudaStream_t s) {
-  k_gram_trial<<<(unsigned)(c.n_isl * c.nb), NT, gram_trial_smem_bytes(c.N), s>>>(
+  if (c.nbg)
+    k_gram_trial<true><<<(unsigned)(c.n_isl * c.nb), NT, gram_trial_smem_bytes(c.N), s>>>(
+      c, P, phase, final_mode, fout, cout);
+  else
+    k_gram_trial<false><<<(unsigned)(c.n_isl * c.nb), NT, gram_trial_smem_bytes(c.N), s>>>(
       c, P, phase, final_mode, fout, cout);
 }
 
@@ -1078,10 +1137,16 @@ void launch_diverged_compare(const ClassDev& c, uint8_t* out,
 
 int uph_solve_setup() {
   cudaError_t e;
-  e = cudaFuncSetAttribute(k_gram_lin, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  e = cudaFuncSetAttribute(k_gram_lin<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)gram_lin_smem_bytes(UPH_MAXK));
   if (e != cudaSuccess) return (int)e;
-  e = cudaFuncSetAttribute(k_gram_trial, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  e = cudaFuncSetAttribute(k_gram_lin<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)gram_lin_smem_bytes(UPH_MAXK));
+  if (e != cudaSuccess) return (int)e;
+  e = cudaFuncSetAttribute(k_gram_trial<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)gram_trial_smem_bytes(UPH_MAXN));
+  if (e != cudaSuccess) return (int)e;
+  e = cudaFuncSetAttribute(k_gram_trial<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)gram_trial_smem_bytes(UPH_MAXN));
   if (e != cudaSuccess) return (int)e;
   e = cudaFuncSetAttribute(k_assemble, cudaFuncAttributeMaxDynamicSharedMemorySize,

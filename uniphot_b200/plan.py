@@ -302,6 +302,11 @@ class IslandFitResult:
     fracmasked: np.ndarray = None
     flux_win: np.ndarray = None
     flux_marg_var: np.ndarray = None
+    # planar background of the member's island per band (c0 + c1 X + c2 Y
+    # over the island window, X, Y = (pixel - (B - 1) / 2) / (B / 2)) and
+    # its error, when the fit solved it jointly (bg_mode="joint"); else 0
+    bg_plane: np.ndarray = None
+    bg_plane_err: np.ndarray = None
     bucket_stats: list = field(default_factory=list)
 
     @property
@@ -316,7 +321,8 @@ def _nan(n):
 def unpack_class_results(plan, host, island_set, res_p, res_f, res_fe,
                          res_chi2, res_conv, res_stall, res_nst,
                          res_perr=None, res_pdchi2=None, res_div=None,
-                         res_ngood=None, n_bands=0, **_unused) -> dict:
+                         res_ngood=None, n_bands=0, res_bg=None, res_bg_err=None,
+                         **_unused) -> dict:
     """Island rows -> source rows for the valid member slots.
 
     Parameter-error, profile and metric columns are NaN here: their
@@ -364,7 +370,11 @@ def unpack_class_results(plan, host, island_set, res_p, res_f, res_fe,
         sersic_n_prior_frac=_nan(n), rchisq=_nan(n), fracflux=_nan(n),
         fracin=_nan(n), fracmasked=_nan(n),
         flux_win=np.full((n, nb), np.nan, np.float32),
-        flux_marg_var=np.full((n, nb), np.nan, np.float32))
+        flux_marg_var=np.full((n, nb), np.nan, np.float32),
+        bg_plane=(res_bg[ii].astype(np.float32) if res_bg is not None
+                  else np.zeros((n, nb, 3), np.float32)),
+        bg_plane_err=(res_bg_err[ii].astype(np.float32) if res_bg_err is not None
+                      else np.zeros((n, nb, 3), np.float32)))
 
 
 def giant_seed_rows(giant_ids, island_set, *, pos_x, pos_y, logre, ee1, ee2,
@@ -398,5 +408,7 @@ def giant_seed_rows(giant_ids, island_set, *, pos_x, pos_y, logre, ee1, ee2,
             ell_prior_frac=nn(), theta_prior_frac=nn(), sersic_n_prior_frac=nn(),
             rchisq=nn(), fracflux=nn(), fracin=nn(), fracmasked=nn(),
             flux_win=np.full((n, nb), np.nan, np.float32),
-            flux_marg_var=np.full((n, nb), np.nan, np.float32)))
+            flux_marg_var=np.full((n, nb), np.nan, np.float32),
+            bg_plane=np.zeros((n, nb, 3), np.float32),
+            bg_plane_err=np.zeros((n, nb, 3), np.float32)))
     return rows

@@ -186,7 +186,8 @@ def make_class_kernels(plan, n_bands: int, n_terms: int, *, render_backend: str,
                        convergence: str = "legacy", plateau_dlnp_tol: float = 0.5,
                        render_mode: str = "reference",
                        native_stamp: int = 0, precision: str = "plain",
-                       tc_min_rows: int = -1, tc_cond_max: float = -1.0) -> ClassKernels:
+                       tc_min_rows: int = -1, tc_cond_max: float = -1.0,
+                       bg_mode: str = "frozen") -> ClassKernels:
     if stall_count_mode not in ("proposals", "changed"):
         raise ValueError(f"stall_count_mode must be 'proposals' or 'changed', "
                          f"got {stall_count_mode!r}")
@@ -208,6 +209,8 @@ def make_class_kernels(plan, n_bands: int, n_terms: int, *, render_backend: str,
                          f"got {render_mode!r}")
     if precision not in _lib.PRECISIONS:
         raise ValueError(f"precision must be 'plain' or 'mixed', got {precision!r}")
+    if bg_mode not in ("frozen", "joint"):
+        raise ValueError(f"bg_mode must be 'frozen' or 'joint', got {bg_mode!r}")
     unsupported = []
     if stall_count_mode != "proposals":
         unsupported.append("stall_count_mode='changed'")
@@ -232,7 +235,7 @@ def make_class_kernels(plan, n_bands: int, n_terms: int, *, render_backend: str,
         step_tol_pix=float(step_tol_pix), un_freeze_steps=int(un_freeze_steps),
         has_priors=int(bool(has_priors)), native_stamp=int(native_stamp),
         precision=_lib.PRECISIONS[precision], tc_min_rows=int(tc_min_rows),
-        tc_cond_max=float(tc_cond_max))
+        bg_joint=int(bg_mode == "joint"), tc_cond_max=float(tc_cond_max))
     return ClassKernels(desc, render_mode, int(n_bands), str(plan.kind))
 
 
@@ -447,7 +450,7 @@ class IslandFitJob:
                  native_stamp: int | None = None, device: int = 0,
                  field: DeviceField | None = None,
                  chunk_budget_bytes: float = 16e9, precision: str = "plain",
-                 plan: "FieldPlan | None" = None):
+                 plan: "FieldPlan | None" = None, bg_mode: str = "frozen"):
         for flag, name in ((compute_param_errors, "compute_param_errors"),
                            (compute_source_metrics, "compute_source_metrics"),
                            (compute_re_profile, "compute_re_profile"),
@@ -500,7 +503,7 @@ class IslandFitJob:
                 has_priors=bool(host["has_priors"]),
                 stall_count_mode=stall_count_mode, convergence=convergence,
                 plateau_dlnp_tol=plateau_dlnp_tol, render_mode=render_mode,
-                native_stamp=fp.native, precision=precision)
+                native_stamp=fp.native, precision=precision, bg_mode=bg_mode)
             chunk = _chunk_size(plan, n_bands, chunk_budget_bytes)
             ids = []
             for lo in range(0, plan.n_islands, chunk):
@@ -545,7 +548,8 @@ class IslandFitJob:
                 plan, host, self.island_set, res["p"], res["fluxes"], res["ferr"],
                 res["chi2"], res["conv"], res["stall"], res["nst"],
                 res_pdchi2=res["stall_dchi2"], res_div=res["diverged"],
-                res_ngood=res["n_good"], n_bands=n_bands))
+                res_ngood=res["n_good"], n_bands=n_bands,
+                res_bg=res.get("bg"), res_bg_err=res.get("bg_err")))
         giant_ids = np.concatenate([np.asarray(self.buckets.giant_ids, np.int64).ravel(),
                                     np.asarray(self.capped, np.int64)])
         if self.include_giants and giant_ids.size:
@@ -581,7 +585,8 @@ def _assemble_result(bandnames, out_rows, bucket_stats) -> IslandFitResult:
         sersic_n_prior_frac=cat["sersic_n_prior_frac"], rchisq=cat["rchisq"],
         fracflux=cat["fracflux"], fracin=cat["fracin"],
         fracmasked=cat["fracmasked"], flux_win=cat["flux_win"],
-        flux_marg_var=cat["flux_marg_var"], bucket_stats=bucket_stats)
+        flux_marg_var=cat["flux_marg_var"], bg_plane=cat["bg_plane"],
+        bg_plane_err=cat["bg_plane_err"], bucket_stats=bucket_stats)
 
 
 def giant_only_result(*, bandnames, island_set, buckets, pos_x, pos_y, logre, ee1,
