@@ -66,6 +66,12 @@ typedef struct uph_class_desc {
   int32_t tc_min_rows;      /* mixed form: Gram-row threshold of the
                                tensor-core path; < 0 selects the default
                                (UPH_TC_MIN_ROWS_DEFAULT)                   */
+  int32_t stall_changed;    /* stall_count_mode: 0 "proposals" (legacy);
+                               1 "changed": a reject counts toward the stall
+                               only when its proposal differs from the
+                               previous rejected one; identical-proposal
+                               runs set the diverged flag in the loop
+                               (island_solver.py:1118-1208)                */
   int32_t bg_joint;         /* 1: each band's planar background (1, X, Y
                                over the island window) is solved with the
                                fluxes in the inner linear step; 0: the data
@@ -108,6 +114,10 @@ typedef struct uph_chunk_in {
   const int32_t* init_consec; /* [n]                                        */
   const int32_t* init_nrej;   /* [n]                                        */
   const int32_t* init_nst;    /* [n]                                        */
+  /* optional "changed"-mode tracker carry (NULL = zeros):                   */
+  const int32_t* init_n_same; /* [n]     identical-proposal reject run      */
+  const float* init_prej;     /* [n*N*6] last rejected proposal             */
+  const uint8_t* init_diverged; /* [n]   sticky diverged flag               */
 } uph_chunk_in;
 
 /* Per-island outputs (run_class_chunk's dict).  Shapes as noted. */
@@ -129,6 +139,8 @@ typedef struct uph_chunk_out {
   float* bg;            /* [n*nb*3] planar background (1, X, Y) per band
                            when bg_joint; may be NULL                      */
   float* bg_err;        /* [n*nb*3] its sqrt(diag inv A64); may be NULL    */
+  int32_t* n_same;      /* [n]     "changed" tracker (0 otherwise); may be NULL */
+  float* prej;          /* [n*N*6] last rejected proposal; may be NULL     */
 } uph_chunk_out;
 
 /* Context: one per device per process. */

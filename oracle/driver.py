@@ -47,11 +47,13 @@ def _one(args):
 def solve_chunk(host, rows, *, B, T, dstack, wstack, psfs, mode, table_path=None,
                 precision="ref", max_steps=30, reg=1e-9, pos_step_max=0.5,
                 ftol_rel=1e-4, step_tol=0.1, processes: int = 1,
-                native: int = 0, bg_joint: bool = False) -> dict:
+                native: int = 0, bg_joint: bool = False,
+                stall_count_mode: str = "proposals") -> dict:
     table = SersicTable.load(table_path) if table_path is not None else None
     psf = psf_bands(psfs, T, mode)
     cfg = SolverConfig(reg=reg, pos_step_max=pos_step_max, ftol_rel=ftol_rel,
-                       step_tol=step_tol, precision=precision)
+                       step_tol=step_tol, precision=precision,
+                       stall_count_mode=stall_count_mode)
     jobs = [(host, int(r), B, T, dstack, wstack, psf, table, mode, cfg, max_steps,
              native, bg_joint) for r in rows]
     if processes > 1 and len(jobs) > 1:
@@ -62,7 +64,7 @@ def solve_chunk(host, rows, *, B, T, dstack, wstack, psfs, mode, table_path=None
         res = [_one(j) for j in jobs]
     out = {}
     for k in ("p", "fluxes", "ferr", "bg", "bg_err", "chi2", "conv", "stall", "diverged",
-              "stall_dchi2", "nst", "lam", "consec", "nrej", "n_good"):
+              "stall_dchi2", "nst", "lam", "consec", "nrej", "n_good", "n_same", "prej"):
         out[k] = np.stack([np.asarray(r[k]) for r in res])
     out["steps_run"] = int(max(r["steps"] for r in res))
     return out

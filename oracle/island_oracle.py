@@ -391,6 +391,11 @@ class SolverConfig:
     step_tol: float = 0.1
     un_freeze_steps: int = 0
     precision: str = "ref"   # "ref" | "f64"
+    # "proposals" (legacy) | "changed": a rejected step counts toward the
+    # stall only when its proposal differs from the previous rejected one
+    # (island_solver.py:1118-1208); identical-proposal runs of
+    # STALL_REJECT_K set the sticky diverged flag in the loop
+    stall_count_mode: str = "proposals"
 
 
 class IslandSolver:
@@ -790,6 +795,9 @@ class IslandSolver:
         dt = self.dt
         isl = self.isl
         cfg = self.cfg
+        changed = cfg.stall_count_mode == "changed"
+        div, n_same = False, 0
+        prej = np.zeros(self.nP, dt)
         if state is None:
             p = isl.p0.astype(dt).copy()
             lam = dt(LM_LAMBDA0)
@@ -801,6 +809,9 @@ class IslandSolver:
             chi2 = dt(state["chi2"])
             consec, nrej, nst = (int(state["consec"]), int(state["nrej"]),
                                  int(state["nst"]))
+            div = bool(state.get("diverged", False))
+            n_same = int(state.get("n_same", 0))
+            prej = np.asarray(state.get("prej", prej), dt).reshape(-1).copy()
         conv = False
         stall = False
         HG = None
@@ -829,7 +840,17 @@ class IslandSolver:
             consec = consec + 1 if small else (0 if accept else consec)
             step_small = accept and pos_step < cfg.step_tol \
                 and shape_step < SHAPE_STEP_TOL
-            nrej = 0 if accept else nrej + 1
+            if changed:
+                # proposal identity (exact comparison) with the previous
+                # rejected proposal (island_solver.py:1180-1192)
+                prop_same = n_same > 0 and bool(np.all(p_try == prej))
+                n_same = 0 if accept else (n_same + 1 if prop_same else 1)
+                if not accept:
+                    prej = p_try.astype(dt).copy()
+                nrej = 0 if accept else (nrej if prop_same else nrej + 1)
+                div = div or n_same >= STALL_REJECT_K
+            else:
+                nrej = 0 if accept else nrej + 1
             stall_now = nrej >= STALL_REJECT_K
             conv = (consec >= 2) or step_small or stall_now
             stall = stall_now
@@ -840,7 +861,8 @@ class IslandSolver:
             lam = lam_new
             nst += 1
         return dict(p=p, lam=lam, chi2=chi2, consec=consec, nrej=nrej,
-                    nst=nst, conv=conv, stall=stall, steps=steps, HG=HG)
+                    nst=nst, conv=conv, stall=stall, steps=steps, HG=HG,
+                    div=div, n_same=n_same, prej=prej)
 
     def diverged_probe(self, p, lam_final, nsteps_final, HG=None):
         """True iff the K rejected proposals of a stall were identical."""
@@ -893,10 +915,12 @@ def solve_island(isl: IslandInput, cfg: SolverConfig, max_steps: int = 30,
     """Full per-island result (the row of run_class_chunk's dict)."""
     s = IslandSolver(isl, cfg)
     out = s.run(max_steps, state)
-    div = False
+    changed = cfg.stall_count_mode == "changed"
+    div = bool(out["div"]) if changed else False
     sd = float("nan")
     if out["stall"]:
-        div = s.diverged_probe(out["p"], out["lam"], out["nst"], out["HG"])
+        if not changed:   # changed mode keeps the in-loop tracker's flag
+            div = s.diverged_probe(out["p"], out["lam"], out["nst"], out["HG"])
         sd = float(s.plateau_probe(out["p"], out["nst"], out["HG"]))
     F, E, G, GE = s.final_fluxes(out["p"])
     n_good = int(np.sum(isl.w > 0))
@@ -904,7 +928,8 @@ def solve_island(isl: IslandInput, cfg: SolverConfig, max_steps: int = 30,
                 fluxes=F, ferr=E, bg=G, bg_err=GE, chi2=out["chi2"], conv=out["conv"],
                 stall=out["stall"], diverged=div, stall_dchi2=sd,
                 nst=out["nst"], lam=out["lam"], consec=out["consec"],
-                nrej=out["nrej"], n_good=n_good, steps=out["steps"])
+                nrej=out["nrej"], n_good=n_good, steps=out["steps"],
+                n_same=out["n_same"], prej=np.asarray(out["prej"], np.float32))
 
 
 def island_inputs_from_host(host: dict, row: int, *, B: int, T: int,

@@ -27,11 +27,18 @@ def test_invalid_options_raise_valueerror(bad):
         solver.make_class_kernels(_plan(), 3, 1, **KW, **bad)
 
 
-@pytest.mark.parametrize("opt", [dict(stall_count_mode="changed"), dict(convergence="dlnp"),
+@pytest.mark.parametrize("opt", [dict(convergence="dlnp"),
                                  dict(crossband={"rank": 1}), dict(scene_subtract=True)])
 def test_unbuilt_options_raise(opt):
     with pytest.raises(ValueError, match="not supported"):
         solver.make_class_kernels(_plan("mixed"), 3, 1, **KW, **opt)
+
+
+def test_changed_stall_counting_sets_the_descriptor():
+    k = solver.make_class_kernels(_plan("mixed"), 3, 1, **KW, stall_count_mode="changed")
+    assert k.desc.stall_changed == 1 and k.step_protocol == "changed"
+    k = solver.make_class_kernels(_plan("mixed"), 3, 1, **KW)
+    assert k.desc.stall_changed == 0 and k.step_protocol == "proposals"
 
 
 def test_class_descriptor_fields():

@@ -1,0 +1,80 @@
+"""Step-protocol variants on the GPU vs the oracle (island_solver.py:1118-
+1208): stall_count_mode="changed" keeps an in-loop tracker of the last
+rejected proposal; identical-proposal rejects escalate lambda without
+counting toward the stall, and a run of 4 sets the sticky diverged flag.
+"""
+import numpy as np
+import pytest
+
+from _common import compare, field_classes, run_gpu, run_oracle
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def small():
+    from uniphot_b200.synth import make_small_field
+    return make_small_field(0)
+
+
+@pytest.mark.parametrize("mode,kinds", [("reference", ("star",)),
+                                        ("analytic", ("star", "mixed"))])
+def test_changed_mode_parity(small, mode, kinds):
+    plans, hosts, PAD, ds, ws, psfs = field_classes(small, mode, kinds)
+    g, _ = run_gpu(plans, hosts, PAD, ds, ws, psfs, mode, native=small.native,
+                   stall_count_mode="changed")
+    o = run_oracle(plans, hosts, PAD, ds, ws, psfs, mode, native=small.native,
+                   stall_count_mode="changed")
+    for p, h, gg, oo in zip(plans, hosts, g, o):
+        r = compare(gg, oo, h["mmask"])
+        msg = f"{p.key}: {r['max_rel']:.2e} {r['max_dpos']:.2e}"
+        assert r["same_nst"].all() and r["same_flags"].all(), msg
+        assert r["flux_ok"].all() and r["pos_ok"].all(), msg
+        np.testing.assert_array_equal(gg["diverged"], oo["diverged"])
+        np.testing.assert_array_equal(gg["n_same"], oo["n_same"])
+
+
+def test_changed_mode_zero_weight_island(small):
+    """Identical proposals never count: the island runs to max_steps with
+    the diverged flag set, as in the oracle."""
+    plans, hosts, PAD, ds, ws, psfs = field_classes(small, "analytic", ("star",))
+    p, h = plans[0], hosts[0]
+    ws2 = ws.copy()
+    oy, ox = int(h["oy"][0]), int(h["ox"][0])
+    ws2[:, oy:oy + p.bbox_class, ox:ox + p.bbox_class] = 0.0
+    g, _ = run_gpu([p], [h], PAD, ds, ws2, psfs, "analytic", native=small.native,
+                   max_steps=12, stall_count_mode="changed")
+    o = run_oracle([p], [h], PAD, ds, ws2, psfs, "analytic", native=small.native,
+                   max_steps=12, stall_count_mode="changed")
+    g, o = g[0], o[0]
+    assert g["nst"][0] == 12 and not g["conv"][0] and g["diverged"][0]
+    assert g["n_same"][0] == o["n_same"][0] == 12
+    np.testing.assert_array_equal(g["nst"], o["nst"])
+    np.testing.assert_array_equal(g["diverged"], o["diverged"])
+
+
+def test_changed_mode_tracker_carries_across_requeue(small):
+    """A re-queued chunk carrying the tracker state equals one pass."""
+    from uniphot_b200 import solver
+    plans, hosts, PAD, ds, ws, psfs = field_classes(small, "analytic", ("mixed",))
+    p, h = plans[0], hosts[0]
+    full, fld = run_gpu([p], [h], PAD, ds, ws, psfs, "analytic", native=small.native,
+                        stall_count_mode="changed")
+    a, _ = run_gpu([p], [h], PAD, ds, ws, psfs, "analytic", max_steps=2, field=fld,
+                   native=small.native, stall_count_mode="changed")
+    a = a[0]
+    tree, nt = solver.build_psf_tree(psfs, p.tier)
+    kern = solver.make_class_kernels(p, ds.shape[0], nt, render_backend="fft", reg=1e-9,
+                                     pos_step_max_pix=0.5, chi2_ftol_rel=1e-4,
+                                     step_tol_pix=0.1, un_freeze_steps=0,
+                                     render_mode="analytic", native_stamp=small.native,
+                                     stall_count_mode="changed")
+    rows = np.nonzero(~a["conv"])[0]
+    assert rows.size > 0
+    init = {k: a[k][rows] for k in ("p", "lam", "chi2", "consec", "nrej", "nst",
+                                    "n_same", "prej", "diverged")}
+    b = solver.run_class_chunk(kern, tree, h, rows, rows.size, 28, fld, fld, PAD,
+                               init_state=init)
+    f = full[0]
+    np.testing.assert_array_equal(b["nst"], f["nst"][rows])
+    np.testing.assert_array_equal(b["p"], f["p"][rows])

@@ -254,3 +254,25 @@ def test_joint_background_jacobian_matches_finite_differences():
                                atol=2e-4 * np.abs(Hn).max())
     gn = Jn @ r
     np.testing.assert_allclose(g[idx], gn, rtol=2e-3, atol=2e-4 * np.abs(gn).max())
+
+
+def test_changed_mode_zero_weight_island_runs_out_diverged():
+    """stall_count_mode='changed' (island_solver.py:1118-1208): a zero-
+    weight island proposes the same step at every escalating damping, so
+    the identical rejects never count toward the stall; the loop runs to
+    max_steps and the sticky diverged flag is set."""
+    isl, _ = _mini_island("analytic", n_src=1, gal=False, noise=False)
+    isl.w[:] = 0.0
+    out = O.solve_island(isl, O.SolverConfig(precision="ref", stall_count_mode="changed"),
+                         max_steps=12)
+    assert not out["stall"] and not out["conv"] and out["nst"] == 12
+    assert out["diverged"] and out["n_same"] == 12 and out["nrej"] == 1
+
+
+def test_changed_mode_matches_legacy_when_no_repeats():
+    isl, _ = _mini_island("analytic", n_src=2, seed=3)
+    a = O.solve_island(isl, O.SolverConfig(precision="ref"), max_steps=30)
+    b = O.solve_island(isl, O.SolverConfig(precision="ref", stall_count_mode="changed"),
+                       max_steps=30)
+    assert a["nst"] == b["nst"] and a["conv"] == b["conv"]
+    np.testing.assert_array_equal(a["p"], b["p"])

@@ -40,21 +40,24 @@ class ClassDesc(C.Structure):
                 ("step_tol_pix", C.c_float), ("un_freeze_steps", C.c_int32),
                 ("has_priors", C.c_int32), ("native_stamp", C.c_int32),
                 ("precision", C.c_int32), ("tc_min_rows", C.c_int32),
-                ("bg_joint", C.c_int32), ("tc_cond_max", C.c_float)]
+                ("stall_changed", C.c_int32), ("bg_joint", C.c_int32),
+                ("tc_cond_max", C.c_float)]
 
 
 class ChunkIn(C.Structure):
     _fields_ = [("n_islands", C.c_int32)] + [(n, _P) for n in (
         "ox", "oy", "x0b", "y0b", "stype", "n_frozen", "free_n", "mmask",
         "keep", "p0", "lower", "upper", "prior_mean", "prior_inv_sigma",
-        "init_lam", "init_chi2", "init_consec", "init_nrej", "init_nst")]
+        "init_lam", "init_chi2", "init_consec", "init_nrej", "init_nst",
+        "init_n_same", "init_prej", "init_diverged")]
 
 
 class ChunkOut(C.Structure):
     _fields_ = [(n, _P) for n in (
         "p", "fluxes", "ferr", "chi2", "conv", "stall", "diverged",
         "stall_dchi2", "nst", "lam", "consec", "nrej", "n_good")] + \
-        [("steps_run", C.c_int32), ("bg", _P), ("bg_err", _P)]
+        [("steps_run", C.c_int32), ("bg", _P), ("bg_err", _P), ("n_same", _P),
+         ("prej", _P)]
 
 
 class UphError(RuntimeError):
@@ -246,6 +249,13 @@ def chunk_in(arrays: dict, init_state: dict | None = None):
         for k, conv in (("lam", f32), ("chi2", f32), ("consec", i32), ("nrej", i32),
                         ("nst", i32)):
             keep["init_" + k] = conv(init_state[k], n)
+        # "changed"-mode tracker carry (the reference's _CARRY_KEYS)
+        if init_state.get("n_same") is not None:
+            keep["init_n_same"] = i32(init_state["n_same"], n)
+        if init_state.get("prej") is not None:
+            keep["init_prej"] = f32(init_state["prej"], (n, nP))
+        if init_state.get("diverged") is not None:
+            keep["init_diverged"] = u8(init_state["diverged"], n)
     cin = ChunkIn(n_islands=n)
     for k, v in keep.items():
         setattr(cin, k, ptr(v))
@@ -261,7 +271,8 @@ def chunk_out(n: int, N: int, nb: int):
                stall_dchi2=np.zeros(n, np.float32), nst=np.zeros(n, np.int32),
                lam=np.zeros(n, np.float32), consec=np.zeros(n, np.int32),
                nrej=np.zeros(n, np.int32), n_good=np.zeros(n, np.int64),
-               bg=np.zeros((n, nb, 3), np.float32), bg_err=np.zeros((n, nb, 3), np.float32))
+               bg=np.zeros((n, nb, 3), np.float32), bg_err=np.zeros((n, nb, 3), np.float32),
+               n_same=np.zeros(n, np.int32), prej=np.zeros((n, 6 * N), np.float32))
     cout = ChunkOut()
     for k, v in out.items():
         setattr(cout, k, ptr(v))

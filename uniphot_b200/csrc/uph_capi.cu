@@ -388,6 +388,9 @@ struct Chunk {
   int* d_nrej0 = nullptr;
   int* d_nst0 = nullptr;
   uint8_t* d_flags0 = nullptr;
+  int* d_nsame0 = nullptr;     // "changed" tracker at the chunk's start
+  float* d_prej0 = nullptr;
+  uint8_t* d_divl0 = nullptr;
   float* d_p0 = nullptr;
   uint8_t* d_div = nullptr;
   cudaGraph_t graph = nullptr;
@@ -577,6 +580,7 @@ int add_chunk(uph_ctx* ctx, Chunk* ch, const uph_class_desc* cls,
   ClassDev& c = ch->c;
   c.n_isl = n; c.nb = nb; c.N = N; c.nP = nP; c.B = B; c.T = T; c.Sz = Sz; c.R = R;
   c.nbg = nbg; c.NL = N + nbg;
+  c.changed = cls->stall_changed ? 1 : 0;
   c.Kmax = Kmax; c.nLmax = nLmax; c.ntile_side = (Sz + UPH_TILE - 1) / UPH_TILE;
   c.mode = mode;
   c.native = (cls->native_stamp > 0 && cls->native_stamp < T) ? (cls->native_stamp | 1) : T;
@@ -672,6 +676,14 @@ int add_chunk(uph_ctx* ctx, Chunk* ch, const uph_class_desc* cls,
       c.gpart = cbuf<float>(ctx, ch, "gpart", (size_t)c.tc_split * n * nb * Kmax * Kmax, &rc);
   }
   ch->d_div = cbuf<uint8_t>(ctx, ch, "div", n, &rc);
+  if (c.changed) {
+    c.n_same = cbuf<int>(ctx, ch, "nsame", n, &rc);
+    c.prej = cbuf<float>(ctx, ch, "prej", (size_t)n * nP, &rc);
+    c.div_live = cbuf<uint8_t>(ctx, ch, "divl", n, &rc);
+    ch->d_nsame0 = cbuf<int>(ctx, ch, "nsame0", n, &rc);
+    ch->d_prej0 = cbuf<float>(ctx, ch, "prej0", (size_t)n * nP, &rc);
+    ch->d_divl0 = cbuf<uint8_t>(ctx, ch, "divl0", n, &rc);
+  }
   if (rc) return rc;
   c.ox = d_ox; c.oy = d_oy; c.x0b = d_x0b; c.y0b = d_y0b; c.stype = d_st;
   c.n_frozen = d_nf; c.free_n = d_fn; c.mmask = d_mm; c.keep = d_keep;
@@ -721,6 +733,24 @@ int add_chunk(uph_ctx* ctx, Chunk* ch, const uph_class_desc* cls,
   if ((rc = upload(ctx, ch->d_nrej0, h_nrej.data(), sizeof(int) * n, "nrej"))) return rc;
   if ((rc = upload(ctx, ch->d_nst0, ch->h_nst0.data(), sizeof(int) * n, "nst"))) return rc;
   if ((rc = upload(ctx, ch->d_flags0, ch->h_flags0.data(), n, "flags"))) return rc;
+  if (c.changed) {
+    // tracker carry (a re-queued chunk) or zeros
+    if (in->init_n_same) {
+      if ((rc = upload(ctx, ch->d_nsame0, in->init_n_same, sizeof(int) * n, "n_same"))) return rc;
+    } else {
+      CK(cudaMemsetAsync(ch->d_nsame0, 0, sizeof(int) * n, ctx->stream), "n_same");
+    }
+    if (in->init_prej) {
+      if ((rc = upload(ctx, ch->d_prej0, in->init_prej, sizeof(float) * n * nP, "prej"))) return rc;
+    } else {
+      CK(cudaMemsetAsync(ch->d_prej0, 0, sizeof(float) * n * nP, ctx->stream), "prej");
+    }
+    if (in->init_diverged) {
+      if ((rc = upload(ctx, ch->d_divl0, in->init_diverged, n, "diverged"))) return rc;
+    } else {
+      CK(cudaMemsetAsync(ch->d_divl0, 0, n, ctx->stream), "diverged");
+    }
+  }
   CK(cudaMemsetAsync(c.stamps, 0, sizeof(float) * (size_t)n * nb * N * R * Sz * Sz,
                      ctx->stream), "memset");
   CK(cudaEventCreateWithFlags(&ch->ev_group, cudaEventDisableTiming), "event");
@@ -739,6 +769,13 @@ int reset_chunk(uph_ctx* ctx, Chunk* ch, cudaStream_t s) {
   CK(cudaMemcpyAsync(c.nrej, ch->d_nrej0, sizeof(int) * n, cudaMemcpyDeviceToDevice, s), "reset");
   CK(cudaMemcpyAsync(c.nst, ch->d_nst0, sizeof(int) * n, cudaMemcpyDeviceToDevice, s), "reset");
   CK(cudaMemcpyAsync(c.flags, ch->d_flags0, n, cudaMemcpyDeviceToDevice, s), "reset");
+  if (c.changed) {
+    CK(cudaMemcpyAsync(c.n_same, ch->d_nsame0, sizeof(int) * n, cudaMemcpyDeviceToDevice, s),
+       "reset");
+    CK(cudaMemcpyAsync(c.prej, ch->d_prej0, sizeof(float) * n * ch->nP,
+                       cudaMemcpyDeviceToDevice, s), "reset");
+    CK(cudaMemcpyAsync(c.div_live, ch->d_divl0, n, cudaMemcpyDeviceToDevice, s), "reset");
+  }
   CK(cudaMemsetAsync(c.err, 0, sizeof(int), s), "reset");
   ch->done = false;
   ch->iters = 0;
@@ -749,10 +786,17 @@ void post_loop(Chunk* ch, Launcher& L) {
   const ClassDev& c = ch->c;
   cudaStream_t s = L.s;
   launch_set_probe(c, s);
-  for (int j = 0; j < 4; ++j) L(3, [&] { launch_step(c, PH_PROBE, j, 0.f, 1, s); });
-  launch_diverged_compare(c, ch->d_div, s);
+  if (c.changed) {
+    // "changed" mode reports the loop's own diverged flag; no post-hoc probe
+    cudaMemcpyAsync(ch->d_div, c.div_live, c.n_isl, cudaMemcpyDeviceToDevice, s);
+    L.job->ctx->launches += 1;
+  } else {
+    for (int j = 0; j < 4; ++j) L(3, [&] { launch_step(c, PH_PROBE, j, 0.f, 1, s); });
+    launch_diverged_compare(c, ch->d_div, s);
+    L.job->ctx->launches += 2;
+  }
   launch_fill_float(c.probe_best, INFINITY, c.n_isl, s);
-  L.job->ctx->launches += 3;
+  L.job->ctx->launches += 1;
   for (int e = -9; e <= 6; ++e) {
     const float lamj = (float)std::pow(10.0, (double)e);
     L(3, [&] { launch_step(c, PH_PROBE, 0, lamj, 2, s); });
@@ -975,6 +1019,13 @@ int job_read(uph_job* job, int id, uph_chunk_out* out) {
   if ((rc = download(ctx, out->p, c.p, sizeof(float) * n * nP, "p"))) return rc;
   if ((rc = download(ctx, out->fluxes, c.flux, sizeof(float) * n * nb * N, "flux"))) return rc;
   if ((rc = download(ctx, out->ferr, c.ferr, sizeof(float) * n * nb * N, "ferr"))) return rc;
+  if (c.changed) {
+    if ((rc = download(ctx, out->n_same, c.n_same, sizeof(int) * n, "n_same"))) return rc;
+    if ((rc = download(ctx, out->prej, c.prej, sizeof(float) * n * ch->nP, "prej"))) return rc;
+  } else {
+    if (out->n_same) std::memset(out->n_same, 0, sizeof(int) * n);
+    if (out->prej) std::memset(out->prej, 0, sizeof(float) * n * ch->nP);
+  }
   if (c.nbg) {
     if ((rc = download(ctx, out->bg, c.bgout, sizeof(float) * n * nb * UPH_MAXBG, "bg"))) return rc;
     if ((rc = download(ctx, out->bg_err, c.bgerr, sizeof(float) * n * nb * UPH_MAXBG, "bg")))
@@ -1000,7 +1051,9 @@ int job_read(uph_job* job, int id, uph_chunk_out* out) {
     if (out->conv) out->conv[i] = (fl[i] & FL_CONV) ? 1 : 0;
     if (out->stall) out->stall[i] = st ? 1 : 0;
     if (out->stall_dchi2) out->stall_dchi2[i] = st ? pbest[i] : NAN;
-    if (out->diverged && !st) out->diverged[i] = 0;
+    // the legacy probe only runs on stalled islands; "changed" mode's flag
+    // is the loop's sticky tracker and stands as it is
+    if (out->diverged && !st && !c.changed) out->diverged[i] = 0;
     if (out->n_good) {
       int64_t t = 0;
       for (int b = 0; b < nb; ++b) t += ng[(size_t)i * nb + b];

@@ -126,6 +126,12 @@ struct ClassDev {
   // else 0); arrays of it have stride NL = N + nbg.
   int nbg;
   int NL;
+  // "changed" stall counting: identical-proposal reject runs (n_same), the
+  // last rejected proposal (prej, n_isl x nP) and the sticky diverged flag
+  int changed;
+  int* n_same;
+  float* prej;
+  uint8_t* div_live;
   float* bgout;            // (n_isl, nb, 3) final background coefficients
   float* bgerr;            // (n_isl, nb, 3) and their errors
   float* fcur;

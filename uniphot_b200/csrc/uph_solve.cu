@@ -993,7 +993,22 @@ __global__ void k_accept(ClassDev c, int phase) {
   int consec = c.consec[isl];
   consec = small ? consec + 1 : (accept ? 0 : consec);
   const bool step_small = accept && (pos_step < c.step_tol) && (shape_step < 0.01f);
-  const int nrej = accept ? 0 : c.nrej[isl] + 1;
+  int nrej = accept ? 0 : c.nrej[isl] + 1;
+  if (c.changed) {
+    // "changed" counting (island_solver.py:1180-1192): the reject counts
+    // only when its proposal differs from the previous rejected one (exact
+    // comparison); identical-proposal runs of 4 set the diverged flag
+    int ns = c.n_same[isl];
+    float* pr = c.prej + (size_t)isl * nP;
+    bool same = ns > 0;
+    for (int q = 0; q < nP && same; ++q) same = pt[q] == pr[q];
+    ns = accept ? 0 : (same ? ns + 1 : 1);
+    if (!accept)
+      for (int q = 0; q < nP; ++q) pr[q] = pt[q];
+    nrej = accept ? 0 : (same ? c.nrej[isl] : c.nrej[isl] + 1);
+    c.n_same[isl] = ns;
+    if (ns >= 4) c.div_live[isl] = 1;
+  }
   const bool stall_now = nrej >= 4;
   const bool conv = (consec >= 2) || step_small || stall_now;
   uint8_t nf = fl;

@@ -212,8 +212,6 @@ def make_class_kernels(plan, n_bands: int, n_terms: int, *, render_backend: str,
     if bg_mode not in ("frozen", "joint"):
         raise ValueError(f"bg_mode must be 'frozen' or 'joint', got {bg_mode!r}")
     unsupported = []
-    if stall_count_mode != "proposals":
-        unsupported.append("stall_count_mode='changed'")
     if step_mode == "trust_region" and plan.kind != "star":
         unsupported.append("step_mode='trust_region'")
     if convergence != "legacy":
@@ -235,8 +233,10 @@ def make_class_kernels(plan, n_bands: int, n_terms: int, *, render_backend: str,
         step_tol_pix=float(step_tol_pix), un_freeze_steps=int(un_freeze_steps),
         has_priors=int(bool(has_priors)), native_stamp=int(native_stamp),
         precision=_lib.PRECISIONS[precision], tc_min_rows=int(tc_min_rows),
+        stall_changed=int(stall_count_mode == "changed"),
         bg_joint=int(bg_mode == "joint"), tc_cond_max=float(tc_cond_max))
-    return ClassKernels(desc, render_mode, int(n_bands), str(plan.kind))
+    return ClassKernels(desc, render_mode, int(n_bands), str(plan.kind),
+                        step_protocol=str(stall_count_mode))
 
 
 def _slice_host(host: dict, rows: np.ndarray) -> dict:
@@ -278,12 +278,14 @@ def run_class_chunk(kernels: ClassKernels, psf_tree: PsfTree, host: dict,
     if init_state is not None:
         init = {k: np.asarray(init_state[k]) for k in ("p", "lam", "chi2", "consec",
                                                        "nrej", "nst")}
+        for k in ("n_same", "prej", "diverged"):   # "changed"-mode tracker carry
+            if init_state.get(k) is not None:
+                init[k] = np.asarray(init_state[k])
     out = dstack_dev.ctx.run_chunk(kernels.desc, arrays, int(max_steps),
                                    kernels.n_bands, init)
     nP = 6 * N
     out.update(perr=None, femarg=None, reprof=None, smetrics=None, swin=None,
                resid=None, resid_w=None, railed=np.zeros(n_c, bool),
-               n_same=np.zeros(n_c, np.int32), prej=np.zeros((n_c, nP), np.float32),
                wall_s=time.perf_counter() - t0)
     return out
 
