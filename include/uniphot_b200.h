@@ -72,6 +72,13 @@ typedef struct uph_class_desc {
                                previous rejected one; identical-proposal
                                runs set the diverged flag in the loop
                                (island_solver.py:1118-1208)                */
+  int32_t convergence_dlnp; /* 1: convergence "dlnp" (island_solver.py:
+                               1210-1333): chi2 carried in float64,
+                               absolute sub-quantum prongs, reject-exits
+                               at the lam cap or on a no-move proposal,
+                               plateau-certified exits reported converged;
+                               implies the "changed" stall counting        */
+  float plateau_dlnp_tol;   /* dlnp: the quantum is 2 * this (0.5)         */
   int32_t bg_joint;         /* 1: each band's planar background (1, X, Y
                                over the island window) is solved with the
                                fluxes in the inner linear step; 0: the data

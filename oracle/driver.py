@@ -48,12 +48,14 @@ def solve_chunk(host, rows, *, B, T, dstack, wstack, psfs, mode, table_path=None
                 precision="ref", max_steps=30, reg=1e-9, pos_step_max=0.5,
                 ftol_rel=1e-4, step_tol=0.1, processes: int = 1,
                 native: int = 0, bg_joint: bool = False,
-                stall_count_mode: str = "proposals") -> dict:
+                stall_count_mode: str = "proposals", convergence: str = "legacy",
+                plateau_dlnp_tol: float = 0.5) -> dict:
     table = SersicTable.load(table_path) if table_path is not None else None
     psf = psf_bands(psfs, T, mode)
     cfg = SolverConfig(reg=reg, pos_step_max=pos_step_max, ftol_rel=ftol_rel,
                        step_tol=step_tol, precision=precision,
-                       stall_count_mode=stall_count_mode)
+                       stall_count_mode=stall_count_mode, convergence=convergence,
+                       plateau_dlnp_tol=plateau_dlnp_tol)
     jobs = [(host, int(r), B, T, dstack, wstack, psf, table, mode, cfg, max_steps,
              native, bg_joint) for r in rows]
     if processes > 1 and len(jobs) > 1:

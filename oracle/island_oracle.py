@@ -396,6 +396,12 @@ class SolverConfig:
     # (island_solver.py:1118-1208); identical-proposal runs of
     # STALL_REJECT_K set the sticky diverged flag in the loop
     stall_count_mode: str = "proposals"
+    # "legacy" | "dlnp" (island_solver.py:1210-1333): chi2 carried in f64,
+    # absolute sub-quantum ftol, quantum-gated step prong, distinct-proposal
+    # stall counting with reject-exits at the lam cap or on a no-move
+    # proposal; plateau-certified reject-exits count as converged
+    convergence: str = "legacy"
+    plateau_dlnp_tol: float = 0.5
 
 
 class IslandSolver:
@@ -688,6 +694,24 @@ class IslandSolver:
         r64 = r.astype(np.float64)
         return float((r64 * r64).sum()), r
 
+    def chi2_of64(self, p):
+        """chi2 with the band sums accumulated in float64 and the prior
+        penalty's float32 squares summed in float64
+        (island_solver.py:741-758)."""
+        c = 0.0
+        for b in range(self.nb):
+            M, _ = self.models_band(b, p, False)
+            f, _, _ = self.fluxes_band(M, self.isl.data[b], self.isl.w[b])
+            cb, _ = self.chi2_band(M, self.isl.data[b], self.isl.w[b], f)
+            c += cb
+        isl = self.isl
+        if isl.has_priors:
+            keep = (isl.keep & isl.mmask[:, None]).reshape(-1)
+            t = (isl.prior_inv_sigma.astype(self.dt) * (p - isl.prior_mean).astype(self.dt))
+            sq = (t * t).astype(self.dt).astype(np.float64)
+            c += float(np.sum(np.where(keep, sq, 0.0)))
+        return c
+
     def prior_pen(self, p):
         isl = self.isl
         if not isl.has_priors:
@@ -795,18 +819,20 @@ class IslandSolver:
         dt = self.dt
         isl = self.isl
         cfg = self.cfg
-        changed = cfg.stall_count_mode == "changed"
+        dlnp = cfg.convergence == "dlnp"
+        changed = cfg.stall_count_mode == "changed" or dlnp
+        quantum = 2.0 * cfg.plateau_dlnp_tol
         div, n_same = False, 0
         prej = np.zeros(self.nP, dt)
         if state is None:
             p = isl.p0.astype(dt).copy()
             lam = dt(LM_LAMBDA0)
-            chi2 = self.chi2_of(p)
+            chi2 = self.chi2_of64(p) if dlnp else self.chi2_of(p)
             consec = nrej = nst = 0
         else:
             p = np.asarray(state["p"], dt).reshape(-1).copy()
             lam = dt(state["lam"])
-            chi2 = dt(state["chi2"])
+            chi2 = self.chi2_of64(p) if dlnp else dt(state["chi2"])
             consec, nrej, nst = (int(state["consec"]), int(state["nrej"]),
                                  int(state["nst"]))
             div = bool(state.get("diverged", False))
@@ -827,19 +853,26 @@ class IslandSolver:
             H, g = HG
             keep = self._keep(nst)
             p_try = self.propose(p, H, g, lam, keep)
-            chi2_try = self.chi2_of(p_try)
+            chi2_try = self.chi2_of64(p_try) if dlnp else self.chi2_of(p_try)
             accept = bool(chi2_try < chi2)
             p_new = p_try if accept else p
             lam_new = dt(max(lam * dt(LM_DOWN), dt(LAM_MIN))) if accept \
                 else dt(min(lam * dt(LM_UP), dt(LAM_MAX)))
-            dchi2 = dt(chi2 - chi2_try)
             se = (p_new - p).astype(np.float64).reshape(N, 6)
             pos_step = float(np.max(mmf * np.hypot(se[:, 0], se[:, 1])))
             shape_step = float(np.max(mmf[:, None] * np.abs(se[:, 2:6])))
-            small = accept and (dchi2 < dt(cfg.ftol_rel) * max(chi2, dt(1.0)))
+            if dlnp:
+                dchi2 = chi2 - chi2_try               # float64
+                sub_q = dchi2 < quantum
+                small = accept and sub_q
+                step_small = accept and pos_step < cfg.step_tol \
+                    and shape_step < SHAPE_STEP_TOL and sub_q
+            else:
+                dchi2 = dt(chi2 - chi2_try)
+                small = accept and (dchi2 < dt(cfg.ftol_rel) * max(chi2, dt(1.0)))
+                step_small = accept and pos_step < cfg.step_tol \
+                    and shape_step < SHAPE_STEP_TOL
             consec = consec + 1 if small else (0 if accept else consec)
-            step_small = accept and pos_step < cfg.step_tol \
-                and shape_step < SHAPE_STEP_TOL
             if changed:
                 # proposal identity (exact comparison) with the previous
                 # rejected proposal (island_solver.py:1180-1192)
@@ -852,11 +885,13 @@ class IslandSolver:
             else:
                 nrej = 0 if accept else nrej + 1
             stall_now = nrej >= STALL_REJECT_K
+            if dlnp and not accept and (lam >= dt(LAM_MAX) or bool(np.all(p_try == p))):
+                stall_now = True     # no further information reachable
             conv = (consec >= 2) or step_small or stall_now
             stall = stall_now
             if accept:
                 p = p_new
-                chi2 = dt(chi2_try)
+                chi2 = chi2_try if dlnp else dt(chi2_try)
                 HG = None
             lam = lam_new
             nst += 1
@@ -915,18 +950,22 @@ def solve_island(isl: IslandInput, cfg: SolverConfig, max_steps: int = 30,
     """Full per-island result (the row of run_class_chunk's dict)."""
     s = IslandSolver(isl, cfg)
     out = s.run(max_steps, state)
-    changed = cfg.stall_count_mode == "changed"
+    changed = cfg.stall_count_mode == "changed" or cfg.convergence == "dlnp"
     div = bool(out["div"]) if changed else False
     sd = float("nan")
     if out["stall"]:
         if not changed:   # changed mode keeps the in-loop tracker's flag
             div = s.diverged_probe(out["p"], out["lam"], out["nst"], out["HG"])
         sd = float(s.plateau_probe(out["p"], out["nst"], out["HG"]))
+    stall = bool(out["stall"])
+    if cfg.convergence == "dlnp" and stall and np.isfinite(sd) \
+            and sd > -2.0 * cfg.plateau_dlnp_tol:
+        stall = False        # certified: converged on the plateau
     F, E, G, GE = s.final_fluxes(out["p"])
     n_good = int(np.sum(isl.w > 0))
     return dict(p=out["p"].reshape(s.N, 6).astype(np.float32),
                 fluxes=F, ferr=E, bg=G, bg_err=GE, chi2=out["chi2"], conv=out["conv"],
-                stall=out["stall"], diverged=div, stall_dchi2=sd,
+                stall=stall, diverged=div, stall_dchi2=sd,
                 nst=out["nst"], lam=out["lam"], consec=out["consec"],
                 nrej=out["nrej"], n_good=n_good, steps=out["steps"],
                 n_same=out["n_same"], prej=np.asarray(out["prej"], np.float32))

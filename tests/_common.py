@@ -34,7 +34,7 @@ def field_classes(f, mode: str, kinds=("star", "mixed")):
 
 def run_gpu(plans, hosts, PAD, ds, ws, psfs, mode, max_steps=30, field=None,
             native=0, precision="plain", tc_min_rows=-1, tc_cond_max=-1.0,
-            bg_mode="frozen", stall_count_mode="proposals"):
+            bg_mode="frozen", stall_count_mode="proposals", convergence="legacy"):
     from uniphot_b200 import solver
     if field is None:
         field = solver.DeviceField(ds, ws, PAD)
@@ -46,7 +46,8 @@ def run_gpu(plans, hosts, PAD, ds, ws, psfs, mode, max_steps=30, field=None,
             pos_step_max_pix=0.5, chi2_ftol_rel=1e-4, step_tol_pix=0.1,
             un_freeze_steps=0, has_priors=bool(host["has_priors"]), render_mode=mode,
             native_stamp=native, precision=precision, tc_min_rows=tc_min_rows,
-            tc_cond_max=tc_cond_max, bg_mode=bg_mode, stall_count_mode=stall_count_mode)
+            tc_cond_max=tc_cond_max, bg_mode=bg_mode, stall_count_mode=stall_count_mode,
+            convergence=convergence)
         rows = np.arange(plan.n_islands)
         outs.append(solver.run_class_chunk(kern, tree, host, rows, rows.size,
                                            max_steps, field, field, PAD))
@@ -55,13 +56,13 @@ def run_gpu(plans, hosts, PAD, ds, ws, psfs, mode, max_steps=30, field=None,
 
 def run_oracle(plans, hosts, PAD, ds, ws, psfs, mode, precision="ref",
                max_steps=30, processes=1, native=0, bg_joint=False,
-               stall_count_mode="proposals"):
+               stall_count_mode="proposals", convergence="legacy"):
     from oracle.driver import solve_chunk
     return [solve_chunk(h, np.arange(p.n_islands), B=p.bbox_class, T=p.tier,
                         dstack=ds, wstack=ws, psfs=psfs, mode=mode, table_path=TABLE,
                         precision=precision, max_steps=max_steps, processes=processes,
                         native=native, bg_joint=bg_joint,
-                        stall_count_mode=stall_count_mode)
+                        stall_count_mode=stall_count_mode, convergence=convergence)
             for p, h in zip(plans, hosts)]
 
 

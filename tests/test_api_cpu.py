@@ -27,11 +27,17 @@ def test_invalid_options_raise_valueerror(bad):
         solver.make_class_kernels(_plan(), 3, 1, **KW, **bad)
 
 
-@pytest.mark.parametrize("opt", [dict(convergence="dlnp"),
-                                 dict(crossband={"rank": 1}), dict(scene_subtract=True)])
+@pytest.mark.parametrize("opt", [dict(crossband={"rank": 1}), dict(scene_subtract=True)])
 def test_unbuilt_options_raise(opt):
     with pytest.raises(ValueError, match="not supported"):
         solver.make_class_kernels(_plan("mixed"), 3, 1, **KW, **opt)
+
+
+def test_dlnp_convergence_sets_the_descriptor():
+    k = solver.make_class_kernels(_plan("mixed"), 3, 1, **KW, convergence="dlnp",
+                                  plateau_dlnp_tol=0.25)
+    assert k.desc.convergence_dlnp == 1 and k.step_protocol == "dlnp"
+    assert abs(k.desc.plateau_dlnp_tol - 0.25) < 1e-7
 
 
 def test_changed_stall_counting_sets_the_descriptor():

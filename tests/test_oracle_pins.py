@@ -276,3 +276,23 @@ def test_changed_mode_matches_legacy_when_no_repeats():
                        max_steps=30)
     assert a["nst"] == b["nst"] and a["conv"] == b["conv"]
     np.testing.assert_array_equal(a["p"], b["p"])
+
+
+def test_dlnp_zero_weight_island_exits_at_once_and_certifies():
+    """convergence='dlnp' (island_solver.py:1210-1333): a no-move proposal
+    is a terminal reject-exit; the plateau certificate (dchi2 = 0 >
+    -quantum) maps it to converged-on-plateau."""
+    isl, _ = _mini_island("analytic", n_src=1, gal=False, noise=False)
+    isl.w[:] = 0.0
+    out = O.solve_island(isl, O.SolverConfig(precision="ref", convergence="dlnp"),
+                         max_steps=30)
+    assert out["nst"] == 1 and out["conv"] and not out["stall"]
+    assert out["stall_dchi2"] == 0.0
+
+
+def test_dlnp_converges_on_a_blend():
+    isl, flux = _mini_island("analytic", n_src=2, seed=4)
+    out = O.solve_island(isl, O.SolverConfig(precision="ref", convergence="dlnp"),
+                         max_steps=30)
+    assert out["conv"] and not out["stall"]
+    np.testing.assert_allclose(out["fluxes"], flux, rtol=0.05)

@@ -40,7 +40,8 @@ class ClassDesc(C.Structure):
                 ("step_tol_pix", C.c_float), ("un_freeze_steps", C.c_int32),
                 ("has_priors", C.c_int32), ("native_stamp", C.c_int32),
                 ("precision", C.c_int32), ("tc_min_rows", C.c_int32),
-                ("stall_changed", C.c_int32), ("bg_joint", C.c_int32),
+                ("stall_changed", C.c_int32), ("convergence_dlnp", C.c_int32),
+                ("plateau_dlnp_tol", C.c_float), ("bg_joint", C.c_int32),
                 ("tc_cond_max", C.c_float)]
 
 

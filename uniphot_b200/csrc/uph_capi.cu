@@ -580,7 +580,9 @@ int add_chunk(uph_ctx* ctx, Chunk* ch, const uph_class_desc* cls,
   ClassDev& c = ch->c;
   c.n_isl = n; c.nb = nb; c.N = N; c.nP = nP; c.B = B; c.T = T; c.Sz = Sz; c.R = R;
   c.nbg = nbg; c.NL = N + nbg;
-  c.changed = cls->stall_changed ? 1 : 0;
+  c.dlnp = cls->convergence_dlnp ? 1 : 0;
+  c.quantum = 2.0f * cls->plateau_dlnp_tol;
+  c.changed = (cls->stall_changed || c.dlnp) ? 1 : 0;
   c.Kmax = Kmax; c.nLmax = nLmax; c.ntile_side = (Sz + UPH_TILE - 1) / UPH_TILE;
   c.mode = mode;
   c.native = (cls->native_stamp > 0 && cls->native_stamp < T) ? (cls->native_stamp | 1) : T;
@@ -676,6 +678,7 @@ int add_chunk(uph_ctx* ctx, Chunk* ch, const uph_class_desc* cls,
       c.gpart = cbuf<float>(ctx, ch, "gpart", (size_t)c.tc_split * n * nb * Kmax * Kmax, &rc);
   }
   ch->d_div = cbuf<uint8_t>(ctx, ch, "div", n, &rc);
+  if (c.dlnp) c.chi2d = cbuf<double>(ctx, ch, "chi2d", n, &rc);
   if (c.changed) {
     c.n_same = cbuf<int>(ctx, ch, "nsame", n, &rc);
     c.prej = cbuf<float>(ctx, ch, "prej", (size_t)n * nP, &rc);
@@ -873,11 +876,12 @@ int job_solve(uph_job* job, int max_steps) {
     Launcher L{job, s, recp};
     // initial chi2 (fresh chunks) and, for the tensor-core Gram, the fluxes
     // at the starting parameters that its residual row needs
-    if (ch->fresh || ch->c.fcur) {
+    // (dlnp: the float64 chi2 carry is recomputed at the starting point)
+    if (ch->fresh || ch->c.fcur || ch->c.dlnp) {
       L(0, [&] { launch_render(ch->c, ch->c.p, PH_ALL, s); }, 2);
       L(4, [&] { launch_gram_trial(ch->c, ch->c.p, PH_ALL, 0, ch->c.fcur, ch->c.acond_cur,
                                    s); });
-      if (ch->fresh) L(5, [&] { launch_accept(ch->c, PH_ALL, s); });
+      if (ch->fresh || ch->c.dlnp) L(5, [&] { launch_accept(ch->c, PH_ALL, s); });
     }
     if (max_steps > 0 && !job->profile && !ch->gexec) {
       Launcher Lc{job, s, nullptr};
@@ -1047,9 +1051,12 @@ int job_read(uph_job* job, int id, uph_chunk_out* out) {
   int steps_run = 0;
   for (int i = 0; i < n; ++i) {
     const bool st = (fl[i] & FL_STALL) != 0;
+    // dlnp: a reject-exit whose plateau certificate passes (the best damped
+    // step gains less than one quantum) converged on the plateau
+    const bool certified = c.dlnp && st && std::isfinite(pbest[i]) && pbest[i] > -c.quantum;
     if (out->nst) out->nst[i] = nst[i];
     if (out->conv) out->conv[i] = (fl[i] & FL_CONV) ? 1 : 0;
-    if (out->stall) out->stall[i] = st ? 1 : 0;
+    if (out->stall) out->stall[i] = (st && !certified) ? 1 : 0;
     if (out->stall_dchi2) out->stall_dchi2[i] = st ? pbest[i] : NAN;
     // the legacy probe only runs on stalled islands; "changed" mode's flag
     // is the loop's sticky tracker and stands as it is

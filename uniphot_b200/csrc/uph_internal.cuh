@@ -129,6 +129,12 @@ struct ClassDev {
   // "changed" stall counting: identical-proposal reject runs (n_same), the
   // last rejected proposal (prej, n_isl x nP) and the sticky diverged flag
   int changed;
+  // convergence "dlnp": chi2 carried in float64 (chi2d), absolute
+  // sub-quantum prongs (quantum = 2 plateau_dlnp_tol), reject-exits at the
+  // lam cap or on a no-move proposal; implies the "changed" counting
+  int dlnp;
+  float quantum;
+  double* chi2d;
   int* n_same;
   float* prej;
   uint8_t* div_live;

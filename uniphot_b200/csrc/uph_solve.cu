@@ -947,23 +947,34 @@ __global__ void k_accept(ClassDev c, int phase) {
   const int nP = c.nP;
   const float* pt = c.p_try + (size_t)isl * nP;
   work_add(c, WK_ACCEPT, 8ull * c.nb + 8ull * nP, 0);
+  // chi2 of p_try: float32 band accumulation (legacy), and for dlnp the
+  // float64 accumulation of the same band sums (island_solver.py:741-758)
   float chi2_try = 0.f;
-  for (int b = 0; b < c.nb; ++b)
-    chi2_try = __fadd_rn(chi2_try, (float)c.chi2b[(size_t)isl * c.nb + b]);
+  double chi2_64 = 0.0;
+  for (int b = 0; b < c.nb; ++b) {
+    const double cb = c.chi2b[(size_t)isl * c.nb + b];
+    chi2_try = __fadd_rn(chi2_try, (float)cb);
+    chi2_64 += cb;
+  }
   if (c.has_priors) {
     float pen = 0.f;
+    double pen64 = 0.0;
     const float* pm = c.prior_mean + (size_t)isl * nP;
     const float* pinv = c.prior_inv + (size_t)isl * nP;
     for (int q = 0; q < nP; ++q) {
       const int k = q / 6;
       if (!(c.keep[(size_t)isl * nP + q] && c.mmask[isl * c.N + k])) continue;
       const float t = __fmul_rn(pinv[q], __fsub_rn(pt[q], pm[q]));
-      pen = __fadd_rn(pen, __fmul_rn(t, t));
+      const float t2 = __fmul_rn(t, t);
+      pen = __fadd_rn(pen, t2);
+      pen64 += (double)t2;
     }
     chi2_try = __fadd_rn(chi2_try, pen);
+    chi2_64 += pen64;
   }
   if (phase == PH_ALL) {
     c.chi2[isl] = chi2_try;
+    if (c.dlnp) c.chi2d[isl] = chi2_64;
     return;
   }
   if (phase == PH_PROBE) {
@@ -974,7 +985,7 @@ __global__ void k_accept(ClassDev c, int phase) {
   float* p = c.p + (size_t)isl * nP;
   const float chi2 = c.chi2[isl];
   const float lam = c.lam[isl];
-  const bool accept = chi2_try < chi2;
+  const bool accept = c.dlnp ? (chi2_64 < c.chi2d[isl]) : (chi2_try < chi2);
   const float lam_new = accept ? fmaxf(__fmul_rn(lam, 0.1f), 1e-9f)
                                : fminf(__fmul_rn(lam, 10.0f), 1e6f);
   const float dchi2 = __fsub_rn(chi2, chi2_try);
@@ -989,10 +1000,15 @@ __global__ void k_accept(ClassDev c, int phase) {
         shape_step = fmaxf(shape_step, mm * fabsf(__fsub_rn(pt[6 * k + j], p[6 * k + j])));
     }
   }
-  const bool small = accept && (dchi2 < __fmul_rn(c.ftol_rel, fmaxf(chi2, 1.0f)));
+  // dlnp (island_solver.py:1283-1292): absolute sub-quantum ftol, and the
+  // step prong only on sub-quantum steps
+  const bool sub_q = c.dlnp && (c.chi2d[isl] - chi2_64 < (double)c.quantum);
+  const bool small = c.dlnp ? (accept && sub_q)
+                            : (accept && (dchi2 < __fmul_rn(c.ftol_rel, fmaxf(chi2, 1.0f))));
   int consec = c.consec[isl];
   consec = small ? consec + 1 : (accept ? 0 : consec);
-  const bool step_small = accept && (pos_step < c.step_tol) && (shape_step < 0.01f);
+  const bool step_small = accept && (pos_step < c.step_tol) && (shape_step < 0.01f) &&
+                          (!c.dlnp || sub_q);
   int nrej = accept ? 0 : c.nrej[isl] + 1;
   if (c.changed) {
     // "changed" counting (island_solver.py:1180-1192): the reject counts
@@ -1009,7 +1025,13 @@ __global__ void k_accept(ClassDev c, int phase) {
     c.n_same[isl] = ns;
     if (ns >= 4) c.div_live[isl] = 1;
   }
-  const bool stall_now = nrej >= 4;
+  bool stall_now = nrej >= 4;
+  if (c.dlnp && !accept) {
+    // terminal reject-exits: tested at the lam cap, or a no-move proposal
+    bool no_move = true;
+    for (int q = 0; q < nP && no_move; ++q) no_move = pt[q] == p[q];
+    if (lam >= 1e6f || no_move) stall_now = true;
+  }
   const bool conv = (consec >= 2) || step_small || stall_now;
   uint8_t nf = fl;
   if (accept) {
@@ -1021,6 +1043,7 @@ __global__ void k_accept(ClassDev c, int phase) {
         c.acond_cur[(size_t)isl * c.nb + b] = c.acond_try[(size_t)isl * c.nb + b];
     }
     c.chi2[isl] = chi2_try;
+    if (c.dlnp) c.chi2d[isl] = chi2_64;
     nf |= FL_NEEDLIN;
   }
   if (conv) nf |= FL_CONV;

@@ -214,8 +214,6 @@ def make_class_kernels(plan, n_bands: int, n_terms: int, *, render_backend: str,
     unsupported = []
     if step_mode == "trust_region" and plan.kind != "star":
         unsupported.append("step_mode='trust_region'")
-    if convergence != "legacy":
-        unsupported.append("convergence='dlnp'")
     if crossband is not None:
         unsupported.append("crossband")
     if scene_subtract:
@@ -234,9 +232,12 @@ def make_class_kernels(plan, n_bands: int, n_terms: int, *, render_backend: str,
         has_priors=int(bool(has_priors)), native_stamp=int(native_stamp),
         precision=_lib.PRECISIONS[precision], tc_min_rows=int(tc_min_rows),
         stall_changed=int(stall_count_mode == "changed"),
+        convergence_dlnp=int(convergence == "dlnp"),
+        plateau_dlnp_tol=float(plateau_dlnp_tol),
         bg_joint=int(bg_mode == "joint"), tc_cond_max=float(tc_cond_max))
     return ClassKernels(desc, render_mode, int(n_bands), str(plan.kind),
-                        step_protocol=str(stall_count_mode))
+                        step_protocol="dlnp" if convergence == "dlnp"
+                        else str(stall_count_mode))
 
 
 def _slice_host(host: dict, rows: np.ndarray) -> dict:
