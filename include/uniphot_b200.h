@@ -88,6 +88,14 @@ typedef struct uph_class_desc {
                                normal matrix has a conditioning indicator
                                above this (in any band) form the Gram in
                                FP32; < 0 selects UPH_TC_COND_MAX_DEFAULT  */
+  int32_t step_tr;          /* step_mode: 0 "clip" (damped step, per-
+                               parameter clips, lam x10 / x0.1); 1
+                               "trust_region" (island_solver.py:1004-1116):
+                               scaled dogleg inside a radius carried in the
+                               lam slot (0 = unset, seeded by the first
+                               Gauss-Newton step), radius updated from the
+                               chi2 gain ratio; excludes stall_changed and
+                               convergence_dlnp                            */
 } uph_class_desc;
 
 #define UPH_TC_MIN_ROWS_DEFAULT 24
@@ -148,6 +156,9 @@ typedef struct uph_chunk_out {
   float* bg_err;        /* [n*nb*3] its sqrt(diag inv A64); may be NULL    */
   int32_t* n_same;      /* [n]     "changed" tracker (0 otherwise); may be NULL */
   float* prej;          /* [n*N*6] last rejected proposal; may be NULL     */
+  uint8_t* railed;      /* [n] trust region: a kept member parameter sits
+                           at its box bound (island_solver.py:1717-1728);
+                           0 in clip mode; may be NULL                     */
 } uph_chunk_out;
 
 /* Context: one per device per process. */

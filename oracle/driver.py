@@ -49,13 +49,13 @@ def solve_chunk(host, rows, *, B, T, dstack, wstack, psfs, mode, table_path=None
                 ftol_rel=1e-4, step_tol=0.1, processes: int = 1,
                 native: int = 0, bg_joint: bool = False,
                 stall_count_mode: str = "proposals", convergence: str = "legacy",
-                plateau_dlnp_tol: float = 0.5) -> dict:
+                plateau_dlnp_tol: float = 0.5, step_mode: str = "clip") -> dict:
     table = SersicTable.load(table_path) if table_path is not None else None
     psf = psf_bands(psfs, T, mode)
     cfg = SolverConfig(reg=reg, pos_step_max=pos_step_max, ftol_rel=ftol_rel,
                        step_tol=step_tol, precision=precision,
                        stall_count_mode=stall_count_mode, convergence=convergence,
-                       plateau_dlnp_tol=plateau_dlnp_tol)
+                       plateau_dlnp_tol=plateau_dlnp_tol, step_mode=step_mode)
     jobs = [(host, int(r), B, T, dstack, wstack, psf, table, mode, cfg, max_steps,
              native, bg_joint) for r in rows]
     if processes > 1 and len(jobs) > 1:
@@ -66,7 +66,8 @@ def solve_chunk(host, rows, *, B, T, dstack, wstack, psfs, mode, table_path=None
         res = [_one(j) for j in jobs]
     out = {}
     for k in ("p", "fluxes", "ferr", "bg", "bg_err", "chi2", "conv", "stall", "diverged",
-              "stall_dchi2", "nst", "lam", "consec", "nrej", "n_good", "n_same", "prej"):
+              "stall_dchi2", "nst", "lam", "consec", "nrej", "n_good", "n_same", "prej",
+              "railed"):
         out[k] = np.stack([np.asarray(r[k]) for r in res])
     out["steps_run"] = int(max(r["steps"] for r in res))
     return out

@@ -41,6 +41,10 @@ Algorithm followed (paths relative to the reference project ``tract7dt/``):
 * LM step (keep mask, damping, f64 solve, clips, bounds, accept/reject,
   three convergence prongs): ``island_solver.py:921-1002`` with constants
   ``:146-152`` and ``fit/grid_gpu/island_plan.py:55-74``.
+* Step variants: trust-region scaled dogleg ``island_solver.py:1004-1116``
+  (radius carried in the lam slot, seeded by the first Gauss-Newton step),
+  "changed" stall counting ``:1118-1208``, "dlnp" convergence
+  ``:1210-1333``; bound-pinned disclosure ``:1717-1728``.
 * Post-hoc divergence probe ``island_solver.py:1335-1399``, plateau probe
   ``:1401-1465``, final fluxes and errors ``:1467-1482``, good-pixel count
   ``:2690-2699``.
@@ -78,6 +82,10 @@ SHAPE_STEP_TOL = 0.01
 LM_LAMBDA0 = 1e-3
 LM_UP, LM_DOWN = 10.0, 0.1
 LAM_MIN, LAM_MAX = 1e-9, 1e6
+# trust-region radius update (island_solver.py:154-163): Nocedal & Wright
+# Alg. 4.1 gain-ratio thresholds, shrink and expand factors
+TR_ETA_LO, TR_ETA_HI = 0.25, 0.75
+TR_SHRINK, TR_EXPAND = 0.25, 2.0
 
 _ORDER_OF_NT = {1: 0, 3: 1, 6: 2, 10: 3, 15: 4, 21: 5}
 
@@ -402,6 +410,11 @@ class SolverConfig:
     # proposal; plateau-certified reject-exits count as converged
     convergence: str = "legacy"
     plateau_dlnp_tol: float = 0.5
+    # "clip" | "trust_region" (island_solver.py:1004-1116): scaled dogleg
+    # inside a radius carried in the lam slot; accept rule and the three
+    # convergence prongs as in the clip step.  Callers pass "clip" for star
+    # classes, which the reference exempts (island_solver.py:1910-1912).
+    step_mode: str = "clip"
 
 
 class IslandSolver:
@@ -814,6 +827,76 @@ class IslandSolver:
                         isl.upper.astype(dt)).astype(dt)
         return p_try
 
+    def propose_tr(self, p, H, g, delta_r, keep):
+        """Scaled dogleg step inside the trust radius (island_solver.py:
+        1021-1078).  Returns (p_try, pred, Dr, Dmax, at_bnd): the predicted
+        chi2 gain of the realised (box-clipped) step, the radius used (the
+        first call seeds it with the Gauss-Newton step's scaled length), the
+        radius cap and whether the step reached the boundary."""
+        dt = self.dt
+        isl = self.isl
+        nP = self.nP
+        ko = keep[:, None] & keep[None, :]
+        Hm = np.where(ko, H, dt(0)).astype(dt) + np.diag(
+            np.where(keep, 0.0, 1.0)).astype(dt)
+        gm = np.where(keep, g, dt(0)).astype(dt)
+        if isl.has_priors:
+            pi2 = (isl.prior_inv_sigma * isl.prior_inv_sigma).astype(dt)
+            pdiag = np.where(keep, pi2, dt(0)).astype(dt)
+            gm = (gm + np.where(keep, pi2 * (p - isl.prior_mean).astype(dt),
+                                dt(0))).astype(dt)
+            Hm = (Hm + np.diag(pdiag) + dt(1e-8) * np.eye(nP, dtype=dt)).astype(dt)
+        else:
+            Hm = (Hm + dt(1e-8) * np.eye(nP, dtype=dt)).astype(dt)
+        H64 = Hm.astype(np.float64)
+        g64 = gm.astype(np.float64)
+        dsc = np.sqrt(np.maximum(np.diag(H64), 1e-12))
+        s_gn = dsc * -np.linalg.solve(H64, g64)
+        n_gn = float(np.sqrt(s_gn @ s_gn))
+        Dr = float(delta_r)
+        if Dr <= 0.0:          # unset: the first Gauss-Newton step's length
+            Dr = max(n_gn, 1e-6)
+        gh = g64 / dsc
+        Hgh = (H64 @ (gh / dsc)) / dsc
+        ghHgh = float(gh @ Hgh)
+        gg = float(gh @ gh)
+        alpha = gg / max(ghHgh, 1e-30) if ghHgh > 0.0 else 1.0
+        s_c = -alpha * gh
+        ss = float(s_c @ s_c)
+        n_c = math.sqrt(ss)
+        diff = s_gn - s_c
+        aa = float(diff @ diff)
+        bb = 2.0 * float(s_c @ diff)
+        cc = ss - Dr * Dr
+        disc = max(bb * bb - 4.0 * aa * cc, 0.0)
+        t = min(max((-bb + math.sqrt(disc)) / max(2.0 * aa, 1e-30), 0.0), 1.0)
+        if n_gn <= Dr:
+            s = s_gn
+        elif n_c >= Dr:
+            s = (Dr / max(n_c, 1e-30)) * s_c if n_c > 0.0 else s_c
+        else:
+            s = s_c + t * diff
+        s_norm = float(np.sqrt(s @ s))
+        delta = np.where(keep, (s / dsc).astype(dt), dt(0)).astype(dt)
+        p_try = np.clip((p + delta).astype(dt), isl.lower.astype(dt),
+                        isl.upper.astype(dt)).astype(dt)
+        d = (p_try - p).astype(dt).astype(np.float64)
+        pred = -(float(g64 @ d) + 0.5 * float(d @ (H64 @ d)))
+        span = (isl.upper.astype(dt) - isl.lower.astype(dt)).astype(dt).astype(np.float64)
+        v = dsc * span
+        Dmax = float(np.sqrt(v @ v))
+        return p_try, pred, Dr, Dmax, s_norm >= 0.99 * Dr
+
+    def railed(self, p):
+        """Any kept member parameter at its box bound (island_solver.py:
+        1717-1728)."""
+        isl = self.isl
+        keep = (isl.keep & isl.mmask[:, None]).reshape(-1)
+        dt = self.dt
+        pp = np.asarray(p, dt).reshape(-1)
+        return bool(np.any(keep & ((pp <= isl.lower.astype(dt))
+                                   | (pp >= isl.upper.astype(dt)))))
+
     # ---------------- LM loop ----------------
     def run(self, max_steps, state=None):
         dt = self.dt
@@ -821,12 +904,13 @@ class IslandSolver:
         cfg = self.cfg
         dlnp = cfg.convergence == "dlnp"
         changed = cfg.stall_count_mode == "changed" or dlnp
+        tr = cfg.step_mode == "trust_region"
         quantum = 2.0 * cfg.plateau_dlnp_tol
         div, n_same = False, 0
         prej = np.zeros(self.nP, dt)
         if state is None:
             p = isl.p0.astype(dt).copy()
-            lam = dt(LM_LAMBDA0)
+            lam = dt(0.0) if tr else dt(LM_LAMBDA0)   # 0: radius unset
             chi2 = self.chi2_of64(p) if dlnp else self.chi2_of(p)
             consec = nrej = nst = 0
         else:
@@ -852,12 +936,28 @@ class IslandSolver:
                 HG = self.hg(p)
             H, g = HG
             keep = self._keep(nst)
-            p_try = self.propose(p, H, g, lam, keep)
+            if tr:
+                p_try, pred, Dr, Dmax, at_bnd = self.propose_tr(p, H, g, lam, keep)
+            else:
+                p_try = self.propose(p, H, g, lam, keep)
             chi2_try = self.chi2_of64(p_try) if dlnp else self.chi2_of(p_try)
             accept = bool(chi2_try < chi2)
             p_new = p_try if accept else p
-            lam_new = dt(max(lam * dt(LM_DOWN), dt(LAM_MIN))) if accept \
-                else dt(min(lam * dt(LM_UP), dt(LAM_MAX)))
+            if tr:
+                # gain ratio on the realised step; radius update of
+                # Nocedal & Wright Alg. 4.1 (island_solver.py:1079-1092)
+                actual = float(dt(chi2 - chi2_try))
+                rho = actual / (pred if pred > 0.0 else 1e-30)
+                if rho < TR_ETA_LO:
+                    Dr_new = Dr * TR_SHRINK
+                elif rho > TR_ETA_HI and at_bnd:
+                    Dr_new = min(Dr * TR_EXPAND, Dmax)
+                else:
+                    Dr_new = Dr
+                lam_new = dt(Dr_new)
+            else:
+                lam_new = dt(max(lam * dt(LM_DOWN), dt(LAM_MIN))) if accept \
+                    else dt(min(lam * dt(LM_UP), dt(LAM_MAX)))
             se = (p_new - p).astype(np.float64).reshape(N, 6)
             pos_step = float(np.max(mmf * np.hypot(se[:, 0], se[:, 1])))
             shape_step = float(np.max(mmf[:, None] * np.abs(se[:, 2:6])))
@@ -963,12 +1063,14 @@ def solve_island(isl: IslandInput, cfg: SolverConfig, max_steps: int = 30,
         stall = False        # certified: converged on the plateau
     F, E, G, GE = s.final_fluxes(out["p"])
     n_good = int(np.sum(isl.w > 0))
+    railed = s.railed(out["p"]) if cfg.step_mode == "trust_region" else False
     return dict(p=out["p"].reshape(s.N, 6).astype(np.float32),
                 fluxes=F, ferr=E, bg=G, bg_err=GE, chi2=out["chi2"], conv=out["conv"],
                 stall=stall, diverged=div, stall_dchi2=sd,
                 nst=out["nst"], lam=out["lam"], consec=out["consec"],
                 nrej=out["nrej"], n_good=n_good, steps=out["steps"],
-                n_same=out["n_same"], prej=np.asarray(out["prej"], np.float32))
+                n_same=out["n_same"], prej=np.asarray(out["prej"], np.float32),
+                railed=railed)
 
 
 def island_inputs_from_host(host: dict, row: int, *, B: int, T: int,

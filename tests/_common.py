@@ -34,7 +34,8 @@ def field_classes(f, mode: str, kinds=("star", "mixed")):
 
 def run_gpu(plans, hosts, PAD, ds, ws, psfs, mode, max_steps=30, field=None,
             native=0, precision="plain", tc_min_rows=-1, tc_cond_max=-1.0,
-            bg_mode="frozen", stall_count_mode="proposals", convergence="legacy"):
+            bg_mode="frozen", stall_count_mode="proposals", convergence="legacy",
+            step_mode="clip"):
     from uniphot_b200 import solver
     if field is None:
         field = solver.DeviceField(ds, ws, PAD)
@@ -47,7 +48,7 @@ def run_gpu(plans, hosts, PAD, ds, ws, psfs, mode, max_steps=30, field=None,
             un_freeze_steps=0, has_priors=bool(host["has_priors"]), render_mode=mode,
             native_stamp=native, precision=precision, tc_min_rows=tc_min_rows,
             tc_cond_max=tc_cond_max, bg_mode=bg_mode, stall_count_mode=stall_count_mode,
-            convergence=convergence)
+            convergence=convergence, step_mode=step_mode)
         rows = np.arange(plan.n_islands)
         outs.append(solver.run_class_chunk(kern, tree, host, rows, rows.size,
                                            max_steps, field, field, PAD))
@@ -56,13 +57,16 @@ def run_gpu(plans, hosts, PAD, ds, ws, psfs, mode, max_steps=30, field=None,
 
 def run_oracle(plans, hosts, PAD, ds, ws, psfs, mode, precision="ref",
                max_steps=30, processes=1, native=0, bg_joint=False,
-               stall_count_mode="proposals", convergence="legacy"):
+               stall_count_mode="proposals", convergence="legacy", step_mode="clip"):
+    """The oracle over every class (star classes keep the clip step, as the
+    reference exempts them from the trust region)."""
     from oracle.driver import solve_chunk
     return [solve_chunk(h, np.arange(p.n_islands), B=p.bbox_class, T=p.tier,
                         dstack=ds, wstack=ws, psfs=psfs, mode=mode, table_path=TABLE,
                         precision=precision, max_steps=max_steps, processes=processes,
                         native=native, bg_joint=bg_joint,
-                        stall_count_mode=stall_count_mode, convergence=convergence)
+                        stall_count_mode=stall_count_mode, convergence=convergence,
+                        step_mode=step_mode if p.kind != "star" else "clip")
             for p, h in zip(plans, hosts)]
 
 

@@ -21,6 +21,7 @@ KW = dict(render_backend="fft", reg=1e-9, pos_step_max_pix=0.5, chi2_ftol_rel=1e
                                  dict(convergence="x"),
                                  dict(convergence="dlnp", step_mode="trust_region"),
                                  dict(convergence="dlnp", stall_count_mode="changed"),
+                                 dict(step_mode="trust_region", stall_count_mode="changed"),
                                  dict(render_mode="x")])
 def test_invalid_options_raise_valueerror(bad):
     with pytest.raises(ValueError):
@@ -67,3 +68,11 @@ def test_psf_tree_padding_keeps_centre():
     tree, nt = solver.build_psf_tree([PsfPolynomial(c, 0, 1, 0, 1, 5, 5)], 9)
     assert nt == 1 and tree.params.shape == (1, 9, 9, 1)
     assert tree.params[0, 4, 4, 0] == 1.0 and tree.params.sum() == 1.0
+
+
+def test_trust_region_sets_the_descriptor_except_on_star_classes():
+    """Star-only classes keep the clip step (island_solver.py:1910-1912)."""
+    k = solver.make_class_kernels(_plan("mixed"), 3, 1, **KW, step_mode="trust_region")
+    assert k.desc.step_tr == 1 and k.step_mode == "trust_region"
+    k = solver.make_class_kernels(_plan("star"), 3, 1, **KW, step_mode="trust_region")
+    assert k.desc.step_tr == 0 and k.step_mode == "clip"

@@ -1,7 +1,8 @@
-"""Step-protocol variants on the GPU vs the oracle (island_solver.py:1118-
-1208): stall_count_mode="changed" keeps an in-loop tracker of the last
-rejected proposal; identical-proposal rejects escalate lambda without
-counting toward the stall, and a run of 4 sets the sticky diverged flag.
+"""Step variants on the GPU vs the oracle: stall_count_mode="changed"
+(island_solver.py:1118-1208) keeps an in-loop tracker of the last rejected
+proposal -- identical-proposal rejects escalate lambda without counting
+toward the stall, and a run of 4 sets the sticky diverged flag;
+convergence="dlnp" (:1210-1333); step_mode="trust_region" (:1004-1116).
 """
 import numpy as np
 import pytest
@@ -116,3 +117,87 @@ def test_dlnp_zero_weight_island_is_certified(small):
     g = g[0]
     assert g["nst"][0] == 1 and g["conv"][0] and not g["stall"][0]
     assert g["stall_dchi2"][0] == 0.0
+
+
+@pytest.mark.parametrize("mode,kinds", [("analytic", ("star", "mixed"))])
+def test_trust_region_parity(small, mode, kinds):
+    """step_mode="trust_region" (island_solver.py:1004-1116) on the mixed
+    classes, clip on the star classes.  The radius update branches on the
+    gain ratio of two float chi2 values, so a near-tie can send the two
+    sides down different radii: iteration counts and flags must agree on
+    90% of islands, fluxes and positions on every island."""
+    plans, hosts, PAD, ds, ws, psfs = field_classes(small, mode, kinds)
+    g, _ = run_gpu(plans, hosts, PAD, ds, ws, psfs, mode, native=small.native,
+                   step_mode="trust_region")
+    o = run_oracle(plans, hosts, PAD, ds, ws, psfs, mode, native=small.native,
+                   step_mode="trust_region")
+    n_same = n_all = 0
+    for p, h, gg, oo in zip(plans, hosts, g, o):
+        r = compare(gg, oo, h["mmask"])
+        msg = f"{p.key}: {r['max_rel']:.2e} {r['max_dpos']:.2e} " \
+              f"gpu nst {gg['nst'].tolist()} oracle nst {oo['nst'].tolist()}"
+        assert r["flux_ok"].all() and r["pos_ok"].all(), msg
+        same = r["same_nst"] & r["same_flags"]
+        n_same += int(same.sum())
+        n_all += same.size
+        np.testing.assert_array_equal(gg["railed"][same], oo["railed"][same])
+        if p.kind == "star":
+            assert not gg["railed"].any()
+        else:
+            assert np.all(gg["lam"][gg["nst"] > 0] > 0)   # a radius, never unset
+    assert n_same >= 0.9 * n_all, f"{n_same}/{n_all}"
+
+
+def test_trust_region_radius_carries_across_requeue(small):
+    """A re-queued chunk carrying the radius in lam equals one pass."""
+    from uniphot_b200 import solver
+    plans, hosts, PAD, ds, ws, psfs = field_classes(small, "analytic", ("mixed",))
+    p, h = plans[0], hosts[0]
+    full, fld = run_gpu([p], [h], PAD, ds, ws, psfs, "analytic", native=small.native,
+                        step_mode="trust_region")
+    a, _ = run_gpu([p], [h], PAD, ds, ws, psfs, "analytic", max_steps=2, field=fld,
+                   native=small.native, step_mode="trust_region")
+    a = a[0]
+    tree, nt = solver.build_psf_tree(psfs, p.tier)
+    kern = solver.make_class_kernels(p, ds.shape[0], nt, render_backend="fft", reg=1e-9,
+                                     pos_step_max_pix=0.5, chi2_ftol_rel=1e-4,
+                                     step_tol_pix=0.1, un_freeze_steps=0,
+                                     render_mode="analytic", native_stamp=small.native,
+                                     step_mode="trust_region")
+    rows = np.nonzero(~a["conv"])[0]
+    assert rows.size > 0
+    init = {k: a[k][rows] for k in ("p", "lam", "chi2", "consec", "nrej", "nst")}
+    b = solver.run_class_chunk(kern, tree, h, rows, rows.size, 28, fld, fld, PAD,
+                               init_state=init)
+    f = full[0]
+    np.testing.assert_array_equal(b["nst"], f["nst"][rows])
+    np.testing.assert_array_equal(b["p"], f["p"][rows])
+    np.testing.assert_array_equal(b["lam"], f["lam"][rows])
+
+
+def test_trust_region_production_field_parity():
+    """Reduced production field (512^2, 3 bands, 300 sources), classes of at
+    most 2 members: galaxies with bounded log-radius and free Sersic n
+    exercise the bound-pinned disclosure."""
+    from uniphot_b200.synth import make_production_field
+    f = make_production_field(3, side=512, n_bands=3, n_src=300)
+    plans, hosts, PAD, ds, ws, psfs = field_classes(f, "analytic", ("mixed",))
+    keep = [i for i, p in enumerate(plans) if p.nsrc_class <= 2]
+    plans = [plans[i] for i in keep]
+    hosts = [hosts[i] for i in keep]
+    g, _ = run_gpu(plans, hosts, PAD, ds, ws, psfs, "analytic", native=f.native,
+                   step_mode="trust_region")
+    o = run_oracle(plans, hosts, PAD, ds, ws, psfs, "analytic", native=f.native,
+                   processes=8, step_mode="trust_region")
+    n_same = n_all = n_railed = 0
+    for p, h, gg, oo in zip(plans, hosts, g, o):
+        r = compare(gg, oo, h["mmask"])
+        assert r["flux_ok"].all() and r["pos_ok"].all(), \
+            f"{p.key}: {r['max_rel']:.2e} {r['max_dpos']:.2e}"
+        same = r["same_nst"] & r["same_flags"]
+        n_same += int(same.sum())
+        n_all += same.size
+        np.testing.assert_array_equal(gg["railed"][same], oo["railed"][same])
+        n_railed += int(oo["railed"].sum())
+    assert n_same >= 0.9 * n_all, f"{n_same}/{n_all}"
+    assert n_railed > 0

@@ -296,3 +296,69 @@ def test_dlnp_converges_on_a_blend():
                          max_steps=30)
     assert out["conv"] and not out["stall"]
     np.testing.assert_allclose(out["fluxes"], flux, rtol=0.05)
+
+
+def _tr_setup(seed=5):
+    isl, flux = _mini_island("analytic", n_src=2, seed=seed)
+    s = O.IslandSolver(isl, O.SolverConfig(precision="f64", step_mode="trust_region"))
+    p = isl.p0.astype(np.float64)
+    H, g = s.hg(p)
+    return isl, s, p, H, g, s._keep(0)
+
+
+def test_trust_region_first_step_is_gauss_newton():
+    """An unset radius (0) is seeded with the scaled Gauss-Newton step's
+    length, so the first proposal is the Gauss-Newton step
+    (island_solver.py:1040-1044)."""
+    isl, s, p, H, g, keep = _tr_setup()
+    pt, pred, Dr, Dmax, at_bnd = s.propose_tr(p, H, g, 0.0, keep)
+    Hm = np.where(keep[:, None] & keep[None, :], H, 0) + np.diag(np.where(keep, 0, 1.0))
+    Hm = Hm + 1e-8 * np.eye(p.size)
+    gn = -np.linalg.solve(Hm, np.where(keep, g, 0))
+    np.testing.assert_allclose(pt - p, gn, rtol=1e-9, atol=1e-12)
+    dsc = np.sqrt(np.diag(Hm))
+    assert abs(Dr - np.linalg.norm(dsc * gn)) <= 1e-12 * Dr
+    assert at_bnd and pred > 0 and Dmax > Dr
+
+
+def test_trust_region_dogleg_respects_the_radius():
+    """A radius below the Cauchy point's length scales the steepest-descent
+    step to the boundary; one between it and the Gauss-Newton length takes
+    the dogleg blend, again on the boundary |D delta| = Dr."""
+    isl, s, p, H, g, keep = _tr_setup()
+    _, _, D0, _, _ = s.propose_tr(p, H, g, 0.0, keep)
+    Hm = np.where(keep[:, None] & keep[None, :], H, 0) + np.diag(np.where(keep, 0, 1.0))
+    dsc = np.sqrt(np.diag(Hm + 1e-8 * np.eye(p.size)))
+    gh = np.where(keep, g, 0) / dsc
+    for frac in (1e-4, 0.5):
+        Dr = frac * D0
+        pt, pred, Dr_used, _, at_bnd = s.propose_tr(p, H, g, Dr, keep)
+        step = dsc * (pt - p)
+        assert Dr_used == Dr and at_bnd and pred > 0
+        np.testing.assert_allclose(np.linalg.norm(step), Dr, rtol=1e-9)
+        if frac == 1e-4:    # pure (scaled) steepest descent direction
+            np.testing.assert_allclose(step / Dr, -gh / np.linalg.norm(gh), atol=1e-9)
+
+
+def test_trust_region_solve_converges_and_matches_clip():
+    isl, flux = _mini_island("analytic", n_src=2, seed=4)
+    a = O.solve_island(isl, O.SolverConfig(precision="f64"), max_steps=30)
+    b = O.solve_island(isl, O.SolverConfig(precision="f64", step_mode="trust_region"),
+                       max_steps=30)
+    assert b["conv"] and not b["stall"] and not b["railed"]
+    assert b["lam"] > 0
+    np.testing.assert_allclose(b["fluxes"], a["fluxes"], rtol=1e-3)
+    np.testing.assert_allclose(b["p"][:, :2], a["p"][:, :2], atol=1e-2)
+
+
+def test_trust_region_railed_flags_a_pinned_bound():
+    """The bound-pinned disclosure (island_solver.py:1717-1728) is set when
+    a kept parameter ends at its box bound."""
+    isl, _ = _mini_island("analytic", n_src=2, seed=4)
+    isl.upper = isl.upper.copy()
+    isl.upper[8] = isl.p0[8]          # member 1's log-radius pinned at its seed
+    out = O.solve_island(isl, O.SolverConfig(precision="ref", step_mode="trust_region"),
+                         max_steps=30)
+    assert out["railed"]
+    out = O.solve_island(isl, O.SolverConfig(precision="ref"), max_steps=30)
+    assert not out["railed"]      # clip mode reports none

@@ -42,7 +42,7 @@ class ClassDesc(C.Structure):
                 ("precision", C.c_int32), ("tc_min_rows", C.c_int32),
                 ("stall_changed", C.c_int32), ("convergence_dlnp", C.c_int32),
                 ("plateau_dlnp_tol", C.c_float), ("bg_joint", C.c_int32),
-                ("tc_cond_max", C.c_float)]
+                ("tc_cond_max", C.c_float), ("step_tr", C.c_int32)]
 
 
 class ChunkIn(C.Structure):
@@ -58,7 +58,7 @@ class ChunkOut(C.Structure):
         "p", "fluxes", "ferr", "chi2", "conv", "stall", "diverged",
         "stall_dchi2", "nst", "lam", "consec", "nrej", "n_good")] + \
         [("steps_run", C.c_int32), ("bg", _P), ("bg_err", _P), ("n_same", _P),
-         ("prej", _P)]
+         ("prej", _P), ("railed", _P)]
 
 
 class UphError(RuntimeError):
@@ -273,7 +273,8 @@ def chunk_out(n: int, N: int, nb: int):
                lam=np.zeros(n, np.float32), consec=np.zeros(n, np.int32),
                nrej=np.zeros(n, np.int32), n_good=np.zeros(n, np.int64),
                bg=np.zeros((n, nb, 3), np.float32), bg_err=np.zeros((n, nb, 3), np.float32),
-               n_same=np.zeros(n, np.int32), prej=np.zeros((n, 6 * N), np.float32))
+               n_same=np.zeros(n, np.int32), prej=np.zeros((n, 6 * N), np.float32),
+               railed=np.zeros(n, np.uint8))
     cout = ChunkOut()
     for k, v in out.items():
         setattr(cout, k, ptr(v))
@@ -281,7 +282,7 @@ def chunk_out(n: int, N: int, nb: int):
 
 
 def finish_out(out: dict, cout: ChunkOut) -> dict:
-    for k in ("conv", "stall", "diverged"):
+    for k in ("conv", "stall", "diverged", "railed"):
         out[k] = out[k].astype(bool)
     out["steps_run"] = int(cout.steps_run)
     return out

@@ -393,6 +393,7 @@ struct Chunk {
   uint8_t* d_divl0 = nullptr;
   float* d_p0 = nullptr;
   uint8_t* d_div = nullptr;
+  uint8_t* d_rail = nullptr;       // trust region: bound-pinned islands
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t gexec = nullptr;
   cudaEvent_t ev_group = nullptr;
@@ -583,6 +584,10 @@ int add_chunk(uph_ctx* ctx, Chunk* ch, const uph_class_desc* cls,
   c.dlnp = cls->convergence_dlnp ? 1 : 0;
   c.quantum = 2.0f * cls->plateau_dlnp_tol;
   c.changed = (cls->stall_changed || c.dlnp) ? 1 : 0;
+  c.tr = cls->step_tr ? 1 : 0;
+  if (c.tr && c.changed)
+    return set_err(ctx, UPH_ERR_INVALID,
+                   "step_tr excludes stall_changed and convergence_dlnp");
   c.Kmax = Kmax; c.nLmax = nLmax; c.ntile_side = (Sz + UPH_TILE - 1) / UPH_TILE;
   c.mode = mode;
   c.native = (cls->native_stamp > 0 && cls->native_stamp < T) ? (cls->native_stamp | 1) : T;
@@ -679,6 +684,10 @@ int add_chunk(uph_ctx* ctx, Chunk* ch, const uph_class_desc* cls,
   }
   ch->d_div = cbuf<uint8_t>(ctx, ch, "div", n, &rc);
   if (c.dlnp) c.chi2d = cbuf<double>(ctx, ch, "chi2d", n, &rc);
+  if (c.tr) {
+    c.trs = cbuf<double>(ctx, ch, "trs", (size_t)n * 4, &rc);
+    ch->d_rail = cbuf<uint8_t>(ctx, ch, "railed", n, &rc);
+  }
   if (c.changed) {
     c.n_same = cbuf<int>(ctx, ch, "nsame", n, &rc);
     c.prej = cbuf<float>(ctx, ch, "prej", (size_t)n * nP, &rc);
@@ -695,7 +704,8 @@ int add_chunk(uph_ctx* ctx, Chunk* ch, const uph_class_desc* cls,
   c.isl_nL = d_nL; c.isl_nr = d_nr; c.row_k = d_rk; c.row_s = d_rs; c.row_p = d_rp;
   c.reg = cls->reg; c.pos_step_max = cls->pos_step_max; c.ftol_rel = cls->chi2_ftol_rel;
   c.step_tol = cls->step_tol_pix; c.un_freeze = cls->un_freeze_steps;
-  std::vector<float> h_lam(n, 1e-3f), h_chi2(n, 0.f);
+  // the trust radius starts unset (0): the first step seeds it
+  std::vector<float> h_lam(n, c.tr ? 0.f : 1e-3f), h_chi2(n, 0.f);
   std::vector<int> h_consec(n, 0), h_nrej(n, 0);
   ch->h_nst0.assign(n, 0);
   ch->h_flags0.assign(n, FL_NEEDLIN | FL_REAL);
@@ -797,6 +807,10 @@ void post_loop(Chunk* ch, Launcher& L) {
     for (int j = 0; j < 4; ++j) L(3, [&] { launch_step(c, PH_PROBE, j, 0.f, 1, s); });
     launch_diverged_compare(c, ch->d_div, s);
     L.job->ctx->launches += 2;
+  }
+  if (c.tr) {
+    launch_railed(c, ch->d_rail, s);
+    L.job->ctx->launches += 1;
   }
   launch_fill_float(c.probe_best, INFINITY, c.n_isl, s);
   L.job->ctx->launches += 1;
@@ -1044,6 +1058,13 @@ int job_read(uph_job* job, int id, uph_chunk_out* out) {
   if ((rc = download(ctx, out->consec, c.consec, sizeof(int) * n, "consec"))) return rc;
   if ((rc = download(ctx, out->nrej, c.nrej, sizeof(int) * n, "nrej"))) return rc;
   if ((rc = download(ctx, out->diverged, ch->d_div, n, "diverged"))) return rc;
+  if (out->railed) {
+    if (c.tr) {
+      if ((rc = download(ctx, out->railed, ch->d_rail, n, "railed"))) return rc;
+    } else {
+      std::memset(out->railed, 0, n);
+    }
+  }
   if ((rc = download(ctx, fl.data(), c.flags, n, "flags"))) return rc;
   if ((rc = download(ctx, ng.data(), c.ngood, sizeof(int) * n * nb, "ngood"))) return rc;
   if ((rc = download(ctx, pbest.data(), c.probe_best, sizeof(float) * n, "probe"))) return rc;

@@ -138,6 +138,11 @@ struct ClassDev {
   int* n_same;
   float* prej;
   uint8_t* div_live;
+  // trust-region step: the radius lives in lam; k_step leaves per island
+  // (predicted gain, radius used, radius cap, step reached the boundary)
+  // in trs for k_accept's radius update
+  int tr;
+  double* trs;             // (n_isl, 4)
   float* bgout;            // (n_isl, nb, 3) final background coefficients
   float* bgerr;            // (n_isl, nb, 3) and their errors
   float* fcur;
@@ -282,6 +287,7 @@ void launch_accept(const ClassDev& c, int phase, cudaStream_t s);
 void launch_count_active(const ClassDev& c, cudaStream_t s);
 void launch_diverged_compare(const ClassDev& c, uint8_t* out,
                              cudaStream_t s);
+void launch_railed(const ClassDev& c, uint8_t* out, cudaStream_t s);
 size_t render_smem_bytes();
 size_t gram_lin_smem_bytes(int Kmax);
 size_t gram_trial_smem_bytes(int N);

@@ -820,8 +820,167 @@ __device__ void lu_solve(double* M, int n, int* piv, double* x) {
   __syncthreads();
 }
 
+// Sum of one double per thread over the block, in a fixed order (warp
+// butterflies, then the warps' partials in warp order); every thread gets
+// the total.  red holds NT / 32 doubles.
+__device__ double block_sum_d(double v, double* red) {
+  for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  double t = 0.0;
+  for (int w = 0; w < NT / 32; ++w) t += red[w];
+  return t;
+}
+
+// Masked, ridged normal matrix entry Hm[i][j] of the live rows (float, the
+// same arithmetic as the matrix handed to the solve): kept rows take H,
+// frozen rows a unit diagonal; the diagonal adds the prior 1/sigma^2 and
+// 1e-8.
+__device__ __forceinline__ float hm_entry(const ClassDev& c, const float* H, int ldH,
+                                          const uint8_t* kp, const int16_t* rp,
+                                          const float* pinv, int i, int j) {
+  float h;
+  if (kp[i] && kp[j]) h = H[i * ldH + j]; else h = (i == j) ? 1.f : 0.f;
+  if (i != j) return h;
+  if (c.has_priors) {
+    const float pi2 = kp[i] ? __fmul_rn(pinv[rp[i]], pinv[rp[i]]) : 0.f;
+    h = __fadd_rn(h, pi2);
+  }
+  return __fadd_rn(h, 1e-8f);
+}
+
+// Gradient entry of live row i with the prior pull (float).
+__device__ __forceinline__ float gm_entry(const ClassDev& c, const float* g,
+                                          const uint8_t* kp, const int16_t* rp,
+                                          const float* p, const float* pm,
+                                          const float* pinv, int i) {
+  float gi = kp[i] ? g[i] : 0.f;
+  if (c.has_priors && kp[i]) {
+    const int pp = rp[i];
+    gi = __fadd_rn(gi, __fmul_rn(__fmul_rn(pinv[pp], pinv[pp]), __fsub_rn(p[pp], pm[pp])));
+  }
+  return gi;
+}
+
+// Trust-region scaled dogleg (island_solver.py:1021-1078) for one island,
+// after the LU solve left x = Hm^-1 g in column nL of M.  With the Marquardt
+// scaling D = sqrt(diag Hm): the Gauss-Newton step s_gn = -D x, the Cauchy
+// point s_c = -alpha D^-1 g along the scaled gradient, and the dogleg to the
+// radius Dr (carried in lam; 0 seeds it with |s_gn|).  Writes p_try =
+// box-clip(p + D^-1 s) and, for k_accept, the predicted chi2 gain of the
+// realised step, Dr, the radius cap |D (upper - lower)| and whether the
+// step reached the boundary.  Parameters outside the live set have unit
+// diagonal and zero gradient: their scaled step is 0 and D = 1.
+__device__ void step_dogleg(const ClassDev& c, int isl, int nL, const double* M,
+                            const uint8_t* kp, const float* H, const float* g,
+                            double* dsc, double* gh, double* sgn, double* red,
+                            int16_t* qlive) {
+  const int tid = threadIdx.x;
+  const int nP = c.nP;
+  const int ldH = c.nLmax;
+  const int ld = nL + 1;
+  const int16_t* rp = c.row_p + (size_t)isl * c.Kmax;
+  const float* p = c.p + (size_t)isl * nP;
+  const float* pm = c.prior_mean + (size_t)isl * nP;
+  const float* pinv = c.prior_inv + (size_t)isl * nP;
+  const float* lo = c.lower + (size_t)isl * nP;
+  const float* hi = c.upper + (size_t)isl * nP;
+  float* out = c.p_try + (size_t)isl * nP;
+  for (int q = tid; q < nP; q += NT) qlive[q] = -1;
+  __syncthreads();
+  double a = 0.0, b = 0.0;
+  for (int i = tid; i < nL; i += NT) {
+    qlive[rp[i]] = (int16_t)i;
+    const double d = sqrt(fmax((double)hm_entry(c, H, ldH, kp, rp, pinv, i, i), 1e-12));
+    const double gi = (double)gm_entry(c, g, kp, rp, p, pm, pinv, i);
+    dsc[i] = d;
+    gh[i] = gi / d;
+    sgn[i] = d * -M[i * ld + nL];
+    a += sgn[i] * sgn[i];
+    b += gh[i] * gh[i];
+  }
+  const double n_gn = sqrt(block_sum_d(a, red));
+  const double gg = block_sum_d(b, red);
+  double Dr = (double)c.lam[isl];
+  if (Dr <= 0.0) Dr = fmax(n_gn, 1e-6);
+  // gh . (D^-1 Hm D^-1) gh
+  a = 0.0;
+  for (int i = tid; i < nL; i += NT) {
+    double t = 0.0;
+    for (int j = 0; j < nL; ++j)
+      t += (double)hm_entry(c, H, ldH, kp, rp, pinv, i, j) * (gh[j] / dsc[j]);
+    a += gh[i] * (t / dsc[i]);
+  }
+  const double ghHgh = block_sum_d(a, red);
+  const double alpha = ghHgh > 0.0 ? gg / fmax(ghHgh, 1e-30) : 1.0;
+  double ss = 0.0, sd = 0.0, dd = 0.0;
+  for (int i = tid; i < nL; i += NT) {
+    const double sc = -alpha * gh[i];
+    const double df = sgn[i] - sc;
+    ss += sc * sc;
+    sd += sc * df;
+    dd += df * df;
+  }
+  ss = block_sum_d(ss, red);
+  sd = block_sum_d(sd, red);
+  dd = block_sum_d(dd, red);
+  const double n_c = sqrt(ss);
+  const double bb = 2.0 * sd;
+  const double cc = ss - Dr * Dr;
+  const double disc = fmax(bb * bb - 4.0 * dd * cc, 0.0);
+  const double t_bl = fmin(fmax((-bb + sqrt(disc)) / fmax(2.0 * dd, 1e-30), 0.0), 1.0);
+  const int leg = (n_gn <= Dr) ? 0 : (n_c >= Dr ? 1 : 2);
+  const double cscale = (n_c > 0.0) ? Dr / fmax(n_c, 1e-30) : 1.0;
+  for (int q = tid; q < nP; q += NT) out[q] = p[q];
+  __syncthreads();
+  a = 0.0;
+  for (int i = tid; i < nL; i += NT) {
+    const double sc = -alpha * gh[i];
+    const double si = leg == 0 ? sgn[i] : (leg == 1 ? cscale * sc : sc + t_bl * (sgn[i] - sc));
+    a += si * si;
+    const float d = kp[i] ? (float)(si / dsc[i]) : 0.f;
+    out[rp[i]] = __fadd_rn(p[rp[i]], d);
+  }
+  const double s_norm = sqrt(block_sum_d(a, red));   // (synchronises)
+  for (int q = tid; q < nP; q += NT) out[q] = fminf(fmaxf(out[q], lo[q]), hi[q]);
+  __syncthreads();
+  // predicted gain of the realised step d = p_try - p (float differences):
+  // -(g.d + d.Hm.d / 2); parameters outside the live set have unit Hm
+  for (int i = tid; i < nL; i += NT) sgn[i] = (double)__fsub_rn(out[rp[i]], p[rp[i]]);
+  __syncthreads();
+  a = 0.0;
+  b = 0.0;
+  for (int i = tid; i < nL; i += NT) {
+    double t = 0.0;
+    for (int j = 0; j < nL; ++j) t += (double)hm_entry(c, H, ldH, kp, rp, pinv, i, j) * sgn[j];
+    a += (double)gm_entry(c, g, kp, rp, p, pm, pinv, i) * sgn[i] + 0.5 * sgn[i] * t;
+  }
+  for (int q = tid; q < nP; q += NT) {
+    const int i = qlive[q];
+    const double span = (double)__fsub_rn(hi[q], lo[q]);
+    const double dq = i >= 0 ? dsc[i] * span : span;
+    b += dq * dq;
+    if (i < 0) {
+      const double d = (double)__fsub_rn(out[q], p[q]);
+      a += 0.5 * d * d;
+    }
+  }
+  const double pred = -block_sum_d(a, red);
+  const double dmax = sqrt(block_sum_d(b, red));
+  if (tid == 0) {
+    double* t = c.trs + (size_t)isl * 4;
+    t[0] = pred;
+    t[1] = Dr;
+    t[2] = dmax;
+    t[3] = (s_norm >= 0.99 * Dr) ? 1.0 : 0.0;
+  }
+}
+
 // probe_mode: 0 normal step, 1 diverged probe j (lam_final * 10^(j-4)),
-// 2 plateau probe (lam = probe_lam)
+// 2 plateau probe (lam = probe_lam).  With c.tr a normal step is the
+// trust-region dogleg (island_solver.py:1004-1078); the probes stay damped
+// steps at lam, as the reference's probes are.
 __global__ void __launch_bounds__(NT)
 k_step(ClassDev c, int phase, int probe_mode, int probe_j, float probe_lam) {
   extern __shared__ double lsm[];
@@ -829,6 +988,9 @@ k_step(ClassDev c, int phase, int probe_mode, int probe_j, float probe_lam) {
   __shared__ double fac[UPH_MAXLIVE];
   __shared__ float delta[UPH_MAXLIVE];
   __shared__ uint8_t kp[UPH_MAXLIVE];
+  __shared__ double tr_a[UPH_MAXLIVE], tr_b[UPH_MAXLIVE], tr_c[UPH_MAXLIVE];
+  __shared__ double red[NT / 32];
+  __shared__ int16_t qlive[6 * UPH_MAXN];
   const int isl = blockIdx.x;
   if (isl >= c.n_isl) return;
   const uint8_t fl = c.flags[isl];
@@ -883,6 +1045,7 @@ k_step(ClassDev c, int phase, int probe_mode, int probe_j, float probe_lam) {
     kp[i] = k;
   }
   __syncthreads();
+  const bool trs = c.tr && probe_mode == 0;
   const bool use_smem = (nL <= UPH_LU_SMEM_N);
   double* M = use_smem ? lsm : (c.lu + (size_t)isl * c.nLmax * (c.nLmax + 1));
   const int ld = nL + 1;
@@ -893,7 +1056,7 @@ k_step(ClassDev c, int phase, int probe_mode, int probe_j, float probe_lam) {
       float h;
       if (kp[i] && kp[j]) h = H[i * ldH + j]; else h = (i == j) ? 1.f : 0.f;
       if (i == j) {
-        float hd = __fadd_rn(h, __fmul_rn(lam, h));
+        float hd = trs ? h : __fadd_rn(h, __fmul_rn(lam, h));
         if (c.has_priors) {
           const int pp = rp[i];
           const float pi2 = kp[i] ? __fmul_rn(pinv[pp], pinv[pp]) : 0.f;
@@ -917,6 +1080,10 @@ k_step(ClassDev c, int phase, int probe_mode, int probe_j, float probe_lam) {
   }
   __syncthreads();
   if (nL > 0) lu_solve(M, nL, &piv, fac);
+  if (trs) {
+    step_dogleg(c, isl, nL, M, kp, H, g, tr_a, tr_b, tr_c, red, qlive);
+    return;
+  }
   for (int i = tid; i < nL; i += NT) {
     const int pp = rp[i];
     float d = -(float)M[i * ld + nL];
@@ -986,8 +1153,20 @@ __global__ void k_accept(ClassDev c, int phase) {
   const float chi2 = c.chi2[isl];
   const float lam = c.lam[isl];
   const bool accept = c.dlnp ? (chi2_64 < c.chi2d[isl]) : (chi2_try < chi2);
-  const float lam_new = accept ? fmaxf(__fmul_rn(lam, 0.1f), 1e-9f)
-                               : fminf(__fmul_rn(lam, 10.0f), 1e6f);
+  float lam_new;
+  if (c.tr) {
+    // radius update from the gain ratio of the realised step
+    // (island_solver.py:1079-1092; Nocedal & Wright Alg. 4.1 constants)
+    const double* t = c.trs + (size_t)isl * 4;
+    const double pred = t[0], Dr = t[1], dmax = t[2];
+    const double actual = (double)__fsub_rn(chi2, chi2_try);
+    const double rho = actual / (pred > 0.0 ? pred : 1e-30);
+    const double dn = (rho < 0.25) ? Dr * 0.25
+                                   : ((rho > 0.75 && t[3] != 0.0) ? fmin(Dr * 2.0, dmax) : Dr);
+    lam_new = (float)dn;
+  } else {
+    lam_new = accept ? fmaxf(__fmul_rn(lam, 0.1f), 1e-9f) : fminf(__fmul_rn(lam, 10.0f), 1e6f);
+  }
   const float dchi2 = __fsub_rn(chi2, chi2_try);
   float pos_step = 0.f, shape_step = 0.f;
   if (accept) {
@@ -1082,6 +1261,21 @@ __global__ void k_diverged_compare(ClassDev c, uint8_t* out) {
   out[isl] = same;
 }
 
+// Bound-pinned disclosure of the trust-region step (island_solver.py:
+// 1717-1728): some kept member parameter sits at its lower or upper bound.
+__global__ void k_railed(ClassDev c, uint8_t* out) {
+  const int isl = blockIdx.x * blockDim.x + threadIdx.x;
+  if (isl >= c.n_isl) return;
+  const size_t o = (size_t)isl * c.nP;
+  bool r = false;
+  for (int q = 0; q < c.nP; ++q) {
+    if (!(c.keep[o + q] && c.mmask[(size_t)isl * c.N + q / 6])) continue;
+    const float v = c.p[o + q];
+    r = r || (v <= c.lower[o + q]) || (v >= c.upper[o + q]);
+  }
+  out[isl] = r ? 1 : 0;
+}
+
 __global__ void k_set_probe(ClassDev c) {
   const int isl = blockIdx.x * blockDim.x + threadIdx.x;
   if (isl >= c.n_isl) return;
@@ -1098,6 +1292,10 @@ __global__ void k_fill_float(float* p, float v, int n) {
 
 void launch_fill_float(float* p, float v, int n, cudaStream_t s) {
   if (n > 0) k_fill_float<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(p, v, n);
+}
+
+void launch_railed(const ClassDev& c, uint8_t* out, cudaStream_t s) {
+  k_railed<<<(unsigned)((c.n_isl + 127) / 128), 128, 0, s>>>(c, out);
 }
 
 void launch_set_probe(const ClassDev& c, cudaStream_t s) {

@@ -322,7 +322,7 @@ def unpack_class_results(plan, host, island_set, res_p, res_f, res_fe,
                          res_chi2, res_conv, res_stall, res_nst,
                          res_perr=None, res_pdchi2=None, res_div=None,
                          res_ngood=None, n_bands=0, res_bg=None, res_bg_err=None,
-                         **_unused) -> dict:
+                         res_railed=None, **_unused) -> dict:
     """Island rows -> source rows for the valid member slots.
 
     Parameter-error, profile and metric columns are NaN here: their
@@ -358,7 +358,8 @@ def unpack_class_results(plan, host, island_set, res_p, res_f, res_fe,
         diverged=(res_div[ii] if res_div is not None else np.zeros(n, bool)),
         stall_dchi2=(res_pdchi2[ii].astype(np.float32) if res_pdchi2 is not None
                      else _nan(n)),
-        railed=np.zeros(n, bool), free_n=fn[ii, kk],
+        railed=(res_railed[ii] if res_railed is not None else np.zeros(n, bool)),
+        free_n=fn[ii, kk],
         island_id=plan.isl_ids[ii].astype(np.int32),
         island_nsrc=island_set.n_src[plan.isl_ids][ii].astype(np.int32),
         island_giant=np.zeros(n, bool),

@@ -22,9 +22,10 @@ Differences, by design:
   is run (``bucket_stats`` still reports the counts);
 * ``dstack_dev`` is a :class:`DeviceField` (the field stacks resident in
   HBM inside the library context); ``wstack_dev`` is accepted and ignored;
-* options whose kernels are not built (trust-region, "changed"/"dlnp"
-  protocols, crossband GLS, scene subtract, post-convergence error / metric
-  / profile kernels) raise ``ValueError``.
+* options whose kernels are not built (crossband GLS, scene subtract,
+  post-convergence error / metric / profile kernels) raise ``ValueError``;
+  the step variants (``step_mode="trust_region"``, ``stall_count_mode=
+  "changed"``, ``convergence="dlnp"``) run on the device.
 """
 
 from __future__ import annotations
@@ -198,6 +199,11 @@ def make_class_kernels(plan, n_bands: int, n_terms: int, *, render_backend: str,
     if convergence == "dlnp" and step_mode != "clip":
         raise ValueError("convergence='dlnp' requires step_mode='clip' "
                          "(trust-region support pending)")
+    if step_mode == "trust_region" and stall_count_mode == "changed":
+        # the reference dispatches the trust-region step but runs the
+        # "changed" tracker loop, whose arity it does not match
+        raise ValueError("step_mode='trust_region' runs with "
+                         "stall_count_mode='proposals' only")
     if convergence == "dlnp" and stall_count_mode == "changed":
         raise ValueError("convergence='dlnp' subsumes stall_count_mode='changed' "
                          "(distinct-proposal counting is the dlnp behavior); "
@@ -212,8 +218,8 @@ def make_class_kernels(plan, n_bands: int, n_terms: int, *, render_backend: str,
     if bg_mode not in ("frozen", "joint"):
         raise ValueError(f"bg_mode must be 'frozen' or 'joint', got {bg_mode!r}")
     unsupported = []
-    if step_mode == "trust_region" and plan.kind != "star":
-        unsupported.append("step_mode='trust_region'")
+    # star-only classes keep the clip step (island_solver.py:1910-1912)
+    step_eff = str(step_mode) if str(plan.kind) != "star" else "clip"
     if crossband is not None:
         unsupported.append("crossband")
     if scene_subtract:
@@ -234,10 +240,11 @@ def make_class_kernels(plan, n_bands: int, n_terms: int, *, render_backend: str,
         stall_changed=int(stall_count_mode == "changed"),
         convergence_dlnp=int(convergence == "dlnp"),
         plateau_dlnp_tol=float(plateau_dlnp_tol),
-        bg_joint=int(bg_mode == "joint"), tc_cond_max=float(tc_cond_max))
+        bg_joint=int(bg_mode == "joint"), tc_cond_max=float(tc_cond_max),
+        step_tr=int(step_eff == "trust_region"))
     return ClassKernels(desc, render_mode, int(n_bands), str(plan.kind),
                         step_protocol="dlnp" if convergence == "dlnp"
-                        else str(stall_count_mode))
+                        else str(stall_count_mode), step_mode=step_eff)
 
 
 def _slice_host(host: dict, rows: np.ndarray) -> dict:
@@ -286,8 +293,7 @@ def run_class_chunk(kernels: ClassKernels, psf_tree: PsfTree, host: dict,
                                    kernels.n_bands, init)
     nP = 6 * N
     out.update(perr=None, femarg=None, reprof=None, smetrics=None, swin=None,
-               resid=None, resid_w=None, railed=np.zeros(n_c, bool),
-               wall_s=time.perf_counter() - t0)
+               resid=None, resid_w=None, wall_s=time.perf_counter() - t0)
     return out
 
 
@@ -443,7 +449,8 @@ class IslandFitJob:
                  nsrc_max: int | None = None, joint_nsrc_cap: int = 32,
                  star_render_split: bool = True,
                  stall_count_mode: str = "proposals", convergence: str = "legacy",
-                 plateau_dlnp_tol: float = 0.5, include_giants: bool = True,
+                 plateau_dlnp_tol: float = 0.5, step_mode: str = "clip",
+                 include_giants: bool = True,
                  compute_param_errors: bool = False,
                  compute_source_metrics: bool = False,
                  compute_re_profile: bool = False,
@@ -505,7 +512,8 @@ class IslandFitJob:
                 star_render_split=star_render_split,
                 has_priors=bool(host["has_priors"]),
                 stall_count_mode=stall_count_mode, convergence=convergence,
-                plateau_dlnp_tol=plateau_dlnp_tol, render_mode=render_mode,
+                plateau_dlnp_tol=plateau_dlnp_tol, step_mode=step_mode,
+                render_mode=render_mode,
                 native_stamp=fp.native, precision=precision, bg_mode=bg_mode)
             chunk = _chunk_size(plan, n_bands, chunk_budget_bytes)
             ids = []
@@ -552,7 +560,8 @@ class IslandFitJob:
                 res["chi2"], res["conv"], res["stall"], res["nst"],
                 res_pdchi2=res["stall_dchi2"], res_div=res["diverged"],
                 res_ngood=res["n_good"], n_bands=n_bands,
-                res_bg=res.get("bg"), res_bg_err=res.get("bg_err")))
+                res_bg=res.get("bg"), res_bg_err=res.get("bg_err"),
+                res_railed=res.get("railed")))
         giant_ids = np.concatenate([np.asarray(self.buckets.giant_ids, np.int64).ravel(),
                                     np.asarray(self.capped, np.int64)])
         if self.include_giants and giant_ids.size:
