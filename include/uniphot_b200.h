@@ -96,6 +96,25 @@ typedef struct uph_class_desc {
                                Gauss-Newton step), radius updated from the
                                chi2 gain ratio; excludes stall_changed and
                                convergence_dlnp                            */
+  int32_t param_errors;     /* 1: after the loop, the marginal covariance of
+                               the nonlinear parameters at the final
+                               parameters (island_solver.py:1484-1547):
+                               the undamped Gauss-Newton matrix relinearised
+                               there, static keep mask, plus the prior
+                               diagonal, inverted in float64; returned in
+                               uph_chunk_out.perr                          */
+  int32_t flux_marg;        /* 1: the shape-marginalised flux-variance
+                               increment (island_solver.py:1549-1613):
+                               per band and extended member, J Sigma J^T
+                               with J the flux solution's sensitivity to
+                               the extended members' kept parameters and
+                               Sigma the covariance of param_errors (which
+                               this pass runs too); uph_chunk_out.femarg  */
+  int32_t source_metrics;   /* 1: per-member model-quality metrics at the
+                               final fit (island_solver.py:1639-1715):
+                               rchisq, fracflux, fracin, fracmasked and the
+                               per-band window flux; uph_chunk_out.smetrics
+                               and .swin                                   */
 } uph_class_desc;
 
 #define UPH_TC_MIN_ROWS_DEFAULT 24
@@ -159,6 +178,20 @@ typedef struct uph_chunk_out {
   uint8_t* railed;      /* [n] trust region: a kept member parameter sits
                            at its box bound (island_solver.py:1717-1728);
                            0 in clip mode; may be NULL                     */
+  float* perr;          /* [n*N*13] with param_errors: per member var of
+                           (x, y, logre, ee1, ee2, u), cov(ee1, ee2), and
+                           the six prior fractions pinv^2/(H_kk + pinv^2)
+                           (NaN without priors); frozen and padded slots
+                           read variance 1; NaN-filled without
+                           param_errors; may be NULL                       */
+  float* femarg;        /* [n*nb*N] with flux_marg: the increment (0 for
+                           star rows and padded slots); NaN-filled
+                           without flux_marg; may be NULL                  */
+  float* smetrics;      /* [n*N*4] with source_metrics: rchisq, fracflux,
+                           fracin, fracmasked (padded slots NaN, 0, NaN,
+                           0); NaN-filled without; may be NULL             */
+  float* swin;          /* [n*nb*N] with source_metrics: f * sum(m) per
+                           band (NaN for padded slots); may be NULL        */
 } uph_chunk_out;
 
 /* Context: one per device per process. */

@@ -37,11 +37,12 @@ def psf_bands(psfs, tier: int, mode: str):
 
 
 def _one(args):
-    host, row, B, T, dstack, wstack, psf, table, mode, cfg, max_steps, native, bg = args
+    host, row, B, T, dstack, wstack, psf, table, mode, cfg, max_steps, native, bg, pe, fm, sm = args
     isl = island_inputs_from_host(host, row, B=B, T=T, dstack=dstack,
                                   wstack=wstack, psf=psf, table=table, mode=mode,
                                   native=native, bg_joint=bg)
-    return solve_island(isl, cfg, max_steps)
+    return solve_island(isl, cfg, max_steps, param_errors=pe, flux_marg=fm,
+                        source_metrics=sm)
 
 
 def solve_chunk(host, rows, *, B, T, dstack, wstack, psfs, mode, table_path=None,
@@ -49,7 +50,9 @@ def solve_chunk(host, rows, *, B, T, dstack, wstack, psfs, mode, table_path=None
                 ftol_rel=1e-4, step_tol=0.1, processes: int = 1,
                 native: int = 0, bg_joint: bool = False,
                 stall_count_mode: str = "proposals", convergence: str = "legacy",
-                plateau_dlnp_tol: float = 0.5, step_mode: str = "clip") -> dict:
+                plateau_dlnp_tol: float = 0.5, step_mode: str = "clip",
+                param_errors: bool = False, flux_marg: bool = False,
+                source_metrics: bool = False) -> dict:
     table = SersicTable.load(table_path) if table_path is not None else None
     psf = psf_bands(psfs, T, mode)
     cfg = SolverConfig(reg=reg, pos_step_max=pos_step_max, ftol_rel=ftol_rel,
@@ -57,7 +60,7 @@ def solve_chunk(host, rows, *, B, T, dstack, wstack, psfs, mode, table_path=None
                        stall_count_mode=stall_count_mode, convergence=convergence,
                        plateau_dlnp_tol=plateau_dlnp_tol, step_mode=step_mode)
     jobs = [(host, int(r), B, T, dstack, wstack, psf, table, mode, cfg, max_steps,
-             native, bg_joint) for r in rows]
+             native, bg_joint, param_errors, flux_marg, source_metrics) for r in rows]
     if processes > 1 and len(jobs) > 1:
         import multiprocessing as mp
         with mp.get_context("spawn").Pool(processes) as pool:
@@ -69,6 +72,10 @@ def solve_chunk(host, rows, *, B, T, dstack, wstack, psfs, mode, table_path=None
               "stall_dchi2", "nst", "lam", "consec", "nrej", "n_good", "n_same", "prej",
               "railed"):
         out[k] = np.stack([np.asarray(r[k]) for r in res])
+    out["perr"] = np.stack([r["perr"] for r in res]) if param_errors else None
+    out["femarg"] = np.stack([r["femarg"] for r in res]) if flux_marg else None
+    out["smetrics"] = np.stack([r["smetrics"] for r in res]) if source_metrics else None
+    out["swin"] = np.stack([r["swin"] for r in res]) if source_metrics else None
     out["steps_run"] = int(max(r["steps"] for r in res))
     return out
 

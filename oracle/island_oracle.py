@@ -46,7 +46,10 @@ Algorithm followed (paths relative to the reference project ``tract7dt/``):
   "changed" stall counting ``:1118-1208``, "dlnp" convergence
   ``:1210-1333``; bound-pinned disclosure ``:1717-1728``.
 * Post-hoc divergence probe ``island_solver.py:1335-1399``, plateau probe
-  ``:1401-1465``, final fluxes and errors ``:1467-1482``, good-pixel count
+  ``:1401-1465``, final fluxes and errors ``:1467-1482``, marginal
+  covariance of the nonlinear parameters ``:1484-1547``, shape-marginalised
+  flux-variance increment ``:1549-1613``, source metrics ``:1639-1715``,
+  good-pixel count
   ``:2690-2699``.
 
 A second render mode, ``analytic``, is the north-star forward model (not in the
@@ -745,10 +748,12 @@ class IslandSolver:
             c = dt(c + dt(self.prior_pen(p)))
         return c
 
-    def hg(self, p):
+    def hg(self, p, flux_jac=None):
         """Un-masked, un-damped Gauss-Newton (H, g) with the explicit
         VarPro Jacobian J_j = -sqrt(w)(f_k D_j + M^T c_j),
-        c_j = A64^{-1}(e_k s_j - f_k u_j)."""
+        c_j = A64^{-1}(e_k s_j - f_k u_j) = d f / d theta_j (the flux
+        solution's sensitivity).  ``flux_jac``, a dict, receives per band
+        (parameter indices, c rows (n_live, n_lin))."""
         dt = self.dt
         nP, N = self.nP, self.N
         H = np.zeros((nP, nP), dtype=dt)
@@ -767,6 +772,7 @@ class IslandSolver:
             Ainv = np.linalg.inv(A64)
             rows = []
             idx = []
+            cjs = []
             for (k, j, Dp) in Ds:
                 D64 = Dp.astype(np.float64).reshape(-1)
                 s = np.dot(D64 * w64, rt)
@@ -776,12 +782,15 @@ class IslandSolver:
                 cj = Ainv @ rhs
                 if dt == np.float32:
                     cj = cj.astype(np.float32).astype(np.float64)
+                cjs.append(cj)
                 J = -sw * (float(f[k]) * D64 + cj @ M64)
                 if dt == np.float32:
                     J = J.astype(np.float32).astype(np.float64)
                 rows.append(J)
                 idx.append(6 * k + j)
             Jb = np.stack(rows)
+            if flux_jac is not None:
+                flux_jac[b] = (np.array(idx), np.stack(cjs))
             Hb = Jb @ Jb.T
             gb = Jb @ r.astype(np.float64).reshape(-1)
             ii = np.array(idx)
@@ -1024,6 +1033,114 @@ class IslandSolver:
             best = v if best is None else min(best, v)
         return best
 
+    def _posterior(self, p, flux_jac=None):
+        """(H, keep, Hm, prior diagonal) at p with the static keep mask."""
+        dt = self.dt
+        isl = self.isl
+        H, _ = self.hg(p, flux_jac)
+        keep = (isl.keep & isl.mmask[:, None]).reshape(-1)
+        Hm = np.where(keep[:, None] & keep[None, :], H, dt(0)).astype(dt) + np.diag(
+            np.where(keep, 0.0, 1.0)).astype(dt)
+        pdiag = None
+        if isl.has_priors:
+            pi2 = (isl.prior_inv_sigma * isl.prior_inv_sigma).astype(dt)
+            pdiag = np.where(keep, pi2, dt(0)).astype(dt)
+            Hm = (Hm + np.diag(pdiag)).astype(dt)
+        return H, keep, Hm, pdiag
+
+    def final_flux_marg(self, p):
+        """Shape-marginalised flux-variance increment (island_solver.py:
+        1549-1613): per band and extended member k, J_k Sigma J_k^T with J
+        the flux solution's sensitivity to the extended members' kept
+        parameters and Sigma the posterior covariance of final_errors;
+        0 for star rows and padded slots.  (n_b, N) float32."""
+        N = self.N
+        isl = self.isl
+        fj = {}
+        _, keep, Hm, _ = self._posterior(p, fj)
+        S = np.linalg.inv(Hm.astype(np.float64))
+        ext = (isl.stype != 0) & isl.mmask
+        marg = (keep.reshape(N, 6) & ext[:, None]).reshape(-1)
+        out = np.zeros((self.nb, N), np.float32)
+        for b, (idx, C) in fj.items():
+            J = np.zeros((N, self.nP))
+            J[:, idx] = C[:, :N].T          # member fluxes only
+            J[:, ~marg] = 0.0
+            dv = np.einsum("ka,ab,kb->k", J, S, J)
+            out[b] = np.where(ext, np.maximum(dv, 0.0), 0.0)
+        return out
+
+    def source_metrics(self, p):
+        """Per-member model-quality metrics at p (island_solver.py:1639-
+        1715): rchisq (own-model-weighted chi2 per unit model flux),
+        fracflux (neighbours' light under the member's profile), fracin
+        (unit-model flux inside the window), fracmasked (unit-model flux on
+        zero-weight pixels), combined over bands as the reference does
+        (fin = clip(sum m, 0, 1) weights fracflux and fracmasked; fracin and
+        rchisq are ratios of band sums); and the per-band window flux
+        f * sum(m).  Returns ((N, 4), (n_b, N)) float32; padded slots give
+        NaN (rchisq, fracin, window flux) or 0.  With a joint background the
+        chi2 uses the full model (members and plane) and the neighbours'
+        light the members only."""
+        isl = self.isl
+        N, nb = self.N, self.nb
+        acc = np.zeros((8, N))
+        fwin = np.zeros((nb, N))
+        for b in range(nb):
+            d = isl.data[b].astype(np.float64)
+            w = isl.w[b].astype(np.float64)
+            M, _ = self.models_band(b, p, False)
+            f = self.fluxes_band(M, isl.data[b], isl.w[b])[0].astype(np.float64)
+            mods = M[:N].astype(np.float64)
+            model_m = np.tensordot(f[:N], mods, 1)
+            full = model_m + (np.tensordot(f[N:], M[N:].astype(np.float64), 1)
+                              if isl.bg_joint else 0.0)
+            own = f[:N, None, None] * mods
+            s_m = mods.sum(axis=(1, 2))
+            fin = np.clip(s_m, 0.0, 1.0)
+            bot = (own * own).sum(axis=(1, 2))
+            top = ((model_m[None] - own) * own).sum(axis=(1, 2))
+            ratio = np.where(bot > 0, top / np.where(bot > 0, bot, 1.0), 0.0)
+            fm = np.clip(((w == 0)[None] * mods).sum(axis=(1, 2)), 0.0, 1.0)
+            rc = (mods * (w * (d - full) ** 2)[None]).sum(axis=(1, 2))
+            acc += np.stack([fin * ratio, fin, np.abs(s_m), np.ones(N), fin * fm, fin,
+                             np.abs(rc), np.abs(s_m)])
+            fwin[b] = f[:N] * s_m
+        mm = isl.mmask
+
+        def ratio_of(n, dd, fill):
+            return np.where((dd > 0) & mm, n / np.where(dd > 0, dd, 1.0), fill)
+        met = np.stack([ratio_of(acc[6], acc[7], np.nan), ratio_of(acc[0], acc[1], 0.0),
+                        ratio_of(acc[2], acc[3], np.nan), ratio_of(acc[4], acc[5], 0.0)],
+                       axis=1)
+        fwin = np.where(mm[None, :], fwin, np.nan)
+        return met.astype(np.float32), fwin.astype(np.float32)
+
+    def final_errors(self, p):
+        """Marginal covariance of the nonlinear parameters at p
+        (island_solver.py:1484-1547): the undamped Gauss-Newton matrix with
+        the static keep mask (no annealing), plus the prior diagonal,
+        inverted in float64.  Returns (N, 13) float32: var(x, y, logre,
+        ee1, ee2, u), cov(ee1, ee2), the prior fractions
+        pinv^2 / (H_kk + pinv^2) (0 where that sum is 0; NaN without
+        priors)."""
+        dt = self.dt
+        N = self.N
+        H, keep, Hm, pdiag = self._posterior(p)
+        if pdiag is not None:
+            hdiag = np.where(keep, np.diag(H), dt(0)).astype(dt)
+            den = (hdiag + pdiag).astype(dt)
+            with np.errstate(invalid="ignore", divide="ignore"):
+                pf = np.where(den > 0, pdiag / np.where(den > 0, den, dt(1)), dt(0))
+            pf6 = pf.reshape(N, 6).astype(np.float64)
+        else:
+            pf6 = np.full((N, 6), np.nan)
+        S = np.linalg.inv(Hm.astype(np.float64))
+        var6 = np.diag(S).reshape(N, 6)
+        k6 = 6 * np.arange(N)
+        cov = S[k6 + 3, k6 + 4]
+        return np.concatenate([var6, cov[:, None], pf6], axis=1).astype(np.float32)
+
     def final_fluxes(self, p):
         """Fluxes and errors (n_b, N), and background coefficients and
         errors (n_b, 3; zero without bg_joint)."""
@@ -1046,7 +1163,8 @@ class IslandSolver:
 
 
 def solve_island(isl: IslandInput, cfg: SolverConfig, max_steps: int = 30,
-                 state=None):
+                 state=None, param_errors: bool = False, flux_marg: bool = False,
+                source_metrics: bool = False):
     """Full per-island result (the row of run_class_chunk's dict)."""
     s = IslandSolver(isl, cfg)
     out = s.run(max_steps, state)
@@ -1064,13 +1182,16 @@ def solve_island(isl: IslandInput, cfg: SolverConfig, max_steps: int = 30,
     F, E, G, GE = s.final_fluxes(out["p"])
     n_good = int(np.sum(isl.w > 0))
     railed = s.railed(out["p"]) if cfg.step_mode == "trust_region" else False
+    perr = s.final_errors(out["p"]) if param_errors else None
+    femarg = s.final_flux_marg(out["p"]) if flux_marg else None
+    smet, swin = s.source_metrics(out["p"]) if source_metrics else (None, None)
     return dict(p=out["p"].reshape(s.N, 6).astype(np.float32),
                 fluxes=F, ferr=E, bg=G, bg_err=GE, chi2=out["chi2"], conv=out["conv"],
                 stall=stall, diverged=div, stall_dchi2=sd,
                 nst=out["nst"], lam=out["lam"], consec=out["consec"],
                 nrej=out["nrej"], n_good=n_good, steps=out["steps"],
                 n_same=out["n_same"], prej=np.asarray(out["prej"], np.float32),
-                railed=railed)
+                railed=railed, perr=perr, femarg=femarg, smetrics=smet, swin=swin)
 
 
 def island_inputs_from_host(host: dict, row: int, *, B: int, T: int,

@@ -12,8 +12,11 @@ ROOT = Path(__file__).resolve().parents[1]
 TABLE = ROOT / "uniphot_b200" / "data" / "sersic_mog_table.npz"
 
 
-def field_classes(f, mode: str, kinds=("star", "mixed")):
-    """(plans, hosts, PAD, dstack, wstack, psfs) for a synthetic field."""
+def field_classes(f, mode: str, kinds=("star", "mixed"), priors: bool = False):
+    """(plans, hosts, PAD, dstack, wstack, psfs) for a synthetic field;
+    ``priors`` adds Gaussian priors on every member's position (0.3 px) and
+    on galaxies' radius (50%), ellipticity (0.2), angle (20 deg) and Sersic
+    index (1.0), centred on the seeds."""
     plans, _ = plan_island_classes(f.island_set, f.buckets, f.source_type, f.logre,
                                    f.sersic_n, f.native, tier_ladder=f.tier_ladder)
     plans = [p for p in plans if p.kind in kinds]
@@ -24,10 +27,16 @@ def field_classes(f, mode: str, kinds=("star", "mixed")):
     ds[:, PAD:PAD + H, PAD:PAD + W] = f.data_minus_bg
     ws[:, PAD:PAD + H, PAD:PAD + W] = f.invvar
     fn = free_n_gate(f.source_type, f.s1_flux, f.s1_flux_var, True, 30.0)
+    pri = {}
+    if priors:
+        n = f.pos_x.size
+        pri = dict(pos_err=np.full(n, 0.3), re_prior_sig=0.5 * np.exp(f.logre),
+                   ell_prior_sig=np.full(n, 0.2), theta_prior_sig=np.full(n, 20.0),
+                   sersic_n_prior_sig=np.full(n, 1.0))
     hosts = [class_host_arrays(p, pos_x=f.pos_x, pos_y=f.pos_y,
                                source_type=f.source_type, logre=f.logre, ee1=f.ee1,
                                ee2=f.ee2, sersic_n=f.sersic_n, free_n_all=fn,
-                               pos_max_shift_pix=5.0, pad=PAD) for p in plans]
+                               pos_max_shift_pix=5.0, pad=PAD, **pri) for p in plans]
     psfs = f.mog_psfs if mode == "analytic" else f.poly_psfs
     return plans, hosts, PAD, ds, ws, psfs
 
@@ -35,7 +44,7 @@ def field_classes(f, mode: str, kinds=("star", "mixed")):
 def run_gpu(plans, hosts, PAD, ds, ws, psfs, mode, max_steps=30, field=None,
             native=0, precision="plain", tc_min_rows=-1, tc_cond_max=-1.0,
             bg_mode="frozen", stall_count_mode="proposals", convergence="legacy",
-            step_mode="clip"):
+            step_mode="clip", param_errors=False):
     from uniphot_b200 import solver
     if field is None:
         field = solver.DeviceField(ds, ws, PAD)
@@ -51,13 +60,15 @@ def run_gpu(plans, hosts, PAD, ds, ws, psfs, mode, max_steps=30, field=None,
             convergence=convergence, step_mode=step_mode)
         rows = np.arange(plan.n_islands)
         outs.append(solver.run_class_chunk(kern, tree, host, rows, rows.size,
-                                           max_steps, field, field, PAD))
+                                           max_steps, field, field, PAD,
+                                           compute_param_errors=param_errors))
     return outs, field
 
 
 def run_oracle(plans, hosts, PAD, ds, ws, psfs, mode, precision="ref",
                max_steps=30, processes=1, native=0, bg_joint=False,
-               stall_count_mode="proposals", convergence="legacy", step_mode="clip"):
+               stall_count_mode="proposals", convergence="legacy", step_mode="clip",
+               param_errors=False):
     """The oracle over every class (star classes keep the clip step, as the
     reference exempts them from the trust region)."""
     from oracle.driver import solve_chunk
@@ -66,7 +77,8 @@ def run_oracle(plans, hosts, PAD, ds, ws, psfs, mode, precision="ref",
                         precision=precision, max_steps=max_steps, processes=processes,
                         native=native, bg_joint=bg_joint,
                         stall_count_mode=stall_count_mode, convergence=convergence,
-                        step_mode=step_mode if p.kind != "star" else "clip")
+                        step_mode=step_mode if p.kind != "star" else "clip",
+                        param_errors=param_errors)
             for p, h in zip(plans, hosts)]
 
 

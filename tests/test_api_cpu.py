@@ -58,7 +58,7 @@ def test_run_class_chunk_rejects_post_convergence_options():
     k = solver.make_class_kernels(_plan(), 3, 1, **KW)
     with pytest.raises(ValueError):
         solver.run_class_chunk(k, None, {}, np.arange(1), 1, 30, None, None, 10,
-                               compute_param_errors=True)
+                               compute_source_metrics=True)
 
 
 def test_psf_tree_padding_keeps_centre():
@@ -76,3 +76,43 @@ def test_trust_region_sets_the_descriptor_except_on_star_classes():
     assert k.desc.step_tr == 1 and k.step_mode == "trust_region"
     k = solver.make_class_kernels(_plan("star"), 3, 1, **KW, step_mode="trust_region")
     assert k.desc.step_tr == 0 and k.step_mode == "clip"
+
+
+def test_catalog_errors_propagate_to_the_catalog_frame():
+    """Variances -> catalog-frame errors (island_plan.py:796-885): Re scales
+    by exp(logre), ELL and THETA take the exact 2x2 quadratic forms with the
+    ee1-ee2 covariance, Sersic n scales by dn/du on free-n members; non-kept
+    slots and non-positive variances read NaN."""
+    from uniphot_b200.plan import SERSIC_N_MAX, SERSIC_N_MIN, catalog_errors
+    res_p = np.zeros((1, 2, 6), np.float32)
+    res_p[0, 0] = [10, 12, np.log(3.0), 0.3, -0.4, 0.0]
+    perr = np.zeros((1, 2, 13), np.float32)
+    perr[0, 0, :7] = [0.04, 0.09, 0.01, 0.02, 0.03, 0.25, 0.005]
+    perr[0, 0, 7:] = [0.5, 0.5, 0.2, 0.1, 0.3, 0.0]
+    perr[0, 1, :6] = [-1.0, 0.0, 1.0, 1.0, 1.0, 1.0]
+    keep = np.zeros((1, 2, 6), bool)
+    keep[0, 0] = True
+    keep[0, 1, :2] = True
+    pinv = np.zeros((1, 2, 6), np.float32)
+    pinv[0, 0, :5] = 1.0
+    host = dict(keep=keep, fn_flag=np.array([[True, False]]), prior_inv_sigma=pinv)
+    nfin = np.array([[2.0, 1.0]], np.float32)
+    e = catalog_errors(res_p, perr, host, np.array([0, 0]), np.array([0, 1]), nfin)
+    np.testing.assert_allclose(e["pos_x_err"][0], 0.2, rtol=1e-6)
+    np.testing.assert_allclose(e["re_err"][0], 3.0 * 0.1, rtol=1e-6)
+    e1, e2, v1, v2, c = 0.3, -0.4, 0.02, 0.03, 0.005
+    r = np.hypot(e1, e2)
+    q = np.exp(-r)
+    g = 2 * q / (2 - q) ** 2 * np.array([e1, e2]) / r
+    S = np.array([[v1, c], [c, v2]])
+    np.testing.assert_allclose(e["ell_err"][0], np.sqrt(g @ S @ g), rtol=1e-5)
+    gt = (90 / np.pi) * np.array([e2, -e1]) / r ** 2
+    np.testing.assert_allclose(e["theta_err"][0], np.sqrt(gt @ S @ gt), rtol=1e-5)
+    dndu = (2.0 - SERSIC_N_MIN) * (SERSIC_N_MAX - 2.0) / (SERSIC_N_MAX - SERSIC_N_MIN)
+    np.testing.assert_allclose(e["sersic_n_err"][0], 0.5 * dndu, rtol=1e-6)
+    assert np.isnan(e["pos_x_err"][1]) and np.isnan(e["pos_y_err"][1])
+    assert np.isnan(e["re_err"][1]) and np.isnan(e["sersic_n_err"][1])
+    np.testing.assert_allclose(e["pos_x_prior_frac"][0], 0.5)
+    np.testing.assert_allclose(e["ell_prior_frac"][0], (e1**2 * 0.1 + e2**2 * 0.3) / r**2,
+                               rtol=1e-6)
+    assert np.isnan(e["sersic_n_prior_frac"][0]) and np.isnan(e["pos_x_prior_frac"][1])

@@ -362,3 +362,101 @@ def test_trust_region_railed_flags_a_pinned_bound():
     assert out["railed"]
     out = O.solve_island(isl, O.SolverConfig(precision="ref"), max_steps=30)
     assert not out["railed"]      # clip mode reports none
+
+
+def test_final_errors_of_a_star_match_the_projected_fisher_matrix():
+    """Known answer for the covariance (island_solver.py:1484-1547): for a
+    noise-free isolated star the (x, y) block is the inverse of
+    sum_b w f_b^2 (D^T D - D^T m (m^T m)^-1 m^T D), D the unit model's
+    position derivatives (flux marginalised by the projection)."""
+    isl, flux = _mini_island("analytic", n_src=1, gal=False, noise=False)
+    s = O.IslandSolver(isl, O.SolverConfig(precision="f64"))
+    p = isl.p0.astype(np.float64)
+    pe = s.final_errors(p)
+    F = np.zeros((2, 2))
+    for b in range(isl.data.shape[0]):
+        m = s.models_band(b, p, False)[0][0].astype(np.float64).reshape(-1)
+        D = []
+        for j in range(2):
+            h = 1e-4
+            q1, q2 = p.copy(), p.copy()
+            q1[j] += h
+            q2[j] -= h
+            D.append((s.models_band(b, q1, False)[0][0].astype(np.float64)
+                      - s.models_band(b, q2, False)[0][0].astype(np.float64)).reshape(-1)
+                     / (2 * h))
+        D = np.array(D).T
+        w = float(isl.w[b, 0, 0])
+        P = D.T @ D - np.outer(D.T @ m, D.T @ m) / (m @ m)
+        F += w * flux[b, 0] ** 2 * P
+    np.testing.assert_allclose(pe[0, :2], np.diag(np.linalg.inv(F)), rtol=1e-4)
+    np.testing.assert_array_equal(pe[0, 2:6], 1.0)     # frozen slots: unit rows
+    assert pe[0, 6] == 0.0 and np.all(np.isnan(pe[0, 7:]))
+
+
+def test_flux_sensitivities_match_finite_differences():
+    """The Golub-Pereyra flux sensitivities c_j = A^-1 (e_k s_j - f_k u_j)
+    that the Jacobian assembly and the marginalised flux error use are the
+    derivatives of the flux solution (island_solver.py:570-590, 1549-1613)."""
+    isl, _ = _mini_island("analytic", n_src=2, seed=6)
+    s = O.IslandSolver(isl, O.SolverConfig(precision="f64"))
+    p = isl.p0.astype(np.float64)
+    fj = {}
+    s.hg(p, fj)
+    for b, (idx, C) in fj.items():
+        for r, q in enumerate(idx):
+            h = 1e-5
+            q1, q2 = p.copy(), p.copy()
+            q1[q] += h
+            q2[q] -= h
+            f1 = s.fluxes_band(s.models_band(b, q1, False)[0], isl.data[b], isl.w[b])[1]
+            f2 = s.fluxes_band(s.models_band(b, q2, False)[0], isl.data[b], isl.w[b])[1]
+            fd = (f1 - f2) / (2 * h)
+            np.testing.assert_allclose(C[r], fd, rtol=2e-4, atol=1e-6 * np.abs(fd).max())
+
+
+def test_flux_marg_is_zero_for_stars_and_the_quadratic_form_for_galaxies():
+    isl, _ = _mini_island("analytic", n_src=2, seed=6)      # member 1 is a galaxy
+    s = O.IslandSolver(isl, O.SolverConfig(precision="f64"))
+    p = isl.p0.astype(np.float64)
+    dv = s.final_flux_marg(p)
+    assert dv.shape == (2, 2) and np.all(dv[:, 0] == 0.0) and np.all(dv[:, 1] > 0)
+    fj = {}
+    _, keep, Hm, _ = s._posterior(p, fj)
+    S = np.linalg.inv(Hm.astype(np.float64))
+    idx, C = fj[0]
+    cols = [r for r, q in enumerate(idx) if q >= 6]          # the galaxy's parameters
+    J = C[cols, 1]
+    q = idx[cols]
+    np.testing.assert_allclose(dv[0, 1], J @ S[np.ix_(q, q)] @ J, rtol=1e-5)
+
+
+def test_source_metrics_known_answers():
+    """Source metrics (island_solver.py:1639-1715): an isolated noise-free
+    star has no neighbour light, no masked flux and zero chi2; masking a
+    half-plane gives the unit model's flux there; a blend's fracflux is the
+    neighbour's light under the member's profile."""
+    isl, flux = _mini_island("analytic", n_src=1, gal=False, noise=False)
+    s = O.IslandSolver(isl, O.SolverConfig(precision="f64"))
+    p = isl.p0.astype(np.float64)
+    met, fwin = s.source_metrics(p)
+    m = s.models_band(0, p, False)[0][0].astype(np.float64)
+    assert met[0, 1] == 0.0 and met[0, 3] == 0.0 and abs(met[0, 0]) < 1e-6
+    np.testing.assert_allclose(met[0, 2], m.sum(), rtol=1e-6)
+    np.testing.assert_allclose(fwin[:, 0], flux[:, 0] * m.sum(), rtol=1e-4)
+    isl.w[:, :, :16] = 0.0
+    met, _ = s.source_metrics(p)
+    np.testing.assert_allclose(met[0, 3], m[:, :16].sum() / 1.0, rtol=1e-4)
+    isl2, flux2 = _mini_island("analytic", n_src=2, gal=False, noise=False, seed=7)
+    s2 = O.IslandSolver(isl2, O.SolverConfig(precision="f64"))
+    p2 = isl2.p0.astype(np.float64)
+    met2, _ = s2.source_metrics(p2)
+    num = den = 0.0
+    for b in range(2):
+        M = s2.models_band(b, p2, False)[0].astype(np.float64)
+        f = s2.fluxes_band(M, isl2.data[b], isl2.w[b])[0].astype(np.float64)
+        own, other = f[0] * M[0], f[1] * M[1]
+        fin = min(max(M[0].sum(), 0.0), 1.0)
+        num += fin * (other * own).sum() / (own * own).sum()
+        den += fin
+    np.testing.assert_allclose(met2[0, 1], num / den, rtol=1e-5)

@@ -42,7 +42,9 @@ class ClassDesc(C.Structure):
                 ("precision", C.c_int32), ("tc_min_rows", C.c_int32),
                 ("stall_changed", C.c_int32), ("convergence_dlnp", C.c_int32),
                 ("plateau_dlnp_tol", C.c_float), ("bg_joint", C.c_int32),
-                ("tc_cond_max", C.c_float), ("step_tr", C.c_int32)]
+                ("tc_cond_max", C.c_float), ("step_tr", C.c_int32),
+                ("param_errors", C.c_int32), ("flux_marg", C.c_int32),
+                ("source_metrics", C.c_int32)]
 
 
 class ChunkIn(C.Structure):
@@ -58,7 +60,8 @@ class ChunkOut(C.Structure):
         "p", "fluxes", "ferr", "chi2", "conv", "stall", "diverged",
         "stall_dchi2", "nst", "lam", "consec", "nrej", "n_good")] + \
         [("steps_run", C.c_int32), ("bg", _P), ("bg_err", _P), ("n_same", _P),
-         ("prej", _P), ("railed", _P)]
+         ("prej", _P), ("railed", _P), ("perr", _P), ("femarg", _P),
+         ("smetrics", _P), ("swin", _P)]
 
 
 class UphError(RuntimeError):
@@ -274,7 +277,9 @@ def chunk_out(n: int, N: int, nb: int):
                nrej=np.zeros(n, np.int32), n_good=np.zeros(n, np.int64),
                bg=np.zeros((n, nb, 3), np.float32), bg_err=np.zeros((n, nb, 3), np.float32),
                n_same=np.zeros(n, np.int32), prej=np.zeros((n, 6 * N), np.float32),
-               railed=np.zeros(n, np.uint8))
+               railed=np.zeros(n, np.uint8), perr=np.zeros((n, N, 13), np.float32),
+               femarg=np.zeros((n, nb, N), np.float32),
+               smetrics=np.zeros((n, N, 4), np.float32), swin=np.zeros((n, nb, N), np.float32))
     cout = ChunkOut()
     for k, v in out.items():
         setattr(cout, k, ptr(v))

@@ -394,6 +394,8 @@ struct Chunk {
   float* d_p0 = nullptr;
   uint8_t* d_div = nullptr;
   uint8_t* d_rail = nullptr;       // trust region: bound-pinned islands
+  float* d_cjac = nullptr;         // flux sensitivities (flux_marg only)
+  bool perr_out = false;           // param_errors requested
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t gexec = nullptr;
   cudaEvent_t ev_group = nullptr;
@@ -688,6 +690,21 @@ int add_chunk(uph_ctx* ctx, Chunk* ch, const uph_class_desc* cls,
     c.trs = cbuf<double>(ctx, ch, "trs", (size_t)n * 4, &rc);
     ch->d_rail = cbuf<uint8_t>(ctx, ch, "railed", n, &rc);
   }
+  if (cls->param_errors || cls->flux_marg) {
+    c.perr = cbuf<float>(ctx, ch, "perr", (size_t)n * N * 13, &rc);
+    c.ews = cbuf<double>(ctx, ch, "ews", (size_t)n * nLmax * 2 * nLmax, &rc);
+    c.flsave = cbuf<uint8_t>(ctx, ch, "flsave", n, &rc);
+  }
+  if (cls->flux_marg) {
+    ch->d_cjac = cbuf<float>(ctx, ch, "cjac", (size_t)n * nb * nLmax * UPH_MAXLIN, &rc);
+    c.femarg = cbuf<float>(ctx, ch, "femarg", (size_t)n * nb * N, &rc);
+  }
+  ch->perr_out = cls->param_errors != 0;
+  if (cls->source_metrics) {
+    c.smom = cbuf<double>(ctx, ch, "smom", (size_t)n * nb * N * 5, &rc);
+    c.smet = cbuf<float>(ctx, ch, "smet", (size_t)n * N * 4, &rc);
+    c.swin = cbuf<float>(ctx, ch, "swin", (size_t)n * nb * N, &rc);
+  }
   if (c.changed) {
     c.n_same = cbuf<int>(ctx, ch, "nsame", n, &rc);
     c.prej = cbuf<float>(ctx, ch, "prej", (size_t)n * nP, &rc);
@@ -812,6 +829,24 @@ void post_loop(Chunk* ch, Launcher& L) {
     launch_railed(c, ch->d_rail, s);
     L.job->ctx->launches += 1;
   }
+  if (c.perr) {
+    // covariance at the final parameters: one more linearisation of every
+    // island, then the float64 inversion
+    // (the assembly also keeps the flux sensitivities when the
+    // marginalised flux variance is wanted)
+    ClassDev ce = c;
+    ce.cjac = ch->d_cjac;
+    launch_errors_begin(c, s);
+    L(0, [&] { launch_render(c, c.p, PH_LIN, s); }, 2);
+    L(1, [&] { launch_gram_lin(c, s); });
+    if (c.tc_min_rows < (1 << 30))
+      L(WK_GRAM_TC, [&] { launch_gram_tc(c, s); }, c.tc_split > 1 ? 2 : 1);
+    L(2, [&] { launch_assemble(ce, s); });
+    L(3, [&] { launch_final_errors(c, s); });
+    if (c.femarg) L(3, [&] { launch_flux_marg(ce, s); });
+    launch_errors_end(c, s);
+    L.job->ctx->launches += 2;
+  }
   launch_fill_float(c.probe_best, INFINITY, c.n_isl, s);
   L.job->ctx->launches += 1;
   for (int e = -9; e <= 6; ++e) {
@@ -823,6 +858,8 @@ void post_loop(Chunk* ch, Launcher& L) {
   }
   L(0, [&] { launch_render(c, c.p, PH_ALL, s); }, 2);
   L(4, [&] { launch_gram_trial(c, c.p, PH_ALL, 1, nullptr, nullptr, s); });
+  // source metrics read the final pass's model rows and fluxes
+  if (c.smet) L(4, [&] { launch_source_metrics(c, s); }, 2);
 }
 
 int job_solve(uph_job* job, int max_steps) {
@@ -1058,6 +1095,36 @@ int job_read(uph_job* job, int id, uph_chunk_out* out) {
   if ((rc = download(ctx, out->consec, c.consec, sizeof(int) * n, "consec"))) return rc;
   if ((rc = download(ctx, out->nrej, c.nrej, sizeof(int) * n, "nrej"))) return rc;
   if ((rc = download(ctx, out->diverged, ch->d_div, n, "diverged"))) return rc;
+  if (out->smetrics) {
+    if (c.smet) {
+      if ((rc = download(ctx, out->smetrics, c.smet, sizeof(float) * n * N * 4, "smetrics")))
+        return rc;
+    } else {
+      for (size_t e = 0; e < (size_t)n * N * 4; ++e) out->smetrics[e] = NAN;
+    }
+  }
+  if (out->swin) {
+    if (c.swin) {
+      if ((rc = download(ctx, out->swin, c.swin, sizeof(float) * n * nb * N, "swin"))) return rc;
+    } else {
+      for (size_t e = 0; e < (size_t)n * nb * N; ++e) out->swin[e] = NAN;
+    }
+  }
+  if (out->femarg) {
+    if (c.femarg) {
+      if ((rc = download(ctx, out->femarg, c.femarg, sizeof(float) * n * nb * N, "femarg")))
+        return rc;
+    } else {
+      for (size_t e = 0; e < (size_t)n * nb * N; ++e) out->femarg[e] = NAN;
+    }
+  }
+  if (out->perr) {
+    if (c.perr && ch->perr_out) {
+      if ((rc = download(ctx, out->perr, c.perr, sizeof(float) * n * N * 13, "perr"))) return rc;
+    } else {
+      for (size_t e = 0; e < (size_t)n * N * 13; ++e) out->perr[e] = NAN;
+    }
+  }
   if (out->railed) {
     if (c.tr) {
       if ((rc = download(ctx, out->railed, ch->d_rail, n, "railed"))) return rc;

@@ -143,6 +143,23 @@ struct ClassDev {
   // in trs for k_accept's radius update
   int tr;
   double* trs;             // (n_isl, 4)
+  // marginal covariance at the final parameters (param_errors): output
+  // (n_isl, N, 13), float64 work space for the inversion (n_isl, nLmax,
+  // 2 nLmax) and the flags saved around the relinearisation
+  float* perr;
+  double* ews;
+  uint8_t* flsave;
+  // shape-marginalised flux variance (flux_marg): the flux sensitivities
+  // d f / d theta of the relinearisation, (n_isl, nb, nLmax, UPH_MAXLIN),
+  // written by k_assemble only when non-null, and the output (n_isl, nb, N)
+  float* cjac;
+  float* femarg;
+  // source metrics (source_metrics): per (island, band, member) moments
+  // (n_isl, nb, N, 5), combined metrics (n_isl, N, 4), window fluxes
+  // (n_isl, nb, N)
+  double* smom;
+  float* smet;
+  float* swin;
   float* bgout;            // (n_isl, nb, 3) final background coefficients
   float* bgerr;            // (n_isl, nb, 3) and their errors
   float* fcur;
@@ -288,6 +305,11 @@ void launch_count_active(const ClassDev& c, cudaStream_t s);
 void launch_diverged_compare(const ClassDev& c, uint8_t* out,
                              cudaStream_t s);
 void launch_railed(const ClassDev& c, uint8_t* out, cudaStream_t s);
+void launch_errors_begin(const ClassDev& c, cudaStream_t s);
+void launch_final_errors(const ClassDev& c, cudaStream_t s);
+void launch_flux_marg(const ClassDev& c, cudaStream_t s);
+void launch_source_metrics(const ClassDev& c, cudaStream_t s);
+void launch_errors_end(const ClassDev& c, cudaStream_t s);
 size_t render_smem_bytes();
 size_t gram_lin_smem_bytes(int Kmax);
 size_t gram_trial_smem_bytes(int N);

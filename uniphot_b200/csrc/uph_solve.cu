@@ -592,6 +592,14 @@ __global__ void __launch_bounds__(NT) k_assemble(ClassDev c) {
     }
   }
   __syncthreads();
+  if (c.cjac) {
+    // the flux sensitivities of this band, for the marginalised flux error
+    float* cj = c.cjac + ((size_t)isl * c.nb + b) * c.nLmax * UPH_MAXLIN;
+    for (int e = tid; e < nL * nl; e += NT) {
+      const int j = e / nl, l = e - (e / nl) * nl;
+      cj[(size_t)j * UPH_MAXLIN + l] = (float)Cm[j * LS + l];
+    }
+  }
   // W_j = A c_j + a_j DM_j
   for (int e = tid; e < nL * nl; e += NT) {
     const int j = e / nl, l = e - (e / nl) * nl;
@@ -1276,6 +1284,228 @@ __global__ void k_railed(ClassDev c, uint8_t* out) {
   out[isl] = r ? 1 : 0;
 }
 
+// Relinearisation at the final parameters for the covariance: every
+// island's flags are saved, then set so that the linearisation kernels
+// (render, Gram, assembly) run on it; k_errors_end puts them back.
+__global__ void k_errors_begin(ClassDev c) {
+  const int isl = blockIdx.x * blockDim.x + threadIdx.x;
+  if (isl >= c.n_isl) return;
+  const uint8_t fl = c.flags[isl];
+  c.flsave[isl] = fl;
+  c.flags[isl] = (uint8_t)(FL_NEEDLIN | (fl & FL_REAL));
+}
+
+__global__ void k_errors_end(ClassDev c) {
+  const int isl = blockIdx.x * blockDim.x + threadIdx.x;
+  if (isl >= c.n_isl) return;
+  c.flags[isl] = c.flsave[isl];
+}
+
+// Marginal covariance of the nonlinear parameters (island_solver.py:
+// 1484-1547) for one island: H = sum over bands of the per-band Gauss-Newton
+// blocks (float, band order as the step), the static keep mask (every live
+// row; no annealing), plus the prior diagonal, inverted in float64 by
+// Gauss-Jordan on [Hm | I].  Rows outside the live set are unit rows of the
+// full matrix, so their variance is 1 and their covariances 0.  Output per
+// member: var(x, y, logre, ee1, ee2, u), cov(ee1, ee2), then the prior
+// fractions pinv^2 / (H_kk + pinv^2) on the data diagonal (0 where that sum
+// is 0, NaN for every slot without priors).
+__global__ void __launch_bounds__(NT) k_final_errors(ClassDev c) {
+  __shared__ double fac[UPH_MAXLIVE];
+  __shared__ float hdiag[UPH_MAXLIVE];
+  __shared__ int16_t qlive[6 * UPH_MAXN];
+  __shared__ int piv;
+  const int isl = blockIdx.x;
+  if (isl >= c.n_isl) return;
+  const int tid = threadIdx.x;
+  const int nL = c.isl_nL[isl];
+  const int nP = c.nP;
+  const int ldH = c.nLmax;
+  const int ld = 2 * c.nLmax;
+  const int16_t* rp = c.row_p + (size_t)isl * c.Kmax;
+  const float* pinv = c.prior_inv + (size_t)isl * nP;
+  double* A = c.ews + (size_t)isl * c.nLmax * ld;
+  for (int q = tid; q < nP; q += NT) qlive[q] = -1;
+  __syncthreads();
+  for (int i = tid; i < nL; i += NT) qlive[rp[i]] = (int16_t)i;
+  for (int e = tid; e < nL * nL; e += NT) {
+    const int i = e / nL, j = e - (e / nL) * nL;
+    float h = 0.f;
+    for (int b = 0; b < c.nb; ++b)
+      h += c.Hb[((size_t)isl * c.nb + b) * ldH * ldH + i * ldH + j];
+    if (i == j) {
+      hdiag[i] = h;
+      if (c.has_priors) h = __fadd_rn(h, __fmul_rn(pinv[rp[i]], pinv[rp[i]]));
+    }
+    A[i * ld + j] = (double)h;
+    A[i * ld + nL + j] = (i == j) ? 1.0 : 0.0;
+  }
+  __syncthreads();
+  if (nL > 0) gauss_jordan(A, nL, 2 * nL, ld, fac, &piv);
+  float* out = c.perr + (size_t)isl * c.N * 13;
+  for (int e = tid; e < c.N * 13; e += NT) {
+    const int k = e / 13, col = e - (e / 13) * 13;
+    float v;
+    if (col < 6) {
+      const int i = qlive[6 * k + col];
+      v = i >= 0 ? (float)A[i * ld + nL + i] : 1.f;
+    } else if (col == 6) {
+      const int i3 = qlive[6 * k + 3], i4 = qlive[6 * k + 4];
+      v = (i3 >= 0 && i4 >= 0) ? (float)A[i3 * ld + nL + i4] : 0.f;
+    } else if (!c.has_priors) {
+      v = NAN;
+    } else {
+      const int i = qlive[6 * k + col - 7];
+      const float pd = i >= 0 ? __fmul_rn(pinv[6 * k + col - 7], pinv[6 * k + col - 7]) : 0.f;
+      const float den = __fadd_rn(i >= 0 ? hdiag[i] : 0.f, pd);
+      v = den > 0.f ? __fdiv_rn(pd, den) : 0.f;
+    }
+    out[e] = v;
+  }
+}
+
+// Shape-marginalised flux-variance increment (island_solver.py:1549-1613)
+// for one island, after k_final_errors left Sigma = Hm^-1 in the right half
+// of its work space: per band b and extended member k,
+// dv = sum_ij J_ki Sigma_ij J_kj over the live parameters of extended
+// members, J_ki = d f_k / d theta_i from the relinearisation's assembly.
+// One warp per member; lanes over i with a fixed-order shuffle reduction.
+__global__ void __launch_bounds__(NT) k_flux_marg(ClassDev c) {
+  __shared__ uint8_t marg[UPH_MAXLIVE];
+  const int isl = blockIdx.x;
+  if (isl >= c.n_isl) return;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int nL = c.isl_nL[isl], nr = c.isl_nr[isl];
+  const int ld = 2 * c.nLmax;
+  const int16_t* rp = c.row_p + (size_t)isl * c.Kmax;
+  const double* A = c.ews + (size_t)isl * c.nLmax * ld;
+  for (int i = tid; i < nL; i += NT) marg[i] = c.stype[(size_t)isl * c.N + rp[i] / 6] != 0;
+  __syncthreads();
+  for (int e = warp; e < c.nb * c.N; e += NT / 32) {
+    const int b = e / c.N, k = e - (e / c.N) * c.N;
+    float* out = c.femarg + ((size_t)isl * c.nb + b) * c.N + k;
+    const bool ext = k < nr && c.stype[(size_t)isl * c.N + k] != 0;
+    if (!ext) {
+      if (lane == 0) *out = 0.f;
+      continue;
+    }
+    const float* J = c.cjac + ((size_t)isl * c.nb + b) * c.nLmax * UPH_MAXLIN;
+    double acc = 0.0;
+    for (int i = lane; i < nL; i += 32) {
+      if (!marg[i]) continue;
+      double t = 0.0;
+      for (int j = 0; j < nL; ++j)
+        if (marg[j]) t += A[i * ld + nL + j] * (double)J[(size_t)j * UPH_MAXLIN + k];
+      acc += (double)J[(size_t)i * UPH_MAXLIN + k] * t;
+    }
+    for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+    if (lane == 0) *out = (float)fmax(acc, 0.0);
+  }
+}
+
+// Source-metric moments of one (island, band) at the final parameters
+// (island_solver.py:1639-1715), from the final pass's model rows and
+// fluxes: per member k over its stamp box, sum m, sum own^2, sum
+// (members' model - own) own, sum m [w == 0], sum m w (d - model)^2, with
+// own = f_k m and the model including the background plane when it is
+// solved.  Double accumulation, fixed-order block reduction.
+template <bool BG>
+__global__ void __launch_bounds__(NT) k_source_metrics(ClassDev c) {
+  __shared__ int4 box[UPH_MAXN];
+  __shared__ float fl[UPH_MAXLIN];
+  __shared__ double red[5][NT / 32];
+  const int isl = blockIdx.x / c.nb, b = blockIdx.x % c.nb;
+  if (isl >= c.n_isl) return;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int nr = c.isl_nr[isl];
+  const int B = c.B, Sz = c.Sz;
+  load_boxes(c, isl, c.p, box);
+  for (int k = tid; k < nr; k += NT) fl[k] = c.flux[((size_t)isl * c.nb + b) * c.N + k];
+  if (BG)
+    for (int j = tid; j < c.nbg; j += NT)
+      fl[nr + j] = c.bgout[((size_t)isl * c.nb + b) * UPH_MAXBG + j];
+  __syncthreads();
+  const size_t plane = (size_t)c.Hp * c.Wp;
+  const float* dbase = c.dstack + b * plane + (size_t)c.oy[isl] * c.Wp + c.ox[isl];
+  const float* wbase = c.wstack + b * plane + (size_t)c.oy[isl] * c.Wp + c.ox[isl];
+  double* out = c.smom + ((size_t)isl * c.nb + b) * c.N * 5;
+  for (int k = 0; k < c.N; ++k) {
+    double a[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    const int4 bk = k < nr ? box[k] : make_int4(0, 0, 0, 0);
+    const int npx = max(bk.z, 0) * max(bk.w, 0);
+    for (int e = tid; e < npx; e += NT) {
+      const int ly = e / bk.z, lx = e - (e / bk.z) * bk.z;
+      const int wy = bk.y + ly, wx = bk.x + lx;
+      const float m = c.stamps[stamp_slot(c, isl, b, k, 0) + (size_t)ly * Sz + lx];
+      float model = 0.f;
+      for (int l = 0; l < nr; ++l) {
+        const int4 bx = box[l];
+        const int yy = wy - bx.y, xx = wx - bx.x;
+        if (yy >= 0 && yy < bx.w && xx >= 0 && xx < bx.z)
+          model = fmaf(fl[l], c.stamps[stamp_slot(c, isl, b, l, 0) + (size_t)yy * Sz + xx], model);
+      }
+      float full = model;
+      if (BG)
+        for (int j = 0; j < c.nbg; ++j) full = fmaf(fl[nr + j], bg_basis(j, wy, wx, B), full);
+      const float w = wbase[(size_t)wy * c.Wp + wx];
+      const float d = dbase[(size_t)wy * c.Wp + wx];
+      const float own = fl[k] * m;
+      const float r = d - full;
+      a[0] += (double)m;
+      a[1] += (double)own * (double)own;
+      a[2] += (double)(model - own) * (double)own;
+      a[3] += (w == 0.f) ? (double)m : 0.0;
+      a[4] += (double)m * (double)w * (double)r * (double)r;
+    }
+    for (int q = 0; q < 5; ++q) {
+      double v = a[q];
+      for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+      if (lane == 0) red[q][warp] = v;
+    }
+    __syncthreads();
+    if (tid < 5) {
+      double t = 0.0;
+      for (int w = 0; w < NT / 32; ++w) t += red[tid][w];
+      out[k * 5 + tid] = t;
+    }
+    __syncthreads();
+  }
+}
+
+// Band combination of the source metrics (island_solver.py:1691-1715), in
+// float32 as the reference: fin = clip(sum m, 0, 1) weights fracflux and
+// fracmasked; fracin and rchisq are ratios of band sums; the window flux
+// f * sum m per band.  Padded slots: NaN (rchisq, fracin, window flux), 0.
+__global__ void k_metrics_combine(ClassDev c) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= c.n_isl * c.N) return;
+  const int isl = e / c.N, k = e - (e / c.N) * c.N;
+  const bool mm = c.mmask[(size_t)isl * c.N + k] != 0;
+  float ffn = 0.f, ffd = 0.f, finn = 0.f, find = 0.f, fmn = 0.f, fmd = 0.f, rcn = 0.f, rcd = 0.f;
+  for (int b = 0; b < c.nb; ++b) {
+    const double* m = c.smom + (((size_t)isl * c.nb + b) * c.N + k) * 5;
+    const float sm = (float)m[0], bot = (float)m[1], top = (float)m[2];
+    const float fin = fminf(fmaxf(sm, 0.f), 1.f);
+    const float ratio = bot > 0.f ? __fdiv_rn(top, bot) : 0.f;
+    const float fm = fminf(fmaxf((float)m[3], 0.f), 1.f);
+    ffn = __fadd_rn(ffn, __fmul_rn(fin, ratio));
+    ffd = __fadd_rn(ffd, fin);
+    finn = __fadd_rn(finn, fabsf(sm));
+    find = __fadd_rn(find, 1.f);
+    fmn = __fadd_rn(fmn, __fmul_rn(fin, fm));
+    fmd = __fadd_rn(fmd, fin);
+    rcn = __fadd_rn(rcn, fabsf((float)m[4]));
+    rcd = __fadd_rn(rcd, fabsf(sm));
+    const float f = c.flux[((size_t)isl * c.nb + b) * c.N + k];
+    c.swin[((size_t)isl * c.nb + b) * c.N + k] = mm ? __fmul_rn(f, sm) : NAN;
+  }
+  float* o = c.smet + ((size_t)isl * c.N + k) * 4;
+  o[0] = (mm && rcd > 0.f) ? __fdiv_rn(rcn, rcd) : NAN;
+  o[1] = (mm && ffd > 0.f) ? __fdiv_rn(ffn, ffd) : 0.f;
+  o[2] = (mm && find > 0.f) ? __fdiv_rn(finn, find) : NAN;
+  o[3] = (mm && fmd > 0.f) ? __fdiv_rn(fmn, fmd) : 0.f;
+}
+
 __global__ void k_set_probe(ClassDev c) {
   const int isl = blockIdx.x * blockDim.x + threadIdx.x;
   if (isl >= c.n_isl) return;
@@ -1296,6 +1526,30 @@ void launch_fill_float(float* p, float v, int n, cudaStream_t s) {
 
 void launch_railed(const ClassDev& c, uint8_t* out, cudaStream_t s) {
   k_railed<<<(unsigned)((c.n_isl + 127) / 128), 128, 0, s>>>(c, out);
+}
+
+void launch_errors_begin(const ClassDev& c, cudaStream_t s) {
+  k_errors_begin<<<(unsigned)((c.n_isl + 127) / 128), 128, 0, s>>>(c);
+}
+
+void launch_errors_end(const ClassDev& c, cudaStream_t s) {
+  k_errors_end<<<(unsigned)((c.n_isl + 127) / 128), 128, 0, s>>>(c);
+}
+
+void launch_final_errors(const ClassDev& c, cudaStream_t s) {
+  k_final_errors<<<(unsigned)c.n_isl, NT, 0, s>>>(c);
+}
+
+void launch_flux_marg(const ClassDev& c, cudaStream_t s) {
+  k_flux_marg<<<(unsigned)c.n_isl, NT, 0, s>>>(c);
+}
+
+void launch_source_metrics(const ClassDev& c, cudaStream_t s) {
+  if (c.nbg)
+    k_source_metrics<true><<<(unsigned)(c.n_isl * c.nb), NT, 0, s>>>(c);
+  else
+    k_source_metrics<false><<<(unsigned)(c.n_isl * c.nb), NT, 0, s>>>(c);
+  k_metrics_combine<<<(unsigned)((c.n_isl * c.N + 127) / 128), 128, 0, s>>>(c);
 }
 
 void launch_set_probe(const ClassDev& c, cudaStream_t s) {

@@ -318,16 +318,82 @@ def _nan(n):
     return np.full(n, np.nan, np.float32)
 
 
+def catalog_errors(res_p, res_perr, host, ii, kk, n_final) -> dict:
+    """Catalog-frame 1-sigma errors and prior fractions of the members
+    (ii, kk) from the per-member covariance rows of ``res_perr`` (n_isl, N,
+    13): var(x, y, logre, ee1, ee2, u), cov(ee1, ee2), six prior fractions
+    (island_plan.py:796-885).
+
+    Non-kept slots and degenerate variances (non-finite or <= 0) give NaN.
+    Re = exp(logre) scales its error by Re; ELL = 2e/(1+e) with e = 1 -
+    exp(-|ee|) and THETA = -atan2(ee2, ee1)/2 in degrees take the exact
+    2x2 quadratic forms of their gradients in (ee1, ee2) with the ee1-ee2
+    covariance (undefined at |ee| = 0: NaN); Sersic n = n(u) scales by
+    dn/du = (n - n_min)(n_max - n)/(n_max - n_min) on free-n members.  The
+    ELL / THETA prior fractions weight the ee1 / ee2 fractions radially
+    (ee1^2, ee2^2) and tangentially (ee2^2, ee1^2) over |ee|^2; a fraction
+    is NaN where its parameter carries no prior or is not fitted."""
+    keep = host["keep"][ii, kk, :]
+    var = res_perr[ii, kk, :6].astype(np.float64)
+    cov = res_perr[ii, kk, 6].astype(np.float64)
+    ok = keep & np.isfinite(var) & (var > 0)
+    sig = np.sqrt(np.where(ok, var, 1.0))
+    sig = np.where(ok, sig, np.nan)
+    e1 = res_p[ii, kk, 3].astype(np.float64)
+    e2 = res_p[ii, kk, 4].astype(np.float64)
+    r2 = e1 * e1 + e2 * e2
+    r = np.sqrt(r2)
+    rs = np.where(r > 0, r, 1.0)
+    radial = (e1 * e1 * var[:, 3] + 2.0 * e1 * e2 * cov + e2 * e2 * var[:, 4]) / (rs * rs)
+    tangential = (e2 * e2 * var[:, 3] - 2.0 * e1 * e2 * cov + e1 * e1 * var[:, 4]) / rs ** 4
+    q = np.exp(-r)
+    dell = 2.0 * q / (2.0 - q) ** 2
+    shape_ok = ok[:, 3] & ok[:, 4] & np.isfinite(cov) & (r > 0)
+
+    def root(v):
+        good = shape_ok & np.isfinite(v) & (v > 0)
+        return np.where(good, np.sqrt(np.where(good, v, 1.0)), np.nan)
+    nm = n_final[ii, kk].astype(np.float64)
+    dndu = (nm - SERSIC_N_MIN) * (SERSIC_N_MAX - nm) / (SERSIC_N_MAX - SERSIC_N_MIN)
+    fn = host["fn_flag"][ii, kk]
+    out = dict(
+        pos_x_err=sig[:, 0], pos_y_err=sig[:, 1],
+        re_err=np.exp(res_p[ii, kk, 2].astype(np.float64)) * sig[:, 2],
+        ell_err=root(dell * dell * radial),
+        theta_err=root((90.0 / np.pi) ** 2 * tangential),
+        sersic_n_err=np.where(fn, sig[:, 5] * np.abs(dndu), np.nan))
+    pf = res_perr[ii, kk, 7:13].astype(np.float64)
+    has = host["prior_inv_sigma"][ii, kk, :] > 0
+
+    def frac(j):
+        return np.where(keep[:, j] & has[:, j], pf[:, j], np.nan)
+    both = keep[:, 3] & keep[:, 4] & has[:, 3] & has[:, 4] & (r2 > 0)
+    r2s = np.where(r2 > 0, r2, 1.0)
+    out.update(
+        pos_x_prior_frac=frac(0), pos_y_prior_frac=frac(1), re_prior_frac=frac(2),
+        ell_prior_frac=np.where(both, (e1 * e1 * pf[:, 3] + e2 * e2 * pf[:, 4]) / r2s,
+                                np.nan),
+        theta_prior_frac=np.where(both, (e2 * e2 * pf[:, 3] + e1 * e1 * pf[:, 4]) / r2s,
+                                  np.nan),
+        sersic_n_prior_frac=np.where(fn & has[:, 5], pf[:, 5], np.nan))
+    return {k: np.asarray(v, np.float32) for k, v in out.items()}
+
+
 def unpack_class_results(plan, host, island_set, res_p, res_f, res_fe,
                          res_chi2, res_conv, res_stall, res_nst,
                          res_perr=None, res_pdchi2=None, res_div=None,
                          res_ngood=None, n_bands=0, res_bg=None, res_bg_err=None,
-                         res_railed=None, **_unused) -> dict:
+                         res_railed=None, res_femarg=None, res_smetrics=None,
+                         res_swin=None, **_unused) -> dict:
     """Island rows -> source rows for the valid member slots.
 
-    Parameter-error, profile and metric columns are NaN here: their
-    kernels are not built (they are post-convergence options that are off by
-    default in ``island_fit``)."""
+    Parameter errors and prior fractions come from ``res_perr`` (the
+    device covariance pass, ``compute_param_errors``; NaN without it);
+    ``flux_marg_var`` from ``res_femarg`` (the shape-marginalised flux
+    variance increment, ``compute_flux_marg``), the source metrics and
+    window fluxes from ``res_smetrics`` / ``res_swin``
+    (``compute_source_metrics``); NaN without them.  The Re-profile
+    columns are NaN: that kernel is not built."""
     midx, mmask, is_ext = plan.midx, host["mmask"], host["is_ext"]
     fn = host["fn_flag"]
     ii, kk = np.nonzero(mmask)
@@ -346,6 +412,20 @@ def unpack_class_results(plan, host, island_set, res_p, res_f, res_fe,
     else:
         chi2_nu = _nan(n)
     nb = max(int(n_bands), 0)
+    if res_smetrics is not None:
+        mets = dict(rchisq=res_smetrics[ii, kk, 0], fracflux=res_smetrics[ii, kk, 1],
+                    fracin=res_smetrics[ii, kk, 2], fracmasked=res_smetrics[ii, kk, 3],
+                    flux_win=res_swin[ii, :, kk])
+    else:
+        mets = dict(rchisq=_nan(n), fracflux=_nan(n), fracin=_nan(n), fracmasked=_nan(n),
+                    flux_win=np.full((n, nb), np.nan, np.float32))
+    if res_perr is not None:
+        errs = catalog_errors(res_p, res_perr, host, ii, kk, nfin)
+    else:
+        errs = {k: _nan(n) for k in (
+            "pos_x_err", "pos_y_err", "re_err", "ell_err", "theta_err", "sersic_n_err",
+            "pos_x_prior_frac", "pos_y_prior_frac", "re_prior_frac", "ell_prior_frac",
+            "theta_prior_frac", "sersic_n_prior_frac")}
     return dict(
         src=midx[ii, kk],
         pos_x=res_p[ii, kk, 0], pos_y=res_p[ii, kk, 1],
@@ -364,14 +444,9 @@ def unpack_class_results(plan, host, island_set, res_p, res_f, res_fe,
         island_nsrc=island_set.n_src[plan.isl_ids][ii].astype(np.int32),
         island_giant=np.zeros(n, bool),
         re_upper_pix=np.exp(host["upper"][ii, kk, 2].astype(np.float64)).astype(np.float32),
-        pos_x_err=_nan(n), pos_y_err=_nan(n), re_err=_nan(n), ell_err=_nan(n),
-        theta_err=_nan(n), re_prof_lo=_nan(n), re_prof_hi=_nan(n),
-        sersic_n_err=_nan(n), pos_x_prior_frac=_nan(n), pos_y_prior_frac=_nan(n),
-        re_prior_frac=_nan(n), ell_prior_frac=_nan(n), theta_prior_frac=_nan(n),
-        sersic_n_prior_frac=_nan(n), rchisq=_nan(n), fracflux=_nan(n),
-        fracin=_nan(n), fracmasked=_nan(n),
-        flux_win=np.full((n, nb), np.nan, np.float32),
-        flux_marg_var=np.full((n, nb), np.nan, np.float32),
+        re_prof_lo=_nan(n), re_prof_hi=_nan(n), **errs, **mets,
+        flux_marg_var=(res_femarg[ii, :, kk].astype(np.float32) if res_femarg is not None
+                       else np.full((n, nb), np.nan, np.float32)),
         bg_plane=(res_bg[ii].astype(np.float32) if res_bg is not None
                   else np.zeros((n, nb, 3), np.float32)),
         bg_plane_err=(res_bg_err[ii].astype(np.float32) if res_bg_err is not None

@@ -22,8 +22,10 @@ Differences, by design:
   is run (``bucket_stats`` still reports the counts);
 * ``dstack_dev`` is a :class:`DeviceField` (the field stacks resident in
   HBM inside the library context); ``wstack_dev`` is accepted and ignored;
-* options whose kernels are not built (crossband GLS, scene subtract,
-  post-convergence error / metric / profile kernels) raise ``ValueError``;
+* options whose kernels are not built (crossband GLS, scene subtract, the
+  Re profile, the island residual) raise ``ValueError``;
+  ``compute_param_errors``, ``compute_flux_marg`` and
+  ``compute_source_metrics`` run on the device;
   the step variants (``step_mode="trust_region"``, ``stall_count_mode=
   "changed"``, ``convergence="dlnp"``) run on the device.
 """
@@ -266,10 +268,7 @@ def run_class_chunk(kernels: ClassKernels, psf_tree: PsfTree, host: dict,
     n_c = int(rows.size)
     if int(width) < n_c:
         raise ValueError(f"chunk width {width} < rows {n_c}")
-    for flag, name in ((compute_param_errors, "compute_param_errors"),
-                       (want_residual, "want_residual"),
-                       (compute_source_metrics, "compute_source_metrics"),
-                       (compute_flux_marg, "compute_flux_marg"),
+    for flag, name in ((want_residual, "want_residual"),
                        (compute_re_profile, "compute_re_profile")):
         if flag:
             raise ValueError(f"{name} is not supported by the B200 island solver")
@@ -289,10 +288,21 @@ def run_class_chunk(kernels: ClassKernels, psf_tree: PsfTree, host: dict,
         for k in ("n_same", "prej", "diverged"):   # "changed"-mode tracker carry
             if init_state.get(k) is not None:
                 init[k] = np.asarray(init_state[k])
-    out = dstack_dev.ctx.run_chunk(kernels.desc, arrays, int(max_steps),
-                                   kernels.n_bands, init)
-    nP = 6 * N
-    out.update(perr=None, femarg=None, reprof=None, smetrics=None, swin=None,
+    desc = kernels.desc
+    if compute_param_errors or compute_flux_marg or compute_source_metrics:
+        # the post-convergence passes are per-call options in the reference
+        desc = _lib.ClassDesc.from_buffer_copy(desc)
+        desc.param_errors = int(bool(compute_param_errors))
+        desc.flux_marg = int(bool(compute_flux_marg))
+        desc.source_metrics = int(bool(compute_source_metrics))
+    out = dstack_dev.ctx.run_chunk(desc, arrays, int(max_steps), kernels.n_bands, init)
+    if not compute_param_errors:
+        out["perr"] = None
+    if not compute_flux_marg:
+        out["femarg"] = None
+    if not compute_source_metrics:
+        out["smetrics"] = out["swin"] = None
+    out.update(reprof=None,
                resid=None, resid_w=None, wall_s=time.perf_counter() - t0)
     return out
 
@@ -452,6 +462,7 @@ class IslandFitJob:
                  plateau_dlnp_tol: float = 0.5, step_mode: str = "clip",
                  include_giants: bool = True,
                  compute_param_errors: bool = False,
+                 compute_flux_marg: bool = False,
                  compute_source_metrics: bool = False,
                  compute_re_profile: bool = False,
                  return_island_residual: bool = False, free_n_override=None,
@@ -461,9 +472,7 @@ class IslandFitJob:
                  field: DeviceField | None = None,
                  chunk_budget_bytes: float = 16e9, precision: str = "plain",
                  plan: "FieldPlan | None" = None, bg_mode: str = "frozen"):
-        for flag, name in ((compute_param_errors, "compute_param_errors"),
-                           (compute_source_metrics, "compute_source_metrics"),
-                           (compute_re_profile, "compute_re_profile"),
+        for flag, name in ((compute_re_profile, "compute_re_profile"),
                            (return_island_residual, "return_island_residual")):
             if flag:
                 raise ValueError(f"{name} is not supported by the B200 island solver")
@@ -515,6 +524,9 @@ class IslandFitJob:
                 plateau_dlnp_tol=plateau_dlnp_tol, step_mode=step_mode,
                 render_mode=render_mode,
                 native_stamp=fp.native, precision=precision, bg_mode=bg_mode)
+            kern.desc.param_errors = int(bool(compute_param_errors))
+            kern.desc.flux_marg = int(bool(compute_flux_marg))
+            kern.desc.source_metrics = int(bool(compute_source_metrics))
             chunk = _chunk_size(plan, n_bands, chunk_budget_bytes)
             ids = []
             for lo in range(0, plan.n_islands, chunk):
@@ -526,6 +538,9 @@ class IslandFitJob:
         self.max_steps_main = max_steps_main
         self.island_set, self.buckets, self.capped = island_set, buckets, capped
         self.include_giants = include_giants
+        self.compute_param_errors = bool(compute_param_errors)
+        self.compute_flux_marg = bool(compute_flux_marg)
+        self.compute_source_metrics = bool(compute_source_metrics)
         self.src = dict(pos_x=pos_x, pos_y=pos_y, logre=logre, ee1=ee1, ee2=ee2,
                         sersic_n=sersic_n)
         self.n_islands = sum(p.n_islands for p, _, _ in self.classes)
@@ -561,7 +576,11 @@ class IslandFitJob:
                 res_pdchi2=res["stall_dchi2"], res_div=res["diverged"],
                 res_ngood=res["n_good"], n_bands=n_bands,
                 res_bg=res.get("bg"), res_bg_err=res.get("bg_err"),
-                res_railed=res.get("railed")))
+                res_railed=res.get("railed"),
+                res_perr=res["perr"] if self.compute_param_errors else None,
+                res_femarg=res["femarg"] if self.compute_flux_marg else None,
+                res_smetrics=res["smetrics"] if self.compute_source_metrics else None,
+                res_swin=res["swin"] if self.compute_source_metrics else None))
         giant_ids = np.concatenate([np.asarray(self.buckets.giant_ids, np.int64).ravel(),
                                     np.asarray(self.capped, np.int64)])
         if self.include_giants and giant_ids.size:
