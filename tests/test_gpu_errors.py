@@ -185,5 +185,8 @@ def test_island_fit_reports_source_metrics(small):
     res = island_fit(**small.fit_kwargs("analytic"), compute_source_metrics=True)
     assert np.all(np.isfinite(res.rchisq)) and np.all(res.rchisq >= 0)
     assert np.all((res.fracin > 0) & (res.fracin <= 1.0 + 1e-3))
-    assert np.all(res.fracflux >= -1e-3) and np.all(res.fracmasked == 0.0)
+    # model light falling on the zero-weight border of the padded field
+    # counts as masked for sources near the edge
+    assert np.all(res.fracflux >= -1e-3)
+    assert np.all((res.fracmasked >= 0) & (res.fracmasked <= 1)) and np.any(res.fracmasked == 0)
     assert res.flux_win.shape == res.fluxes.shape and np.all(np.isfinite(res.flux_win))
