@@ -115,7 +115,21 @@ typedef struct uph_class_desc {
                                rchisq, fracflux, fracin, fracmasked and the
                                per-band window flux; uph_chunk_out.smetrics
                                and .swin                                   */
+  int32_t re_profile;       /* 1: chi2 profile along each extended member's
+                               log-radius at the final fit, at the offsets
+                               UPH_REPROF_DELTAS (island_solver.py:1779-
+                               1792); uph_chunk_out.reprof                 */
+  int32_t residual;         /* 1: band-coadded residual sum_b w (d - model)
+                               and weight sum_b w over the island window
+                               at the final fit (island_solver.py:1615-
+                               1637); uph_chunk_out.resid and .resid_w     */
 } uph_class_desc;
+
+/* log-radius offsets of the Re profile (the reference's REPROF_DELTAS_LN,
+ * island_plan.py:58-60) */
+#define UPH_REPROF_K 12
+#define UPH_REPROF_DELTAS {-2.5f, -1.5f, -0.9f, -0.5f, -0.25f, -0.1f, \
+                           0.1f, 0.25f, 0.5f, 0.9f, 1.5f, 2.5f}
 
 #define UPH_TC_MIN_ROWS_DEFAULT 24
 #define UPH_TC_COND_MAX_DEFAULT 10.0f
@@ -192,6 +206,12 @@ typedef struct uph_chunk_out {
                            0); NaN-filled without; may be NULL             */
   float* swin;          /* [n*nb*N] with source_metrics: f * sum(m) per
                            band (NaN for padded slots); may be NULL        */
+  float* reprof;        /* [n*N*12] with re_profile: chi2(p + dk e_logre)
+                           - chi2(p); 0 for star and padded slots; NaN-
+                           filled without; may be NULL                     */
+  float* resid;         /* [n*B*B] with residual: sum_b w (d - model)      */
+  float* resid_w;       /* [n*B*B] with residual: sum_b w; both NaN-filled
+                           without; may be NULL                            */
 } uph_chunk_out;
 
 /* Context: one per device per process. */

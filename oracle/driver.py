@@ -37,12 +37,13 @@ def psf_bands(psfs, tier: int, mode: str):
 
 
 def _one(args):
-    host, row, B, T, dstack, wstack, psf, table, mode, cfg, max_steps, native, bg, pe, fm, sm = args
+    (host, row, B, T, dstack, wstack, psf, table, mode, cfg, max_steps, native, bg, pe, fm, sm,
+     rp, rs) = args
     isl = island_inputs_from_host(host, row, B=B, T=T, dstack=dstack,
                                   wstack=wstack, psf=psf, table=table, mode=mode,
                                   native=native, bg_joint=bg)
     return solve_island(isl, cfg, max_steps, param_errors=pe, flux_marg=fm,
-                        source_metrics=sm)
+                        source_metrics=sm, re_profile=rp, residual=rs)
 
 
 def solve_chunk(host, rows, *, B, T, dstack, wstack, psfs, mode, table_path=None,
@@ -52,7 +53,9 @@ def solve_chunk(host, rows, *, B, T, dstack, wstack, psfs, mode, table_path=None
                 stall_count_mode: str = "proposals", convergence: str = "legacy",
                 plateau_dlnp_tol: float = 0.5, step_mode: str = "clip",
                 param_errors: bool = False, flux_marg: bool = False,
-                source_metrics: bool = False) -> dict:
+                source_metrics: bool = False, re_profile=None,
+                residual: bool = False) -> dict:
+    """``re_profile``: the log-radius offsets of the Re profile, or None."""
     table = SersicTable.load(table_path) if table_path is not None else None
     psf = psf_bands(psfs, T, mode)
     cfg = SolverConfig(reg=reg, pos_step_max=pos_step_max, ftol_rel=ftol_rel,
@@ -60,7 +63,8 @@ def solve_chunk(host, rows, *, B, T, dstack, wstack, psfs, mode, table_path=None
                        stall_count_mode=stall_count_mode, convergence=convergence,
                        plateau_dlnp_tol=plateau_dlnp_tol, step_mode=step_mode)
     jobs = [(host, int(r), B, T, dstack, wstack, psf, table, mode, cfg, max_steps,
-             native, bg_joint, param_errors, flux_marg, source_metrics) for r in rows]
+             native, bg_joint, param_errors, flux_marg, source_metrics, re_profile, residual)
+            for r in rows]
     if processes > 1 and len(jobs) > 1:
         import multiprocessing as mp
         with mp.get_context("spawn").Pool(processes) as pool:
@@ -76,6 +80,9 @@ def solve_chunk(host, rows, *, B, T, dstack, wstack, psfs, mode, table_path=None
     out["femarg"] = np.stack([r["femarg"] for r in res]) if flux_marg else None
     out["smetrics"] = np.stack([r["smetrics"] for r in res]) if source_metrics else None
     out["swin"] = np.stack([r["swin"] for r in res]) if source_metrics else None
+    out["reprof"] = np.stack([r["reprof"] for r in res]) if re_profile is not None else None
+    out["resid"] = np.stack([r["resid"] for r in res]) if residual else None
+    out["resid_w"] = np.stack([r["resid_w"] for r in res]) if residual else None
     out["steps_run"] = int(max(r["steps"] for r in res))
     return out
 

@@ -49,6 +49,7 @@ Algorithm followed (paths relative to the reference project ``tract7dt/``):
   ``:1401-1465``, final fluxes and errors ``:1467-1482``, marginal
   covariance of the nonlinear parameters ``:1484-1547``, shape-marginalised
   flux-variance increment ``:1549-1613``, source metrics ``:1639-1715``,
+  band-coadded residual ``:1615-1637``, Re profile ``:1779-1792``,
   good-pixel count
   ``:2690-2699``.
 
@@ -1116,6 +1117,38 @@ class IslandSolver:
         fwin = np.where(mm[None, :], fwin, np.nan)
         return met.astype(np.float32), fwin.astype(np.float32)
 
+    def re_profile(self, p, deltas):
+        """chi2 along each member slot's log-radius (island_solver.py:
+        1779-1792): chi2_of(p + dk e_{6n+2}) - chi2_of(p) for every slot n
+        and offset dk (the parameter moved by a float add).  (N, K)
+        float32."""
+        dt = self.dt
+        base = self.chi2_of(p)
+        out = np.zeros((self.N, len(deltas)), np.float32)
+        for n in range(self.N):
+            for j, dk in enumerate(deltas):
+                q = np.asarray(p, dt).copy()
+                q[6 * n + 2] = dt(q[6 * n + 2] + dt(dk))
+                out[n, j] = dt(self.chi2_of(q) - base)
+        return out
+
+    def residual_coadd(self, p):
+        """Band-coadded residual (island_solver.py:1615-1637): per window
+        pixel sum_b w (d - model) and sum_b w, float32 in band order; the
+        model includes the plane when it is solved.  ((B, B), (B, B))."""
+        isl = self.isl
+        dt = np.float32
+        R = np.zeros((isl.B, isl.B), dt)
+        W = np.zeros((isl.B, isl.B), dt)
+        for b in range(self.nb):
+            M, _ = self.models_band(b, p, False)
+            f = self.fluxes_band(M, isl.data[b], isl.w[b])[0].astype(dt)
+            model = np.tensordot(f, M.astype(dt), 1).astype(dt)
+            w = isl.w[b].astype(dt)
+            R = (R + w * (isl.data[b].astype(dt) - model)).astype(dt)
+            W = (W + w).astype(dt)
+        return R, W
+
     def final_errors(self, p):
         """Marginal covariance of the nonlinear parameters at p
         (island_solver.py:1484-1547): the undamped Gauss-Newton matrix with
@@ -1164,7 +1197,8 @@ class IslandSolver:
 
 def solve_island(isl: IslandInput, cfg: SolverConfig, max_steps: int = 30,
                  state=None, param_errors: bool = False, flux_marg: bool = False,
-                source_metrics: bool = False):
+                source_metrics: bool = False, re_profile=None,
+                residual: bool = False):
     """Full per-island result (the row of run_class_chunk's dict)."""
     s = IslandSolver(isl, cfg)
     out = s.run(max_steps, state)
@@ -1185,13 +1219,16 @@ def solve_island(isl: IslandInput, cfg: SolverConfig, max_steps: int = 30,
     perr = s.final_errors(out["p"]) if param_errors else None
     femarg = s.final_flux_marg(out["p"]) if flux_marg else None
     smet, swin = s.source_metrics(out["p"]) if source_metrics else (None, None)
+    reprof = s.re_profile(out["p"], re_profile) if re_profile is not None else None
+    resid, resid_w = s.residual_coadd(out["p"]) if residual else (None, None)
     return dict(p=out["p"].reshape(s.N, 6).astype(np.float32),
                 fluxes=F, ferr=E, bg=G, bg_err=GE, chi2=out["chi2"], conv=out["conv"],
                 stall=stall, diverged=div, stall_dchi2=sd,
                 nst=out["nst"], lam=out["lam"], consec=out["consec"],
                 nrej=out["nrej"], n_good=n_good, steps=out["steps"],
                 n_same=out["n_same"], prej=np.asarray(out["prej"], np.float32),
-                railed=railed, perr=perr, femarg=femarg, smetrics=smet, swin=swin)
+                railed=railed, perr=perr, femarg=femarg, smetrics=smet, swin=swin,
+                reprof=reprof, resid=resid, resid_w=resid_w)
 
 
 def island_inputs_from_host(host: dict, row: int, *, B: int, T: int,

@@ -190,3 +190,58 @@ def test_island_fit_reports_source_metrics(small):
     assert np.all(res.fracflux >= -1e-3)
     assert np.all((res.fracmasked >= 0) & (res.fracmasked <= 1)) and np.any(res.fracmasked == 0)
     assert res.flux_win.shape == res.fluxes.shape and np.all(np.isfinite(res.flux_win))
+
+
+def test_re_profile_and_residual_parity(small):
+    """Re profile (island_solver.py:1779-1792) and band-coadded residual
+    (:1615-1637) vs the oracle on islands whose fits agree: profile values
+    within 1e-5 of the island chi2 (plus 1e-3 relative), residuals within
+    1e-3 of the window's largest |w d|, weights bitwise."""
+    from uniphot_b200 import solver
+    from uniphot_b200.plan import REPROF_DELTAS_LN
+    from oracle.driver import solve_chunk
+    from _common import TABLE
+    plans, hosts, PAD, ds, ws, psfs = field_classes(small, "analytic", ("star", "mixed"))
+    field = solver.DeviceField(ds, ws, PAD)
+    n_gal = 0
+    for plan, host in zip(plans, hosts):
+        tree, nt = solver.build_psf_tree(psfs, plan.tier)
+        kern = solver.make_class_kernels(
+            plan, ds.shape[0], nt, render_backend="fft", reg=1e-9, pos_step_max_pix=0.5,
+            chi2_ftol_rel=1e-4, step_tol_pix=0.1, un_freeze_steps=0,
+            render_mode="analytic", native_stamp=small.native)
+        rows = np.arange(plan.n_islands)
+        gg = solver.run_class_chunk(kern, tree, host, rows, rows.size, 30, field, field, PAD,
+                                    compute_re_profile=True, want_residual=True)
+        oo = solve_chunk(host, rows, B=plan.bbox_class, T=plan.tier, dstack=ds, wstack=ws,
+                         psfs=psfs, mode="analytic", table_path=TABLE, native=small.native,
+                         re_profile=REPROF_DELTAS_LN, residual=True)
+        r = compare(gg, oo, host["mmask"])
+        same = r["same_nst"] & r["same_flags"] & r["pos_ok"] & r["flux_ok"]
+        ext = (host["st"] != 0) & host["mmask"]
+        assert np.all(gg["reprof"][~ext] == 0.0)
+        pg, po = gg["reprof"][same], oo["reprof"][same]
+        tol = 1e-5 * np.abs(oo["chi2"][same])[:, None, None] + 1e-3 * np.abs(po)
+        assert np.all(np.abs(pg - po) <= tol), float(np.max(np.abs(pg - po) - tol))
+        n_gal += int(ext[same].sum())
+        np.testing.assert_array_equal(gg["resid_w"], oo["resid_w"])
+        B = plan.bbox_class
+        for i in np.nonzero(same)[0]:
+            oy, ox = int(host["oy"][i]), int(host["ox"][i])
+            wd = np.abs(ws[:, oy:oy + B, ox:ox + B] * ds[:, oy:oy + B, ox:ox + B]).sum(axis=0)
+            dr = np.abs(gg["resid"][i] - oo["resid"][i]).max()
+            assert dr <= 1e-3 * wd.max(), (plan.key, i, float(dr), float(wd.max()))
+    assert n_gal > 0
+
+
+def test_island_fit_re_interval_and_residual_export(small):
+    from uniphot_b200.solver import island_fit
+    res, resid = island_fit(**small.fit_kwargs("analytic"), compute_re_profile=True,
+                            return_island_residual=True)
+    gal = np.isfinite(res.re_prof_lo)
+    assert gal.any() and np.all(res.re_prof_lo[gal] < res.re_prof_hi[gal])
+    re = np.exp(res.logre[gal])
+    assert np.all(res.re_prof_lo[gal] <= re * 1.0001) and np.all(res.re_prof_hi[gal] >= re * 0.9999)
+    assert len(resid) == len(np.unique(res.island_id))
+    one = next(iter(resid.values()))
+    assert one["resid"].shape == (one["B"], one["B"]) and np.all(one["resid_w"] >= 0)

@@ -460,3 +460,41 @@ def test_source_metrics_known_answers():
         num += fin * (other * own).sum() / (own * own).sum()
         den += fin
     np.testing.assert_allclose(met2[0, 1], num / den, rtol=1e-5)
+
+
+def test_re_profile_and_residual_known_answers():
+    """Re profile (island_solver.py:1779-1792): 0 for a star slot, a
+    positive bowl around a galaxy's converged log-radius; the band-coadded
+    residual (:1615-1637) of a noise-free fit at the truth is ~0 and its
+    weight is the band sum of w."""
+    isl, flux = _mini_island("analytic", n_src=2, seed=8, noise=False)
+    s = O.IslandSolver(isl, O.SolverConfig(precision="f64"))
+    p = isl.p0.astype(np.float64)
+    from uniphot_b200.plan import REPROF_DELTAS_LN
+    prof = s.re_profile(p, REPROF_DELTAS_LN)
+    assert np.all(prof[0] == 0.0)
+    assert np.all(prof[1] > 0) and prof[1, 0] > prof[1, 5] and prof[1, -1] > prof[1, 6]
+    R, W = s.residual_coadd(p)
+    np.testing.assert_allclose(W, isl.w.sum(axis=0), rtol=1e-6)
+    assert np.abs(R).max() <= 1e-3 * np.abs(isl.w * isl.data).sum(axis=0).max()
+
+
+def test_re_profile_interval_interpolates_the_unit_crossing():
+    """island_plan.py:913-952: the interval ends where the profile first
+    reaches 1 on each side, linearly interpolated; a side that never does
+    ends at its outermost offset."""
+    from uniphot_b200.plan import REPROF_DELTAS_LN, re_profile_interval
+    d = REPROF_DELTAS_LN.astype(np.float64)
+    sig = 0.3
+    prof = np.zeros((1, 2, d.size), np.float32)
+    prof[0, 0] = (d / sig) ** 2
+    prof[0, 0, d < 0] = 0.5               # never reaches 1 on the left
+    res_p = np.zeros((1, 2, 6), np.float32)
+    res_p[0, 0, 2] = np.log(4.0)
+    is_ext = np.array([[True, False]])
+    lo, hi = re_profile_interval(res_p, prof, d, np.array([0, 0]), np.array([0, 1]), is_ext)
+    p0, p1 = (0.25 / sig) ** 2, (0.5 / sig) ** 2
+    cross = 0.25 + (1 - p0) / (p1 - p0) * 0.25
+    np.testing.assert_allclose(hi[0], 4.0 * np.exp(cross), rtol=1e-6)
+    np.testing.assert_allclose(lo[0], 4.0 * np.exp(-2.5), rtol=1e-6)
+    assert np.isnan(lo[1]) and np.isnan(hi[1])

@@ -44,7 +44,8 @@ class ClassDesc(C.Structure):
                 ("plateau_dlnp_tol", C.c_float), ("bg_joint", C.c_int32),
                 ("tc_cond_max", C.c_float), ("step_tr", C.c_int32),
                 ("param_errors", C.c_int32), ("flux_marg", C.c_int32),
-                ("source_metrics", C.c_int32)]
+                ("source_metrics", C.c_int32), ("re_profile", C.c_int32),
+                ("residual", C.c_int32)]
 
 
 class ChunkIn(C.Structure):
@@ -61,7 +62,8 @@ class ChunkOut(C.Structure):
         "stall_dchi2", "nst", "lam", "consec", "nrej", "n_good")] + \
         [("steps_run", C.c_int32), ("bg", _P), ("bg_err", _P), ("n_same", _P),
          ("prej", _P), ("railed", _P), ("perr", _P), ("femarg", _P),
-         ("smetrics", _P), ("swin", _P)]
+         ("smetrics", _P), ("swin", _P), ("reprof", _P), ("resid", _P),
+         ("resid_w", _P)]
 
 
 class UphError(RuntimeError):
@@ -210,7 +212,7 @@ class Context:
         """One chunk through uph_run_chunk (upload, solve, read)."""
         cin, keep_alive = chunk_in(arrays, init_state)
         n, N = arrays["mmask"].shape
-        out, cout = chunk_out(n, N, nb)
+        out, cout = chunk_out(n, N, nb, int(desc.bbox) if desc.residual else 0)
         rc = lib().uph_run_chunk(self._h, C.byref(desc), C.byref(cin), int(max_steps),
                                  C.byref(cout))
         self.check(rc, "uph_run_chunk")
@@ -266,7 +268,8 @@ def chunk_in(arrays: dict, init_state: dict | None = None):
     return cin, keep
 
 
-def chunk_out(n: int, N: int, nb: int):
+def chunk_out(n: int, N: int, nb: int, B: int = 0):
+    """Output arrays of one chunk (the residual images only when B > 0)."""
     out = dict(p=np.zeros((n, N, 6), np.float32),
                fluxes=np.zeros((n, nb, N), np.float32),
                ferr=np.zeros((n, nb, N), np.float32),
@@ -279,7 +282,11 @@ def chunk_out(n: int, N: int, nb: int):
                n_same=np.zeros(n, np.int32), prej=np.zeros((n, 6 * N), np.float32),
                railed=np.zeros(n, np.uint8), perr=np.zeros((n, N, 13), np.float32),
                femarg=np.zeros((n, nb, N), np.float32),
-               smetrics=np.zeros((n, N, 4), np.float32), swin=np.zeros((n, nb, N), np.float32))
+               smetrics=np.zeros((n, N, 4), np.float32), swin=np.zeros((n, nb, N), np.float32),
+               reprof=np.zeros((n, N, 12), np.float32))
+    if B > 0:
+        out["resid"] = np.zeros((n, B, B), np.float32)
+        out["resid_w"] = np.zeros((n, B, B), np.float32)
     cout = ChunkOut()
     for k, v in out.items():
         setattr(cout, k, ptr(v))
@@ -310,15 +317,15 @@ class Job:
         self.ctx.check(lib().uph_job_add_chunk(self._h, C.byref(desc), C.byref(cin),
                                                C.byref(cid)), "uph_job_add_chunk")
         n, N = arrays["mmask"].shape
-        self.shapes.append((n, N, nb))
+        self.shapes.append((n, N, nb, int(desc.bbox) if desc.residual else 0))
         return int(cid.value)
 
     def solve(self, max_steps: int):
         self.ctx.check(lib().uph_job_solve(self._h, int(max_steps)), "uph_job_solve")
 
     def read(self, cid: int) -> dict:
-        n, N, nb = self.shapes[cid]
-        out, cout = chunk_out(n, N, nb)
+        n, N, nb, B = self.shapes[cid]
+        out, cout = chunk_out(n, N, nb, B)
         self.ctx.check(lib().uph_job_read(self._h, int(cid), C.byref(cout)),
                        "uph_job_read")
         return finish_out(out, cout)

@@ -693,7 +693,13 @@ int add_chunk(uph_ctx* ctx, Chunk* ch, const uph_class_desc* cls,
   if (cls->param_errors || cls->flux_marg) {
     c.perr = cbuf<float>(ctx, ch, "perr", (size_t)n * N * 13, &rc);
     c.ews = cbuf<double>(ctx, ch, "ews", (size_t)n * nLmax * 2 * nLmax, &rc);
+  }
+  if (cls->param_errors || cls->flux_marg || cls->re_profile)
     c.flsave = cbuf<uint8_t>(ctx, ch, "flsave", n, &rc);
+  if (cls->re_profile) c.reprof = cbuf<float>(ctx, ch, "reprof", (size_t)n * N * UPH_REPROF_K, &rc);
+  if (cls->residual) {
+    c.resid = cbuf<float>(ctx, ch, "resid", (size_t)n * B * B, &rc);
+    c.resid_w = cbuf<float>(ctx, ch, "residw", (size_t)n * B * B, &rc);
   }
   if (cls->flux_marg) {
     ch->d_cjac = cbuf<float>(ctx, ch, "cjac", (size_t)n * nb * nLmax * UPH_MAXLIN, &rc);
@@ -856,10 +862,27 @@ void post_loop(Chunk* ch, Launcher& L) {
     L(4, [&] { launch_gram_trial(c, c.p_try, PH_PROBE, 0, nullptr, nullptr, s); });
     L(5, [&] { launch_accept(c, PH_PROBE, s); });
   }
+  if (c.reprof) {
+    // Re profile: one trial pass per (member slot, offset) on the islands
+    // whose slot holds an extended member; flags saved around it
+    static const float kDeltas[UPH_REPROF_K] = UPH_REPROF_DELTAS;
+    launch_errors_begin(c, s);
+    for (int n = 0; n < c.N; ++n)
+      for (int j = 0; j < UPH_REPROF_K; ++j) {
+        L(3, [&] { launch_reprof_set(c, n, j, kDeltas[j], s); });
+        L(0, [&] { launch_render(c, c.p_try, PH_PROBE, s); }, 2);
+        L(4, [&] { launch_gram_trial(c, c.p_try, PH_PROBE, 0, nullptr, nullptr, s); });
+        L(5, [&] { launch_reprof_store(c, n, j, s); });
+      }
+    launch_errors_end(c, s);
+    L.job->ctx->launches += 2;
+  }
   L(0, [&] { launch_render(c, c.p, PH_ALL, s); }, 2);
   L(4, [&] { launch_gram_trial(c, c.p, PH_ALL, 1, nullptr, nullptr, s); });
-  // source metrics read the final pass's model rows and fluxes
+  // source metrics and the residual read the final pass's model rows and
+  // fluxes
   if (c.smet) L(4, [&] { launch_source_metrics(c, s); }, 2);
+  if (c.resid) L(4, [&] { launch_residual_coadd(c, s); });
 }
 
 int job_solve(uph_job* job, int max_steps) {
@@ -1095,6 +1118,26 @@ int job_read(uph_job* job, int id, uph_chunk_out* out) {
   if ((rc = download(ctx, out->consec, c.consec, sizeof(int) * n, "consec"))) return rc;
   if ((rc = download(ctx, out->nrej, c.nrej, sizeof(int) * n, "nrej"))) return rc;
   if ((rc = download(ctx, out->diverged, ch->d_div, n, "diverged"))) return rc;
+  if (out->reprof) {
+    if (c.reprof) {
+      if ((rc = download(ctx, out->reprof, c.reprof, sizeof(float) * n * N * UPH_REPROF_K,
+                         "reprof")))
+        return rc;
+    } else {
+      for (size_t e = 0; e < (size_t)n * N * UPH_REPROF_K; ++e) out->reprof[e] = NAN;
+    }
+  }
+  for (int q = 0; q < 2; ++q) {
+    float* dst = q ? out->resid_w : out->resid;
+    const float* src = q ? c.resid_w : c.resid;
+    if (!dst) continue;
+    const size_t cnt = (size_t)n * c.B * c.B;
+    if (src) {
+      if ((rc = download(ctx, dst, src, sizeof(float) * cnt, "residual"))) return rc;
+    } else {
+      for (size_t e = 0; e < cnt; ++e) dst[e] = NAN;
+    }
+  }
   if (out->smetrics) {
     if (c.smet) {
       if ((rc = download(ctx, out->smetrics, c.smet, sizeof(float) * n * N * 4, "smetrics")))

@@ -160,6 +160,11 @@ struct ClassDev {
   double* smom;
   float* smet;
   float* swin;
+  // Re profile (n_isl, N, 12) chi2 differences; band-coadded residual and
+  // weight (n_isl, B, B)
+  float* reprof;
+  float* resid;
+  float* resid_w;
   float* bgout;            // (n_isl, nb, 3) final background coefficients
   float* bgerr;            // (n_isl, nb, 3) and their errors
   float* fcur;
@@ -309,6 +314,9 @@ void launch_errors_begin(const ClassDev& c, cudaStream_t s);
 void launch_final_errors(const ClassDev& c, cudaStream_t s);
 void launch_flux_marg(const ClassDev& c, cudaStream_t s);
 void launch_source_metrics(const ClassDev& c, cudaStream_t s);
+void launch_residual_coadd(const ClassDev& c, cudaStream_t s);
+void launch_reprof_set(const ClassDev& c, int n, int j, float dk, cudaStream_t s);
+void launch_reprof_store(const ClassDev& c, int n, int j, cudaStream_t s);
 void launch_errors_end(const ClassDev& c, cudaStream_t s);
 size_t render_smem_bytes();
 size_t gram_lin_smem_bytes(int Kmax);

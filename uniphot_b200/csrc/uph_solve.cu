@@ -1506,6 +1506,97 @@ __global__ void k_metrics_combine(ClassDev c) {
   o[3] = (mm && fmd > 0.f) ? __fdiv_rn(fmn, fmd) : 0.f;
 }
 
+// Band-coadded residual of one island at the final parameters
+// (island_solver.py:1615-1637): per window pixel, sum over bands in band
+// order of w (d - model) and of w (float32), the model being the final
+// pass's fluxes times its model rows (and the plane when it is solved).
+template <bool BG>
+__global__ void __launch_bounds__(NT) k_residual_coadd(ClassDev c) {
+  __shared__ int4 box[UPH_MAXN];
+  __shared__ float fl[UPH_MAXLIN];
+  const int isl = blockIdx.x;
+  if (isl >= c.n_isl) return;
+  const int tid = threadIdx.x;
+  const int nr = c.isl_nr[isl];
+  const int B = c.B, Sz = c.Sz;
+  const size_t plane = (size_t)c.Hp * c.Wp;
+  load_boxes(c, isl, c.p, box);
+  float* R = c.resid + (size_t)isl * B * B;
+  float* W = c.resid_w + (size_t)isl * B * B;
+  for (int pix = tid; pix < B * B; pix += NT) {
+    R[pix] = 0.f;
+    W[pix] = 0.f;
+  }
+  for (int b = 0; b < c.nb; ++b) {
+    __syncthreads();
+    for (int k = tid; k < nr; k += NT) fl[k] = c.flux[((size_t)isl * c.nb + b) * c.N + k];
+    if (BG)
+      for (int j = tid; j < c.nbg; j += NT)
+        fl[nr + j] = c.bgout[((size_t)isl * c.nb + b) * UPH_MAXBG + j];
+    __syncthreads();
+    const float* dbase = c.dstack + b * plane + (size_t)c.oy[isl] * c.Wp + c.ox[isl];
+    const float* wbase = c.wstack + b * plane + (size_t)c.oy[isl] * c.Wp + c.ox[isl];
+    for (int pix = tid; pix < B * B; pix += NT) {
+      const int wy = pix / B, wx = pix - (pix / B) * B;
+      float model = 0.f;
+      for (int k = 0; k < nr; ++k) {
+        const int4 bx = box[k];
+        const int ly = wy - bx.y, lx = wx - bx.x;
+        if (ly >= 0 && ly < bx.w && lx >= 0 && lx < bx.z)
+          model = fmaf(fl[k], c.stamps[stamp_slot(c, isl, b, k, 0) + (size_t)ly * Sz + lx], model);
+      }
+      if (BG)
+        for (int j = 0; j < c.nbg; ++j) model = fmaf(fl[nr + j], bg_basis(j, wy, wx, B), model);
+      const float w = wbase[(size_t)wy * c.Wp + wx];
+      const float d = dbase[(size_t)wy * c.Wp + wx];
+      R[pix] = __fadd_rn(R[pix], __fmul_rn(w, __fsub_rn(d, model)));
+      W[pix] = __fadd_rn(W[pix], w);
+    }
+  }
+}
+
+// Re profile (island_solver.py:1779-1792), one scan point: p_try = p with
+// member n's log-radius moved by dk (float add), for the islands where slot
+// n holds an extended member; the others are left out of the probe phase
+// and their profile entry is 0 (their model does not depend on it).
+__global__ void k_reprof_set(ClassDev c, int n, int j, float dk) {
+  const int isl = blockIdx.x;
+  if (isl >= c.n_isl) return;
+  const int nP = c.nP;
+  const bool ext = n < c.isl_nr[isl] && c.stype[(size_t)isl * c.N + n] != 0;
+  const float* p = c.p + (size_t)isl * nP;
+  float* pt = c.p_try + (size_t)isl * nP;
+  for (int q = threadIdx.x; q < nP; q += blockDim.x)
+    pt[q] = (q == 6 * n + 2 && ext) ? __fadd_rn(p[q], dk) : p[q];
+  if (threadIdx.x == 0) {
+    c.flags[isl] = ext ? (uint8_t)(FL_PROBE | FL_REAL) : (uint8_t)FL_REAL;
+    if (!ext) c.reprof[((size_t)isl * c.N + n) * 12 + j] = 0.f;
+  }
+}
+
+// chi2 of p_try (float32 band accumulation plus the prior penalty, as the
+// step's accept) minus the chi2 at p, for the probed islands.
+__global__ void k_reprof_store(ClassDev c, int n, int j) {
+  const int isl = blockIdx.x * blockDim.x + threadIdx.x;
+  if (isl >= c.n_isl || !(c.flags[isl] & FL_PROBE)) return;
+  const int nP = c.nP;
+  const float* pt = c.p_try + (size_t)isl * nP;
+  float chi2 = 0.f;
+  for (int b = 0; b < c.nb; ++b) chi2 = __fadd_rn(chi2, (float)c.chi2b[(size_t)isl * c.nb + b]);
+  if (c.has_priors) {
+    float pen = 0.f;
+    const float* pm = c.prior_mean + (size_t)isl * nP;
+    const float* pinv = c.prior_inv + (size_t)isl * nP;
+    for (int q = 0; q < nP; ++q) {
+      if (!(c.keep[(size_t)isl * nP + q] && c.mmask[isl * c.N + q / 6])) continue;
+      const float t = __fmul_rn(pinv[q], __fsub_rn(pt[q], pm[q]));
+      pen = __fadd_rn(pen, __fmul_rn(t, t));
+    }
+    chi2 = __fadd_rn(chi2, pen);
+  }
+  c.reprof[((size_t)isl * c.N + n) * 12 + j] = __fsub_rn(chi2, c.chi2[isl]);
+}
+
 __global__ void k_set_probe(ClassDev c) {
   const int isl = blockIdx.x * blockDim.x + threadIdx.x;
   if (isl >= c.n_isl) return;
@@ -1550,6 +1641,21 @@ void launch_source_metrics(const ClassDev& c, cudaStream_t s) {
   else
     k_source_metrics<false><<<(unsigned)(c.n_isl * c.nb), NT, 0, s>>>(c);
   k_metrics_combine<<<(unsigned)((c.n_isl * c.N + 127) / 128), 128, 0, s>>>(c);
+}
+
+void launch_residual_coadd(const ClassDev& c, cudaStream_t s) {
+  if (c.nbg)
+    k_residual_coadd<true><<<(unsigned)c.n_isl, NT, 0, s>>>(c);
+  else
+    k_residual_coadd<false><<<(unsigned)c.n_isl, NT, 0, s>>>(c);
+}
+
+void launch_reprof_set(const ClassDev& c, int n, int j, float dk, cudaStream_t s) {
+  k_reprof_set<<<(unsigned)c.n_isl, 64, 0, s>>>(c, n, j, dk);
+}
+
+void launch_reprof_store(const ClassDev& c, int n, int j, cudaStream_t s) {
+  k_reprof_store<<<(unsigned)((c.n_isl + 127) / 128), 128, 0, s>>>(c, n, j);
 }
 
 void launch_set_probe(const ClassDev& c, cudaStream_t s) {

@@ -24,6 +24,9 @@ SOURCE_STAR = 0
 SOURCE_SERSIC = 3
 SERSIC_N_MIN = 0.29
 SERSIC_N_MAX = 6.3
+# log-radius offsets of the Re profile scan (island_plan.py:58-60)
+REPROF_DELTAS_LN = np.array([-2.5, -1.5, -0.9, -0.5, -0.25, -0.1,
+                             0.1, 0.25, 0.5, 0.9, 1.5, 2.5], np.float32)
 
 DEFAULT_MAX_STEPS = 30
 DEFAULT_MAX_STEPS_MAIN = 8
@@ -318,6 +321,37 @@ def _nan(n):
     return np.full(n, np.nan, np.float32)
 
 
+def re_profile_interval(res_p, res_reprof, deltas, ii, kk, is_ext):
+    """Re interval where the chi2 profile along log Re stays below 1
+    (island_plan.py:913-952): walking outward from the fit on each side,
+    the first offset whose profile reaches 1 is linearly interpolated with
+    the previous point (the fit itself at 0); a side that never reaches 1
+    ends at its outermost offset.  NaN for point sources."""
+    d = np.asarray(deltas, np.float64)
+    order = np.argsort(d)
+    d = d[order]
+    prof = res_reprof[ii, kk, :].astype(np.float64)[:, order]
+    prof = np.where(np.isfinite(prof), prof, np.inf)
+
+    def crossing(pr, dd):
+        P = np.concatenate([np.zeros((pr.shape[0], 1)), pr], axis=1)
+        D = np.concatenate([[0.0], dd])
+        hit = P >= 1.0
+        any_hit = hit.any(axis=1)
+        j = np.maximum(np.argmax(hit, axis=1), 1)
+        p0 = P[np.arange(P.shape[0]), j - 1]
+        p1 = P[np.arange(P.shape[0]), j]
+        t = np.where(p1 > p0, (1.0 - p0) / np.maximum(p1 - p0, 1e-30), 1.0)
+        return np.where(any_hit, D[j - 1] + np.clip(t, 0.0, 1.0) * (D[j] - D[j - 1]), dd[-1])
+    neg, pos = d < 0, d > 0
+    lo = crossing(prof[:, neg][:, ::-1], d[neg][::-1])
+    hi = crossing(prof[:, pos], d[pos])
+    re = np.exp(res_p[ii, kk, 2].astype(np.float64))
+    ext = is_ext[ii, kk]
+    return (np.where(ext, re * np.exp(lo), np.nan).astype(np.float32),
+            np.where(ext, re * np.exp(hi), np.nan).astype(np.float32))
+
+
 def catalog_errors(res_p, res_perr, host, ii, kk, n_final) -> dict:
     """Catalog-frame 1-sigma errors and prior fractions of the members
     (ii, kk) from the per-member covariance rows of ``res_perr`` (n_isl, N,
@@ -384,7 +418,8 @@ def unpack_class_results(plan, host, island_set, res_p, res_f, res_fe,
                          res_perr=None, res_pdchi2=None, res_div=None,
                          res_ngood=None, n_bands=0, res_bg=None, res_bg_err=None,
                          res_railed=None, res_femarg=None, res_smetrics=None,
-                         res_swin=None, **_unused) -> dict:
+                         res_swin=None, res_reprof=None, reprof_deltas=None,
+                         **_unused) -> dict:
     """Island rows -> source rows for the valid member slots.
 
     Parameter errors and prior fractions come from ``res_perr`` (the
@@ -392,8 +427,8 @@ def unpack_class_results(plan, host, island_set, res_p, res_f, res_fe,
     ``flux_marg_var`` from ``res_femarg`` (the shape-marginalised flux
     variance increment, ``compute_flux_marg``), the source metrics and
     window fluxes from ``res_smetrics`` / ``res_swin``
-    (``compute_source_metrics``); NaN without them.  The Re-profile
-    columns are NaN: that kernel is not built."""
+    (``compute_source_metrics``), the Re interval from ``res_reprof``
+    (``compute_re_profile``); NaN without them."""
     midx, mmask, is_ext = plan.midx, host["mmask"], host["is_ext"]
     fn = host["fn_flag"]
     ii, kk = np.nonzero(mmask)
@@ -412,6 +447,10 @@ def unpack_class_results(plan, host, island_set, res_p, res_f, res_fe,
     else:
         chi2_nu = _nan(n)
     nb = max(int(n_bands), 0)
+    if res_reprof is not None and reprof_deltas is not None:
+        rlo, rhi = re_profile_interval(res_p, res_reprof, reprof_deltas, ii, kk, is_ext)
+    else:
+        rlo, rhi = _nan(n), _nan(n)
     if res_smetrics is not None:
         mets = dict(rchisq=res_smetrics[ii, kk, 0], fracflux=res_smetrics[ii, kk, 1],
                     fracin=res_smetrics[ii, kk, 2], fracmasked=res_smetrics[ii, kk, 3],
@@ -444,7 +483,7 @@ def unpack_class_results(plan, host, island_set, res_p, res_f, res_fe,
         island_nsrc=island_set.n_src[plan.isl_ids][ii].astype(np.int32),
         island_giant=np.zeros(n, bool),
         re_upper_pix=np.exp(host["upper"][ii, kk, 2].astype(np.float64)).astype(np.float32),
-        re_prof_lo=_nan(n), re_prof_hi=_nan(n), **errs, **mets,
+        re_prof_lo=rlo, re_prof_hi=rhi, **errs, **mets,
         flux_marg_var=(res_femarg[ii, :, kk].astype(np.float32) if res_femarg is not None
                        else np.full((n, nb), np.nan, np.float32)),
         bg_plane=(res_bg[ii].astype(np.float32) if res_bg is not None

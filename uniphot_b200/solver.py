@@ -22,10 +22,10 @@ Differences, by design:
   is run (``bucket_stats`` still reports the counts);
 * ``dstack_dev`` is a :class:`DeviceField` (the field stacks resident in
   HBM inside the library context); ``wstack_dev`` is accepted and ignored;
-* options whose kernels are not built (crossband GLS, scene subtract, the
-  Re profile, the island residual) raise ``ValueError``;
-  ``compute_param_errors``, ``compute_flux_marg`` and
-  ``compute_source_metrics`` run on the device;
+* options whose kernels are not built (crossband GLS, scene subtract) raise
+  ``ValueError``; the post-convergence passes (``compute_param_errors``,
+  ``compute_flux_marg``, ``compute_source_metrics``, ``compute_re_profile``,
+  ``want_residual`` / ``return_island_residual``) run on the device;
   the step variants (``step_mode="trust_region"``, ``stall_count_mode=
   "changed"``, ``convergence="dlnp"``) run on the device.
 """
@@ -41,7 +41,7 @@ from typing import Callable, Optional
 import numpy as np
 
 from . import _lib
-from .plan import (DEFAULT_CHI2_FTOL_REL, DEFAULT_MAX_STEPS,
+from .plan import (DEFAULT_CHI2_FTOL_REL, DEFAULT_MAX_STEPS, REPROF_DELTAS_LN,
                    DEFAULT_MAX_STEPS_MAIN, DEFAULT_POS_STEP_MAX,
                    DEFAULT_STEP_TOL_PIX, DEFAULT_UN_FREEZE_STEPS,
                    IslandFitResult, class_host_arrays, free_n_gate,
@@ -268,10 +268,6 @@ def run_class_chunk(kernels: ClassKernels, psf_tree: PsfTree, host: dict,
     n_c = int(rows.size)
     if int(width) < n_c:
         raise ValueError(f"chunk width {width} < rows {n_c}")
-    for flag, name in ((want_residual, "want_residual"),
-                       (compute_re_profile, "compute_re_profile")):
-        if flag:
-            raise ValueError(f"{name} is not supported by the B200 island solver")
     if not isinstance(dstack_dev, DeviceField):
         raise ValueError("dstack_dev must be a uniphot_b200.solver.DeviceField")
     if int(pad) != dstack_dev.pad:
@@ -289,12 +285,15 @@ def run_class_chunk(kernels: ClassKernels, psf_tree: PsfTree, host: dict,
             if init_state.get(k) is not None:
                 init[k] = np.asarray(init_state[k])
     desc = kernels.desc
-    if compute_param_errors or compute_flux_marg or compute_source_metrics:
+    if (compute_param_errors or compute_flux_marg or compute_source_metrics
+            or compute_re_profile or want_residual):
         # the post-convergence passes are per-call options in the reference
         desc = _lib.ClassDesc.from_buffer_copy(desc)
         desc.param_errors = int(bool(compute_param_errors))
         desc.flux_marg = int(bool(compute_flux_marg))
         desc.source_metrics = int(bool(compute_source_metrics))
+        desc.re_profile = int(bool(compute_re_profile))
+        desc.residual = int(bool(want_residual))
     out = dstack_dev.ctx.run_chunk(desc, arrays, int(max_steps), kernels.n_bands, init)
     if not compute_param_errors:
         out["perr"] = None
@@ -302,8 +301,11 @@ def run_class_chunk(kernels: ClassKernels, psf_tree: PsfTree, host: dict,
         out["femarg"] = None
     if not compute_source_metrics:
         out["smetrics"] = out["swin"] = None
-    out.update(reprof=None,
-               resid=None, resid_w=None, wall_s=time.perf_counter() - t0)
+    if not compute_re_profile:
+        out["reprof"] = None
+    if not want_residual:
+        out["resid"] = out["resid_w"] = None
+    out["wall_s"] = time.perf_counter() - t0
     return out
 
 
@@ -472,10 +474,6 @@ class IslandFitJob:
                  field: DeviceField | None = None,
                  chunk_budget_bytes: float = 16e9, precision: str = "plain",
                  plan: "FieldPlan | None" = None, bg_mode: str = "frozen"):
-        for flag, name in ((compute_re_profile, "compute_re_profile"),
-                           (return_island_residual, "return_island_residual")):
-            if flag:
-                raise ValueError(f"{name} is not supported by the B200 island solver")
         self.log_fn = log_fn
         if render_mode is None:
             render_mode = "analytic" if _is_mog(psfs[0]) else "reference"
@@ -527,6 +525,8 @@ class IslandFitJob:
             kern.desc.param_errors = int(bool(compute_param_errors))
             kern.desc.flux_marg = int(bool(compute_flux_marg))
             kern.desc.source_metrics = int(bool(compute_source_metrics))
+            kern.desc.re_profile = int(bool(compute_re_profile))
+            kern.desc.residual = int(bool(return_island_residual))
             chunk = _chunk_size(plan, n_bands, chunk_budget_bytes)
             ids = []
             for lo in range(0, plan.n_islands, chunk):
@@ -541,6 +541,9 @@ class IslandFitJob:
         self.compute_param_errors = bool(compute_param_errors)
         self.compute_flux_marg = bool(compute_flux_marg)
         self.compute_source_metrics = bool(compute_source_metrics)
+        self.compute_re_profile = bool(compute_re_profile)
+        self.return_island_residual = bool(return_island_residual)
+        self.island_residuals = {}
         self.src = dict(pos_x=pos_x, pos_y=pos_y, logre=logre, ee1=ee1, ee2=ee2,
                         sersic_n=sersic_n)
         self.n_islands = sum(p.n_islands for p, _, _ in self.classes)
@@ -580,7 +583,17 @@ class IslandFitJob:
                 res_perr=res["perr"] if self.compute_param_errors else None,
                 res_femarg=res["femarg"] if self.compute_flux_marg else None,
                 res_smetrics=res["smetrics"] if self.compute_source_metrics else None,
-                res_swin=res["swin"] if self.compute_source_metrics else None))
+                res_swin=res["swin"] if self.compute_source_metrics else None,
+                res_reprof=res["reprof"] if self.compute_re_profile else None,
+                reprof_deltas=REPROF_DELTAS_LN if self.compute_re_profile else None))
+            if self.return_island_residual:
+                # per-island coadded residual at the converged parameters,
+                # keyed by global island id with the window origin
+                for r in range(plan.n_islands):
+                    self.island_residuals[int(plan.isl_ids[r])] = dict(
+                        resid=res["resid"][r], resid_w=res["resid_w"][r],
+                        x0b=float(host["x0b"][r]), y0b=float(host["y0b"][r]),
+                        B=int(plan.bbox_class))
         giant_ids = np.concatenate([np.asarray(self.buckets.giant_ids, np.int64).ravel(),
                                     np.asarray(self.capped, np.int64)])
         if self.include_giants and giant_ids.size:
@@ -642,7 +655,10 @@ def island_fit(**kwargs) -> IslandFitResult:
     job = IslandFitJob(**kwargs)
     try:
         job.solve()
-        return job.result()
+        res = job.result()
+        if job.return_island_residual:
+            return res, job.island_residuals
+        return res
     finally:
         job.close()
 
