@@ -117,11 +117,15 @@ def test_zero_weight_island_stalls_like_oracle(small):
     _assert_parity([p], [h], g, o, "zero-weight")
 
 
-def test_reference_mode_galaxy_is_rejected(small):
+def test_reference_mode_galaxies_parity(small):
+    """Reference render mode with galaxies: the Sersic mixture convolved
+    with the pixelised PSF in the Fourier domain (sersic_mog.py:153-207),
+    then the Lanczos shift as for stars; same bar as the other classes."""
     plans, hosts, PAD, ds, ws, psfs = field_classes(small, "reference", ("mixed",))
-    with pytest.raises(ValueError):
-        run_gpu(plans[:1], hosts[:1], PAD, ds, ws, psfs, "reference",
-                native=small.native)
+    assert plans
+    g, _ = run_gpu(plans, hosts, PAD, ds, ws, psfs, "reference", native=small.native)
+    o = run_oracle(plans, hosts, PAD, ds, ws, psfs, "reference", native=small.native)
+    _assert_parity(plans, hosts, g, o, "reference-galaxies")
 
 
 def test_unpadded_upload_matches_padded(small):

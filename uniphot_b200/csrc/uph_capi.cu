@@ -543,10 +543,9 @@ int add_chunk(uph_ctx* ctx, Chunk* ch, const uph_class_desc* cls,
       return set_err(ctx, UPH_ERR_INVALID, "island %d window outside the padded field", i);
   }
   if (nLmax > UPH_MAXLIVE) return set_err(ctx, UPH_ERR_INVALID, "too many live parameters");
-  if (any_gal && mode == UPH_RENDER_REFERENCE)
+  if (any_gal && mode == UPH_RENDER_REFERENCE && fft_pad_for(T) > 512)
     return set_err(ctx, UPH_ERR_INVALID,
-                   "reference render mode supports STAR members only in this build; "
-                   "galaxies need render_mode='analytic'");
+                   "reference-mode galaxies: tier %d needs a Fourier grid above 512", T);
   if (any_gal && !ctx->tb_knots.ptr)
     return set_err(ctx, UPH_ERR_STATE, "no Sersic table uploaded");
   std::vector<int16_t> row_k((size_t)n * Kmax, 0), row_s((size_t)n * Kmax, -1),
@@ -696,6 +695,14 @@ int add_chunk(uph_ctx* ctx, Chunk* ch, const uph_class_desc* cls,
   }
   if (cls->param_errors || cls->flux_marg || cls->re_profile)
     c.flsave = cbuf<uint8_t>(ctx, ch, "flsave", n, &rc);
+  if (any_gal && mode == UPH_RENDER_REFERENCE) {
+    // galaxy stamps by the Fourier-domain convolution with the pixel PSF
+    c.fft_P = fft_pad_for(T);
+    c.gfft_floats = gal_fft_floats(T, c.fft_P);
+    c.gfft_ctas = (int)std::min<long long>((long long)n * nb * N, 2LL * ctx->sm_count);
+    c.gstamp = cbuf<float>(ctx, ch, "gstamp", (size_t)n * nb * N * 7 * T * T, &rc);
+    c.gfft_ws = cbuf<float>(ctx, ch, "gfftws", (size_t)c.gfft_ctas * c.gfft_floats, &rc);
+  }
   if (cls->re_profile) c.reprof = cbuf<float>(ctx, ch, "reprof", (size_t)n * N * UPH_REPROF_K, &rc);
   if (cls->residual) {
     c.resid = cbuf<float>(ctx, ch, "resid", (size_t)n * B * B, &rc);

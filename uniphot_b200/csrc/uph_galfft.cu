@@ -1,0 +1,212 @@
+// Galaxy stamps of the reference render mode (pixelised polynomial PSF):
+// the Fourier-domain convolution of the PSF stamp with the galaxy's Sersic
+// Gaussian mixture (sersic_mog.py:153-207, source_model.py:264-328),
+//
+//   S = irfft2(rfft2(pad(psf)) * sum_c a_c exp(v_c e(k)))[:T, :T] + core psf,
+//   e(k) = -2 pi^2 (cxx kx^2 + cyy ky^2 + 2 cxy kx ky),
+//
+// on a P x P grid (P the power of two >= 3T/2), and the partials the Gauss-
+// Newton rows need: through the PSF's spatial variation (Sx, Sy: the same
+// product with the PSF's position derivatives), the shape (F1 de/dtheta
+// with F1 = sum a_c v_c exp(v_c e)) and the Sersic index (sum (da_c + a_c
+// dv_c e) exp(v_c e) plus dcore psf, times dn/du).  The mixture's transform
+// is real (zero-centred Gaussians), so every product is a complex spectrum
+// times a real factor.
+//
+// The transforms are dense DFTs over the stamp's support -- rows of T
+// inputs to P/2 + 1 frequencies, columns of T inputs (or outputs) against
+// P frequencies -- with a shared-memory twiddle table: only T of the P
+// padded rows and columns are non-zero on the way in and needed on the way
+// out.  One CTA per (island, band, galaxy member), looping over the members
+// of a grid sized to the SM count, with its work space in global memory
+// (L2-resident per CTA).  The unshifted rows land in c.gstamp, which the
+// render's Lanczos passes read in place of the star's polynomial PSF.
+
+#include "uph_internal.cuh"
+
+namespace {
+
+constexpr int GT = 256;
+constexpr int MAXP = 512;
+
+__global__ void __launch_bounds__(GT) k_gal_fft(ClassDev c, const float* __restrict__ Pp,
+                                                int phase) {
+  __shared__ float cw[MAXP], sw[MAXP];
+  __shared__ int need[7];
+  __shared__ int is_gal;
+  const int tid = threadIdx.x;
+  const int T = c.T, PP = c.fft_P, H = PP / 2 + 1, msk = PP - 1;
+  const int TT = T * T;
+  for (int m = tid; m < PP; m += GT) {
+    double sn, cs;
+    sincospi(2.0 * (double)m / (double)PP, &sn, &cs);
+    cw[m] = (float)cs;
+    sw[m] = (float)sn;
+  }
+  float* ws = c.gfft_ws + (size_t)blockIdx.x * c.gfft_floats;
+  float* img = ws;                          // 3 real T x T: psf, psf_x, psf_y
+  float* R = img + 3 * TT;                  // row transform, T x H complex
+  float* X = R + 2 * (size_t)T * H;         // 3 spectra, P x H complex
+  float* Fs = X + 6 * (size_t)PP * H;       // F, F1, dF, P x H real
+  float* Cc = Fs + 3 * (size_t)PP * H;      // inverse column pass, T x H complex
+  const size_t PH = (size_t)PP * H;
+  const int nitems = c.n_isl * c.nb * c.N;
+  const bool lin = phase == PH_LIN;
+  for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
+    const int k = item % c.N;
+    const int b = (item / c.N) % c.nb;
+    const int isl = item / (c.N * c.nb);
+    __syncthreads();
+    if (tid == 0) {
+      is_gal = isl_active(c.flags[isl], phase) && c.mmask[isl * c.N + k] &&
+               c.stype[isl * c.N + k] != 0;
+      const uint8_t* kp = c.keep + ((size_t)isl * c.N + k) * 6;
+      need[0] = 1;
+      need[1] = lin && kp[0] && c.psf_varies;
+      need[2] = lin && kp[1] && c.psf_varies;
+      for (int q = 0; q < 3; ++q) need[3 + q] = lin && kp[2 + q];
+      need[6] = lin && kp[5];
+    }
+    __syncthreads();
+    if (!is_gal) continue;
+    const MemberRecord* rec = c.mrec + ((size_t)isl * c.nb + b) * c.N + k;
+    // ---- PSF stamp at the member position and its position partials ----
+    for (int e = tid; e < TT; e += GT) {
+      const int i = e / T, j = e - (e / T) * T;
+      const float* cf = c.psf_coefs + (((size_t)b * T + i) * T + j) * c.nt;
+      float v0 = 0.f, v1 = 0.f, v2 = 0.f;
+      for (int tt = 0; tt < c.nt; ++tt) {
+        const float cv = cf[tt];
+        v0 = fmaf(cv, rec->beta[tt], v0);
+        v1 = fmaf(cv, rec->betax[tt], v1);
+        v2 = fmaf(cv, rec->betay[tt], v2);
+      }
+      img[e] = v0;
+      img[TT + e] = v1;
+      img[2 * TT + e] = v2;
+    }
+    __syncthreads();
+    // ---- forward transforms of the zero-padded images ----
+    for (int im = 0; im < 3; ++im) {
+      if (!need[im]) continue;
+      const float* a = img + im * TT;
+      for (int e = tid; e < T * H; e += GT) {
+        const int i = e / H, u = e - (e / H) * H;
+        float re = 0.f, imv = 0.f;
+        for (int j = 0; j < T; ++j) {
+          const int m = (j * u) & msk;
+          const float v = a[i * T + j];
+          re = fmaf(v, cw[m], re);
+          imv = fmaf(-v, sw[m], imv);
+        }
+        R[2 * e] = re;
+        R[2 * e + 1] = imv;
+      }
+      __syncthreads();
+      float* Xi = X + 2 * PH * im;
+      for (int e = tid; e < (int)PH; e += GT) {
+        const int w = e / H, u = e - (e / H) * H;
+        float re = 0.f, imv = 0.f;
+        for (int i = 0; i < T; ++i) {
+          const int m = (i * w) & msk;
+          const float ar = R[2 * (i * H + u)], ai = R[2 * (i * H + u) + 1];
+          // (ar + i ai)(cos - i sin)
+          re = fmaf(ar, cw[m], fmaf(ai, sw[m], re));
+          imv = fmaf(ai, cw[m], fmaf(-ar, sw[m], imv));
+        }
+        Xi[2 * e] = re;
+        Xi[2 * e + 1] = imv;
+      }
+      __syncthreads();
+    }
+    // ---- the mixture's transform and its partials on the grid ----
+    const double kk = -2.0 * 9.869604401089358;   // -2 pi^2
+    for (int e = tid; e < (int)PH; e += GT) {
+      const int w = e / H, u = e - (e / H) * H;
+      const double nu = (double)u / PP;
+      const double nw = (double)(w < PP / 2 ? w : w - PP) / PP;
+      const double ex = kk * ((double)rec->cg[0] * nu * nu + (double)rec->cg[1] * nw * nw +
+                              2.0 * (double)rec->cg[2] * nu * nw);
+      double F = 0.0, F1 = 0.0, dF = 0.0;
+      for (int g = 0; g < rec->ngal; ++g) {
+        const double E = exp(rec->gv[g] * ex);
+        F += rec->ga[g] * E;
+        F1 += rec->ga[g] * rec->gv[g] * E;
+        dF += (rec->gda[g] + rec->ga[g] * rec->gdv[g] * ex) * E;
+      }
+      Fs[e] = (float)F;
+      Fs[PH + e] = (float)F1;
+      Fs[2 * PH + e] = (float)dF;
+    }
+    __syncthreads();
+    // ---- inverse transforms of the needed products, cropped to T x T ----
+    const double inv = 1.0 / ((double)PP * (double)PP);
+    float* out = c.gstamp + (size_t)item * 7 * TT;
+    for (int s = 0; s < 7; ++s) {
+      if (!need[s]) continue;
+      const float* Xb = X + 2 * PH * (s < 3 ? s : 0);
+      const float* fac = Fs + PH * (s < 3 ? 0 : (s < 6 ? 1 : 2));
+      float dc0 = 0.f, dc1 = 0.f, dc2 = 0.f;
+      if (s >= 3 && s < 6) {
+        dc0 = rec->dcov[s - 3][0];
+        dc1 = rec->dcov[s - 3][1];
+        dc2 = rec->dcov[s - 3][2];
+      }
+      for (int e = tid; e < T * H; e += GT) {
+        const int i = e / H, u = e - (e / H) * H;
+        const float nu = (float)u / (float)PP;
+        float re = 0.f, imv = 0.f;
+        for (int w = 0; w < PP; ++w) {
+          float f = fac[w * H + u];
+          if (s >= 3 && s < 6) {
+            const float nw = (float)(w < PP / 2 ? w : w - PP) / (float)PP;
+            f *= (float)kk * (dc0 * nu * nu + dc1 * nw * nw + 2.f * dc2 * nu * nw);
+          }
+          const float ar = f * Xb[2 * (w * H + u)], ai = f * Xb[2 * (w * H + u) + 1];
+          const int m = (i * w) & msk;
+          // (ar + i ai)(cos + i sin)
+          re = fmaf(ar, cw[m], fmaf(-ai, sw[m], re));
+          imv = fmaf(ai, cw[m], fmaf(ar, sw[m], imv));
+        }
+        Cc[2 * e] = re;
+        Cc[2 * e + 1] = imv;
+      }
+      __syncthreads();
+      for (int e = tid; e < TT; e += GT) {
+        const int i = e / T, j = e - (e / T) * T;
+        const float* ci = Cc + 2 * (size_t)i * H;
+        float v = ci[0] + ((j & 1) ? -ci[2 * (H - 1)] : ci[2 * (H - 1)]);
+        float acc = 0.f;
+        for (int u = 1; u < H - 1; ++u) {
+          const int m = (j * u) & msk;
+          acc = fmaf(ci[2 * u], cw[m], fmaf(-ci[2 * u + 1], sw[m], acc));
+        }
+        double r = ((double)v + 2.0 * (double)acc) * inv;
+        if (s == 0) r += rec->gcore * (double)img[e];
+        else if (s == 1) r += rec->gcore * (double)img[TT + e];
+        else if (s == 2) r += rec->gcore * (double)img[2 * TT + e];
+        else if (s == 6) r = (r + rec->gdcore * (double)img[e]) * (double)rec->dndu;
+        out[(size_t)s * TT + e] = (float)r;
+      }
+      __syncthreads();
+    }
+  }
+}
+
+}  // namespace
+
+int fft_pad_for(int T) {
+  int n = 1;
+  while (n < T + T / 2) n <<= 1;
+  return n;
+}
+
+size_t gal_fft_floats(int T, int P) {
+  const size_t H = (size_t)P / 2 + 1;
+  const size_t f = 3 * (size_t)T * T + 4 * (size_t)T * H + 9 * (size_t)P * H;
+  return (f + 63) & ~(size_t)63;
+}
+
+void launch_gal_fft(const ClassDev& c, const float* P, int phase, cudaStream_t s) {
+  if (c.gfft_ctas > 0) k_gal_fft<<<(unsigned)c.gfft_ctas, GT, 0, s>>>(c, P, phase);
+}

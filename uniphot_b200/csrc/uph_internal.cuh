@@ -60,6 +60,13 @@ struct MemberRecord {
   float dndu;
   int ncomp;
   GComp comps[UPH_MAXKPSF * UPH_MAXGAL];
+  // reference render mode, galaxies: the Sersic mixture at the member's
+  // index (amplitude, variance in units of the galaxy covariance, their
+  // derivatives in n; the zero-variance core apart), for the Fourier-
+  // domain convolution with the pixelised PSF
+  int ngal;
+  double ga[UPH_MAXGAL], gv[UPH_MAXGAL], gda[UPH_MAXGAL], gdv[UPH_MAXGAL];
+  double gcore, gdcore;
 };
 
 struct ClassDev {
@@ -165,6 +172,15 @@ struct ClassDev {
   float* reprof;
   float* resid;
   float* resid_w;
+  // reference render mode with galaxies: the unshifted galaxy stamp and its
+  // partials (S, Sx, Sy, S_lr, S_e1, S_e2, S_u) per (island, band, member),
+  // (n_isl, nb, N, 7, T, T), from the Fourier-domain convolution; its work
+  // space per resident CTA (gfft_ctas of gfft_floats floats); the pad size
+  int fft_P;
+  int gfft_ctas;
+  size_t gfft_floats;
+  float* gstamp;
+  float* gfft_ws;
   float* bgout;            // (n_isl, nb, 3) final background coefficients
   float* bgerr;            // (n_isl, nb, 3) and their errors
   float* fcur;
@@ -299,6 +315,9 @@ __device__ __forceinline__ size_t stamp_slot(const ClassDev& c, int isl, int b,
 // Kernel launch wrappers (defined in the .cu units).
 void launch_render(const ClassDev& c, const float* P, int phase,
                    cudaStream_t s);
+int fft_pad_for(int T);
+size_t gal_fft_floats(int T, int P);
+void launch_gal_fft(const ClassDev& c, const float* P, int phase, cudaStream_t s);
 void launch_gram_lin(const ClassDev& c, cudaStream_t s);
 void launch_assemble(const ClassDev& c, cudaStream_t s);
 void launch_gram_trial(const ClassDev& c, const float* P, int phase,

@@ -278,7 +278,8 @@ k_member_setup(ClassDev c, const float* __restrict__ P, int phase) {
     }
     rec->dndu = 0.f;
     rec->ncomp = 0;
-    if (c.mode == 1 && is_gal) {
+    rec->ngal = 0;
+    if (is_gal) {
       const float* pk = P + (size_t)isl * c.nP + 6 * k;
       double n;
       if (c.free_n[isl * c.N + k]) {
@@ -338,7 +339,29 @@ k_member_setup(ClassDev c, const float* __restrict__ P, int phase) {
     }
   }
   __syncthreads();
-  if (c.mode != 1) return;
+  if (c.mode != 1) {
+    // reference mode: the galaxy's Sersic mixture for the Fourier-domain
+    // convolution (sersic_mog.py:81-100), core apart
+    if (!is_gal) return;
+    const int g = tid;
+    if (g < c.tb_k) {
+      const int seg = sc.seg;
+      const double t = sc.t, dt = sc.dt;
+      const double a0 = c.tb_amps[seg * c.tb_k + g], a1 = c.tb_amps[(seg + 1) * c.tb_k + g];
+      const double l0 = c.tb_lv[seg * c.tb_k + g], l1 = c.tb_lv[(seg + 1) * c.tb_k + g];
+      const double v = exp((1 - t) * l0 + t * l1);
+      rec->ga[g] = (1 - t) * a0 + t * a1;
+      rec->gv[g] = v;
+      rec->gda[g] = dt * (a1 - a0);
+      rec->gdv[g] = v * dt * (l1 - l0);
+    } else if (g == c.tb_k) {
+      const int seg = sc.seg;
+      rec->gcore = (1 - sc.t) * c.tb_core[seg] + sc.t * c.tb_core[seg + 1];
+      rec->gdcore = sc.dt * (c.tb_core[seg + 1] - c.tb_core[seg]);
+      rec->ngal = c.tb_k;
+    }
+    return;
+  }
   if (tid == 0) {
     double W = 0, Wx = 0, Wy = 0;
     for (int q = 0; q < c.kpsf; ++q) {
@@ -580,7 +603,20 @@ k_render(ClassDev c, const float* __restrict__ P, int phase, int nsa) {
 
   // ---- un-shifted stamp (and partials) on the halo region ----
   const int nh = hr * hc;
-  if (c.mode == 0) {
+  if (c.mode == 0 && ms.is_gal) {
+    // reference-mode galaxy: the unshifted rows from the Fourier-domain
+    // convolution (k_gal_fft)
+    const float* gs = c.gstamp + (((size_t)isl * c.nb + b) * c.N + k) * 7 * (size_t)(T * T);
+    for (int e = tid; e < nh; e += blockDim.x) {
+      const int r = e / hc, cc = e % hc;
+      const int si = si0 - 3 + r, sj = sj0 - 3 + cc;
+      const bool ok = si >= 0 && si < T && sj >= 0 && sj < T;
+      const size_t o = (size_t)si * T + sj;
+      for (int q = 0; q < NS; ++q)
+        if (q == 0 || ms.need[q])
+          S[(q * UPH_HALO + r) * HP + cc] = ok ? gs[(size_t)q * T * T + o] : 0.f;
+    }
+  } else if (c.mode == 0) {
     for (int e = tid; e < nh; e += blockDim.x) {
       const int r = e / hc, cc = e % hc;
       const int si = si0 - 3 + r, sj = sj0 - 3 + cc;
@@ -747,6 +783,7 @@ void launch_render(const ClassDev& c, const float* P, int phase,
   const int nsa = render_arrays(c, phase);
   const size_t bytes = sizeof(float) * (size_t)nsa * UPH_HALO * HP;
   k_member_setup<<<(unsigned)((long long)c.n_isl * c.nb * c.N), 128, 0, s>>>(c, P, phase);
+  if (c.mode == 0 && c.gstamp) launch_gal_fft(c, P, phase, s);
   if (phase == PH_LIN)
     k_render<true><<<(unsigned)nblk, 256, bytes, s>>>(c, P, phase, nsa);
   else

@@ -347,15 +347,19 @@ def run_class_chunk_resilient(kernels, psf_tree, host, rows, width, max_steps,
         return merged
 
 
-def _chunk_size(plan, n_bands: int, budget_bytes: float) -> int:
+def _chunk_size(plan, n_bands: int, budget_bytes: float,
+                fft_galaxies: bool = False) -> int:
     """Islands per chunk under a device scratch budget (stamps, Gram, GN
-    blocks dominate)."""
+    blocks dominate; reference-mode galaxies add their unshifted Fourier
+    rows, 7 T x T per member and band)."""
     N, B, T = int(plan.nsrc_class), int(plan.bbox_class), int(plan.tier)
     Sz = min(T, B)
     R = 7 if plan.kind == "mixed" else 3
     nL = N * (6 if plan.kind == "mixed" else 2)
     K = nL + N + 1
     per = 4.0 * n_bands * (N * R * Sz * Sz + K * K + nL * nL + nL) + 8.0 * nL * nL
+    if fft_galaxies and plan.kind == "mixed":
+        per += 4.0 * n_bands * N * 7 * T * T
     return int(max(1, min(plan.n_islands, budget_bytes // max(per, 1.0))))
 
 
@@ -527,7 +531,8 @@ class IslandFitJob:
             kern.desc.source_metrics = int(bool(compute_source_metrics))
             kern.desc.re_profile = int(bool(compute_re_profile))
             kern.desc.residual = int(bool(return_island_residual))
-            chunk = _chunk_size(plan, n_bands, chunk_budget_bytes)
+            chunk = _chunk_size(plan, n_bands, chunk_budget_bytes,
+                                fft_galaxies=render_mode == "reference")
             ids = []
             for lo in range(0, plan.n_islands, chunk):
                 rows = np.arange(lo, min(lo + chunk, plan.n_islands))
