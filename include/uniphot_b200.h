@@ -309,6 +309,49 @@ int uph_job_kernel_work(const uph_job* job, int32_t kind, double* bytes,
  * chunk's work (its LM iterations, probes and final pass), in ms. */
 int uph_job_chunk_time(const uph_job* job, int32_t chunk_id, float* ms);
 
+/* ---- Per-grid sparse forced photometry of one band ----------------------
+ * Replaces solve_band_sparse (forced_phot_sparse.py:690-718, solver_inner
+ * :498-555, assemble_and_solve :443-496) for point sources: every source's
+ * PSF stamp at its fixed full-image position (psf_polynomial.py:134-197),
+ * renormalised to unit sum when `renorm`, Lanczos-3 shifted by the
+ * fractional grid-local position and placed at rint - half the stamp; the
+ * weighted normal matrix of stamps and the polynomial background (order 0,
+ * 1, 2: 1, 3, 6 terms X^m Y^n, X = (full-image x - x_origin) / x_scale),
+ * stamp-overlap pairs taken from the caller's neighbour list
+ * (build_neighbor_list, :272-330) and scatter-added; ridge
+ * reg * max(|diag|, 1e-30) per diagonal element; a float64 solve and the
+ * diagonal of the inverse.  Host arrays in and out. */
+typedef struct uph_sparse_band {
+  int32_t band_h, band_w;
+  const float* data;          /* [band_h*band_w]                             */
+  const float* invvar;        /* [band_h*band_w]                             */
+  const uint8_t* pix_good;    /* [band_h*band_w] 0 = masked                  */
+  int32_t n_sources;
+  const float* pos_x;         /* [n] full-image pixel coordinates            */
+  const float* pos_y;
+  int32_t grid_x0, grid_y0;   /* this grid's top-left in the full image      */
+  const float* psf_coefs;     /* [psf_h*psf_w*psf_nterms]                    */
+  int32_t psf_h, psf_w, psf_nterms;
+  float psf_x_origin, psf_x_scale, psf_y_origin, psf_y_scale;
+  int32_t renorm;             /* 1: unit-sum stamps (the reference default)  */
+  double bg_x_origin, bg_x_scale, bg_y_origin, bg_y_scale;
+  int32_t bg_order;           /* 0, 1 or 2                                   */
+  int32_t k_max;
+  const int32_t* neighbor_idx;   /* [n*k_max], -1 where unused            */
+  const uint8_t* neighbor_mask;  /* [n*k_max]                              */
+  float reg;
+} uph_sparse_band;
+
+typedef struct uph_sparse_out {
+  float* fluxes;      /* [n]                                                  */
+  float* bg_coefs;    /* [M]                                                  */
+  float* flux_var;    /* [n] diagonal of the inverse normal matrix            */
+  float* bg_var;      /* [M]                                                  */
+  int32_t converged;  /* 1 when every flux and coefficient is finite          */
+} uph_sparse_out;
+
+int uph_sparse_band_solve(uph_ctx* ctx, const uph_sparse_band* in, uph_sparse_out* out);
+
 /* ---- Allocation-free final-flux pass.  No counterpart in the reference:
  * it exists for callers that cannot call cudaMalloc (a host inside a
  * framework that owns the device memory pool, or a serving process that

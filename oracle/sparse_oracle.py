@@ -1,0 +1,126 @@
+"""CPU restatement of the reference's per-grid sparse forced photometry for
+point sources (test infrastructure only: the checker of
+``uph_sparse_band_solve``; nothing in ``uniphot_b200`` imports it).
+
+Follows ``tract7dt/fit/grid_gpu/forced_phot_sparse.py``:
+
+* stamps: the polynomial PSF at each source's full-image position
+  (``psf_polynomial.py:134-197``), renormalised to unit sum, Lanczos-3
+  shifted by the fractional grid-local position (``:126-170``,
+  ``lanczos.py:50-181``), placed at ``stamp_top_left`` (``:255-269``);
+* ``solver_inner`` (``:498-555``): per-source diagonal, data and background
+  couplings under the stamp (``per_source_self_blocks``, ``:355-376``),
+  stamp-overlap pairs from the neighbour list (``per_pair_overlap``,
+  ``:378-405``), the background Gram over the whole grid (``:417-441``);
+* ``assemble_and_solve`` (``:443-496``): scatter-add of the pairs, element-
+  wise ridge ``reg |diag|``, float64 solve and the diagonal of the inverse.
+
+Arithmetic: float32 stamps and products with float64 sums rounded to
+float32 (the reference sums float32 on the device), float64 solve.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+
+from .island_oracle import correlate_x, correlate_y, lanczos3_taps, poly_basis
+
+_TERMS = {0: ((0, 0),), 1: ((0, 0), (1, 0), (0, 1)),
+          2: ((0, 0), (1, 0), (0, 1), (2, 0), (1, 1), (0, 2))}
+
+
+def stamps(psf, pos_x, pos_y, grid_x0, grid_y0, renorm=True):
+    """(n, H, W) float32 Lanczos-shifted unit-sum PSF stamps."""
+    f32 = np.float32
+    coefs = np.asarray(psf.coefs, np.float32)
+    nt = coefs.shape[-1]
+    out = []
+    for x, y in zip(np.asarray(pos_x, np.float32), np.asarray(pos_y, np.float32)):
+        X = float(f32((f32(x) - f32(psf.x_origin)) / f32(psf.x_scale)))
+        Y = float(f32((f32(y) - f32(psf.y_origin)) / f32(psf.y_scale)))
+        b, _, _ = poly_basis(X, Y, nt)
+        raw = (coefs.astype(np.float64) @ b).astype(np.float32)
+        if renorm:
+            raw = (raw / np.float32(max(float(raw.astype(np.float64).sum()), 1e-12))
+                   ).astype(np.float32)
+        xg = f32(f32(x) - f32(grid_x0))
+        yg = f32(f32(y) - f32(grid_y0))
+        dx = float(f32(xg - np.rint(xg)))
+        dy = float(f32(yg - np.rint(yg)))
+        Lx = lanczos3_taps(dx)[0].astype(np.float32)
+        Ly = lanczos3_taps(dy)[0].astype(np.float32)
+        out.append(correlate_y(correlate_x(raw, Lx), Ly).astype(np.float32))
+    return np.stack(out)
+
+
+def bg_basis(h, w, x0, y0, xo, xs, yo, ys, order):
+    X = (np.arange(w, dtype=np.float64) + x0 - xo) / xs
+    Y = (np.arange(h, dtype=np.float64) + y0 - yo) / ys
+    return np.stack([(X[None, :] ** m * Y[:, None] ** n) for m, n in _TERMS[order]],
+                    axis=-1).astype(np.float32)        # (h, w, M)
+
+
+def solve_band(data, invvar, pix_good, pos_x, pos_y, psf, grid_x0, grid_y0,
+               bg_norm, order, nbr_idx, nbr_mask, reg=1e-9, renorm=True):
+    """(fluxes, bg_coefs, flux_var, bg_var) of one band, float32."""
+    h, w = data.shape
+    S = stamps(psf, pos_x, pos_y, grid_x0, grid_y0, renorm)
+    n, H, W = S.shape
+    x = np.asarray(pos_x, np.float32) - np.float32(grid_x0)
+    y = np.asarray(pos_y, np.float32) - np.float32(grid_y0)
+    ixt = np.rint(x).astype(np.int64) - W // 2
+    iyt = np.rint(y).astype(np.int64) - H // 2
+    wg = np.where(pix_good, invvar, 0.0).astype(np.float32)
+    Bg = bg_basis(h, w, grid_x0, grid_y0, *bg_norm, order)
+    M = Bg.shape[-1]
+    # values under each stamp (zero outside the grid)
+    ky = np.arange(H)[:, None]
+    kx = np.arange(W)[None, :]
+    Wu = np.zeros((n, H, W), np.float32)
+    Du = np.zeros((n, H, W), np.float32)
+    Bu = np.zeros((n, H, W, M), np.float32)
+    Se = np.zeros_like(S)
+    for s in range(n):
+        ys_, xs_ = iyt[s] + ky, ixt[s] + kx
+        inb = (ys_ >= 0) & (ys_ < h) & (xs_ >= 0) & (xs_ < w)
+        yc, xc = np.clip(ys_, 0, h - 1), np.clip(xs_, 0, w - 1)
+        Wu[s] = np.where(inb, wg[yc, xc], 0.0)
+        Du[s] = data[yc, xc]
+        Bu[s] = Bg[yc, xc]
+        Se[s] = np.where(inb, S[s], 0.0)
+    ws = (Wu * Se).astype(np.float32)
+    f64 = np.float64
+    diag = (ws.astype(f64) * Se).sum(axis=(1, 2)).astype(np.float32)
+    tWd = (ws.astype(f64) * Du).sum(axis=(1, 2)).astype(np.float32)
+    tWB = (ws[..., None].astype(f64) * Bu).sum(axis=(1, 2)).astype(np.float32)
+    k_max = nbr_idx.shape[1]
+    off = np.zeros((n, k_max), np.float32)
+    for s in range(n):
+        for k in range(k_max):
+            if not nbr_mask[s, k]:
+                continue
+            t = int(nbr_idx[s, k])
+            di, dj = iyt[s] - iyt[t], ixt[s] - ixt[t]
+            tky, tkx = ky + di, kx + dj
+            inn = (tky >= 0) & (tky < H) & (tkx >= 0) & (tkx < W)
+            st = np.where(inn, Se[t][np.clip(tky, 0, H - 1), np.clip(tkx, 0, W - 1)], 0.0)
+            off[s, k] = f64((Wu[s].astype(f64) * Se[s] * st).sum())
+    bw = (Bg.reshape(-1, M) * wg.reshape(-1, 1)).astype(np.float32)
+    BtWB = (bw.T.astype(f64) @ Bg.reshape(-1, M)).astype(np.float32)
+    BtWd = (bw.T.astype(f64) @ data.reshape(-1).astype(f64)).astype(np.float32)
+    A = np.zeros((n + M, n + M), np.float32)
+    A[np.arange(n), np.arange(n)] = diag
+    for s in range(n):
+        for k in range(k_max):
+            if nbr_mask[s, k]:
+                A[s, int(nbr_idx[s, k])] += off[s, k]
+    A[:n, n:] = tWB
+    A[n:, :n] = tWB.T
+    A[n:, n:] = BtWB
+    b = np.concatenate([tWd, BtWd])
+    d = np.diag(A).copy()
+    A = A + np.diag((np.float32(reg) * np.maximum(np.abs(d), np.float32(1e-30))).astype(np.float32))
+    A64 = A.astype(f64)
+    xs = np.linalg.solve(A64, b.astype(f64)).astype(np.float32)
+    var = np.diag(np.linalg.inv(A64)).astype(np.float32)
+    return xs[:n], xs[n:], var[:n], var[n:]

@@ -8,12 +8,14 @@ checkout, bypassing the package ``__init__`` which needs matplotlib):
 * ``tract7dt/fit/grid_gpu/island_plan.py`` -- class planning, host arrays,
   free-n gate;
 * ``tract7dt/fit/grid_gpu/psf_polynomial.py`` -- numpy PSF stamp evaluation;
-* ``tract7dt/fit/grid_gpu/sersic_mog.py`` -- the table loader.
+* ``tract7dt/fit/grid_gpu/sersic_mog.py`` -- the table loader;
+* ``tract7dt/fit/grid_gpu/bg_polynomial.py`` -- the grid background basis.
 
 Inputs are the seeded synthetic catalogs of ``uniphot_b200.synth``.  Output:
-``tests/golden/*.npz``.  Usage::
+``tests/golden/*.npz``.  Usage (optionally naming the fixtures to write:
+plan, psf, table, bg_basis)::
 
-    python tests/golden/make_golden.py /root/reference
+    python tests/golden/make_golden.py /root/reference [fixture ...]
 """
 
 from __future__ import annotations
@@ -133,19 +135,40 @@ def table_fixture(ref):
     return out
 
 
-def main(ref_root):
+def bg_basis_fixture(ref):
+    """The grid background basis at orders 0-2 on a few grid geometries."""
+    bp = ref["bg_polynomial"]
+    out = {}
+    cases = [(37, 53, 0, 0, 1024.0, 1024.0, 1024.0, 1024.0),
+             (41, 29, 300, 1700, 1000.5, 950.0, 1020.25, 990.0),
+             (64, 64, 2048, 512, 2047.5, 2048.0, 2047.5, 2048.0)]
+    for ci, (h, w, x0, y0, xo, xs, yo, ys) in enumerate(cases):
+        out[f"case{ci}_geom"] = np.array([h, w, x0, y0, xo, xs, yo, ys], np.float64)
+        for order in (0, 1, 2):
+            out[f"case{ci}_o{order}"] = bp.make_bg_basis(h, w, x0, y0, xo, xs, yo, ys,
+                                                         order=order)
+    return out
+
+
+def main(ref_root, which=None):
     ref = load_reference(ref_root)
-    for seed in (0, 1):
-        f = catalog_small(seed)
-        np.savez_compressed(HERE / f"plan_small_s{seed}.npz",
-                            **planning_fixture(ref, f, 55, "fof", (111, 221)))
-    f = catalog_field(3)
-    np.savez_compressed(HERE / "plan_field_s3.npz",
-                        **planning_fixture(ref, f, 31, "flux", (111, 221)))
-    np.savez_compressed(HERE / "psf_poly_eval.npz", **psf_fixture(ref))
-    np.savez_compressed(HERE / "sersic_table_ref.npz", **table_fixture(ref))
+    want = set(which or ("plan", "psf", "table", "bg_basis"))
+    if "plan" in want:
+        for seed in (0, 1):
+            f = catalog_small(seed)
+            np.savez_compressed(HERE / f"plan_small_s{seed}.npz",
+                                **planning_fixture(ref, f, 55, "fof", (111, 221)))
+        f = catalog_field(3)
+        np.savez_compressed(HERE / "plan_field_s3.npz",
+                            **planning_fixture(ref, f, 31, "flux", (111, 221)))
+    if "psf" in want:
+        np.savez_compressed(HERE / "psf_poly_eval.npz", **psf_fixture(ref))
+    if "table" in want:
+        np.savez_compressed(HERE / "sersic_table_ref.npz", **table_fixture(ref))
+    if "bg_basis" in want:
+        np.savez_compressed(HERE / "bg_basis_ref.npz", **bg_basis_fixture(ref))
     print("golden fixtures written to", HERE)
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference", sys.argv[2:] or None)

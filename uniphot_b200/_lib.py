@@ -26,7 +26,7 @@ EXPORTED = ("uph_create", "uph_destroy", "uph_last_error", "uph_set_stream",
             "uph_last_launch_count", "uph_job_create", "uph_job_destroy",
             "uph_job_add_chunk", "uph_job_solve", "uph_job_read",
             "uph_job_set_profile", "uph_job_kernel_time", "uph_job_kernel_work",
-            "uph_job_chunk_time")
+            "uph_job_chunk_time", "uph_sparse_band_solve")
 KERNEL_KINDS = ("render", "gram", "assemble", "step", "trial_chi2", "accept",
                 "gram_tc")
 
@@ -64,6 +64,26 @@ class ChunkOut(C.Structure):
          ("prej", _P), ("railed", _P), ("perr", _P), ("femarg", _P),
          ("smetrics", _P), ("swin", _P), ("reprof", _P), ("resid", _P),
          ("resid_w", _P)]
+
+
+class SparseBand(C.Structure):
+    _fields_ = [("band_h", C.c_int32), ("band_w", C.c_int32), ("data", _P),
+                ("invvar", _P), ("pix_good", _P), ("n_sources", C.c_int32),
+                ("pos_x", _P), ("pos_y", _P), ("grid_x0", C.c_int32),
+                ("grid_y0", C.c_int32), ("psf_coefs", _P), ("psf_h", C.c_int32),
+                ("psf_w", C.c_int32), ("psf_nterms", C.c_int32),
+                ("psf_x_origin", C.c_float), ("psf_x_scale", C.c_float),
+                ("psf_y_origin", C.c_float), ("psf_y_scale", C.c_float),
+                ("renorm", C.c_int32), ("bg_x_origin", C.c_double),
+                ("bg_x_scale", C.c_double), ("bg_y_origin", C.c_double),
+                ("bg_y_scale", C.c_double), ("bg_order", C.c_int32),
+                ("k_max", C.c_int32), ("neighbor_idx", _P), ("neighbor_mask", _P),
+                ("reg", C.c_float)]
+
+
+class SparseOut(C.Structure):
+    _fields_ = [("fluxes", _P), ("bg_coefs", _P), ("flux_var", _P), ("bg_var", _P),
+                ("converged", C.c_int32)]
 
 
 class UphError(RuntimeError):
@@ -113,6 +133,7 @@ def lib():
         L.uph_job_kernel_work.argtypes = [_P, C.c_int32, C.POINTER(C.c_double),
                                           C.POINTER(C.c_double)]
         L.uph_job_chunk_time.argtypes = [_P, C.c_int32, C.POINTER(C.c_float)]
+        L.uph_sparse_band_solve.argtypes = [_P, C.POINTER(SparseBand), C.POINTER(SparseOut)]
         _lib = L
     return _lib
 
@@ -172,6 +193,46 @@ class Context:
         nb, Hp, Wp = d.shape
         self.check(lib().uph_upload_field(self._h, ptr(d), ptr(w), nb, Hp, Wp, int(pad)),
                    "uph_upload_field")
+
+    def sparse_band_solve(self, inputs, nbr_idx, nbr_mask, reg: float, order: int, M: int):
+        """One band of one grid through uph_sparse_band_solve; returns a
+        ``uniphot_b200.sparse.SparseForcedPhotResult``."""
+        from .sparse import SparseForcedPhotResult
+        h, w = int(inputs.band_h), int(inputs.band_w)
+        d = np.ascontiguousarray(np.asarray(inputs.data, np.float32).reshape(h, w))
+        iv = np.ascontiguousarray(np.asarray(inputs.invvar, np.float32).reshape(h, w))
+        gd = np.ascontiguousarray(np.asarray(inputs.pix_good).astype(np.uint8).reshape(h, w))
+        px = np.ascontiguousarray(inputs.pos_x, np.float32)
+        py = np.ascontiguousarray(inputs.pos_y, np.float32)
+        n = int(px.size)
+        psf = inputs.psf
+        cf = np.ascontiguousarray(psf.coefs, np.float32)
+        H, W, nterms = cf.shape
+        kmax = int(nbr_idx.shape[1]) if nbr_idx.ndim == 2 else 0
+        ni = np.ascontiguousarray(nbr_idx, np.int32)
+        nm = np.ascontiguousarray(nbr_mask).astype(np.uint8)
+        ib = SparseBand(band_h=h, band_w=w, data=ptr(d), invvar=ptr(iv), pix_good=ptr(gd),
+                        n_sources=n, pos_x=ptr(px), pos_y=ptr(py),
+                        grid_x0=int(inputs.grid_x0), grid_y0=int(inputs.grid_y0),
+                        psf_coefs=ptr(cf), psf_h=H, psf_w=W, psf_nterms=nterms,
+                        psf_x_origin=float(psf.x_origin), psf_x_scale=float(psf.x_scale),
+                        psf_y_origin=float(psf.y_origin), psf_y_scale=float(psf.y_scale),
+                        renorm=int(bool(getattr(inputs, "renorm", True))),
+                        bg_x_origin=float(inputs.bg_x_origin),
+                        bg_x_scale=float(inputs.bg_x_scale),
+                        bg_y_origin=float(inputs.bg_y_origin),
+                        bg_y_scale=float(inputs.bg_y_scale), bg_order=int(order),
+                        k_max=kmax, neighbor_idx=ptr(ni), neighbor_mask=ptr(nm),
+                        reg=float(reg))
+        fl = np.zeros(n, np.float32)
+        fv = np.zeros(n, np.float32)
+        bg = np.zeros(M, np.float32)
+        bv = np.zeros(M, np.float32)
+        ob = SparseOut(fluxes=ptr(fl), bg_coefs=ptr(bg), flux_var=ptr(fv), bg_var=ptr(bv))
+        self.check(lib().uph_sparse_band_solve(self._h, C.byref(ib), C.byref(ob)),
+                   "uph_sparse_band_solve")
+        return SparseForcedPhotResult(fluxes=fl, bg_coefs=bg, flux_var=fv, bg_var=bv,
+                                      converged=bool(ob.converged))
 
     def upload_field_unpadded(self, data: np.ndarray, invvar: np.ndarray, pad: int):
         d = np.ascontiguousarray(data, np.float32)
@@ -347,7 +408,7 @@ class Job:
         """ms from the start of the last solve to the end of one chunk."""
         ms = C.c_float(0)
         self.ctx.check(lib().uph_job_chunk_time(self._h, int(chunk_id), C.byref(ms)),
-                       "uph_job_chunk_time")
+                       "uph_job_chunk_time", "uph_sparse_band_solve")
         return float(ms.value)
 
     def kernel_work(self) -> dict:

@@ -57,6 +57,7 @@ struct PolyPsf {
 
 struct uph_ctx {
   int device = 0;
+  DevBuf sp[24];   // sparse grid solve: inputs, per-source work, the system
   cudaStream_t stream = nullptr;
   bool own_stream = false;
   std::string err;
@@ -164,7 +165,8 @@ int uph_create(int device, uph_ctx** out) {
     return UPH_ERR_CUDA;
   }
   ctx->own_stream = true;
-  if (uph_render_setup() != 0 || uph_solve_setup() != 0 || uph_gram_tc_setup() != 0) {
+  if (uph_render_setup() != 0 || uph_solve_setup() != 0 || uph_gram_tc_setup() != 0 ||
+      sparse_setup() != 0) {
     cudaStreamDestroy(ctx->stream);
     delete ctx;
     return UPH_ERR_CUDA;
@@ -195,6 +197,7 @@ int uph_destroy(uph_ctx* ctx) {
   ctx->tb_amps.release();
   ctx->tb_lv.release();
   ctx->tb_core.release();
+  for (auto& b : ctx->sp) b.release();
   for (auto& ev : ctx->ev)
     if (ev) cudaEventDestroy(ev);
   if (ctx->h_active) cudaFreeHost(ctx->h_active);
@@ -1293,6 +1296,118 @@ int uph_job_kernel_time(const uph_job* job, int32_t kind, float* ms,
   if (!job || kind < 0 || kind >= WK_KINDS) return UPH_ERR_INVALID;
   if (ms) *ms = job->ktime[kind];
   if (launches) *launches = job->kcount[kind];
+  return UPH_OK;
+}
+
+int uph_sparse_band_solve(uph_ctx* ctx, const uph_sparse_band* in, uph_sparse_out* out) {
+  if (!ctx || !in || !out) return UPH_ERR_INVALID;
+  const int n = in->n_sources, H = in->psf_h, W = in->psf_w, h = in->band_h, w = in->band_w;
+  const int kmax = in->k_max;
+  if (n < 0 || h <= 0 || w <= 0 || H <= 0 || W <= 0 || kmax < 0 || in->psf_nterms <= 0 ||
+      in->psf_nterms > UPH_MAXNT || in->bg_order < 0 || in->bg_order > 2)
+    return set_err(ctx, UPH_ERR_INVALID, "invalid sparse band shape");
+  if (!in->data || !in->invvar || !in->pix_good || !in->psf_coefs ||
+      (n > 0 && (!in->pos_x || !in->pos_y)) ||
+      (n > 0 && kmax > 0 && (!in->neighbor_idx || !in->neighbor_mask)))
+    return set_err(ctx, UPH_ERR_INVALID, "null sparse band input");
+  if (sparse_stamp_smem(H, W) > 200 * 1024)
+    return set_err(ctx, UPH_ERR_INVALID, "PSF stamp %dx%d too large", H, W);
+  if (!(in->psf_x_scale != 0.f && in->psf_y_scale != 0.f && in->bg_x_scale != 0.0 &&
+        in->bg_y_scale != 0.0))
+    return set_err(ctx, UPH_ERR_INVALID, "zero normalisation scale");
+  for (size_t e = 0; e < (size_t)n * kmax; ++e)
+    if (in->neighbor_mask[e] && (in->neighbor_idx[e] < 0 || in->neighbor_idx[e] >= n))
+      return set_err(ctx, UPH_ERR_INVALID, "neighbour index out of range");
+  cudaSetDevice(ctx->device);
+  const int M = in->bg_order == 0 ? 1 : (in->bg_order == 1 ? 3 : 6);
+  const int nt = n + M;
+  const size_t npix = (size_t)h * w;
+  const int nparts = (int)std::max<size_t>(1, std::min<size_t>(2 * (size_t)ctx->sm_count,
+                                                            (npix + 255) / 256));
+  const size_t nq = (size_t)M * M + M;
+  const size_t sizes[] = {
+      sizeof(float) * npix, sizeof(float) * npix, npix, sizeof(float) * npix,
+      sizeof(float) * (size_t)std::max(n, 1), sizeof(float) * (size_t)std::max(n, 1),
+      sizeof(float) * (size_t)H * W * in->psf_nterms, sizeof(float) * 4, sizeof(double) * 4,
+      sizeof(int) * std::max<size_t>((size_t)n * kmax, 1), std::max<size_t>((size_t)n * kmax, 1),
+      sizeof(float) * std::max<size_t>((size_t)n * H * W, 1),
+      sizeof(int) * (size_t)std::max(n, 1), sizeof(int) * (size_t)std::max(n, 1),
+      sizeof(float) * (size_t)std::max(n, 1), sizeof(float) * (size_t)std::max(n, 1),
+      sizeof(float) * std::max<size_t>((size_t)n * M, 1),
+      sizeof(float) * std::max<size_t>((size_t)n * kmax, 1), sizeof(double) * nparts * nq,
+      sizeof(float) * (size_t)nt * nt, sizeof(double) * (size_t)nt * (2 * (size_t)nt + 1),
+      sizeof(int), sizeof(float) * nt, sizeof(float) * nt};
+  for (int i = 0; i < 24; ++i) {
+    int rc = ensure(ctx, ctx->sp[i], sizes[i], "sparse solve");
+    if (rc) return rc;
+  }
+  SparseDev d{};
+  d.n = n; d.H = H; d.W = W; d.nterms = in->psf_nterms; d.M = M; d.h = h; d.w = w;
+  d.gx0 = in->grid_x0; d.gy0 = in->grid_y0; d.renorm = in->renorm ? 1 : 0; d.kmax = kmax;
+  d.nparts = nparts; d.reg = in->reg;
+  float* data = (float*)ctx->sp[0].ptr;
+  float* invvar = (float*)ctx->sp[1].ptr;
+  uint8_t* good = (uint8_t*)ctx->sp[2].ptr;
+  d.wgrid = (float*)ctx->sp[3].ptr;
+  float* px = (float*)ctx->sp[4].ptr;
+  float* py = (float*)ctx->sp[5].ptr;
+  float* coefs = (float*)ctx->sp[6].ptr;
+  float* os = (float*)ctx->sp[7].ptr;
+  double* bn = (double*)ctx->sp[8].ptr;
+  int* nidx = (int*)ctx->sp[9].ptr;
+  uint8_t* nmask = (uint8_t*)ctx->sp[10].ptr;
+  d.data = data; d.invvar = invvar; d.good = good; d.px = px; d.py = py; d.coefs = coefs;
+  d.os = os; d.bn = bn; d.nidx = nidx; d.nmask = nmask;
+  d.stamps = (float*)ctx->sp[11].ptr;
+  d.ixt = (int*)ctx->sp[12].ptr;
+  d.iyt = (int*)ctx->sp[13].ptr;
+  d.diag = (float*)ctx->sp[14].ptr;
+  d.twd = (float*)ctx->sp[15].ptr;
+  d.twb = (float*)ctx->sp[16].ptr;
+  d.off = (float*)ctx->sp[17].ptr;
+  d.part = (double*)ctx->sp[18].ptr;
+  d.Af = (float*)ctx->sp[19].ptr;
+  d.G = (double*)ctx->sp[20].ptr;
+  d.prow = (int*)ctx->sp[21].ptr;
+  d.x = (float*)ctx->sp[22].ptr;
+  d.var = (float*)ctx->sp[23].ptr;
+  const float osh[4] = {in->psf_x_origin, in->psf_x_scale, in->psf_y_origin, in->psf_y_scale};
+  const double bnh[4] = {in->bg_x_origin, in->bg_x_scale, in->bg_y_origin, in->bg_y_scale};
+  int rc;
+  if ((rc = upload(ctx, data, in->data, sizeof(float) * npix, "data"))) return rc;
+  if ((rc = upload(ctx, invvar, in->invvar, sizeof(float) * npix, "invvar"))) return rc;
+  if ((rc = upload(ctx, good, in->pix_good, npix, "pix_good"))) return rc;
+  if (n > 0) {
+    if ((rc = upload(ctx, px, in->pos_x, sizeof(float) * n, "pos_x"))) return rc;
+    if ((rc = upload(ctx, py, in->pos_y, sizeof(float) * n, "pos_y"))) return rc;
+  }
+  if ((rc = upload(ctx, coefs, in->psf_coefs, sizeof(float) * (size_t)H * W * in->psf_nterms,
+                   "psf")))
+    return rc;
+  if ((rc = upload(ctx, os, osh, sizeof(osh), "psf origin"))) return rc;
+  if ((rc = upload(ctx, bn, bnh, sizeof(bnh), "bg origin"))) return rc;
+  if (n > 0 && kmax > 0) {
+    if ((rc = upload(ctx, nidx, in->neighbor_idx, sizeof(int) * (size_t)n * kmax, "nbr")))
+      return rc;
+    if ((rc = upload(ctx, nmask, in->neighbor_mask, (size_t)n * kmax, "nbr"))) return rc;
+  }
+  launch_sparse_band(d, ctx->stream);
+  CK(cudaGetLastError(), "sparse launch");
+  std::vector<float> x(nt), var(nt);
+  if ((rc = download(ctx, x.data(), d.x, sizeof(float) * nt, "x"))) return rc;
+  if ((rc = download(ctx, var.data(), d.var, sizeof(float) * nt, "var"))) return rc;
+  CK(cudaStreamSynchronize(ctx->stream), "sparse solve");
+  bool fin = true;
+  for (int i = 0; i < nt; ++i) fin = fin && std::isfinite(x[i]);
+  for (int i = 0; i < n; ++i) {
+    if (out->fluxes) out->fluxes[i] = x[i];
+    if (out->flux_var) out->flux_var[i] = var[i];
+  }
+  for (int m = 0; m < M; ++m) {
+    if (out->bg_coefs) out->bg_coefs[m] = x[n + m];
+    if (out->bg_var) out->bg_var[m] = var[n + m];
+  }
+  out->converged = fin ? 1 : 0;
   return UPH_OK;
 }
 

@@ -312,6 +312,81 @@ __device__ __forceinline__ size_t stamp_slot(const ClassDev& c, int isl, int b,
          (size_t)(c.Sz * c.Sz);
 }
 
+__device__ inline void lanczos_taps(double d, float* L, float* dL) {
+  double v[7], dv[7], s = 0.0, ds = 0.0;
+  const double pi = 3.141592653589793;
+  for (int t = 0; t < 7; ++t) {
+    double x = (double)(t - 3) + d;
+    double ax = fabs(x);
+    if (ax < 1e-12) {
+      v[t] = 1.0;
+      dv[t] = 0.0;
+    } else if (ax >= 3.0) {
+      v[t] = 0.0;
+      dv[t] = 0.0;
+    } else {
+      double px = pi * x;
+      double s1, c1, s3, c3;
+      sincos(px, &s1, &c1);
+      sincos(px / 3.0, &s3, &c3);
+      v[t] = 3.0 * s1 * s3 / (px * px);
+      dv[t] = 3.0 * (pi * c1 * s3 + (pi / 3.0) * s1 * c3) / (px * px) -
+              6.0 * s1 * s3 / (pi * pi * x * x * x);
+    }
+    s += v[t];
+    ds += dv[t];
+  }
+  for (int t = 0; t < 7; ++t) {
+    L[t] = (float)(v[t] / s);
+    dL[t] = (float)((dv[t] * s - v[t] * ds) / (s * s));
+  }
+}
+
+// polynomial term exponents, low order first
+__device__ __forceinline__ void term_mn(int t, int& m, int& n) {
+  int deg = 0, start = 0;
+  while (start + deg + 1 <= t) {
+    start += deg + 1;
+    ++deg;
+  }
+  n = t - start;
+  m = deg - n;
+}
+
+// Per-grid sparse forced photometry of one band (uph_sparse.cu): inputs,
+// per-source work and the float64 system [A | I | b] in device memory.
+struct SparseDev {
+  int n, H, W, nterms, M, h, w, gx0, gy0, renorm, kmax, nparts;
+  float reg;
+  const float* coefs;      // (H, W, nterms)
+  const float* os;         // x_origin, x_scale, y_origin, y_scale
+  const float* px;
+  const float* py;
+  const float* data;       // (h, w)
+  const float* invvar;
+  const uint8_t* good;
+  const int* nidx;         // (n, kmax)
+  const uint8_t* nmask;
+  const double* bn;        // background x_origin, x_scale, y_origin, y_scale
+  float* wgrid;            // invvar where good, else 0
+  float* stamps;           // (n, H, W)
+  int* ixt;
+  int* iyt;
+  float* diag;
+  float* twd;
+  float* twb;              // (n, M)
+  float* off;              // (n, kmax)
+  double* part;            // (nparts, M*M + M)
+  float* Af;               // (n + M)^2
+  double* G;               // (n + M, 2 (n + M) + 1)
+  int* prow;
+  float* x;                // solution (n + M)
+  float* var;              // diagonal of the inverse (n + M)
+};
+size_t sparse_stamp_smem(int H, int W);
+int sparse_setup();
+void launch_sparse_band(const SparseDev& d, cudaStream_t s);
+
 // Kernel launch wrappers (defined in the .cu units).
 void launch_render(const ClassDev& c, const float* P, int phase,
                    cudaStream_t s);

@@ -103,47 +103,6 @@ __device__ float qmin_box(float ia, float ib, float ic, float x0, float x1,
   return best;
 }
 
-__device__ void lanczos_taps(double d, float* L, float* dL) {
-  double v[7], dv[7], s = 0.0, ds = 0.0;
-  const double pi = 3.141592653589793;
-  for (int t = 0; t < 7; ++t) {
-    double x = (double)(t - 3) + d;
-    double ax = fabs(x);
-    if (ax < 1e-12) {
-      v[t] = 1.0;
-      dv[t] = 0.0;
-    } else if (ax >= 3.0) {
-      v[t] = 0.0;
-      dv[t] = 0.0;
-    } else {
-      double px = pi * x;
-      double s1, c1, s3, c3;
-      sincos(px, &s1, &c1);
-      sincos(px / 3.0, &s3, &c3);
-      v[t] = 3.0 * s1 * s3 / (px * px);
-      dv[t] = 3.0 * (pi * c1 * s3 + (pi / 3.0) * s1 * c3) / (px * px) -
-              6.0 * s1 * s3 / (pi * pi * x * x * x);
-    }
-    s += v[t];
-    ds += dv[t];
-  }
-  for (int t = 0; t < 7; ++t) {
-    L[t] = (float)(v[t] / s);
-    dL[t] = (float)((dv[t] * s - v[t] * ds) / (s * s));
-  }
-}
-
-// polynomial term exponents, low order first
-__device__ __forceinline__ void term_mn(int t, int& m, int& n) {
-  int deg = 0, start = 0;
-  while (start + deg + 1 <= t) {
-    start += deg + 1;
-    ++deg;
-  }
-  n = t - start;
-  m = deg - n;
-}
-
 __device__ double ipow(double x, int e) {
   double r = 1.0;
   for (int i = 0; i < e; ++i) r *= x;
