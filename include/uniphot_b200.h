@@ -352,6 +352,17 @@ typedef struct uph_sparse_out {
 
 int uph_sparse_band_solve(uph_ctx* ctx, const uph_sparse_band* in, uph_sparse_out* out);
 
+/* ---- Island decomposition ------------------------------------------------
+ * Replaces the coupled-pair search and connected-components labelling of
+ * build_islands (islands.py:361-470, 423-560): sources i and j couple when
+ * dist(i, j) < r_i + r_j (float64); rows flagged in forced_singleton (may
+ * be NULL) couple with nothing.  root_out[i] = the minimum source index of
+ * i's island, so islands ordered by root are the reference's deterministic
+ * labels.  Positions and radii must be finite, radii positive. */
+int uph_island_roots(uph_ctx* ctx, const double* pos_x, const double* pos_y,
+                     const double* radius, const uint8_t* forced_singleton,
+                     int32_t n, int32_t* root_out);
+
 /* ---- Allocation-free final-flux pass.  No counterpart in the reference:
  * it exists for callers that cannot call cudaMalloc (a host inside a
  * framework that owns the device memory pool, or a serving process that

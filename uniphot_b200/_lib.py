@@ -26,7 +26,7 @@ EXPORTED = ("uph_create", "uph_destroy", "uph_last_error", "uph_set_stream",
             "uph_last_launch_count", "uph_job_create", "uph_job_destroy",
             "uph_job_add_chunk", "uph_job_solve", "uph_job_read",
             "uph_job_set_profile", "uph_job_kernel_time", "uph_job_kernel_work",
-            "uph_job_chunk_time", "uph_sparse_band_solve")
+            "uph_job_chunk_time", "uph_sparse_band_solve", "uph_island_roots")
 KERNEL_KINDS = ("render", "gram", "assemble", "step", "trial_chi2", "accept",
                 "gram_tc")
 
@@ -134,6 +134,7 @@ def lib():
                                           C.POINTER(C.c_double)]
         L.uph_job_chunk_time.argtypes = [_P, C.c_int32, C.POINTER(C.c_float)]
         L.uph_sparse_band_solve.argtypes = [_P, C.POINTER(SparseBand), C.POINTER(SparseOut)]
+        L.uph_island_roots.argtypes = [_P, _P, _P, _P, _P, C.c_int32, _P]
         _lib = L
     return _lib
 
@@ -193,6 +194,18 @@ class Context:
         nb, Hp, Wp = d.shape
         self.check(lib().uph_upload_field(self._h, ptr(d), ptr(w), nb, Hp, Wp, int(pad)),
                    "uph_upload_field")
+
+    def island_roots(self, x, y, radius, forced_singleton=None) -> np.ndarray:
+        """Minimum member index of every source's island (uph_island_roots)."""
+        xs = np.ascontiguousarray(x, np.float64)
+        ys = np.ascontiguousarray(y, np.float64)
+        rs = np.ascontiguousarray(radius, np.float64)
+        fs = (None if forced_singleton is None
+              else np.ascontiguousarray(np.asarray(forced_singleton).astype(np.uint8)))
+        out = np.zeros(xs.size, np.int32)
+        self.check(lib().uph_island_roots(self._h, ptr(xs), ptr(ys), ptr(rs), ptr(fs),
+                                          int(xs.size), ptr(out)), "uph_island_roots")
+        return out
 
     def sparse_band_solve(self, inputs, nbr_idx, nbr_mask, reg: float, order: int, M: int):
         """One band of one grid through uph_sparse_band_solve; returns a

@@ -58,6 +58,7 @@ struct PolyPsf {
 struct uph_ctx {
   int device = 0;
   DevBuf sp[24];   // sparse grid solve: inputs, per-source work, the system
+  DevBuf isl[13];  // island decomposition
   cudaStream_t stream = nullptr;
   bool own_stream = false;
   std::string err;
@@ -198,6 +199,7 @@ int uph_destroy(uph_ctx* ctx) {
   ctx->tb_lv.release();
   ctx->tb_core.release();
   for (auto& b : ctx->sp) b.release();
+  for (auto& b : ctx->isl) b.release();
   for (auto& ev : ctx->ev)
     if (ev) cudaEventDestroy(ev);
   if (ctx->h_active) cudaFreeHost(ctx->h_active);
@@ -1408,6 +1410,74 @@ int uph_sparse_band_solve(uph_ctx* ctx, const uph_sparse_band* in, uph_sparse_ou
     if (out->bg_var) out->bg_var[m] = var[n + m];
   }
   out->converged = fin ? 1 : 0;
+  return UPH_OK;
+}
+
+int uph_island_roots(uph_ctx* ctx, const double* pos_x, const double* pos_y,
+                     const double* radius, const uint8_t* forced_singleton,
+                     int32_t n, int32_t* root_out) {
+  if (!ctx) return UPH_ERR_INVALID;
+  if (n < 0) return set_err(ctx, UPH_ERR_INVALID, "negative source count");
+  if (n == 0) return UPH_OK;
+  if (!pos_x || !pos_y || !radius || !root_out)
+    return set_err(ctx, UPH_ERR_INVALID, "null island input");
+  double xmin = INFINITY, xmax = -INFINITY, ymin = INFINITY, ymax = -INFINITY, rmax = 0.0;
+  for (int i = 0; i < n; ++i) {
+    if (!std::isfinite(pos_x[i]) || !std::isfinite(pos_y[i]) || !std::isfinite(radius[i]) ||
+        !(radius[i] > 0.0))
+      return set_err(ctx, UPH_ERR_INVALID, "non-finite position or radius at %d", i);
+    xmin = std::min(xmin, pos_x[i]);
+    xmax = std::max(xmax, pos_x[i]);
+    ymin = std::min(ymin, pos_y[i]);
+    ymax = std::max(ymax, pos_y[i]);
+    rmax = std::max(rmax, radius[i]);
+  }
+  // coupled sources lie in the same or adjacent cells of pitch >= 2 r_max;
+  // the grid is capped at 4096 cells a side
+  const double span = std::max(xmax - xmin, ymax - ymin);
+  const double cell = std::max(2.0 * rmax, span / 4096.0);
+  const int ncx = (int)std::floor((xmax - xmin) / cell) + 1;
+  const int ncy = (int)std::floor((ymax - ymin) / cell) + 1;
+  const size_t ncell = (size_t)ncx * ncy;
+  cudaSetDevice(ctx->device);
+  const size_t sizes[13] = {sizeof(double) * n, sizeof(double) * n, sizeof(double) * n,
+                            (size_t)n, sizeof(int) * n, sizeof(int) * ncell,
+                            sizeof(int) * (ncell + 1), sizeof(int) * ncell, sizeof(int) * n,
+                            sizeof(int) * n, sizeof(int) * n, sizeof(int), 16};
+  for (int i = 0; i < 13; ++i) {
+    int rc = ensure(ctx, ctx->isl[i], sizes[i], "island decomposition");
+    if (rc) return rc;
+  }
+  IslandDev d{};
+  d.n = n; d.ncx = ncx; d.ncy = ncy; d.x0 = xmin; d.y0 = ymin; d.cell = cell;
+  double* x = (double*)ctx->isl[0].ptr;
+  double* y = (double*)ctx->isl[1].ptr;
+  double* r = (double*)ctx->isl[2].ptr;
+  uint8_t* single = (uint8_t*)ctx->isl[3].ptr;
+  d.x = x; d.y = y; d.r = r; d.single = forced_singleton ? single : nullptr;
+  d.cid = (int*)ctx->isl[4].ptr;
+  d.count = (int*)ctx->isl[5].ptr;
+  d.start = (int*)ctx->isl[6].ptr;
+  d.cursor = (int*)ctx->isl[7].ptr;
+  d.bucket = (int*)ctx->isl[8].ptr;
+  d.parent = (int*)ctx->isl[9].ptr;
+  d.root = (int*)ctx->isl[10].ptr;
+  d.err = (int*)ctx->isl[11].ptr;
+  int rc;
+  if ((rc = upload(ctx, x, pos_x, sizeof(double) * n, "pos_x"))) return rc;
+  if ((rc = upload(ctx, y, pos_y, sizeof(double) * n, "pos_y"))) return rc;
+  if ((rc = upload(ctx, r, radius, sizeof(double) * n, "radius"))) return rc;
+  if (forced_singleton && (rc = upload(ctx, single, forced_singleton, (size_t)n, "singleton")))
+    return rc;
+  CK(cudaMemsetAsync(d.count, 0, sizeof(int) * ncell, ctx->stream), "island counts");
+  CK(cudaMemsetAsync(d.err, 0, sizeof(int), ctx->stream), "island flag");
+  launch_island_roots(d, ctx->stream);
+  CK(cudaGetLastError(), "island launch");
+  int err = 0;
+  if ((rc = download(ctx, root_out, d.root, sizeof(int) * n, "roots"))) return rc;
+  if ((rc = download(ctx, &err, d.err, sizeof(int), "island flag"))) return rc;
+  CK(cudaStreamSynchronize(ctx->stream), "island decomposition");
+  if (err) return set_err(ctx, UPH_ERR_TIMEOUT, "union-find retries exhausted");
   return UPH_OK;
 }
 

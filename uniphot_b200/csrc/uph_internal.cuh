@@ -387,6 +387,25 @@ size_t sparse_stamp_smem(int H, int W);
 int sparse_setup();
 void launch_sparse_band(const SparseDev& d, cudaStream_t s);
 
+// Device island decomposition (uph_islands.cu).
+struct IslandDev {
+  int n, ncx, ncy;
+  double x0, y0, cell;
+  const double* x;
+  const double* y;
+  const double* r;
+  const uint8_t* single;   // forced singletons (nullable)
+  int* cid;                // (n) cell of each source
+  int* count;              // (ncx * ncy)
+  int* start;              // (ncx * ncy + 1)
+  int* cursor;             // (ncx * ncy)
+  int* bucket;             // (n) sources by cell
+  int* parent;             // (n) union-find
+  int* root;               // (n) minimum member index of the component
+  int* err;
+};
+void launch_island_roots(const IslandDev& d, cudaStream_t s);
+
 // Kernel launch wrappers (defined in the .cu units).
 void launch_render(const ClassDev& c, const float* P, int phase,
                    cudaStream_t s);

@@ -167,7 +167,11 @@ def _coupled_pairs(x, y, r):
 
 
 def build_islands(pos_x, pos_y, source_type, logre, sersic_n, r_psf, *,
-                  radius=None, forced_singleton=None) -> IslandSet:
+                  radius=None, forced_singleton=None, context=None) -> IslandSet:
+    """Coupling islands of a catalog (islands.py:423-560).  With
+    ``context`` (a ``uniphot_b200._lib.Context``) the coupled-pair search
+    and the connected components run on its GPU (``uph_island_roots``);
+    the labels, member lists and boxes are the same."""
     x = np.asarray(pos_x, dtype=np.float64)
     y = np.asarray(pos_y, dtype=np.float64)
     n = x.shape[0]
@@ -194,18 +198,24 @@ def build_islands(pos_x, pos_y, source_type, logre, sersic_n, r_psf, *,
         return IslandSet(0, 0, np.empty(0, np.int32), radius, [],
                          np.empty(0, np.int32), np.empty((0, 4), np.int64),
                          float(r_psf))
-    gi, gj = _coupled_pairs(x, y, radius)
-    if forced_singleton is not None and gi.size:
-        fs = np.asarray(forced_singleton, dtype=bool)
-        if fs.shape[0] != n:
-            raise ValueError("forced_singleton must have the same length as pos_x")
-        ok = ~(fs[gi] | fs[gj])
-        gi, gj = gi[ok], gj[ok]
-    if gi.size:
-        g = sparse.coo_matrix((np.ones(gi.size, np.int8), (gi, gj)), shape=(n, n))
-        _, raw = connected_components(g, directed=False)
+    if forced_singleton is not None and np.asarray(forced_singleton).shape[0] != n:
+        raise ValueError("forced_singleton must have the same length as pos_x")
+    if context is not None:
+        # component roots are minimum member indices: their ascending order
+        # is the order of islands by minimum member
+        _, raw = np.unique(context.island_roots(x, y, radius, forced_singleton),
+                           return_inverse=True)
     else:
-        raw = np.arange(n)
+        gi, gj = _coupled_pairs(x, y, radius)
+        if forced_singleton is not None and gi.size:
+            fs = np.asarray(forced_singleton, dtype=bool)
+            ok = ~(fs[gi] | fs[gj])
+            gi, gj = gi[ok], gj[ok]
+        if gi.size:
+            g = sparse.coo_matrix((np.ones(gi.size, np.int8), (gi, gj)), shape=(n, n))
+            _, raw = connected_components(g, directed=False)
+        else:
+            raw = np.arange(n)
     n_isl = int(raw.max()) + 1
     first = np.full(n_isl, n, dtype=np.int64)
     np.minimum.at(first, raw, np.arange(n))
