@@ -340,6 +340,16 @@ typedef struct uph_sparse_band {
   const int32_t* neighbor_idx;   /* [n*k_max], -1 where unused            */
   const uint8_t* neighbor_mask;  /* [n*k_max]                              */
   float reg;
+  /* Extended sources ("fft" backend, source_model.py:304-318; may be NULL:
+   * all stars): type (0 star, 1 EXP, 2 DEV, 3 SERSIC), ln Re, ee1, ee2 and
+   * the Sersic index the mixture table is read at.  Galaxies need the
+   * table (uph_upload_sersic_table); with any galaxy the stamps are not
+   * renormalised, as the reference's mixed renderer. */
+  const int32_t* source_type;
+  const float* logre;
+  const float* ee1;
+  const float* ee2;
+  const float* sersic_n;
 } uph_sparse_band;
 
 typedef struct uph_sparse_out {

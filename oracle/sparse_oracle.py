@@ -1,11 +1,14 @@
-"""CPU restatement of the reference's per-grid sparse forced photometry for
-point sources (test infrastructure only: the checker of
+"""CPU restatement of the reference's per-grid sparse forced photometry
+(test infrastructure only: the checker of
 ``uph_sparse_band_solve``; nothing in ``uniphot_b200`` imports it).
 
 Follows ``tract7dt/fit/grid_gpu/forced_phot_sparse.py``:
 
 * stamps: the polynomial PSF at each source's full-image position
-  (``psf_polynomial.py:134-197``), renormalised to unit sum, Lanczos-3
+  (``psf_polynomial.py:134-197``) -- for extended sources the "fft"
+  backend's galaxy stamp (``source_model.py:304-318``,
+  ``sersic_mog.py:153-194``) -- renormalised to unit sum on the all-star
+  path (``:126-170``), Lanczos-3
   shifted by the fractional grid-local position (``:126-170``,
   ``lanczos.py:50-181``), placed at ``stamp_top_left`` (``:255-269``);
 * ``solver_inner`` (``:498-555``): per-source diagonal, data and background
@@ -23,23 +26,47 @@ from __future__ import annotations
 
 import numpy as np
 
-from .island_oracle import correlate_x, correlate_y, lanczos3_taps, poly_basis
+from .island_oracle import (correlate_x, correlate_y, cov_terms, fft_pad_for,
+                            lanczos3_taps, poly_basis)
 
 _TERMS = {0: ((0, 0),), 1: ((0, 0), (1, 0), (0, 1)),
           2: ((0, 0), (1, 0), (0, 1), (2, 0), (1, 1), (0, 2))}
 
 
-def stamps(psf, pos_x, pos_y, grid_x0, grid_y0, renorm=True):
-    """(n, H, W) float32 Lanczos-shifted unit-sum PSF stamps."""
+def galaxy_fft(psf_img, amps, vars_, core, cg):
+    """The "fft" backend's galaxy stamp (sersic_mog.py:153-194): the
+    mixture's transform times rfft2 of the zero-padded PSF, cropped, plus
+    core times the PSF."""
+    H, W = psf_img.shape
+    pad = fft_pad_for(max(H, W))
+    z = np.zeros((pad, pad))
+    z[:H, :W] = psf_img
+    P = np.fft.rfft2(z)
+    v = np.fft.rfftfreq(pad)[None, :]
+    w = np.fft.fftfreq(pad)[:, None]
+    expo = -2.0 * np.pi ** 2 * (cg[0] * v * v + cg[1] * w * w + 2.0 * cg[2] * v * w)
+    F = sum(a * np.exp(vv * expo) for a, vv in zip(amps, vars_))
+    return np.fft.irfft2(P * F, s=(pad, pad))[:H, :W] + core * psf_img
+
+
+def stamps(psf, pos_x, pos_y, grid_x0, grid_y0, renorm=True, gal=None, table=None):
+    """(n, H, W) float32 Lanczos-shifted PSF stamps (unit sum when
+    ``renorm``); ``gal`` = (source_type, logre, ee1, ee2, sersic_n) renders
+    the extended sources with the "fft" backend from ``table``."""
     f32 = np.float32
     coefs = np.asarray(psf.coefs, np.float32)
     nt = coefs.shape[-1]
     out = []
-    for x, y in zip(np.asarray(pos_x, np.float32), np.asarray(pos_y, np.float32)):
+    for s_i, (x, y) in enumerate(zip(np.asarray(pos_x, np.float32),
+                                     np.asarray(pos_y, np.float32))):
         X = float(f32((f32(x) - f32(psf.x_origin)) / f32(psf.x_scale)))
         Y = float(f32((f32(y) - f32(psf.y_origin)) / f32(psf.y_scale)))
         b, _, _ = poly_basis(X, Y, nt)
         raw = (coefs.astype(np.float64) @ b).astype(np.float32)
+        if gal is not None and int(gal[0][s_i]) != 0:
+            amps, vars_, core = table.lookup(float(gal[4][s_i]))[:3]
+            cg, _ = cov_terms(float(gal[1][s_i]), float(gal[2][s_i]), float(gal[3][s_i]))
+            raw = galaxy_fft(raw.astype(np.float64), amps, vars_, core, cg).astype(np.float32)
         if renorm:
             raw = (raw / np.float32(max(float(raw.astype(np.float64).sum()), 1e-12))
                    ).astype(np.float32)
@@ -61,10 +88,14 @@ def bg_basis(h, w, x0, y0, xo, xs, yo, ys, order):
 
 
 def solve_band(data, invvar, pix_good, pos_x, pos_y, psf, grid_x0, grid_y0,
-               bg_norm, order, nbr_idx, nbr_mask, reg=1e-9, renorm=True):
-    """(fluxes, bg_coefs, flux_var, bg_var) of one band, float32."""
+               bg_norm, order, nbr_idx, nbr_mask, reg=1e-9, renorm=True, gal=None,
+               table=None):
+    """(fluxes, bg_coefs, flux_var, bg_var) of one band, float32.  With
+    extended sources in ``gal`` no stamp is renormalised."""
     h, w = data.shape
-    S = stamps(psf, pos_x, pos_y, grid_x0, grid_y0, renorm)
+    mixed = gal is not None and bool(np.any(np.asarray(gal[0]) != 0))
+    S = stamps(psf, pos_x, pos_y, grid_x0, grid_y0, renorm and not mixed,
+               gal if mixed else None, table)
     n, H, W = S.shape
     x = np.asarray(pos_x, np.float32) - np.float32(grid_x0)
     y = np.asarray(pos_y, np.float32) - np.float32(grid_y0)

@@ -80,3 +80,28 @@ def test_sparse_band_noise_free_known_answer_and_empty_grid(ctx):
     assert r0.fluxes.size == 0 and r0.converged
     w = g["invvar"].astype(np.float64)
     np.testing.assert_allclose(r0.bg_coefs[0], (w * g["data"]).sum() / w.sum(), rtol=1e-5)
+
+
+def test_sparse_band_with_galaxies_fft_backend(ctx):
+    """Stars and EXP/DEV/SERSIC galaxies with the "fft" backend
+    (source_model.py:304-318): galaxy stamps from the Sersic mixture's
+    transform times the PSF's, no renormalisation on the mixed path."""
+    from oracle import sparse_oracle as SO
+    from oracle.island_oracle import SersicTable
+    from _common import TABLE
+    g = _grid(seed=7, n=16, order=1, noise=5.0)
+    rng = np.random.default_rng(7)
+    st = np.array([0, 1, 2, 3] * 4, np.int32)
+    lr = rng.uniform(0.0, 1.2, 16).astype(np.float32)
+    e1 = rng.uniform(-0.3, 0.3, 16).astype(np.float32)
+    e2 = rng.uniform(-0.3, 0.3, 16).astype(np.float32)
+    sn = np.where(st == 1, 1.0, np.where(st == 2, 4.0, rng.uniform(0.7, 5.0, 16))).astype(np.float32)
+    idx, mask = build_neighbor_list(g["px"], g["py"], 15, 15, k_max=32)
+    inp = _inputs(g)
+    inp.source_type, inp.logre, inp.ee1, inp.ee2, inp.sersic_n = st, lr, e1, e2, sn
+    inp.render_backend = "fft"
+    r = solve_band_sparse(inp, idx, mask, reg=1e-9, bg_poly_order=1, context=ctx)
+    o = SO.solve_band(g["data"], g["invvar"], g["good"], g["px"], g["py"], g["psf"],
+                      g["gx0"], g["gy0"], g["bn"], 1, idx, mask, reg=1e-9,
+                      gal=(st, lr, e1, e2, sn), table=SersicTable.load(TABLE))
+    _check(r, o)

@@ -103,3 +103,25 @@ def test_extended_sources_raise():
                          source_type=np.array([0, 1, 0]))
     with pytest.raises(ValueError, match="not supported"):
         solve_band_sparse(inp, np.zeros((3, 4), np.int32), np.zeros((3, 4), bool))
+
+
+def test_grid_galaxy_stamp_matches_the_island_fft_render():
+    """The grid solve's "fft" galaxy stamp is the island solver's reference-
+    mode galaxy render (sersic_mog.py:153-194) for the same PSF image."""
+    import oracle.island_oracle as O
+    from oracle import sparse_oracle as SO
+    from test_oracle_pins import _mini_island
+    isl, _ = _mini_island("reference", n_src=2, seed=3, T=55, B=48)
+    isl.stype[:] = np.array([0, 3])
+    isl.free_n[:] = [False, False]
+    isl.n_frozen[:] = 2.5
+    s = O.IslandSolver(isl, O.SolverConfig(precision="f64"))
+    p = isl.p0.astype(np.float64)
+    gal = s._gal_params(1, p)
+    x, y = float(p[6]), float(p[7])
+    S = s._galaxy_fft(0, x, y, gal, False)[0]
+    psf = s._star_unshifted(0, x, y)[0]
+    amps, vars_, core = isl.table.lookup(2.5)[:3]
+    cg, _ = O.cov_terms(float(p[8]), float(p[9]), float(p[10]))
+    np.testing.assert_allclose(SO.galaxy_fft(psf.astype(np.float64), amps, vars_, core, cg), S,
+                               rtol=1e-9, atol=1e-12)

@@ -78,7 +78,8 @@ class SparseBand(C.Structure):
                 ("bg_x_scale", C.c_double), ("bg_y_origin", C.c_double),
                 ("bg_y_scale", C.c_double), ("bg_order", C.c_int32),
                 ("k_max", C.c_int32), ("neighbor_idx", _P), ("neighbor_mask", _P),
-                ("reg", C.c_float)]
+                ("reg", C.c_float), ("source_type", _P), ("logre", _P), ("ee1", _P),
+                ("ee2", _P), ("sersic_n", _P)]
 
 
 class SparseOut(C.Structure):
@@ -237,6 +238,24 @@ class Context:
                         bg_y_scale=float(inputs.bg_y_scale), bg_order=int(order),
                         k_max=kmax, neighbor_idx=ptr(ni), neighbor_mask=ptr(nm),
                         reg=float(reg))
+        keep = []
+        st = getattr(inputs, "source_type", None)
+        if st is not None and np.any(np.asarray(st) != 0):
+            if not getattr(self, "_table", False):
+                from .sersic import load_table
+                self.upload_sersic_table(load_table())
+                self._table = True
+            zeros = np.zeros(n, np.float32)
+
+            def f32(a, fill):
+                return np.ascontiguousarray(fill if a is None else a, np.float32)
+            arrs = (np.ascontiguousarray(st, np.int32),
+                    f32(getattr(inputs, "logre", None), zeros),
+                    f32(getattr(inputs, "ee1", None), zeros),
+                    f32(getattr(inputs, "ee2", None), zeros),
+                    f32(getattr(inputs, "sersic_n", None), np.ones(n, np.float32)))
+            keep.extend(arrs)
+            ib.source_type, ib.logre, ib.ee1, ib.ee2, ib.sersic_n = (ptr(a) for a in arrs)
         fl = np.zeros(n, np.float32)
         fv = np.zeros(n, np.float32)
         bg = np.zeros(M, np.float32)

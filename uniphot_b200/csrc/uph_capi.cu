@@ -57,7 +57,7 @@ struct PolyPsf {
 
 struct uph_ctx {
   int device = 0;
-  DevBuf sp[24];   // sparse grid solve: inputs, per-source work, the system
+  DevBuf sp[32];   // sparse grid solve: inputs, per-source work, the system
   DevBuf isl[13];  // island decomposition
   cudaStream_t stream = nullptr;
   bool own_stream = false;
@@ -1320,6 +1320,21 @@ int uph_sparse_band_solve(uph_ctx* ctx, const uph_sparse_band* in, uph_sparse_ou
   for (size_t e = 0; e < (size_t)n * kmax; ++e)
     if (in->neighbor_mask[e] && (in->neighbor_idx[e] < 0 || in->neighbor_idx[e] >= n))
       return set_err(ctx, UPH_ERR_INVALID, "neighbour index out of range");
+  bool any_gal = false;
+  if (in->source_type) {
+    if (!in->logre || !in->ee1 || !in->ee2 || !in->sersic_n)
+      return set_err(ctx, UPH_ERR_INVALID, "source types without shapes");
+    for (int i = 0; i < n; ++i) {
+      if (in->source_type[i] < 0 || in->source_type[i] > 3)
+        return set_err(ctx, UPH_ERR_INVALID, "unknown source type %d", in->source_type[i]);
+      any_gal = any_gal || in->source_type[i] != 0;
+    }
+  }
+  const int fftP = fft_pad_for(std::max(H, W));
+  if (any_gal && !ctx->tb_knots.ptr)
+    return set_err(ctx, UPH_ERR_STATE, "no Sersic table uploaded");
+  if (any_gal && fftP > 512)
+    return set_err(ctx, UPH_ERR_INVALID, "PSF stamp %dx%d needs a Fourier grid above 512", H, W);
   cudaSetDevice(ctx->device);
   const int M = in->bg_order == 0 ? 1 : (in->bg_order == 1 ? 3 : 6);
   const int nt = n + M;
@@ -1338,8 +1353,17 @@ int uph_sparse_band_solve(uph_ctx* ctx, const uph_sparse_band* in, uph_sparse_ou
       sizeof(float) * std::max<size_t>((size_t)n * M, 1),
       sizeof(float) * std::max<size_t>((size_t)n * kmax, 1), sizeof(double) * nparts * nq,
       sizeof(float) * (size_t)nt * nt, sizeof(double) * (size_t)nt * (2 * (size_t)nt + 1),
-      sizeof(int), sizeof(float) * nt, sizeof(float) * nt};
-  for (int i = 0; i < 24; ++i) {
+      sizeof(int), sizeof(float) * nt, sizeof(float) * nt,
+      // extended sources
+      sizeof(int) * (size_t)std::max(n, 1), sizeof(float) * (size_t)std::max(n, 1),
+      sizeof(float) * (size_t)std::max(n, 1), sizeof(float) * (size_t)std::max(n, 1),
+      sizeof(float) * (size_t)std::max(n, 1),
+      any_gal ? sizeof(float) * (size_t)n * H * W : 16,
+      any_gal ? sizeof(float) * std::min<size_t>((size_t)n, 2 * (size_t)ctx->sm_count) *
+                    sparse_gal_floats(H, W, fftP)
+              : 16,
+      16};
+  for (int i = 0; i < 32; ++i) {
     int rc = ensure(ctx, ctx->sp[i], sizes[i], "sparse solve");
     if (rc) return rc;
   }
@@ -1373,6 +1397,27 @@ int uph_sparse_band_solve(uph_ctx* ctx, const uph_sparse_band* in, uph_sparse_ou
   d.prow = (int*)ctx->sp[21].ptr;
   d.x = (float*)ctx->sp[22].ptr;
   d.var = (float*)ctx->sp[23].ptr;
+  if (any_gal) {
+    d.stype = (const int*)ctx->sp[24].ptr;
+    d.lr = (const float*)ctx->sp[25].ptr;
+    d.e1 = (const float*)ctx->sp[26].ptr;
+    d.e2 = (const float*)ctx->sp[27].ptr;
+    d.sn = (const float*)ctx->sp[28].ptr;
+    d.gal = (float*)ctx->sp[29].ptr;
+    d.gws = (float*)ctx->sp[30].ptr;
+    d.fft_P = fftP;
+    d.gal_floats = sparse_gal_floats(H, W, fftP);
+    d.gal_ctas = (int)std::min<long long>(n, 2LL * ctx->sm_count);
+    d.tb_knots = (const double*)ctx->tb_knots.ptr;
+    d.tb_amps = (const double*)ctx->tb_amps.ptr;
+    d.tb_lv = (const double*)ctx->tb_lv.ptr;
+    d.tb_core = (const double*)ctx->tb_core.ptr;
+    d.tb_n = ctx->tb_n;
+    d.tb_k = ctx->tb_k;
+    d.tb_nmin = ctx->tb_nmin;
+    d.tb_nmax = ctx->tb_nmax;
+    d.renorm = 0;   // the reference's mixed renderer does not renormalise
+  }
   const float osh[4] = {in->psf_x_origin, in->psf_x_scale, in->psf_y_origin, in->psf_y_scale};
   const double bnh[4] = {in->bg_x_origin, in->bg_x_scale, in->bg_y_origin, in->bg_y_scale};
   int rc;
@@ -1388,6 +1433,14 @@ int uph_sparse_band_solve(uph_ctx* ctx, const uph_sparse_band* in, uph_sparse_ou
     return rc;
   if ((rc = upload(ctx, os, osh, sizeof(osh), "psf origin"))) return rc;
   if ((rc = upload(ctx, bn, bnh, sizeof(bnh), "bg origin"))) return rc;
+  if (any_gal) {
+    if ((rc = upload(ctx, ctx->sp[24].ptr, in->source_type, sizeof(int) * n, "types"))) return rc;
+    if ((rc = upload(ctx, ctx->sp[25].ptr, in->logre, sizeof(float) * n, "logre"))) return rc;
+    if ((rc = upload(ctx, ctx->sp[26].ptr, in->ee1, sizeof(float) * n, "ee1"))) return rc;
+    if ((rc = upload(ctx, ctx->sp[27].ptr, in->ee2, sizeof(float) * n, "ee2"))) return rc;
+    if ((rc = upload(ctx, ctx->sp[28].ptr, in->sersic_n, sizeof(float) * n, "sersic_n")))
+      return rc;
+  }
   if (n > 0 && kmax > 0) {
     if ((rc = upload(ctx, nidx, in->neighbor_idx, sizeof(int) * (size_t)n * kmax, "nbr")))
       return rc;

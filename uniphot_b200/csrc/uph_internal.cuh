@@ -382,8 +382,27 @@ struct SparseDev {
   int* prow;
   float* x;                // solution (n + M)
   float* var;              // diagonal of the inverse (n + M)
+  // extended sources ("fft" backend): per-source type and shape (stype
+  // null: all stars), the Sersic table, the unshifted galaxy stamps and
+  // the Fourier work space (gal_ctas CTAs of gal_floats floats, pad fft_P)
+  const int* stype;
+  const float* lr;
+  const float* e1;
+  const float* e2;
+  const float* sn;
+  const double* tb_knots;
+  const double* tb_amps;
+  const double* tb_lv;
+  const double* tb_core;
+  int tb_n, tb_k;
+  double tb_nmin, tb_nmax;
+  int fft_P, gal_ctas;
+  size_t gal_floats;
+  float* gal;
+  float* gws;
 };
 size_t sparse_stamp_smem(int H, int W);
+size_t sparse_gal_floats(int H, int W, int P);
 int sparse_setup();
 void launch_sparse_band(const SparseDev& d, cudaStream_t s);
 
@@ -405,6 +424,58 @@ struct IslandDev {
   int* err;
 };
 void launch_island_roots(const IslandDev& d, cudaStream_t s);
+
+// Ellipse (logre, ee1, ee2) -> unit covariance and its Jacobian
+// (sersic_mog.py:108-150, incl. the round-source nudge).
+__device__ inline void cov_terms(double lr, double e1, double e2, float* cg,
+                          float dc[3][3]) {
+  double ex = exp(lr);
+  double re = fmin(fmax(ex, 0.1), 1000.0);
+  double dre = (ex > 0.1 && ex < 1000.0) ? re : 0.0;
+  bool nudge = (e1 == 0.0) && (e2 == 0.0);
+  double e1n = nudge ? 1e-4 : e1;
+  double de1n = nudge ? 0.0 : 1.0;
+  double ee = hypot(e1n, e2);
+  double dee1 = e1n / ee * de1n, dee2 = e2 / ee;
+  double ex2 = exp(-ee);
+  double e = 1.0 - ex2;
+  double den = 1.0 - e, dden = -1.0;
+  if (!(den > 1e-4)) {
+    den = 1e-4;
+    dden = 0.0;
+  }
+  double ibr = (1.0 + e) / den;
+  double dibr = (den - (1.0 + e) * dden) / (den * den);
+  double ib = ibr, dib = dibr;
+  if (!(ibr < 1000.0)) {
+    ib = 1000.0;
+    dib = 0.0;
+  }
+  double th = 0.5 * atan2(e2, e1n);
+  double dth1 = -0.5 * e2 / (ee * ee) * de1n, dth2 = 0.5 * e1n / (ee * ee);
+  double st, ct;
+  sincos(th, &st, &ct);
+  double s2 = 1.0 / (ib * ib);
+  double r2 = re * re;
+  cg[0] = (float)(r2 * (ct * ct * s2 + st * st));
+  cg[1] = (float)(r2 * (st * st * s2 + ct * ct));
+  cg[2] = (float)(r2 * ct * st * (1.0 - s2));
+  double d_re[3] = {2 * re * (ct * ct * s2 + st * st),
+                    2 * re * (st * st * s2 + ct * ct),
+                    2 * re * ct * st * (1.0 - s2)};
+  double ib3 = ib * ib * ib;
+  double d_ib[3] = {r2 * ct * ct * (-2.0 / ib3), r2 * st * st * (-2.0 / ib3),
+                    r2 * ct * st * (2.0 / ib3)};
+  double d_th[3] = {2 * r2 * ct * st * (1.0 - s2),
+                    -2 * r2 * ct * st * (1.0 - s2),
+                    r2 * (ct * ct - st * st) * (1.0 - s2)};
+  double dib_dee = dib * ex2;
+  for (int q = 0; q < 3; ++q) {
+    dc[0][q] = (float)(d_re[q] * dre);
+    dc[1][q] = (float)(d_ib[q] * dib_dee * dee1 + d_th[q] * dth1);
+    dc[2][q] = (float)(d_ib[q] * dib_dee * dee2 + d_th[q] * dth2);
+  }
+}
 
 // Kernel launch wrappers (defined in the .cu units).
 void launch_render(const ClassDev& c, const float* P, int phase,

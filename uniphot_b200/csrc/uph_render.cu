@@ -109,58 +109,6 @@ __device__ double ipow(double x, int e) {
   return r;
 }
 
-// Ellipse (logre, ee1, ee2) -> unit covariance and its Jacobian
-// (sersic_mog.py:108-150, incl. the round-source nudge).
-__device__ void cov_terms(double lr, double e1, double e2, float* cg,
-                          float dc[3][3]) {
-  double ex = exp(lr);
-  double re = fmin(fmax(ex, 0.1), 1000.0);
-  double dre = (ex > 0.1 && ex < 1000.0) ? re : 0.0;
-  bool nudge = (e1 == 0.0) && (e2 == 0.0);
-  double e1n = nudge ? 1e-4 : e1;
-  double de1n = nudge ? 0.0 : 1.0;
-  double ee = hypot(e1n, e2);
-  double dee1 = e1n / ee * de1n, dee2 = e2 / ee;
-  double ex2 = exp(-ee);
-  double e = 1.0 - ex2;
-  double den = 1.0 - e, dden = -1.0;
-  if (!(den > 1e-4)) {
-    den = 1e-4;
-    dden = 0.0;
-  }
-  double ibr = (1.0 + e) / den;
-  double dibr = (den - (1.0 + e) * dden) / (den * den);
-  double ib = ibr, dib = dibr;
-  if (!(ibr < 1000.0)) {
-    ib = 1000.0;
-    dib = 0.0;
-  }
-  double th = 0.5 * atan2(e2, e1n);
-  double dth1 = -0.5 * e2 / (ee * ee) * de1n, dth2 = 0.5 * e1n / (ee * ee);
-  double st, ct;
-  sincos(th, &st, &ct);
-  double s2 = 1.0 / (ib * ib);
-  double r2 = re * re;
-  cg[0] = (float)(r2 * (ct * ct * s2 + st * st));
-  cg[1] = (float)(r2 * (st * st * s2 + ct * ct));
-  cg[2] = (float)(r2 * ct * st * (1.0 - s2));
-  double d_re[3] = {2 * re * (ct * ct * s2 + st * st),
-                    2 * re * (st * st * s2 + ct * ct),
-                    2 * re * ct * st * (1.0 - s2)};
-  double ib3 = ib * ib * ib;
-  double d_ib[3] = {r2 * ct * ct * (-2.0 / ib3), r2 * st * st * (-2.0 / ib3),
-                    r2 * ct * st * (2.0 / ib3)};
-  double d_th[3] = {2 * r2 * ct * st * (1.0 - s2),
-                    -2 * r2 * ct * st * (1.0 - s2),
-                    r2 * (ct * ct - st * st) * (1.0 - s2)};
-  double dib_dee = dib * ex2;
-  for (int q = 0; q < 3; ++q) {
-    dc[0][q] = (float)(d_re[q] * dre);
-    dc[1][q] = (float)(d_ib[q] * dib_dee * dee1 + d_th[q] * dth1);
-    dc[2][q] = (float)(d_ib[q] * dib_dee * dee2 + d_th[q] * dth2);
-  }
-}
-
 // Per-member scratch of the parallel setup (analytic mode).
 struct PsfComp {
   double w, wx, wy;          // raw weight and its d/dx, d/dy

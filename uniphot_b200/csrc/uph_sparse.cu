@@ -3,8 +3,14 @@
 // normal matrix of stamps and a polynomial background, an element-wise
 // ridge, a float64 solve and the diagonal of the inverse.
 //
-//   k_sp_stamps   one CTA per source: PSF polynomial at the source, unit-sum
-//                 renormalisation, Lanczos-3 x then y pass in shared memory
+//   k_sp_gal      galaxies (the "fft" backend, source_model.py:304-318):
+//                 the PSF at the source, the Sersic mixture's transform
+//                 times the padded PSF's (sersic_mog.py:153-194) by dense
+//                 row/column DFTs over the stamp support, cropped to the
+//                 stamp, plus the core times the PSF
+//   k_sp_stamps   one CTA per source: PSF polynomial at the source (or the
+//                 galaxy stamp), unit-sum renormalisation on the all-star
+//                 path, Lanczos-3 x then y pass in shared memory
 //   k_sp_self     one CTA per source: sum w s^2, sum w s d, sum w s B_m over
 //                 the stamp (zero weight outside the grid)
 //   k_sp_pairs    one warp per neighbour slot: sum w_s s_s s_t over the
@@ -40,11 +46,145 @@ __device__ __forceinline__ float bg_term(int t, int gx, int gy, const double* bn
   }
 }
 
+__device__ void psf_basis_at(float x, float y, const float* os, int nt, float* beta) {
+  const float X = __fdiv_rn(__fsub_rn(x, os[0]), os[1]);
+  const float Y = __fdiv_rn(__fsub_rn(y, os[2]), os[3]);
+  for (int t = 0; t < nt; ++t) {
+    int m, q;
+    term_mn(t, m, q);
+    float xm = 1.f, yq = 1.f;
+    for (int i = 0; i < m; ++i) xm *= X;
+    for (int i = 0; i < q; ++i) yq *= Y;
+    beta[t] = xm * yq;
+  }
+}
+
+constexpr int MAXPS = 512;
+
+// Unshifted galaxy stamps (H x W) of the extended sources; a grid of CTAs
+// loops over the sources with a work space each of sparse_gal_floats.
+__global__ void __launch_bounds__(ST)
+k_sp_gal(const SparseDev d) {
+  __shared__ float cw[MAXPS], sw[MAXPS];
+  __shared__ float beta[UPH_MAXNT];
+  __shared__ double ga[UPH_MAXGAL], gv[UPH_MAXGAL];
+  __shared__ double gcore;
+  __shared__ float cg[3];
+  const int tid = threadIdx.x;
+  const int H = d.H, W = d.W, PP = d.fft_P, Hf = PP / 2 + 1, msk = PP - 1;
+  for (int m = tid; m < PP; m += ST) {
+    double sn, cs;
+    sincospi(2.0 * (double)m / (double)PP, &sn, &cs);
+    cw[m] = (float)cs;
+    sw[m] = (float)sn;
+  }
+  float* ws = d.gws + (size_t)blockIdx.x * d.gal_floats;
+  float* img = ws;                           // H x W
+  float* R = img + (size_t)H * W;            // H x Hf complex
+  float* X = R + 2 * (size_t)H * Hf;         // P x Hf complex
+  float* Fs = X + 2 * (size_t)PP * Hf;       // P x Hf real
+  float* Cc = Fs + (size_t)PP * Hf;          // H x Hf complex
+  for (int s = blockIdx.x; s < d.n; s += gridDim.x) {
+    __syncthreads();
+    if (d.stype[s] == 0) continue;     // stars take the PSF itself
+    if (tid == 0) {
+      psf_basis_at(d.px[s], d.py[s], d.os, d.nterms, beta);
+      // Sersic mixture at the source's index (sersic_mog.py:81-100)
+      const double nc = fmin(fmax((double)d.sn[s], d.tb_nmin), d.tb_nmax);
+      int lo = 0, hi = d.tb_n;
+      while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (d.tb_knots[mid] <= nc) lo = mid + 1; else hi = mid;
+      }
+      const int seg = max(0, min(lo - 1, d.tb_n - 2));
+      const double n0 = d.tb_knots[seg], n1 = d.tb_knots[seg + 1];
+      const double t = (n1 > n0) ? (nc - n0) / (n1 - n0) : 0.0;
+      for (int g = 0; g < d.tb_k; ++g) {
+        ga[g] = (1 - t) * d.tb_amps[seg * d.tb_k + g] + t * d.tb_amps[(seg + 1) * d.tb_k + g];
+        gv[g] = exp((1 - t) * d.tb_lv[seg * d.tb_k + g] + t * d.tb_lv[(seg + 1) * d.tb_k + g]);
+      }
+      gcore = (1 - t) * d.tb_core[seg] + t * d.tb_core[seg + 1];
+      float dc[3][3];
+      cov_terms((double)d.lr[s], (double)d.e1[s], (double)d.e2[s], cg, dc);
+    }
+    __syncthreads();
+    for (int e = tid; e < H * W; e += ST) {
+      const float* cf = d.coefs + (size_t)e * d.nterms;
+      float v = 0.f;
+      for (int t = 0; t < d.nterms; ++t) v = fmaf(cf[t], beta[t], v);
+      img[e] = v;
+    }
+    __syncthreads();
+    for (int e = tid; e < H * Hf; e += ST) {
+      const int i = e / Hf, u = e - (e / Hf) * Hf;
+      float re = 0.f, imv = 0.f;
+      for (int j = 0; j < W; ++j) {
+        const int m = (j * u) & msk;
+        const float v = img[i * W + j];
+        re = fmaf(v, cw[m], re);
+        imv = fmaf(-v, sw[m], imv);
+      }
+      R[2 * e] = re;
+      R[2 * e + 1] = imv;
+    }
+    __syncthreads();
+    const double kk = -2.0 * 9.869604401089358;
+    for (int e = tid; e < PP * Hf; e += ST) {
+      const int w = e / Hf, u = e - (e / Hf) * Hf;
+      float re = 0.f, imv = 0.f;
+      for (int i = 0; i < H; ++i) {
+        const int m = (i * w) & msk;
+        const float ar = R[2 * (i * Hf + u)], ai = R[2 * (i * Hf + u) + 1];
+        re = fmaf(ar, cw[m], fmaf(ai, sw[m], re));
+        imv = fmaf(ai, cw[m], fmaf(-ar, sw[m], imv));
+      }
+      X[2 * e] = re;
+      X[2 * e + 1] = imv;
+      const double nu = (double)u / PP;
+      const double nw = (double)(w < PP / 2 ? w : w - PP) / PP;
+      const double ex = kk * ((double)cg[0] * nu * nu + (double)cg[1] * nw * nw +
+                              2.0 * (double)cg[2] * nu * nw);
+      double F = 0.0;
+      for (int g = 0; g < d.tb_k; ++g) F += ga[g] * exp(gv[g] * ex);
+      Fs[e] = (float)F;
+    }
+    __syncthreads();
+    for (int e = tid; e < H * Hf; e += ST) {
+      const int i = e / Hf, u = e - (e / Hf) * Hf;
+      float re = 0.f, imv = 0.f;
+      for (int w = 0; w < PP; ++w) {
+        const float f = Fs[w * Hf + u];
+        const float ar = f * X[2 * (w * Hf + u)], ai = f * X[2 * (w * Hf + u) + 1];
+        const int m = (i * w) & msk;
+        re = fmaf(ar, cw[m], fmaf(-ai, sw[m], re));
+        imv = fmaf(ai, cw[m], fmaf(ar, sw[m], imv));
+      }
+      Cc[2 * e] = re;
+      Cc[2 * e + 1] = imv;
+    }
+    __syncthreads();
+    const double inv = 1.0 / ((double)PP * (double)PP);
+    float* o = d.gal + (size_t)s * H * W;
+    for (int e = tid; e < H * W; e += ST) {
+      const int i = e / W, j = e - (e / W) * W;
+      const float* ci = Cc + 2 * (size_t)i * Hf;
+      const float v = ci[0] + ((j & 1) ? -ci[2 * (Hf - 1)] : ci[2 * (Hf - 1)]);
+      float acc = 0.f;
+      for (int u = 1; u < Hf - 1; ++u) {
+        const int m = (j * u) & msk;
+        acc = fmaf(ci[2 * u], cw[m], fmaf(-ci[2 * u + 1], sw[m], acc));
+      }
+      o[e] = (float)(((double)v + 2.0 * (double)acc) * inv + gcore * (double)img[e]);
+    }
+  }
+}
+
 __global__ void __launch_bounds__(ST)
 k_sp_stamps(int n, int H, int W, const float* __restrict__ coefs, int nt,
             const float* __restrict__ os, const float* __restrict__ px,
             const float* __restrict__ py, float gx0, float gy0, int renorm,
-            float* __restrict__ out, int* __restrict__ ixt, int* __restrict__ iyt) {
+            float* __restrict__ out, int* __restrict__ ixt, int* __restrict__ iyt,
+            const int* __restrict__ stype, const float* __restrict__ gal) {
   extern __shared__ float sm[];
   __shared__ float beta[UPH_MAXNT];
   __shared__ float Lx[7], Ly[7], dL[7];
@@ -55,17 +195,9 @@ k_sp_stamps(int n, int H, int W, const float* __restrict__ coefs, int nt,
   const int tid = threadIdx.x;
   float* raw = sm;            // H x W
   float* tmp = sm + H * W;    // H x W
+  const bool is_gal = stype && stype[s] != 0;
   if (tid == 0) {
-    const float X = __fdiv_rn(__fsub_rn(px[s], os[0]), os[1]);
-    const float Y = __fdiv_rn(__fsub_rn(py[s], os[2]), os[3]);
-    for (int t = 0; t < nt; ++t) {
-      int m, q;
-      term_mn(t, m, q);
-      float xm = 1.f, yq = 1.f;
-      for (int i = 0; i < m; ++i) xm *= X;
-      for (int i = 0; i < q; ++i) yq *= Y;
-      beta[t] = xm * yq;
-    }
+    psf_basis_at(px[s], py[s], os, nt, beta);
     const float xg = __fsub_rn(px[s], gx0), yg = __fsub_rn(py[s], gy0);
     lanczos_taps((double)__fsub_rn(xg, rintf(xg)), Lx, dL);
     lanczos_taps((double)__fsub_rn(yg, rintf(yg)), Ly, dL);
@@ -76,9 +208,14 @@ k_sp_stamps(int n, int H, int W, const float* __restrict__ coefs, int nt,
   __syncthreads();
   double acc = 0.0;
   for (int e = tid; e < H * W; e += ST) {
-    const float* cf = coefs + (size_t)e * nt;
-    float v = 0.f;
-    for (int t = 0; t < nt; ++t) v = fmaf(cf[t], beta[t], v);
+    float v;
+    if (is_gal) {
+      v = gal[(size_t)s * H * W + e];
+    } else {
+      const float* cf = coefs + (size_t)e * nt;
+      v = 0.f;
+      for (int t = 0; t < nt; ++t) v = fmaf(cf[t], beta[t], v);
+    }
     raw[e] = v;
     acc += (double)v;
   }
@@ -380,6 +517,12 @@ __global__ void k_sp_wgrid(size_t npix, const float* __restrict__ invvar,
 
 size_t sparse_stamp_smem(int H, int W) { return 2 * sizeof(float) * (size_t)H * W; }
 
+size_t sparse_gal_floats(int H, int W, int P) {
+  const size_t Hf = (size_t)P / 2 + 1;
+  const size_t f = (size_t)H * W + 4 * (size_t)H * Hf + 3 * (size_t)P * Hf;
+  return (f + 63) & ~(size_t)63;
+}
+
 int sparse_setup() {
   return (int)cudaFuncSetAttribute(k_sp_stamps, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    200 * 1024);
@@ -390,9 +533,10 @@ void launch_sparse_band(const SparseDev& d, cudaStream_t s) {
   const size_t npix = (size_t)d.h * d.w;
   k_sp_wgrid<<<(unsigned)((npix + 255) / 256), 256, 0, s>>>(npix, d.invvar, d.good, d.wgrid);
   if (n > 0) {
+    if (d.gal_ctas > 0) k_sp_gal<<<(unsigned)d.gal_ctas, ST, 0, s>>>(d);
     k_sp_stamps<<<(unsigned)n, ST, sparse_stamp_smem(H, W), s>>>(
         n, H, W, d.coefs, d.nterms, d.os, d.px, d.py, (float)d.gx0, (float)d.gy0, d.renorm,
-        d.stamps, d.ixt, d.iyt);
+        d.stamps, d.ixt, d.iyt, d.stype, d.gal);
     k_sp_self<<<(unsigned)n, ST, 0, s>>>(n, H, W, d.stamps, d.ixt, d.iyt, d.data, d.wgrid,
                                          d.h, d.w, d.gx0, d.gy0, d.bn, M, d.diag, d.twd,
                                          d.twb);

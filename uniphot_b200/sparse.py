@@ -16,8 +16,13 @@ Mirrors the reference's entry points for point sources:
   wise ridge ``reg |diag|``, a float64 solve and the diagonal of the
   inverse -- all in the CUDA library (``uph_sparse_band_solve``).
 
-Extended sources (EXP/DEV/SERSIC) raise ``ValueError``: their stamp
-renderer is not built for the grid solve.
+Extended sources (EXP/DEV/SERSIC) take the reference's "fft" backend
+(``source_model.py:304-318``): the Sersic mixture's Fourier transform times
+the padded PSF's (``sersic_mog.py:153-194``), cropped to the stamp, plus the
+core times the PSF, then the stars' Lanczos shift; with any extended source
+no stamp is renormalised (the reference's mixed renderer).  The legacy
+"direct" EXP backend is not built: extended sources with
+``render_backend="direct"`` raise ``ValueError``.
 """
 
 from __future__ import annotations
@@ -62,8 +67,12 @@ class GridBandInputs:
     bg_y_origin: float
     bg_y_scale: float
     source_type: np.ndarray | None = None
+    logre: np.ndarray | None = None
+    ee1: np.ndarray | None = None
+    ee2: np.ndarray | None = None
+    sersic_n: np.ndarray | None = None
     render_backend: str = "direct"
-    renorm: bool = True          # unit-sum stamps (the reference's default)
+    renorm: bool = True          # unit-sum stamps on the all-star path (the default)
 
 
 @dataclass
@@ -134,9 +143,10 @@ def solve_band_sparse(inputs: GridBandInputs, neighbor_idx, neighbor_mask,
     (forced_phot_sparse.py:690-718) on the GPU.  ``context`` is a
     ``uniphot_b200._lib.Context`` to reuse (one is created otherwise)."""
     from . import _lib
-    if inputs.source_type is not None and np.any(np.asarray(inputs.source_type) != SOURCE_STAR):
-        raise ValueError("not supported by the B200 grid solve: extended sources "
-                         "(EXP/DEV/SERSIC) in the sparse forced photometry")
+    if inputs.source_type is not None and np.any(np.asarray(inputs.source_type) != SOURCE_STAR) \
+            and inputs.render_backend not in ("fft", "auto"):
+        raise ValueError("not supported by the B200 grid solve: extended sources with "
+                         f"render_backend={inputs.render_backend!r} (the 'fft' backend is built)")
     M = n_terms_for_order(bg_poly_order)
     ctx = context if context is not None else _lib.Context(device)
     return ctx.sparse_band_solve(inputs, np.asarray(neighbor_idx), np.asarray(neighbor_mask),
