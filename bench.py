@@ -201,6 +201,29 @@ def run_reference_arm(args, rank, world):
                 "d2h_bytes_per_step": 0}}))
 
 
+def _reference_render_measure(args, local):
+    """islands/s of the production field in the reference render mode:
+    the same catalog with the band PSFs as pixelised polynomials."""
+    import torch
+    from uniphot_b200.solver import IslandFitJob
+    from uniphot_b200.synth import make_production_field
+    field = make_production_field(args.seed, device="cuda", side=args.side, n_src=args.n_src)
+    kw = field.fit_kwargs("reference")
+    kw["precision"] = args.precision
+    job = IslandFitJob(**kw, device=local)
+    stream = torch.cuda.ExternalStream(job.field.ctx.stream_ptr())
+    for _ in range(args.warmup):
+        job.solve()
+    ms, launches = _timed_solves(job, args.steps, stream, torch.cuda.synchronize, None)
+    n_gal = int(np.sum(np.asarray(field.source_type) != 0))
+    out = {"value": job.n_islands * args.steps / (ms / 1e3), "unit": "islands/s",
+           "ms_per_step": ms / args.steps, "n_islands": job.n_islands,
+           "galaxies": n_gal, "precision": args.precision, "gpu_launches": int(launches),
+           "workload": WORKLOAD + ", reference render mode (polynomial PSF)"}
+    job.close()
+    return out
+
+
 def _timed_solves(job, steps, stream, barrier, dist):
     """Device time (ms) of `steps` solves, max over ranks, and launches."""
     import torch
@@ -442,6 +465,10 @@ def main():
                     help="run only the serving measurement (rates from "
                          "--serve-rates) and print its JSON line")
     ap.add_argument("--serve-rates", default="10,50,200,2000")
+    ap.add_argument("--reference-render", action="store_true",
+                    help="time the solve of the production field in the reference "
+                         "render mode (pixelised polynomial PSF; galaxies by the "
+                         "Fourier-domain convolution) and print its JSON line")
     ap.add_argument("--precision-stress", action="store_true",
                     help="run only the precision-stress measurement (crowded "
                          "blends, 40 bands) and print its JSON line")
@@ -465,6 +492,11 @@ def main():
     if args.precision_stress:
         if rank == 0:
             print(json.dumps({"precision_stress": _stress_measure(args, local)}),
+                  flush=True)
+        return
+    if args.reference_render:
+        if rank == 0:
+            print(json.dumps({"reference_render": _reference_render_measure(args, local)}),
                   flush=True)
         return
     if args.serve_only:

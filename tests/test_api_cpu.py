@@ -116,3 +116,12 @@ def test_catalog_errors_propagate_to_the_catalog_frame():
     np.testing.assert_allclose(e["ell_prior_frac"][0], (e1**2 * 0.1 + e2**2 * 0.3) / r**2,
                                rtol=1e-6)
     assert np.isnan(e["sersic_n_prior_frac"][0]) and np.isnan(e["pos_x_prior_frac"][1])
+
+
+def test_direct_backend_galaxies_raise_in_reference_mode():
+    with pytest.raises(ValueError, match="not supported"):
+        solver.make_class_kernels(_plan("mixed"), 3, 1, **dict(KW, render_backend="direct"),
+                                  render_mode="reference")
+    k = solver.make_class_kernels(_plan("star"), 3, 1, **dict(KW, render_backend="direct"),
+                                  render_mode="reference")
+    assert k.desc.render_mode == 0

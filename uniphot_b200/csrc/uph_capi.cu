@@ -704,7 +704,10 @@ int add_chunk(uph_ctx* ctx, Chunk* ch, const uph_class_desc* cls,
     // galaxy stamps by the Fourier-domain convolution with the pixel PSF
     c.fft_P = fft_pad_for(T);
     c.gfft_floats = gal_fft_floats(T, c.fft_P);
-    c.gfft_ctas = (int)std::min<long long>((long long)n * nb * N, 2LL * ctx->sm_count);
+    // concurrent chunks each hold a work space: half an SM's worth of CTAs
+    // per chunk keeps the device busy without multiplying the memory
+    c.gfft_ctas = (int)std::min<long long>((long long)n * nb * N,
+                                           std::max(16, ctx->sm_count / 2));
     c.gstamp = cbuf<float>(ctx, ch, "gstamp", (size_t)n * nb * N * 7 * T * T, &rc);
     c.gfft_ws = cbuf<float>(ctx, ch, "gfftws", (size_t)c.gfft_ctas * c.gfft_floats, &rc);
   }

@@ -222,6 +222,10 @@ def make_class_kernels(plan, n_bands: int, n_terms: int, *, render_backend: str,
     unsupported = []
     # star-only classes keep the clip step (island_solver.py:1910-1912)
     step_eff = str(step_mode) if str(plan.kind) != "star" else "clip"
+    if render_mode == "reference" and render_backend == "direct" and plan.kind != "star":
+        # the legacy EXP-only direct-convolution backend (source_model.py:
+        # 298-303); galaxies render through the "fft" backend here
+        unsupported.append("render_backend='direct' for galaxies")
     if crossband is not None:
         unsupported.append("crossband")
     if scene_subtract:
