@@ -219,7 +219,9 @@ def _reference_render_measure(args, local):
     out = {"value": job.n_islands * args.steps / (ms / 1e3), "unit": "islands/s",
            "ms_per_step": ms / args.steps, "n_islands": job.n_islands,
            "galaxies": n_gal, "precision": args.precision, "gpu_launches": int(launches),
-           "workload": WORKLOAD + ", reference render mode (polynomial PSF)"}
+           "workload": WORKLOAD.replace("analytic render", "reference render (pixelised "
+                                        "polynomial PSF; galaxies by Fourier-domain "
+                                        "convolution)")}
     job.close()
     return out
 

@@ -13,11 +13,10 @@
 // is real (zero-centred Gaussians), so every product is a complex spectrum
 // times a real factor.
 //
-// The transforms are dense DFTs over the stamp's support -- rows of T
-// inputs to P/2 + 1 frequencies, columns of T inputs (or outputs) against
-// P frequencies -- with a shared-memory twiddle table: only T of the P
-// padded rows and columns are non-zero on the way in and needed on the way
-// out.  One CTA per (island, band, galaxy member), looping over the members
+// The transforms are radix-2 FFTs of whole lines in shared memory (a batch
+// of lines per pass, 32 KB): the T non-zero rows of the padded image, then
+// the P/2 + 1 columns of their half spectra; on the way back the columns,
+// keeping the T rows of the crop, then those rows' real inverses.  One CTA per (island, band, galaxy member), looping over the members
 // of a grid sized to the SM count, with its work space in global memory
 // (L2-resident per CTA).  The unshifted rows land in c.gstamp, which the
 // render's Lanczos passes read in place of the star's polynomial PSF.
@@ -28,14 +27,20 @@ namespace {
 
 constexpr int GT = 256;
 constexpr int MAXP = 512;
+constexpr int FFT_SMEM_BYTES = 32768;      // shared line buffer of the FFTs
+
+__host__ __device__ inline size_t align64(size_t f) { return (f + 63) & ~(size_t)63; }
 
 __global__ void __launch_bounds__(GT) k_gal_fft(ClassDev c, const float* __restrict__ Pp,
                                                 int phase) {
+  extern __shared__ float2 fbuf[];          // LB lines of P complex values
   __shared__ float cw[MAXP], sw[MAXP];
   __shared__ int need[7];
   __shared__ int is_gal;
   const int tid = threadIdx.x;
-  const int T = c.T, PP = c.fft_P, H = PP / 2 + 1, msk = PP - 1;
+  const int T = c.T, PP = c.fft_P, H = PP / 2 + 1;
+  const int logP = 31 - __clz(PP);
+  const int lb = FFT_SMEM_BYTES / (8 * PP);
   const int TT = T * T;
   for (int m = tid; m < PP; m += GT) {
     double sn, cs;
@@ -44,12 +49,12 @@ __global__ void __launch_bounds__(GT) k_gal_fft(ClassDev c, const float* __restr
     sw[m] = (float)sn;
   }
   float* ws = c.gfft_ws + (size_t)blockIdx.x * c.gfft_floats;
-  float* img = ws;                          // 3 real T x T: psf, psf_x, psf_y
-  float* R = img + 3 * TT;                  // row transform, T x H complex
-  float* X = R + 2 * (size_t)T * H;         // 3 spectra, P x H complex
-  float* Fs = X + 6 * (size_t)PP * H;       // F, F1, dF, P x H real
-  float* Cc = Fs + 3 * (size_t)PP * H;      // inverse column pass, T x H complex
   const size_t PH = (size_t)PP * H;
+  float* img = ws;                                          // 3 real T x T
+  float2* R = (float2*)(ws + align64(3 * (size_t)TT));      // T x H
+  float2* X = R + (size_t)T * H;                            // 3 spectra, P x H
+  float* Fs = (float*)(X + 3 * PH);                         // F, F1, dF, P x H
+  float2* Cc = (float2*)(Fs + align64(3 * PH));             // T x H
   const int nitems = c.n_isl * c.nb * c.N;
   const bool lin = phase == PH_LIN;
   for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
@@ -86,39 +91,8 @@ __global__ void __launch_bounds__(GT) k_gal_fft(ClassDev c, const float* __restr
       img[2 * TT + e] = v2;
     }
     __syncthreads();
-    // ---- forward transforms of the zero-padded images ----
-    for (int im = 0; im < 3; ++im) {
-      if (!need[im]) continue;
-      const float* a = img + im * TT;
-      for (int e = tid; e < T * H; e += GT) {
-        const int i = e / H, u = e - (e / H) * H;
-        float re = 0.f, imv = 0.f;
-        for (int j = 0; j < T; ++j) {
-          const int m = (j * u) & msk;
-          const float v = a[i * T + j];
-          re = fmaf(v, cw[m], re);
-          imv = fmaf(-v, sw[m], imv);
-        }
-        R[2 * e] = re;
-        R[2 * e + 1] = imv;
-      }
-      __syncthreads();
-      float* Xi = X + 2 * PH * im;
-      for (int e = tid; e < (int)PH; e += GT) {
-        const int w = e / H, u = e - (e / H) * H;
-        float re = 0.f, imv = 0.f;
-        for (int i = 0; i < T; ++i) {
-          const int m = (i * w) & msk;
-          const float ar = R[2 * (i * H + u)], ai = R[2 * (i * H + u) + 1];
-          // (ar + i ai)(cos - i sin)
-          re = fmaf(ar, cw[m], fmaf(ai, sw[m], re));
-          imv = fmaf(ai, cw[m], fmaf(-ar, sw[m], imv));
-        }
-        Xi[2 * e] = re;
-        Xi[2 * e + 1] = imv;
-      }
-      __syncthreads();
-    }
+    for (int im = 0; im < 3; ++im)
+      if (need[im]) fft2_forward(img + im * TT, T, T, PP, logP, R, X + PH * im, fbuf, lb, cw, sw);
     // ---- the mixture's transform and its partials on the grid ----
     const double kk = -2.0 * 9.869604401089358;   // -2 pi^2
     for (int e = tid; e < (int)PH; e += GT) {
@@ -140,53 +114,24 @@ __global__ void __launch_bounds__(GT) k_gal_fft(ClassDev c, const float* __restr
     }
     __syncthreads();
     // ---- inverse transforms of the needed products, cropped to T x T ----
-    const double inv = 1.0 / ((double)PP * (double)PP);
     float* out = c.gstamp + (size_t)item * 7 * TT;
     for (int s = 0; s < 7; ++s) {
       if (!need[s]) continue;
-      const float* Xb = X + 2 * PH * (s < 3 ? s : 0);
+      const float2* Xb = X + PH * (s < 3 ? s : 0);
       const float* fac = Fs + PH * (s < 3 ? 0 : (s < 6 ? 1 : 2));
-      float dc0 = 0.f, dc1 = 0.f, dc2 = 0.f;
-      if (s >= 3 && s < 6) {
-        dc0 = rec->dcov[s - 3][0];
-        dc1 = rec->dcov[s - 3][1];
-        dc2 = rec->dcov[s - 3][2];
-      }
-      for (int e = tid; e < T * H; e += GT) {
-        const int i = e / H, u = e - (e / H) * H;
-        const float nu = (float)u / (float)PP;
-        float re = 0.f, imv = 0.f;
-        for (int w = 0; w < PP; ++w) {
-          float f = fac[w * H + u];
-          if (s >= 3 && s < 6) {
-            const float nw = (float)(w < PP / 2 ? w : w - PP) / (float)PP;
-            f *= (float)kk * (dc0 * nu * nu + dc1 * nw * nw + 2.f * dc2 * nu * nw);
-          }
-          const float ar = f * Xb[2 * (w * H + u)], ai = f * Xb[2 * (w * H + u) + 1];
-          const int m = (i * w) & msk;
-          // (ar + i ai)(cos + i sin)
-          re = fmaf(ar, cw[m], fmaf(-ai, sw[m], re));
-          imv = fmaf(ai, cw[m], fmaf(ar, sw[m], imv));
-        }
-        Cc[2 * e] = re;
-        Cc[2 * e + 1] = imv;
-      }
-      __syncthreads();
+      const bool shp = s >= 3 && s < 6;
+      fft2_inverse_cols(Xb, fac, shp, shp ? rec->dcov[s - 3][0] : 0.f,
+                        shp ? rec->dcov[s - 3][1] : 0.f, shp ? rec->dcov[s - 3][2] : 0.f, T, PP,
+                        logP, Cc, fbuf, lb, cw, sw);
+      float* o = out + (size_t)s * TT;
+      fft2_inverse_rows(Cc, T, T, PP, logP, o, fbuf, lb, cw, sw);
       for (int e = tid; e < TT; e += GT) {
-        const int i = e / T, j = e - (e / T) * T;
-        const float* ci = Cc + 2 * (size_t)i * H;
-        float v = ci[0] + ((j & 1) ? -ci[2 * (H - 1)] : ci[2 * (H - 1)]);
-        float acc = 0.f;
-        for (int u = 1; u < H - 1; ++u) {
-          const int m = (j * u) & msk;
-          acc = fmaf(ci[2 * u], cw[m], fmaf(-ci[2 * u + 1], sw[m], acc));
-        }
-        double r = ((double)v + 2.0 * (double)acc) * inv;
+        double r = (double)o[e];
         if (s == 0) r += rec->gcore * (double)img[e];
         else if (s == 1) r += rec->gcore * (double)img[TT + e];
         else if (s == 2) r += rec->gcore * (double)img[2 * TT + e];
         else if (s == 6) r = (r + rec->gdcore * (double)img[e]) * (double)rec->dndu;
-        out[(size_t)s * TT + e] = (float)r;
+        o[e] = (float)r;
       }
       __syncthreads();
     }
@@ -203,10 +148,12 @@ int fft_pad_for(int T) {
 
 size_t gal_fft_floats(int T, int P) {
   const size_t H = (size_t)P / 2 + 1;
-  const size_t f = 3 * (size_t)T * T + 4 * (size_t)T * H + 9 * (size_t)P * H;
-  return (f + 63) & ~(size_t)63;
+  // img, R (complex), X (3 complex), Fs (3 real), Cc (complex), each aligned
+  return align64(3 * (size_t)T * T) + align64(2 * (size_t)T * H) + 6 * (size_t)P * H +
+         align64(3 * (size_t)P * H) + align64(2 * (size_t)T * H) + 64;
 }
 
 void launch_gal_fft(const ClassDev& c, const float* P, int phase, cudaStream_t s) {
-  if (c.gfft_ctas > 0) k_gal_fft<<<(unsigned)c.gfft_ctas, GT, 0, s>>>(c, P, phase);
+  if (c.gfft_ctas > 0)
+    k_gal_fft<<<(unsigned)c.gfft_ctas, GT, FFT_SMEM_BYTES, s>>>(c, P, phase);
 }

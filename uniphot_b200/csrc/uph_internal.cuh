@@ -477,6 +477,139 @@ __device__ inline void cov_terms(double lr, double e1, double e2, float* cg,
   }
 }
 
+// ---- Shared-memory radix-2 FFTs for the Fourier-domain galaxy stamps ----
+// In-place decimation-in-time FFTs of nl lines of length P = 2^logP stored
+// contiguously in shared memory; sign -1 forward, +1 inverse (unnormalised);
+// cw/sw hold cos and sin of 2 pi m / P.  Ends with a barrier.
+__device__ inline void smem_fft_lines(float2* buf, int nl, int P, int logP, float sign,
+                                      const float* cw, const float* sw) {
+  const int tid = threadIdx.x, nth = blockDim.x;
+  for (int e = tid; e < nl * P; e += nth) {
+    const int base = (e >> logP) << logP, k = e & (P - 1);
+    const int r = (int)(__brev((unsigned)k) >> (32 - logP));
+    if (k < r) {
+      const float2 a = buf[base + k];
+      buf[base + k] = buf[base + r];
+      buf[base + r] = a;
+    }
+  }
+  __syncthreads();
+  const int hp = P >> 1;
+  for (int len = 2, step = hp; len <= P; len <<= 1, step >>= 1) {
+    const int half = len >> 1;
+    for (int e = tid; e < nl * hp; e += nth) {
+      const int line = e / hp, b = e - line * hp;
+      const int grp = b / half, j = b - grp * half;
+      const int i0 = (line << logP) + grp * len + j, i1 = i0 + half;
+      const int m = j * step;
+      const float wr = cw[m], wi = sign * sw[m];
+      const float2 v = buf[i1], u = buf[i0];
+      const float tr = wr * v.x - wi * v.y, ti = wr * v.y + wi * v.x;
+      buf[i0] = make_float2(u.x + tr, u.y + ti);
+      buf[i1] = make_float2(u.x - tr, u.y - ti);
+    }
+    __syncthreads();
+  }
+}
+
+// Forward 2-D transform of an Hs x Ws real image zero-padded to P x P:
+// X (P x Hf, Hf = P/2 + 1) from row transforms R (Hs x Hf) and column
+// transforms; buf holds lb lines of P in shared memory.
+__device__ inline void fft2_forward(const float* img, int Hs, int Ws, int P, int logP,
+                                    float2* R, float2* X, float2* buf, int lb,
+                                    const float* cw, const float* sw) {
+  const int tid = threadIdx.x, nth = blockDim.x, Hf = P / 2 + 1;
+  for (int i0 = 0; i0 < Hs; i0 += lb) {
+    const int nl = min(lb, Hs - i0);
+    for (int e = tid; e < nl * P; e += nth) {
+      const int line = e >> logP, k = e & (P - 1);
+      buf[e] = make_float2(k < Ws ? img[(i0 + line) * Ws + k] : 0.f, 0.f);
+    }
+    __syncthreads();
+    smem_fft_lines(buf, nl, P, logP, -1.f, cw, sw);
+    for (int e = tid; e < nl * Hf; e += nth) {
+      const int line = e / Hf, u = e - line * Hf;
+      R[(size_t)(i0 + line) * Hf + u] = buf[(line << logP) + u];
+    }
+    __syncthreads();
+  }
+  for (int u0 = 0; u0 < Hf; u0 += lb) {
+    const int nl = min(lb, Hf - u0);
+    for (int e = tid; e < nl * P; e += nth) {
+      const int k = e / nl, line = e - k * nl;
+      buf[(line << logP) + k] = k < Hs ? R[(size_t)k * Hf + u0 + line] : make_float2(0.f, 0.f);
+    }
+    __syncthreads();
+    smem_fft_lines(buf, nl, P, logP, -1.f, cw, sw);
+    for (int e = tid; e < nl * P; e += nth) {
+      const int w = e / nl, line = e - w * nl;
+      X[(size_t)w * Hf + u0 + line] = buf[(line << logP) + w];
+    }
+    __syncthreads();
+  }
+}
+
+// Inverse column transforms of Q = Xb * fac (fac real, P x Hf; times the
+// shape factor -2 pi^2 (d0 nu^2 + d1 nw^2 + 2 d2 nu nw) when dexpo), rows
+// below Hs kept in C (Hs x Hf).
+__device__ inline void fft2_inverse_cols(const float2* Xb, const float* fac, bool dexpo,
+                                         float d0, float d1, float d2, int Hs, int P, int logP,
+                                         float2* C, float2* buf, int lb, const float* cw,
+                                         const float* sw) {
+  const int tid = threadIdx.x, nth = blockDim.x, Hf = P / 2 + 1;
+  for (int u0 = 0; u0 < Hf; u0 += lb) {
+    const int nl = min(lb, Hf - u0);
+    for (int e = tid; e < nl * P; e += nth) {
+      const int w = e / nl, line = e - w * nl, u = u0 + line;
+      float f = fac[(size_t)w * Hf + u];
+      if (dexpo) {
+        const float nu = (float)u / (float)P;
+        const float nw = (float)(w < P / 2 ? w : w - P) / (float)P;
+        f *= -19.739208802178716f * (d0 * nu * nu + d1 * nw * nw + 2.f * d2 * nu * nw);
+      }
+      const float2 x = Xb[(size_t)w * Hf + u];
+      buf[(line << logP) + w] = make_float2(f * x.x, f * x.y);
+    }
+    __syncthreads();
+    smem_fft_lines(buf, nl, P, logP, 1.f, cw, sw);
+    for (int e = tid; e < nl * Hs; e += nth) {
+      const int i = e / nl, line = e - i * nl;
+      C[(size_t)i * Hf + u0 + line] = buf[(line << logP) + i];
+    }
+    __syncthreads();
+  }
+}
+
+// Inverse row transforms (real output) of C (Hs x Hf, the half spectrum;
+// the imaginary parts of the zero and Nyquist bins are dropped as a real
+// inverse does), scaled by 1/P^2 and cropped to Hs x Ws, into out.
+__device__ inline void fft2_inverse_rows(const float2* C, int Hs, int Ws, int P, int logP,
+                                         float* out, float2* buf, int lb, const float* cw,
+                                         const float* sw) {
+  const int tid = threadIdx.x, nth = blockDim.x, Hf = P / 2 + 1;
+  const float inv = 1.f / ((float)P * (float)P);
+  for (int i0 = 0; i0 < Hs; i0 += lb) {
+    const int nl = min(lb, Hs - i0);
+    for (int e = tid; e < nl * P; e += nth) {
+      const int line = e >> logP, k = e & (P - 1);
+      const float2* ci = C + (size_t)(i0 + line) * Hf;
+      float2 v;
+      if (k == 0) v = make_float2(ci[0].x, 0.f);
+      else if (k == P / 2) v = make_float2(ci[Hf - 1].x, 0.f);
+      else if (k < P / 2) v = ci[k];
+      else v = make_float2(ci[P - k].x, -ci[P - k].y);
+      buf[e] = v;
+    }
+    __syncthreads();
+    smem_fft_lines(buf, nl, P, logP, 1.f, cw, sw);
+    for (int e = tid; e < nl * Ws; e += nth) {
+      const int line = e / Ws, j = e - line * Ws;
+      out[(i0 + line) * Ws + j] = buf[(line << logP) + j].x * inv;
+    }
+    __syncthreads();
+  }
+}
+
 // Kernel launch wrappers (defined in the .cu units).
 void launch_render(const ClassDev& c, const float* P, int phase,
                    cudaStream_t s);

@@ -5,9 +5,9 @@
 //
 //   k_sp_gal      galaxies (the "fft" backend, source_model.py:304-318):
 //                 the PSF at the source, the Sersic mixture's transform
-//                 times the padded PSF's (sersic_mog.py:153-194) by dense
-//                 row/column DFTs over the stamp support, cropped to the
-//                 stamp, plus the core times the PSF
+//                 times the padded PSF's (sersic_mog.py:153-194) by radix-2
+//                 shared-memory FFTs, cropped to the stamp, plus the core
+//                 times the PSF
 //   k_sp_stamps   one CTA per source: PSF polynomial at the source (or the
 //                 galaxy stamp), unit-sum renormalisation on the all-star
 //                 path, Lanczos-3 x then y pass in shared memory
@@ -62,16 +62,24 @@ __device__ void psf_basis_at(float x, float y, const float* os, int nt, float* b
 constexpr int MAXPS = 512;
 
 // Unshifted galaxy stamps (H x W) of the extended sources; a grid of CTAs
-// loops over the sources with a work space each of sparse_gal_floats.
+// loops over the sources with a work space each of sparse_gal_floats and a
+// shared line buffer for the radix-2 FFTs.
+constexpr int SP_FFT_SMEM = 32768;
+
+__host__ __device__ inline size_t sp_align64(size_t f) { return (f + 63) & ~(size_t)63; }
+
 __global__ void __launch_bounds__(ST)
 k_sp_gal(const SparseDev d) {
+  extern __shared__ float2 fbuf[];
   __shared__ float cw[MAXPS], sw[MAXPS];
   __shared__ float beta[UPH_MAXNT];
   __shared__ double ga[UPH_MAXGAL], gv[UPH_MAXGAL];
   __shared__ double gcore;
   __shared__ float cg[3];
   const int tid = threadIdx.x;
-  const int H = d.H, W = d.W, PP = d.fft_P, Hf = PP / 2 + 1, msk = PP - 1;
+  const int H = d.H, W = d.W, PP = d.fft_P, Hf = PP / 2 + 1;
+  const int logP = 31 - __clz(PP);
+  const int lb = SP_FFT_SMEM / (8 * PP);
   for (int m = tid; m < PP; m += ST) {
     double sn, cs;
     sincospi(2.0 * (double)m / (double)PP, &sn, &cs);
@@ -79,11 +87,12 @@ k_sp_gal(const SparseDev d) {
     sw[m] = (float)sn;
   }
   float* ws = d.gws + (size_t)blockIdx.x * d.gal_floats;
-  float* img = ws;                           // H x W
-  float* R = img + (size_t)H * W;            // H x Hf complex
-  float* X = R + 2 * (size_t)H * Hf;         // P x Hf complex
-  float* Fs = X + 2 * (size_t)PP * Hf;       // P x Hf real
-  float* Cc = Fs + (size_t)PP * Hf;          // H x Hf complex
+  const size_t PH = (size_t)PP * Hf;
+  float* img = ws;                                            // H x W
+  float2* R = (float2*)(ws + sp_align64((size_t)H * W));      // H x Hf
+  float2* X = R + (size_t)H * Hf;                             // P x Hf
+  float* Fs = (float*)(X + PH);                               // P x Hf
+  float2* Cc = (float2*)(Fs + sp_align64(PH));                // H x Hf
   for (int s = blockIdx.x; s < d.n; s += gridDim.x) {
     __syncthreads();
     if (d.stype[s] == 0) continue;     // stars take the PSF itself
@@ -115,31 +124,10 @@ k_sp_gal(const SparseDev d) {
       img[e] = v;
     }
     __syncthreads();
-    for (int e = tid; e < H * Hf; e += ST) {
-      const int i = e / Hf, u = e - (e / Hf) * Hf;
-      float re = 0.f, imv = 0.f;
-      for (int j = 0; j < W; ++j) {
-        const int m = (j * u) & msk;
-        const float v = img[i * W + j];
-        re = fmaf(v, cw[m], re);
-        imv = fmaf(-v, sw[m], imv);
-      }
-      R[2 * e] = re;
-      R[2 * e + 1] = imv;
-    }
-    __syncthreads();
+    fft2_forward(img, H, W, PP, logP, R, X, fbuf, lb, cw, sw);
     const double kk = -2.0 * 9.869604401089358;
-    for (int e = tid; e < PP * Hf; e += ST) {
+    for (int e = tid; e < (int)PH; e += ST) {
       const int w = e / Hf, u = e - (e / Hf) * Hf;
-      float re = 0.f, imv = 0.f;
-      for (int i = 0; i < H; ++i) {
-        const int m = (i * w) & msk;
-        const float ar = R[2 * (i * Hf + u)], ai = R[2 * (i * Hf + u) + 1];
-        re = fmaf(ar, cw[m], fmaf(ai, sw[m], re));
-        imv = fmaf(ai, cw[m], fmaf(-ar, sw[m], imv));
-      }
-      X[2 * e] = re;
-      X[2 * e + 1] = imv;
       const double nu = (double)u / PP;
       const double nw = (double)(w < PP / 2 ? w : w - PP) / PP;
       const double ex = kk * ((double)cg[0] * nu * nu + (double)cg[1] * nw * nw +
@@ -149,33 +137,10 @@ k_sp_gal(const SparseDev d) {
       Fs[e] = (float)F;
     }
     __syncthreads();
-    for (int e = tid; e < H * Hf; e += ST) {
-      const int i = e / Hf, u = e - (e / Hf) * Hf;
-      float re = 0.f, imv = 0.f;
-      for (int w = 0; w < PP; ++w) {
-        const float f = Fs[w * Hf + u];
-        const float ar = f * X[2 * (w * Hf + u)], ai = f * X[2 * (w * Hf + u) + 1];
-        const int m = (i * w) & msk;
-        re = fmaf(ar, cw[m], fmaf(-ai, sw[m], re));
-        imv = fmaf(ai, cw[m], fmaf(ar, sw[m], imv));
-      }
-      Cc[2 * e] = re;
-      Cc[2 * e + 1] = imv;
-    }
-    __syncthreads();
-    const double inv = 1.0 / ((double)PP * (double)PP);
+    fft2_inverse_cols(X, Fs, false, 0.f, 0.f, 0.f, H, PP, logP, Cc, fbuf, lb, cw, sw);
     float* o = d.gal + (size_t)s * H * W;
-    for (int e = tid; e < H * W; e += ST) {
-      const int i = e / W, j = e - (e / W) * W;
-      const float* ci = Cc + 2 * (size_t)i * Hf;
-      const float v = ci[0] + ((j & 1) ? -ci[2 * (Hf - 1)] : ci[2 * (Hf - 1)]);
-      float acc = 0.f;
-      for (int u = 1; u < Hf - 1; ++u) {
-        const int m = (j * u) & msk;
-        acc = fmaf(ci[2 * u], cw[m], fmaf(-ci[2 * u + 1], sw[m], acc));
-      }
-      o[e] = (float)(((double)v + 2.0 * (double)acc) * inv + gcore * (double)img[e]);
-    }
+    fft2_inverse_rows(Cc, H, W, PP, logP, o, fbuf, lb, cw, sw);
+    for (int e = tid; e < H * W; e += ST) o[e] = (float)((double)o[e] + gcore * (double)img[e]);
   }
 }
 
@@ -519,8 +484,8 @@ size_t sparse_stamp_smem(int H, int W) { return 2 * sizeof(float) * (size_t)H * 
 
 size_t sparse_gal_floats(int H, int W, int P) {
   const size_t Hf = (size_t)P / 2 + 1;
-  const size_t f = (size_t)H * W + 4 * (size_t)H * Hf + 3 * (size_t)P * Hf;
-  return (f + 63) & ~(size_t)63;
+  return sp_align64((size_t)H * W) + sp_align64(2 * (size_t)H * Hf) + 2 * (size_t)P * Hf +
+         sp_align64((size_t)P * Hf) + sp_align64(2 * (size_t)H * Hf) + 64;
 }
 
 int sparse_setup() {
@@ -533,7 +498,7 @@ void launch_sparse_band(const SparseDev& d, cudaStream_t s) {
   const size_t npix = (size_t)d.h * d.w;
   k_sp_wgrid<<<(unsigned)((npix + 255) / 256), 256, 0, s>>>(npix, d.invvar, d.good, d.wgrid);
   if (n > 0) {
-    if (d.gal_ctas > 0) k_sp_gal<<<(unsigned)d.gal_ctas, ST, 0, s>>>(d);
+    if (d.gal_ctas > 0) k_sp_gal<<<(unsigned)d.gal_ctas, ST, SP_FFT_SMEM, s>>>(d);
     k_sp_stamps<<<(unsigned)n, ST, sparse_stamp_smem(H, W), s>>>(
         n, H, W, d.coefs, d.nterms, d.os, d.px, d.py, (float)d.gx0, (float)d.gy0, d.renorm,
         d.stamps, d.ixt, d.iyt, d.stype, d.gal);
