@@ -1,0 +1,57 @@
+"""An island of 32 Sersic galaxies with free index: 192 live parameters,
+above the 160 the step factors in shared memory, so the damped system is
+factored in the global-memory work space.  Two LM steps on the GPU vs the
+oracle (the first steps of a 32-galaxy blend: the trajectories agree before
+float32 path differences can grow)."""
+import numpy as np
+import pytest
+
+from _common import compare, field_classes, run_gpu, run_oracle
+
+pytestmark = pytest.mark.gpu
+
+
+def _cluster_field(seed=11, n=32, side=112, nb=2):
+    from uniphot_b200.psf import MogPsf, rasterize_mog_psf
+    from uniphot_b200.synth import (SOURCE_SERSIC, Field, _islands, _noise, ellipse_soft,
+                                    render_truth)
+    rng = np.random.default_rng(seed)
+    mogs = [MogPsf.constant(np.array([1.3, 2.4]), np.zeros(2), np.zeros(2),
+                            np.array([0.8, 0.2]), x_origin=side / 2, x_scale=side / 2,
+                            y_origin=side / 2, y_scale=side / 2) for _ in range(nb)]
+    native = 31
+    polys = [rasterize_mog_psf(m, native, side / 2, side / 2) for m in mogs]
+    tx = side / 2 + rng.uniform(-30, 30, n)
+    ty = side / 2 + rng.uniform(-30, 30, n)
+    st = np.full(n, SOURCE_SERSIC, np.int32)
+    lr, e1, e2 = ellipse_soft(rng.uniform(1.0, 2.5, n), rng.uniform(0.5, 1.0, n),
+                              rng.uniform(0, 180, n))
+    lr, e1, e2 = (np.asarray(a, np.float32) for a in (lr, e1, e2))
+    sn = rng.uniform(1.0, 3.0, n).astype(np.float32)
+    flux = np.exp(rng.uniform(np.log(3e4), np.log(1e5), (n, nb)))
+    model = render_truth((nb, side, side), mogs, tx, ty, st, lr, e1, e2, sn, flux,
+                         np.full(n, native // 2), "cpu")
+    dmb, iv = _noise(model, np.full((nb, side, side), 100.0), rng)
+    px = (tx + rng.normal(0, 0.2, n)).astype(np.float32)
+    py = (ty + rng.normal(0, 0.2, n)).astype(np.float32)
+    s1 = flux.astype(np.float32)
+    s1v = ((0.01 * flux) ** 2 + 25.0).astype(np.float32)
+    iset, bk = _islands(px, py, st, lr, sn, native, radius=np.full(n, 40.0))
+    return Field(dmb, iv, mogs, polys, px, py, st, lr, e1, e2, sn, s1, s1v,
+                 tx, ty, flux, iset, bk, native, (63, 127))
+
+
+def test_192_parameter_island_takes_the_global_memory_factorisation():
+    f = _cluster_field()
+    plans, hosts, PAD, ds, ws, psfs = field_classes(f, "analytic", ("mixed",))
+    assert len(plans) == 1 and plans[0].n_islands == 1
+    live = int((hosts[0]["keep"] & hosts[0]["mmask"][:, :, None]).sum())
+    assert live > 160
+    g, _ = run_gpu(plans, hosts, PAD, ds, ws, psfs, "analytic", max_steps=2,
+                   native=f.native)
+    o = run_oracle(plans, hosts, PAD, ds, ws, psfs, "analytic", max_steps=2,
+                   native=f.native)
+    r = compare(g[0], o[0], hosts[0]["mmask"])
+    assert r["same_nst"].all() and r["same_flags"].all()
+    assert r["pos_ok"].all(), r["max_dpos"]
+    assert r["flux_ok"].all(), r["max_rel"]
