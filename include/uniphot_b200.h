@@ -123,6 +123,13 @@ typedef struct uph_class_desc {
                                and weight sum_b w over the island window
                                at the final fit (island_solver.py:1615-
                                1637); uph_chunk_out.resid and .resid_w     */
+  int32_t scene_subtract;   /* 1: the field stacks are scene-subtracted; each
+                               island's window gets its members added back
+                               at their seed parameters and S1 fluxes,
+                               sum_k member_s1_flux[k, b] m_k(seed)
+                               (island_solver.py:1795-1818, 2781-2790), in
+                               a private copy of the window, before the
+                               solve; needs uph_chunk_in.member_s1_flux   */
 } uph_class_desc;
 
 /* log-radius offsets of the Re profile (the reference's REPROF_DELTAS_LN,
@@ -166,6 +173,11 @@ typedef struct uph_chunk_in {
   const int32_t* init_n_same; /* [n]     identical-proposal reject run      */
   const float* init_prej;     /* [n*N*6] last rejected proposal             */
   const uint8_t* init_diverged; /* [n]   sticky diverged flag               */
+  /* scene subtract (uph_class_desc.scene_subtract):                          */
+  const float* member_s1_flux;  /* [n*N*nb] members' S1 fluxes (0 for the
+                                   members not subtracted field-wide)      */
+  const float* seed_p;          /* [n*N*6] seed parameters of the add-back;
+                                   NULL = p0                               */
 } uph_chunk_in;
 
 /* Per-island outputs (run_class_chunk's dict).  Shapes as noted. */

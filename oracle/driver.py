@@ -8,8 +8,8 @@ from __future__ import annotations
 
 import numpy as np
 
-from .island_oracle import (MogPsfBand, PolyPsfBand, SersicTable, SolverConfig,
-                            island_inputs_from_host, solve_island)
+from .island_oracle import (IslandSolver, MogPsfBand, PolyPsfBand, SersicTable,
+                            SolverConfig, island_inputs_from_host, solve_island)
 
 
 def psf_bands(psfs, tier: int, mode: str):
@@ -38,12 +38,27 @@ def psf_bands(psfs, tier: int, mode: str):
 
 def _one(args):
     (host, row, B, T, dstack, wstack, psf, table, mode, cfg, max_steps, native, bg, pe, fm, sm,
-     rp, rs) = args
+     rp, rs, ss) = args
     isl = island_inputs_from_host(host, row, B=B, T=T, dstack=dstack,
                                   wstack=wstack, psf=psf, table=table, mode=mode,
                                   native=native, bg_joint=bg)
+    if ss:
+        add_back_members(isl, cfg, np.asarray(host["member_s1_flux"])[row])
     return solve_island(isl, cfg, max_steps, param_errors=pe, flux_marg=fm,
                         source_metrics=sm, re_profile=rp, residual=rs)
+
+
+def add_back_members(isl, cfg, msf):
+    """Scene subtract (island_solver.py:1795-1818, 2781-2790): the window
+    data gain sum_k msf[k, b] m_k at the seed parameters, float32."""
+    s = IslandSolver(isl, cfg)
+    N = isl.stype.shape[0]
+    data = isl.data.copy()
+    for b in range(data.shape[0]):
+        M, _ = s.models_band(b, isl.p0.astype(s.dt), False)
+        add = np.tensordot(np.asarray(msf[:, b], np.float32), M[:N].astype(np.float32), 1)
+        data[b] = (data[b] + add.astype(np.float32)).astype(np.float32)
+    isl.data = data
 
 
 def solve_chunk(host, rows, *, B, T, dstack, wstack, psfs, mode, table_path=None,
@@ -54,7 +69,7 @@ def solve_chunk(host, rows, *, B, T, dstack, wstack, psfs, mode, table_path=None
                 plateau_dlnp_tol: float = 0.5, step_mode: str = "clip",
                 param_errors: bool = False, flux_marg: bool = False,
                 source_metrics: bool = False, re_profile=None,
-                residual: bool = False) -> dict:
+                residual: bool = False, scene_subtract: bool = False) -> dict:
     """``re_profile``: the log-radius offsets of the Re profile, or None."""
     table = SersicTable.load(table_path) if table_path is not None else None
     psf = psf_bands(psfs, T, mode)
@@ -63,8 +78,8 @@ def solve_chunk(host, rows, *, B, T, dstack, wstack, psfs, mode, table_path=None
                        stall_count_mode=stall_count_mode, convergence=convergence,
                        plateau_dlnp_tol=plateau_dlnp_tol, step_mode=step_mode)
     jobs = [(host, int(r), B, T, dstack, wstack, psf, table, mode, cfg, max_steps,
-             native, bg_joint, param_errors, flux_marg, source_metrics, re_profile, residual)
-            for r in rows]
+             native, bg_joint, param_errors, flux_marg, source_metrics, re_profile, residual,
+             scene_subtract) for r in rows]
     if processes > 1 and len(jobs) > 1:
         import multiprocessing as mp
         with mp.get_context("spawn").Pool(processes) as pool:

@@ -36,7 +36,8 @@ def field_classes(f, mode: str, kinds=("star", "mixed"), priors: bool = False):
     hosts = [class_host_arrays(p, pos_x=f.pos_x, pos_y=f.pos_y,
                                source_type=f.source_type, logre=f.logre, ee1=f.ee1,
                                ee2=f.ee2, sersic_n=f.sersic_n, free_n_all=fn,
-                               pos_max_shift_pix=5.0, pad=PAD, **pri) for p in plans]
+                               pos_max_shift_pix=5.0, pad=PAD, s1_flux=f.s1_flux, **pri)
+             for p in plans]
     psfs = f.mog_psfs if mode == "analytic" else f.poly_psfs
     return plans, hosts, PAD, ds, ws, psfs
 
@@ -44,7 +45,7 @@ def field_classes(f, mode: str, kinds=("star", "mixed"), priors: bool = False):
 def run_gpu(plans, hosts, PAD, ds, ws, psfs, mode, max_steps=30, field=None,
             native=0, precision="plain", tc_min_rows=-1, tc_cond_max=-1.0,
             bg_mode="frozen", stall_count_mode="proposals", convergence="legacy",
-            step_mode="clip", param_errors=False):
+            step_mode="clip", param_errors=False, scene_subtract=False):
     from uniphot_b200 import solver
     if field is None:
         field = solver.DeviceField(ds, ws, PAD)
@@ -57,7 +58,7 @@ def run_gpu(plans, hosts, PAD, ds, ws, psfs, mode, max_steps=30, field=None,
             un_freeze_steps=0, has_priors=bool(host["has_priors"]), render_mode=mode,
             native_stamp=native, precision=precision, tc_min_rows=tc_min_rows,
             tc_cond_max=tc_cond_max, bg_mode=bg_mode, stall_count_mode=stall_count_mode,
-            convergence=convergence, step_mode=step_mode)
+            convergence=convergence, step_mode=step_mode, scene_subtract=scene_subtract)
         rows = np.arange(plan.n_islands)
         outs.append(solver.run_class_chunk(kern, tree, host, rows, rows.size,
                                            max_steps, field, field, PAD,
@@ -68,7 +69,7 @@ def run_gpu(plans, hosts, PAD, ds, ws, psfs, mode, max_steps=30, field=None,
 def run_oracle(plans, hosts, PAD, ds, ws, psfs, mode, precision="ref",
                max_steps=30, processes=1, native=0, bg_joint=False,
                stall_count_mode="proposals", convergence="legacy", step_mode="clip",
-               param_errors=False):
+               param_errors=False, scene_subtract=False):
     """The oracle over every class (star classes keep the clip step, as the
     reference exempts them from the trust region)."""
     from oracle.driver import solve_chunk
@@ -78,7 +79,7 @@ def run_oracle(plans, hosts, PAD, ds, ws, psfs, mode, precision="ref",
                         native=native, bg_joint=bg_joint,
                         stall_count_mode=stall_count_mode, convergence=convergence,
                         step_mode=step_mode if p.kind != "star" else "clip",
-                        param_errors=param_errors)
+                        param_errors=param_errors, scene_subtract=scene_subtract)
             for p, h in zip(plans, hosts)]
 
 

@@ -28,7 +28,7 @@ def test_invalid_options_raise_valueerror(bad):
         solver.make_class_kernels(_plan(), 3, 1, **KW, **bad)
 
 
-@pytest.mark.parametrize("opt", [dict(crossband={"rank": 1}), dict(scene_subtract=True)])
+@pytest.mark.parametrize("opt", [dict(crossband={"rank": 1})])
 def test_unbuilt_options_raise(opt):
     with pytest.raises(ValueError, match="not supported"):
         solver.make_class_kernels(_plan("mixed"), 3, 1, **KW, **opt)
@@ -125,3 +125,16 @@ def test_direct_backend_galaxies_raise_in_reference_mode():
     k = solver.make_class_kernels(_plan("star"), 3, 1, **dict(KW, render_backend="direct"),
                                   render_mode="reference")
     assert k.desc.render_mode == 0
+
+
+def test_scene_subtract_sets_the_descriptor_and_needs_s1_fluxes():
+    k = solver.make_class_kernels(_plan("mixed"), 3, 1, **KW, scene_subtract=True)
+    assert k.desc.scene_subtract == 1
+    host = dict(ox=[0], oy=[0], x0b=[0.0], y0b=[0.0], st=np.zeros((1, 1)), sn=np.ones((1, 1)),
+                fn_flag=np.zeros((1, 1), bool), mmask=np.ones((1, 1), bool),
+                keep=np.ones((1, 1, 6), bool), p0=np.zeros((1, 1, 6)),
+                lower=np.zeros((1, 1, 6)), upper=np.ones((1, 1, 6)),
+                prior_mean=np.zeros((1, 1, 6)), prior_inv_sigma=np.zeros((1, 1, 6)),
+                member_s1_flux=None)
+    with pytest.raises(ValueError, match="member_s1_flux"):
+        solver._slice_host(host, np.arange(1), scene_subtract=True)

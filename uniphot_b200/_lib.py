@@ -45,7 +45,7 @@ class ClassDesc(C.Structure):
                 ("tc_cond_max", C.c_float), ("step_tr", C.c_int32),
                 ("param_errors", C.c_int32), ("flux_marg", C.c_int32),
                 ("source_metrics", C.c_int32), ("re_profile", C.c_int32),
-                ("residual", C.c_int32)]
+                ("residual", C.c_int32), ("scene_subtract", C.c_int32)]
 
 
 class ChunkIn(C.Structure):
@@ -53,7 +53,7 @@ class ChunkIn(C.Structure):
         "ox", "oy", "x0b", "y0b", "stype", "n_frozen", "free_n", "mmask",
         "keep", "p0", "lower", "upper", "prior_mean", "prior_inv_sigma",
         "init_lam", "init_chi2", "init_consec", "init_nrej", "init_nst",
-        "init_n_same", "init_prej", "init_diverged")]
+        "init_n_same", "init_prej", "init_diverged", "member_s1_flux", "seed_p")]
 
 
 class ChunkOut(C.Structure):
@@ -343,6 +343,10 @@ def chunk_in(arrays: dict, init_state: dict | None = None):
         lower=f32(arrays["lower"], (n, nP)), upper=f32(arrays["upper"], (n, nP)),
         prior_mean=f32(arrays["prior_mean"], (n, nP)),
         prior_inv_sigma=f32(arrays["prior_inv_sigma"], (n, nP)))
+    if arrays.get("member_s1_flux") is not None:
+        # scene subtract: S1 fluxes and the seeds of the add-back
+        keep["member_s1_flux"] = f32(arrays["member_s1_flux"], (n, N, -1))
+        keep["seed_p"] = f32(arrays["p0"], (n, nP))
     if init_state is not None:
         keep["p0"] = f32(init_state["p"], (n, nP))
         for k, conv in (("lam", f32), ("chi2", f32), ("consec", i32), ("nrej", i32),

@@ -400,6 +400,16 @@ struct Chunk {
   uint8_t* d_div = nullptr;
   uint8_t* d_rail = nullptr;       // trust region: bound-pinned islands
   float* d_cjac = nullptr;         // flux sensitivities (flux_marg only)
+  // scene subtract: the field stacks and window origins the private
+  // windows are copied from, the seeds and S1 fluxes of the add-back
+  bool scene = false;
+  const float* fd = nullptr;
+  const float* fw = nullptr;
+  int fHp = 0, fWp = 0;
+  const int* ox_f = nullptr;
+  const int* oy_f = nullptr;
+  float* d_seed = nullptr;
+  float* d_msf = nullptr;
   bool perr_out = false;           // param_errors requested
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t gexec = nullptr;
@@ -711,6 +721,13 @@ int add_chunk(uph_ctx* ctx, Chunk* ch, const uph_class_desc* cls,
     c.gstamp = cbuf<float>(ctx, ch, "gstamp", (size_t)n * nb * N * 7 * T * T, &rc);
     c.gfft_ws = cbuf<float>(ctx, ch, "gfftws", (size_t)c.gfft_ctas * c.gfft_floats, &rc);
   }
+  if (cls->scene_subtract) {
+    if (!in->member_s1_flux)
+      return set_err(ctx, UPH_ERR_INVALID, "scene_subtract needs member_s1_flux");
+    ch->scene = true;
+    ch->d_seed = cbuf<float>(ctx, ch, "seed", (size_t)n * nP, &rc);
+    ch->d_msf = cbuf<float>(ctx, ch, "msf", (size_t)n * N * nb, &rc);
+  }
   if (cls->re_profile) c.reprof = cbuf<float>(ctx, ch, "reprof", (size_t)n * N * UPH_REPROF_K, &rc);
   if (cls->residual) {
     c.resid = cbuf<float>(ctx, ch, "resid", (size_t)n * B * B, &rc);
@@ -733,6 +750,16 @@ int add_chunk(uph_ctx* ctx, Chunk* ch, const uph_class_desc* cls,
     ch->d_nsame0 = cbuf<int>(ctx, ch, "nsame0", n, &rc);
     ch->d_prej0 = cbuf<float>(ctx, ch, "prej0", (size_t)n * nP, &rc);
     ch->d_divl0 = cbuf<uint8_t>(ctx, ch, "divl0", n, &rc);
+  }
+  float* d_dwin = nullptr;
+  float* d_wwin = nullptr;
+  int* d_ox2 = nullptr;
+  int* d_oy2 = nullptr;
+  if (ch->scene) {
+    d_dwin = cbuf<float>(ctx, ch, "dwin", (size_t)nb * n * B * B, &rc);
+    d_wwin = cbuf<float>(ctx, ch, "wwin", (size_t)nb * n * B * B, &rc);
+    d_ox2 = cbuf<int>(ctx, ch, "ox2", n, &rc);
+    d_oy2 = cbuf<int>(ctx, ch, "oy2", n, &rc);
   }
   if (rc) return rc;
   c.ox = d_ox; c.oy = d_oy; c.x0b = d_x0b; c.y0b = d_y0b; c.stype = d_st;
@@ -761,6 +788,23 @@ int add_chunk(uph_ctx* ctx, Chunk* ch, const uph_class_desc* cls,
   }
   if ((rc = upload(ctx, d_ox, in->ox, sizeof(int) * n, "ox"))) return rc;
   if ((rc = upload(ctx, d_oy, in->oy, sizeof(int) * n, "oy"))) return rc;
+  if (ch->scene) {
+    // the solve reads the private windows: island isl at rows isl*B of a
+    // B-wide stack per band
+    std::vector<int> zx(n, 0), wy(n);
+    for (int i = 0; i < n; ++i) wy[i] = i * B;
+    if ((rc = upload(ctx, d_ox2, zx.data(), sizeof(int) * n, "ox"))) return rc;
+    if ((rc = upload(ctx, d_oy2, wy.data(), sizeof(int) * n, "oy"))) return rc;
+    if ((rc = upload(ctx, ch->d_msf, in->member_s1_flux, sizeof(float) * n * N * nb, "msf")))
+      return rc;
+    if ((rc = upload(ctx, ch->d_seed, in->seed_p ? in->seed_p : in->p0,
+                     sizeof(float) * n * nP, "seed")))
+      return rc;
+    ch->fd = c.dstack; ch->fw = c.wstack; ch->fHp = c.Hp; ch->fWp = c.Wp;
+    ch->ox_f = d_ox; ch->oy_f = d_oy;
+    c.dstack = d_dwin; c.wstack = d_wwin; c.Hp = n * B; c.Wp = B;
+    c.ox = d_ox2; c.oy = d_oy2;
+  }
   if ((rc = upload(ctx, d_x0b, in->x0b, sizeof(float) * n, "x0b"))) return rc;
   if ((rc = upload(ctx, d_y0b, in->y0b, sizeof(float) * n, "y0b"))) return rc;
   if ((rc = upload(ctx, d_st, in->stype, sizeof(int) * n * N, "stype"))) return rc;
@@ -963,6 +1007,13 @@ int job_solve(uph_job* job, int max_steps) {
     int rc = reset_chunk(ctx, ch, s);
     if (rc) return rc;
     Launcher L{job, s, recp};
+    if (ch->scene) {
+      // scene subtract: fresh private windows plus the members at their seeds
+      launch_copy_windows(ch->c, ch->fd, ch->fw, ch->fHp, ch->fWp, ch->ox_f, ch->oy_f, s);
+      L(0, [&] { launch_render(ch->c, ch->d_seed, PH_ALL, s); }, 2);
+      launch_addback(ch->c, ch->d_seed, ch->d_msf, s);
+      ctx->launches += 2;
+    }
     // initial chi2 (fresh chunks) and, for the tensor-core Gram, the fluxes
     // at the starting parameters that its residual row needs
     // (dlnp: the float64 chi2 carry is recomputed at the starting point)

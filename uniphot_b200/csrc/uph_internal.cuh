@@ -631,6 +631,9 @@ void launch_errors_begin(const ClassDev& c, cudaStream_t s);
 void launch_final_errors(const ClassDev& c, cudaStream_t s);
 void launch_flux_marg(const ClassDev& c, cudaStream_t s);
 void launch_source_metrics(const ClassDev& c, cudaStream_t s);
+void launch_copy_windows(const ClassDev& c, const float* fd, const float* fw, int fHp, int fWp,
+                         const int* ox_f, const int* oy_f, cudaStream_t s);
+void launch_addback(const ClassDev& c, const float* seed, const float* msf, cudaStream_t s);
 void launch_residual_coadd(const ClassDev& c, cudaStream_t s);
 void launch_reprof_set(const ClassDev& c, int n, int j, float dk, cudaStream_t s);
 void launch_reprof_store(const ClassDev& c, int n, int j, cudaStream_t s);

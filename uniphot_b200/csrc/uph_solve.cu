@@ -1597,6 +1597,54 @@ __global__ void k_reprof_store(ClassDev c, int n, int j) {
   c.reprof[((size_t)isl * c.N + n) * 12 + j] = __fsub_rn(chi2, c.chi2[isl]);
 }
 
+// Scene subtract: each island's windows copied out of the field stacks
+// into the chunk's private stacks (island isl at rows isl*B.. of a B-wide
+// stack per band), so the add-back below changes no other island's data.
+__global__ void k_copy_windows(ClassDev c, const float* __restrict__ fd,
+                               const float* __restrict__ fw, int fHp, int fWp,
+                               const int* __restrict__ ox_f, const int* __restrict__ oy_f) {
+  const int isl = blockIdx.x / c.nb, b = blockIdx.x % c.nb;
+  if (isl >= c.n_isl) return;
+  const int B = c.B;
+  const size_t fplane = (size_t)fHp * fWp, plane = (size_t)c.Hp * c.Wp;
+  const float* sd = fd + b * fplane + (size_t)oy_f[isl] * fWp + ox_f[isl];
+  const float* sw = fw + b * fplane + (size_t)oy_f[isl] * fWp + ox_f[isl];
+  float* dd = const_cast<float*>(c.dstack) + b * plane + (size_t)isl * B * B;
+  float* dw = const_cast<float*>(c.wstack) + b * plane + (size_t)isl * B * B;
+  for (int pix = threadIdx.x; pix < B * B; pix += blockDim.x) {
+    const int y = pix / B, x = pix - (pix / B) * B;
+    dd[pix] = sd[(size_t)y * fWp + x];
+    dw[pix] = sw[(size_t)y * fWp + x];
+  }
+}
+
+// Scene subtract add-back (island_solver.py:1795-1818): window data +=
+// sum_k member_s1_flux[k, b] m_k, the model rows of the render at the seed
+// parameters, members in slot order.
+__global__ void __launch_bounds__(NT) k_addback(ClassDev c, const float* __restrict__ seed,
+                                                const float* __restrict__ msf) {
+  __shared__ int4 box[UPH_MAXN];
+  __shared__ float fl[UPH_MAXN];
+  const int isl = blockIdx.x / c.nb, b = blockIdx.x % c.nb;
+  if (isl >= c.n_isl) return;
+  const int tid = threadIdx.x, nr = c.isl_nr[isl], B = c.B, Sz = c.Sz;
+  load_boxes(c, isl, seed, box);
+  for (int k = tid; k < nr; k += NT) fl[k] = msf[((size_t)isl * c.N + k) * c.nb + b];
+  __syncthreads();
+  float* dd = const_cast<float*>(c.dstack) + b * (size_t)c.Hp * c.Wp + (size_t)isl * B * B;
+  for (int pix = tid; pix < B * B; pix += NT) {
+    const int wy = pix / B, wx = pix - (pix / B) * B;
+    float model = 0.f;
+    for (int k = 0; k < nr; ++k) {
+      const int4 bx = box[k];
+      const int ly = wy - bx.y, lx = wx - bx.x;
+      if (ly >= 0 && ly < bx.w && lx >= 0 && lx < bx.z)
+        model = fmaf(fl[k], c.stamps[stamp_slot(c, isl, b, k, 0) + (size_t)ly * Sz + lx], model);
+    }
+    dd[pix] = __fadd_rn(dd[pix], model);
+  }
+}
+
 __global__ void k_set_probe(ClassDev c) {
   const int isl = blockIdx.x * blockDim.x + threadIdx.x;
   if (isl >= c.n_isl) return;
@@ -1656,6 +1704,15 @@ void launch_reprof_set(const ClassDev& c, int n, int j, float dk, cudaStream_t s
 
 void launch_reprof_store(const ClassDev& c, int n, int j, cudaStream_t s) {
   k_reprof_store<<<(unsigned)((c.n_isl + 127) / 128), 128, 0, s>>>(c, n, j);
+}
+
+void launch_copy_windows(const ClassDev& c, const float* fd, const float* fw, int fHp, int fWp,
+                         const int* ox_f, const int* oy_f, cudaStream_t s) {
+  k_copy_windows<<<(unsigned)(c.n_isl * c.nb), 256, 0, s>>>(c, fd, fw, fHp, fWp, ox_f, oy_f);
+}
+
+void launch_addback(const ClassDev& c, const float* seed, const float* msf, cudaStream_t s) {
+  k_addback<<<(unsigned)(c.n_isl * c.nb), NT, 0, s>>>(c, seed, msf);
 }
 
 void launch_set_probe(const ClassDev& c, cudaStream_t s) {

@@ -22,8 +22,9 @@ Differences, by design:
   is run (``bucket_stats`` still reports the counts);
 * ``dstack_dev`` is a :class:`DeviceField` (the field stacks resident in
   HBM inside the library context); ``wstack_dev`` is accepted and ignored;
-* options whose kernels are not built (crossband GLS, scene subtract) raise
-  ``ValueError``; the post-convergence passes (``compute_param_errors``,
+* options whose kernels are not built (crossband GLS) raise ``ValueError``;
+  ``scene_subtract`` adds each island's members back at their seeds on the
+  device; the post-convergence passes (``compute_param_errors``,
   ``compute_flux_marg``, ``compute_source_metrics``, ``compute_re_profile``,
   ``want_residual`` / ``return_island_residual``) run on the device;
   the step variants (``step_mode="trust_region"``, ``stall_count_mode=
@@ -228,8 +229,6 @@ def make_class_kernels(plan, n_bands: int, n_terms: int, *, render_backend: str,
         unsupported.append("render_backend='direct' for galaxies")
     if crossband is not None:
         unsupported.append("crossband")
-    if scene_subtract:
-        unsupported.append("scene_subtract")
     if unsupported:
         raise ValueError("not supported by the B200 island solver: "
                          + ", ".join(unsupported))
@@ -247,16 +246,23 @@ def make_class_kernels(plan, n_bands: int, n_terms: int, *, render_backend: str,
         convergence_dlnp=int(convergence == "dlnp"),
         plateau_dlnp_tol=float(plateau_dlnp_tol),
         bg_joint=int(bg_mode == "joint"), tc_cond_max=float(tc_cond_max),
+        scene_subtract=int(bool(scene_subtract)),
         step_tr=int(step_eff == "trust_region"))
     return ClassKernels(desc, render_mode, int(n_bands), str(plan.kind),
                         step_protocol="dlnp" if convergence == "dlnp"
                         else str(stall_count_mode), step_mode=step_eff)
 
 
-def _slice_host(host: dict, rows: np.ndarray) -> dict:
+def _slice_host(host: dict, rows: np.ndarray, scene_subtract: bool = False) -> dict:
     keys = ("ox", "oy", "x0b", "y0b", "st", "sn", "fn_flag", "mmask", "keep",
             "p0", "lower", "upper", "prior_mean", "prior_inv_sigma")
-    return {k: np.asarray(host[k])[rows] for k in keys}
+    out = {k: np.asarray(host[k])[rows] for k in keys}
+    if scene_subtract:
+        if host.get("member_s1_flux") is None:
+            raise ValueError("scene_subtract needs the class host arrays' member_s1_flux "
+                             "(class_host_arrays with s1_flux)")
+        out["member_s1_flux"] = np.asarray(host["member_s1_flux"])[rows]
+    return out
 
 
 def run_class_chunk(kernels: ClassKernels, psf_tree: PsfTree, host: dict,
@@ -280,7 +286,7 @@ def run_class_chunk(kernels: ClassKernels, psf_tree: PsfTree, host: dict,
     if np.any(np.asarray(host["st"])[rows] != SOURCE_STAR):
         dstack_dev.ensure_table()
     N = int(host["mmask"].shape[1])
-    arrays = _slice_host(host, rows)
+    arrays = _slice_host(host, rows, bool(kernels.desc.scene_subtract))
     init = None
     if init_state is not None:
         init = {k: np.asarray(init_state[k]) for k in ("p", "lam", "chi2", "consec",
