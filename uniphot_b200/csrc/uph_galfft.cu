@@ -94,7 +94,7 @@ __global__ void __launch_bounds__(GT) k_gal_fft(ClassDev c, const float* __restr
     for (int im = 0; im < 3; ++im)
       if (need[im]) fft2_forward(img + im * TT, T, T, PP, logP, R, X + PH * im, fbuf, lb, cw, sw);
     // ---- the mixture's transform and its partials on the grid ----
-    const double kk = -2.0 * 9.869604401089358;   // -2 pi^2
+    const double kk = -UPH_TWO_PI2;
     for (int e = tid; e < (int)PH; e += GT) {
       const int w = e / H, u = e - (e / H) * H;
       const double nu = (double)u / PP;

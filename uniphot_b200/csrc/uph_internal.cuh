@@ -477,6 +477,29 @@ __device__ inline void cov_terms(double lr, double e1, double e2, float* cg,
   }
 }
 
+// 2 pi^2: the Gaussian Fourier exponent exp(-2 pi^2 k^T C k)
+constexpr double UPH_TWO_PI2 = 19.739208802178716;
+
+// Segment, interpolation weight and its derivative in n of the Sersic
+// mixture table at index n (the piecewise-linear interpolant of
+// sersic_mog.py:81-100); the index is clamped to the table's range, where
+// the derivative is 0.
+__device__ inline void sersic_segment(const double* knots, int nk, double nmin, double nmax,
+                                      double n, int* seg, double* t, double* dt) {
+  const bool inside = (n > nmin) && (n < nmax);
+  const double nc = fmin(fmax(n, nmin), nmax);
+  int lo = 0, hi = nk;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (knots[mid] <= nc) lo = mid + 1; else hi = mid;
+  }
+  const int s = max(0, min(lo - 1, nk - 2));
+  const double n0 = knots[s], n1 = knots[s + 1];
+  *seg = s;
+  *t = (n1 > n0) ? (nc - n0) / (n1 - n0) : 0.0;
+  *dt = (n1 > n0 && inside) ? 1.0 / (n1 - n0) : 0.0;
+}
+
 // ---- Shared-memory radix-2 FFTs for the Fourier-domain galaxy stamps ----
 // In-place decimation-in-time FFTs of nl lines of length P = 2^logP stored
 // contiguously in shared memory; sign -1 forward, +1 inverse (unnormalised);
@@ -565,7 +588,7 @@ __device__ inline void fft2_inverse_cols(const float2* Xb, const float* fac, boo
       if (dexpo) {
         const float nu = (float)u / (float)P;
         const float nw = (float)(w < P / 2 ? w : w - P) / (float)P;
-        f *= -19.739208802178716f * (d0 * nu * nu + d1 * nw * nw + 2.f * d2 * nu * nw);
+        f *= -(float)UPH_TWO_PI2 * (d0 * nu * nu + d1 * nw * nw + 2.f * d2 * nu * nw);
       }
       const float2 x = Xb[(size_t)w * Hf + u];
       buf[(line << logP) + w] = make_float2(f * x.x, f * x.y);

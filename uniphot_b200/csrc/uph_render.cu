@@ -197,18 +197,7 @@ k_member_setup(ClassDev c, const float* __restrict__ P, int phase) {
       } else {
         n = (double)c.n_frozen[isl * c.N + k];
       }
-      const bool inside = (n > c.tb_nmin) && (n < c.tb_nmax);
-      const double nc = fmin(fmax(n, c.tb_nmin), c.tb_nmax);
-      int lo = 0, hi = c.tb_n;
-      while (lo < hi) {
-        const int mid = (lo + hi) >> 1;
-        if (c.tb_knots[mid] <= nc) lo = mid + 1; else hi = mid;
-      }
-      const int seg = max(0, min(lo - 1, c.tb_n - 2));
-      const double n0 = c.tb_knots[seg], n1 = c.tb_knots[seg + 1];
-      sc.seg = seg;
-      sc.t = (n1 > n0) ? (nc - n0) / (n1 - n0) : 0.0;
-      sc.dt = (n1 > n0 && inside) ? 1.0 / (n1 - n0) : 0.0;
+      sersic_segment(c.tb_knots, c.tb_n, c.tb_nmin, c.tb_nmax, n, &sc.seg, &sc.t, &sc.dt);
       cov_terms((double)pk[2], (double)pk[3], (double)pk[4], rec->cg, rec->dcov);
     }
   } else if (tid == 32) {

@@ -99,15 +99,9 @@ k_sp_gal(const SparseDev d) {
     if (tid == 0) {
       psf_basis_at(d.px[s], d.py[s], d.os, d.nterms, beta);
       // Sersic mixture at the source's index (sersic_mog.py:81-100)
-      const double nc = fmin(fmax((double)d.sn[s], d.tb_nmin), d.tb_nmax);
-      int lo = 0, hi = d.tb_n;
-      while (lo < hi) {
-        const int mid = (lo + hi) >> 1;
-        if (d.tb_knots[mid] <= nc) lo = mid + 1; else hi = mid;
-      }
-      const int seg = max(0, min(lo - 1, d.tb_n - 2));
-      const double n0 = d.tb_knots[seg], n1 = d.tb_knots[seg + 1];
-      const double t = (n1 > n0) ? (nc - n0) / (n1 - n0) : 0.0;
+      int seg;
+      double t, dt;
+      sersic_segment(d.tb_knots, d.tb_n, d.tb_nmin, d.tb_nmax, (double)d.sn[s], &seg, &t, &dt);
       for (int g = 0; g < d.tb_k; ++g) {
         ga[g] = (1 - t) * d.tb_amps[seg * d.tb_k + g] + t * d.tb_amps[(seg + 1) * d.tb_k + g];
         gv[g] = exp((1 - t) * d.tb_lv[seg * d.tb_k + g] + t * d.tb_lv[(seg + 1) * d.tb_k + g]);
@@ -125,7 +119,7 @@ k_sp_gal(const SparseDev d) {
     }
     __syncthreads();
     fft2_forward(img, H, W, PP, logP, R, X, fbuf, lb, cw, sw);
-    const double kk = -2.0 * 9.869604401089358;
+    const double kk = -UPH_TWO_PI2;
     for (int e = tid; e < (int)PH; e += ST) {
       const int w = e / Hf, u = e - (e / Hf) * Hf;
       const double nu = (double)u / PP;
