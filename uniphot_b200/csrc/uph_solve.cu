@@ -828,6 +828,12 @@ __device__ void lu_solve(double* M, int n, int* piv, double* x) {
   __syncthreads();
 }
 
+// Trust-region radius update (island_solver.py:154-163): Nocedal & Wright
+// Alg. 4.1 gain-ratio thresholds, shrink and expand factors; a step counts
+// as reaching the boundary at 99% of the radius.
+constexpr double TR_ETA_LO = 0.25, TR_ETA_HI = 0.75;
+constexpr double TR_SHRINK = 0.25, TR_EXPAND = 2.0, TR_AT_BOUNDARY = 0.99;
+
 // Sum of one double per thread over the block, in a fixed order (warp
 // butterflies, then the warps' partials in warp order); every thread gets
 // the total.  red holds NT / 32 doubles.
@@ -981,7 +987,7 @@ __device__ void step_dogleg(const ClassDev& c, int isl, int nL, const double* M,
     t[0] = pred;
     t[1] = Dr;
     t[2] = dmax;
-    t[3] = (s_norm >= 0.99 * Dr) ? 1.0 : 0.0;
+    t[3] = (s_norm >= TR_AT_BOUNDARY * Dr) ? 1.0 : 0.0;
   }
 }
 
@@ -1169,8 +1175,9 @@ __global__ void k_accept(ClassDev c, int phase) {
     const double pred = t[0], Dr = t[1], dmax = t[2];
     const double actual = (double)__fsub_rn(chi2, chi2_try);
     const double rho = actual / (pred > 0.0 ? pred : 1e-30);
-    const double dn = (rho < 0.25) ? Dr * 0.25
-                                   : ((rho > 0.75 && t[3] != 0.0) ? fmin(Dr * 2.0, dmax) : Dr);
+    const double dn = (rho < TR_ETA_LO)
+                          ? Dr * TR_SHRINK
+                          : ((rho > TR_ETA_HI && t[3] != 0.0) ? fmin(Dr * TR_EXPAND, dmax) : Dr);
     lam_new = (float)dn;
   } else {
     lam_new = accept ? fmaxf(__fmul_rn(lam, 0.1f), 1e-9f) : fminf(__fmul_rn(lam, 10.0f), 1e6f);
