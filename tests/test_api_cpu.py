@@ -138,3 +138,33 @@ def test_scene_subtract_sets_the_descriptor_and_needs_s1_fluxes():
                 member_s1_flux=None)
     with pytest.raises(ValueError, match="member_s1_flux"):
         solver._slice_host(host, np.arange(1), scene_subtract=True)
+
+
+def test_re_profile_interval_edges():
+    """A side whose profile never reaches 1 ends at its outermost offset; a
+    non-finite profile value counts as beyond 1 (island_plan.py:913-952)."""
+    from uniphot_b200.plan import REPROF_DELTAS_LN, re_profile_interval
+    d = REPROF_DELTAS_LN.astype(np.float64)
+    prof = np.full((1, 1, d.size), 0.2, np.float32)
+    prof[0, 0, d == 0.25] = np.nan                 # +0.25 counts as >= 1
+    res_p = np.zeros((1, 1, 6), np.float32)
+    lo, hi = re_profile_interval(res_p, prof, d, np.array([0]), np.array([0]),
+                                 np.array([[True]]))
+    np.testing.assert_allclose(lo[0], np.exp(-2.5), rtol=1e-6)
+    # crossing between 0.1 (profile 0.2) and 0.25 (infinite): t = 0.8 / inf -> 0
+    np.testing.assert_allclose(hi[0], np.exp(0.1), rtol=1e-6)
+
+
+def test_catalog_errors_round_source_and_degenerate_variances():
+    from uniphot_b200.plan import catalog_errors
+    res_p = np.zeros((1, 1, 6), np.float32)          # ee = 0: direction undefined
+    perr = np.zeros((1, 1, 13), np.float32)
+    perr[0, 0, :6] = [np.inf, -1.0, 0.04, 0.01, 0.01, 0.0]
+    host = dict(keep=np.ones((1, 1, 6), bool), fn_flag=np.array([[False]]),
+                prior_inv_sigma=np.zeros((1, 1, 6), np.float32))
+    e = catalog_errors(res_p, perr, host, np.array([0]), np.array([0]),
+                       np.ones((1, 1), np.float32))
+    assert np.isnan(e["pos_x_err"][0]) and np.isnan(e["pos_y_err"][0])
+    np.testing.assert_allclose(e["re_err"][0], 0.2, rtol=1e-6)
+    assert np.isnan(e["ell_err"][0]) and np.isnan(e["theta_err"][0])
+    assert np.isnan(e["sersic_n_err"][0]) and np.isnan(e["pos_x_prior_frac"][0])

@@ -125,3 +125,11 @@ def test_grid_galaxy_stamp_matches_the_island_fft_render():
     cg, _ = O.cov_terms(float(p[8]), float(p[9]), float(p[10]))
     np.testing.assert_allclose(SO.galaxy_fft(psf.astype(np.float64), amps, vars_, core, cg), S,
                                rtol=1e-9, atol=1e-12)
+
+
+def test_neighbor_list_skips_non_finite_positions():
+    x = np.array([0.0, 5.0, np.nan, 10.0])
+    y = np.array([0.0, 3.0, 1.0, np.inf])
+    idx, mask = build_neighbor_list(x, y, 15, 15, k_max=4)
+    assert not mask[2].any() and not mask[3].any()
+    assert set(idx[0][mask[0]].tolist()) == {1} and set(idx[1][mask[1]].tolist()) == {0}
