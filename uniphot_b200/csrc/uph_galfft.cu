@@ -37,6 +37,7 @@ __global__ void __launch_bounds__(GT) k_gal_fft(ClassDev c, const float* __restr
   __shared__ float cw[MAXP], sw[MAXP];
   __shared__ int need[7];
   __shared__ int is_gal;
+  __shared__ float fa[UPH_MAXGAL], fv[UPH_MAXGAL], fda[UPH_MAXGAL], fdv[UPH_MAXGAL];
   const int tid = threadIdx.x;
   const int T = c.T, PP = c.fft_P, H = PP / 2 + 1;
   const int logP = 31 - __clz(PP);
@@ -75,6 +76,12 @@ __global__ void __launch_bounds__(GT) k_gal_fft(ClassDev c, const float* __restr
     __syncthreads();
     if (!is_gal) continue;
     const MemberRecord* rec = c.mrec + ((size_t)isl * c.nb + b) * c.N + k;
+    for (int g = tid; g < rec->ngal; g += GT) {
+      fa[g] = (float)rec->ga[g];
+      fv[g] = (float)rec->gv[g];
+      fda[g] = (float)rec->gda[g];
+      fdv[g] = (float)rec->gdv[g];
+    }
     // ---- PSF stamp at the member position and its position partials ----
     for (int e = tid; e < TT; e += GT) {
       const int i = e / T, j = e - (e / T) * T;
@@ -93,24 +100,26 @@ __global__ void __launch_bounds__(GT) k_gal_fft(ClassDev c, const float* __restr
     __syncthreads();
     for (int im = 0; im < 3; ++im)
       if (need[im]) fft2_forward(img + im * TT, T, T, PP, logP, R, X + PH * im, fbuf, lb, cw, sw);
-    // ---- the mixture's transform and its partials on the grid ----
-    const double kk = -UPH_TWO_PI2;
+    // ---- the mixture's transform and its partials on the grid, in float32
+    //      as the reference evaluates it ----
+    const float kk = -(float)UPH_TWO_PI2;
+    const float cg0 = rec->cg[0], cg1 = rec->cg[1], cg2 = rec->cg[2];
+    const int ng = rec->ngal;
     for (int e = tid; e < (int)PH; e += GT) {
       const int w = e / H, u = e - (e / H) * H;
-      const double nu = (double)u / PP;
-      const double nw = (double)(w < PP / 2 ? w : w - PP) / PP;
-      const double ex = kk * ((double)rec->cg[0] * nu * nu + (double)rec->cg[1] * nw * nw +
-                              2.0 * (double)rec->cg[2] * nu * nw);
-      double F = 0.0, F1 = 0.0, dF = 0.0;
-      for (int g = 0; g < rec->ngal; ++g) {
-        const double E = exp(rec->gv[g] * ex);
-        F += rec->ga[g] * E;
-        F1 += rec->ga[g] * rec->gv[g] * E;
-        dF += (rec->gda[g] + rec->ga[g] * rec->gdv[g] * ex) * E;
+      const float nu = (float)u / (float)PP;
+      const float nw = (float)(w < PP / 2 ? w : w - PP) / (float)PP;
+      const float ex = kk * (cg0 * nu * nu + cg1 * nw * nw + 2.f * cg2 * nu * nw);
+      float F = 0.f, F1 = 0.f, dF = 0.f;
+      for (int g = 0; g < ng; ++g) {
+        const float E = expf(fv[g] * ex);
+        F = fmaf(fa[g], E, F);
+        F1 = fmaf(fa[g] * fv[g], E, F1);
+        dF = fmaf(fmaf(fa[g] * fdv[g], ex, fda[g]), E, dF);
       }
-      Fs[e] = (float)F;
-      Fs[PH + e] = (float)F1;
-      Fs[2 * PH + e] = (float)dF;
+      Fs[e] = F;
+      Fs[PH + e] = F1;
+      Fs[2 * PH + e] = dF;
     }
     __syncthreads();
     // ---- inverse transforms of the needed products, cropped to T x T ----

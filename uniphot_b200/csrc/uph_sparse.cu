@@ -119,16 +119,16 @@ k_sp_gal(const SparseDev d) {
     }
     __syncthreads();
     fft2_forward(img, H, W, PP, logP, R, X, fbuf, lb, cw, sw);
-    const double kk = -UPH_TWO_PI2;
+    // the mixture's transform in float32, as the reference evaluates it
+    const float kk = -(float)UPH_TWO_PI2;
     for (int e = tid; e < (int)PH; e += ST) {
       const int w = e / Hf, u = e - (e / Hf) * Hf;
-      const double nu = (double)u / PP;
-      const double nw = (double)(w < PP / 2 ? w : w - PP) / PP;
-      const double ex = kk * ((double)cg[0] * nu * nu + (double)cg[1] * nw * nw +
-                              2.0 * (double)cg[2] * nu * nw);
-      double F = 0.0;
-      for (int g = 0; g < d.tb_k; ++g) F += ga[g] * exp(gv[g] * ex);
-      Fs[e] = (float)F;
+      const float nu = (float)u / (float)PP;
+      const float nw = (float)(w < PP / 2 ? w : w - PP) / (float)PP;
+      const float ex = kk * (cg[0] * nu * nu + cg[1] * nw * nw + 2.f * cg[2] * nu * nw);
+      float F = 0.f;
+      for (int g = 0; g < d.tb_k; ++g) F = fmaf((float)ga[g], expf((float)gv[g] * ex), F);
+      Fs[e] = F;
     }
     __syncthreads();
     fft2_inverse_cols(X, Fs, false, 0.f, 0.f, 0.f, H, PP, logP, Cc, fbuf, lb, cw, sw);
