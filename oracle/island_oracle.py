@@ -393,6 +393,10 @@ class IslandInput:
     mode: str                # "reference" | "analytic"
     native: int = 0          # star support side (0 = the tier)
     bg_joint: bool = False   # planar background (1, X, Y) solved with the fluxes
+    # cross-band GLS (island_solver.py:607-723, 867-919): {"rank": r,
+    # "u": (r, n_b), "lam": (r,)} and the island's amplitude scale; None = off
+    crossband: dict | None = None
+    cb_scale: float = 1.0
 
 
 @dataclass
@@ -716,12 +720,17 @@ class IslandSolver:
         penalty's float32 squares summed in float64
         (island_solver.py:741-758)."""
         c = 0.0
+        resids = []
         for b in range(self.nb):
             M, _ = self.models_band(b, p, False)
             f, _, _ = self.fluxes_band(M, self.isl.data[b], self.isl.w[b])
-            cb, _ = self.chi2_band(M, self.isl.data[b], self.isl.w[b], f)
+            cb, r = self.chi2_band(M, self.isl.data[b], self.isl.w[b], f)
             c += cb
+            resids.append(r)
         isl = self.isl
+        if isl.crossband is not None:
+            q, s_b, wk = self._cb_filters(p)
+            c -= self._cb_chi2_corr(resids, q, s_b, wk)[0]
         if isl.has_priors:
             keep = (isl.keep & isl.mmask[:, None]).reshape(-1)
             t = (isl.prior_inv_sigma.astype(self.dt) * (p - isl.prior_mean).astype(self.dt))
@@ -737,14 +746,73 @@ class IslandSolver:
         t = isl.prior_inv_sigma * (p - isl.prior_mean)
         return float(np.sum(np.where(keep, t * t, 0.0)))
 
+    def _cb_filters(self, p):
+        """Cross-band GLS channels (island_solver.py:607-666): per band the
+        filter q_b = rfft2 of the PSF at the members' mean position (zero-
+        padded to, or centre-cropped to, B x B), the channel weights
+        s_b = sqrt(lam) sqrt(max(cb_scale, 0)) u_b, and the rfft half-plane
+        weights (2, with 1 on the zero and Nyquist columns)."""
+        isl = self.isl
+        cb = isl.crossband
+        if isl.mode != "reference":
+            raise ValueError("cross-band GLS needs the pixelised PSF (reference mode)")
+        B, T = isl.B, isl.T
+        pp = np.asarray(p, np.float32).reshape(self.N, 6)
+        mm = isl.mmask.astype(np.float32)
+        den = np.float32(max(float(mm.sum()), 1.0))
+        cx = float(np.float32((pp[:, 0] * mm).sum()) / den)
+        cy = float(np.float32((pp[:, 1] * mm).sum()) / den)
+        u = np.asarray(cb["u"], np.float64)
+        sl = np.sqrt(np.clip(np.asarray(cb["lam"], np.float64), 0.0, None))
+        scale = math.sqrt(max(float(isl.cb_scale), 0.0))
+        q = []
+        for b in range(self.nb):
+            st = isl.psf[b].stamp(cx, cy, np.float64)[0]
+            if T <= B:
+                z = np.zeros((B, B))
+                z[:T, :T] = st
+            else:
+                o = (T - B) // 2
+                z = st[o:o + B, o:o + B]
+            q.append(np.fft.rfft2(z))
+        wk = np.full((B, B // 2 + 1), 2.0)
+        wk[:, 0] = 1.0
+        if B % 2 == 0:
+            wk[:, -1] = 1.0
+        s_b = (sl * scale)[None, :] * u.T            # (n_b, r)
+        return np.stack(q), s_b, wk
+
+    def _cb_chi2_corr(self, resids, q, s_b, wk):
+        """Woodbury correction (1/B^2) sum_k w_k z^H M^-1 z of the GLS chi2
+        (island_solver.py:686-712)."""
+        B = self.isl.B
+        r_ = s_b.shape[1]
+        z = np.zeros((r_,) + wk.shape, complex)
+        Mc = np.zeros((r_, r_) + wk.shape)
+        for b, rb in enumerate(resids):
+            rh = np.fft.rfft2(rb.astype(np.float64).reshape(B, B))
+            z += s_b[b][:, None, None] * (np.conj(q[b]) * rh)[None]
+            Mc += s_b[b][:, None, None, None] * s_b[b][None, :, None, None] * \
+                (np.abs(q[b]) ** 2)[None, None]
+        Mk = np.moveaxis(Mc, (0, 1), (-2, -1)) + np.eye(r_)
+        zk = np.moveaxis(z, 0, -1)
+        sol = np.linalg.solve(Mk, zk[..., None])[..., 0]
+        return float(np.sum(wk * np.real(np.sum(np.conj(zk) * sol, axis=-1)))) / (B * B), \
+            Mk, zk
+
     def chi2_of(self, p):
         dt = self.dt
         c = dt(0.0)
+        resids = []
         for b in range(self.nb):
             M, _ = self.models_band(b, p, False)
             f, _, _ = self.fluxes_band(M, self.isl.data[b], self.isl.w[b])
-            cb, _ = self.chi2_band(M, self.isl.data[b], self.isl.w[b], f)
+            cb, r = self.chi2_band(M, self.isl.data[b], self.isl.w[b], f)
             c = dt(c + dt(cb))
+            resids.append(r)
+        if self.isl.crossband is not None:
+            q, s_b, wk = self._cb_filters(p)
+            c = dt(c - dt(self._cb_chi2_corr(resids, q, s_b, wk)[0]))
         if self.isl.has_priors:
             c = dt(c + dt(self.prior_pen(p)))
         return c
@@ -759,11 +827,16 @@ class IslandSolver:
         nP, N = self.nP, self.N
         H = np.zeros((nP, nP), dtype=dt)
         g = np.zeros(nP, dtype=dt)
+        cbx = self.isl.crossband is not None
+        cb_r, cb_J = [], []
         for b in range(self.nb):
             d, w = self.isl.data[b], self.isl.w[b]
             M, Ds = self.models_band(b, p, True)
             f, f64, A64 = self.fluxes_band(M, d, w)
             _, r = self.chi2_band(M, d, w, f)
+            if cbx:
+                cb_r.append(r)
+                cb_J.append(np.zeros((nP, r.size)))
             if not Ds:
                 continue
             w64 = w.astype(np.float64).reshape(-1)
@@ -790,6 +863,8 @@ class IslandSolver:
                 rows.append(J)
                 idx.append(6 * k + j)
             Jb = np.stack(rows)
+            if cbx:
+                cb_J[-1][np.array(idx)] = Jb
             if flux_jac is not None:
                 flux_jac[b] = (np.array(idx), np.stack(cjs))
             Hb = Jb @ Jb.T
@@ -801,6 +876,23 @@ class IslandSolver:
             gf[ii] = gb
             H = (H + Hf.astype(dt)).astype(dt)
             g = (g + gf.astype(dt)).astype(dt)
+        if cbx:
+            # Woodbury corrections of the GLS Gauss-Newton system
+            # (island_solver.py:894-919): JZ_p = sum_b s_b conj(q_b) FFT(J_b,p)
+            B = self.isl.B
+            q, s_b, wk = self._cb_filters(p)
+            _, Mk, zk = self._cb_chi2_corr(cb_r, q, s_b, wk)
+            JZ = np.zeros((nP, s_b.shape[1]) + wk.shape, complex)
+            for b in range(self.nb):
+                Jh = np.fft.rfft2(cb_J[b].reshape(nP, B, B))
+                JZ += s_b[b][None, :, None, None] * (np.conj(q[b])[None] * Jh)[:, None]
+            JZk = np.moveaxis(JZ, (0, 1), (-2, -1))          # (B, Bh, nP, r)
+            solz = np.linalg.solve(Mk, zk[..., None])[..., 0]
+            solJ = np.linalg.solve(Mk, np.conj(np.swapaxes(JZk, -1, -2)))
+            Hc2 = np.real(np.einsum("ab,abpr,abrq->pq", wk, JZk, solJ)) / (B * B)
+            gc2 = np.real(np.einsum("ab,abpr,abr->p", wk, np.conj(JZk), solz)) / (B * B)
+            H = (H - Hc2.astype(dt)).astype(dt)
+            g = (g - gc2.astype(dt)).astype(dt)
         return H, g
 
     def _keep(self, nsteps):
