@@ -38,10 +38,13 @@ def psf_bands(psfs, tier: int, mode: str):
 
 def _one(args):
     (host, row, B, T, dstack, wstack, psf, table, mode, cfg, max_steps, native, bg, pe, fm, sm,
-     rp, rs, ss) = args
+     rp, rs, ss, cb) = args
     isl = island_inputs_from_host(host, row, B=B, T=T, dstack=dstack,
                                   wstack=wstack, psf=psf, table=table, mode=mode,
                                   native=native, bg_joint=bg)
+    if cb is not None:
+        isl.crossband = cb
+        isl.cb_scale = float(np.asarray(host["cb_scale"])[row])
     if ss:
         add_back_members(isl, cfg, np.asarray(host["member_s1_flux"])[row])
     return solve_island(isl, cfg, max_steps, param_errors=pe, flux_marg=fm,
@@ -69,8 +72,11 @@ def solve_chunk(host, rows, *, B, T, dstack, wstack, psfs, mode, table_path=None
                 plateau_dlnp_tol: float = 0.5, step_mode: str = "clip",
                 param_errors: bool = False, flux_marg: bool = False,
                 source_metrics: bool = False, re_profile=None,
-                residual: bool = False, scene_subtract: bool = False) -> dict:
-    """``re_profile``: the log-radius offsets of the Re profile, or None."""
+                residual: bool = False, scene_subtract: bool = False,
+                crossband: dict | None = None) -> dict:
+    """``re_profile``: the log-radius offsets of the Re profile, or None;
+    ``crossband``: the cross-band GLS channels ({"rank", "u", "lam"}, with
+    the per-island scale from ``host["cb_scale"]``), or None."""
     table = SersicTable.load(table_path) if table_path is not None else None
     psf = psf_bands(psfs, T, mode)
     cfg = SolverConfig(reg=reg, pos_step_max=pos_step_max, ftol_rel=ftol_rel,
@@ -79,7 +85,7 @@ def solve_chunk(host, rows, *, B, T, dstack, wstack, psfs, mode, table_path=None
                        plateau_dlnp_tol=plateau_dlnp_tol, step_mode=step_mode)
     jobs = [(host, int(r), B, T, dstack, wstack, psf, table, mode, cfg, max_steps,
              native, bg_joint, param_errors, flux_marg, source_metrics, re_profile, residual,
-             scene_subtract) for r in rows]
+             scene_subtract, crossband) for r in rows]
     if processes > 1 and len(jobs) > 1:
         import multiprocessing as mp
         with mp.get_context("spawn").Pool(processes) as pool:

@@ -12,13 +12,15 @@ ROOT = Path(__file__).resolve().parents[1]
 TABLE = ROOT / "uniphot_b200" / "data" / "sersic_mog_table.npz"
 
 
-def field_classes(f, mode: str, kinds=("star", "mixed"), priors: bool = False):
+def field_classes(f, mode: str, kinds=("star", "mixed"), priors: bool = False,
+                  tier_ladder=None):
     """(plans, hosts, PAD, dstack, wstack, psfs) for a synthetic field;
     ``priors`` adds Gaussian priors on every member's position (0.3 px) and
     on galaxies' radius (50%), ellipticity (0.2), angle (20 deg) and Sersic
     index (1.0), centred on the seeds."""
     plans, _ = plan_island_classes(f.island_set, f.buckets, f.source_type, f.logre,
-                                   f.sersic_n, f.native, tier_ladder=f.tier_ladder)
+                                   f.sersic_n, f.native,
+                                   tier_ladder=f.tier_ladder if tier_ladder is None else tier_ladder)
     plans = [p for p in plans if p.kind in kinds]
     PAD = max(p.bbox_class for p in plans) + 8
     nb, H, W = f.data_minus_bg.shape
