@@ -7,8 +7,9 @@ Follows ``tract7dt/fit/grid_gpu/forced_phot_sparse.py``:
 * stamps: the polynomial PSF at each source's full-image position
   (``psf_polynomial.py:134-197``) -- for extended sources the "fft"
   backend's galaxy stamp (``source_model.py:304-318``,
-  ``sersic_mog.py:153-194``) -- renormalised to unit sum on the all-star
-  path (``:126-170``), Lanczos-3
+  ``sersic_mog.py:153-194``), or the "direct" backend's EXP stamp
+  (``source_model.py:218-256, 298-303``) -- renormalised to unit sum on the
+  all-star path (``:126-170``), Lanczos-3
   shifted by the fractional grid-local position (``:126-170``,
   ``lanczos.py:50-181``), placed at ``stamp_top_left`` (``:255-269``);
 * ``solver_inner`` (``:498-555``): per-source diagonal, data and background
@@ -49,10 +50,60 @@ def galaxy_fft(psf_img, amps, vars_, core, cg):
     return np.fft.irfft2(P * F, s=(pad, pad))[:H, :W] + core * psf_img
 
 
-def stamps(psf, pos_x, pos_y, grid_x0, grid_y0, renorm=True, gal=None, table=None):
+def exp_profile_direct(H, W, logre, ee1, ee2, amp, var):
+    """The "direct" backend's intrinsic exponential profile
+    (source_model.py:218-256): the six-Gaussian mixture ``amp``/``var``
+    sampled at pixel centres on a grid centred at (W//2, H//2), the
+    quadratic form clipped at 200, normalised to unit sum."""
+    y, x = np.meshgrid(np.arange(H) - H // 2, np.arange(W) - W // 2, indexing="ij")
+    re = float(np.clip(np.exp(logre), 0.1, 1000.0))
+    ee = float(np.hypot(ee1, ee2))
+    e = 1.0 - np.exp(-ee)
+    inv_ba = min((1.0 + e) / max(1.0 - e, 1e-4), 1000.0)
+    th = 0.5 * np.arctan2(ee2, ee1)
+    # rows of the shape matrix: (a, b) and (c, d)
+    a, b = re * np.cos(th) / inv_ba, re * np.sin(th)
+    c, d = -re * np.sin(th) / inv_ba, re * np.cos(th)
+    prof = np.zeros((H, W))
+    for am, v in zip(np.asarray(amp, np.float64), np.asarray(var, np.float64)):
+        sxx, sxy, syy = v * (a * a + b * b), v * (a * c + b * d), v * (c * c + d * d)
+        det = max(sxx * syy - sxy * sxy, 1e-12)
+        q = (syy * x * x - 2.0 * sxy * x * y + sxx * y * y) / det
+        prof += am / (2.0 * np.pi * np.sqrt(det)) * np.exp(-0.5 * np.minimum(q, 200.0))
+    tot = prof.sum()
+    return prof / tot if tot > 0 else prof
+
+
+def convolve_same(img, ker):
+    """Linear 2-D convolution cropped to ``img``'s shape, centred as
+    scipy's / JAX's ``mode="same"``: the full result's rows and columns from
+    (K - 1) // 2 on, K the kernel side."""
+    H, W = img.shape
+    kh, kw = ker.shape
+    full = np.zeros((H + kh - 1, W + kw - 1))
+    for i in range(kh):
+        for j in range(kw):
+            full[i:i + H, j:j + W] += ker[i, j] * img
+    oy, ox = (kh - 1) // 2, (kw - 1) // 2
+    return full[oy:oy + H, ox:ox + W]
+
+
+def exp_stamp_direct(psf_img, logre, ee1, ee2, amp, var):
+    """The "direct" backend's EXP stamp (source_model.py:298-303): the
+    profile convolved with the PSF stamp ("same") and renormalised to unit
+    box sum."""
+    H, W = psf_img.shape
+    s = convolve_same(exp_profile_direct(H, W, logre, ee1, ee2, amp, var), psf_img)
+    tot = s.sum()
+    return s / tot if tot > 0 else s
+
+
+def stamps(psf, pos_x, pos_y, grid_x0, grid_y0, renorm=True, gal=None, table=None,
+           backend="fft", exp_mog=None):
     """(n, H, W) float32 Lanczos-shifted PSF stamps (unit sum when
     ``renorm``); ``gal`` = (source_type, logre, ee1, ee2, sersic_n) renders
-    the extended sources with the "fft" backend from ``table``."""
+    the extended sources with the "fft" backend from ``table``, or, with
+    ``backend="direct"``, the EXP sources from ``exp_mog`` = (amp, var)."""
     f32 = np.float32
     coefs = np.asarray(psf.coefs, np.float32)
     nt = coefs.shape[-1]
@@ -63,7 +114,13 @@ def stamps(psf, pos_x, pos_y, grid_x0, grid_y0, renorm=True, gal=None, table=Non
         Y = float(f32((f32(y) - f32(psf.y_origin)) / f32(psf.y_scale)))
         b, _, _ = poly_basis(X, Y, nt)
         raw = (coefs.astype(np.float64) @ b).astype(np.float32)
-        if gal is not None and int(gal[0][s_i]) != 0:
+        if gal is not None and int(gal[0][s_i]) != 0 and backend == "direct":
+            if int(gal[0][s_i]) != 1:
+                raise ValueError("the direct backend renders STAR and EXP sources only")
+            raw = exp_stamp_direct(raw.astype(np.float64), float(gal[1][s_i]),
+                                   float(gal[2][s_i]), float(gal[3][s_i]),
+                                   *exp_mog).astype(np.float32)
+        elif gal is not None and int(gal[0][s_i]) != 0:
             amps, vars_, core = table.lookup(float(gal[4][s_i]))[:3]
             cg, _ = cov_terms(float(gal[1][s_i]), float(gal[2][s_i]), float(gal[3][s_i]))
             raw = galaxy_fft(raw.astype(np.float64), amps, vars_, core, cg).astype(np.float32)
@@ -89,13 +146,14 @@ def bg_basis(h, w, x0, y0, xo, xs, yo, ys, order):
 
 def solve_band(data, invvar, pix_good, pos_x, pos_y, psf, grid_x0, grid_y0,
                bg_norm, order, nbr_idx, nbr_mask, reg=1e-9, renorm=True, gal=None,
-               table=None):
+               table=None, backend="fft", exp_mog=None):
     """(fluxes, bg_coefs, flux_var, bg_var) of one band, float32.  With
-    extended sources in ``gal`` no stamp is renormalised."""
+    extended sources in ``gal`` no stamp is renormalised (the "direct"
+    backend's EXP stamps carry their own unit-sum normalisation)."""
     h, w = data.shape
     mixed = gal is not None and bool(np.any(np.asarray(gal[0]) != 0))
     S = stamps(psf, pos_x, pos_y, grid_x0, grid_y0, renorm and not mixed,
-               gal if mixed else None, table)
+               gal if mixed else None, table, backend, exp_mog)
     n, H, W = S.shape
     x = np.asarray(pos_x, np.float32) - np.float32(grid_x0)
     y = np.asarray(pos_y, np.float32) - np.float32(grid_y0)
