@@ -362,6 +362,16 @@ typedef struct uph_sparse_band {
   const float* ee1;
   const float* ee2;
   const float* sersic_n;
+  /* "direct" backend (source_model.py:218-256, 298-303) when render_direct
+   * is 1: EXP sources are the exp_k-Gaussian mixture exp_amp / exp_var
+   * sampled at pixel centres around the stamp centre, normalised, convolved
+   * with the PSF stamp (same size, centred as mode "same") and renormalised
+   * to unit sum; only STAR and EXP types are accepted and no Sersic table is
+   * read.  0: the "fft" backend above. */
+  int32_t render_direct;
+  int32_t exp_k;              /* 1..16                                        */
+  const float* exp_amp;       /* [exp_k]                                      */
+  const float* exp_var;       /* [exp_k]                                      */
 } uph_sparse_band;
 
 typedef struct uph_sparse_out {

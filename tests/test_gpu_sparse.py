@@ -105,3 +105,30 @@ def test_sparse_band_with_galaxies_fft_backend(ctx):
                       g["gx0"], g["gy0"], g["bn"], 1, idx, mask, reg=1e-9,
                       gal=(st, lr, e1, e2, sn), table=SersicTable.load(TABLE))
     _check(r, o)
+
+
+def test_sparse_band_exp_direct_backend(ctx):
+    """Stars and EXP galaxies on the legacy "direct" backend
+    (source_model.py:218-256, 298-303): the pixel-centre exponential mixture
+    convolved with the PSF stamp and renormalised, then the stars' Lanczos
+    shift.  Checked against the oracle and against the reference's own
+    solve of the same grid (tests/golden/sparse_exp_direct.npz)."""
+    import sys
+    from pathlib import Path
+    from oracle import sparse_oracle as SO
+    from uniphot_b200.sparse import exp_mixture
+    golden = Path(__file__).parent / "golden"
+    sys.path.insert(0, str(golden))
+    from make_golden_sparse import case_inputs
+    g, idx, mask, order, gal, backend = case_inputs("exp_direct")
+    assert backend == "direct"
+    inp = _inputs(g)
+    inp.source_type, inp.logre, inp.ee1, inp.ee2, inp.sersic_n = gal
+    inp.render_backend = "direct"
+    r = solve_band_sparse(inp, idx, mask, reg=1e-9, bg_poly_order=order, context=ctx)
+    o = SO.solve_band(g["data"], g["invvar"], g["good"], g["px"], g["py"], g["psf"],
+                      g["gx0"], g["gy0"], g["bn"], order, idx, mask, reg=1e-9, gal=gal,
+                      backend="direct", exp_mog=exp_mixture())
+    _check(r, o)
+    ref = np.load(golden / "sparse_exp_direct.npz")
+    _check(r, (ref["fluxes"], ref["bg_coefs"], ref["flux_var"], ref["bg_var"]))

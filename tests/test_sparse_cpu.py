@@ -92,7 +92,12 @@ def test_oracle_recovers_noise_free_fluxes_and_background(order):
     assert np.all(fv > 0) and np.all(bv > 0)
 
 
-def test_extended_sources_raise():
+@pytest.mark.parametrize("stype,backend", [((0, 2, 0), "direct"), ((0, 3, 1), "direct"),
+                                           ((0, 1, 0), "bogus")])
+def test_direct_backend_rejects_dev_sersic_and_unknown_backends(stype, backend):
+    """The "direct" backend renders STAR and EXP only (the reference's
+    pipeline rejects DEV/SERSIC there, pipeline.py:1582-1586); checked on
+    the host before any device call."""
     from uniphot_b200.sparse import GridBandInputs, solve_band_sparse
     g = _grid(n=3)
     h, w = g["data"].shape
@@ -100,9 +105,21 @@ def test_extended_sources_raise():
                          pos_x=g["px"], pos_y=g["py"], psf=g["psf"], band_h=h, band_w=w,
                          grid_x0=g["gx0"], grid_y0=g["gy0"], bg_x_origin=0.0, bg_x_scale=1.0,
                          bg_y_origin=0.0, bg_y_scale=1.0,
-                         source_type=np.array([0, 1, 0]))
-    with pytest.raises(ValueError, match="not supported"):
+                         source_type=np.array(stype), render_backend=backend)
+    with pytest.raises(ValueError):
         solve_band_sparse(inp, np.zeros((3, 4), np.int32), np.zeros((3, 4), bool))
+
+
+def test_exp_mixture_data_matches_the_reference_constants():
+    """``data/exp_mog.npz`` holds source_model.py:56-75's arrays: six
+    components, amplitudes normalised to unit sum, the reference's fixture
+    agreeing with the oracle through it."""
+    from uniphot_b200.sparse import exp_mixture
+    amp, var = exp_mixture()
+    assert amp.dtype == np.float32 and var.dtype == np.float32
+    assert amp.size == var.size == 6
+    assert abs(float(amp.astype(np.float64).sum()) - 1.0) < 1e-6
+    assert np.all(np.diff(var) > 0) and np.all(amp > 0)
 
 
 def test_grid_galaxy_stamp_matches_the_island_fft_render():

@@ -79,7 +79,8 @@ class SparseBand(C.Structure):
                 ("bg_y_scale", C.c_double), ("bg_order", C.c_int32),
                 ("k_max", C.c_int32), ("neighbor_idx", _P), ("neighbor_mask", _P),
                 ("reg", C.c_float), ("source_type", _P), ("logre", _P), ("ee1", _P),
-                ("ee2", _P), ("sersic_n", _P)]
+                ("ee2", _P), ("sersic_n", _P), ("render_direct", C.c_int32),
+                ("exp_k", C.c_int32), ("exp_amp", _P), ("exp_var", _P)]
 
 
 class SparseOut(C.Structure):
@@ -241,7 +242,13 @@ class Context:
         keep = []
         st = getattr(inputs, "source_type", None)
         if st is not None and np.any(np.asarray(st) != 0):
-            if not getattr(self, "_table", False):
+            if getattr(inputs, "render_backend", "fft") == "direct":
+                from .sparse import exp_mixture
+                amp, var = exp_mixture()
+                keep.extend((amp, var))
+                ib.render_direct, ib.exp_k = 1, int(amp.size)
+                ib.exp_amp, ib.exp_var = ptr(amp), ptr(var)
+            elif not getattr(self, "_table", False):
                 from .sersic import load_table
                 self.upload_sersic_table(load_table())
                 self._table = True

@@ -1375,19 +1375,23 @@ int uph_sparse_band_solve(uph_ctx* ctx, const uph_sparse_band* in, uph_sparse_ou
     if (in->neighbor_mask[e] && (in->neighbor_idx[e] < 0 || in->neighbor_idx[e] >= n))
       return set_err(ctx, UPH_ERR_INVALID, "neighbour index out of range");
   bool any_gal = false;
+  const bool direct = in->render_direct != 0;
   if (in->source_type) {
     if (!in->logre || !in->ee1 || !in->ee2 || !in->sersic_n)
       return set_err(ctx, UPH_ERR_INVALID, "source types without shapes");
     for (int i = 0; i < n; ++i) {
-      if (in->source_type[i] < 0 || in->source_type[i] > 3)
-        return set_err(ctx, UPH_ERR_INVALID, "unknown source type %d", in->source_type[i]);
+      if (in->source_type[i] < 0 || in->source_type[i] > (direct ? 1 : 3))
+        return set_err(ctx, UPH_ERR_INVALID, "source type %d not rendered by the %s backend",
+                       in->source_type[i], direct ? "direct" : "fft");
       any_gal = any_gal || in->source_type[i] != 0;
     }
   }
+  if (direct && (in->exp_k < 1 || in->exp_k > 16 || !in->exp_amp || !in->exp_var))
+    return set_err(ctx, UPH_ERR_INVALID, "direct backend needs 1..16 mixture components");
   const int fftP = fft_pad_for(std::max(H, W));
-  if (any_gal && !ctx->tb_knots.ptr)
+  if (any_gal && !direct && !ctx->tb_knots.ptr)
     return set_err(ctx, UPH_ERR_STATE, "no Sersic table uploaded");
-  if (any_gal && fftP > 512)
+  if (any_gal && !direct && fftP > 512)
     return set_err(ctx, UPH_ERR_INVALID, "PSF stamp %dx%d needs a Fourier grid above 512", H, W);
   cudaSetDevice(ctx->device);
   const int M = in->bg_order == 0 ? 1 : (in->bg_order == 1 ? 3 : 6);
@@ -1413,10 +1417,10 @@ int uph_sparse_band_solve(uph_ctx* ctx, const uph_sparse_band* in, uph_sparse_ou
       sizeof(float) * (size_t)std::max(n, 1), sizeof(float) * (size_t)std::max(n, 1),
       sizeof(float) * (size_t)std::max(n, 1),
       any_gal ? sizeof(float) * (size_t)n * H * W : 16,
-      any_gal ? sizeof(float) * std::min<size_t>((size_t)n, 2 * (size_t)ctx->sm_count) *
-                    sparse_gal_floats(H, W, fftP)
-              : 16,
-      16};
+      any_gal && !direct ? sizeof(float) * std::min<size_t>((size_t)n, 2 * (size_t)ctx->sm_count) *
+                               sparse_gal_floats(H, W, fftP)
+                         : 16,
+      direct ? sizeof(float) * 2 * (size_t)in->exp_k : 16};
   for (int i = 0; i < 32; ++i) {
     int rc = ensure(ctx, ctx->sp[i], sizes[i], "sparse solve");
     if (rc) return rc;
@@ -1461,7 +1465,10 @@ int uph_sparse_band_solve(uph_ctx* ctx, const uph_sparse_band* in, uph_sparse_ou
     d.gws = (float*)ctx->sp[30].ptr;
     d.fft_P = fftP;
     d.gal_floats = sparse_gal_floats(H, W, fftP);
-    d.gal_ctas = (int)std::min<long long>(n, 2LL * ctx->sm_count);
+    d.gal_ctas = direct ? 0 : (int)std::min<long long>(n, 2LL * ctx->sm_count);
+    d.direct = direct ? 1 : 0;
+    d.exp_k = direct ? in->exp_k : 0;
+    d.exp_mog = (const float*)ctx->sp[31].ptr;
     d.tb_knots = (const double*)ctx->tb_knots.ptr;
     d.tb_amps = (const double*)ctx->tb_amps.ptr;
     d.tb_lv = (const double*)ctx->tb_lv.ptr;
@@ -1494,6 +1501,11 @@ int uph_sparse_band_solve(uph_ctx* ctx, const uph_sparse_band* in, uph_sparse_ou
     if ((rc = upload(ctx, ctx->sp[27].ptr, in->ee2, sizeof(float) * n, "ee2"))) return rc;
     if ((rc = upload(ctx, ctx->sp[28].ptr, in->sersic_n, sizeof(float) * n, "sersic_n")))
       return rc;
+    if (direct) {
+      const size_t kb = sizeof(float) * (size_t)in->exp_k;
+      if ((rc = upload(ctx, ctx->sp[31].ptr, in->exp_amp, kb, "exp_amp"))) return rc;
+      if ((rc = upload(ctx, (char*)ctx->sp[31].ptr + kb, in->exp_var, kb, "exp_var"))) return rc;
+    }
   }
   if (n > 0 && kmax > 0) {
     if ((rc = upload(ctx, nidx, in->neighbor_idx, sizeof(int) * (size_t)n * kmax, "nbr")))

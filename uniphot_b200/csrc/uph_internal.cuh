@@ -400,6 +400,9 @@ struct SparseDev {
   size_t gal_floats;
   float* gal;
   float* gws;
+  // "direct" backend: EXP stamps from the exp_k-Gaussian mixture (amp, var)
+  int direct, exp_k;
+  const float* exp_mog;    // amp[exp_k] then var[exp_k]
 };
 size_t sparse_stamp_smem(int H, int W);
 size_t sparse_gal_floats(int H, int W, int P);

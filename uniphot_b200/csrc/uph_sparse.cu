@@ -8,6 +8,11 @@
 //                 times the padded PSF's (sersic_mog.py:153-194) by radix-2
 //                 shared-memory FFTs, cropped to the stamp, plus the core
 //                 times the PSF
+//   k_sp_exp_direct  EXP galaxies on the "direct" backend (source_model.py:
+//                 218-256, 298-303), one CTA per source: the PSF stamp and
+//                 the exponential mixture at pixel centres in shared memory,
+//                 the profile normalised, their same-size convolution
+//                 renormalised to unit sum
 //   k_sp_stamps   one CTA per source: PSF polynomial at the source (or the
 //                 galaxy stamp), unit-sum renormalisation on the all-star
 //                 path, Lanczos-3 x then y pass in shared memory
@@ -136,6 +141,93 @@ k_sp_gal(const SparseDev d) {
     fft2_inverse_rows(Cc, H, W, PP, logP, o, fbuf, lb, cw, sw);
     for (int e = tid; e < H * W; e += ST) o[e] = (float)((double)o[e] + gcore * (double)img[e]);
   }
+}
+
+__device__ __forceinline__ double block_sum_sp(double v, double* red) {
+  // red: ST / 32 doubles; every thread returns the CTA's sum
+  for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  double t = 0.0;
+  for (int w = 0; w < ST / 32; ++w) t += red[w];
+  return t;
+}
+
+// "direct" EXP stamps, unshifted (H x W) into d.gal; dynamic shared memory
+// sparse_stamp_smem(H, W): the profile then the PSF stamp.
+__global__ void __launch_bounds__(ST)
+k_sp_exp_direct(const SparseDev d) {
+  extern __shared__ float sm[];
+  __shared__ float beta[UPH_MAXNT];
+  __shared__ float shp[4];
+  __shared__ double red[ST / 32];
+  const int s = blockIdx.x;
+  if (s >= d.n || d.stype[s] != 1) return;   // one source per CTA: uniform exit
+  const int tid = threadIdx.x, H = d.H, W = d.W, HW = H * W;
+  float* prof = sm;
+  float* psf = sm + HW;
+  if (tid == 0) {
+    psf_basis_at(d.px[s], d.py[s], d.os, d.nterms, beta);
+    // the shape matrix rows (a, b), (c, d) of source_model.py:226-237
+    const float re = fminf(fmaxf(expf(d.lr[s]), 0.1f), 1000.f);
+    const float e1 = d.e1[s], e2 = d.e2[s];
+    const float e = 1.f - expf(-hypotf(e1, e2));
+    const float inv_ba = fminf((1.f + e) / fmaxf(1.f - e, 1e-4f), 1000.f);
+    float st, ct;
+    sincosf(0.5f * atan2f(e2, e1), &st, &ct);
+    shp[0] = re * ct / inv_ba;
+    shp[1] = re * st;
+    shp[2] = -re * st / inv_ba;
+    shp[3] = re * ct;
+  }
+  __syncthreads();
+  const float* amp = d.exp_mog;
+  const float* var = d.exp_mog + d.exp_k;
+  const float a = shp[0], b = shp[1], c = shp[2], dd = shp[3];
+  double acc = 0.0;
+  for (int e = tid; e < HW; e += ST) {
+    const float* cf = d.coefs + (size_t)e * d.nterms;
+    float v = 0.f;
+    for (int t = 0; t < d.nterms; ++t) v = fmaf(cf[t], beta[t], v);
+    psf[e] = v;
+    const float y = (float)(e / W - H / 2), x = (float)(e % W - W / 2);
+    float p = 0.f;
+    for (int k = 0; k < d.exp_k; ++k) {
+      const float vk = var[k];
+      const float sxx = vk * (a * a + b * b), sxy = vk * (a * c + b * dd);
+      const float syy = vk * (c * c + dd * dd);
+      const float det = fmaxf(sxx * syy - sxy * sxy, 1e-12f);
+      const float q = (syy * x * x - 2.f * sxy * x * y + sxx * y * y) / det;
+      p += amp[k] / (2.f * 3.14159265358979f * sqrtf(det)) * expf(-0.5f * fminf(q, 200.f));
+    }
+    prof[e] = p;
+    acc += (double)p;
+  }
+  const double tp = block_sum_sp(acc, red);
+  if (tp > 0.0)
+    for (int e = tid; e < HW; e += ST) prof[e] = (float)((double)prof[e] / tp);
+  __syncthreads();
+  // out[y][x] = sum_{i,j} psf[i][j] prof[y + oy - i][x + ox - j] over the
+  // profile's extent: the full convolution's window from ((H-1)/2, (W-1)/2)
+  const int oy = (H - 1) / 2, ox = (W - 1) / 2;
+  float* o = d.gal + (size_t)s * HW;
+  acc = 0.0;
+  for (int e = tid; e < HW; e += ST) {
+    const int y = e / W, x = e - (e / W) * W;
+    const int i0 = max(0, y + oy - (H - 1)), i1 = min(H - 1, y + oy);
+    const int j0 = max(0, x + ox - (W - 1)), j1 = min(W - 1, x + ox);
+    float v = 0.f;
+    for (int i = i0; i <= i1; ++i) {
+      const int r = (y + oy - i) * W + x + ox;     // r - j indexes the profile
+      for (int j = j0; j <= j1; ++j) v = fmaf(psf[i * W + j], prof[r - j], v);
+    }
+    o[e] = v;
+    acc += (double)v;
+  }
+  const double tc = block_sum_sp(acc, red);
+  if (tc > 0.0)
+    for (int e = tid; e < HW; e += ST) o[e] = (float)((double)o[e] / tc);
 }
 
 __global__ void __launch_bounds__(ST)
@@ -483,7 +575,11 @@ size_t sparse_gal_floats(int H, int W, int P) {
 }
 
 int sparse_setup() {
-  return (int)cudaFuncSetAttribute(k_sp_stamps, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  const int rc = (int)cudaFuncSetAttribute(k_sp_stamps,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           200 * 1024);
+  if (rc) return rc;
+  return (int)cudaFuncSetAttribute(k_sp_exp_direct, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    200 * 1024);
 }
 
@@ -492,7 +588,10 @@ void launch_sparse_band(const SparseDev& d, cudaStream_t s) {
   const size_t npix = (size_t)d.h * d.w;
   k_sp_wgrid<<<(unsigned)((npix + 255) / 256), 256, 0, s>>>(npix, d.invvar, d.good, d.wgrid);
   if (n > 0) {
-    if (d.gal_ctas > 0) k_sp_gal<<<(unsigned)d.gal_ctas, ST, SP_FFT_SMEM, s>>>(d);
+    if (d.direct)
+      k_sp_exp_direct<<<(unsigned)n, ST, sparse_stamp_smem(H, W), s>>>(d);
+    else if (d.gal_ctas > 0)
+      k_sp_gal<<<(unsigned)d.gal_ctas, ST, SP_FFT_SMEM, s>>>(d);
     k_sp_stamps<<<(unsigned)n, ST, sparse_stamp_smem(H, W), s>>>(
         n, H, W, d.coefs, d.nterms, d.os, d.px, d.py, (float)d.gx0, (float)d.gy0, d.renorm,
         d.stamps, d.ixt, d.iyt, d.stype, d.gal);

@@ -21,8 +21,11 @@ Extended sources (EXP/DEV/SERSIC) take the reference's "fft" backend
 the padded PSF's (``sersic_mog.py:153-194``), cropped to the stamp, plus the
 core times the PSF, then the stars' Lanczos shift; with any extended source
 no stamp is renormalised (the reference's mixed renderer).  The legacy
-"direct" EXP backend is not built: extended sources with
-``render_backend="direct"`` raise ``ValueError``.
+"direct" backend (``source_model.py:218-256, 298-303``) renders EXP sources
+as the six-Gaussian exponential mixture (``data/exp_mog.npz``) at pixel
+centres, convolved with the PSF stamp and renormalised to unit sum; it
+accepts STAR and EXP sources only (DEV/SERSIC raise ``ValueError``, as the
+reference's pipeline enforces upstream, pipeline.py:1582-1586).
 """
 
 from __future__ import annotations
@@ -38,6 +41,21 @@ SOURCE_STAR = 0
 # (bg_polynomial.py:25-37)
 _TERMS = {0: ((0, 0),), 1: ((0, 0), (1, 0), (0, 1)),
           2: ((0, 0), (1, 0), (0, 1), (2, 0), (1, 1), (0, 2))}
+
+
+_EXP_MOG = None
+
+
+def exp_mixture():
+    """(amp, var) float32 of the exponential profile's six-Gaussian mixture
+    (source_model.py:56-75), from ``data/exp_mog.npz``."""
+    global _EXP_MOG
+    if _EXP_MOG is None:
+        from pathlib import Path
+        z = np.load(Path(__file__).with_name("data") / "exp_mog.npz")
+        _EXP_MOG = (np.ascontiguousarray(z["amp"], np.float32),
+                    np.ascontiguousarray(z["var"], np.float32))
+    return _EXP_MOG
 
 
 def n_terms_for_order(order: int) -> int:
@@ -143,10 +161,12 @@ def solve_band_sparse(inputs: GridBandInputs, neighbor_idx, neighbor_mask,
     (forced_phot_sparse.py:690-718) on the GPU.  ``context`` is a
     ``uniphot_b200._lib.Context`` to reuse (one is created otherwise)."""
     from . import _lib
-    if inputs.source_type is not None and np.any(np.asarray(inputs.source_type) != SOURCE_STAR) \
-            and inputs.render_backend not in ("fft", "auto"):
-        raise ValueError("not supported by the B200 grid solve: extended sources with "
-                         f"render_backend={inputs.render_backend!r} (the 'fft' backend is built)")
+    if inputs.render_backend not in ("fft", "auto", "direct"):
+        raise ValueError(f"unknown render_backend: {inputs.render_backend!r}")
+    if inputs.source_type is not None and inputs.render_backend == "direct" and \
+            np.any(np.asarray(inputs.source_type) > 1):
+        raise ValueError("render_backend='direct' cannot render DEV/SERSIC sources; "
+                         "use 'fft' or 'auto'")
     M = n_terms_for_order(bg_poly_order)
     ctx = context if context is not None else _lib.Context(device)
     return ctx.sparse_band_solve(inputs, np.asarray(neighbor_idx), np.asarray(neighbor_mask),
