@@ -46,6 +46,11 @@ def _galaxies():
     return make_production_field(4, side=320, n_bands=3, n_src=40, margin=40)
 
 
+def _giants():
+    from uniphot_b200.synth import make_production_field
+    return make_production_field(1, side=320, n_bands=3, n_src=40, margin=40)
+
+
 def _blends():
     from uniphot_b200.synth import make_blend_field
     return make_blend_field(0, n_islands=6, n_bands=3)
@@ -70,6 +75,8 @@ CASES = {
     "galaxies_changed": (_galaxies, lambda f: dict(stall_count_mode="changed")),
     "galaxies_dlnp": (_galaxies, lambda f: dict(convergence="dlnp")),
     "blends": (_blends, lambda f: dict(_POST)),
+    # a 34-member island above the joint cap of 32 takes the giant path
+    "giants": (_giants, lambda f: dict(_POST)),
 }
 
 

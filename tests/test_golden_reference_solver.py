@@ -38,6 +38,7 @@ CASES = {
     "galaxies_changed": ("galaxies", dict(stall_count_mode="changed"), ()),
     "galaxies_dlnp": ("galaxies", dict(convergence="dlnp"), ()),
     "blends": ("blends", dict(param_errors=True, source_metrics=True), _POST_COLS),
+    "giants": ("giants", dict(param_errors=True, source_metrics=True), _POST_COLS),
 }
 
 
@@ -55,6 +56,8 @@ def _field(name):
         return synth.make_small_field(0)
     if name == "galaxies":
         return synth.make_production_field(4, side=320, n_bands=3, n_src=40, margin=40)
+    if name == "giants":
+        return synth.make_production_field(1, side=320, n_bands=3, n_src=40, margin=40)
     return synth.make_blend_field(0, n_islands=6, n_bands=3)
 
 
@@ -72,12 +75,18 @@ def _digest(f):
 def _oracle_rows(f, opts):
     """Per-source rows of the oracle's float64 solve, sorted by source."""
     from oracle.driver import solve_chunk
+    from uniphot_b200.plan import giant_seed_rows, plan_island_classes
     opts = dict(opts)
     priors = opts.pop("priors", False)
     re_prof = opts.pop("re_profile", False)
     # the reference's island_fit uses its default tier ladder (111, 221)
     plans, hosts, PAD, ds, ws, psfs = field_classes(f, "reference", priors=priors,
                                                     tier_ladder=(111, 221))
+    # islands in nsrc buckets above the joint cap (32) keep their seeds
+    _, capped = plan_island_classes(f.island_set, f.buckets, f.source_type, f.logre,
+                                    f.sersic_n, f.native, tier_ladder=(111, 221))
+    giant_ids = np.concatenate([np.asarray(f.buckets.giant_ids, np.int64).ravel(),
+                                np.asarray(capped, np.int64)])
     rows = []
     for p, h in zip(plans, hosts):
         o = solve_chunk(h, np.arange(p.n_islands), B=p.bbox_class, T=p.tier, dstack=ds,
@@ -91,6 +100,10 @@ def _oracle_rows(f, opts):
             res_ngood=o["n_good"], n_bands=ds.shape[0], res_perr=o["perr"],
             res_smetrics=o["smetrics"], res_swin=o["swin"], res_reprof=o["reprof"],
             reprof_deltas=REPROF_DELTAS_LN if re_prof else None))
+    if giant_ids.size:
+        rows.extend(giant_seed_rows(giant_ids, f.island_set, n_bands=ds.shape[0],
+                                    pos_x=f.pos_x, pos_y=f.pos_y, logre=f.logre, ee1=f.ee1,
+                                    ee2=f.ee2, sersic_n=f.sersic_n))
     cat = {k: np.concatenate([r[k] for r in rows]) for k in rows[0]}
     order = np.argsort(cat["src"])
     return {k: v[order] for k, v in cat.items()}
@@ -117,17 +130,21 @@ def test_oracle_matches_reference_solver(case):
     ref = {k: v[order] for k, v in ref.items()}
     o = _oracle_rows(f, opts)
     np.testing.assert_array_equal(o["src"], ref["source_idx"])
-    assert not ref["island_giant"].any()
+    assert ref["island_giant"].any() == (case == "giants")
     np.testing.assert_array_equal(o["n_steps"], ref["n_steps"])
-    for k in ("converged", "stalled", "diverged", "free_n", "island_id", "island_nsrc"):
+    for k in ("converged", "stalled", "diverged", "free_n", "island_id", "island_nsrc",
+              "island_giant"):
         np.testing.assert_array_equal(o[k], ref[k], err_msg=k)
     _close("pos_x", o["pos_x"], ref["pos_x"], 1e-4)
     _close("pos_y", o["pos_y"], ref["pos_y"], 1e-4)
     for k in ("logre", "ee1", "ee2", "sersic_n"):
         _close(k, o[k], ref[k], 1e-5)
     # fluxes within 1e-5 relative or 1e-3 of their error
-    df = np.abs(o["fluxes"].astype(np.float64) - ref["fluxes"])
-    bound = np.maximum(1e-5 * np.abs(ref["fluxes"]), 1e-3 * ref["flux_err"])
+    # (giant rows carry NaN fluxes on both sides)
+    np.testing.assert_array_equal(np.isnan(o["fluxes"]), np.isnan(ref["fluxes"]))
+    fin = ~np.isnan(ref["fluxes"])
+    df = np.abs(o["fluxes"].astype(np.float64) - ref["fluxes"])[fin]
+    bound = np.maximum(1e-5 * np.abs(ref["fluxes"]), 1e-3 * ref["flux_err"])[fin]
     assert np.all(df <= bound), f"fluxes: worst {np.max(df / bound):.3g} x the bound"
     _close("flux_err", o["flux_err"], ref["flux_err"], 0.0, ERR_RTOL[case])
     _close("chi2", o["chi2"], ref["chi2"], 1e-3, 1e-6)
