@@ -149,6 +149,8 @@ def test_oracle_matches_reference_solver(case):
     _close("flux_err", o["flux_err"], ref["flux_err"], 0.0, ERR_RTOL[case])
     _close("chi2", o["chi2"], ref["chi2"], 1e-3, 1e-6)
     _close("chi2_nu", o["chi2_nu"], ref["chi2_nu"], 1e-6, 1e-6)
+    # the stalled islands' plateau-probe certificate (island_solver.py:1401-1465)
+    _close("stall_dchi2", o["stall_dchi2"], ref["stall_dchi2"], 1e-3, 1e-4)
     _close("re_upper_pix", o["re_upper_pix"], ref["re_upper_pix"], 0.0, 1e-6)
     for k in cols:
         _close(k, o[k], ref[k], 1e-5, ERR_RTOL[case])
