@@ -43,10 +43,6 @@ class JArr(np.ndarray):
     def block_until_ready(self):
         return self
 
-    def __array_wrap__(self, obj, context=None, return_scalar=False):
-        out = super().__array_wrap__(obj, context, return_scalar)
-        return out
-
 
 class _AtIdx:
     def __init__(self, arr, idx):
@@ -174,28 +170,15 @@ class _DT:
         return self.base.type
 
 
-def _dtype_hook(self):
-    return self.base
-
-
-_DT.__array_interface__ = None
-del _DT.__array_interface__
-
-
-def _mk_dtype(base):
-    d = _DT(base)
-    return d
-
-
-# numpy resolves dtype= arguments through np.dtype(obj); give _DT a
-# ``dtype`` attribute (np.dtype accepts objects with one)
+# numpy resolves dtype= arguments through np.dtype(obj), which accepts an
+# object with a ``dtype`` attribute, as _DT has
 for _name, _base in (("float32", np.float64), ("float64", np.float64),
                      ("float16", np.float64), ("bfloat16", np.float64),
                      ("complex64", np.complex128), ("complex128", np.complex128),
                      ("int8", np.int8), ("int16", np.int16), ("int32", np.int32),
                      ("int64", np.int64), ("uint8", np.uint8), ("uint32", np.uint32),
                      ("bool_", np.bool_)):
-    setattr(jnp, _name, _mk_dtype(_base))
+    setattr(jnp, _name, _DT(_base))
 jnp.bool = jnp.bool_
 jnp.ndarray = np.ndarray
 jnp.pi = np.pi
@@ -242,8 +225,8 @@ for _n in ("where", "zeros", "ones", "full", "zeros_like", "ones_like", "full_li
            "add", "subtract", "multiply", "divide", "true_divide", "negative",
            "reciprocal", "float_power", "cbrt", "logaddexp", "select", "vdot",
            "inner", "kron", "indices", "diag_indices", "triu_indices", "tril_indices",
-           "broadcast_arrays", "shape", "ndim", "size", "result_type_", "isscalar",
-           "max_", "amax", "amin", "ptp", "average", "histogram", "digitize",
+           "broadcast_arrays", "shape", "ndim", "size", "isscalar",
+           "amax", "amin", "ptp", "average", "histogram", "digitize",
            "argwhere", "flatnonzero", "lexsort", "partition", "trapezoid"):
     if hasattr(np, _n):
         setattr(jnp, _n, _fn(getattr(np, _n)))

@@ -106,6 +106,7 @@ def test_oracle_matches_reference_chunk_runner(case):
         _close(f"{tag}: ferr", np.where(fm, o["ferr"], 0.0), np.where(fm, r["ferr"], 0.0),
                0.0, 1e-4)
         _close(f"{tag}: chi2", o["chi2"], r["chi2"], 1e-3, 1e-6)
+        _close(f"{tag}: stall_dchi2", o["stall_dchi2"], r["stall_dchi2"], 1e-3, 1e-4)
         for k in cols:
             a, b = np.asarray(o[k], np.float64), np.asarray(r[k], np.float64)
             if k == "femarg":
