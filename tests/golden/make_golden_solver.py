@@ -51,6 +51,11 @@ def _giants():
     return make_production_field(1, side=320, n_bands=3, n_src=40, margin=40)
 
 
+def _large():
+    from uniphot_b200.synth import make_production_field
+    return make_production_field(3, side=256, n_bands=3, n_src=30, margin=40)
+
+
 def _blends():
     from uniphot_b200.synth import make_blend_field
     return make_blend_field(0, n_islands=6, n_bands=3)
@@ -77,6 +82,8 @@ CASES = {
     "blends": (_blends, lambda f: dict(_POST)),
     # a 34-member island above the joint cap of 32 takes the giant path
     "giants": (_giants, lambda f: dict(_POST)),
+    # a 14-member mixed island (class of 16, tier 111) and an 8-member one
+    "large": (_large, lambda f: dict(_POST)),
 }
 
 

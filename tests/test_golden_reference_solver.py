@@ -39,6 +39,7 @@ CASES = {
     "galaxies_dlnp": ("galaxies", dict(convergence="dlnp"), ()),
     "blends": ("blends", dict(param_errors=True, source_metrics=True), _POST_COLS),
     "giants": ("giants", dict(param_errors=True, source_metrics=True), _POST_COLS),
+    "large": ("large", dict(param_errors=True, source_metrics=True), _POST_COLS),
 }
 
 
@@ -47,7 +48,12 @@ CASES = {
 # 6e-3 px between linearisation steps of 1e-7 and 1e-8 (relative) in the
 # generator, so its error columns are compared at the 1e-3 level the
 # stand-in's derivative supports.
-ERR_RTOL = {c: (1e-3 if c == "blends" else 1e-4) for c in CASES}
+# The large case's 14-member island stalls after 24 LM steps; along that
+# trajectory the same derivative differences move one galaxy's ee2 by 1.5e-4
+# and a theta error by 1.3e-4 relative, so its shapes are compared to 5e-4
+# and its error columns to 1e-3.
+ERR_RTOL = {c: (1e-3 if c in ("blends", "large") else 1e-4) for c in CASES}
+SHAPE_ATOL = {c: (5e-4 if c == "large" else 1e-5) for c in CASES}
 
 
 def _field(name):
@@ -58,6 +64,8 @@ def _field(name):
         return synth.make_production_field(4, side=320, n_bands=3, n_src=40, margin=40)
     if name == "giants":
         return synth.make_production_field(1, side=320, n_bands=3, n_src=40, margin=40)
+    if name == "large":
+        return synth.make_production_field(3, side=256, n_bands=3, n_src=30, margin=40)
     return synth.make_blend_field(0, n_islands=6, n_bands=3)
 
 
@@ -138,7 +146,7 @@ def test_oracle_matches_reference_solver(case):
     _close("pos_x", o["pos_x"], ref["pos_x"], 1e-4)
     _close("pos_y", o["pos_y"], ref["pos_y"], 1e-4)
     for k in ("logre", "ee1", "ee2", "sersic_n"):
-        _close(k, o[k], ref[k], 1e-5)
+        _close(k, o[k], ref[k], SHAPE_ATOL[case])
     # fluxes within 1e-5 relative or 1e-3 of their error
     # (giant rows carry NaN fluxes on both sides)
     np.testing.assert_array_equal(np.isnan(o["fluxes"]), np.isnan(ref["fluxes"]))
