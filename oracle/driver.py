@@ -38,10 +38,12 @@ def psf_bands(psfs, tier: int, mode: str):
 
 def _one(args):
     (host, row, B, T, dstack, wstack, psf, table, mode, cfg, max_steps, native, bg, pe, fm, sm,
-     rp, rs, ss, cb) = args
+     rp, rs, ss, cb, rb) = args
     isl = island_inputs_from_host(host, row, B=B, T=T, dstack=dstack,
                                   wstack=wstack, psf=psf, table=table, mode=mode,
                                   native=native, bg_joint=bg)
+    if rb is not None:
+        isl.render_backend, isl.exp_mog = rb
     if cb is not None:
         isl.crossband = cb
         isl.cb_scale = float(np.asarray(host["cb_scale"])[row])
@@ -73,10 +75,13 @@ def solve_chunk(host, rows, *, B, T, dstack, wstack, psfs, mode, table_path=None
                 param_errors: bool = False, flux_marg: bool = False,
                 source_metrics: bool = False, re_profile=None,
                 residual: bool = False, scene_subtract: bool = False,
-                crossband: dict | None = None) -> dict:
+                crossband: dict | None = None, render_backend: str = "fft",
+                exp_mog=None) -> dict:
     """``re_profile``: the log-radius offsets of the Re profile, or None;
     ``crossband``: the cross-band GLS channels ({"rank", "u", "lam"}, with
-    the per-island scale from ``host["cb_scale"]``), or None."""
+    the per-island scale from ``host["cb_scale"]``), or None;
+    ``render_backend``: "fft" or the legacy "direct" (EXP galaxies from the
+    exponential mixture ``exp_mog`` = (amp, var))."""
     table = SersicTable.load(table_path) if table_path is not None else None
     psf = psf_bands(psfs, T, mode)
     cfg = SolverConfig(reg=reg, pos_step_max=pos_step_max, ftol_rel=ftol_rel,
@@ -85,7 +90,8 @@ def solve_chunk(host, rows, *, B, T, dstack, wstack, psfs, mode, table_path=None
                        plateau_dlnp_tol=plateau_dlnp_tol, step_mode=step_mode)
     jobs = [(host, int(r), B, T, dstack, wstack, psf, table, mode, cfg, max_steps,
              native, bg_joint, param_errors, flux_marg, source_metrics, re_profile, residual,
-             scene_subtract, crossband) for r in rows]
+             scene_subtract, crossband,
+             (render_backend, exp_mog) if render_backend != "fft" else None) for r in rows]
     if processes > 1 and len(jobs) > 1:
         import multiprocessing as mp
         with mp.get_context("spawn").Pool(processes) as pool:

@@ -401,6 +401,12 @@ class IslandInput:
     # "u": (r, n_b), "lam": (r,)} and the island's amplitude scale; None = off
     crossband: dict | None = None
     cb_scale: float = 1.0
+    # galaxy render backend in the pixelised-PSF mode: "fft" (the Sersic
+    # mixture's transform) or the legacy "direct" (EXP only: the
+    # exponential mixture exp_mog = (amp, var) at pixel centres convolved
+    # with the PSF, source_model.py:218-256, 298-303)
+    render_backend: str = "fft"
+    exp_mog: tuple | None = None
 
 
 @dataclass
@@ -575,6 +581,47 @@ class IslandSolver:
             Sy = (irf(rf(psfy) * F) + core * psfy.astype(np.float64)).astype(dt)
         return S, Sx, Sy, Ssh.astype(dt), Su.astype(dt)
 
+    def _galaxy_direct(self, band, x, y, k, p, need):
+        """Legacy 'direct' backend EXP stamp (source_model.py:218-256,
+        298-303): the exponential mixture at pixel centres, normalised,
+        convolved with the PSF stamp ("same") and renormalised to unit sum.
+        Position partials through the PSF's spatial variation by the
+        quotient rule; shape partials (log r_e, e1, e2) by float64 central
+        differences of the whole stamp (step 1e-6); no Sersic-index row."""
+        from .sparse_oracle import convolve_same, exp_profile_direct
+        if self.isl.stype[k] != 1:
+            raise ValueError("the direct backend renders STAR and EXP sources only")
+        dt = self.dt
+        amp, var = self.isl.exp_mog
+        T = self.isl.T
+        psf, psfx, psfy = self._star_unshifted(band, x, y)
+        psf64 = np.asarray(psf, np.float64)
+        lr, e1, e2 = (float(p[6 * k + 2]), float(p[6 * k + 3]), float(p[6 * k + 4]))
+
+        def stamp(lr_, e1_, e2_):
+            c = convolve_same(exp_profile_direct(T, T, lr_, e1_, e2_, amp, var), psf64)
+            t = c.sum()
+            return (c / t if t > 0 else c), c, t
+        S, C, tot = stamp(lr, e1, e2)
+        if not need:
+            return S.astype(dt), None, None, None, None
+        prof = exp_profile_direct(T, T, lr, e1, e2, amp, var)
+
+        def dpos(dpsf):
+            if dpsf is None or tot <= 0:
+                return None
+            dc = convolve_same(prof, np.asarray(dpsf, np.float64))
+            return ((dc - S * dc.sum()) / tot).astype(dt)
+        h = 1e-6
+        Ssh = []
+        for j in range(3):
+            a = [lr, e1, e2]
+            b = [lr, e1, e2]
+            a[j] += h
+            b[j] -= h
+            Ssh.append(((stamp(*a)[0] - stamp(*b)[0]) / (2 * h)).astype(dt))
+        return S.astype(dt), dpos(psfx), dpos(psfy), Ssh, np.zeros((T, T), dt)
+
     def _gal_params(self, k, p):
         isl = self.isl
         lr, e1, e2, u = (float(p[6 * k + 2]), float(p[6 * k + 3]),
@@ -606,9 +653,12 @@ class IslandSolver:
             S, Sx, Sy = self._star_unshifted(band, x, y)
             Ssh = Su = None
         else:
-            gal = self._gal_params(k, p)
+            direct = isl.mode != "analytic" and isl.render_backend == "direct"
+            gal = None if direct else self._gal_params(k, p)
             if isl.mode == "analytic":
                 S, Sx, Sy, Ssh, Su = self._analytic(band, x, y, gal, need)
+            elif isl.render_backend == "direct":
+                S, Sx, Sy, Ssh, Su = self._galaxy_direct(band, x, y, k, p, need)
             else:
                 S, Sx, Sy, Ssh, Su = self._galaxy_fft(band, x, y, gal, need)
         Lx, dLx = lanczos3_taps(dx)

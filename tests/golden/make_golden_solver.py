@@ -76,6 +76,8 @@ CASES = {
     "small_priors": (_small, lambda f: dict(_priors(f), compute_param_errors=True)),
     "small_changed": (_small, lambda f: dict(stall_count_mode="changed")),
     "small_dlnp": (_small, lambda f: dict(convergence="dlnp")),
+    # EXP galaxies on the legacy "direct" render backend
+    "small_direct": (_small, lambda f: dict(render_backend="direct")),
     "galaxies": (_galaxies, lambda f: dict(_POST)),
     "galaxies_changed": (_galaxies, lambda f: dict(stall_count_mode="changed")),
     "galaxies_dlnp": (_galaxies, lambda f: dict(convergence="dlnp")),

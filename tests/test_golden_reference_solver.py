@@ -34,6 +34,7 @@ CASES = {
     "small_priors": ("small", dict(param_errors=True, priors=True), _PRIOR_COLS),
     "small_changed": ("small", dict(stall_count_mode="changed"), ()),
     "small_dlnp": ("small", dict(convergence="dlnp"), ()),
+    "small_direct": ("small", dict(render_backend="direct"), ()),
     "galaxies": ("galaxies", dict(param_errors=True, source_metrics=True), _POST_COLS),
     "galaxies_changed": ("galaxies", dict(stall_count_mode="changed"), ()),
     "galaxies_dlnp": ("galaxies", dict(convergence="dlnp"), ()),
@@ -85,6 +86,9 @@ def _oracle_rows(f, opts):
     from oracle.driver import solve_chunk
     from uniphot_b200.plan import giant_seed_rows, plan_island_classes
     opts = dict(opts)
+    if opts.get("render_backend") == "direct":
+        z = np.load(Path(__file__).parents[1] / "uniphot_b200" / "data" / "exp_mog.npz")
+        opts["exp_mog"] = (z["amp"], z["var"])
     priors = opts.pop("priors", False)
     re_prof = opts.pop("re_profile", False)
     # the reference's island_fit uses its default tier ladder (111, 221)
