@@ -68,7 +68,7 @@ def add_back_members(isl, cfg, msf):
 
 def solve_chunk(host, rows, *, B, T, dstack, wstack, psfs, mode, table_path=None,
                 precision="ref", max_steps=30, reg=1e-9, pos_step_max=0.5,
-                ftol_rel=1e-4, step_tol=0.1, processes: int = 1,
+                ftol_rel=1e-4, step_tol=0.1, processes: int = 1, un_freeze_steps: int = 0,
                 native: int = 0, bg_joint: bool = False,
                 stall_count_mode: str = "proposals", convergence: str = "legacy",
                 plateau_dlnp_tol: float = 0.5, step_mode: str = "clip",
@@ -86,6 +86,7 @@ def solve_chunk(host, rows, *, B, T, dstack, wstack, psfs, mode, table_path=None
     psf = psf_bands(psfs, T, mode)
     cfg = SolverConfig(reg=reg, pos_step_max=pos_step_max, ftol_rel=ftol_rel,
                        step_tol=step_tol, precision=precision,
+                       un_freeze_steps=un_freeze_steps,
                        stall_count_mode=stall_count_mode, convergence=convergence,
                        plateau_dlnp_tol=plateau_dlnp_tol, step_mode=step_mode)
     jobs = [(host, int(r), B, T, dstack, wstack, psf, table, mode, cfg, max_steps,

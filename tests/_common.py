@@ -13,7 +13,7 @@ TABLE = ROOT / "uniphot_b200" / "data" / "sersic_mog_table.npz"
 
 
 def field_classes(f, mode: str, kinds=("star", "mixed"), priors: bool = False,
-                  tier_ladder=None):
+                  tier_ladder=None, free_n=None):
     """(plans, hosts, PAD, dstack, wstack, psfs) for a synthetic field;
     ``priors`` adds Gaussian priors on every member's position (0.3 px) and
     on galaxies' radius (50%), ellipticity (0.2), angle (20 deg) and Sersic
@@ -28,7 +28,8 @@ def field_classes(f, mode: str, kinds=("star", "mixed"), priors: bool = False,
     ws = np.zeros_like(ds)
     ds[:, PAD:PAD + H, PAD:PAD + W] = f.data_minus_bg
     ws[:, PAD:PAD + H, PAD:PAD + W] = f.invvar
-    fn = free_n_gate(f.source_type, f.s1_flux, f.s1_flux_var, True, 30.0)
+    fn = (free_n_gate(f.source_type, f.s1_flux, f.s1_flux_var, True, 30.0)
+          if free_n is None else np.asarray(free_n, bool))
     pri = {}
     if priors:
         n = f.pos_x.size

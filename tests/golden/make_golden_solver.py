@@ -81,6 +81,11 @@ CASES = {
     "galaxies": (_galaxies, lambda f: dict(_POST)),
     "galaxies_changed": (_galaxies, lambda f: dict(stall_count_mode="changed")),
     "galaxies_dlnp": (_galaxies, lambda f: dict(convergence="dlnp")),
+    # the Sersic index of every SERSIC source fitted (free_n_override), with
+    # and without the u_n annealing budget (n live only in the first 3 steps)
+    "galaxies_free_n": (_galaxies, lambda f: dict(free_n_override=(f.source_type == 3))),
+    "galaxies_free_n_unfreeze": (_galaxies, lambda f: dict(
+        free_n_override=(f.source_type == 3), un_freeze_steps=3)),
     "blends": (_blends, lambda f: dict(_POST)),
     # a 34-member island above the joint cap of 32 takes the giant path
     "giants": (_giants, lambda f: dict(_POST)),

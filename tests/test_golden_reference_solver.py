@@ -38,6 +38,8 @@ CASES = {
     "galaxies": ("galaxies", dict(param_errors=True, source_metrics=True), _POST_COLS),
     "galaxies_changed": ("galaxies", dict(stall_count_mode="changed"), ()),
     "galaxies_dlnp": ("galaxies", dict(convergence="dlnp"), ()),
+    "galaxies_free_n": ("galaxies", dict(free_n="sersic"), ()),
+    "galaxies_free_n_unfreeze": ("galaxies", dict(free_n="sersic", un_freeze_steps=3), ()),
     "blends": ("blends", dict(param_errors=True, source_metrics=True), _POST_COLS),
     "giants": ("giants", dict(param_errors=True, source_metrics=True), _POST_COLS),
     "large": ("large", dict(param_errors=True, source_metrics=True), _POST_COLS),
@@ -91,9 +93,11 @@ def _oracle_rows(f, opts):
         opts["exp_mog"] = (z["amp"], z["var"])
     priors = opts.pop("priors", False)
     re_prof = opts.pop("re_profile", False)
+    # island_fit's free_n_override: here every SERSIC source
+    free_n = (f.source_type == 3) if opts.pop("free_n", None) == "sersic" else None
     # the reference's island_fit uses its default tier ladder (111, 221)
     plans, hosts, PAD, ds, ws, psfs = field_classes(f, "reference", priors=priors,
-                                                    tier_ladder=(111, 221))
+                                                    tier_ladder=(111, 221), free_n=free_n)
     # islands in nsrc buckets above the joint cap (32) keep their seeds
     _, capped = plan_island_classes(f.island_set, f.buckets, f.source_type, f.logre,
                                     f.sersic_n, f.native, tier_ladder=(111, 221))
