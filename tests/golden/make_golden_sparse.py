@@ -57,6 +57,11 @@ CASES = {
                      lambda n: _galaxy_params(n, 7), "fft"),
     "exp_direct": (dict(seed=8, n=12, order=1, noise=5.0), 1, 32,
                    lambda n: _exp_params(n, 8), "direct"),
+    # denser grids: many overlapping stamp pairs and stamps clipped at the edge
+    "field_stars": (dict(seed=11, n=150, order=2, h=200, w=220, noise=5.0), 2, 32, None,
+                    "direct"),
+    "field_mixed": (dict(seed=12, n=80, order=1, h=160, w=150, noise=5.0), 1, 32,
+                    lambda n: _galaxy_params(n, 12), "fft"),
 }
 
 
