@@ -95,9 +95,10 @@ CASES = {
 
 
 # Chunk-level cases: the reference's make_class_kernels / run_class_chunk on
-# every class of the small field, for options island_fit does not expose.
+# every class of a field (the small one unless named), for options island_fit
+# does not expose.
 # case -> (make_class_kernels arguments, run_class_chunk arguments,
-#          class_host_arrays extras (a callable of the field))
+#          class_host_arrays extras (a callable of the field)[, field builder])
 CROSSBAND = {"rank": 2,
              "u": np.array([[0.6, 0.64, 0.48], [0.0, 0.6, -0.8]], np.float32),
              "lam": np.array([400.0, 60.0], np.float32)}
@@ -109,6 +110,9 @@ CHUNK_CASES = {
                              lambda f: dict(s1_flux=f.s1_flux)),
     "chunk_crossband": (dict(crossband=CROSSBAND), {},
                         lambda f: dict(cb_scale=np.linspace(0.5, 1.5, f.pos_x.size))),
+    # the trust region on the galaxy field (stalls, long trajectories)
+    "chunk_trust_region_galaxies": (dict(step_mode="trust_region"), {}, lambda f: {},
+                                    _galaxies),
 }
 
 
@@ -164,8 +168,8 @@ def run_case(ref_root: str, case: str) -> None:
 def run_chunk_case(ref_root: str, case: str) -> None:
     solver, psfmod = load_reference_solver(ref_root)
     plan_mod = importlib.import_module("tract7dt.fit.grid_gpu.island_plan")
-    kern_kw, run_kw, host_kw = CHUNK_CASES[case]
-    f = _small()
+    kern_kw, run_kw, host_kw = CHUNK_CASES[case][:3]
+    f = (CHUNK_CASES[case][3] if len(CHUNK_CASES[case]) > 3 else _small)()
     psfs = [psfmod.PsfPolynomial(coefs=np.asarray(p.coefs, np.float32),
                                  x_origin=p.x_origin, x_scale=p.x_scale,
                                  y_origin=p.y_origin, y_scale=p.y_scale,

@@ -3,7 +3,8 @@
 
 ``tests/golden/solver_chunk_*.npz`` hold the output dicts of the reference's
 ``make_class_kernels`` / ``run_class_chunk`` (island_solver.py:1874-1922,
-2793-3131) on every class of the small field, made by
+2793-3131) on every class of the small field (the galaxy field for the second
+trust-region case), made by
 ``tests/golden/make_golden_solver.py`` with its float64 numpy stand-in for
 JAX: the trust-region step (``:1004-1116``), the marginal flux errors and
 the band-coadded residual (``:1549-1637``), scene subtraction with the
@@ -26,7 +27,8 @@ CROSSBAND = {"rank": 2,
              "u": np.array([[0.6, 0.64, 0.48], [0.0, 0.6, -0.8]], np.float32),
              "lam": np.array([400.0, 60.0], np.float32)}
 
-# case -> (oracle options, class_host_arrays extras, compared pass outputs)
+# case -> (oracle options, class_host_arrays extras, compared pass outputs
+#          [, field name: the small field unless given])
 CASES = {
     "chunk_trust_region": (dict(step_mode="trust_region"), lambda f: {}, ("railed",)),
     "chunk_flux_marg_residual": (dict(flux_marg=True, residual=True), lambda f: {},
@@ -34,6 +36,8 @@ CASES = {
     "chunk_scene_subtract": (dict(scene_subtract=True), lambda f: {}, ()),
     "chunk_crossband": (dict(crossband=CROSSBAND),
                         lambda f: dict(cb_scale=np.linspace(0.5, 1.5, f.pos_x.size)), ()),
+    "chunk_trust_region_galaxies": (dict(step_mode="trust_region"), lambda f: {},
+                                    ("railed",), "galaxies"),
 }
 
 
@@ -68,15 +72,14 @@ def _close(name, a, b, atol, rtol=0.0):
 @pytest.mark.parametrize("case", sorted(CASES))
 def test_oracle_matches_reference_chunk_runner(case):
     from oracle.driver import solve_chunk
-    from test_golden_reference_solver import _digest
-    from uniphot_b200.synth import make_small_field
+    from test_golden_reference_solver import _digest, _field
     path = GOLDEN / f"solver_{case}.npz"
     if not path.exists():
         pytest.skip(f"fixture {path.name} not generated")
     ref = dict(np.load(path))
-    f = make_small_field(0)
+    f = _field(CASES[case][3] if len(CASES[case]) > 3 else "small")
     assert str(ref.pop("digest")) == _digest(f), "synthetic field changed since the fixture"
-    opts, host_extra, cols = CASES[case]
+    opts, host_extra, cols = CASES[case][:3]
     plans, hosts, PAD, ds, ws = _classes(f, host_extra(f))
     by_key = {}
     for k, v in ref.items():
