@@ -4,7 +4,7 @@
  *
  * The reference (uniphot / tract7dt) exposes this path as Python functions
  * over JAX device arrays; this ABI is the boundary a maintainer binds with
- * ctypes.  Every entry point returns an int status
+ * ctypes (the Python package's _lib module is such a binding).  Every entry point returns an int status
  * (UPH_OK on success) and never throws; uph_last_error() gives the text of
  * the last failure on a context.  All pointers are plain host pointers unless
  * the name says _device; sizes are element counts.
@@ -400,18 +400,25 @@ int uph_island_roots(uph_ctx* ctx, const double* pos_x, const double* pos_y,
  * framework that owns the device memory pool, or a serving process that
  * must not allocate after start-up).  Every buffer is a caller-owned DEVICE
  * pointer; the intermediates live in one fixed device array of
- * UPH_NOALLOC_SCRATCH_BYTES inside the library (held by every GPU that
- * loads it, until exit).  Star members, reference render mode: renders each
- * member at parameters p, solves the per-band VarPro fluxes and returns
- * fluxes, sqrt(diag inv A64) and the island chi2 -- the same numbers as
- * uph_run_chunk with max_steps = 0.  Real members must occupy the first
- * slots of each island.  Calls share the array: calls that overlap on the
- * GPU race and must be serialised by the caller.  The first call on a
- * device does a one-time set-up (symbol address, kernel limits) and should
- * come before any stream capture.  Work that does not fit the array is
- * rejected with UPH_ERR_INVALID and a message in err_buf; the call never
- * allocates and does not synchronise (results are ready when `stream`
- * is). */
+ * UPH_NOALLOC_SCRATCH_BYTES inside the library.  Star members, reference
+ * render mode: renders each member at parameters p, solves the per-band
+ * VarPro fluxes and returns fluxes, sqrt(diag inv A64) and the island chi2
+ * -- the same numbers as uph_run_chunk with max_steps = 0.
+ * Each island is checked on the device first: its real members must occupy
+ * the leading member slots (at least one), all be SOURCE_STAR (0), and sit
+ * within a stamp of the window; the window (bbox x bbox at ox, oy) must lie
+ * inside the padded field.  An island that fails a check is not rendered
+ * and its fluxes, ferr and chi2 come back NaN; the other islands are
+ * unaffected.
+ * Calls share the array: calls that overlap on the GPU race and must be
+ * serialised by the caller.  The first call on a device does a one-time
+ * set-up (the array's device address, kernel limits).  With CUDA's lazy
+ * module loading (the default since CUDA 12.2) that first call is also when
+ * the driver loads the library's kernels and commits the array's device
+ * memory, so make it at start-up, before the memory budget is fixed and
+ * before any stream capture.  Work that does not fit the array is rejected
+ * with UPH_ERR_INVALID and a message in err_buf; later calls never allocate
+ * and do not synchronise (results are ready when `stream` is). */
 #define UPH_NOALLOC_SCRATCH_BYTES (32u << 20)
 typedef struct uph_noalloc_args {
   const float* data;             /* (n_bands, Hp, Wp) padded field, data - bg */
@@ -422,7 +429,7 @@ typedef struct uph_noalloc_args {
   const int32_t* oy;             /* [n]                                     */
   const float* x0b;              /* [n] window origins in field coords      */
   const float* y0b;              /* [n]                                     */
-  const int32_t* stype;          /* [n*N] all SOURCE_STAR (0)               */
+  const int32_t* stype;          /* [n*N] SOURCE_STAR (0) for real members  */
   const uint8_t* mmask;          /* [n*N]                                   */
   const float* p;                /* [n*N*6] parameters (x, y used)          */
   float* fluxes;                 /* [n*n_bands*N] out                       */

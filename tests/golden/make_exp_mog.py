@@ -5,10 +5,10 @@ the six-component mixture the reference keeps in
 ``tract7dt/fit/grid_gpu/source_model.py:56-75`` (Tractor's published
 exponential-profile fit, amplitudes normalised to unit sum, float32); the
 rendered stamps must use the same numbers to agree, so this script copies
-the two arrays out of that module.  Run once in a checkout that has the
-reference mounted:
+the two arrays out of that module.  Run once with the path of a reference
+checkout:
 
-    python uniphot_b200/data/make_exp_mog.py /root/reference
+    python tests/golden/make_exp_mog.py <reference checkout>
 """
 import ast
 import sys
@@ -32,10 +32,12 @@ def main(ref_root: str) -> None:
     amp = np.asarray(_literal(tree, "EXP_AMP"), np.float32)
     amp = (amp / np.sum(amp)).astype(np.float32)
     var = np.asarray(_literal(tree, "EXP_VAR"), np.float32)
-    out = Path(__file__).with_name("exp_mog.npz")
+    out = Path(__file__).resolve().parents[2] / "uniphot_b200" / "data" / "exp_mog.npz"
     np.savez_compressed(out, amp=amp, var=var)
     print(f"wrote {out}: {amp.size} components")
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit(f"usage: python {sys.argv[0]} <reference checkout>")
+    main(sys.argv[1])

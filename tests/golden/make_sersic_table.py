@@ -5,9 +5,9 @@ The galaxy profiles must use the same mixture table as the reference
 ``tract7dt/fit/grid_gpu/sersic_mog.py:48-56``) for the rendered models to
 agree; the table is data, so this script copies its numeric arrays (knots,
 amplitudes, log-variances, delta-core amplitude, bounds) into the package.
-Run once in a checkout that has the reference mounted:
+Run once with the path of a reference checkout:
 
-    python uniphot_b200/data/make_sersic_table.py /root/reference
+    python tests/golden/make_sersic_table.py <reference checkout>
 """
 import sys
 from pathlib import Path
@@ -18,7 +18,7 @@ import numpy as np
 def main(ref_root: str) -> None:
     src = Path(ref_root) / "tract7dt" / "data" / "sersic_mog_table.npz"
     z = np.load(src)
-    out = Path(__file__).with_name("sersic_mog_table.npz")
+    out = Path(__file__).resolve().parents[2] / "uniphot_b200" / "data" / "sersic_mog_table.npz"
     np.savez_compressed(
         out, n_knots=z["n_knots"], amps=z["amps"], log_vars=z["log_vars"],
         core_amp=z["core_amp"], n_min=z["n_min"], n_max=z["n_max"])
@@ -26,4 +26,6 @@ def main(ref_root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit(f"usage: python {sys.argv[0]} <reference checkout>")
+    main(sys.argv[1])

@@ -1,7 +1,7 @@
 """CUDA path vs the CPU oracle (parity tests proper, through the C ABI).
 
 Bar: identical LM iteration counts and converged/stalled flags; fluxes within
-1e-4 relative or 0.01 sigma; positions within 1e-3 px (SURVEY parity bar).
+1e-4 relative or 0.01 sigma; positions within 1e-3 px (the parity bar of the forced-photometry path).
 """
 import numpy as np
 import pytest

@@ -195,10 +195,15 @@ __global__ void __launch_bounds__(NT) k_gram_tc(ClassDev c, int rcap) {
     uint8_t* zl = zh + (size_t)rcap * KC * 2;
     if (lc >= 2) {
       // the MMAs of chunk lc - 2 read this stage: wait for their commit
+      // (an expired wait is not counted as observed: the drain below waits
+      // for that commit again before the tensor memory is freed)
       if (tid == 0) {
-        if (!mbar_wait(&mbar[st], phase[st])) abort_flag = 1;
-        phase[st] ^= 1u;
-        ++waited[st];
+        if (mbar_wait(&mbar[st], phase[st])) {
+          phase[st] ^= 1u;
+          ++waited[st];
+        } else {
+          abort_flag = 1;
+        }
       }
       __syncthreads();
       if (abort_flag) break;
@@ -300,13 +305,16 @@ __global__ void __launch_bounds__(NT) k_gram_tc(ClassDev c, int rcap) {
       ++issued[st];
     }
   }
-  // drain: wait for every commit not yet observed (bounded, also on abort)
+  // drain: wait for every commit not yet observed, so that no MMA this CTA
+  // issued still writes the tensor memory when it is freed below.  Each
+  // wait is bounded; after an expiry the commit gets one more bounded wait
+  // before the kernel gives up on it (error flag raised, memory freed).
   if (tid == 0) {
     for (int st = 0; st < 2; ++st) {
       while (waited[st] < issued[st]) {
         if (!mbar_wait(&mbar[st], phase[st])) {
           abort_flag = 1;
-          break;
+          if (!mbar_wait(&mbar[st], phase[st])) break;
         }
         phase[st] ^= 1u;
         ++waited[st];

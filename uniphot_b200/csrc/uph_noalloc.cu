@@ -54,23 +54,54 @@ void put_err(const uph_noalloc_args* a, const char* msg) {
 
 size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
-// Island flags (every island active) and the real-member count: the leading
-// run of set member-mask slots, as the class planning lays them out.
-__global__ void k_noalloc_prepare(int n, int N, const uint8_t* mmask,
-                                  uint8_t* flags, int* nr) {
+// Per-island validation and set-up.  An island is solved only when its
+// real members occupy the leading member slots (at least one), every real
+// member is a point source, its window lies inside the padded field and
+// every real member's position is finite and near the window; such an
+// island gets the flags of an active island.  Any other island is marked
+// converged, which the render and flux kernels skip (they run in the trial
+// phase), and k_noalloc_finish sets its outputs to NaN.
+__global__ void k_noalloc_prepare(int n, int N, int B, int T, int Hp, int Wp,
+                                  const uint8_t* mmask, const int32_t* stype,
+                                  const int32_t* ox, const int32_t* oy,
+                                  const float* x0b, const float* y0b,
+                                  const float* p, uint8_t* flags, int* nr) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   int cnt = 0;
   while (cnt < N && mmask[(size_t)i * N + cnt]) ++cnt;
-  nr[i] = cnt;
-  flags[i] = FL_REAL;
+  bool ok = cnt >= 1;
+  for (int k = cnt; k < N; ++k) ok = ok && !mmask[(size_t)i * N + k];
+  // the window (B x B at ox, oy) inside the padded field
+  ok = ok && ox[i] >= 0 && oy[i] >= 0 && ox[i] <= Wp - B && oy[i] <= Hp - B;
+  // positions relative to the window origin: finite and within a stamp of
+  // the window, so that the stamp placement arithmetic stays in range
+  const float lo = -(float)(T + B), hi = (float)(2 * B + T);
+  for (int k = 0; k < cnt && ok; ++k) {
+    const float gx = p[(size_t)i * 6 * N + 6 * k] - x0b[i];
+    const float gy = p[(size_t)i * 6 * N + 6 * k + 1] - y0b[i];
+    ok = stype[(size_t)i * N + k] == 0 && gx >= lo && gx <= hi && gy >= lo && gy <= hi;
+  }
+  nr[i] = ok ? cnt : 0;
+  flags[i] = ok ? FL_REAL : (FL_REAL | FL_CONV);
 }
 
 // Island chi2: per-band sums (formed exactly) accumulated in float32 in band
-// order, as the solver's accept step does.
-__global__ void k_noalloc_chi2(int n, int nb, const double* chi2b, float* chi2) {
+// order, as the solver's accept step does; NaN outputs for the islands that
+// k_noalloc_prepare rejected.
+__global__ void k_noalloc_finish(int n, int nb, int N, const uint8_t* flags,
+                                 const double* chi2b, float* chi2, float* flux,
+                                 float* ferr) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
+  if (flags[i] & FL_CONV) {
+    chi2[i] = __int_as_float(0x7fc00000);
+    for (int j = 0; j < nb * N; ++j) {
+      flux[(size_t)i * nb * N + j] = __int_as_float(0x7fc00000);
+      ferr[(size_t)i * nb * N + j] = __int_as_float(0x7fc00000);
+    }
+    return;
+  }
   float c = 0.f;
   for (int b = 0; b < nb; ++b) c = __fadd_rn(c, (float)chi2b[(size_t)i * nb + b]);
   chi2[i] = c;
@@ -163,11 +194,15 @@ extern "C" int uph_fluxes_noalloc(const uph_noalloc_args* a) {
   c.flux = a->fluxes;
   c.ferr = a->ferr;
   c.reg = a->reg;
-  k_noalloc_prepare<<<(n + 127) / 128, 128, 0, s>>>(n, N, a->mmask, c.flags,
-                                                   (int*)(base + o_nr));
-  launch_render(c, c.p, PH_ALL, s);
-  launch_gram_trial(c, c.p, PH_ALL, 1, nullptr, nullptr, s);
-  k_noalloc_chi2<<<(n + 127) / 128, 128, 0, s>>>(n, nb, c.chi2b, a->chi2);
+  k_noalloc_prepare<<<(n + 127) / 128, 128, 0, s>>>(
+      n, N, B, T, a->Hp, a->Wp, a->mmask, a->stype, a->ox, a->oy, a->x0b, a->y0b,
+      a->p, c.flags, (int*)(base + o_nr));
+  // trial phase: every island without the converged flag, i.e. every
+  // island that passed the checks above
+  launch_render(c, c.p, PH_TRIAL, s);
+  launch_gram_trial(c, c.p, PH_TRIAL, 1, nullptr, nullptr, s);
+  k_noalloc_finish<<<(n + 127) / 128, 128, 0, s>>>(n, nb, N, c.flags, c.chi2b, a->chi2,
+                                                  a->fluxes, a->ferr);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {
     char msg[256];

@@ -178,7 +178,7 @@ k_member_setup(ClassDev c, const float* __restrict__ P, int phase) {
   const float px = P[(size_t)isl * c.nP + 6 * k];
   const float py = P[(size_t)isl * c.nP + 6 * k + 1];
   if (tid == 0) {
-    is_gal = c.stype[isl * c.N + k] != 0;
+    is_gal = c.has_gal && c.stype[isl * c.N + k] != 0;
     for (int a = 0; a < 3; ++a) {
       rec->cg[a] = 0.f;
       for (int q = 0; q < 3; ++q) rec->dcov[a][q] = 0.f;
@@ -372,7 +372,7 @@ k_render(ClassDev c, const float* __restrict__ P, int phase, int nsa) {
   const MemberRecord* rec = c.mrec + ((size_t)isl * c.nb + b) * c.N + k;
   if (tid == 0) {
     mb = member_box(c, isl, P, k);
-    ms.is_gal = c.stype[isl * c.N + k] != 0;
+    ms.is_gal = c.has_gal && c.stype[isl * c.N + k] != 0;
     ms.support_half = ms.is_gal ? c.T / 2 : c.native / 2;
     const uint8_t* kp = c.keep + ((size_t)isl * c.N + k) * 6;
     int row = 1;
