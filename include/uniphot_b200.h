@@ -395,6 +395,16 @@ int uph_island_roots(uph_ctx* ctx, const double* pos_x, const double* pos_y,
                      const double* radius, const uint8_t* forced_singleton,
                      int32_t n, int32_t* root_out);
 
+/* Attempts the union-find makes to link two coupled sources' roots before it
+ * gives up (default UPH_ISLAND_TRIES_DEFAULT; each lost attempt means another
+ * thread re-linked one of the roots first).  When a pair runs out the call
+ * returns UPH_ERR_TIMEOUT and root_out is not a valid labelling; the context
+ * stays usable.  0 makes any coupled pair that is not yet linked run out, so
+ * the error path can be exercised on demand.  No counterpart in the
+ * reference (its host cKDTree search has no retry loop). */
+#define UPH_ISLAND_TRIES_DEFAULT (1 << 20)
+int uph_set_island_retry_limit(uph_ctx* ctx, int32_t tries);
+
 /* ---- Allocation-free final-flux pass.  No counterpart in the reference:
  * it exists for callers that cannot call cudaMalloc (a host inside a
  * framework that owns the device memory pool, or a serving process that

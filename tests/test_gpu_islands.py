@@ -49,3 +49,25 @@ def test_device_islands_on_the_synthetic_fields(ctx):
         dev = build_islands(f.pos_x, f.pos_y, f.source_type, f.logre, f.sersic_n, s.r_psf,
                             radius=s.radius, context=ctx)
         _same(s, dev)
+
+
+def test_union_find_gives_up_with_a_timeout_status_and_the_context_recovers(ctx):
+    """With the retry limit at 0 every coupled pair that is not yet linked
+    runs out at once: the call reports UPH_ERR_TIMEOUT (no device fault,
+    no hang); after the default limit is restored the same context labels
+    the field correctly."""
+    from uniphot_b200 import _lib
+    rng = np.random.default_rng(5)
+    n = 2000
+    xy = rng.uniform(0, 400.0, (n, 2))
+    r = np.full(n, 6.0)
+    host = build_islands(xy[:, 0], xy[:, 1], None, None, None, 15.0, radius=r)
+    assert host.n_islands < n
+    ctx.set_island_retry_limit(0)
+    try:
+        with pytest.raises(_lib.UphError, match="status 4.*retries exhausted"):
+            ctx.island_roots(xy[:, 0], xy[:, 1], r)
+    finally:
+        ctx.set_island_retry_limit(_lib.ISLAND_TRIES_DEFAULT)
+    dev = build_islands(xy[:, 0], xy[:, 1], None, None, None, 15.0, radius=r, context=ctx)
+    _same(host, dev)

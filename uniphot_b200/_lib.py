@@ -16,6 +16,7 @@ LIB_PATH = Path(__file__).resolve().parent / "libuniphot_b200.so"
 
 UPH_OK, UPH_ERR_INVALID, UPH_ERR_OOM, UPH_ERR_CUDA, UPH_ERR_TIMEOUT, \
     UPH_ERR_STATE = range(6)
+ISLAND_TRIES_DEFAULT = 1 << 20      # UPH_ISLAND_TRIES_DEFAULT
 RENDER_MODES = {"reference": 0, "analytic": 1}
 PRECISIONS = {"plain": 0, "mixed": 1}
 
@@ -26,7 +27,8 @@ EXPORTED = ("uph_create", "uph_destroy", "uph_last_error", "uph_set_stream",
             "uph_last_launch_count", "uph_job_create", "uph_job_destroy",
             "uph_job_add_chunk", "uph_job_solve", "uph_job_read",
             "uph_job_set_profile", "uph_job_kernel_time", "uph_job_kernel_work",
-            "uph_job_chunk_time", "uph_sparse_band_solve", "uph_island_roots")
+            "uph_job_chunk_time", "uph_sparse_band_solve", "uph_island_roots",
+            "uph_set_island_retry_limit")
 KERNEL_KINDS = ("render", "gram", "assemble", "step", "trial_chi2", "accept",
                 "gram_tc")
 
@@ -137,6 +139,7 @@ def lib():
         L.uph_job_chunk_time.argtypes = [_P, C.c_int32, C.POINTER(C.c_float)]
         L.uph_sparse_band_solve.argtypes = [_P, C.POINTER(SparseBand), C.POINTER(SparseOut)]
         L.uph_island_roots.argtypes = [_P, _P, _P, _P, _P, C.c_int32, _P]
+        L.uph_set_island_retry_limit.argtypes = [_P, C.c_int32]
         _lib = L
     return _lib
 
@@ -208,6 +211,12 @@ class Context:
         self.check(lib().uph_island_roots(self._h, ptr(xs), ptr(ys), ptr(rs), ptr(fs),
                                           int(xs.size), ptr(out)), "uph_island_roots")
         return out
+
+    def set_island_retry_limit(self, tries: int):
+        """Unite attempts per coupled pair in island_roots before it gives up
+        with UphError (status UPH_ERR_TIMEOUT); see uph_set_island_retry_limit."""
+        self.check(lib().uph_set_island_retry_limit(self._h, int(tries)),
+                   "uph_set_island_retry_limit")
 
     def sparse_band_solve(self, inputs, nbr_idx, nbr_mask, reg: float, order: int, M: int):
         """One band of one grid through uph_sparse_band_solve; returns a
@@ -451,7 +460,7 @@ class Job:
         """ms from the start of the last solve to the end of one chunk."""
         ms = C.c_float(0)
         self.ctx.check(lib().uph_job_chunk_time(self._h, int(chunk_id), C.byref(ms)),
-                       "uph_job_chunk_time", "uph_sparse_band_solve")
+                       "uph_job_chunk_time")
         return float(ms.value)
 
     def kernel_work(self) -> dict:

@@ -59,6 +59,7 @@ struct uph_ctx {
   int device = 0;
   DevBuf sp[32];   // sparse grid solve: inputs, per-source work, the system
   DevBuf isl[13];  // island decomposition
+  int isl_tries = UPH_ISLAND_TRIES_DEFAULT;  // unite attempts per coupled pair
   cudaStream_t stream = nullptr;
   bool own_stream = false;
   std::string err;
@@ -1569,6 +1570,7 @@ int uph_island_roots(uph_ctx* ctx, const double* pos_x, const double* pos_y,
   }
   IslandDev d{};
   d.n = n; d.ncx = ncx; d.ncy = ncy; d.x0 = xmin; d.y0 = ymin; d.cell = cell;
+  d.tries = ctx->isl_tries;
   double* x = (double*)ctx->isl[0].ptr;
   double* y = (double*)ctx->isl[1].ptr;
   double* r = (double*)ctx->isl[2].ptr;
@@ -1596,7 +1598,17 @@ int uph_island_roots(uph_ctx* ctx, const double* pos_x, const double* pos_y,
   if ((rc = download(ctx, root_out, d.root, sizeof(int) * n, "roots"))) return rc;
   if ((rc = download(ctx, &err, d.err, sizeof(int), "island flag"))) return rc;
   CK(cudaStreamSynchronize(ctx->stream), "island decomposition");
-  if (err) return set_err(ctx, UPH_ERR_TIMEOUT, "union-find retries exhausted");
+  if (err)
+    return set_err(ctx, UPH_ERR_TIMEOUT,
+                   "union-find retries exhausted (%d attempts per coupled pair)",
+                   ctx->isl_tries);
+  return UPH_OK;
+}
+
+int uph_set_island_retry_limit(uph_ctx* ctx, int32_t tries) {
+  if (!ctx) return UPH_ERR_INVALID;
+  if (tries < 0) return set_err(ctx, UPH_ERR_INVALID, "negative retry limit");
+  ctx->isl_tries = tries;
   return UPH_OK;
 }
 

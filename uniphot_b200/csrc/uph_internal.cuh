@@ -412,6 +412,7 @@ void launch_sparse_band(const SparseDev& d, cudaStream_t s);
 // Device island decomposition (uph_islands.cu).
 struct IslandDev {
   int n, ncx, ncy;
+  int tries;               // unite attempts per coupled pair before giving up
   double x0, y0, cell;
   const double* x;
   const double* y;

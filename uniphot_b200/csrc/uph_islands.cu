@@ -22,7 +22,6 @@
 namespace {
 
 constexpr int IT = 256;
-constexpr int UNION_TRIES = 1 << 20;
 
 __device__ __forceinline__ int find_root(const volatile int* parent, int x) {
   // parents only ever decrease, so the walk ends at a self-parented root;
@@ -92,7 +91,7 @@ __global__ void k_isl_union(int n, const double* __restrict__ x, const double* _
                             const double* __restrict__ r, const uint8_t* __restrict__ single,
                             const int* __restrict__ cid, int ncx, int ncy,
                             const int* __restrict__ start, const int* __restrict__ bucket,
-                            int* parent, int* __restrict__ err) {
+                            int* parent, int tries_max, int* __restrict__ err) {
   const int i = blockIdx.x * IT + threadIdx.x;
   if (i >= n) return;
   if (single && single[i]) return;
@@ -113,17 +112,18 @@ __global__ void k_isl_union(int n, const double* __restrict__ x, const double* _
         const double ddx = xi - x[j], ddy = yi - y[j];
         const double rs = ri + r[j];
         if (!(ddx * ddx + ddy * ddy < rs * rs)) continue;
-        // unite: hook the larger root under the smaller
+        // unite: hook the larger root under the smaller, at most tries_max
+        // attempts (a lost CAS means another thread re-linked a root first)
         int tries = 0;
         while (true) {
           const int a = find_root(parent, i), b = find_root(parent, j);
           if (a == b) break;
-          const int hi = a > b ? a : b, lo = a > b ? b : a;
-          if (atomicCAS(&parent[hi], hi, lo) == hi) break;
-          if (++tries >= UNION_TRIES) {
+          if (tries++ >= tries_max) {
             atomicExch(err, 1);
             break;
           }
+          const int hi = a > b ? a : b, lo = a > b ? b : a;
+          if (atomicCAS(&parent[hi], hi, lo) == hi) break;
         }
       }
     }
@@ -144,6 +144,6 @@ void launch_island_roots(const IslandDev& d, cudaStream_t s) {
   k_isl_scan<<<1, 1024, 0, s>>>(d.ncx * d.ncy, d.count, d.start, d.cursor);
   k_isl_fill<<<g, IT, 0, s>>>(d.n, d.cid, d.cursor, d.bucket);
   k_isl_union<<<g, IT, 0, s>>>(d.n, d.x, d.y, d.r, d.single, d.cid, d.ncx, d.ncy, d.start,
-                               d.bucket, d.parent, d.err);
+                               d.bucket, d.parent, d.tries, d.err);
   k_isl_roots<<<g, IT, 0, s>>>(d.n, d.parent, d.root);
 }
