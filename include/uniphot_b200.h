@@ -314,9 +314,25 @@ int uph_job_kernel_time(const uph_job* job, int32_t kind, float* ms,
  * counted by every working CTA: bytes (stamps written by the render; stamp
  * rows over their member boxes, data, weights and the result for the Gram
  * and the trial chi2; small per-island arrays for the rest) and flops (the
- * Gram's K (K + 1) per window pixel; the step's 2/3 nL^3 LU). */
+ * Gram's K (K + 1) per window pixel; the step's 2/3 nL^3 LU; the render's
+ * FP32 multiply-adds: per support pixel and Gaussian term reaching the tile
+ * 4 + 4 x (derivative rows), per shifted array and pixel 14 for the Lanczos
+ * passes, or the PSF polynomial in the pixelised-PSF mode). */
 int uph_job_kernel_work(const uph_job* job, int32_t kind, double* bytes,
                         double* flops);
+/* Exponential evaluations (SFU) of the same kernels over the last
+ * instrumented solve: for the render, one per support pixel and Gaussian
+ * term that reaches the pixel's tile (analytic mode). */
+int uph_job_kernel_exps(const uph_job* job, int32_t kind, double* exps);
+
+/* Compute-pipe peaks of the context's device for the roofline of the
+ * kernels above (independent dependency chains over every SM, CUDA events,
+ * best of three launches, about 10 ms in all): out[0] FP32 multiply-add
+ * rate in TFLOP/s, out[1] exp2f evaluations in 10^12/s, out[2] FP64
+ * multiply-add rate in TFLOP/s, out[3] the SM clock over the FP32 run in
+ * MHz.  Allocates and frees a small device buffer.  No counterpart in the
+ * reference. */
+int uph_measure_peaks(uph_ctx* ctx, double* out);
 /* Device time from the start of the last uph_job_solve to the end of one
  * chunk's work (its LM iterations, probes and final pass), in ms. */
 int uph_job_chunk_time(const uph_job* job, int32_t chunk_id, float* ms);

@@ -118,3 +118,12 @@ def solve_chunk(host, rows, *, B, T, dstack, wstack, psfs, mode, table_path=None
 def solve_one_input(isl, cfg, max_steps: int = 30):
     """Pool entry: solve one prepared IslandInput."""
     return solve_island(isl, cfg, max_steps)
+
+
+def solve_one_input_timed(isl, cfg, max_steps: int = 30):
+    """Pool entry for timing the CPU path: (result, seconds spent solving
+    inside the worker, excluding process start-up and transfers)."""
+    import time
+    t0 = time.perf_counter()
+    res = solve_island(isl, cfg, max_steps)
+    return res, time.perf_counter() - t0

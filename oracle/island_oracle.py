@@ -357,11 +357,18 @@ class MogPsfBand:
         return w, cov, wx, wy, dcov(sx, a1x, a2x), dcov(sy, a1y, a2y)
 
 
-def _gauss_and_dlog(xx, yy, A, C, B):
-    """Normalised 2-D Gaussian at offsets and d ln N / d(A, C, B)."""
+def _gauss(xx, yy, A, C, B):
+    """Normalised 2-D Gaussian at offsets, its Mahalanobis distance and the
+    covariance determinant."""
     det = A * C - B * B
     Q = (C * xx * xx - 2.0 * B * xx * yy + A * yy * yy) / det
     N = np.exp(-0.5 * Q) / (2.0 * np.pi * np.sqrt(det))
+    return N, Q, det
+
+
+def _gauss_and_dlog(xx, yy, A, C, B):
+    """Normalised 2-D Gaussian at offsets and d ln N / d(A, C, B)."""
+    N, Q, det = _gauss(xx, yy, A, C, B)
     dA = (Q * C - yy * yy - C) / (2.0 * det)
     dC = (Q * A - xx * xx - A) / (2.0 * det)
     dB = (xx * yy - B * Q + B) / det
@@ -503,7 +510,10 @@ class IslandSolver:
         C = (gv[None, :] * cgal[1] + cq[:, 1, None]).reshape(-1)[:, None, None]
         Bc = (gv[None, :] * cgal[2] + cq[:, 2, None]).reshape(-1)[:, None, None]
         wa = (wq[:, None] * ga[None, :]).reshape(-1)[:, None, None]
-        N, lA, lC, lB = _gauss_and_dlog(xx, yy, A, C, Bc)
+        if need:
+            N, lA, lC, lB = _gauss_and_dlog(xx, yy, A, C, Bc)
+        else:
+            N = _gauss(xx, yy, A, C, Bc)[0]
         Nw = wa * N
         Sfull = np.zeros((6, T, T))
         sub = (slice(c0 - hs, c0 + hs + 1), slice(c0 - hs, c0 + hs + 1))

@@ -28,7 +28,7 @@ EXPORTED = ("uph_create", "uph_destroy", "uph_last_error", "uph_set_stream",
             "uph_job_add_chunk", "uph_job_solve", "uph_job_read",
             "uph_job_set_profile", "uph_job_kernel_time", "uph_job_kernel_work",
             "uph_job_chunk_time", "uph_sparse_band_solve", "uph_island_roots",
-            "uph_set_island_retry_limit")
+            "uph_set_island_retry_limit", "uph_job_kernel_exps", "uph_measure_peaks")
 KERNEL_KINDS = ("render", "gram", "assemble", "step", "trial_chi2", "accept",
                 "gram_tc")
 
@@ -140,6 +140,8 @@ def lib():
         L.uph_sparse_band_solve.argtypes = [_P, C.POINTER(SparseBand), C.POINTER(SparseOut)]
         L.uph_island_roots.argtypes = [_P, _P, _P, _P, _P, C.c_int32, _P]
         L.uph_set_island_retry_limit.argtypes = [_P, C.c_int32]
+        L.uph_job_kernel_exps.argtypes = [_P, C.c_int32, C.POINTER(C.c_double)]
+        L.uph_measure_peaks.argtypes = [_P, C.POINTER(C.c_double)]
         _lib = L
     return _lib
 
@@ -211,6 +213,14 @@ class Context:
         self.check(lib().uph_island_roots(self._h, ptr(xs), ptr(ys), ptr(rs), ptr(fs),
                                           int(xs.size), ptr(out)), "uph_island_roots")
         return out
+
+    def measure_peaks(self) -> dict:
+        """FP32 / FP64 multiply-add and exp2f rates of this device
+        (uph_measure_peaks)."""
+        out = (C.c_double * 4)()
+        self.check(lib().uph_measure_peaks(self._h, out), "uph_measure_peaks")
+        return {"fp32_tflops": out[0], "exp2_tera_per_s": out[1], "fp64_tflops": out[2],
+                "sm_mhz": out[3]}
 
     def set_island_retry_limit(self, tries: int):
         """Unite attempts per coupled pair in island_roots before it gives up
@@ -464,14 +474,16 @@ class Job:
         return float(ms.value)
 
     def kernel_work(self) -> dict:
-        """Algorithmic (bytes, flops) per kernel kind of the last
-        instrumented solve."""
+        """Algorithmic (bytes, flops, exponentials) per kernel kind of the
+        last instrumented solve."""
         res = {}
         for i, name in enumerate(KERNEL_KINDS):
             by = C.c_double(0)
             fl = C.c_double(0)
+            ex = C.c_double(0)
             lib().uph_job_kernel_work(self._h, i, C.byref(by), C.byref(fl))
-            res[name] = (float(by.value), float(fl.value))
+            lib().uph_job_kernel_exps(self._h, i, C.byref(ex))
+            res[name] = (float(by.value), float(fl.value), float(ex.value))
         return res
 
     def close(self):

@@ -441,7 +441,8 @@ struct uph_job {
   int64_t kcount[WK_KINDS] = {};
   double kbytes[WK_KINDS] = {};
   double kflops[WK_KINDS] = {};
-  unsigned long long* d_work = nullptr;   // (WK_KINDS, 2) device counters
+  double kexps[WK_KINDS] = {};
+  unsigned long long* d_work = nullptr;   // (WK_KINDS, WK_FIELDS) device counters
   ~uph_job() {
     for (auto* c : chunks) delete c;
     for (auto s : streams) cudaStreamDestroy(s);
@@ -995,8 +996,9 @@ int job_solve(uph_job* job, int max_steps) {
   auto* recp = job->profile ? &rec : nullptr;
   if (job->profile) {
     if (!job->d_work)
-      CK(cudaMalloc((void**)&job->d_work, sizeof(unsigned long long) * 2 * WK_KINDS), "work");
-    CK(cudaMemsetAsync(job->d_work, 0, sizeof(unsigned long long) * 2 * WK_KINDS,
+      CK(cudaMalloc((void**)&job->d_work, sizeof(unsigned long long) * WK_FIELDS * WK_KINDS),
+         "work");
+    CK(cudaMemsetAsync(job->d_work, 0, sizeof(unsigned long long) * WK_FIELDS * WK_KINDS,
                        ctx->stream), "work");
   }
   for (auto* ch : job->chunks) ch->c.work = job->profile ? job->d_work : nullptr;
@@ -1128,13 +1130,14 @@ int job_solve(uph_job* job, int max_steps) {
   ctx->timing[2] = 0.f;
   for (auto* ch : job->chunks) ch->c.work = nullptr;
   if (job->profile) {
-    unsigned long long w[2 * WK_KINDS];
+    unsigned long long w[WK_FIELDS * WK_KINDS];
     CK(cudaMemcpy(w, job->d_work, sizeof w, cudaMemcpyDeviceToHost), "work");
     for (int k = 0; k < WK_KINDS; ++k) {
       job->ktime[k] = 0.f;
       job->kcount[k] = 0;
-      job->kbytes[k] = (double)w[2 * k];
-      job->kflops[k] = (double)w[2 * k + 1];
+      job->kbytes[k] = (double)w[WK_FIELDS * k];
+      job->kflops[k] = (double)w[WK_FIELDS * k + 1];
+      job->kexps[k] = (double)w[WK_FIELDS * k + 2];
     }
     for (auto& r : rec) {
       float ms = 0.f;
@@ -1624,6 +1627,21 @@ int uph_job_kernel_work(const uph_job* job, int32_t kind, double* bytes,
   if (!job || kind < 0 || kind >= WK_KINDS) return UPH_ERR_INVALID;
   if (bytes) *bytes = job->kbytes[kind];
   if (flops) *flops = job->kflops[kind];
+  return UPH_OK;
+}
+
+int uph_job_kernel_exps(const uph_job* job, int32_t kind, double* exps) {
+  if (!job || !exps || kind < 0 || kind >= WK_KINDS) return UPH_ERR_INVALID;
+  *exps = job->kexps[kind];
+  return UPH_OK;
+}
+
+int uph_measure_peaks(uph_ctx* ctx, double* out) {
+  if (!ctx) return UPH_ERR_INVALID;
+  if (!out) return set_err(ctx, UPH_ERR_INVALID, "null output");
+  cudaSetDevice(ctx->device);
+  const int rc = measure_peaks(ctx->stream, ctx->sm_count, out);
+  if (rc) return cuda_err(ctx, (cudaError_t)rc, "peak kernels");
   return UPH_OK;
 }
 

@@ -197,7 +197,8 @@ struct ClassDev {
   int* n_active;
   int* err;                // device error flag: 1 a bounded wait expired,
                            // 2 a launch had too little shared memory
-  // (WK_KINDS, 2) algorithmic bytes and flops per kernel kind, added by every
+  // (WK_KINDS, WK_FIELDS) algorithmic bytes, flops and exponentials per
+  // kernel kind, added by every
   // working CTA; non-null only during instrumented solves
   unsigned long long* work;
   int tc_min_rows;         // islands with more Gram rows use the tensor-core Gram
@@ -239,13 +240,18 @@ __device__ __forceinline__ bool tc_island(const ClassDev& c, int isl, int K) {
 // Kernel kinds of the instrumented solve (uph_job_kernel_time numbering).
 enum { WK_RENDER = 0, WK_GRAM = 1, WK_ASSEMBLE = 2, WK_STEP = 3, WK_TRIAL = 4,
        WK_ACCEPT = 5, WK_GRAM_TC = 6, WK_KINDS = 7 };
+// Per kind: algorithmic bytes, floating-point operations (tensor-core or
+// FP32 CUDA-core, by kind) and exponential evaluations (SFU).
+constexpr int WK_FIELDS = 3;
 
 __device__ __forceinline__ void work_add(const ClassDev& c, int kind,
                                          unsigned long long bytes,
-                                         unsigned long long flops) {
+                                         unsigned long long flops,
+                                         unsigned long long exps = 0) {
   if (c.work) {
-    atomicAdd(c.work + 2 * kind, bytes);
-    if (flops) atomicAdd(c.work + 2 * kind + 1, flops);
+    atomicAdd(c.work + WK_FIELDS * kind, bytes);
+    if (flops) atomicAdd(c.work + WK_FIELDS * kind + 1, flops);
+    if (exps) atomicAdd(c.work + WK_FIELDS * kind + 2, exps);
   }
 }
 
@@ -674,3 +680,7 @@ void launch_gram_tc(const ClassDev& c, cudaStream_t s);
 size_t gram_tc_smem_bytes(int kmax);
 int gram_tc_splits(int n_isl, int nb, int B, int sm_count);
 int uph_kernel_setup();
+
+// Compute-pipe peak kernels (uph_peaks.cu): FP32 and FP64 multiply-add and
+// exp2f rates and the SM clock into out[0..3]; returns a cudaError_t.
+int measure_peaks(cudaStream_t s, int sms, double* out);

@@ -413,12 +413,6 @@ k_render(ClassDev c, const float* __restrict__ P, int phase, int nsa) {
   if (oy0 >= mb.wy0 + mb.bh || ox0 >= mb.wx0 + mb.bw) return;
   const int oh = min(UPH_TILE, mb.wy0 + mb.bh - oy0);
   const int ow = min(UPH_TILE, mb.wx0 + mb.bw - ox0);
-  if (tid == 0 && c.work) {
-    int rows = 1;
-    if (lin)
-      for (int j = 0; j < 6; ++j) rows += ms.live_row[j] != 0;
-    work_add(c, WK_RENDER, 4ull * (unsigned long long)(oh * ow * rows), 0);
-  }
   const int si0 = oy0 - mb.iyt, sj0 = ox0 - mb.ixt;  // stamp coords of tile
   const int hr = oh + 6, hc = ow + 6;
   float* S = smem;   // nsa * UPH_HALO * HP; the x pass overwrites it in place
@@ -451,6 +445,35 @@ k_render(ClassDev c, const float* __restrict__ P, int phase, int nsa) {
   // analytic records: 0 derivative rows (trial), 2 (star: x, y) or 6
   int nout = 0;
   if (lin) nout = ms.is_gal ? 6 : ((ms.need[1] || ms.need[2]) ? 2 : 0);
+  if (tid == 0 && c.work) {
+    // algorithmic work of this tile: the stamp rows written; on the tile's
+    // pixels inside the member's support, per Gaussian term that reaches the
+    // tile (analytic) one exponential and 4 + 4 nout FP32 multiply-adds, or
+    // (pixelised PSF) the polynomial per needed S array; then 7 + 7
+    // multiply-adds per shifted S array and pixel for the Lanczos passes
+    int rows = 1;
+    if (lin)
+      for (int j = 0; j < 6; ++j) rows += ms.live_row[j] != 0;
+    unsigned long long flops = 0, exps = 0;
+    if (!empty) {
+      const int sy = min(si0 + oh, c0 + hs + 1) - max(si0, c0 - hs);
+      const int sx = min(sj0 + ow, c0 + hs + 1) - max(sj0, c0 - hs);
+      const unsigned long long sup = (unsigned long long)max(sy, 0) * max(sx, 0);
+      int nsarr = 0;
+      for (int q = 0; q < NS; ++q) nsarr += (q == 0 || ms.need[q]) ? 1 : 0;
+      if (c.mode == 1) {
+        exps = sup * (unsigned long long)ms.nact;
+        flops = exps * 2ull * (4 + 4 * nout);
+      } else if (!ms.is_gal) {
+        flops = sup * 2ull * c.nt * (unsigned long long)nsarr;
+      }
+      // shifted arrays: S and its partials, plus the tap derivatives of the
+      // position rows
+      const int nshift = nsarr + (ms.live_row[0] ? 1 : 0) + (ms.live_row[1] ? 1 : 0);
+      flops += 28ull * (unsigned long long)(oh * ow) * nshift;
+    }
+    work_add(c, WK_RENDER, 4ull * (unsigned long long)(oh * ow * rows), flops, exps);
+  }
   if (!empty && c.mode == 1) {
     for (int a = tid; a < ms.nact; a += blockDim.x) {
       const GComp& o = rec->comps[ms.act[a]];
