@@ -443,8 +443,10 @@ k_render(ClassDev c, const float* __restrict__ P, int phase, int nsa) {
     empty = (ms.nact == 0);
   }
   // analytic records: 0 derivative rows (trial), 2 (star: x, y) or 6
+  // (galaxies: x, y, three shape rows, and the Sersic-index row only when
+  // the index is live)
   int nout = 0;
-  if (lin) nout = ms.is_gal ? 6 : ((ms.need[1] || ms.need[2]) ? 2 : 0);
+  if (lin) nout = ms.is_gal ? (ms.need[6] ? 6 : 5) : ((ms.need[1] || ms.need[2]) ? 2 : 0);
   if (tid == 0 && c.work) {
     // algorithmic work of this tile: the stamp rows written; on the tile's
     // pixels inside the member's support, per Gaussian term that reaches the
@@ -497,10 +499,12 @@ k_render(ClassDev c, const float* __restrict__ P, int phase, int nsa) {
       };
       r[1] = comb(o.dAx, o.dCx, o.dBx, o.nrm, o.nx);
       r[2] = comb(o.dAy, o.dCy, o.dBy, o.nrm, o.ny);
-      if (nout == 6) {
+      if (nout >= 5) {
         const float nv = o.nrm * o.v;
         for (int q = 0; q < 3; ++q)
           r[3 + q] = comb(ms.dcov[q][0], ms.dcov[q][1], ms.dcov[q][2], nv, 0.f);
+      }
+      if (nout == 6) {
         const float4 u = comb(ms.cg[0], ms.cg[1], ms.cg[2], o.nrm * o.dv, o.nu);
         r[6] = make_float4(ms.dndu * u.x, ms.dndu * u.y, ms.dndu * u.z, ms.dndu * u.w);
       }
@@ -555,22 +559,32 @@ k_render(ClassDev c, const float* __restrict__ P, int phase, int nsa) {
       if (ms.need[2]) S[(2 * UPH_HALO + r) * HP + cc] = v2;
     }
   } else {
-    // two halo pixels per thread share every component record
+    // halo pixels outside the member's support (and outside the stamp) are
+    // zero: clear them, then evaluate only the support rectangle
+    // [ylo, yhi] x [xlo, xhi] (offsets from the stamp centre), two pixels
+    // per thread sharing every component record
+    const int ry0 = ylo + c0 - (si0 - 3), rx0 = xlo + c0 - (sj0 - 3);
+    const int rh = yhi - ylo + 1, rw = xhi - xlo + 1;
+    const int nr = rh * rw;
+    for (int e = tid; e < nh; e += blockDim.x) {
+      const int r = e / hc, cc = e - r * hc;
+      if (r >= ry0 && r < ry0 + rh && cc >= rx0 && cc < rx0 + rw) continue;
+      S[(0 * UPH_HALO + r) * HP + cc] = 0.f;
+      for (int q = 1; q <= nout; ++q)
+        if (ms.need[q]) S[(q * UPH_HALO + r) * HP + cc] = 0.f;
+    }
     const int step = 2 * blockDim.x;
-    for (int e0 = tid; e0 < nh; e0 += step) {
+    for (int e0 = tid; e0 < nr; e0 += step) {
       const int e1 = e0 + blockDim.x;
-      bool ok[2];
       float x2[2], xy[2], y2[2];
       int rr[2], cs[2];
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
-        const int e = h ? e1 : e0;
-        rr[h] = e / hc;
-        cs[h] = e - rr[h] * hc;
-        const int si = si0 - 3 + rr[h], sj = sj0 - 3 + cs[h];
-        ok[h] = e < nh && si >= 0 && si < T && sj >= 0 && sj < T && abs(si - c0) <= hs &&
-                abs(sj - c0) <= hs;
-        const float xo = (float)(sj - c0), yo = (float)(si - c0);
+        const int e = min(h ? e1 : e0, nr - 1);
+        const int ry = e / rw, rx = e - ry * rw;
+        rr[h] = ry0 + ry;
+        cs[h] = rx0 + rx;
+        const float xo = (float)(xlo + rx), yo = (float)(ylo + ry);
         x2[h] = xo * xo;
         xy[h] = xo * yo;
         y2[h] = yo * yo;
@@ -578,18 +592,20 @@ k_render(ClassDev c, const float* __restrict__ P, int phase, int nsa) {
       float va[NS], vb[NS];
       if (nout == 6)
         mog_pair<6>(trec, ms.nact, x2[0], xy[0], y2[0], x2[1], xy[1], y2[1], va, vb);
+      else if (nout == 5)
+        mog_pair<5>(trec, ms.nact, x2[0], xy[0], y2[0], x2[1], xy[1], y2[1], va, vb);
       else if (nout == 2)
         mog_pair<2>(trec, ms.nact, x2[0], xy[0], y2[0], x2[1], xy[1], y2[1], va, vb);
       else
         mog_pair<0>(trec, ms.nact, x2[0], xy[0], y2[0], x2[1], xy[1], y2[1], va, vb);
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
-        if ((h ? e1 : e0) >= nh) continue;
+        if ((h ? e1 : e0) >= nr) continue;
         const float* v = h ? vb : va;
         const int r = rr[h], cc = cs[h];
-        S[(0 * UPH_HALO + r) * HP + cc] = ok[h] ? v[0] : 0.f;
+        S[(0 * UPH_HALO + r) * HP + cc] = v[0];
         for (int q = 1; q <= nout; ++q)
-          if (ms.need[q]) S[(q * UPH_HALO + r) * HP + cc] = ok[h] ? v[q] : 0.f;
+          if (ms.need[q]) S[(q * UPH_HALO + r) * HP + cc] = v[q];
       }
     }
   }
