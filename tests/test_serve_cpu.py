@@ -128,3 +128,46 @@ def test_all_giant_request_returns_seed_rows():
     assert res.island_giant.all()
     order = np.argsort(res.source_idx)
     np.testing.assert_array_equal(res.pos_x[order], f.pos_x)
+
+
+def test_resident_field_bytes_stay_charged_between_requests():
+    """A worker keeps its field stacks after a request (they are reused and
+    regrown), so those bytes stay charged: with one worker, a 60-byte
+    request of which 30 are field leaves 30 in use; a second request with a
+    smaller field is charged only its transient bytes; a larger field is
+    charged its growth.  Two workers each holding a resident field cannot
+    then admit a request that would exceed the budget beside them."""
+    def plan(kw):
+        return kw["rid"], kw["bytes"], 1, kw["field"]
+
+    def solve(state, kw, p):
+        return p
+
+    def run(srv, kw):
+        # the future resolves before the worker releases the request's
+        # bytes; its stats entry is appended after the release
+        n = len(srv.stats)
+        srv.submit(kw).result(timeout=10)
+        t0 = time.perf_counter()
+        while len(srv.stats) <= n and time.perf_counter() - t0 < 10:
+            time.sleep(0.001)
+
+    srv = Server(workers=1, hbm_budget_bytes=100, plan_fn=plan, solve_fn=solve,
+                 worker_init=lambda i: {})
+    with srv:
+        run(srv, {"rid": 0, "bytes": 60, "field": 30})
+        assert srv.in_use == 30 and srv.resident == [30]
+        run(srv, {"rid": 1, "bytes": 50, "field": 20})
+        assert srv.in_use == 30 and srv.peak_in_use == 60
+        run(srv, {"rid": 2, "bytes": 70, "field": 45})
+        assert srv.in_use == 45 and srv.resident == [45]
+        assert srv.peak_in_use == 30 + 15 + 25     # resident + growth + transient
+
+    dev = FakeDevice()
+    srv = Server(workers=2, hbm_budget_bytes=100, plan_fn=lambda kw: (*dev.plan(kw), kw["field"]),
+                 solve_fn=dev.solve, worker_init=lambda i: {})
+    with srv:
+        futs = [srv.submit({"rid": i, "bytes": 40, "field": 20, "t": 0.05}) for i in range(6)]
+        [f.result(timeout=30) for f in futs]
+    assert srv.peak_in_use <= 100
+    assert srv.in_use == sum(srv.resident) <= 40

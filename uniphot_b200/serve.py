@@ -18,6 +18,15 @@ A request's result does not depend on what else is in flight: every request
 owns its device buffers and every kernel is deterministic, so a result in
 the mix is bitwise the result alone.
 
+Budget accounting: a worker's context keeps its padded field stacks between
+requests (reused, and regrown when a larger cutout arrives), so those bytes
+stay charged to the budget after the request that allocated them: a request
+is charged its transient bytes (chunk buffers and the rest, released when
+it finishes) plus the growth of its worker's resident field.  Freed chunk
+buffers stay cached in the stream-ordered memory pool, but the pool never
+holds more than the largest admitted total, so device memory stays within
+the budget.
+
 Latency of a request = time from its submission to its result (queueing,
 planning, upload, solve, download and unpack).
 """
@@ -63,9 +72,11 @@ class Server:
     """Continuous-batching request server for one GPU.
 
     ``solve_fn(worker_state, kwargs, plan) -> result`` and
-    ``plan_fn(kwargs) -> (plan, device_bytes, n_islands)`` default to the
-    CUDA solver (:func:`default_plan`, :func:`default_solve`); tests may pass
-    host-only stand-ins to exercise admission without a GPU.
+    ``plan_fn(kwargs) -> (plan, device_bytes, n_islands[, field_bytes])``
+    default to the CUDA solver (:func:`default_plan`, :func:`default_solve`);
+    ``field_bytes`` (part of ``device_bytes``, 0 when omitted) is what the
+    worker keeps resident after the request.  Tests may pass host-only
+    stand-ins to exercise admission without a GPU.
     """
 
     def __init__(self, device: int = 0, workers: int = 4,
@@ -89,6 +100,8 @@ class Server:
         self._next = 0
         self._lock = threading.Lock()
         self.stats: list[RequestStats] = []
+        # bytes each worker keeps resident between requests (field stacks)
+        self.resident = [0.0] * workers
         self._threads = [threading.Thread(target=self._run, args=(i,), daemon=True)
                          for i in range(workers)]
         self._closed = False
@@ -150,11 +163,20 @@ class Server:
             st.worker = wi
             held = 0.0
             try:
-                plan, nbytes, n_isl = self._plan(item.kwargs)
+                planned = self._plan(item.kwargs)
+                plan, nbytes, n_isl = planned[:3]
+                field_bytes = float(planned[3]) if len(planned) > 3 else 0.0
                 st.device_bytes, st.n_islands = int(nbytes), int(n_isl)
                 d = item.kwargs.get("data_minus_bg")
                 st.pixels = int(np.prod(np.shape(d))) if d is not None else 0
-                held = self._acquire(nbytes)
+                # transient bytes plus the growth of this worker's resident
+                # field; the resident part stays charged after the request
+                growth = max(0.0, field_bytes - self.resident[wi])
+                held = self._acquire(nbytes - field_bytes + growth)
+                if growth:
+                    keep = min(growth, held)
+                    held -= keep
+                    self.resident[wi] += keep
                 st.admitted = time.perf_counter()
                 res = self._solve(state, item.kwargs, plan)
                 st.finished = time.perf_counter()
@@ -182,7 +204,8 @@ def default_plan(kwargs: dict):
     nb, H, W = np.shape(kwargs["data_minus_bg"])
     nbytes = estimate_device_bytes(fp, nb, H, W,
                                    precision=kwargs.get("precision", "mixed"))
-    return fp, nbytes, sum(p.n_islands for p, _ in fp.classes)
+    field_bytes = 2 * 4 * nb * (H + 2 * fp.PAD) * (W + 2 * fp.PAD)
+    return fp, nbytes, sum(p.n_islands for p, _ in fp.classes), field_bytes
 
 
 def default_solve(state: dict, kwargs: dict, plan):
