@@ -298,6 +298,26 @@ int uph_job_add_chunk(uph_job* job, const uph_class_desc* cls,
                       const uph_chunk_in* in, int32_t* chunk_id);
 /* Solve every chunk for up to max_steps LM iterations (device-resident). */
 int uph_job_solve(uph_job* job, int32_t max_steps);
+/* LM loop engine of uph_job_solve.  UPH_ENGINE_QUEUE: every LM iteration
+ * runs for all chunks of a lane at once, one persistent kernel per kernel
+ * kind pulling (chunk, island, unit) items from a device work queue; the
+ * queue holds the islands still iterating, compacted on the device at the
+ * start of each iteration from a longest-first order, and one CUDA graph
+ * per iteration is launched per lane.  UPH_ENGINE_CHUNKS (the default):
+ * each chunk's iterations run as its own CUDA graph on one of a pool of
+ * streams.
+ * Both compute every island identically (bitwise the same results); the
+ * queue engine needs every chunk of the job to share the background mode
+ * and otherwise falls back to the per-chunk engine.  Replaces the vmapped
+ * chunk step of island_solver.py:1730-1752 with its width probe
+ * (island_solver.py:2257). */
+#define UPH_ENGINE_CHUNKS 0
+#define UPH_ENGINE_QUEUE 1
+/* lanes (queue engine): the chunks are dealt to this many lanes, longest
+ * processing time first, each with its own stream, work lists and iteration
+ * graph, so that the lanes' phases overlap on the device (0: the default of
+ * 8; at most 32). */
+int uph_job_set_engine(uph_job* job, int32_t engine, int32_t lanes);
 /* Copy one chunk's results to host buffers. */
 int uph_job_read(uph_job* job, int32_t chunk_id, uph_chunk_out* out);
 /* Per-kernel device time of the last instrumented solve: kind in

@@ -19,6 +19,7 @@ UPH_OK, UPH_ERR_INVALID, UPH_ERR_OOM, UPH_ERR_CUDA, UPH_ERR_TIMEOUT, \
 ISLAND_TRIES_DEFAULT = 1 << 20      # UPH_ISLAND_TRIES_DEFAULT
 RENDER_MODES = {"reference": 0, "analytic": 1}
 PRECISIONS = {"plain": 0, "mixed": 1}
+ENGINES = {"chunks": 0, "queue": 1}      # UPH_ENGINE_CHUNKS, UPH_ENGINE_QUEUE
 
 EXPORTED = ("uph_create", "uph_destroy", "uph_last_error", "uph_set_stream",
             "uph_get_stream", "uph_upload_field", "uph_upload_field_device", "uph_upload_field_unpadded",
@@ -28,7 +29,8 @@ EXPORTED = ("uph_create", "uph_destroy", "uph_last_error", "uph_set_stream",
             "uph_job_add_chunk", "uph_job_solve", "uph_job_read",
             "uph_job_set_profile", "uph_job_kernel_time", "uph_job_kernel_work",
             "uph_job_chunk_time", "uph_sparse_band_solve", "uph_island_roots",
-            "uph_set_island_retry_limit", "uph_job_kernel_exps", "uph_measure_peaks")
+            "uph_set_island_retry_limit", "uph_job_kernel_exps", "uph_measure_peaks",
+            "uph_job_set_engine")
 KERNEL_KINDS = ("render", "gram", "assemble", "step", "trial_chi2", "accept",
                 "gram_tc")
 
@@ -141,6 +143,7 @@ def lib():
         L.uph_island_roots.argtypes = [_P, _P, _P, _P, _P, C.c_int32, _P]
         L.uph_set_island_retry_limit.argtypes = [_P, C.c_int32]
         L.uph_job_kernel_exps.argtypes = [_P, C.c_int32, C.POINTER(C.c_double)]
+        L.uph_job_set_engine.argtypes = [_P, C.c_int32, C.c_int32]
         L.uph_measure_peaks.argtypes = [_P, C.POINTER(C.c_double)]
         _lib = L
     return _lib
@@ -442,6 +445,14 @@ class Job:
         n, N = arrays["mmask"].shape
         self.shapes.append((n, N, nb, int(desc.bbox) if desc.residual else 0))
         return int(cid.value)
+
+    def set_engine(self, engine: str, lanes: int = 0):
+        """LM loop engine: "queue" (persistent work-queue kernels, one per
+        kernel kind, for all chunks of a lane; ``lanes`` lanes overlap, 0
+        for the default) or "chunks" (each chunk's iterations as its own
+        graph on a stream pool); see uph_job_set_engine."""
+        self.ctx.check(lib().uph_job_set_engine(self._h, ENGINES[engine], int(lanes)),
+                       "uph_job_set_engine")
 
     def solve(self, max_steps: int):
         self.ctx.check(lib().uph_job_solve(self._h, int(max_steps)), "uph_job_solve")

@@ -28,6 +28,7 @@ void launch_fill_float(float* p, float v, int n, cudaStream_t s);
 #define UPH_CHECK_EVERY 4
 #define UPH_MAX_STREAMS 32
 #define UPH_HIGH_PRIORITY_STREAMS 4
+#define UPH_QUEUE_LANES 8
 
 namespace {
 
@@ -430,6 +431,31 @@ struct Chunk {
   }
 };
 
+// One lane of the queue engine: a set of chunks on one stream with its own
+// work lists (linearisation and trial phases) and iteration graph.
+struct QueueLane {
+  std::vector<int> chunks;   // chunk indices, heaviest first
+  int off = 0, n = 0;        // the lane's islands in the job's order
+  QueueList ql[2];
+  size_t sm_rlin = 0, sm_rtry = 0, sm_glin = 0, sm_gtc = 0, sm_asm = 0, sm_step = 0,
+         sm_trial = 0;
+  bool any_tc = false, any_red = false, any_fft = false;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t gexec = nullptr;
+  int graph_kernels = 0;
+  cudaEvent_t ev = nullptr;
+  int iters = 0;
+  bool live = false, inflight = false;
+  void release() {
+    if (gexec) cudaGraphExecDestroy(gexec);
+    if (graph) cudaGraphDestroy(graph);
+    if (ev) cudaEventDestroy(ev);
+    gexec = nullptr;
+    graph = nullptr;
+    ev = nullptr;
+  }
+};
+
 struct uph_job {
   uph_ctx* ctx = nullptr;
   std::vector<Chunk*> chunks;
@@ -443,7 +469,20 @@ struct uph_job {
   double kflops[WK_KINDS] = {};
   double kexps[WK_KINDS] = {};
   unsigned long long* d_work = nullptr;   // (WK_KINDS, WK_FIELDS) device counters
+  // LM loop engine: UPH_ENGINE_QUEUE runs each phase of every chunk as one
+  // persistent queue kernel per kind (device-compacted active islands, one
+  // CUDA graph per iteration for the whole job); UPH_ENGINE_CHUNKS runs each
+  // chunk's iterations as its own graph on one of several streams
+  int engine = UPH_ENGINE_CHUNKS;
+  DevBuf q_cls, q_order, q_count, q_act[2], q_n[2], q_pre[2], q_next[2];
+  std::vector<QueueLane> lanes;
+  int lanes_max = 0;        // lanes of the queue engine (0: UPH_QUEUE_LANES)
+  bool q_graph_valid = false;
   ~uph_job() {
+    for (auto& ln : lanes) ln.release();
+    for (DevBuf* b : {&q_cls, &q_order, &q_count, &q_act[0], &q_act[1], &q_n[0], &q_n[1],
+                      &q_pre[0], &q_pre[1], &q_next[0], &q_next[1]})
+      b->release();
     for (auto* c : chunks) delete c;
     for (auto s : streams) cudaStreamDestroy(s);
     if (h_active) cudaFreeHost(h_active);
@@ -946,6 +985,53 @@ void post_loop(Chunk* ch, Launcher& L) {
   if (c.resid) L(4, [&] { launch_residual_coadd(c, s); });
 }
 
+using LaunchRecords = std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>>;
+
+// End of a solve (everything joined on the library stream): wait for it,
+// turn device error flags into status codes, record the timings and, for an
+// instrumented solve, the per-kind times and work counters.
+int job_finish(uph_job* job, LaunchRecords& rec) {
+  uph_ctx* ctx = job->ctx;
+  const int nch = (int)job->chunks.size();
+  CK(cudaEventRecord(ctx->ev[2], ctx->stream), "event");
+  CK(cudaStreamSynchronize(ctx->stream), "solve");
+  for (int i = 0; i < nch; ++i) {
+    int e = 0;
+    CK(cudaMemcpy(&e, job->chunks[i]->c.err, sizeof(int), cudaMemcpyDeviceToHost), "err");
+    if (e == 1)
+      return set_err(ctx, UPH_ERR_TIMEOUT,
+                     "a bounded device wait expired in chunk %d (tensor-core Gram)", i);
+    if (e)
+      return set_err(ctx, UPH_ERR_CUDA,
+                     "chunk %d: a kernel was launched with less shared memory than its "
+                     "tiles need (device check %d)", i, e);
+  }
+  cudaEventElapsedTime(&ctx->timing[1], ctx->ev[0], ctx->ev[2]);
+  for (auto* ch : job->chunks) cudaEventElapsedTime(&ch->done_ms, ctx->ev[0], ch->ev_done);
+  ctx->timing[2] = 0.f;
+  for (auto* ch : job->chunks) ch->c.work = nullptr;
+  if (job->profile) {
+    unsigned long long w[WK_FIELDS * WK_KINDS];
+    CK(cudaMemcpy(w, job->d_work, sizeof w, cudaMemcpyDeviceToHost), "work");
+    for (int k = 0; k < WK_KINDS; ++k) {
+      job->ktime[k] = 0.f;
+      job->kcount[k] = 0;
+      job->kbytes[k] = (double)w[WK_FIELDS * k];
+      job->kflops[k] = (double)w[WK_FIELDS * k + 1];
+      job->kexps[k] = (double)w[WK_FIELDS * k + 2];
+    }
+    for (auto& r : rec) {
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, r.second.first, r.second.second);
+      job->ktime[r.first] += ms;
+      job->kcount[r.first] += 1;
+      cudaEventDestroy(r.second.first);
+      cudaEventDestroy(r.second.second);
+    }
+  }
+  return UPH_OK;
+}
+
 int job_solve(uph_job* job, int max_steps) {
   uph_ctx* ctx = job->ctx;
   cudaSetDevice(ctx->device);
@@ -1112,43 +1198,331 @@ int job_solve(uph_job* job, int max_steps) {
     CK(cudaStreamWaitEvent(ctx->stream, e, 0), "join");
     cudaEventDestroy(e);
   }
-  CK(cudaEventRecord(ctx->ev[2], ctx->stream), "event");
-  CK(cudaStreamSynchronize(ctx->stream), "solve");
-  for (int i = 0; i < nch; ++i) {
-    int e = 0;
-    CK(cudaMemcpy(&e, job->chunks[i]->c.err, sizeof(int), cudaMemcpyDeviceToHost), "err");
-    if (e == 1)
-      return set_err(ctx, UPH_ERR_TIMEOUT,
-                     "a bounded device wait expired in chunk %d (tensor-core Gram)", i);
-    if (e)
-      return set_err(ctx, UPH_ERR_CUDA,
-                     "chunk %d: a kernel was launched with less shared memory than its "
-                     "tiles need (device check %d)", i, e);
+  return job_finish(job, rec);
+}
+
+// Streams of a job (created once; the first ones get the highest priority)
+// and each chunk's slot: heaviest chunks first onto the least-loaded stream
+// (longest processing time first); cost ~ one iteration's Gram and render.
+int job_streams(uph_job* job, int nstreams, std::vector<int>& order) {
+  uph_ctx* ctx = job->ctx;
+  const int nch = (int)job->chunks.size();
+  if ((int)job->streams.size() < nstreams) {
+    int prio_lo = 0, prio_hi = 0;
+    CK(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi), "stream priorities");
+    while ((int)job->streams.size() < nstreams) {
+      const int prio = (int)job->streams.size() < UPH_HIGH_PRIORITY_STREAMS ? prio_hi : prio_lo;
+      cudaStream_t st;
+      CK(cudaStreamCreateWithPriority(&st, cudaStreamNonBlocking, prio), "stream");
+      job->streams.push_back(st);
+    }
   }
-  cudaEventElapsedTime(&ctx->timing[1], ctx->ev[0], ctx->ev[2]);
-  for (auto* ch : job->chunks) cudaEventElapsedTime(&ch->done_ms, ctx->ev[0], ch->ev_done);
-  ctx->timing[2] = 0.f;
-  for (auto* ch : job->chunks) ch->c.work = nullptr;
-  if (job->profile) {
-    unsigned long long w[WK_FIELDS * WK_KINDS];
-    CK(cudaMemcpy(w, job->d_work, sizeof w, cudaMemcpyDeviceToHost), "work");
-    for (int k = 0; k < WK_KINDS; ++k) {
-      job->ktime[k] = 0.f;
-      job->kcount[k] = 0;
-      job->kbytes[k] = (double)w[WK_FIELDS * k];
-      job->kflops[k] = (double)w[WK_FIELDS * k + 1];
-      job->kexps[k] = (double)w[WK_FIELDS * k + 2];
-    }
-    for (auto& r : rec) {
-      float ms = 0.f;
-      cudaEventElapsedTime(&ms, r.second.first, r.second.second);
-      job->ktime[r.first] += ms;
-      job->kcount[r.first] += 1;
-      cudaEventDestroy(r.second.first);
-      cudaEventDestroy(r.second.second);
-    }
+  order.resize(nch);
+  std::vector<double> cost(nch);
+  for (int i = 0; i < nch; ++i) {
+    const ClassDev& c = job->chunks[i]->c;
+    order[i] = i;
+    cost[i] = (double)c.n_isl * c.nb *
+              ((double)c.B * c.B * c.Kmax + (double)c.N * c.T * c.T * c.R);
+  }
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost[a] > cost[b]; });
+  std::vector<double> load(nstreams, 0.0);
+  for (int i : order) {
+    const int j = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+    job->chunks[i]->slot = j;
+    load[j] += cost[i];
   }
   return UPH_OK;
+}
+
+// Every stream of the job waits for the work enqueued so far on `from`.
+int job_fork(uph_job* job, cudaStream_t from, int nstreams) {
+  uph_ctx* ctx = job->ctx;
+  cudaEvent_t e;
+  CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
+  CK(cudaEventRecord(e, from), "event");
+  for (int i = 0; i < nstreams; ++i) CK(cudaStreamWaitEvent(job->streams[i], e, 0), "fork");
+  cudaEventDestroy(e);
+  return UPH_OK;
+}
+
+// `to` waits for the work enqueued so far on every stream of the job.
+int job_join(uph_job* job, cudaStream_t to, int nstreams) {
+  uph_ctx* ctx = job->ctx;
+  for (int i = 0; i < nstreams; ++i) {
+    cudaEvent_t e;
+    CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
+    CK(cudaEventRecord(e, job->streams[i]), "event");
+    CK(cudaStreamWaitEvent(to, e, 0), "join");
+    cudaEventDestroy(e);
+  }
+  return UPH_OK;
+}
+
+// The LM loop of the whole job on the work queues (UPH_ENGINE_QUEUE).  The
+// chunks are dealt to up to UPH_QUEUE_LANES lanes, longest processing time
+// first; each lane runs on its own stream, with its own device work lists
+// and a CUDA graph of one LM iteration: the device compacts the lane's
+// islands still active in the linearisation and trial phases, then one
+// persistent kernel per kernel kind works through their units.  Lanes
+// overlap on the device the way the per-chunk streams did, with a few
+// launches per iteration per lane instead of one graph per chunk.  The
+// per-chunk set-up (state reset, scene add-back, initial chi2) and the
+// post-loop passes (probes, final fluxes) run per chunk on the lane's
+// stream.  Every per-island computation is the per-chunk kernels' own, so
+// the results are bitwise those of job_solve.
+int job_solve_queue(uph_job* job, int max_steps) {
+  uph_ctx* ctx = job->ctx;
+  cudaSetDevice(ctx->device);
+  if (max_steps < 0) return set_err(ctx, UPH_ERR_INVALID, "max_steps < 0");
+  const int nch = (int)job->chunks.size();
+  if (nch == 0) return UPH_OK;
+  ctx->launches = 0;
+  cudaStream_t s = ctx->stream;
+  const int nl = job->profile ? 1 : std::min(nch, job->lanes_max > 0 ? job->lanes_max
+                                                                      : UPH_QUEUE_LANES);
+  std::vector<int> order;
+  int rc = job_streams(job, nl, order);
+  if (rc) return rc;
+  if (job->h_active_cap < std::max(nch, nl)) {
+    if (job->h_active) cudaFreeHost(job->h_active);
+    CK(cudaMallocHost((void**)&job->h_active, sizeof(int) * std::max(nch, nl)), "pinned");
+    job->h_active_cap = std::max(nch, nl);
+  }
+  LaunchRecords rec;
+  auto* recp = job->profile ? &rec : nullptr;
+  if (job->profile) {
+    if (!job->d_work)
+      CK(cudaMalloc((void**)&job->d_work, sizeof(unsigned long long) * WK_FIELDS * WK_KINDS),
+         "work");
+    CK(cudaMemsetAsync(job->d_work, 0, sizeof(unsigned long long) * WK_FIELDS * WK_KINDS, s),
+       "work");
+  }
+  for (auto* ch : job->chunks) ch->c.work = job->profile ? job->d_work : nullptr;
+  // lanes: the chunks of each stream slot, heaviest first, and their islands'
+  // range in the job's order
+  if ((int)job->lanes.size() != nl || !job->q_graph_valid) {
+    for (auto& ln : job->lanes) ln.release();
+    job->lanes.assign(nl, QueueLane{});
+    job->q_graph_valid = false;
+  }
+  int n_total = 0;
+  for (auto& ln : job->lanes) ln.chunks.clear();
+  for (int i : order) job->lanes[job->chunks[i]->slot].chunks.push_back(i);
+  std::vector<int2> hord;
+  for (auto& ln : job->lanes) {
+    ln.off = n_total;
+    for (int i : ln.chunks)
+      for (int j = 0; j < job->chunks[i]->c.n_isl; ++j) hord.push_back(make_int2(i, j));
+    ln.n = (int)hord.size() - ln.off;
+    n_total = (int)hord.size();
+  }
+  std::vector<ClassDev> hcls(nch);
+  for (int i = 0; i < nch; ++i) hcls[i] = job->chunks[i]->c;
+  if ((rc = ensure(ctx, job->q_cls, sizeof(ClassDev) * nch, "queue"))) return rc;
+  if ((rc = ensure(ctx, job->q_order, sizeof(int2) * n_total, "queue"))) return rc;
+  if ((rc = ensure(ctx, job->q_count, sizeof(int) * nl, "queue"))) return rc;
+  for (int k = 0; k < 2; ++k) {
+    if ((rc = ensure(ctx, job->q_act[k], sizeof(int2) * n_total, "queue"))) return rc;
+    if ((rc = ensure(ctx, job->q_n[k], sizeof(int) * nl, "queue"))) return rc;
+    if ((rc = ensure(ctx, job->q_pre[k], sizeof(int) * (size_t)QK_KINDS * (n_total + nl),
+                     "queue")))
+      return rc;
+    if ((rc = ensure(ctx, job->q_next[k], sizeof(int) * QK_KINDS * nl, "queue"))) return rc;
+  }
+  const ClassDev* dcls = (const ClassDev*)job->q_cls.ptr;
+  const int2* dord = (const int2*)job->q_order.ptr;
+  int* dcount = (int*)job->q_count.ptr;
+  const bool bg = job->chunks[0]->c.nbg > 0;
+  for (int l = 0; l < nl; ++l) {
+    QueueLane& ln = job->lanes[l];
+    for (int k = 0; k < 2; ++k) {
+      QueueList& q = ln.ql[k];
+      q.cls = dcls;
+      q.act = (int2*)job->q_act[k].ptr + ln.off;
+      q.n_act = (int*)job->q_n[k].ptr + l;
+      q.pre = (int*)job->q_pre[k].ptr + (size_t)QK_KINDS * (ln.off + l);
+      q.stride = ln.n + 1;
+      q.next = (int*)job->q_next[k].ptr + QK_KINDS * l;
+      for (int kind = 0; kind < QK_KINDS; ++kind) {
+        long long cap = 0;
+        for (int i : ln.chunks)
+          cap += (long long)job->chunks[i]->c.n_isl * queue_units(job->chunks[i]->c, kind);
+        q.cap[kind] = (int)std::min<long long>(cap, 1 << 30);
+      }
+    }
+    // launch shapes: the largest footprint over the lane's chunks
+    ln.sm_rlin = ln.sm_rtry = ln.sm_glin = ln.sm_gtc = ln.sm_asm = ln.sm_step = ln.sm_trial = 0;
+    ln.any_tc = ln.any_red = ln.any_fft = false;
+    for (int i : ln.chunks) {
+      const ClassDev& c = job->chunks[i]->c;
+      ln.sm_rlin = std::max(ln.sm_rlin, render_phase_smem(c, PH_LIN));
+      ln.sm_rtry = std::max(ln.sm_rtry, render_phase_smem(c, PH_TRIAL));
+      ln.sm_glin = std::max(ln.sm_glin, gram_lin_smem_bytes(c.Kmax));
+      ln.sm_asm = std::max(ln.sm_asm, assemble_smem_bytes(c.nLmax, c.N));
+      ln.sm_step = std::max(ln.sm_step, step_smem_bytes(c.nLmax));
+      ln.sm_trial = std::max(ln.sm_trial, gram_trial_smem_bytes(c.N));
+      if (c.tc_min_rows < (1 << 30)) {
+        ln.any_tc = true;
+        ln.any_red = ln.any_red || c.tc_split > 1;
+        ln.sm_gtc = std::max(ln.sm_gtc,
+                             gram_tc_smem_bytes(c.Kmax < UPH_MAXK ? c.Kmax : UPH_MAXK));
+      }
+      ln.any_fft = ln.any_fft || (c.mode == 0 && c.gstamp);
+    }
+    ln.iters = 0;
+    ln.live = max_steps > 0;
+    ln.inflight = false;
+  }
+  CK(cudaEventRecord(ctx->ev[0], s), "event");
+  CK(cudaMemcpyAsync(job->q_cls.ptr, hcls.data(), sizeof(ClassDev) * nch,
+                     cudaMemcpyHostToDevice, s), "queue");
+  CK(cudaMemcpyAsync(job->q_order.ptr, hord.data(), sizeof(int2) * n_total,
+                     cudaMemcpyHostToDevice, s), "queue");
+  if ((rc = job_fork(job, s, nl))) return rc;
+  // per-chunk set-up on the lanes' streams
+  for (int i : order) {
+    Chunk* ch = job->chunks[i];
+    cudaStream_t cs = job->streams[ch->slot];
+    if ((rc = reset_chunk(ctx, ch, cs))) return rc;
+    Launcher L{job, cs, recp};
+    if (ch->scene) {
+      launch_copy_windows(ch->c, ch->fd, ch->fw, ch->fHp, ch->fWp, ch->ox_f, ch->oy_f, cs);
+      L(0, [&] { launch_render(ch->c, ch->d_seed, PH_ALL, cs); }, 2);
+      launch_addback(ch->c, ch->d_seed, ch->d_msf, cs);
+      ctx->launches += 2;
+    }
+    if (ch->fresh || ch->c.fcur || ch->c.dlnp) {
+      L(0, [&] { launch_render(ch->c, ch->c.p, PH_ALL, cs); }, 2);
+      L(4, [&] { launch_gram_trial(ch->c, ch->c.p, PH_ALL, 0, ch->c.fcur, ch->c.acond_cur,
+                                   cs); });
+      if (ch->fresh || ch->c.dlnp) L(5, [&] { launch_accept(ch->c, PH_ALL, cs); });
+    }
+  }
+  CK(cudaGetLastError(), "launch");
+  const int sms = ctx->sm_count;
+  auto iteration = [&](QueueLane& ln, cudaStream_t ls, Launcher& L) {
+    const int2* lord = dord + ln.off;
+    launch_q_build(dcls, lord, ln.n, ln.ql[0], PH_LIN, ls);
+    launch_q_build(dcls, lord, ln.n, ln.ql[1], PH_TRIAL, ls);
+    ctx->launches += 2;
+    auto gal_fft = [&](int phase, bool p_try) {
+      if (!ln.any_fft) return;
+      for (int i : ln.chunks) {
+        const ClassDev& c = job->chunks[i]->c;
+        if (c.mode == 0 && c.gstamp) {
+          launch_gal_fft(c, p_try ? c.p_try : c.p, phase, ls);
+          ctx->launches += 1;
+        }
+      }
+    };
+    L(0, [&] {
+      launch_q_setup(ln.ql[0], PH_LIN, false, sms, ls);
+      gal_fft(PH_LIN, false);
+      launch_q_render(ln.ql[0], PH_LIN, true, false, ln.sm_rlin, sms, ls);
+    }, 2);
+    L(1, [&] { launch_q_gram_lin(ln.ql[0], bg, ln.sm_glin, sms, ls); });
+    if (ln.any_tc)
+      L(WK_GRAM_TC, [&] { launch_q_gram_tc(ln.ql[0], ln.sm_gtc, ln.any_red, sms, ls); },
+        ln.any_red ? 2 : 1);
+    L(2, [&] { launch_q_assemble(ln.ql[0], ln.sm_asm, sms, ls); });
+    L(3, [&] { launch_q_step(ln.ql[1], ln.sm_step, sms, ls); });
+    L(0, [&] {
+      launch_q_setup(ln.ql[1], PH_TRIAL, true, sms, ls);
+      gal_fft(PH_TRIAL, true);
+      launch_q_render(ln.ql[1], PH_TRIAL, false, true, ln.sm_rtry, sms, ls);
+    }, 2);
+    L(4, [&] { launch_q_trial(ln.ql[1], bg, ln.sm_trial, sms, ls); });
+    L(5, [&] { launch_q_accept(ln.ql[1], sms, ls); });
+  };
+  if (max_steps > 0 && !job->profile && !job->q_graph_valid) {
+    for (int l = 0; l < nl; ++l) {
+      QueueLane& ln = job->lanes[l];
+      cudaStream_t ls = job->streams[l];
+      Launcher Lc{job, ls, nullptr};
+      CK(cudaStreamBeginCapture(ls, cudaStreamCaptureModeThreadLocal), "capture");
+      const int64_t before = ctx->launches;
+      iteration(ln, ls, Lc);
+      ln.graph_kernels = (int)(ctx->launches - before);
+      ctx->launches = before;
+      cudaError_t ce = cudaStreamEndCapture(ls, &ln.graph);
+      if (ce != cudaSuccess) return cuda_err(ctx, ce, "end capture");
+      CK(cudaGraphInstantiate(&ln.gexec, ln.graph, 0), "graph instantiate");
+    }
+    job->q_graph_valid = true;
+  }
+  for (auto& ln : job->lanes)
+    if (!ln.ev) CK(cudaEventCreateWithFlags(&ln.ev, cudaEventDisableTiming), "event");
+  // LM loop: each lane advances in groups of UPH_CHECK_EVERY iterations; as
+  // soon as a group's count of islands still iterating reaches the host, the
+  // lane's next group -- or, once it has finished, its chunks' post-loop
+  // passes -- is enqueued, so no lane waits for another
+  auto enqueue_group = [&](int l) -> int {
+    QueueLane& ln = job->lanes[l];
+    cudaStream_t ls = job->streams[l];
+    const int group = std::min(UPH_CHECK_EVERY, max_steps - ln.iters);
+    for (int j = 0; j < group; ++j) {
+      if (job->profile) {
+        Launcher L{job, ls, recp};
+        iteration(ln, ls, L);
+      } else {
+        CK(cudaGraphLaunch(ln.gexec, ls), "graph launch");
+        ctx->launches += ln.graph_kernels;
+      }
+    }
+    ln.iters += group;
+    launch_q_count(dcls, dord + ln.off, ln.n, dcount + l, ls);
+    ctx->launches += 1;
+    CK(cudaMemcpyAsync(job->h_active + l, dcount + l, sizeof(int), cudaMemcpyDeviceToHost, ls),
+       "count");
+    CK(cudaEventRecord(ln.ev, ls), "event");
+    ln.inflight = true;
+    return UPH_OK;
+  };
+  auto finish_lane = [&](int l) {
+    QueueLane& ln = job->lanes[l];
+    cudaStream_t ls = job->streams[l];
+    ln.live = false;
+    for (int i : ln.chunks) {
+      Chunk* ch = job->chunks[i];
+      ch->iters = ln.iters;
+      ch->done = true;
+      Launcher L{job, ls, recp};
+      post_loop(ch, L);
+      cudaEventRecord(ch->ev_done, ls);
+    }
+  };
+  int live = 0;
+  for (int l = 0; l < nl; ++l) {
+    if (!job->lanes[l].live) {
+      finish_lane(l);
+      continue;
+    }
+    if ((rc = enqueue_group(l))) return rc;
+    ++live;
+  }
+  while (live > 0) {
+    bool progress = false;
+    for (int l = 0; l < nl; ++l) {
+      QueueLane& ln = job->lanes[l];
+      if (!ln.inflight) continue;
+      const cudaError_t q = cudaEventQuery(ln.ev);
+      if (q == cudaErrorNotReady) continue;
+      if (q != cudaSuccess) return cuda_err(ctx, q, "lm loop");
+      ln.inflight = false;
+      progress = true;
+      if (job->h_active[l] == 0 || ln.iters >= max_steps) {
+        finish_lane(l);
+        --live;
+      } else if ((rc = enqueue_group(l))) {
+        return rc;
+      }
+    }
+    if (!progress) std::this_thread::yield();
+  }
+  CK(cudaGetLastError(), "post-loop");
+  if ((rc = job_join(job, s, nl))) return rc;
+  return job_finish(job, rec);
 }
 
 int job_read(uph_job* job, int id, uph_chunk_out* out) {
@@ -1322,13 +1696,34 @@ int uph_job_add_chunk(uph_job* job, const uph_class_desc* cls,
   if (job->chunks.empty()) ctx->timing[0] = 0.f;
   ctx->timing[0] += ms;
   job->chunks.push_back(ch);
+  job->q_graph_valid = false;   // the queue engine's graph covers the old chunk set
   if (chunk_id) *chunk_id = (int32_t)job->chunks.size() - 1;
   return UPH_OK;
 }
 
 int uph_job_solve(uph_job* job, int32_t max_steps) {
   if (!job) return UPH_ERR_INVALID;
+  if (job->engine == UPH_ENGINE_QUEUE && !job->chunks.empty()) {
+    // the queue kernels are instantiated per background setting: every chunk
+    // of the job must share it (else the per-chunk engine runs)
+    bool same_bg = true;
+    for (auto* ch : job->chunks)
+      same_bg = same_bg && ((ch->c.nbg > 0) == (job->chunks[0]->c.nbg > 0));
+    if (same_bg) return job_solve_queue(job, max_steps);
+  }
   return job_solve(job, max_steps);
+}
+
+int uph_job_set_engine(uph_job* job, int32_t engine, int32_t lanes) {
+  if (!job) return UPH_ERR_INVALID;
+  if (engine != UPH_ENGINE_QUEUE && engine != UPH_ENGINE_CHUNKS)
+    return set_err(job->ctx, UPH_ERR_INVALID, "unknown engine %d", engine);
+  if (lanes < 0 || lanes > UPH_MAX_STREAMS)
+    return set_err(job->ctx, UPH_ERR_INVALID, "lanes %d outside 0..%d", lanes, UPH_MAX_STREAMS);
+  job->engine = engine;
+  if (lanes != job->lanes_max) job->q_graph_valid = false;
+  job->lanes_max = lanes;
+  return UPH_OK;
 }
 
 int uph_job_read(uph_job* job, int32_t chunk_id, uph_chunk_out* out) {

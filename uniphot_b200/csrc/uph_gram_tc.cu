@@ -115,7 +115,13 @@ __device__ __forceinline__ int gram_rows(const ClassDev& c, int isl) {
   return gram_K(c, isl);
 }
 
-__global__ void __launch_bounds__(NT) k_gram_tc(ClassDev c, int rcap) {
+// One (island, band, pixel split) Gram on the tensor cores.  RELINQUISH:
+// the CTA frees its tensor-memory allocation permit after allocating (a CTA
+// that runs one unit); a persistent CTA that allocates again for its next
+// unit keeps the permit.  Returns true when a bounded wait expired (the
+// error flag is raised and the unit's Gram is not written).
+template <bool RELINQUISH>
+__device__ __forceinline__ bool gram_tc_body(const ClassDev& c, int rcap, int bx) {
   extern __shared__ __align__(1024) uint8_t tsm[];
   __shared__ __align__(8) uint64_t mbar[2];
   __shared__ uint32_t tmem_base;
@@ -127,12 +133,12 @@ __global__ void __launch_bounds__(NT) k_gram_tc(ClassDev c, int rcap) {
   __shared__ float rsd[2][KC];
   __shared__ int pwy[2][KC], pwx[2][KC];   // window pixel of each chunk slot
   __shared__ int abort_flag;
-  const int split = blockIdx.x % c.tc_split;
-  const int ib = blockIdx.x / c.tc_split;
+  const int split = bx % c.tc_split;
+  const int ib = bx / c.tc_split;
   const int isl = ib / c.nb, b = ib % c.nb;
-  if (isl >= c.n_isl || !isl_active(c.flags[isl], PH_LIN)) return;
+  if (isl >= c.n_isl || !isl_active(c.flags[isl], PH_LIN)) return false;
   const int K = gram_rows(c, isl);
-  if (!tc_island(c, isl, K)) return;         // handled by k_gram_lin
+  if (!tc_island(c, isl, K)) return false;   // handled by k_gram_lin
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int Mh = (K + 127) / 128;            // M = 128 halves
   const int R = Mh * 128;                    // stored rows
@@ -169,7 +175,7 @@ __global__ void __launch_bounds__(NT) k_gram_tc(ClassDev c, int rcap) {
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
                  ::"r"(smem_u32(&tmem_base)), "r"(ncols));
-    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    if (RELINQUISH) asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     asm volatile("tcgen05.fence::before_thread_sync;");
   }
   __syncthreads();
@@ -353,12 +359,17 @@ __global__ void __launch_bounds__(NT) k_gram_tc(ClassDev c, int rcap) {
   __syncthreads();
   if (warp == 0)
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase), "r"(ncols));
+  return abort_flag != 0;
+}
+
+__global__ void __launch_bounds__(NT) k_gram_tc(ClassDev c, int rcap) {
+  gram_tc_body<true>(c, rcap, blockIdx.x);
 }
 
 // Sum of the tc_split partial Grams of every tensor-core island, in split
 // order (deterministic), into the chunk's Gram.
-__global__ void __launch_bounds__(NT) k_gram_tc_reduce(ClassDev c) {
-  const int isl = blockIdx.x / c.nb, b = blockIdx.x % c.nb;
+__device__ __forceinline__ void gram_tc_reduce_body(const ClassDev& c, int bx) {
+  const int isl = bx / c.nb, b = bx % c.nb;
   if (isl >= c.n_isl || !isl_active(c.flags[isl], PH_LIN)) return;
   const int K = gram_rows(c, isl);
   if (!tc_island(c, isl, K)) return;
@@ -375,7 +386,44 @@ __global__ void __launch_bounds__(NT) k_gram_tc_reduce(ClassDev c) {
   }
 }
 
+__global__ void __launch_bounds__(NT) k_gram_tc_reduce(ClassDev c) {
+  gram_tc_reduce_body(c, blockIdx.x);
+}
+
+// Queue kernels of the LM loop: the tensor-core Grams of every active island
+// of the job (a persistent CTA allocates and frees tensor memory per unit and
+// keeps its allocation permit; it stops after an expired wait), and their
+// split reductions.
+__global__ void __launch_bounds__(NT, 3) kq_gram_tc(QueueList q) {
+  queue_run(q, QK_GTC, 1, [&](const ClassDev& c, int isl, int u) {
+    const int kmax = c.Kmax < UPH_MAXK ? c.Kmax : UPH_MAXK;
+    return gram_tc_body<false>(c, rows_cap(kmax), isl * c.nb * c.tc_split + u);
+  });
+}
+
+__global__ void __launch_bounds__(NT) kq_gram_tc_reduce(QueueList q) {
+  queue_run(q, QK_GTCR, 1, [&](const ClassDev& c, int isl, int u) {
+    gram_tc_reduce_body(c, isl * c.nb + u);
+    return false;
+  });
+}
+
 }  // namespace
+
+void launch_q_gram_tc(const QueueList& q, size_t smem, bool reduce, int sms, cudaStream_t s) {
+  int per = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kq_gram_tc, NT, smem) != cudaSuccess ||
+      per < 1)
+    per = 1;
+  kq_gram_tc<<<(unsigned)std::max(1, std::min(per * sms, q.cap[QK_GTC])), NT, smem, s>>>(q);
+  if (reduce) {
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kq_gram_tc_reduce, NT, 0) !=
+            cudaSuccess || per < 1)
+      per = 1;
+    kq_gram_tc_reduce<<<(unsigned)std::max(1, std::min(per * sms, q.cap[QK_GTCR])), NT, 0, s>>>(
+        q);
+  }
+}
 
 int gram_tc_splits(int n_isl, int nb, int B, int sm_count) {
   // enough CTAs for about four per SM, each over at least 8 pixel chunks
@@ -395,6 +443,10 @@ void launch_gram_tc(const ClassDev& c, cudaStream_t s) {
 }
 
 int uph_gram_tc_setup() {
-  return (int)cudaFuncSetAttribute(k_gram_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  const cudaError_t e = cudaFuncSetAttribute(k_gram_tc,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)gram_tc_smem_bytes(UPH_MAXK));
+  if (e != cudaSuccess) return (int)e;
+  return (int)cudaFuncSetAttribute(kq_gram_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)gram_tc_smem_bytes(UPH_MAXK));
 }

@@ -684,3 +684,134 @@ int uph_kernel_setup();
 // Compute-pipe peak kernels (uph_peaks.cu): FP32 and FP64 multiply-add and
 // exp2f rates and the SM clock into out[0..3]; returns a cudaError_t.
 int measure_peaks(cudaStream_t s, int sms, double* out);
+
+// ---- Job-wide work queues of the LM loop -----------------------------------
+// Each LM phase of a job runs as one persistent kernel per kernel kind over
+// every chunk: its CTAs pull items from an atomic counter, an item being one
+// unit of work (the CTA-sized piece the per-chunk kernels map to a block) of
+// an active island.  The active islands of a phase are compacted on the
+// device from a fixed longest-first order of every (chunk, island) of the
+// job, with an exclusive prefix of units per kind, at the start of every
+// iteration, so converged islands drop out of the queue on the device.
+enum { QK_SETUP = 0, QK_RENDER, QK_GLIN, QK_GTC, QK_GTCR, QK_ASSEMBLE, QK_STEP, QK_TRIAL,
+       QK_ACCEPT, QK_KINDS };
+
+struct QueueList {
+  const ClassDev* cls;   // (nch) chunk descriptors
+  int2* act;             // (n_total) active (chunk, island) entries, longest first
+  int* n_act;            // [1]
+  int* pre;              // (QK_KINDS, stride) exclusive prefix of units per kind
+  int stride;            // n_total + 1
+  int* next;             // (QK_KINDS) item counters, zeroed by the build
+  int cap[QK_KINDS];     // units per kind if every island of the list were
+                         // active (the host caps the persistent grids by it)
+};
+
+// Pixel splits of a chunk's FP32 Gram (the per-chunk kernel's grid y).
+__host__ __device__ __forceinline__ int gram_lin_parts(int Kmax) {
+  const int nbk = (Kmax + 7) / 8;
+  const int nblk = nbk * (nbk + 1) / 2;
+  return nblk <= 256 ? 1 : (nblk + 255) / 256;
+}
+
+// Units of work per island of a chunk for each kernel kind: the blocks the
+// per-chunk kernel gives one island.
+__host__ __device__ __forceinline__ int queue_units(const ClassDev& c, int kind) {
+  const bool tc = c.tc_min_rows < (1 << 30);
+  switch (kind) {
+    case QK_SETUP: return c.nb * c.N;
+    case QK_RENDER: return c.nb * c.N * c.ntile_side * c.ntile_side;
+    case QK_GLIN: return c.nb * gram_lin_parts(c.Kmax);
+    case QK_GTC: return tc ? c.nb * c.tc_split : 0;
+    case QK_GTCR: return (tc && c.tc_split > 1) ? c.nb : 0;
+    case QK_ASSEMBLE: return c.nb;
+    case QK_TRIAL: return c.nb;
+    default: return 1;   // step, accept
+  }
+}
+
+// Entry of unit `it` in an exclusive prefix pre[0..n] (pre[0] = 0 <= it <
+// pre[n]): the largest a with pre[a] <= it.  Warp-cooperative (called by all
+// 32 lanes of one warp): each round compares 32 probes spread over the
+// remaining range in one memory round trip and keeps the sub-range between
+// the last probe at or below `it` and the next one.
+__device__ __forceinline__ int queue_find(const int* pre, int n, int it) {
+  const int lane = threadIdx.x & 31;
+  int lo = 0, hi = n;                     // pre[lo] <= it < pre[hi]
+  while (hi - lo > 32) {
+    const long long span = hi - lo;       // >= 33: probes lo + span (j + 1) / 33 lie
+    const int pos = lo + (int)(span * (lane + 1) / 33);   // in [lo + 1, hi - 1]
+    const unsigned m = __ballot_sync(0xffffffffu, pre[pos] <= it);
+    if (m) {
+      const int k = 31 - __clz(m);
+      const int nlo = lo + (int)(span * (k + 1) / 33);
+      if (k < 31) hi = lo + (int)(span * (k + 2) / 33);
+      lo = nlo;
+    } else {
+      hi = lo + (int)(span / 33);
+    }
+  }
+  const int pos = lo + 1 + lane;
+  const unsigned m = __ballot_sync(0xffffffffu, pos < hi && pre[pos] <= it);
+  return m ? lo + 1 + (31 - __clz(m)) : lo;
+}
+
+// Persistent loop of a queue kernel: ranges of `grab` consecutive units from
+// q.next until the kind's units run out (the first unit's entry found by
+// warp 0, the next ones by stepping forward).  The chunk's descriptor is
+// copied into shared memory when the chunk changes; body(c, island, unit)
+// runs the per-chunk kernel's work for that unit with the whole CTA and
+// returns true to stop this CTA (a bounded device wait expired).
+template <class Body>
+__device__ __forceinline__ void queue_run(const QueueList& q, int kind, int grab, Body body) {
+  __shared__ ClassDev sc;
+  __shared__ int s_base, s_a;
+  const int n = *q.n_act;
+  const int* pre = q.pre + (size_t)kind * q.stride;
+  const int total = pre[n];
+  int cur = -1;
+  for (;;) {
+    if (threadIdx.x == 0) s_base = atomicAdd(q.next + kind, grab);
+    __syncthreads();
+    const int base = s_base;
+    if (base >= total) break;
+    if (threadIdx.x < 32) {
+      const int a0 = queue_find(pre, n, base);
+      if (threadIdx.x == 0) s_a = a0;
+    }
+    __syncthreads();
+    int a = s_a;
+    const int end = min(base + grab, total);
+    for (int it = base; it < end; ++it) {
+      while (pre[a + 1] <= it) ++a;         // the same values in every thread
+      const int ch = q.act[a].x;
+      if (ch != cur) {
+        const int* src = reinterpret_cast<const int*>(q.cls + ch);
+        int* dst = reinterpret_cast<int*>(&sc);
+        for (int i = threadIdx.x; i < (int)(sizeof(ClassDev) / sizeof(int)); i += blockDim.x)
+          dst[i] = src[i];
+        cur = ch;
+        __syncthreads();
+      }
+      const bool stop = body(sc, q.act[a].y, it - pre[a]);
+      __syncthreads();
+      if (stop) return;
+    }
+  }
+}
+
+// Launchers of the queue kernels (grid: resident CTAs on every SM).
+void launch_q_setup(const QueueList& q, int phase, bool p_try, int sms, cudaStream_t s);
+void launch_q_render(const QueueList& q, int phase, bool lin, bool p_try, size_t render_smem,
+                     int sms, cudaStream_t s);
+void launch_q_gram_lin(const QueueList& q, bool bg, size_t smem, int sms, cudaStream_t s);
+void launch_q_assemble(const QueueList& q, size_t smem, int sms, cudaStream_t s);
+void launch_q_step(const QueueList& q, size_t smem, int sms, cudaStream_t s);
+void launch_q_trial(const QueueList& q, bool bg, size_t smem, int sms, cudaStream_t s);
+void launch_q_accept(const QueueList& q, int sms, cudaStream_t s);
+void launch_q_gram_tc(const QueueList& q, size_t smem, bool reduce, int sms, cudaStream_t s);
+void launch_q_build(const ClassDev* cls, const int2* order, int n_total, const QueueList& q,
+                    int phase, cudaStream_t s);
+void launch_q_count(const ClassDev* cls, const int2* order, int n_total, int* out,
+                    cudaStream_t s);
+size_t render_phase_smem(const ClassDev& c, int phase);

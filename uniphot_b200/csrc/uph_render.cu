@@ -16,6 +16,8 @@
 // S is either the pixelised polynomial PSF (render mode "reference",
 // psf_polynomial.py:134-197) or the analytic Gaussian-mixture PSF convolved
 // with the Sersic MoG galaxy (render mode "analytic").
+#include <algorithm>
+
 #include "uph_internal.cuh"
 
 namespace {
@@ -162,14 +164,15 @@ __device__ void psf_component(const ClassDev& c, int b, double X, double Y,
 // (reference mode) or the combined Gaussian components (analytic mode),
 // written once to the member record that every render tile of the member
 // reads.
-__global__ void __launch_bounds__(128)
-k_member_setup(ClassDev c, const float* __restrict__ P, int phase) {
+__device__ __forceinline__ void member_setup_body(const ClassDev& c,
+                                                  const float* __restrict__ P, int phase,
+                                                  int bx) {
   __shared__ SetupScratch sc;
   __shared__ int is_gal;
   __shared__ int ncomp;
-  const int k = blockIdx.x % c.N;
-  const int b = (blockIdx.x / c.N) % c.nb;
-  const int isl = blockIdx.x / (c.N * c.nb);
+  const int k = bx % c.N;
+  const int b = (bx / c.N) % c.nb;
+  const int isl = bx / (c.N * c.nb);
   if (isl >= c.n_isl) return;
   if (!isl_active(c.flags[isl], phase)) return;
   if (!c.mmask[isl * c.N + k]) return;
@@ -345,9 +348,14 @@ k_member_setup(ClassDev c, const float* __restrict__ P, int phase) {
   }
 }
 
+__global__ void __launch_bounds__(128)
+k_member_setup(ClassDev c, const float* __restrict__ P, int phase) {
+  member_setup_body(c, P, phase, blockIdx.x);
+}
+
 template <bool LIN>
-__global__ void __launch_bounds__(256)
-k_render(ClassDev c, const float* __restrict__ P, int phase, int nsa) {
+__device__ __forceinline__ void render_body(const ClassDev& c, const float* __restrict__ P,
+                                            int phase, int bx) {
   // LIN: linearisation render (model and derivative rows); the trial and
   // probe renders (model row only) are a separate instantiation that needs
   // far fewer registers, hence more CTAs per SM
@@ -356,7 +364,7 @@ k_render(ClassDev c, const float* __restrict__ P, int phase, int nsa) {
   __shared__ float4 trec[MAXCOMP * (LIN ? 7 : 1)];   // per-tile component records
   __shared__ MemberBox mb;
   const int ntile = c.ntile_side * c.ntile_side;
-  int t = blockIdx.x;
+  int t = bx;
   const int tile = t % ntile;
   t /= ntile;
   const int k = t % c.N;
@@ -698,7 +706,60 @@ k_render(ClassDev c, const float* __restrict__ P, int phase, int nsa) {
   }
 }
 
+template <bool LIN>
+__global__ void __launch_bounds__(256)
+k_render(ClassDev c, const float* __restrict__ P, int phase) {
+  render_body<LIN>(c, P, phase, blockIdx.x);
+}
+
+// Queue kernels of the LM loop: the member set-up and the render of every
+// active island of the job (P = the chunk's p, or p_try for the trial point).
+__global__ void __launch_bounds__(128) kq_member_setup(QueueList q, int phase, int p_try) {
+  queue_run(q, QK_SETUP, 8, [&](const ClassDev& c, int isl, int u) {
+    member_setup_body(c, p_try ? c.p_try : c.p, phase, isl * c.nb * c.N + u);
+    return false;
+  });
+}
+
+// (three resident CTAs per SM, as the per-chunk linearisation render's
+// shared memory allows: the descriptor fields then stay in shared memory
+// instead of registers)
+template <bool LIN>
+__global__ void __launch_bounds__(256, 3) kq_render(QueueList q, int phase, int p_try) {
+  queue_run(q, QK_RENDER, 4, [&](const ClassDev& c, int isl, int u) {
+    render_body<LIN>(c, p_try ? c.p_try : c.p, phase,
+                     isl * c.nb * c.N * c.ntile_side * c.ntile_side + u);
+    return false;
+  });
+}
+
 }  // namespace
+
+// Resident CTAs of kernel f on every SM at `smem` dynamic bytes (at least
+// one per SM).
+template <class F>
+static unsigned queue_grid(F f, int threads, size_t smem, int sms, int cap) {
+  int per = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, f, threads, smem) != cudaSuccess ||
+      per < 1)
+    per = 1;
+  return (unsigned)std::max(1, std::min(per * sms, cap));
+}
+
+void launch_q_setup(const QueueList& q, int phase, bool p_try, int sms, cudaStream_t s) {
+  kq_member_setup<<<queue_grid(kq_member_setup, 128, 0, sms, q.cap[QK_SETUP]), 128, 0, s>>>(
+      q, phase, p_try);
+}
+
+void launch_q_render(const QueueList& q, int phase, bool lin, bool p_try, size_t render_smem,
+                     int sms, cudaStream_t s) {
+  if (lin)
+    kq_render<true><<<queue_grid(kq_render<true>, 256, render_smem, sms, q.cap[QK_RENDER]), 256,
+                      render_smem, s>>>(q, phase, p_try);
+  else
+    kq_render<false><<<queue_grid(kq_render<false>, 256, render_smem, sms, q.cap[QK_RENDER]),
+                       256, render_smem, s>>>(q, phase, p_try);
+}
 
 size_t render_smem_bytes() {
   return sizeof(float) * (size_t)NS * UPH_HALO * HP;
@@ -711,6 +772,10 @@ static int render_arrays(const ClassDev& c, int phase) {
   return c.has_gal ? NS : 3;
 }
 
+size_t render_phase_smem(const ClassDev& c, int phase) {
+  return sizeof(float) * (size_t)render_arrays(c, phase) * UPH_HALO * HP;
+}
+
 void launch_render(const ClassDev& c, const float* P, int phase,
                    cudaStream_t s) {
   const long long nblk = (long long)c.n_isl * c.nb * c.N * c.ntile_side * c.ntile_side;
@@ -720,15 +785,21 @@ void launch_render(const ClassDev& c, const float* P, int phase,
   k_member_setup<<<(unsigned)((long long)c.n_isl * c.nb * c.N), 128, 0, s>>>(c, P, phase);
   if (c.mode == 0 && c.gstamp) launch_gal_fft(c, P, phase, s);
   if (phase == PH_LIN)
-    k_render<true><<<(unsigned)nblk, 256, bytes, s>>>(c, P, phase, nsa);
+    k_render<true><<<(unsigned)nblk, 256, bytes, s>>>(c, P, phase);
   else
-    k_render<false><<<(unsigned)nblk, 256, bytes, s>>>(c, P, phase, nsa);
+    k_render<false><<<(unsigned)nblk, 256, bytes, s>>>(c, P, phase);
 }
 
 int uph_render_setup() {
   cudaError_t e = cudaFuncSetAttribute(k_render<true>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)render_smem_bytes());
+  if (e != cudaSuccess) return (int)e;
+  e = cudaFuncSetAttribute(kq_render<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)render_smem_bytes());
+  if (e != cudaSuccess) return (int)e;
+  e = cudaFuncSetAttribute(kq_render<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)render_smem_bytes());
   if (e != cudaSuccess) return (int)e;
   return (int)cudaFuncSetAttribute(k_render<false>,
                                    cudaFuncAttributeMaxDynamicSharedMemorySize,

@@ -20,6 +20,8 @@
 //                 bounds (island_solver.py:921-967).
 // k_accept     -- accept/reject, lambda update, three convergence prongs
 //                 (island_solver.py:968-1002).
+#include <algorithm>
+
 #include "uph_internal.cuh"
 
 namespace {
@@ -398,21 +400,21 @@ __device__ void load_boxes(const ClassDev& c, int isl, const float* P,
 }
 
 template <bool BG>
-__global__ void __launch_bounds__(NT) k_gram_lin(ClassDev c) {
+__device__ __forceinline__ void gram_lin_body(const ClassDev& c, int bx, int by) {
   extern __shared__ float sm[];
   __shared__ int4 box[UPH_MAXN];
-  const int isl = blockIdx.x / c.nb, b = blockIdx.x % c.nb;
+  const int isl = bx / c.nb, b = bx % c.nb;
   if (isl >= c.n_isl || !isl_active(c.flags[isl], PH_LIN)) return;
   const int nr = c.isl_nr[isl];
   const int K = gram_K(c, isl);
   if (tc_island(c, isl, K)) return;  // the tensor-core Gram handles this island
   const int nbk = (K + 7) / 8;
   const int nblk = nbk * (nbk + 1) / 2;
-  if ((int)blockIdx.y * NT >= max(nblk, 1) && blockIdx.y > 0) return;
-  if (nblk <= NT && blockIdx.y > 0) return;
+  if (by * NT >= max(nblk, 1) && by > 0) return;
+  if (nblk <= NT && by > 0) return;
   load_boxes(c, isl, c.p, box);
   __syncthreads();
-  if (threadIdx.x == 0 && blockIdx.y == 0)
+  if (threadIdx.x == 0 && by == 0)
     gram_work(c, WK_GRAM, c.row_k + (size_t)isl * c.Kmax, c.row_s + (size_t)isl * c.Kmax,
               K, box);
   // the mixed form forms every Gram in residual form (k_assemble matches)
@@ -420,7 +422,12 @@ __global__ void __launch_bounds__(NT) k_gram_lin(ClassDev c) {
               c.fcur ? c.fcur + ((size_t)isl * c.nb + b) * c.NL : nullptr, nr, c.nbg, c.N};
   gram_window<BG>(c, isl, b, rows, box,
               c.gram + ((size_t)isl * c.nb + b) * c.Kmax * c.Kmax, c.Kmax,
-              blockIdx.y, sm);
+              by, sm);
+}
+
+template <bool BG>
+__global__ void __launch_bounds__(NT) k_gram_lin(ClassDev c) {
+  gram_lin_body<BG>(c, blockIdx.x, blockIdx.y);
 }
 
 // Gauss-Jordan elimination with partial pivoting on M (n x ncol, pitch ld):
@@ -486,12 +493,12 @@ __device__ void gauss_jordan(double* M, int n, int ncol, int ld, double* fac,
   if (tid == 0 && cond) *cond = rmin > 0.0 ? (float)(rmax / rmin) : INFINITY;
 }
 
-__global__ void __launch_bounds__(NT) k_assemble(ClassDev c) {
+__device__ __forceinline__ void assemble_body(const ClassDev& c, int bx) {
   extern __shared__ double dsm[];
   __shared__ double fac[UPH_MAXLIN];
   __shared__ double ridge[UPH_MAXLIN];
   __shared__ int piv;
-  const int isl = blockIdx.x / c.nb, b = blockIdx.x % c.nb;
+  const int isl = bx / c.nb, b = bx % c.nb;
   if (isl >= c.n_isl || !isl_active(c.flags[isl], PH_LIN)) return;
   const int tid = threadIdx.x;
   const int nL = c.isl_nL[isl], nr = c.isl_nr[isl];
@@ -641,10 +648,13 @@ __global__ void __launch_bounds__(NT) k_assemble(ClassDev c) {
   }
 }
 
+__global__ void __launch_bounds__(NT) k_assemble(ClassDev c) { assemble_body(c, blockIdx.x); }
+
 template <bool BG>
-__global__ void __launch_bounds__(NT)
-k_gram_trial(ClassDev c, const float* __restrict__ P, int phase,
-             int final_mode, float* __restrict__ fout, float* __restrict__ cout) {
+__device__ __forceinline__ void gram_trial_body(const ClassDev& c, const float* __restrict__ P,
+                                                int phase, int final_mode,
+                                                float* __restrict__ fout,
+                                                float* __restrict__ cout, int bx) {
   extern __shared__ float sm[];
   __shared__ int4 box[UPH_MAXN];
   __shared__ int16_t rk[UPH_MAXLIN + 1], rs[UPH_MAXLIN + 1];
@@ -657,7 +667,7 @@ k_gram_trial(ClassDev c, const float* __restrict__ P, int phase,
   __shared__ double red[NT];
   __shared__ int redi[NT];
   __shared__ int piv;
-  const int isl = blockIdx.x / c.nb, b = blockIdx.x % c.nb;
+  const int isl = bx / c.nb, b = bx % c.nb;
   if (isl >= c.n_isl || !isl_active(c.flags[isl], phase)) return;
   const int tid = threadIdx.x;
   const int nr = c.isl_nr[isl];
@@ -769,6 +779,13 @@ k_gram_trial(ClassDev c, const float* __restrict__ P, int phase,
       }
     if (tid == 0) c.ngood[(size_t)isl * c.nb + b] = redi[0];
   }
+}
+
+template <bool BG>
+__global__ void __launch_bounds__(NT)
+k_gram_trial(ClassDev c, const float* __restrict__ P, int phase,
+             int final_mode, float* __restrict__ fout, float* __restrict__ cout) {
+  gram_trial_body<BG>(c, P, phase, final_mode, fout, cout, blockIdx.x);
 }
 
 // LU with partial pivoting of the n x (n+1) augmented system in M (pitch
@@ -995,8 +1012,8 @@ __device__ void step_dogleg(const ClassDev& c, int isl, int nL, const double* M,
 // 2 plateau probe (lam = probe_lam).  With c.tr a normal step is the
 // trust-region dogleg (island_solver.py:1004-1078); the probes stay damped
 // steps at lam, as the reference's probes are.
-__global__ void __launch_bounds__(NT)
-k_step(ClassDev c, int phase, int probe_mode, int probe_j, float probe_lam) {
+__device__ __forceinline__ void step_body(const ClassDev& c, int phase, int probe_mode,
+                                          int probe_j, float probe_lam, int bx) {
   extern __shared__ double lsm[];
   __shared__ int piv;
   __shared__ double fac[UPH_MAXLIVE];
@@ -1005,7 +1022,7 @@ k_step(ClassDev c, int phase, int probe_mode, int probe_j, float probe_lam) {
   __shared__ double tr_a[UPH_MAXLIVE], tr_b[UPH_MAXLIVE], tr_c[UPH_MAXLIVE];
   __shared__ double red[NT / 32];
   __shared__ int16_t qlive[6 * UPH_MAXN];
-  const int isl = blockIdx.x;
+  const int isl = bx;
   if (isl >= c.n_isl) return;
   const uint8_t fl = c.flags[isl];
   if (!isl_active(fl, phase)) return;
@@ -1120,8 +1137,12 @@ k_step(ClassDev c, int phase, int probe_mode, int probe_j, float probe_lam) {
   for (int q = tid; q < nP; q += NT) out[q] = fminf(fmaxf(out[q], lo[q]), hi[q]);
 }
 
-__global__ void k_accept(ClassDev c, int phase) {
-  const int isl = blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(NT)
+k_step(ClassDev c, int phase, int probe_mode, int probe_j, float probe_lam) {
+  step_body(c, phase, probe_mode, probe_j, probe_lam, blockIdx.x);
+}
+
+__device__ __forceinline__ void accept_one(const ClassDev& c, int phase, int isl) {
   if (isl >= c.n_isl) return;
   const uint8_t fl = c.flags[isl];
   if (!isl_active(fl, phase)) return;
@@ -1247,6 +1268,144 @@ __global__ void k_accept(ClassDev c, int phase) {
   c.consec[isl] = consec;
   c.nrej[isl] = nrej;
   c.nst[isl] = c.nst[isl] + 1;
+}
+
+__global__ void k_accept(ClassDev c, int phase) {
+  accept_one(c, phase, blockIdx.x * blockDim.x + threadIdx.x);
+}
+
+// ---- queue kernels of the LM loop (one launch per kind for the job) ----
+
+// BG: every chunk of the job solves the planar background jointly (the
+// host launches the variant that matches the job)
+template <bool BG>
+__global__ void __launch_bounds__(NT) kq_gram_lin(QueueList q) {
+  queue_run(q, QK_GLIN, 1, [&](const ClassDev& c, int isl, int u) {
+    const int parts = gram_lin_parts(c.Kmax);
+    gram_lin_body<BG>(c, isl * c.nb + u / parts, u % parts);
+    return false;
+  });
+}
+
+__global__ void __launch_bounds__(NT) kq_assemble(QueueList q) {
+  queue_run(q, QK_ASSEMBLE, 1, [&](const ClassDev& c, int isl, int u) {
+    assemble_body(c, isl * c.nb + u);
+    return false;
+  });
+}
+
+// the LM step of every island still iterating (PH_TRIAL: not converged)
+__global__ void __launch_bounds__(NT) kq_step(QueueList q) {
+  queue_run(q, QK_STEP, 1, [&](const ClassDev& c, int isl, int u) {
+    step_body(c, PH_TRIAL, 0, 0, 0.f, isl);
+    return false;
+  });
+}
+
+// the trial chi2 at p_try (fluxes and conditioning of the trial point kept
+// for the mixed form)
+template <bool BG>
+__global__ void __launch_bounds__(NT) kq_gram_trial(QueueList q) {
+  queue_run(q, QK_TRIAL, 1, [&](const ClassDev& c, int isl, int u) {
+    gram_trial_body<BG>(c, c.p_try, PH_TRIAL, 0, c.ftry, c.acond_try, isl * c.nb + u);
+    return false;
+  });
+}
+
+// accept / reject of every active island, one thread per island
+__global__ void kq_accept(QueueList q) {
+  const int n = *q.n_act;
+  for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < n; a += gridDim.x * blockDim.x) {
+    const int2 e = q.act[a];
+    accept_one(q.cls[e.x], PH_TRIAL, e.y);
+  }
+}
+
+// Exclusive scan of v over the CTA (blockDim.x = QB_THREADS); *total gets the
+// CTA's sum.  wsum: 32 ints of shared scratch.
+constexpr int QB_THREADS = 1024;
+__device__ int block_excl_scan(int v, int* wsum, int* total) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int x = v;
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) wsum[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    int w = wsum[lane];
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, w, o);
+      if (lane >= o) w += y;
+    }
+    wsum[lane] = w;
+  }
+  __syncthreads();
+  const int ex = x - v + (warp ? wsum[warp - 1] : 0);
+  *total = wsum[31];
+  __syncthreads();
+  return ex;
+}
+
+// Compacts the job's (chunk, island) order to the islands active in `phase`
+// (order kept: longest first) and writes, per kernel kind, the exclusive
+// prefix of units over the active entries; zeroes the item counters.  One
+// CTA of QB_THREADS threads.
+__global__ void __launch_bounds__(QB_THREADS)
+k_queue_build(const ClassDev* __restrict__ cls, const int2* __restrict__ order, int n_total,
+              QueueList q, int phase) {
+  __shared__ int wsum[32];
+  int run_n = 0;
+  int run[QK_KINDS];
+#pragma unroll
+  for (int k = 0; k < QK_KINDS; ++k) run[k] = 0;
+  for (int base = 0; base < n_total; base += QB_THREADS) {
+    const int i = base + threadIdx.x;
+    int2 e = make_int2(0, 0);
+    bool act = false;
+    if (i < n_total) {
+      e = order[i];
+      act = isl_active(cls[e.x].flags[e.y], phase);
+    }
+    int tot;
+    const int pos = block_excl_scan(act ? 1 : 0, wsum, &tot);
+    if (act) q.act[run_n + pos] = e;
+#pragma unroll
+    for (int k = 0; k < QK_KINDS; ++k) {
+      const int u = act ? queue_units(cls[e.x], k) : 0;
+      int tk;
+      const int ex = block_excl_scan(u, wsum, &tk);
+      if (act) q.pre[(size_t)k * q.stride + run_n + pos] = run[k] + ex;
+      run[k] += tk;
+    }
+    run_n += tot;
+  }
+  if (threadIdx.x == 0) {
+    *q.n_act = run_n;
+    for (int k = 0; k < QK_KINDS; ++k) {
+      q.pre[(size_t)k * q.stride + run_n] = run[k];
+      q.next[k] = 0;
+    }
+  }
+}
+
+// Islands of the job still iterating (not converged), into *out.
+__global__ void k_queue_count(const ClassDev* __restrict__ cls, const int2* __restrict__ order,
+                              int n_total, int* out) {
+  __shared__ int red[NT];
+  int cnt = 0;
+  for (int i = threadIdx.x; i < n_total; i += NT) {
+    const int2 e = order[i];
+    cnt += (cls[e.x].flags[e.y] & FL_CONV) ? 0 : 1;
+  }
+  red[threadIdx.x] = cnt;
+  __syncthreads();
+  for (int st = NT / 2; st > 0; st >>= 1) {
+    if (threadIdx.x < st) red[threadIdx.x] += red[threadIdx.x + st];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *out = red[0];
 }
 
 __global__ void k_count_active(ClassDev c) {
@@ -1726,6 +1885,46 @@ void launch_set_probe(const ClassDev& c, cudaStream_t s) {
   k_set_probe<<<(unsigned)((c.n_isl + 127) / 128), 128, 0, s>>>(c);
 }
 
+template <class F>
+static unsigned queue_grid(F f, int threads, size_t smem, int sms, int cap) {
+  int per = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, f, threads, smem) != cudaSuccess ||
+      per < 1)
+    per = 1;
+  return (unsigned)std::max(1, std::min(per * sms, cap));
+}
+
+void launch_q_gram_lin(const QueueList& q, bool bg, size_t smem, int sms, cudaStream_t s) {
+  if (bg)
+    kq_gram_lin<true><<<queue_grid(kq_gram_lin<true>, NT, smem, sms, q.cap[QK_GLIN]), NT, smem, s>>>(q);
+  else
+    kq_gram_lin<false><<<queue_grid(kq_gram_lin<false>, NT, smem, sms, q.cap[QK_GLIN]), NT, smem, s>>>(q);
+}
+void launch_q_assemble(const QueueList& q, size_t smem, int sms, cudaStream_t s) {
+  kq_assemble<<<queue_grid(kq_assemble, NT, smem, sms, q.cap[QK_ASSEMBLE]), NT, smem, s>>>(q);
+}
+void launch_q_step(const QueueList& q, size_t smem, int sms, cudaStream_t s) {
+  kq_step<<<queue_grid(kq_step, NT, smem, sms, q.cap[QK_STEP]), NT, smem, s>>>(q);
+}
+void launch_q_trial(const QueueList& q, bool bg, size_t smem, int sms, cudaStream_t s) {
+  if (bg)
+    kq_gram_trial<true><<<queue_grid(kq_gram_trial<true>, NT, smem, sms, q.cap[QK_TRIAL]), NT, smem, s>>>(q);
+  else
+    kq_gram_trial<false><<<queue_grid(kq_gram_trial<false>, NT, smem, sms, q.cap[QK_TRIAL]), NT, smem, s>>>(q);
+}
+void launch_q_accept(const QueueList& q, int sms, cudaStream_t s) {
+  kq_accept<<<(unsigned)std::max(1, std::min(4 * sms, (q.cap[QK_ACCEPT] + 127) / 128)), 128,
+              0, s>>>(q);
+}
+void launch_q_build(const ClassDev* cls, const int2* order, int n_total, const QueueList& q,
+                    int phase, cudaStream_t s) {
+  k_queue_build<<<1, QB_THREADS, 0, s>>>(cls, order, n_total, q, phase);
+}
+void launch_q_count(const ClassDev* cls, const int2* order, int n_total, int* out,
+                    cudaStream_t s) {
+  k_queue_count<<<1, NT, 0, s>>>(cls, order, n_total, out);
+}
+
 size_t gram_lin_smem_bytes(int Kmax) {
   // the largest staged-tile footprint over every K <= Kmax (the tile width
   // shrinks as K grows; the trial pass stages tiles for its residual even
@@ -1752,9 +1951,7 @@ size_t step_smem_bytes(int nLmax) {
 }
 
 void launch_gram_lin(const ClassDev& c, cudaStream_t s) {
-  const int nbk = (c.Kmax + 7) / 8;
-  const int nblk = nbk * (nbk + 1) / 2;
-  const int parts = nblk <= NT ? 1 : (nblk + NT - 1) / NT;
+  const int parts = gram_lin_parts(c.Kmax);
   dim3 grid((unsigned)(c.n_isl * c.nb), (unsigned)parts);
   if (c.nbg)
     k_gram_lin<true><<<grid, NT, gram_lin_smem_bytes(c.Kmax), s>>>(c);
@@ -1813,6 +2010,23 @@ int uph_solve_setup() {
                            (int)assemble_smem_bytes(UPH_MAXLIVE, UPH_MAXN));
   if (e != cudaSuccess) return (int)e;
   e = cudaFuncSetAttribute(k_step, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)step_smem_bytes(UPH_MAXLIVE));
+  if (e != cudaSuccess) return (int)e;
+  // the queue kernels take the same largest dynamic footprints
+  for (auto f : {kq_gram_lin<false>, kq_gram_lin<true>}) {
+    e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)gram_lin_smem_bytes(UPH_MAXK));
+    if (e != cudaSuccess) return (int)e;
+  }
+  for (auto f : {kq_gram_trial<false>, kq_gram_trial<true>}) {
+    e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)gram_trial_smem_bytes(UPH_MAXN));
+    if (e != cudaSuccess) return (int)e;
+  }
+  e = cudaFuncSetAttribute(kq_assemble, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)assemble_smem_bytes(UPH_MAXLIVE, UPH_MAXN));
+  if (e != cudaSuccess) return (int)e;
+  e = cudaFuncSetAttribute(kq_step, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)step_smem_bytes(UPH_MAXLIVE));
   return (int)e;
 }

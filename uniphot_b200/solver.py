@@ -457,7 +457,11 @@ class IslandFitJob:
     """``island_fit`` split into its three phases: construction plans the
     classes and uploads the field and every chunk's inputs to the device,
     :meth:`solve` runs all chunks (device-resident, concurrent), and
-    :meth:`result` reads them back and unpacks the per-source rows."""
+    :meth:`result` reads them back and unpacks the per-source rows.
+    ``engine`` picks the LM loop's scheduling: "queue" (every chunk's
+    iteration as one persistent work-queue kernel per kernel kind, islands
+    retired on the device) or "chunks" (each chunk's iterations as its own
+    graph on a stream pool); the results are the same bit for bit."""
 
     def __init__(self, *, bandnames: list, data_minus_bg: np.ndarray,
                  invvar: np.ndarray, psfs: list, island_set, buckets, pos_x, pos_y,
@@ -487,7 +491,8 @@ class IslandFitJob:
                  native_stamp: int | None = None, device: int = 0,
                  field: DeviceField | None = None,
                  chunk_budget_bytes: float = 16e9, precision: str = "plain",
-                 plan: "FieldPlan | None" = None, bg_mode: str = "frozen"):
+                 plan: "FieldPlan | None" = None, bg_mode: str = "frozen",
+                 engine: str = "chunks", lanes: int = 0):
         self.log_fn = log_fn
         if render_mode is None:
             render_mode = "analytic" if _is_mog(psfs[0]) else "reference"
@@ -516,6 +521,7 @@ class IslandFitJob:
         plans = [p for p, _ in fp.classes]
         capped = fp.capped
         self.job = _lib.Job(field.ctx)
+        self.job.set_engine(engine, lanes)
         self.classes = []
         trees = {}
         for plan, host in fp.classes:
