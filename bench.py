@@ -606,6 +606,9 @@ def main():
         if dist is not None:
             dist.barrier()
 
+    # the LM-loop engine of each form is picked by timing its candidates on
+    # this job (bitwise the same results), before the warm-up
+    tuning = {args.precision: job.autotune()}
     for _ in range(args.warmup):
         job.solve()
     with ClockSampler(local) as clk:
@@ -614,6 +617,7 @@ def main():
     # the other Gram form on the same resident field
     other = "plain" if args.precision == "mixed" else "mixed"
     job_o = IslandFitJob(**dict(kw, precision=other), device=local, field=job.field)
+    tuning[other] = job_o.autotune()
     for _ in range(args.warmup):
         job_o.solve()
     ms_o, _ = _timed_solves(job_o, args.steps, stream, barrier, dist)
@@ -706,6 +710,7 @@ def main():
         "e2e": {"value": e2e_v, "unit": "islands/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},
         "gpu_launches": int(launches),
+        "autotune": tuning,
         "clocks": clk.summary(),
         "roofline": roof,
         "device_peaks": pk,

@@ -299,20 +299,23 @@ int uph_job_add_chunk(uph_job* job, const uph_class_desc* cls,
 /* Solve every chunk for up to max_steps LM iterations (device-resident). */
 int uph_job_solve(uph_job* job, int32_t max_steps);
 /* LM loop engine of uph_job_solve.  UPH_ENGINE_QUEUE: every LM iteration
- * runs for all chunks of a lane at once, one persistent kernel per kernel
- * kind pulling (chunk, island, unit) items from a device work queue; the
- * queue holds the islands still iterating, compacted on the device at the
- * start of each iteration from a longest-first order, and one CUDA graph
- * per iteration is launched per lane.  UPH_ENGINE_CHUNKS (the default):
- * each chunk's iterations run as its own CUDA graph on one of a pool of
- * streams.
- * Both compute every island identically (bitwise the same results); the
- * queue engine needs every chunk of the job to share the background mode
- * and otherwise falls back to the per-chunk engine.  Replaces the vmapped
+ * runs for all chunks of a lane at once, one kernel per kernel kind over a
+ * device work queue of (chunk, island, unit) items; the queue holds the
+ * islands still iterating, compacted on the device at the start of each
+ * iteration from a longest-first order, and one CUDA graph per iteration is
+ * launched per lane.  Its CTAs stay resident and pull units from an atomic
+ * counter until the queue is empty.  UPH_ENGINE_QUEUE_PER_CTA: the same
+ * queue with one unit per CTA (the grid covers the lane's units; CTAs past
+ * the active ones exit at once).  UPH_ENGINE_CHUNKS (the default): each
+ * chunk's iterations run as its own CUDA graph on one of a pool of streams.
+ * All compute every island identically (bitwise the same results); the
+ * queue engines need every chunk of the job to share the background mode
+ * and otherwise fall back to the per-chunk engine.  Replaces the vmapped
  * chunk step of island_solver.py:1730-1752 with its width probe
  * (island_solver.py:2257). */
 #define UPH_ENGINE_CHUNKS 0
 #define UPH_ENGINE_QUEUE 1
+#define UPH_ENGINE_QUEUE_PER_CTA 2
 /* lanes (queue engine): the chunks are dealt to this many lanes, longest
  * processing time first, each with its own stream, work lists and iteration
  * graph, so that the lanes' phases overlap on the device (0: the default of

@@ -1,6 +1,6 @@
 """The job-wide work-queue engine against the per-chunk engine.
 
-Both engines run the same per-island computations (the queue kernels call
+The engines run the same per-island computations (the queue kernels call
 the per-chunk kernels' bodies for each unit of work; only the CTA that
 processes a unit, and when, differs), so every output of a solve must be
 bitwise identical: parameters, fluxes, errors, chi2, iteration counts and
@@ -49,10 +49,11 @@ def test_queue_engine_equals_chunk_engine_small_field(mode, kw):
     from uniphot_b200.synth import make_small_field
     f = make_small_field(0)
     a, la = _job(f, mode, "chunks", **kw)
-    b, lb = _job(f, mode, "queue", **kw)
-    assert len(a) == len(b) > 1
-    for i, (x, y) in enumerate(zip(a, b)):
-        _same(x, y, f"{mode} {kw} chunk {i}")
+    for engine in ("queue", "queue_per_cta"):
+        b, lb = _job(f, mode, engine, **kw)
+        assert len(a) == len(b) > 1
+        for i, (x, y) in enumerate(zip(a, b)):
+            _same(x, y, f"{engine} {mode} {kw} chunk {i}")
 
 
 @pytest.mark.parametrize("precision", ["plain", "mixed"])
@@ -62,9 +63,10 @@ def test_queue_engine_equals_chunk_engine_production_field(precision):
     from uniphot_b200.synth import make_production_field
     f = make_production_field(3, side=512, n_bands=3, n_src=300)
     a, la = _job(f, "analytic", "chunks", precision=precision)
-    b, lb = _job(f, "analytic", "queue", precision=precision)
-    assert len(a) == len(b) > 10
-    for i, (x, y) in enumerate(zip(a, b)):
-        _same(x, y, f"{precision} chunk {i}")
-    print(f"launches: chunks engine {la}, queue engine {lb}")
-    assert lb < la
+    for engine in ("queue", "queue_per_cta"):
+        b, lb = _job(f, "analytic", engine, precision=precision)
+        assert len(a) == len(b) > 10
+        for i, (x, y) in enumerate(zip(a, b)):
+            _same(x, y, f"{engine} {precision} chunk {i}")
+        print(f"launches: chunks engine {la}, {engine} engine {lb}")
+        assert lb < la

@@ -19,7 +19,7 @@ UPH_OK, UPH_ERR_INVALID, UPH_ERR_OOM, UPH_ERR_CUDA, UPH_ERR_TIMEOUT, \
 ISLAND_TRIES_DEFAULT = 1 << 20      # UPH_ISLAND_TRIES_DEFAULT
 RENDER_MODES = {"reference": 0, "analytic": 1}
 PRECISIONS = {"plain": 0, "mixed": 1}
-ENGINES = {"chunks": 0, "queue": 1}      # UPH_ENGINE_CHUNKS, UPH_ENGINE_QUEUE
+ENGINES = {"chunks": 0, "queue": 1, "queue_per_cta": 2}   # UPH_ENGINE_*
 
 EXPORTED = ("uph_create", "uph_destroy", "uph_last_error", "uph_set_stream",
             "uph_get_stream", "uph_upload_field", "uph_upload_field_device", "uph_upload_field_unpadded",
@@ -449,8 +449,9 @@ class Job:
     def set_engine(self, engine: str, lanes: int = 0):
         """LM loop engine: "queue" (persistent work-queue kernels, one per
         kernel kind, for all chunks of a lane; ``lanes`` lanes overlap, 0
-        for the default) or "chunks" (each chunk's iterations as its own
-        graph on a stream pool); see uph_job_set_engine."""
+        for the default), "queue_per_cta" (the same queue, one unit per
+        CTA) or "chunks" (each chunk's iterations as its own graph on a
+        stream pool); see uph_job_set_engine."""
         self.ctx.check(lib().uph_job_set_engine(self._h, ENGINES[engine], int(lanes)),
                        "uph_job_set_engine")
 

@@ -1344,6 +1344,7 @@ int job_solve_queue(uph_job* job, int max_steps) {
       q.pre = (int*)job->q_pre[k].ptr + (size_t)QK_KINDS * (ln.off + l);
       q.stride = ln.n + 1;
       q.next = (int*)job->q_next[k].ptr + QK_KINDS * l;
+      q.per_cta = job->engine == UPH_ENGINE_QUEUE_PER_CTA ? 1 : 0;
       for (int kind = 0; kind < QK_KINDS; ++kind) {
         long long cap = 0;
         for (int i : ln.chunks)
@@ -1703,7 +1704,8 @@ int uph_job_add_chunk(uph_job* job, const uph_class_desc* cls,
 
 int uph_job_solve(uph_job* job, int32_t max_steps) {
   if (!job) return UPH_ERR_INVALID;
-  if (job->engine == UPH_ENGINE_QUEUE && !job->chunks.empty()) {
+  if ((job->engine == UPH_ENGINE_QUEUE || job->engine == UPH_ENGINE_QUEUE_PER_CTA) &&
+      !job->chunks.empty()) {
     // the queue kernels are instantiated per background setting: every chunk
     // of the job must share it (else the per-chunk engine runs)
     bool same_bg = true;
@@ -1716,12 +1718,13 @@ int uph_job_solve(uph_job* job, int32_t max_steps) {
 
 int uph_job_set_engine(uph_job* job, int32_t engine, int32_t lanes) {
   if (!job) return UPH_ERR_INVALID;
-  if (engine != UPH_ENGINE_QUEUE && engine != UPH_ENGINE_CHUNKS)
+  if (engine != UPH_ENGINE_QUEUE && engine != UPH_ENGINE_CHUNKS &&
+      engine != UPH_ENGINE_QUEUE_PER_CTA)
     return set_err(job->ctx, UPH_ERR_INVALID, "unknown engine %d", engine);
   if (lanes < 0 || lanes > UPH_MAX_STREAMS)
     return set_err(job->ctx, UPH_ERR_INVALID, "lanes %d outside 0..%d", lanes, UPH_MAX_STREAMS);
+  if (lanes != job->lanes_max || engine != job->engine) job->q_graph_valid = false;
   job->engine = engine;
-  if (lanes != job->lanes_max) job->q_graph_valid = false;
   job->lanes_max = lanes;
   return UPH_OK;
 }

@@ -415,13 +415,15 @@ void launch_q_gram_tc(const QueueList& q, size_t smem, bool reduce, int sms, cud
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kq_gram_tc, NT, smem) != cudaSuccess ||
       per < 1)
     per = 1;
-  kq_gram_tc<<<(unsigned)std::max(1, std::min(per * sms, q.cap[QK_GTC])), NT, smem, s>>>(q);
+  kq_gram_tc<<<(unsigned)std::max(1, q.per_cta ? q.cap[QK_GTC] : std::min(per * sms, q.cap[QK_GTC])),
+               NT, smem, s>>>(q);
   if (reduce) {
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kq_gram_tc_reduce, NT, 0) !=
             cudaSuccess || per < 1)
       per = 1;
-    kq_gram_tc_reduce<<<(unsigned)std::max(1, std::min(per * sms, q.cap[QK_GTCR])), NT, 0, s>>>(
-        q);
+    kq_gram_tc_reduce<<<(unsigned)std::max(
+                            1, q.per_cta ? q.cap[QK_GTCR] : std::min(per * sms, q.cap[QK_GTCR])),
+                        NT, 0, s>>>(q);
   }
 }
 

@@ -705,6 +705,8 @@ struct QueueList {
   int* next;             // (QK_KINDS) item counters, zeroed by the build
   int cap[QK_KINDS];     // units per kind if every island of the list were
                          // active (the host caps the persistent grids by it)
+  int per_cta;           // 1: one unit per CTA, grid = cap (CTAs past the
+                         // active units exit at once); 0: persistent CTAs
 };
 
 // Pixel splits of a chunk's FP32 Gram (the per-chunk kernel's grid y).
@@ -770,6 +772,30 @@ __device__ __forceinline__ void queue_run(const QueueList& q, int kind, int grab
   const int* pre = q.pre + (size_t)kind * q.stride;
   const int total = pre[n];
   int cur = -1;
+  if (q.per_cta) {
+    // one unit per CTA (grid-stride when the grid is smaller than the units)
+    for (int it = blockIdx.x; it < total; it += gridDim.x) {
+      if (threadIdx.x < 32) {
+        const int a0 = queue_find(pre, n, it);
+        if (threadIdx.x == 0) s_a = a0;
+      }
+      __syncthreads();
+      const int a = s_a;
+      const int ch = q.act[a].x;
+      if (ch != cur) {
+        const int* src = reinterpret_cast<const int*>(q.cls + ch);
+        int* dst = reinterpret_cast<int*>(&sc);
+        for (int i = threadIdx.x; i < (int)(sizeof(ClassDev) / sizeof(int)); i += blockDim.x)
+          dst[i] = src[i];
+        cur = ch;
+      }
+      __syncthreads();
+      const bool stop = body(sc, q.act[a].y, it - pre[a]);
+      __syncthreads();
+      if (stop) return;
+    }
+    return;
+  }
   for (;;) {
     if (threadIdx.x == 0) s_base = atomicAdd(q.next + kind, grab);
     __syncthreads();

@@ -738,7 +738,9 @@ __global__ void __launch_bounds__(256, 3) kq_render(QueueList q, int phase, int 
 // Resident CTAs of kernel f on every SM at `smem` dynamic bytes (at least
 // one per SM).
 template <class F>
-static unsigned queue_grid(F f, int threads, size_t smem, int sms, int cap) {
+static unsigned queue_grid(F f, int threads, size_t smem, int sms, int cap, int per_cta) {
+  if (cap <= 0) return 1;
+  if (per_cta) return (unsigned)cap;
   int per = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, f, threads, smem) != cudaSuccess ||
       per < 1)
@@ -747,17 +749,17 @@ static unsigned queue_grid(F f, int threads, size_t smem, int sms, int cap) {
 }
 
 void launch_q_setup(const QueueList& q, int phase, bool p_try, int sms, cudaStream_t s) {
-  kq_member_setup<<<queue_grid(kq_member_setup, 128, 0, sms, q.cap[QK_SETUP]), 128, 0, s>>>(
+  kq_member_setup<<<queue_grid(kq_member_setup, 128, 0, sms, q.cap[QK_SETUP], q.per_cta), 128, 0, s>>>(
       q, phase, p_try);
 }
 
 void launch_q_render(const QueueList& q, int phase, bool lin, bool p_try, size_t render_smem,
                      int sms, cudaStream_t s) {
   if (lin)
-    kq_render<true><<<queue_grid(kq_render<true>, 256, render_smem, sms, q.cap[QK_RENDER]), 256,
+    kq_render<true><<<queue_grid(kq_render<true>, 256, render_smem, sms, q.cap[QK_RENDER], q.per_cta), 256,
                       render_smem, s>>>(q, phase, p_try);
   else
-    kq_render<false><<<queue_grid(kq_render<false>, 256, render_smem, sms, q.cap[QK_RENDER]),
+    kq_render<false><<<queue_grid(kq_render<false>, 256, render_smem, sms, q.cap[QK_RENDER], q.per_cta),
                        256, render_smem, s>>>(q, phase, p_try);
 }
 

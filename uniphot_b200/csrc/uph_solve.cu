@@ -1886,7 +1886,9 @@ void launch_set_probe(const ClassDev& c, cudaStream_t s) {
 }
 
 template <class F>
-static unsigned queue_grid(F f, int threads, size_t smem, int sms, int cap) {
+static unsigned queue_grid(F f, int threads, size_t smem, int sms, int cap, int per_cta) {
+  if (cap <= 0) return 1;
+  if (per_cta) return (unsigned)cap;
   int per = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, f, threads, smem) != cudaSuccess ||
       per < 1)
@@ -1896,21 +1898,21 @@ static unsigned queue_grid(F f, int threads, size_t smem, int sms, int cap) {
 
 void launch_q_gram_lin(const QueueList& q, bool bg, size_t smem, int sms, cudaStream_t s) {
   if (bg)
-    kq_gram_lin<true><<<queue_grid(kq_gram_lin<true>, NT, smem, sms, q.cap[QK_GLIN]), NT, smem, s>>>(q);
+    kq_gram_lin<true><<<queue_grid(kq_gram_lin<true>, NT, smem, sms, q.cap[QK_GLIN], q.per_cta), NT, smem, s>>>(q);
   else
-    kq_gram_lin<false><<<queue_grid(kq_gram_lin<false>, NT, smem, sms, q.cap[QK_GLIN]), NT, smem, s>>>(q);
+    kq_gram_lin<false><<<queue_grid(kq_gram_lin<false>, NT, smem, sms, q.cap[QK_GLIN], q.per_cta), NT, smem, s>>>(q);
 }
 void launch_q_assemble(const QueueList& q, size_t smem, int sms, cudaStream_t s) {
-  kq_assemble<<<queue_grid(kq_assemble, NT, smem, sms, q.cap[QK_ASSEMBLE]), NT, smem, s>>>(q);
+  kq_assemble<<<queue_grid(kq_assemble, NT, smem, sms, q.cap[QK_ASSEMBLE], q.per_cta), NT, smem, s>>>(q);
 }
 void launch_q_step(const QueueList& q, size_t smem, int sms, cudaStream_t s) {
-  kq_step<<<queue_grid(kq_step, NT, smem, sms, q.cap[QK_STEP]), NT, smem, s>>>(q);
+  kq_step<<<queue_grid(kq_step, NT, smem, sms, q.cap[QK_STEP], q.per_cta), NT, smem, s>>>(q);
 }
 void launch_q_trial(const QueueList& q, bool bg, size_t smem, int sms, cudaStream_t s) {
   if (bg)
-    kq_gram_trial<true><<<queue_grid(kq_gram_trial<true>, NT, smem, sms, q.cap[QK_TRIAL]), NT, smem, s>>>(q);
+    kq_gram_trial<true><<<queue_grid(kq_gram_trial<true>, NT, smem, sms, q.cap[QK_TRIAL], q.per_cta), NT, smem, s>>>(q);
   else
-    kq_gram_trial<false><<<queue_grid(kq_gram_trial<false>, NT, smem, sms, q.cap[QK_TRIAL]), NT, smem, s>>>(q);
+    kq_gram_trial<false><<<queue_grid(kq_gram_trial<false>, NT, smem, sms, q.cap[QK_TRIAL], q.per_cta), NT, smem, s>>>(q);
 }
 void launch_q_accept(const QueueList& q, int sms, cudaStream_t s) {
   kq_accept<<<(unsigned)std::max(1, std::min(4 * sms, (q.cap[QK_ACCEPT] + 127) / 128)), 128,

@@ -522,6 +522,7 @@ class IslandFitJob:
         capped = fp.capped
         self.job = _lib.Job(field.ctx)
         self.job.set_engine(engine, lanes)
+        self.tuning = None
         self.classes = []
         trees = {}
         for plan, host in fp.classes:
@@ -573,6 +574,35 @@ class IslandFitJob:
         t0 = time.perf_counter()
         self.job.solve(self.max_steps)
         self.solve_wall_s = time.perf_counter() - t0
+
+    # LM-loop engine configurations the autotuner times: (engine, lanes)
+    AUTOTUNE_CANDIDATES = (("chunks", 0), ("queue", 8), ("queue", 16), ("queue", 32),
+                           ("queue_per_cta", 16))
+
+    def autotune(self, candidates=AUTOTUNE_CANDIDATES, repeats: int = 2) -> dict:
+        """Time this job's solve under each LM-loop engine configuration and
+        keep the fastest.  Every configuration computes bitwise the same
+        results (the queue kernels run the per-chunk kernels' work for each
+        unit), so the choice changes only the speed.  Each candidate runs one
+        untimed solve (graph capture, allocations) and ``repeats`` timed ones
+        (device time of the whole solve from the library's events, best of
+        the repeats).  The choice and the times are kept in ``self.tuning``
+        and returned."""
+        times = {}
+        for engine, lanes in candidates:
+            self.job.set_engine(engine, lanes)
+            self.solve()
+            best = float("inf")
+            for _ in range(max(1, repeats)):
+                self.solve()
+                best = min(best, self.field.ctx.last_timing()[1])
+            times[f"{engine}/{lanes}"] = best
+        pick = min(times, key=times.get)
+        engine, lanes = pick.split("/")
+        self.job.set_engine(engine, int(lanes))
+        self.tuning = {"ms_per_solve": times, "picked": pick,
+                       "what": "LM-loop engine and lanes, by device time of a full solve"}
+        return self.tuning
 
     def result(self) -> IslandFitResult:
         out_rows, bucket_stats = [], []
