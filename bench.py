@@ -5,22 +5,32 @@ Workload (one "step"): every fitted island of the synthetic production field
 4-component elliptical Gaussian-mixture PSF varying as an order-2 polynomial,
 analytic render mode) solved to convergence (max 30 LM iterations) on one GPU.
 
-* ``value``: islands/s with the field and every chunk's inputs already
-  resident in HBM (``IslandFitJob.solve``), CUDA events on the library stream,
-  synchronize + barrier on both sides, max over ranks.  The field stacks
-  (671 MB) exceed L2, so no explicit flush is needed between steps.
-* ``e2e``: islands/s through the public API ``island_fit(...)`` from host
-  arrays: planning, field + inputs host->device, solve, results
+* ``value``: islands/s at the metric's tolerance: the solve's islands/s with
+  the field and every chunk's inputs already resident in HBM
+  (``IslandFitJob.solve``; CUDA events on the library stream, synchronize +
+  barrier on both sides, max over ranks) times the fraction of islands whose
+  every flux is within 1e-4 relative or 0.01 sigma of the float64 oracle,
+  estimated on a class-stratified sample (every class in it, >= 100
+  islands).  ``forms.*.value_all_islands`` counts every island.  The field
+  stacks (671 MB) exceed L2, so no explicit flush is needed between steps.
+  The LM-loop engine of each form is picked by ``IslandFitJob.autotune``
+  before the warm-up (``autotune`` in the line).
+* ``e2e``: the same metric through the public API ``island_fit(...)`` from
+  host arrays: planning, field + inputs host->device, solve, results
   device->host, unpack.
-* ``roofline``: the dominant kernel of an instrumented solve (per-launch CUDA
-  events) against the measured peaks in MEASURED_PEAKS.json.
+* ``roofline``: the dominant kernel of an instrumented solve against its
+  binding peak, and the t_lb model over every kernel kind (bytes / HBM,
+  flops / pipe, exp2 / SFU; HBM and BF16 from MEASURED_PEAKS.json, FP32,
+  FP64 and exp2f measured in the run).
 * ``cpu_baseline``: the CPU restatement of the reference algorithm (the
   oracle, reference precision) on a seeded 1% sample of the same islands,
-  over all host cores.
+  every sampled island solved and timed inside its worker, over all host
+  cores: islands x cores / core-seconds.
 
-``--impl reference`` prints the reference arm: the CPU restatement timed on
-the same workload (bounded samples), since the reference's own JAX solver is
-not installable here.
+``--impl reference`` prints the reference arm: the same CPU measurement,
+since the reference's own JAX solver is installed neither here nor on the
+GPU box.  ``--batched``, ``--precision-stress``, ``--reference-render`` and
+``--serve-only`` print the other configurations' lines.
 
 Multi-GPU (torchrun): weak scaling, every rank solves its own seeded field
 (islands are independent: no collective on the data path); time = max over
@@ -423,6 +433,108 @@ def _stress_measure(args, device):
     return out
 
 
+def _host_bytes_available() -> float:
+    """Host memory this process may still use: MemAvailable, capped by the
+    container's memory limit when one is set."""
+    avail = float("inf")
+    try:
+        for line in open("/proc/meminfo"):
+            if line.startswith("MemAvailable:"):
+                avail = float(line.split()[1]) * 1024
+    except OSError:
+        pass
+    for path in ("/sys/fs/cgroup/memory.max", "/sys/fs/cgroup/memory/memory.limit_in_bytes"):
+        try:
+            lim = open(path).read().strip()
+            used_p = path.replace("memory.max", "memory.current").replace(
+                "limit_in_bytes", "usage_in_bytes")
+            if lim != "max" and float(lim) < 1e18:
+                avail = min(avail, float(lim) - float(open(used_p).read().strip()))
+        except (OSError, ValueError):
+            pass
+    return avail
+
+
+def _batched_measure(args, device):
+    """The batched configuration: about ``args.batched_islands`` islands spread
+    over three production-style fields (generator of the production field at
+    its source density, 60/20/12/8% STAR/EXP/DEV/SERSIC, clustered islands of
+    1-64 members) with 5, 20 and 40 bands, a third of the islands each.
+    Every field is solved in both forms, the LM-loop engine picked by the
+    autotuner (per-chunk engine or work queue with 16 lanes); islands/s per
+    field and form, and per member-count class on the 20-band field (each
+    class group solved as its own job).  Islands above 32 members keep their
+    seeds (giant rows, the reference's joint cap) and are counted apart."""
+    import dataclasses
+    import gc
+    import math
+    import torch
+    from uniphot_b200.solver import IslandFitJob, plan_field
+    from uniphot_b200.synth import make_production_field
+
+    def timed(job, steps):
+        stream = torch.cuda.ExternalStream(job.field.ctx.stream_ptr())
+        job.solve()
+        ms, _ = _timed_solves(job, steps, stream, torch.cuda.synchronize, None)
+        return ms / steps
+
+    out = {"target_islands": args.batched_islands, "fields": []}
+    per_field = args.batched_islands / 3.0
+    for k, nb in enumerate((5, 20, 40)):
+        # the production field: 5000 sources give 1134 fitted islands on 2048^2
+        n_src = int(round(per_field * 5000 / 1134))
+        # host arrays: data and weights (float32), twice over for padding and
+        # generation; keep a third of what is available free
+        need = 4.0 * 4 * nb * (2048.0 ** 2) * n_src / 5000
+        scale = min(1.0, _host_bytes_available() / (1.5 * need))
+        n_src = int(n_src * scale)
+        side = int(round(2048 * math.sqrt(n_src / 5000)))
+        t0 = time.perf_counter()
+        f = make_production_field(args.seed + 101 * k, side=side, n_bands=nb, n_src=n_src,
+                                  device="cuda")
+        row = {"n_bands": nb, "side": side, "n_src": n_src, "host_memory_scale": scale,
+               "generation_s": time.perf_counter() - t0}
+        kw = f.fit_kwargs("analytic")
+        fp = plan_field(**kw)
+        n_isl = sum(p.n_islands for p, _ in fp.classes)
+        row["n_islands"] = n_isl
+        row["giant_islands"] = int(len(fp.capped))
+        field = None
+        for prec in ("plain", "mixed"):
+            job = IslandFitJob(**dict(kw, precision=prec), device=device, plan=fp, field=field)
+            field = job.field
+            tun = job.autotune(candidates=(("chunks", 0), ("queue", 16)), repeats=1)
+            ms = timed(job, args.batched_steps)
+            row[prec] = {"islands_per_s": n_isl / (ms / 1e3), "ms_per_solve": ms,
+                         "autotune": tun}
+            job.close()
+            if nb == 20:
+                groups = {}
+                for p, h in fp.classes:
+                    groups.setdefault(int(p.nsrc_class), []).append((p, h))
+                per_class = {}
+                for nsrc, cl in sorted(groups.items()):
+                    sub = dataclasses.replace(fp, classes=cl)
+                    jb = IslandFitJob(**dict(kw, precision=prec), device=device, plan=sub,
+                                      field=field)
+                    m = sum(p.n_islands for p, _ in cl)
+                    msc = timed(jb, args.batched_steps)
+                    per_class[str(nsrc)] = {"islands": m, "islands_per_s": m / (msc / 1e3),
+                                            "ms_per_solve": msc}
+                    jb.close()
+                row[prec]["by_member_class"] = per_class
+        out["fields"].append(row)
+        del f, field, kw, fp
+        gc.collect()
+        torch.cuda.empty_cache()
+    for prec in ("plain", "mixed"):
+        isl = sum(r["n_islands"] for r in out["fields"])
+        t = sum(r[prec]["ms_per_solve"] for r in out["fields"]) / 1e3
+        out[prec + "_islands_per_s"] = isl / t
+    out["n_islands"] = sum(r["n_islands"] for r in out["fields"])
+    return out
+
+
 def _serve_measure(args, rates, device):
     """Serving: the same seeded request pool streamed with Poisson arrivals
     through the batched+mixed server and through one plain FP32 worker (one
@@ -542,6 +654,11 @@ def main():
     ap.add_argument("--precision-stress", action="store_true",
                     help="run only the precision-stress measurement (crowded "
                          "blends, 40 bands) and print its JSON line")
+    ap.add_argument("--batched", action="store_true",
+                    help="run only the batched configuration (about --batched-islands "
+                         "islands over fields of 5, 20 and 40 bands) and print its JSON line")
+    ap.add_argument("--batched-islands", type=int, default=100000)
+    ap.add_argument("--batched-steps", type=int, default=2)
     ap.add_argument("--stress-islands", type=int, default=2000)
     ap.add_argument("--stress-sample", type=int, default=120)
     ap.add_argument("--only-class", default=None,
@@ -563,6 +680,10 @@ def main():
         if rank == 0:
             print(json.dumps({"precision_stress": _stress_measure(args, local)}),
                   flush=True)
+        return
+    if args.batched:
+        if rank == 0:
+            print(json.dumps({"batched": _batched_measure(args, local)}), flush=True)
         return
     if args.reference_render:
         if rank == 0:
