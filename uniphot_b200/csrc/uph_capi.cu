@@ -439,7 +439,7 @@ struct QueueLane {
   QueueList ql[2];
   size_t sm_rlin = 0, sm_rtry = 0, sm_glin = 0, sm_gtc = 0, sm_asm = 0, sm_step = 0,
          sm_trial = 0;
-  bool any_tc = false, any_red = false, any_fft = false;
+  bool any_tc = false, any_red = false, any_fft = false, any_glr = false;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t gexec = nullptr;
   int graph_kernels = 0;
@@ -525,7 +525,7 @@ struct Launcher {
 void iteration(const ClassDev& c, Launcher& L) {
   cudaStream_t s = L.s;
   L(0, [&] { launch_render(c, c.p, PH_LIN, s); }, 2);
-  L(1, [&] { launch_gram_lin(c, s); });
+  L(1, [&] { launch_gram_lin(c, s); }, c.gl_split > 1 ? 2 : 1);
   if (c.tc_min_rows < (1 << 30))
     L(WK_GRAM_TC, [&] { launch_gram_tc(c, s); }, c.tc_split > 1 ? 2 : 1);
   L(2, [&] { launch_assemble(c, s); });
@@ -728,6 +728,9 @@ int add_chunk(uph_ctx* ctx, Chunk* ch, const uph_class_desc* cls,
   c.probe_p = cbuf<float>(ctx, ch, "probep", (size_t)n * 4 * nP, &rc);
   c.n_active = cbuf<int>(ctx, ch, "nact", 1, &rc);
   c.err = cbuf<int>(ctx, ch, "err", 1, &rc);
+  c.gl_split = gram_lin_splits(B, Kmax);
+  if (c.gl_split > 1)
+    c.glpart = cbuf<float>(ctx, ch, "glpart", (size_t)c.gl_split * n * nb * Kmax * Kmax, &rc);
   c.tc_split = 1;
   if (c.tc_min_rows < (1 << 30)) {
     c.fcur = cbuf<float>(ctx, ch, "fcur", (size_t)n * nb * c.NL, &rc);
@@ -944,7 +947,7 @@ void post_loop(Chunk* ch, Launcher& L) {
     ce.cjac = ch->d_cjac;
     launch_errors_begin(c, s);
     L(0, [&] { launch_render(c, c.p, PH_LIN, s); }, 2);
-    L(1, [&] { launch_gram_lin(c, s); });
+    L(1, [&] { launch_gram_lin(c, s); }, c.gl_split > 1 ? 2 : 1);
     if (c.tc_min_rows < (1 << 30))
       L(WK_GRAM_TC, [&] { launch_gram_tc(c, s); }, c.tc_split > 1 ? 2 : 1);
     L(2, [&] { launch_assemble(ce, s); });
@@ -1354,12 +1357,13 @@ int job_solve_queue(uph_job* job, int max_steps) {
     }
     // launch shapes: the largest footprint over the lane's chunks
     ln.sm_rlin = ln.sm_rtry = ln.sm_glin = ln.sm_gtc = ln.sm_asm = ln.sm_step = ln.sm_trial = 0;
-    ln.any_tc = ln.any_red = ln.any_fft = false;
+    ln.any_tc = ln.any_red = ln.any_fft = ln.any_glr = false;
     for (int i : ln.chunks) {
       const ClassDev& c = job->chunks[i]->c;
       ln.sm_rlin = std::max(ln.sm_rlin, render_phase_smem(c, PH_LIN));
       ln.sm_rtry = std::max(ln.sm_rtry, render_phase_smem(c, PH_TRIAL));
       ln.sm_glin = std::max(ln.sm_glin, gram_lin_smem_bytes(c.Kmax));
+      ln.any_glr = ln.any_glr || c.gl_split > 1;
       ln.sm_asm = std::max(ln.sm_asm, assemble_smem_bytes(c.nLmax, c.N));
       ln.sm_step = std::max(ln.sm_step, step_smem_bytes(c.nLmax));
       ln.sm_trial = std::max(ln.sm_trial, gram_trial_smem_bytes(c.N));
@@ -1422,7 +1426,8 @@ int job_solve_queue(uph_job* job, int max_steps) {
       gal_fft(PH_LIN, false);
       launch_q_render(ln.ql[0], PH_LIN, true, false, ln.sm_rlin, sms, ls);
     }, 2);
-    L(1, [&] { launch_q_gram_lin(ln.ql[0], bg, ln.sm_glin, sms, ls); });
+    L(1, [&] { launch_q_gram_lin(ln.ql[0], bg, ln.any_glr, ln.sm_glin, sms, ls); },
+      ln.any_glr ? 2 : 1);
     if (ln.any_tc)
       L(WK_GRAM_TC, [&] { launch_q_gram_tc(ln.ql[0], ln.sm_gtc, ln.any_red, sms, ls); },
         ln.any_red ? 2 : 1);

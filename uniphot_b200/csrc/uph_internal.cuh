@@ -206,6 +206,11 @@ struct ClassDev {
                            // each over a contiguous range of pixel chunks
   float* gpart;            // (tc_split, n_isl, nb, Kmax, Kmax) partial Grams
                            // (tc_split > 1), summed in split order
+  int gl_split;            // CTAs per (island, band, block set) of the FP32
+                           // Gram, each over a contiguous range of pixel tiles
+                           // (a function of the window side only)
+  float* glpart;           // (gl_split, n_isl, nb, Kmax, Kmax) its partial
+                           // Grams (gl_split > 1), summed in split order
   float reg, pos_step_max, ftol_rel, step_tol;
   int un_freeze;
 };
@@ -693,8 +698,8 @@ int measure_peaks(cudaStream_t s, int sms, double* out);
 // device from a fixed longest-first order of every (chunk, island) of the
 // job, with an exclusive prefix of units per kind, at the start of every
 // iteration, so converged islands drop out of the queue on the device.
-enum { QK_SETUP = 0, QK_RENDER, QK_GLIN, QK_GTC, QK_GTCR, QK_ASSEMBLE, QK_STEP, QK_TRIAL,
-       QK_ACCEPT, QK_KINDS };
+enum { QK_SETUP = 0, QK_RENDER, QK_GLIN, QK_GLINR, QK_GTC, QK_GTCR, QK_ASSEMBLE, QK_STEP,
+       QK_TRIAL, QK_ACCEPT, QK_KINDS };
 
 struct QueueList {
   const ClassDev* cls;   // (nch) chunk descriptors
@@ -709,11 +714,29 @@ struct QueueList {
                          // active units exit at once); 0: persistent CTAs
 };
 
-// Pixel splits of a chunk's FP32 Gram (the per-chunk kernel's grid y).
+// Block sets of a chunk's FP32 Gram (CTAs that share the 8 x 8 blocks of the
+// upper triangle when there are more blocks than threads).
 __host__ __device__ __forceinline__ int gram_lin_parts(int Kmax) {
   const int nbk = (Kmax + 7) / 8;
   const int nblk = nbk * (nbk + 1) / 2;
   return nblk <= 256 ? 1 : (nblk + 255) / 256;
+}
+
+// The per-chunk FP32 Gram kernel's grid y: block sets x pixel splits.
+__host__ __device__ __forceinline__ int gram_lin_ydim(const ClassDev& c) {
+  return gram_lin_parts(c.Kmax) * (c.gl_split > 1 ? c.gl_split : 1);
+}
+
+// Pixel splits of the FP32 Gram for a window of side B and Kmax rows: one
+// CTA per 2048 window pixels of a large Gram, at most 8 (windows of 96 and
+// 128 px hold the blends with the largest Grams and the fewest islands per
+// class, whose Gram CTAs would otherwise run alone); no split for small
+// Grams or windows.  Depends on the class only, so an island's Gram does not
+// depend on how many islands its chunk holds.
+__host__ __device__ __forceinline__ int gram_lin_splits(int B, int Kmax) {
+  if (Kmax <= 32 || B * B < 4096) return 1;
+  const int s = (B * B) / 2048;
+  return s < 8 ? s : 8;
 }
 
 // Units of work per island of a chunk for each kernel kind: the blocks the
@@ -723,7 +746,8 @@ __host__ __device__ __forceinline__ int queue_units(const ClassDev& c, int kind)
   switch (kind) {
     case QK_SETUP: return c.nb * c.N;
     case QK_RENDER: return c.nb * c.N * c.ntile_side * c.ntile_side;
-    case QK_GLIN: return c.nb * gram_lin_parts(c.Kmax);
+    case QK_GLIN: return c.nb * gram_lin_ydim(c);
+    case QK_GLINR: return c.gl_split > 1 ? c.nb : 0;
     case QK_GTC: return tc ? c.nb * c.tc_split : 0;
     case QK_GTCR: return (tc && c.tc_split > 1) ? c.nb : 0;
     case QK_ASSEMBLE: return c.nb;
@@ -830,7 +854,8 @@ __device__ __forceinline__ void queue_run(const QueueList& q, int kind, int grab
 void launch_q_setup(const QueueList& q, int phase, bool p_try, int sms, cudaStream_t s);
 void launch_q_render(const QueueList& q, int phase, bool lin, bool p_try, size_t render_smem,
                      int sms, cudaStream_t s);
-void launch_q_gram_lin(const QueueList& q, bool bg, size_t smem, int sms, cudaStream_t s);
+void launch_q_gram_lin(const QueueList& q, bool bg, bool reduce, size_t smem, int sms,
+                       cudaStream_t s);
 void launch_q_assemble(const QueueList& q, size_t smem, int sms, cudaStream_t s);
 void launch_q_step(const QueueList& q, size_t smem, int sms, cudaStream_t s);
 void launch_q_trial(const QueueList& q, bool bg, size_t smem, int sms, cudaStream_t s);

@@ -250,14 +250,17 @@ __device__ __forceinline__ unsigned dynamic_smem_bytes() {
 // of the upper triangle over its share of the pixels; the s threads sharing
 // a block are s consecutive lanes (s a power of two), reduced by shuffles in
 // a fixed order, and through a small shared buffer when s > 32.
+// sp / nsp: this CTA's share of the window's pixel tiles (contiguous, in
+// order), for a Gram split over nsp CTAs whose partial Grams are summed
+// afterwards; the small path (K <= 8) runs whole in split 0.
 template <bool BG>
 __device__ void gram_window(const ClassDev& c, int isl, int b, RowSrc rows,
                             const int4* box, float* out, int ld, int part,
-                            float* sm) {
+                            float* sm, int sp = 0, int nsp = 1) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int K = rows.K;
   if (K <= 8) {
-    if (part == 0) gram_window_small<BG>(c, isl, b, rows, box, out, ld, sm);
+    if (part == 0 && sp == 0) gram_window_small<BG>(c, isl, b, rows, box, out, ld, sm);
     return;
   }
   if (sizeof(float) * (size_t)tile_floats(K) > dynamic_smem_bytes()) {
@@ -301,16 +304,19 @@ __device__ void gram_window(const ClassDev& c, int isl, int b, RowSrc rows,
   for (int i = 0; i < 8; ++i)
 #pragma unroll
     for (int j = 0; j < 8; ++j) acc[i][j] = 0.f;
-  const int ntile = (npix + TP - 1) / TP;
+  const int ntall = (npix + TP - 1) / TP;
+  const int tps = (ntall + nsp - 1) / nsp;        // tiles per split
+  const int t0 = sp * tps;
+  const int ntile = min(ntall, t0 + tps);
   // padding rows K..nrows-1 of both tiles stay zero for the whole pass
   for (int e = tid; e < (nrows - K) * LD; e += NT) {
     sm[K * LD + e] = 0.f;
     sm[nrows * LD + K * LD + e] = 0.f;
   }
   __syncthreads();
-  stage(0, 0);
-  for (int t = 0; t < ntile; ++t) {
-    const int cur = t & 1;
+  if (t0 < ntile) stage(t0 * TP, 0);
+  for (int t = t0; t < ntile; ++t) {
+    const int cur = (t - t0) & 1;
     cp_async_wait_all();
     __syncthreads();
     float* Z = sm + cur * nrows * LD;
@@ -408,10 +414,14 @@ __device__ __forceinline__ void gram_lin_body(const ClassDev& c, int bx, int by)
   const int nr = c.isl_nr[isl];
   const int K = gram_K(c, isl);
   if (tc_island(c, isl, K)) return;  // the tensor-core Gram handles this island
+  // by = block set + parts x pixel split
+  const int parts = gram_lin_parts(c.Kmax);
+  const int part = by % parts, sp = by / parts;
+  const int nsp = c.gl_split > 1 ? c.gl_split : 1;
   const int nbk = (K + 7) / 8;
   const int nblk = nbk * (nbk + 1) / 2;
-  if (by * NT >= max(nblk, 1) && by > 0) return;
-  if (nblk <= NT && by > 0) return;
+  if (part * NT >= max(nblk, 1) && part > 0) return;
+  if (nblk <= NT && part > 0) return;
   load_boxes(c, isl, c.p, box);
   __syncthreads();
   if (threadIdx.x == 0 && by == 0)
@@ -420,9 +430,37 @@ __device__ __forceinline__ void gram_lin_body(const ClassDev& c, int bx, int by)
   // the mixed form forms every Gram in residual form (k_assemble matches)
   RowSrc rows{c.row_k + (size_t)isl * c.Kmax, c.row_s + (size_t)isl * c.Kmax, K,
               c.fcur ? c.fcur + ((size_t)isl * c.nb + b) * c.NL : nullptr, nr, c.nbg, c.N};
-  gram_window<BG>(c, isl, b, rows, box,
-              c.gram + ((size_t)isl * c.nb + b) * c.Kmax * c.Kmax, c.Kmax,
-              by, sm);
+  const size_t mat = (size_t)c.Kmax * c.Kmax;
+  float* out = nsp > 1 ? c.glpart + (size_t)sp * c.n_isl * c.nb * mat
+                       : c.gram;
+  gram_window<BG>(c, isl, b, rows, box, out + ((size_t)isl * c.nb + b) * mat, c.Kmax,
+                  part, sm, sp, nsp);
+}
+
+// Sum of the gl_split partial FP32 Grams of an (island, band), in split order
+// (deterministic), into the chunk's Gram; a Gram of K <= 8 rows was formed
+// whole by split 0.
+__device__ __forceinline__ void gram_lin_reduce_body(const ClassDev& c, int bx) {
+  const int isl = bx / c.nb, b = bx % c.nb;
+  if (isl >= c.n_isl || !isl_active(c.flags[isl], PH_LIN)) return;
+  const int K = gram_K(c, isl);
+  if (tc_island(c, isl, K)) return;
+  const size_t mat = (size_t)c.Kmax * c.Kmax;
+  const size_t stride = (size_t)c.n_isl * c.nb * mat;
+  const float* src = c.glpart + ((size_t)isl * c.nb + b) * mat;
+  float* dst = c.gram + ((size_t)isl * c.nb + b) * mat;
+  const int nsp = K <= 8 ? 1 : c.gl_split;
+  for (int e = threadIdx.x; e < K * K; e += NT) {
+    const int r = e / K, q = e - (e / K) * K;
+    const size_t o = (size_t)r * c.Kmax + q;
+    float t = src[o];
+    for (int sp = 1; sp < nsp; ++sp) t += src[sp * stride + o];
+    dst[o] = t;
+  }
+}
+
+__global__ void __launch_bounds__(NT) k_gram_lin_reduce(ClassDev c) {
+  gram_lin_reduce_body(c, blockIdx.x);
 }
 
 template <bool BG>
@@ -1281,8 +1319,15 @@ __global__ void k_accept(ClassDev c, int phase) {
 template <bool BG>
 __global__ void __launch_bounds__(NT) kq_gram_lin(QueueList q) {
   queue_run(q, QK_GLIN, 1, [&](const ClassDev& c, int isl, int u) {
-    const int parts = gram_lin_parts(c.Kmax);
-    gram_lin_body<BG>(c, isl * c.nb + u / parts, u % parts);
+    const int ydim = gram_lin_ydim(c);
+    gram_lin_body<BG>(c, isl * c.nb + u / ydim, u % ydim);
+    return false;
+  });
+}
+
+__global__ void __launch_bounds__(NT) kq_gram_lin_reduce(QueueList q) {
+  queue_run(q, QK_GLINR, 1, [&](const ClassDev& c, int isl, int u) {
+    gram_lin_reduce_body(c, isl * c.nb + u);
     return false;
   });
 }
@@ -1896,11 +1941,17 @@ static unsigned queue_grid(F f, int threads, size_t smem, int sms, int cap, int 
   return (unsigned)std::max(1, std::min(per * sms, cap));
 }
 
-void launch_q_gram_lin(const QueueList& q, bool bg, size_t smem, int sms, cudaStream_t s) {
+void launch_q_gram_lin(const QueueList& q, bool bg, bool reduce, size_t smem, int sms,
+                       cudaStream_t s) {
   if (bg)
-    kq_gram_lin<true><<<queue_grid(kq_gram_lin<true>, NT, smem, sms, q.cap[QK_GLIN], q.per_cta), NT, smem, s>>>(q);
+    kq_gram_lin<true><<<queue_grid(kq_gram_lin<true>, NT, smem, sms, q.cap[QK_GLIN], q.per_cta),
+                        NT, smem, s>>>(q);
   else
-    kq_gram_lin<false><<<queue_grid(kq_gram_lin<false>, NT, smem, sms, q.cap[QK_GLIN], q.per_cta), NT, smem, s>>>(q);
+    kq_gram_lin<false><<<queue_grid(kq_gram_lin<false>, NT, smem, sms, q.cap[QK_GLIN],
+                                    q.per_cta), NT, smem, s>>>(q);
+  if (reduce)
+    kq_gram_lin_reduce<<<queue_grid(kq_gram_lin_reduce, NT, 0, sms, q.cap[QK_GLINR], q.per_cta),
+                         NT, 0, s>>>(q);
 }
 void launch_q_assemble(const QueueList& q, size_t smem, int sms, cudaStream_t s) {
   kq_assemble<<<queue_grid(kq_assemble, NT, smem, sms, q.cap[QK_ASSEMBLE], q.per_cta), NT, smem, s>>>(q);
@@ -1953,12 +2004,12 @@ size_t step_smem_bytes(int nLmax) {
 }
 
 void launch_gram_lin(const ClassDev& c, cudaStream_t s) {
-  const int parts = gram_lin_parts(c.Kmax);
-  dim3 grid((unsigned)(c.n_isl * c.nb), (unsigned)parts);
+  dim3 grid((unsigned)(c.n_isl * c.nb), (unsigned)gram_lin_ydim(c));
   if (c.nbg)
     k_gram_lin<true><<<grid, NT, gram_lin_smem_bytes(c.Kmax), s>>>(c);
   else
     k_gram_lin<false><<<grid, NT, gram_lin_smem_bytes(c.Kmax), s>>>(c);
+  if (c.gl_split > 1) k_gram_lin_reduce<<<(unsigned)(c.n_isl * c.nb), NT, 0, s>>>(c);
 }
 
 void launch_assemble(const ClassDev& c, cudaStream_t s) {

@@ -391,6 +391,9 @@ def estimate_device_bytes(fp: "FieldPlan", n_bands: int, H: int, W: int,
         nL = N * (6 if plan.kind == "mixed" else 2)
         K = nL + N + 1
         per = 4.0 * n_bands * (N * R * Sz * Sz + K * K + nL * nL + nL) + 8.0 * nL * nL
+        # partial FP32 Grams of large windows (the library's pixel split)
+        if K > 32 and B * B >= 4096:
+            per += min(8, B * B // 2048) * 4.0 * n_bands * K * K
         if precision == "mixed":
             per += 16 * 4.0 * n_bands * K * K
         total += per * n + 64 * 1024 * -(-n // max(per_chunk, 1))
