@@ -352,9 +352,8 @@ int uph_job_kernel_exps(const uph_job* job, int32_t kind, double* exps);
  * kernels above (independent dependency chains over every SM, CUDA events,
  * best of three launches, about 10 ms in all): out[0] FP32 multiply-add
  * rate in TFLOP/s, out[1] exp2f evaluations in 10^12/s, out[2] FP64
- * multiply-add rate in TFLOP/s, out[3] the SM clock over the FP32 run in
- * MHz.  Allocates and frees a small device buffer.  No counterpart in the
- * reference. */
+ * multiply-add rate in TFLOP/s.  Allocates and frees a small device buffer.
+ * No counterpart in the reference. */
 int uph_measure_peaks(uph_ctx* ctx, double* out);
 /* Device time from the start of the last uph_job_solve to the end of one
  * chunk's work (its LM iterations, probes and final pass), in ms. */

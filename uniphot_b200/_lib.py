@@ -220,10 +220,9 @@ class Context:
     def measure_peaks(self) -> dict:
         """FP32 / FP64 multiply-add and exp2f rates of this device
         (uph_measure_peaks)."""
-        out = (C.c_double * 4)()
+        out = (C.c_double * 3)()
         self.check(lib().uph_measure_peaks(self._h, out), "uph_measure_peaks")
-        return {"fp32_tflops": out[0], "exp2_tera_per_s": out[1], "fp64_tflops": out[2],
-                "sm_mhz": out[3]}
+        return {"fp32_tflops": out[0], "exp2_tera_per_s": out[1], "fp64_tflops": out[2]}
 
     def set_island_retry_limit(self, tries: int):
         """Unite attempts per coupled pair in island_roots before it gives up

@@ -687,7 +687,7 @@ int gram_tc_splits(int n_isl, int nb, int B, int sm_count);
 int uph_kernel_setup();
 
 // Compute-pipe peak kernels (uph_peaks.cu): FP32 and FP64 multiply-add and
-// exp2f rates and the SM clock into out[0..3]; returns a cudaError_t.
+// exp2f rates into out[0..2]; returns a cudaError_t.
 int measure_peaks(cudaStream_t s, int sms, double* out);
 
 // ---- Job-wide work queues of the LM loop -----------------------------------
@@ -744,7 +744,7 @@ __host__ __device__ __forceinline__ int gram_lin_splits(int B, int Kmax) {
 __host__ __device__ __forceinline__ int queue_units(const ClassDev& c, int kind) {
   const bool tc = c.tc_min_rows < (1 << 30);
   switch (kind) {
-    case QK_SETUP: return c.nb * c.N;
+    case QK_SETUP: return (c.nb * c.N + 3) / 4;   // four member records per CTA
     case QK_RENDER: return c.nb * c.N * c.ntile_side * c.ntile_side;
     case QK_GLIN: return c.nb * gram_lin_ydim(c);
     case QK_GLINR: return c.gl_split > 1 ? c.nb : 0;

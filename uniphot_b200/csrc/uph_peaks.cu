@@ -4,8 +4,6 @@
 //   out[0]  FP32 multiply-add rate, TFLOP/s (2 flops per FMA)
 //   out[1]  exp2f rate, 10^12 evaluations/s (the render's exponential)
 //   out[2]  FP64 multiply-add rate, TFLOP/s
-//   out[3]  SM clock during the FP32 run, MHz (one CTA's clock64 span over
-//           the launch's event time; every CTA is resident for the whole run)
 // Each kernel runs independent dependency chains in every thread of a grid
 // of 8 CTAs of 256 threads per SM, a few ms per launch so that launch
 // overhead is negligible; the best of three timed launches after a warm-up
@@ -21,9 +19,7 @@ namespace {
 constexpr int PK_THREADS = 256;
 constexpr int PK_CHAINS = 8;
 
-__global__ void __launch_bounds__(PK_THREADS) k_peak_fma(int iters, float* out,
-                                                         long long* cycles) {
-  const long long t0 = clock64();
+__global__ void __launch_bounds__(PK_THREADS) k_peak_fma(int iters, float* out) {
   float a[PK_CHAINS];
 #pragma unroll
   for (int j = 0; j < PK_CHAINS; ++j) a[j] = 1.0f + 1e-3f * (threadIdx.x + j);
@@ -38,7 +34,6 @@ __global__ void __launch_bounds__(PK_THREADS) k_peak_fma(int iters, float* out,
 #pragma unroll
   for (int j = 0; j < PK_CHAINS; ++j) s += a[j];
   if (s == -1.0f) out[blockIdx.x * blockDim.x + threadIdx.x] = s;   // never true
-  if (threadIdx.x == 0 && blockIdx.x == 0) *cycles = clock64() - t0;
 }
 
 __global__ void __launch_bounds__(PK_THREADS) k_peak_exp2(int iters, float* out) {
@@ -96,23 +91,15 @@ int measure_peaks(cudaStream_t s, int sms, double* out) {
   const int blocks = sms * 8;
   const size_t threads = (size_t)blocks * PK_THREADS;
   void* sink = nullptr;
-  long long* cyc = nullptr;
   cudaError_t err = cudaMalloc(&sink, threads * sizeof(double));
   if (err != cudaSuccess) return (int)err;
-  err = cudaMalloc((void**)&cyc, sizeof(long long));
-  if (err != cudaSuccess) {
-    cudaFree(sink);
-    return (int)err;
-  }
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
   const int it_fma = 4096, it_exp = 2048, it_dfma = 1024;
   const float ms_fma = best_ms([&] {
-    k_peak_fma<<<blocks, PK_THREADS, 0, s>>>(it_fma, (float*)sink, cyc);
+    k_peak_fma<<<blocks, PK_THREADS, 0, s>>>(it_fma, (float*)sink);
   }, e0, e1, s);
-  long long cycles = 0;
-  cudaMemcpy(&cycles, cyc, sizeof cycles, cudaMemcpyDeviceToHost);
   const float ms_exp = best_ms([&] {
     k_peak_exp2<<<blocks, PK_THREADS, 0, s>>>(it_exp, (float*)sink);
   }, e0, e1, s);
@@ -123,12 +110,10 @@ int measure_peaks(cudaStream_t s, int sms, double* out) {
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   cudaFree(sink);
-  cudaFree(cyc);
   if (err != cudaSuccess) return (int)err;
   const double n = (double)threads * PK_CHAINS;
   out[0] = 2.0 * n * it_fma * 16 / (ms_fma * 1e-3) / 1e12;
   out[1] = n * it_exp * 4 / (ms_exp * 1e-3) / 1e12;
   out[2] = 2.0 * n * it_dfma * 4 / (ms_dfma * 1e-3) / 1e12;
-  out[3] = (double)cycles / (ms_fma * 1e-3) / 1e6;
   return 0;
 }

@@ -164,23 +164,21 @@ __device__ void psf_component(const ClassDev& c, int b, double X, double Y,
 // (reference mode) or the combined Gaussian components (analytic mode),
 // written once to the member record that every render tile of the member
 // reads.
-__device__ __forceinline__ void member_setup_body(const ClassDev& c,
+__device__ __forceinline__ void member_setup_warp(const ClassDev& c,
                                                   const float* __restrict__ P, int phase,
-                                                  int bx) {
-  __shared__ SetupScratch sc;
-  __shared__ int is_gal;
-  __shared__ int ncomp;
+                                                  int bx, SetupScratch& sc, int& is_gal,
+                                                  int& ncomp) {
   const int k = bx % c.N;
   const int b = (bx / c.N) % c.nb;
   const int isl = bx / (c.N * c.nb);
   if (isl >= c.n_isl) return;
   if (!isl_active(c.flags[isl], phase)) return;
   if (!c.mmask[isl * c.N + k]) return;
-  const int tid = threadIdx.x;
+  const int lane = threadIdx.x & 31;
   MemberRecord* rec = c.mrec + ((size_t)isl * c.nb + b) * c.N + k;
   const float px = P[(size_t)isl * c.nP + 6 * k];
   const float py = P[(size_t)isl * c.nP + 6 * k + 1];
-  if (tid == 0) {
+  if (lane == 0) {
     is_gal = c.has_gal && c.stype[isl * c.N + k] != 0;
     for (int a = 0; a < 3; ++a) {
       rec->cg[a] = 0.f;
@@ -203,14 +201,14 @@ __device__ __forceinline__ void member_setup_body(const ClassDev& c,
       sersic_segment(c.tb_knots, c.tb_n, c.tb_nmin, c.tb_nmax, n, &sc.seg, &sc.t, &sc.dt);
       cov_terms((double)pk[2], (double)pk[3], (double)pk[4], rec->cg, rec->dcov);
     }
-  } else if (tid == 32) {
+  } else if (lane == 1) {
     const float gx = __fsub_rn(px, c.x0b[isl]);
     lanczos_taps((double)__fsub_rn(gx, rintf(gx)), rec->Lx, rec->dLx);
-  } else if (tid == 64) {
+  } else if (lane == 2) {
     const float gy = __fsub_rn(py, c.y0b[isl]);
     lanczos_taps((double)__fsub_rn(gy, rintf(gy)), rec->Ly, rec->dLy);
-  } else if (tid >= 96 && tid < 96 + UPH_MAXNT && c.mode == 0) {
-    const int tt = tid - 96;
+  } else if (lane >= 11 && lane < 11 + UPH_MAXNT && c.mode == 0) {
+    const int tt = lane - 11;
     if (tt < c.nt) {
       const float* os = c.psf_os + 4 * b;
       const float X = __fdiv_rn(__fsub_rn(px, os[0]), os[1]);
@@ -228,8 +226,8 @@ __device__ __forceinline__ void member_setup_body(const ClassDev& c,
       rec->betax[tt] = m > 0 ? (float)m * xm1 * yn * ix : 0.f;
       rec->betay[tt] = n > 0 ? (float)n * xm * yn1 * iy : 0.f;
     }
-  } else if (tid >= 96 && tid < 96 + UPH_MAXKPSF && c.mode == 1) {
-    const int q = tid - 96;
+  } else if (lane >= 3 && lane < 3 + UPH_MAXKPSF && c.mode == 1) {
+    const int q = lane - 3;
     if (q < c.kpsf) {
       const float* os = c.psf_os + 4 * b;
       const double X = ((double)px - os[0]) / os[1];
@@ -237,12 +235,12 @@ __device__ __forceinline__ void member_setup_body(const ClassDev& c,
       psf_component(c, b, X, Y, 1.0 / os[1], 1.0 / os[3], q, sc.pq[q]);
     }
   }
-  __syncthreads();
+  __syncwarp();
   if (c.mode != 1) {
     // reference mode: the galaxy's Sersic mixture for the Fourier-domain
     // convolution (sersic_mog.py:81-100), core apart
     if (!is_gal) return;
-    const int g = tid;
+    const int g = lane;
     if (g < c.tb_k) {
       const int seg = sc.seg;
       const double t = sc.t, dt = sc.dt;
@@ -261,7 +259,7 @@ __device__ __forceinline__ void member_setup_body(const ClassDev& c,
     }
     return;
   }
-  if (tid == 0) {
+  if (lane == 0) {
     double W = 0, Wx = 0, Wy = 0;
     for (int q = 0; q < c.kpsf; ++q) {
       W += sc.pq[q].w;
@@ -271,8 +269,8 @@ __device__ __forceinline__ void member_setup_body(const ClassDev& c,
     sc.W = W;
     sc.Wx = Wx;
     sc.Wy = Wy;
-  } else if (tid >= 32 && tid < 32 + UPH_MAXGAL && is_gal) {
-    const int g = tid - 32;
+  } else if (lane >= 16 && lane < 16 + UPH_MAXGAL && is_gal) {
+    const int g = lane - 16;
     const int seg = sc.seg;
     const double t = sc.t, dt = sc.dt;
     GalComp& o = sc.gg[g];
@@ -290,8 +288,8 @@ __device__ __forceinline__ void member_setup_body(const ClassDev& c,
       o.dv = 0.0;
     }
   }
-  __syncthreads();
-  if (tid == 0) {
+  __syncwarp();
+  if (lane == 0) {
     // compact the galaxy components that contribute (non-zero amplitude or
     // amplitude derivative); a star is a single unit delta
     int ng = 0;
@@ -309,9 +307,9 @@ __device__ __forceinline__ void member_setup_body(const ClassDev& c,
     ncomp = c.kpsf * ng;
     rec->ncomp = ncomp;
   }
-  __syncthreads();
+  __syncwarp();
   const float* cg = rec->cg;
-  for (int e = tid; e < ncomp; e += blockDim.x) {
+  for (int e = lane; e < ncomp; e += 32) {
     const int q = e / sc.ng, g = e - (e / sc.ng) * sc.ng;
     const PsfComp& pq = sc.pq[q];
     const GalComp& gq = sc.gg[g];
@@ -348,9 +346,24 @@ __device__ __forceinline__ void member_setup_body(const ClassDev& c,
   }
 }
 
-__global__ void __launch_bounds__(128)
+// One warp per member record, four records per CTA (warp-level syncs only:
+// the warps of a CTA are independent).
+constexpr int SETUP_WARPS = 4;
+
+__device__ __forceinline__ void member_setup_body(const ClassDev& c,
+                                                  const float* __restrict__ P, int phase,
+                                                  int rec0, int nrec) {
+  __shared__ SetupScratch sc[SETUP_WARPS];
+  __shared__ int is_gal[SETUP_WARPS], ncomp[SETUP_WARPS];
+  const int w = threadIdx.x >> 5;
+  if (w < nrec) member_setup_warp(c, P, phase, rec0 + w, sc[w], is_gal[w], ncomp[w]);
+}
+
+__global__ void __launch_bounds__(32 * SETUP_WARPS)
 k_member_setup(ClassDev c, const float* __restrict__ P, int phase) {
-  member_setup_body(c, P, phase, blockIdx.x);
+  const long long nrec = (long long)c.n_isl * c.nb * c.N;
+  const long long r0 = (long long)blockIdx.x * SETUP_WARPS;
+  member_setup_body(c, P, phase, (int)r0, (int)std::min<long long>(SETUP_WARPS, nrec - r0));
 }
 
 template <bool LIN>
@@ -716,7 +729,10 @@ k_render(ClassDev c, const float* __restrict__ P, int phase) {
 // active island of the job (P = the chunk's p, or p_try for the trial point).
 __global__ void __launch_bounds__(128) kq_member_setup(QueueList q, int phase, int p_try) {
   queue_run(q, QK_SETUP, 8, [&](const ClassDev& c, int isl, int u) {
-    member_setup_body(c, p_try ? c.p_try : c.p, phase, isl * c.nb * c.N + u);
+    // unit u: the island's records 4u .. 4u + 3
+    const int nr = c.nb * c.N;
+    member_setup_body(c, p_try ? c.p_try : c.p, phase, isl * nr + SETUP_WARPS * u,
+                      min(SETUP_WARPS, nr - SETUP_WARPS * u));
     return false;
   });
 }
@@ -784,7 +800,9 @@ void launch_render(const ClassDev& c, const float* P, int phase,
   if (nblk <= 0) return;
   const int nsa = render_arrays(c, phase);
   const size_t bytes = sizeof(float) * (size_t)nsa * UPH_HALO * HP;
-  k_member_setup<<<(unsigned)((long long)c.n_isl * c.nb * c.N), 128, 0, s>>>(c, P, phase);
+  const long long nrec = (long long)c.n_isl * c.nb * c.N;
+  k_member_setup<<<(unsigned)((nrec + SETUP_WARPS - 1) / SETUP_WARPS), 32 * SETUP_WARPS, 0, s>>>(
+      c, P, phase);
   if (c.mode == 0 && c.gstamp) launch_gal_fft(c, P, phase, s);
   if (phase == PH_LIN)
     k_render<true><<<(unsigned)nblk, 256, bytes, s>>>(c, P, phase);
