@@ -34,7 +34,8 @@ GPU box.  ``--batched``, ``--precision-stress``, ``--reference-render`` and
 
 Multi-GPU (torchrun): weak scaling, every rank solves its own seeded field
 (islands are independent: no collective on the data path); time = max over
-ranks.
+ranks.  ``--split-field``: strong scaling, the ranks split one field's
+islands by longest processing time (``shard.shard_plan``).
 """
 
 from __future__ import annotations
@@ -654,6 +655,9 @@ def main():
     ap.add_argument("--precision-stress", action="store_true",
                     help="run only the precision-stress measurement (crowded "
                          "blends, 40 bands) and print its JSON line")
+    ap.add_argument("--split-field", action="store_true",
+                    help="multi-GPU strong scaling: every rank takes its share of one "
+                         "field's islands (default: weak scaling, a field per rank)")
     ap.add_argument("--batched", action="store_true",
                     help="run only the batched configuration (about --batched-islands "
                          "islands over fields of 5, 20 and 40 bands) and print its JSON line")
@@ -702,12 +706,24 @@ def main():
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))
     from uniphot_b200.solver import IslandFitJob, island_fit
     from uniphot_b200.synth import make_production_field
-    field = make_production_field(args.seed + 7919 * rank, device="cuda",
-                                  side=args.side, n_src=args.n_src)
+    # weak scaling: every rank its own seeded field; --split-field (strong
+    # scaling): every rank the same field, its islands partitioned over the
+    # ranks by longest processing time (shard.shard_plan), no collective on
+    # the data path
+    field = make_production_field(args.seed + (0 if args.split_field else 7919 * rank),
+                                  device="cuda", side=args.side, n_src=args.n_src)
     kw = field.fit_kwargs("analytic")
     kw["precision"] = args.precision
-    job = IslandFitJob(**kw, device=local)
+    plan_kw = {}
+    if args.split_field:
+        from uniphot_b200.shard import shard_plan
+        from uniphot_b200.solver import plan_field
+        fp_all = plan_field(**kw)
+        plan_kw = {"plan": shard_plan(fp_all, world, rank)}
+    job = IslandFitJob(**kw, **plan_kw, device=local)
     n_isl = job.n_islands
+    tot_isl = (sum(p.n_islands for p, _ in fp_all.classes) if args.split_field
+               else world * n_isl)
     stream = torch.cuda.ExternalStream(job.field.ctx.stream_ptr())
     if args.profile_run:
         if args.only_class:
@@ -734,19 +750,20 @@ def main():
         job.solve()
     with ClockSampler(local) as clk:
         ms, launches = _timed_solves(job, args.steps, stream, barrier, dist)
-    value = world * n_isl * args.steps / (ms / 1e3)
+    value = tot_isl * args.steps / (ms / 1e3)
     # the other Gram form on the same resident field
     other = "plain" if args.precision == "mixed" else "mixed"
-    job_o = IslandFitJob(**dict(kw, precision=other), device=local, field=job.field)
+    job_o = IslandFitJob(**dict(kw, precision=other), **plan_kw, device=local,
+                         field=job.field)
     tuning[other] = job_o.autotune()
     for _ in range(args.warmup):
         job_o.solve()
     ms_o, _ = _timed_solves(job_o, args.steps, stream, barrier, dist)
-    value_o = world * n_isl * args.steps / (ms_o / 1e3)
+    value_o = tot_isl * args.steps / (ms_o / 1e3)
     # the production post-convergence set (parameter covariance and source
     # metrics) on top of the same solve
-    job_p = IslandFitJob(**kw, device=local, field=job.field, compute_param_errors=True,
-                         compute_source_metrics=True)
+    job_p = IslandFitJob(**kw, **plan_kw, device=local, field=job.field,
+                         compute_param_errors=True, compute_source_metrics=True)
     for _ in range(args.warmup):
         job_p.solve()
     ms_p, _ = _timed_solves(job_p, args.steps, stream, barrier, dist)
@@ -759,10 +776,20 @@ def main():
     for _ in range(args.e2e_steps):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        island_fit(**kw, device=local)
+        if args.split_field:
+            # the rank's share through the job API (planning, upload, solve,
+            # read-back, unpack), from the field's host arrays
+            part = IslandFitJob(**kw, **plan_kw, device=local)
+            part.solve()
+            part.result()
+            part.close()
+        else:
+            island_fit(**kw, device=local)
         torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
         e2e_t.append(time.perf_counter() - t0)
-    e2e_v = world * n_isl / float(np.median(e2e_t))
+    e2e_v = tot_isl / float(np.median(e2e_t))
     nb, H, W = field.data_minus_bg.shape
     PAD = job.PAD
     h2d = 2 * 4 * nb * (H + 2 * PAD) * (W + 2 * PAD)
@@ -816,9 +843,13 @@ def main():
         "metric": METRIC, "value": value, "unit": "islands/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": dtypes[args.precision],
+        "scaling": "strong" if args.split_field else "weak", "vs_baseline": None,
+        "dtype": dtypes[args.precision],
         "data": "synthetic (seeded production field; per-rank seed)",
-        "config": _config(n_isl, world),
+        "config": dict(_config(tot_isl if args.split_field else n_isl, world),
+                       parallelism=(f"dp{world} (one field's islands split over the ranks "
+                                    f"by longest processing time)" if args.split_field
+                                    else f"dp{world} (island partition by field)")),
         "form": forms[args.precision],
         "forms": {args.precision: {"value_all_islands": value,
                                    "ms_per_step": ms / args.steps, "kernels": ktab},
@@ -826,7 +857,7 @@ def main():
                           "kernels": ktab_o, "form": forms[other], "dtype": dtypes[other]}},
         "post_convergence": {
             "options": ["compute_param_errors", "compute_source_metrics"],
-            "value": world * n_isl * args.steps / (ms_p / 1e3), "unit": "islands/s",
+            "value": tot_isl * args.steps / (ms_p / 1e3), "unit": "islands/s",
             "ms_per_step": ms_p / args.steps},
         "e2e": {"value": e2e_v, "unit": "islands/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},

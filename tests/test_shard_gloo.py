@@ -74,3 +74,33 @@ def test_gloo_two_ranks_cover_field(world):
     assert merged["src"].size == n_src
     assert np.unique(merged["src"]).size == n_src
     assert np.all(np.diff(merged["src"]) > 0)
+
+
+def test_shard_plan_slices_plans_and_host_arrays_consistently():
+    """Every rank's share of a planned field: the class plans and host
+    arrays sliced to the same rows, every fitted island on exactly one rank,
+    the giants on rank 0 only."""
+    from uniphot_b200.shard import shard_plan
+    from uniphot_b200.solver import plan_field
+    from uniphot_b200.synth import make_production_field
+    f = make_production_field(1, side=320, n_bands=2, n_src=40, margin=40)
+    fp = plan_field(**f.fit_kwargs("analytic"))
+    full = {(p.key, int(i)) for p, _ in fp.classes for i in p.isl_ids}
+    index = {(p.key, int(i)): (p, h, r) for p, h in fp.classes
+             for r, i in enumerate(p.isl_ids)}
+    for world in (1, 2, 3):
+        seen = set()
+        for rank in range(world):
+            sp = shard_plan(fp, world, rank)
+            assert (len(sp.capped) > 0) == (rank == 0 and len(fp.capped) > 0)
+            for p, h in sp.classes:
+                assert p.n_islands > 0
+                for r, i in enumerate(p.isl_ids):
+                    key = (p.key, int(i))
+                    assert key not in seen
+                    seen.add(key)
+                    p0, h0, r0 = index[key]
+                    np.testing.assert_array_equal(p.midx[r], p0.midx[r0])
+                    np.testing.assert_array_equal(h["p0"][r], h0["p0"][r0])
+                    np.testing.assert_array_equal(h["ox"][r], h0["ox"][r0])
+        assert seen == full

@@ -52,3 +52,27 @@ def merge_rows(parts: list) -> dict:
     cat = {k: np.concatenate([p[k] for p in parts], axis=0) for k in keys}
     order = np.argsort(cat["src"], kind="stable")
     return {k: v[order] for k, v in cat.items()}
+
+
+def shard_plan(fp, world: int, rank: int):
+    """The rank's share of a planned field (``solver.plan_field``): per class,
+    the rows ``shard_islands`` assigns to the rank, with the class plan's
+    per-island arrays and the host arrays sliced to them (classes with no
+    rows on this rank dropped).  The giant islands (seed rows, no fit) go to
+    rank 0 alone, so the ranks' results together cover every source once.
+    ``IslandFitJob(plan=...)`` solves the share."""
+    import dataclasses
+    plans = [p for p, _ in fp.classes]
+    share = shard_islands(plans, world)[rank]
+    classes = []
+    for ci, rows in share:
+        p, h = fp.classes[ci]
+        n = p.n_islands
+        sp = dataclasses.replace(p, isl_ids=p.isl_ids[rows], midx=p.midx[rows],
+                                 mmask=p.mmask[rows], bbox=p.bbox[rows],
+                                 n_src_of=p.n_src_of[rows])
+        sh = {k: (v[rows] if isinstance(v, np.ndarray) and v.ndim >= 1 and v.shape[0] == n
+                  else v) for k, v in h.items()}
+        classes.append((sp, sh))
+    return dataclasses.replace(fp, classes=classes,
+                               capped=fp.capped if rank == 0 else type(fp.capped)())
