@@ -456,15 +456,50 @@ def _host_bytes_available() -> float:
     return avail
 
 
+def _plan_batches(fp, n_bands, H, W, precision, budget):
+    """Split a planned field into plans whose chunk buffers (the library's
+    own estimate, field stacks apart) fit ``budget`` bytes each, classes kept
+    whole where they fit and split by rows where one class alone does not."""
+    import dataclasses
+    from uniphot_b200.shard import slice_class
+    from uniphot_b200.solver import estimate_device_bytes
+    field = 8.0 * n_bands * (H + 2 * fp.PAD) * (W + 2 * fp.PAD)
+    batches, cur, used = [], [], 0.0
+    for p, h in fp.classes:
+        one = estimate_device_bytes(dataclasses.replace(fp, classes=[(p, h)]), n_bands, H, W,
+                                    precision=precision) - field
+        per = one / max(p.n_islands, 1)
+        rows = np.arange(p.n_islands)
+        while rows.size:
+            room = budget - used
+            take = int(min(rows.size, max(room // per, 0)))
+            if take == 0:
+                if cur:
+                    batches.append(cur)
+                    cur, used = [], 0.0
+                    continue
+                take = 1               # a single island larger than the budget
+            part = rows[:take]
+            rows = rows[take:]
+            cur.append((p, h) if part.size == p.n_islands else slice_class(p, h, part))
+            used += per * part.size
+    if cur:
+        batches.append(cur)
+    return [dataclasses.replace(fp, classes=b, capped=fp.capped if i == 0 else [])
+            for i, b in enumerate(batches)]
+
+
 def _batched_measure(args, device):
     """The batched configuration: about ``args.batched_islands`` islands spread
     over three production-style fields (generator of the production field at
     its source density, 60/20/12/8% STAR/EXP/DEV/SERSIC, clustered islands of
     1-64 members) with 5, 20 and 40 bands, a third of the islands each.
-    Every field is solved in both forms, the LM-loop engine picked by the
-    autotuner (per-chunk engine or work queue with 16 lanes); islands/s per
-    field and form, and per member-count class on the 20-band field (each
-    class group solved as its own job).  Islands above 32 members keep their
+    Every field is solved in both forms as a sequence of jobs whose chunk
+    buffers fit the device next to the field (the library's own estimate),
+    the LM-loop engine picked by the autotuner on the first job (per-chunk
+    engine or work queue with 16 lanes); islands/s per field and form (all
+    islands over the summed device time of the jobs), and per member-count
+    class on the 20-band field.  Islands above 32 members keep their
     seeds (giant rows, the reference's joint cap) and are counted apart."""
     import dataclasses
     import gc
@@ -478,6 +513,26 @@ def _batched_measure(args, device):
         job.solve()
         ms, _ = _timed_solves(job, steps, stream, torch.cuda.synchronize, None)
         return ms / steps
+
+    def solve_batches(kw, fp, prec, field, tune):
+        """Device ms of one pass over every batch (jobs of at most the chunk
+        budget each, solved one after the other on the resident field)."""
+        nb, H, W = np.shape(kw["data_minus_bg"])
+        budget = min(80e9, 150e9 - 8.0 * nb * (H + 2 * fp.PAD) * (W + 2 * fp.PAD))
+        total, tuning, nbatch = 0.0, None, 0
+        for sub in _plan_batches(fp, nb, H, W, prec, budget):
+            job = IslandFitJob(**dict(kw, precision=prec), device=device, plan=sub,
+                               field=field)
+            field = job.field
+            if tune and tuning is None:
+                tuning = job.autotune(candidates=(("chunks", 0), ("queue", 16)), repeats=1)
+            elif tuning is not None:
+                eng, lanes = tuning["picked"].split("/")
+                job.job.set_engine(eng, int(lanes))
+            total += timed(job, args.batched_steps)
+            nbatch += 1
+            job.close()
+        return total, tuning, nbatch, field
 
     out = {"target_islands": args.batched_islands, "fields": []}
     per_field = args.batched_islands / 3.0
@@ -502,27 +557,20 @@ def _batched_measure(args, device):
         row["giant_islands"] = int(len(fp.capped))
         field = None
         for prec in ("plain", "mixed"):
-            job = IslandFitJob(**dict(kw, precision=prec), device=device, plan=fp, field=field)
-            field = job.field
-            tun = job.autotune(candidates=(("chunks", 0), ("queue", 16)), repeats=1)
-            ms = timed(job, args.batched_steps)
+            ms, tun, nbatch, field = solve_batches(kw, fp, prec, field, True)
             row[prec] = {"islands_per_s": n_isl / (ms / 1e3), "ms_per_solve": ms,
-                         "autotune": tun}
-            job.close()
+                         "jobs": nbatch, "autotune": tun}
             if nb == 20:
                 groups = {}
                 for p, h in fp.classes:
                     groups.setdefault(int(p.nsrc_class), []).append((p, h))
                 per_class = {}
                 for nsrc, cl in sorted(groups.items()):
-                    sub = dataclasses.replace(fp, classes=cl)
-                    jb = IslandFitJob(**dict(kw, precision=prec), device=device, plan=sub,
-                                      field=field)
+                    sub = dataclasses.replace(fp, classes=cl, capped=[])
                     m = sum(p.n_islands for p, _ in cl)
-                    msc = timed(jb, args.batched_steps)
+                    msc, _, nbc, field = solve_batches(kw, sub, prec, field, False)
                     per_class[str(nsrc)] = {"islands": m, "islands_per_s": m / (msc / 1e3),
-                                            "ms_per_solve": msc}
-                    jb.close()
+                                            "ms_per_solve": msc, "jobs": nbc}
                 row[prec]["by_member_class"] = per_class
         out["fields"].append(row)
         del f, field, kw, fp

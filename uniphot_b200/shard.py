@@ -64,15 +64,20 @@ def shard_plan(fp, world: int, rank: int):
     import dataclasses
     plans = [p for p, _ in fp.classes]
     share = shard_islands(plans, world)[rank]
-    classes = []
-    for ci, rows in share:
-        p, h = fp.classes[ci]
-        n = p.n_islands
-        sp = dataclasses.replace(p, isl_ids=p.isl_ids[rows], midx=p.midx[rows],
-                                 mmask=p.mmask[rows], bbox=p.bbox[rows],
-                                 n_src_of=p.n_src_of[rows])
-        sh = {k: (v[rows] if isinstance(v, np.ndarray) and v.ndim >= 1 and v.shape[0] == n
-                  else v) for k, v in h.items()}
-        classes.append((sp, sh))
+    classes = [slice_class(*fp.classes[ci], rows) for ci, rows in share]
     return dataclasses.replace(fp, classes=classes,
                                capped=fp.capped if rank == 0 else type(fp.capped)())
+
+
+def slice_class(plan, host: dict, rows):
+    """(class plan, host arrays) restricted to the given island rows: the
+    plan's per-island arrays and every host array with one row per island."""
+    import dataclasses
+    rows = np.asarray(rows, np.int64)
+    n = plan.n_islands
+    sp = dataclasses.replace(plan, isl_ids=plan.isl_ids[rows], midx=plan.midx[rows],
+                             mmask=plan.mmask[rows], bbox=plan.bbox[rows],
+                             n_src_of=plan.n_src_of[rows])
+    sh = {k: (v[rows] if isinstance(v, np.ndarray) and v.ndim >= 1 and v.shape[0] == n
+              else v) for k, v in host.items()}
+    return sp, sh
