@@ -89,9 +89,10 @@ def test_dlnp_parity(small, mode, kinds):
     dlnp accepts a step when the float64 chi2 decreases; once steps are
     tiny the two sides' per-band float64 sums (different summation orders,
     ~1e-16 relative) can disagree on such a near-tie, as the reference's own
-    reductions can, so iteration counts and flags are required to agree on
-    90% of islands while fluxes and positions must meet the parity bar on
-    every island."""
+    reductions can.  Fluxes and positions must meet the parity bar on every
+    island; iteration counts and flags must agree on every island except
+    such near-ties, each reported with its final chi2 difference in float32
+    ulps and held to 1e-6 relative (on the B200: 1 island of 26)."""
     plans, hosts, PAD, ds, ws, psfs = field_classes(small, mode, kinds)
     g, _ = run_gpu(plans, hosts, PAD, ds, ws, psfs, mode, native=small.native,
                    convergence="dlnp")
@@ -102,8 +103,16 @@ def test_dlnp_parity(small, mode, kinds):
         r = compare(gg, oo, h["mmask"])
         msg = f"{p.key}: {r['max_rel']:.2e} {r['max_dpos']:.2e}"
         assert r["flux_ok"].all() and r["pos_ok"].all(), msg
-        same.append(r["same_nst"] & r["same_flags"])
-    assert np.concatenate(same).mean() >= 0.9
+        ok = r["same_nst"] & r["same_flags"]
+        for i in np.nonzero(~ok)[0]:
+            c32, c64 = np.float32(gg["chi2"][i]), float(oo["chi2"][i])
+            ulps = abs(float(c32) - c64) / float(np.spacing(c32))
+            print(f"{p.key} island {i}: steps {gg['nst'][i]} vs {oo['nst'][i]}, final chi2 "
+                  f"{float(c32):.9g} vs {c64:.9g} ({ulps:.1f} float32 ulps)")
+            assert abs(float(c32) - c64) <= 1e-6 * abs(c64), msg
+        same.append(ok)
+    same = np.concatenate(same)
+    assert same.mean() >= 0.9, same.mean()
 
 
 def test_dlnp_zero_weight_island_is_certified(small):
@@ -122,10 +131,10 @@ def test_dlnp_zero_weight_island_is_certified(small):
 @pytest.mark.parametrize("mode,kinds", [("analytic", ("star", "mixed"))])
 def test_trust_region_parity(small, mode, kinds):
     """step_mode="trust_region" (island_solver.py:1004-1116) on the mixed
-    classes, clip on the star classes.  The radius update branches on the
-    gain ratio of two float chi2 values, so a near-tie can send the two
-    sides down different radii: iteration counts and flags must agree on
-    90% of islands, fluxes and positions on every island."""
+    classes, clip on the star classes.  Iteration counts, flags and the
+    bound-pinned flag agree on every island (they did on all 38 on the
+    B200, although the radius update branches on the gain ratio of two
+    float chi2 values), fluxes and positions meet the parity bar."""
     plans, hosts, PAD, ds, ws, psfs = field_classes(small, mode, kinds)
     g, _ = run_gpu(plans, hosts, PAD, ds, ws, psfs, mode, native=small.native,
                    step_mode="trust_region")
@@ -145,7 +154,7 @@ def test_trust_region_parity(small, mode, kinds):
             assert not gg["railed"].any()
         else:
             assert np.all(gg["lam"][gg["nst"] > 0] > 0)   # a radius, never unset
-    assert n_same >= 0.9 * n_all, f"{n_same}/{n_all}"
+    assert n_same == n_all, f"{n_same}/{n_all}"
 
 
 def test_trust_region_radius_carries_across_requeue(small):
@@ -178,7 +187,8 @@ def test_trust_region_radius_carries_across_requeue(small):
 def test_trust_region_production_field_parity():
     """Reduced production field (512^2, 3 bands, 300 sources), classes of at
     most 2 members: galaxies with bounded log-radius and free Sersic n
-    exercise the bound-pinned disclosure."""
+    exercise the bound-pinned disclosure.  Iteration counts and flags agree
+    on every island (28 of 28 on the B200)."""
     from uniphot_b200.synth import make_production_field
     f = make_production_field(3, side=512, n_bands=3, n_src=300)
     plans, hosts, PAD, ds, ws, psfs = field_classes(f, "analytic", ("mixed",))
@@ -199,5 +209,5 @@ def test_trust_region_production_field_parity():
         n_all += same.size
         np.testing.assert_array_equal(gg["railed"][same], oo["railed"][same])
         n_railed += int(oo["railed"].sum())
-    assert n_same >= 0.9 * n_all, f"{n_same}/{n_all}"
+    assert n_same == n_all, f"{n_same}/{n_all}"
     assert n_railed > 0
