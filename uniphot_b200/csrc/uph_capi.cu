@@ -726,7 +726,7 @@ int add_chunk(uph_ctx* ctx, Chunk* ch, const uph_class_desc* cls,
   c.ngood = cbuf<int>(ctx, ch, "ngood", (size_t)n * nb, &rc);
   c.probe_best = cbuf<float>(ctx, ch, "pbest", n, &rc);
   c.probe_p = cbuf<float>(ctx, ch, "probep", (size_t)n * 4 * nP, &rc);
-  c.n_active = cbuf<int>(ctx, ch, "nact", 1, &rc);
+  c.n_active = cbuf<int>(ctx, ch, "nact", 2, &rc);
   c.err = cbuf<int>(ctx, ch, "err", 1, &rc);
   c.gl_split = gram_lin_splits(B, Kmax);
   if (c.gl_split > 1)
@@ -921,7 +921,10 @@ int reset_chunk(uph_ctx* ctx, Chunk* ch, cudaStream_t s) {
   return UPH_OK;
 }
 
-void post_loop(Chunk* ch, Launcher& L) {
+// probes: whether the chunk may hold stalled islands (the diverged and
+// plateau probes act on stalled islands only, and the outputs of the others
+// do not read them: with none, their launches are skipped)
+void post_loop(Chunk* ch, Launcher& L, bool probes = true) {
   const ClassDev& c = ch->c;
   cudaStream_t s = L.s;
   launch_set_probe(c, s);
@@ -929,7 +932,7 @@ void post_loop(Chunk* ch, Launcher& L) {
     // "changed" mode reports the loop's own diverged flag; no post-hoc probe
     cudaMemcpyAsync(ch->d_div, c.div_live, c.n_isl, cudaMemcpyDeviceToDevice, s);
     L.job->ctx->launches += 1;
-  } else {
+  } else if (probes) {
     for (int j = 0; j < 4; ++j) L(3, [&] { launch_step(c, PH_PROBE, j, 0.f, 1, s); });
     launch_diverged_compare(c, ch->d_div, s);
     L.job->ctx->launches += 2;
@@ -956,14 +959,16 @@ void post_loop(Chunk* ch, Launcher& L) {
     launch_errors_end(c, s);
     L.job->ctx->launches += 2;
   }
-  launch_fill_float(c.probe_best, INFINITY, c.n_isl, s);
-  L.job->ctx->launches += 1;
-  for (int e = -9; e <= 6; ++e) {
-    const float lamj = (float)std::pow(10.0, (double)e);
-    L(3, [&] { launch_step(c, PH_PROBE, 0, lamj, 2, s); });
-    L(0, [&] { launch_render(c, c.p_try, PH_PROBE, s); }, 2);
-    L(4, [&] { launch_gram_trial(c, c.p_try, PH_PROBE, 0, nullptr, nullptr, s); });
-    L(5, [&] { launch_accept(c, PH_PROBE, s); });
+  if (probes) {
+    launch_fill_float(c.probe_best, INFINITY, c.n_isl, s);
+    L.job->ctx->launches += 1;
+    for (int e = -9; e <= 6; ++e) {
+      const float lamj = (float)std::pow(10.0, (double)e);
+      L(3, [&] { launch_step(c, PH_PROBE, 0, lamj, 2, s); });
+      L(0, [&] { launch_render(c, c.p_try, PH_PROBE, s); }, 2);
+      L(4, [&] { launch_gram_trial(c, c.p_try, PH_PROBE, 0, nullptr, nullptr, s); });
+      L(5, [&] { launch_accept(c, PH_PROBE, s); });
+    }
   }
   if (c.reprof) {
     // Re profile: one trial pass per (member slot, offset) on the islands
@@ -1076,11 +1081,12 @@ int job_solve(uph_job* job, int max_steps) {
       load[j] += cost[i];
     }
   }
-  if (job->h_active_cap < nch) {
+  if (job->h_active_cap < 2 * nch) {
     if (job->h_active) cudaFreeHost(job->h_active);
-    CK(cudaMallocHost((void**)&job->h_active, sizeof(int) * nch), "pinned");
-    job->h_active_cap = nch;
+    CK(cudaMallocHost((void**)&job->h_active, sizeof(int) * 2 * nch), "pinned");
+    job->h_active_cap = 2 * nch;
   }
+  std::vector<char> counted(nch, 0);
   std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> rec;
   auto* recp = job->profile ? &rec : nullptr;
   if (job->profile) {
@@ -1150,8 +1156,9 @@ int job_solve(uph_job* job, int max_steps) {
     ch->iters += group;
     launch_count_active(ch->c, s);
     ctx->launches += 1;
-    CK(cudaMemcpyAsync(job->h_active + i, ch->c.n_active, sizeof(int),
+    CK(cudaMemcpyAsync(job->h_active + 2 * i, ch->c.n_active, 2 * sizeof(int),
                        cudaMemcpyDeviceToHost, s), "count");
+    counted[i] = 1;
     CK(cudaEventRecord(ch->ev_group, s), "event");
     inflight[i] = 1;
     return UPH_OK;
@@ -1160,7 +1167,7 @@ int job_solve(uph_job* job, int max_steps) {
     Chunk* ch = job->chunks[i];
     ch->done = true;
     Launcher L{job, job->streams[ch->slot], recp};
-    post_loop(ch, L);
+    post_loop(ch, L, !counted[i] || job->h_active[2 * i + 1] > 0);
     cudaEventRecord(ch->ev_done, job->streams[ch->slot]);
   };
   int live = 0;
@@ -1183,7 +1190,7 @@ int job_solve(uph_job* job, int max_steps) {
       if (q != cudaSuccess) return cuda_err(ctx, q, "lm loop");
       inflight[i] = 0;
       progress = true;
-      if (job->h_active[i] == 0 || ch->iters >= max_steps) {
+      if (job->h_active[2 * i] == 0 || ch->iters >= max_steps) {
         finish(i);
         --live;
       } else {

@@ -1453,17 +1453,29 @@ __global__ void k_queue_count(const ClassDev* __restrict__ cls, const int2* __re
   if (threadIdx.x == 0) *out = red[0];
 }
 
+// Islands of the chunk still iterating into n_active[0], stalled islands
+// (the post-loop probes' subjects) into n_active[1].
 __global__ void k_count_active(ClassDev c) {
-  __shared__ int s[NT];
-  int t = 0;
-  for (int i = threadIdx.x; i < c.n_isl; i += NT) t += !(c.flags[i] & FL_CONV);
+  __shared__ int s[NT], z[NT];
+  int t = 0, u = 0;
+  for (int i = threadIdx.x; i < c.n_isl; i += NT) {
+    t += !(c.flags[i] & FL_CONV);
+    u += (c.flags[i] & FL_STALL) ? 1 : 0;
+  }
   s[threadIdx.x] = t;
+  z[threadIdx.x] = u;
   __syncthreads();
   for (int st = NT / 2; st > 0; st >>= 1) {
-    if (threadIdx.x < st) s[threadIdx.x] += s[threadIdx.x + st];
+    if (threadIdx.x < st) {
+      s[threadIdx.x] += s[threadIdx.x + st];
+      z[threadIdx.x] += z[threadIdx.x + st];
+    }
     __syncthreads();
   }
-  if (threadIdx.x == 0) *c.n_active = s[0];
+  if (threadIdx.x == 0) {
+    c.n_active[0] = s[0];
+    c.n_active[1] = z[0];
+  }
 }
 
 __global__ void k_diverged_compare(ClassDev c, uint8_t* out) {
