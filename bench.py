@@ -434,78 +434,27 @@ def _stress_measure(args, device):
     return out
 
 
-def _host_bytes_available() -> float:
-    """Host memory this process may still use: MemAvailable, capped by the
-    container's memory limit when one is set."""
-    avail = float("inf")
-    try:
-        for line in open("/proc/meminfo"):
-            if line.startswith("MemAvailable:"):
-                avail = float(line.split()[1]) * 1024
-    except OSError:
-        pass
-    for path in ("/sys/fs/cgroup/memory.max", "/sys/fs/cgroup/memory/memory.limit_in_bytes"):
-        try:
-            lim = open(path).read().strip()
-            used_p = path.replace("memory.max", "memory.current").replace(
-                "limit_in_bytes", "usage_in_bytes")
-            if lim != "max" and float(lim) < 1e18:
-                avail = min(avail, float(lim) - float(open(used_p).read().strip()))
-        except (OSError, ValueError):
-            pass
-    return avail
-
-
-def _plan_batches(fp, n_bands, H, W, precision, budget):
-    """Split a planned field into plans whose chunk buffers (the library's
-    own estimate, field stacks apart) fit ``budget`` bytes each, classes kept
-    whole where they fit and split by rows where one class alone does not."""
-    import dataclasses
-    from uniphot_b200.shard import slice_class
-    from uniphot_b200.solver import estimate_device_bytes
-    field = 8.0 * n_bands * (H + 2 * fp.PAD) * (W + 2 * fp.PAD)
-    batches, cur, used = [], [], 0.0
-    for p, h in fp.classes:
-        one = estimate_device_bytes(dataclasses.replace(fp, classes=[(p, h)]), n_bands, H, W,
-                                    precision=precision) - field
-        per = one / max(p.n_islands, 1)
-        rows = np.arange(p.n_islands)
-        while rows.size:
-            room = budget - used
-            take = int(min(rows.size, max(room // per, 0)))
-            if take == 0:
-                if cur:
-                    batches.append(cur)
-                    cur, used = [], 0.0
-                    continue
-                take = 1               # a single island larger than the budget
-            part = rows[:take]
-            rows = rows[take:]
-            cur.append((p, h) if part.size == p.n_islands else slice_class(p, h, part))
-            used += per * part.size
-    if cur:
-        batches.append(cur)
-    return [dataclasses.replace(fp, classes=b, capped=fp.capped if i == 0 else [])
-            for i, b in enumerate(batches)]
-
-
 def _batched_measure(args, device):
-    """The batched configuration: about ``args.batched_islands`` islands spread
-    over three production-style fields (generator of the production field at
-    its source density, 60/20/12/8% STAR/EXP/DEV/SERSIC, clustered islands of
-    1-64 members) with 5, 20 and 40 bands, a third of the islands each.
-    Every field is solved in both forms as a sequence of jobs whose chunk
-    buffers fit the device next to the field (the library's own estimate),
-    the LM-loop engine picked by the autotuner on the first job (per-chunk
-    engine or work queue with 16 lanes); islands/s per field and form (all
-    islands over the summed device time of the jobs), and per member-count
-    class on the 20-band field.  Islands above 32 members keep their
-    seeds (giant rows, the reference's joint cap) and are counted apart."""
+    """The batched configuration: ``args.batched_tiles`` distinct 2048^2
+    production-style tiles (the production field's generator at its source
+    density, 60/20/12/8% STAR/EXP/DEV/SERSIC, clustered islands of 1-64
+    members) for each band count 5, 20 and 40.  A band count's tiles are
+    packed into one job (every tile's chunks bound to its own field and PSF;
+    tiles beyond the device budget go to the next job), the LM-loop engine
+    picked by the autotuner on the first job (per-chunk engine or work queue
+    with 16 lanes).  The ``args.batched_islands`` island stream is that job
+    solved repeatedly: islands/s per band count and form is the job's
+    islands over its device time per solve, and the whole configuration's
+    islands/s weights the three band counts equally (a third of the stream
+    each).  Per member-count class on the first 20-band tile.  Islands above
+    32 members keep their seeds (giant rows, the reference's joint cap) and
+    are counted apart.  Host memory holds one band count's tiles at a
+    time."""
     import dataclasses
     import gc
-    import math
     import torch
-    from uniphot_b200.solver import IslandFitJob, plan_field
+    from uniphot_b200 import _lib
+    from uniphot_b200.solver import DeviceField, IslandFitJob, estimate_device_bytes, plan_field
     from uniphot_b200.synth import make_production_field
 
     def timed(job, steps):
@@ -514,53 +463,69 @@ def _batched_measure(args, device):
         ms, _ = _timed_solves(job, steps, stream, torch.cuda.synchronize, None)
         return ms / steps
 
-    def solve_batches(kw, fp, prec, field, tune):
-        """Device ms of one pass over every batch (jobs of at most the chunk
-        budget each, solved one after the other on the resident field)."""
-        nb, H, W = np.shape(kw["data_minus_bg"])
-        budget = min(80e9, 150e9 - 8.0 * nb * (H + 2 * fp.PAD) * (W + 2 * fp.PAD))
-        total, tuning, nbatch = 0.0, None, 0
-        for sub in _plan_batches(fp, nb, H, W, prec, budget):
-            job = IslandFitJob(**dict(kw, precision=prec), device=device, plan=sub,
-                               field=field)
-            field = job.field
-            if tune and tuning is None:
-                tuning = job.autotune(candidates=(("chunks", 0), ("queue", 16)), repeats=1)
+    def solve_packed(tiles, prec, tune_first, tuning):
+        """Device ms of one pass over the tiles, packed into jobs under the
+        device budget; the engine picked on the first job."""
+        budget, total, njobs, groups, cur, used = 120e9, 0.0, 0, [], [], 0.0
+        for kw, fp in tiles:
+            nb, H, W = np.shape(kw["data_minus_bg"])
+            need = estimate_device_bytes(fp, nb, H, W, precision=prec)
+            if cur and used + need > budget:
+                groups.append(cur)
+                cur, used = [], 0.0
+            cur.append((kw, fp))
+            used += need
+        groups.append(cur)
+        for grp in groups:
+            ctx = _lib.Context(device)
+            job = _lib.Job(ctx)
+            fits = []
+            for kw, fp in grp:
+                fld = DeviceField.from_unpadded(kw["data_minus_bg"], kw["invvar"], fp.PAD,
+                                                device=device, context=ctx)
+                fits.append(IslandFitJob(**dict(kw, precision=prec), device=device,
+                                         field=fld, plan=fp, job=job))
+            if tune_first and tuning is None:
+                tuning = fits[-1].autotune(candidates=(("chunks", 0), ("queue", 16)),
+                                           repeats=1)
             elif tuning is not None:
                 eng, lanes = tuning["picked"].split("/")
-                job.job.set_engine(eng, int(lanes))
-            total += timed(job, args.batched_steps)
-            nbatch += 1
+                job.set_engine(eng, int(lanes))
+            total += timed(fits[-1], args.batched_steps)
+            njobs += 1
             job.close()
-        return total, tuning, nbatch, field
+            ctx.close()
+        return total, tuning, njobs
 
-    out = {"target_islands": args.batched_islands, "fields": []}
-    per_field = args.batched_islands / 3.0
+    def solve_alone(kw, fp, prec):
+        job = IslandFitJob(**dict(kw, precision=prec), device=device, plan=fp)
+        ms = timed(job, args.batched_steps)
+        job.close()
+        job.field.ctx.close()
+        return ms
+
+    out = {"target_islands": args.batched_islands, "tiles_per_band_count": args.batched_tiles,
+           "band_counts": [5, 20, 40], "fields": []}
+    tuning = {"plain": None, "mixed": None}
     for k, nb in enumerate((5, 20, 40)):
-        # the production field: 5000 sources give 1134 fitted islands on 2048^2
-        n_src = int(round(per_field * 5000 / 1134))
-        # host arrays: data and weights (float32), twice over for padding and
-        # generation; keep a third of what is available free
-        need = 4.0 * 4 * nb * (2048.0 ** 2) * n_src / 5000
-        scale = min(1.0, _host_bytes_available() / (1.5 * need))
-        n_src = int(n_src * scale)
-        side = int(round(2048 * math.sqrt(n_src / 5000)))
         t0 = time.perf_counter()
-        f = make_production_field(args.seed + 101 * k, side=side, n_bands=nb, n_src=n_src,
-                                  device="cuda")
-        row = {"n_bands": nb, "side": side, "n_src": n_src, "host_memory_scale": scale,
-               "generation_s": time.perf_counter() - t0}
-        kw = f.fit_kwargs("analytic")
-        fp = plan_field(**kw)
-        n_isl = sum(p.n_islands for p, _ in fp.classes)
-        row["n_islands"] = n_isl
-        row["giant_islands"] = int(len(fp.capped))
-        field = None
+        tiles = []
+        for t in range(args.batched_tiles):
+            f = make_production_field(args.seed + 101 * k + 7 * t, side=2048, n_bands=nb,
+                                      n_src=5000, device="cuda")
+            kw = f.fit_kwargs("analytic")
+            tiles.append((kw, plan_field(**kw)))
+            del f
+        row = {"n_bands": nb, "tiles": len(tiles), "side": 2048, "n_src_per_tile": 5000,
+               "generation_s": time.perf_counter() - t0,
+               "n_islands": sum(sum(p.n_islands for p, _ in fp.classes) for _, fp in tiles),
+               "giant_islands": sum(int(len(fp.capped)) for _, fp in tiles)}
         for prec in ("plain", "mixed"):
-            ms, tun, nbatch, field = solve_batches(kw, fp, prec, field, True)
-            row[prec] = {"islands_per_s": n_isl / (ms / 1e3), "ms_per_solve": ms,
-                         "jobs": nbatch, "autotune": tun}
+            ms, tuning[prec], njobs = solve_packed(tiles, prec, True, tuning[prec])
+            row[prec] = {"islands_per_s": row["n_islands"] / (ms / 1e3), "ms_per_solve": ms,
+                         "jobs": njobs, "autotune": tuning[prec]}
             if nb == 20:
+                kw, fp = tiles[0]
                 groups = {}
                 for p, h in fp.classes:
                     groups.setdefault(int(p.nsrc_class), []).append((p, h))
@@ -568,27 +533,30 @@ def _batched_measure(args, device):
                 for nsrc, cl in sorted(groups.items()):
                     sub = dataclasses.replace(fp, classes=cl, capped=[])
                     m = sum(p.n_islands for p, _ in cl)
-                    msc, _, nbc, field = solve_batches(kw, sub, prec, field, False)
+                    msc = solve_alone(kw, sub, prec)
                     per_class[str(nsrc)] = {"islands": m, "islands_per_s": m / (msc / 1e3),
-                                            "ms_per_solve": msc, "jobs": nbc}
-                row[prec]["by_member_class"] = per_class
+                                            "ms_per_solve": msc}
+                row[prec]["by_member_class_first_tile"] = per_class
         out["fields"].append(row)
-        del f, field, kw, fp
+        del tiles
         gc.collect()
         torch.cuda.empty_cache()
     for prec in ("plain", "mixed"):
-        isl = sum(r["n_islands"] for r in out["fields"])
-        t = sum(r[prec]["ms_per_solve"] for r in out["fields"]) / 1e3
-        out[prec + "_islands_per_s"] = isl / t
-    out["n_islands"] = sum(r["n_islands"] for r in out["fields"])
+        # a third of the island stream per band count: harmonic weighting
+        per_isl_s = sum(1.0 / r[prec]["islands_per_s"] for r in out["fields"]) / 3.0
+        out[prec + "_islands_per_s"] = 1.0 / per_isl_s
+        out[prec + "_stream_seconds"] = args.batched_islands * per_isl_s
+    out["n_islands_distinct"] = sum(r["n_islands"] for r in out["fields"])
     return out
 
 
 def _serve_measure(args, rates, device):
     """Serving: the same seeded request pool streamed with Poisson arrivals
-    through the batched+mixed server and through one plain FP32 worker (one
-    request at a time)."""
-    from uniphot_b200.serve import Server, latency_summary, poisson_stream
+    through the packing server (admitted requests solved as one job through
+    the work-queue engine, mixed precision), through the batched+mixed
+    server (worker contexts overlapping on the device) and through one plain
+    FP32 worker (one request at a time)."""
+    from uniphot_b200.serve import PackedServer, Server, latency_summary, poisson_stream
     from uniphot_b200.synth import make_serving_request
     pool = [make_serving_request(i, device="cuda").fit_kwargs("analytic")
             for i in range(args.serve_requests)]
@@ -598,24 +566,34 @@ def _serve_measure(args, rates, device):
                              "sources 5-2000 at the production density, PSF "
                              "polynomial coefficients drawn per request",
            "rates": []}
-    forms = (("batched_mixed", "mixed", args.serve_workers),
-             ("one_at_a_time_plain", "plain", 1))
-    for name, prec, workers in forms:
-        with Server(device=device, workers=workers, hbm_budget_bytes=160e9,
-                    precision=prec) as srv:
-            # warm-up: every worker's context, allocations and graphs
+    def packed(prec):
+        return PackedServer(device=device, planners=2, engines=2, hbm_budget_bytes=160e9,
+                            precision=prec, engine="queue")
+
+    def workers(n):
+        return lambda prec: Server(device=device, workers=n, hbm_budget_bytes=160e9,
+                                   precision=prec)
+
+    forms = (("packed_mixed", "mixed", packed, 2),
+             ("batched_mixed", "mixed", workers(args.serve_workers), args.serve_workers),
+             ("one_at_a_time_plain", "plain", workers(1), 1))
+    for name, prec, make, warm in forms:
+        with make(prec) as srv:
+            # warm-up: every context, allocations and graphs
             for f in [srv.submit(dict(pool[i % len(pool)], precision=prec))
-                      for i in range(workers)]:
+                      for i in range(warm)]:
                 f.result()
         for rate in rates:
-            with Server(device=device, workers=workers, hbm_budget_bytes=160e9,
-                        precision=prec) as srv:
+            with make(prec) as srv:
                 futs = poisson_stream(srv, [dict(kw, precision=prec) for kw in pool],
                                       rate, seed=7)
                 for f in futs:
                     f.result()
             summ = latency_summary(srv.stats)
             summ["peak_admitted_bytes"] = srv.peak_in_use
+            if hasattr(srv, "packs"):
+                summ["packs"] = len(srv.packs)
+                summ["mean_pack_size"] = float(np.mean(srv.packs))
             row = next((r for r in out["rates"] if r["rate_hz"] == rate), None)
             if row is None:
                 row = {"rate_hz": rate}
@@ -707,9 +685,12 @@ def main():
                     help="multi-GPU strong scaling: every rank takes its share of one "
                          "field's islands (default: weak scaling, a field per rank)")
     ap.add_argument("--batched", action="store_true",
-                    help="run only the batched configuration (about --batched-islands "
-                         "islands over fields of 5, 20 and 40 bands) and print its JSON line")
+                    help="run only the batched configuration (--batched-tiles 2048^2 tiles "
+                         "per band count 5, 20 and 40, packed into one job per band count) "
+                         "and print its JSON line")
     ap.add_argument("--batched-islands", type=int, default=100000)
+    ap.add_argument("--batched-tiles", type=int, default=3,
+                    help="distinct 2048^2 tiles per band count in the batched configuration")
     ap.add_argument("--batched-steps", type=int, default=2)
     ap.add_argument("--stress-islands", type=int, default=2000)
     ap.add_argument("--stress-sample", type=int, default=120)
@@ -924,8 +905,8 @@ def main():
         sv = _serve_measure(args, [args.serve_rate], local)
         r = sv["rates"][0]
         out["serve"] = sv
-        out["serve_latency_ms"] = {k: r["batched_mixed"][k]
-                                   for k in ("p50_ms", "p95_ms", "p99_ms")}
+        out["serve_latency_ms"] = {form: {k: r[form][k] for k in ("p50_ms", "p95_ms", "p99_ms")}
+                                   for form in ("packed_mixed", "batched_mixed")}
     # CPU legs after every GPU measurement: the CPU baseline and the float64
     # comparison that qualifies the metric
     if not args.no_cpu and rank == 0:

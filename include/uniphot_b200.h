@@ -235,7 +235,13 @@ int uph_set_stream(uph_ctx* ctx, void* stream);
 void* uph_get_stream(const uph_ctx* ctx);
 
 /* Padded field stacks (n_bands, Hp, Wp) float32: data - bg and inverse
- * variance (masked pixels 0); ``pad`` is the border width.  Copied to HBM. */
+ * variance (masked pixels 0); ``pad`` is the border width.  Copied to HBM.
+ * A chunk added to a job binds the field, PSF and Sersic table the context
+ * holds at that moment, and keeps them while the job lives: a later upload
+ * of any of them to the context allocates fresh buffers instead of
+ * overwriting ones a live chunk holds (and reuses them in place otherwise).
+ * One job may therefore hold the chunks of several fields, each solved
+ * against its own field and PSF -- requests packed into one solve. */
 int uph_upload_field(uph_ctx* ctx, const float* data, const float* invvar,
                      int32_t n_bands, int32_t Hp, int32_t Wp, int32_t pad);
 /* Same from device pointers (copied device-to-device). */

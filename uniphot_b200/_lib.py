@@ -165,6 +165,9 @@ class Context:
         self._h = h
         self.device = int(device)
         self._keep = []
+        # bumped by every field upload: a DeviceField records the value it
+        # was uploaded under, so a superseded one is detected
+        self.field_gen = 0
 
     def close(self):
         if getattr(self, "_h", None):
@@ -204,6 +207,7 @@ class Context:
         nb, Hp, Wp = d.shape
         self.check(lib().uph_upload_field(self._h, ptr(d), ptr(w), nb, Hp, Wp, int(pad)),
                    "uph_upload_field")
+        self.field_gen += 1
 
     def island_roots(self, x, y, radius, forced_singleton=None) -> np.ndarray:
         """Minimum member index of every source's island (uph_island_roots)."""
@@ -300,10 +304,12 @@ class Context:
         nb, H, W = d.shape
         self.check(lib().uph_upload_field_unpadded(self._h, ptr(d), ptr(w), nb, H, W,
                                                    int(pad)), "uph_upload_field_unpadded")
+        self.field_gen += 1
 
     def upload_field_device(self, d_ptr: int, w_ptr: int, nb, Hp, Wp, pad):
         self.check(lib().uph_upload_field_device(self._h, _P(d_ptr), _P(w_ptr), nb, Hp,
                                                  Wp, int(pad)), "uph_upload_field_device")
+        self.field_gen += 1
 
     def upload_psf_poly(self, tier: int, coefs: np.ndarray, origin_scale: np.ndarray):
         cf = np.ascontiguousarray(coefs, np.float32)

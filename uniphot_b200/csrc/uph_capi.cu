@@ -12,6 +12,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <memory>
 #include <string>
 #include <thread>
 #include <vector>
@@ -49,8 +50,25 @@ struct DevBuf {
   }
 };
 
+// A context buffer that the chunks of a live job may bind (field stacks,
+// PSF models, the Sersic table).  The chunk keeps a reference; an upload
+// overwrites the buffer in place only when no chunk holds it, and otherwise
+// swaps in a fresh allocation, so a job's chunks keep reading the inputs
+// they were added with while the context takes the next field (one job may
+// hold the chunks of several fields).
+using SBuf = std::shared_ptr<DevBuf>;
+
+SBuf sbuf_new() {
+  return SBuf(new DevBuf(), [](DevBuf* b) {
+    b->release();
+    delete b;
+  });
+}
+
+inline void* sptr(const SBuf& b) { return b ? b->ptr : nullptr; }
+
 struct PolyPsf {
-  DevBuf coefs, os;
+  SBuf coefs, os;
   int nt = 0, nb = 0;
 };
 
@@ -65,14 +83,14 @@ struct uph_ctx {
   bool own_stream = false;
   std::string err;
   // field
-  DevBuf dstack, wstack;
+  SBuf dstack, wstack;
   int nb = 0, Hp = 0, Wp = 0, pad = 0;
   // psf
   std::map<int, PolyPsf> poly;
-  DevBuf mog, mog_os;
+  SBuf mog, mog_os;
   int mog_k = 0, mog_nt = 0, mog_nb = 0;
   // table
-  DevBuf tb_knots, tb_amps, tb_lv, tb_core;
+  SBuf tb_knots, tb_amps, tb_lv, tb_core;
   int tb_n = 0, tb_k = 0;
   double tb_nmin = 0, tb_nmax = 0;
   int* h_active = nullptr;  // pinned
@@ -120,6 +138,12 @@ int ensure(uph_ctx* ctx, DevBuf& b, size_t bytes, const char* what) {
   }
   b.cap = bytes;
   return UPH_OK;
+}
+
+// ensure() for a bindable buffer: a buffer some chunk holds is left to it
+int ensure_shared(uph_ctx* ctx, SBuf& b, size_t bytes, const char* what) {
+  if (!b || b.use_count() > 1) b = sbuf_new();
+  return ensure(ctx, *b, bytes, what);
 }
 
 int upload(uph_ctx* ctx, void* dst, const void* src, size_t bytes,
@@ -188,18 +212,15 @@ int uph_destroy(uph_ctx* ctx) {
   if (!ctx) return UPH_OK;
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
-  ctx->dstack.release();
-  ctx->wstack.release();
-  for (auto& kv : ctx->poly) {
-    kv.second.coefs.release();
-    kv.second.os.release();
-  }
-  ctx->mog.release();
-  ctx->mog_os.release();
-  ctx->tb_knots.release();
-  ctx->tb_amps.release();
-  ctx->tb_lv.release();
-  ctx->tb_core.release();
+  ctx->dstack.reset();
+  ctx->wstack.reset();
+  ctx->poly.clear();
+  ctx->mog.reset();
+  ctx->mog_os.reset();
+  ctx->tb_knots.reset();
+  ctx->tb_amps.reset();
+  ctx->tb_lv.reset();
+  ctx->tb_core.reset();
   for (auto& b : ctx->sp) b.release();
   for (auto& b : ctx->isl) b.release();
   for (auto& ev : ctx->ev)
@@ -245,12 +266,12 @@ static int upload_field_impl(uph_ctx* ctx, const float* d, const float* w,
     return set_err(ctx, UPH_ERR_INVALID, "invalid field arguments");
   cudaSetDevice(ctx->device);
   size_t bytes = sizeof(float) * (size_t)nb * Hp * Wp;
-  int rc = ensure(ctx, ctx->dstack, bytes, "field data");
+  int rc = ensure_shared(ctx, ctx->dstack, bytes, "field data");
   if (rc) return rc;
-  rc = ensure(ctx, ctx->wstack, bytes, "field invvar");
+  rc = ensure_shared(ctx, ctx->wstack, bytes, "field invvar");
   if (rc) return rc;
-  CK(cudaMemcpyAsync(ctx->dstack.ptr, d, bytes, kind, ctx->stream), "field copy");
-  CK(cudaMemcpyAsync(ctx->wstack.ptr, w, bytes, kind, ctx->stream), "field copy");
+  CK(cudaMemcpyAsync(sptr(ctx->dstack), d, bytes, kind, ctx->stream), "field copy");
+  CK(cudaMemcpyAsync(sptr(ctx->wstack), w, bytes, kind, ctx->stream), "field copy");
   CK(cudaStreamSynchronize(ctx->stream), "field copy");
   ctx->nb = nb;
   ctx->Hp = Hp;
@@ -272,19 +293,19 @@ int uph_upload_field_unpadded(uph_ctx* ctx, const float* d, const float* w,
   cudaSetDevice(ctx->device);
   const int Hp = H + 2 * pad, Wp = W + 2 * pad;
   const size_t bytes = sizeof(float) * (size_t)nb * Hp * Wp;
-  int rc = ensure(ctx, ctx->dstack, bytes, "field data");
+  int rc = ensure_shared(ctx, ctx->dstack, bytes, "field data");
   if (rc) return rc;
-  rc = ensure(ctx, ctx->wstack, bytes, "field invvar");
+  rc = ensure_shared(ctx, ctx->wstack, bytes, "field invvar");
   if (rc) return rc;
-  CK(cudaMemsetAsync(ctx->dstack.ptr, 0, bytes, ctx->stream), "field pad");
-  CK(cudaMemsetAsync(ctx->wstack.ptr, 0, bytes, ctx->stream), "field pad");
+  CK(cudaMemsetAsync(sptr(ctx->dstack), 0, bytes, ctx->stream), "field pad");
+  CK(cudaMemsetAsync(sptr(ctx->wstack), 0, bytes, ctx->stream), "field pad");
   for (int b = 0; b < nb; ++b) {
     const size_t o = ((size_t)b * Hp + pad) * Wp + pad;
     const size_t so = (size_t)b * H * W;
-    CK(cudaMemcpy2DAsync((float*)ctx->dstack.ptr + o, sizeof(float) * Wp, d + so,
+    CK(cudaMemcpy2DAsync((float*)sptr(ctx->dstack) + o, sizeof(float) * Wp, d + so,
                          sizeof(float) * W, sizeof(float) * W, H,
                          cudaMemcpyHostToDevice, ctx->stream), "field copy");
-    CK(cudaMemcpy2DAsync((float*)ctx->wstack.ptr + o, sizeof(float) * Wp, w + so,
+    CK(cudaMemcpy2DAsync((float*)sptr(ctx->wstack) + o, sizeof(float) * Wp, w + so,
                          sizeof(float) * W, sizeof(float) * W, H,
                          cudaMemcpyHostToDevice, ctx->stream), "field copy");
   }
@@ -310,12 +331,12 @@ int uph_upload_psf_poly(uph_ctx* ctx, int32_t tier, const float* coefs,
   cudaSetDevice(ctx->device);
   PolyPsf& p = ctx->poly[tier];
   size_t bytes = sizeof(float) * (size_t)nb * tier * tier * nt;
-  int rc = ensure(ctx, p.coefs, bytes, "psf coefs");
+  int rc = ensure_shared(ctx, p.coefs, bytes, "psf coefs");
   if (rc) return rc;
-  rc = ensure(ctx, p.os, sizeof(float) * 4 * nb, "psf origin");
+  rc = ensure_shared(ctx, p.os, sizeof(float) * 4 * nb, "psf origin");
   if (rc) return rc;
-  CK(cudaMemcpyAsync(p.coefs.ptr, coefs, bytes, cudaMemcpyHostToDevice, ctx->stream), "psf");
-  CK(cudaMemcpyAsync(p.os.ptr, os, sizeof(float) * 4 * nb, cudaMemcpyHostToDevice, ctx->stream), "psf");
+  CK(cudaMemcpyAsync(sptr(p.coefs), coefs, bytes, cudaMemcpyHostToDevice, ctx->stream), "psf");
+  CK(cudaMemcpyAsync(sptr(p.os), os, sizeof(float) * 4 * nb, cudaMemcpyHostToDevice, ctx->stream), "psf");
   CK(cudaStreamSynchronize(ctx->stream), "psf");
   p.nt = nt;
   p.nb = nb;
@@ -330,12 +351,12 @@ int uph_upload_psf_mog(uph_ctx* ctx, const float* params, const float* os,
     return set_err(ctx, UPH_ERR_INVALID, "invalid MoG PSF (K %d, nt %d)", K, nt);
   cudaSetDevice(ctx->device);
   size_t bytes = sizeof(float) * (size_t)nb * K * 4 * nt;
-  int rc = ensure(ctx, ctx->mog, bytes, "mog psf");
+  int rc = ensure_shared(ctx, ctx->mog, bytes, "mog psf");
   if (rc) return rc;
-  rc = ensure(ctx, ctx->mog_os, sizeof(float) * 4 * nb, "mog origin");
+  rc = ensure_shared(ctx, ctx->mog_os, sizeof(float) * 4 * nb, "mog origin");
   if (rc) return rc;
-  CK(cudaMemcpyAsync(ctx->mog.ptr, params, bytes, cudaMemcpyHostToDevice, ctx->stream), "mog");
-  CK(cudaMemcpyAsync(ctx->mog_os.ptr, os, sizeof(float) * 4 * nb, cudaMemcpyHostToDevice, ctx->stream), "mog");
+  CK(cudaMemcpyAsync(sptr(ctx->mog), params, bytes, cudaMemcpyHostToDevice, ctx->stream), "mog");
+  CK(cudaMemcpyAsync(sptr(ctx->mog_os), os, sizeof(float) * 4 * nb, cudaMemcpyHostToDevice, ctx->stream), "mog");
   CK(cudaStreamSynchronize(ctx->stream), "mog");
   ctx->mog_k = K;
   ctx->mog_nt = nt;
@@ -351,15 +372,15 @@ int uph_upload_sersic_table(uph_ctx* ctx, const double* knots,
   if (!knots || !amps || !lv || !core || n < 2 || kmax <= 0 || kmax > UPH_MAXGAL - 1)
     return set_err(ctx, UPH_ERR_INVALID, "invalid Sersic table");
   cudaSetDevice(ctx->device);
-  int rc = ensure(ctx, ctx->tb_knots, sizeof(double) * n, "table");
-  if (!rc) rc = ensure(ctx, ctx->tb_amps, sizeof(double) * n * kmax, "table");
-  if (!rc) rc = ensure(ctx, ctx->tb_lv, sizeof(double) * n * kmax, "table");
-  if (!rc) rc = ensure(ctx, ctx->tb_core, sizeof(double) * n, "table");
+  int rc = ensure_shared(ctx, ctx->tb_knots, sizeof(double) * n, "table");
+  if (!rc) rc = ensure_shared(ctx, ctx->tb_amps, sizeof(double) * n * kmax, "table");
+  if (!rc) rc = ensure_shared(ctx, ctx->tb_lv, sizeof(double) * n * kmax, "table");
+  if (!rc) rc = ensure_shared(ctx, ctx->tb_core, sizeof(double) * n, "table");
   if (rc) return rc;
-  CK(cudaMemcpyAsync(ctx->tb_knots.ptr, knots, sizeof(double) * n, cudaMemcpyHostToDevice, ctx->stream), "table");
-  CK(cudaMemcpyAsync(ctx->tb_amps.ptr, amps, sizeof(double) * n * kmax, cudaMemcpyHostToDevice, ctx->stream), "table");
-  CK(cudaMemcpyAsync(ctx->tb_lv.ptr, lv, sizeof(double) * n * kmax, cudaMemcpyHostToDevice, ctx->stream), "table");
-  CK(cudaMemcpyAsync(ctx->tb_core.ptr, core, sizeof(double) * n, cudaMemcpyHostToDevice, ctx->stream), "table");
+  CK(cudaMemcpyAsync(sptr(ctx->tb_knots), knots, sizeof(double) * n, cudaMemcpyHostToDevice, ctx->stream), "table");
+  CK(cudaMemcpyAsync(sptr(ctx->tb_amps), amps, sizeof(double) * n * kmax, cudaMemcpyHostToDevice, ctx->stream), "table");
+  CK(cudaMemcpyAsync(sptr(ctx->tb_lv), lv, sizeof(double) * n * kmax, cudaMemcpyHostToDevice, ctx->stream), "table");
+  CK(cudaMemcpyAsync(sptr(ctx->tb_core), core, sizeof(double) * n, cudaMemcpyHostToDevice, ctx->stream), "table");
   CK(cudaStreamSynchronize(ctx->stream), "table");
   ctx->tb_n = n;
   ctx->tb_k = kmax;
@@ -413,6 +434,7 @@ struct Chunk {
   float* d_seed = nullptr;
   float* d_msf = nullptr;
   bool perr_out = false;           // param_errors requested
+  std::vector<SBuf> bound;         // the context buffers the chunk reads
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t gexec = nullptr;
   cudaEvent_t ev_group = nullptr;
@@ -543,7 +565,7 @@ int add_chunk(uph_ctx* ctx, Chunk* ch, const uph_class_desc* cls,
     return set_err(ctx, UPH_ERR_INVALID, "nsrc class %d outside 1..%d", N, UPH_MAXN);
   if (B <= 0 || T <= 0 || (T % 2) == 0)
     return set_err(ctx, UPH_ERR_INVALID, "invalid bbox %d / tier %d", B, T);
-  if (!ctx->dstack.ptr) return set_err(ctx, UPH_ERR_STATE, "no field uploaded");
+  if (!sptr(ctx->dstack)) return set_err(ctx, UPH_ERR_STATE, "no field uploaded");
   if (!in->ox || !in->oy || !in->x0b || !in->y0b || !in->stype || !in->n_frozen ||
       !in->free_n || !in->mmask || !in->keep || !in->p0 || !in->lower ||
       !in->upper || !in->prior_mean || !in->prior_inv_sigma)
@@ -558,7 +580,7 @@ int add_chunk(uph_ctx* ctx, Chunk* ch, const uph_class_desc* cls,
     pp = &it->second;
     if (pp->nb != nb) return set_err(ctx, UPH_ERR_INVALID, "PSF band count mismatch");
   } else if (mode == UPH_RENDER_ANALYTIC) {
-    if (!ctx->mog.ptr || ctx->mog_nb != nb)
+    if (!sptr(ctx->mog) || ctx->mog_nb != nb)
       return set_err(ctx, UPH_ERR_STATE, "no analytic PSF uploaded for %d bands", nb);
   } else {
     return set_err(ctx, UPH_ERR_INVALID, "unknown render mode %d", mode);
@@ -602,7 +624,7 @@ int add_chunk(uph_ctx* ctx, Chunk* ch, const uph_class_desc* cls,
   if (any_gal && mode == UPH_RENDER_REFERENCE && fft_pad_for(T) > 512)
     return set_err(ctx, UPH_ERR_INVALID,
                    "reference-mode galaxies: tier %d needs a Fourier grid above 512", T);
-  if (any_gal && !ctx->tb_knots.ptr)
+  if (any_gal && !sptr(ctx->tb_knots))
     return set_err(ctx, UPH_ERR_STATE, "no Sersic table uploaded");
   std::vector<int16_t> row_k((size_t)n * Kmax, 0), row_s((size_t)n * Kmax, -1),
       row_p((size_t)n * Kmax, -1);
@@ -655,24 +677,29 @@ int add_chunk(uph_ctx* ctx, Chunk* ch, const uph_class_desc* cls,
                       ? (cls->tc_min_rows < 0 ? UPH_TC_MIN_ROWS_DEFAULT : cls->tc_min_rows)
                       : (1 << 30);
   c.Hp = ctx->Hp; c.Wp = ctx->Wp;
-  c.dstack = (const float*)ctx->dstack.ptr;
-  c.wstack = (const float*)ctx->wstack.ptr;
+  c.dstack = (const float*)sptr(ctx->dstack);
+  c.wstack = (const float*)sptr(ctx->wstack);
+  ch->bound = {ctx->dstack, ctx->wstack, ctx->tb_knots, ctx->tb_amps, ctx->tb_lv, ctx->tb_core};
   if (mode == UPH_RENDER_REFERENCE) {
-    c.psf_coefs = (const float*)pp->coefs.ptr;
-    c.psf_os = (const float*)pp->os.ptr;
+    ch->bound.push_back(pp->coefs);
+    ch->bound.push_back(pp->os);
+    c.psf_coefs = (const float*)sptr(pp->coefs);
+    c.psf_os = (const float*)sptr(pp->os);
     c.nt = pp->nt;
     c.psf_varies = pp->nt > 1;
   } else {
-    c.mog = (const float*)ctx->mog.ptr;
-    c.psf_os = (const float*)ctx->mog_os.ptr;
+    ch->bound.push_back(ctx->mog);
+    ch->bound.push_back(ctx->mog_os);
+    c.mog = (const float*)sptr(ctx->mog);
+    c.psf_os = (const float*)sptr(ctx->mog_os);
     c.nt = ctx->mog_nt;
     c.kpsf = ctx->mog_k;
     c.psf_varies = ctx->mog_nt > 1;
   }
-  c.tb_knots = (const double*)ctx->tb_knots.ptr;
-  c.tb_amps = (const double*)ctx->tb_amps.ptr;
-  c.tb_lv = (const double*)ctx->tb_lv.ptr;
-  c.tb_core = (const double*)ctx->tb_core.ptr;
+  c.tb_knots = (const double*)sptr(ctx->tb_knots);
+  c.tb_amps = (const double*)sptr(ctx->tb_amps);
+  c.tb_lv = (const double*)sptr(ctx->tb_lv);
+  c.tb_core = (const double*)sptr(ctx->tb_core);
   c.tb_n = ctx->tb_n; c.tb_k = ctx->tb_k; c.tb_nmin = ctx->tb_nmin; c.tb_nmax = ctx->tb_nmax;
   int rc = UPH_OK;
   int* d_ox = cbuf<int>(ctx, ch, "ox", n, &rc);
@@ -1803,7 +1830,7 @@ int uph_sparse_band_solve(uph_ctx* ctx, const uph_sparse_band* in, uph_sparse_ou
   if (direct && (in->exp_k < 1 || in->exp_k > 16 || !in->exp_amp || !in->exp_var))
     return set_err(ctx, UPH_ERR_INVALID, "direct backend needs 1..16 mixture components");
   const int fftP = fft_pad_for(std::max(H, W));
-  if (any_gal && !direct && !ctx->tb_knots.ptr)
+  if (any_gal && !direct && !sptr(ctx->tb_knots))
     return set_err(ctx, UPH_ERR_STATE, "no Sersic table uploaded");
   if (any_gal && !direct && fftP > 512)
     return set_err(ctx, UPH_ERR_INVALID, "PSF stamp %dx%d needs a Fourier grid above 512", H, W);
@@ -1883,10 +1910,10 @@ int uph_sparse_band_solve(uph_ctx* ctx, const uph_sparse_band* in, uph_sparse_ou
     d.direct = direct ? 1 : 0;
     d.exp_k = direct ? in->exp_k : 0;
     d.exp_mog = (const float*)ctx->sp[31].ptr;
-    d.tb_knots = (const double*)ctx->tb_knots.ptr;
-    d.tb_amps = (const double*)ctx->tb_amps.ptr;
-    d.tb_lv = (const double*)ctx->tb_lv.ptr;
-    d.tb_core = (const double*)ctx->tb_core.ptr;
+    d.tb_knots = (const double*)sptr(ctx->tb_knots);
+    d.tb_amps = (const double*)sptr(ctx->tb_amps);
+    d.tb_lv = (const double*)sptr(ctx->tb_lv);
+    d.tb_core = (const double*)sptr(ctx->tb_core);
     d.tb_n = ctx->tb_n;
     d.tb_k = ctx->tb_k;
     d.tb_nmin = ctx->tb_nmin;

@@ -27,6 +27,15 @@ buffers stay cached in the stream-ordered memory pool, but the pool never
 holds more than the largest admitted total, so device memory stays within
 the budget.
 
+:class:`PackedServer` packs instead: the requests admitted while the device
+is busy are solved together as ONE library job holding every request's
+chunks (each chunk bound to its own request's field and PSF on the device),
+so their islands of every size run through the same LM-loop kernels -- with
+the "queue" engine, one persistent work-queue kernel per kernel kind and LM
+phase over the islands of all packed requests, converged islands retired on
+the device.  Results are again bitwise those of each request alone: a
+chunk's islands are computed the same whatever else the job holds.
+
 Latency of a request = time from its submission to its result (queueing,
 planning, upload, solve, download and unpack).
 """
@@ -54,6 +63,8 @@ class RequestStats:
     n_islands: int = 0
     pixels: int = 0                # n_bands * H * W
     worker: int = -1
+    pack: int = -1                 # PackedServer: the pack it was solved in
+    pack_size: int = 0
 
     @property
     def latency(self) -> float:
@@ -189,6 +200,255 @@ class Server:
                     self._release(held)
                 with self._lock:
                     self.stats.append(st)
+
+
+@dataclass
+class _Admitted:
+    item: _Item
+    plan: object
+    charged: float                 # budget bytes held while in flight
+    field_bytes: float
+    key: object                    # requests of one pack share it
+
+
+class PackedServer:
+    """Continuous-batching server that packs requests into one solve.
+
+    ``planners`` host threads take requests in arrival order, plan them and
+    admit them by the HBM budget (a request waits on the host until its
+    device bytes fit next to those in flight).  ``engines`` device threads,
+    each with its own library context, take every admitted request not yet
+    taken (up to ``max_pack``, sharing the first one's LM step limit) as one
+    pack: upload each request's field and PSF, add all their chunks to one
+    job, solve it once (``engine``/``lanes`` as ``uph_job_set_engine``) and
+    unpack each request's result.  Requests that arrive while a pack is on
+    the device are admitted meanwhile and form the next pack; with two
+    engines one pack uploads and unpacks while the other solves.
+
+    ``pack_fn(engine_state, [(kwargs, plan), ...]) -> [result or exception]``
+    and ``plan_fn`` (as :class:`Server`) default to the CUDA solver
+    (:func:`default_pack`, :func:`default_plan`); tests pass host stand-ins.
+    A request fails alone: an exception in its planning, upload or unpacking
+    reaches its own future only.
+    """
+
+    def __init__(self, device: int = 0, planners: int = 2, engines: int = 2,
+                 hbm_budget_bytes: float = 160e9, precision: str = "mixed",
+                 max_pack: int = 64, engine: str = "queue", lanes: int = 0,
+                 plan_fn: Optional[Callable] = None,
+                 pack_fn: Optional[Callable] = None,
+                 engine_init: Optional[Callable] = None,
+                 key_fn: Optional[Callable] = None):
+        if planners < 1 or engines < 1 or max_pack < 1:
+            raise ValueError("planners, engines and max_pack must be >= 1")
+        self.device = int(device)
+        self.precision = precision
+        self.budget = float(hbm_budget_bytes)
+        self.max_pack = int(max_pack)
+        self.in_use = 0.0
+        self.peak_in_use = 0.0
+        self._plan = plan_fn or default_plan
+        self._pack = pack_fn or default_pack
+        self._key = key_fn or (lambda kw: kw.get("max_steps"))
+        self._init = engine_init or (lambda i: {"device": self.device,
+                                                "precision": self.precision,
+                                                "engine": engine, "lanes": int(lanes)})
+        self._q: "queue.Queue[Optional[_Item]]" = queue.Queue()
+        self._cv = threading.Condition()            # budget
+        self._rcv = threading.Condition()           # admitted requests
+        self._ready: list[_Admitted] = []
+        self._planning = int(planners)
+        self._next = 0
+        self._npack = 0
+        self._lock = threading.Lock()
+        self.stats: list[RequestStats] = []
+        self.packs: list[int] = []                  # size of every pack solved
+        self.resident = [0.0] * engines             # field bytes kept per engine
+        self._planners = [threading.Thread(target=self._plan_loop, daemon=True)
+                          for _ in range(planners)]
+        self._engines = [threading.Thread(target=self._engine_loop, args=(i,), daemon=True)
+                         for i in range(engines)]
+        self._closed = False
+        for t in self._planners + self._engines:
+            t.start()
+
+    # ------------------------------------------------------------------ API
+    def submit(self, kwargs: dict) -> Future:
+        """Queue one request (``island_fit`` keywords); returns a future of
+        its ``IslandFitResult``."""
+        if self._closed:
+            raise RuntimeError("server is closed")
+        with self._lock:
+            rid = self._next
+            self._next += 1
+        st = RequestStats(rid, time.perf_counter())
+        fut: Future = Future()
+        self._q.put(_Item(rid, kwargs, fut, st))
+        return fut
+
+    def close(self):
+        """Finish every queued request, then stop the threads."""
+        if self._closed:
+            return
+        self._closed = True
+        for _ in self._planners:
+            self._q.put(None)
+        for t in self._planners:
+            t.join()
+        for t in self._engines:
+            t.join()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # ------------------------------------------------------------ internals
+    def _acquire(self, nbytes: float):
+        nbytes = min(float(nbytes), self.budget)   # a request larger than the budget runs alone
+        with self._cv:
+            while self.in_use + nbytes > self.budget:
+                self._cv.wait()
+            self.in_use += nbytes
+            self.peak_in_use = max(self.peak_in_use, self.in_use)
+        return nbytes
+
+    def _finish(self, item: _Item, result=None, error=None):
+        item.stats.finished = time.perf_counter()
+        with self._lock:
+            self.stats.append(item.stats)
+        if error is not None:
+            item.future.set_exception(error)
+        else:
+            item.future.set_result(result)
+
+    def _plan_loop(self):
+        while True:
+            item = self._q.get()
+            if item is None:
+                break
+            st = item.stats
+            try:
+                planned = self._plan(item.kwargs)
+                plan, nbytes, n_isl = planned[:3]
+                fb = float(planned[3]) if len(planned) > 3 else 0.0
+                st.device_bytes, st.n_islands = int(nbytes), int(n_isl)
+                d = item.kwargs.get("data_minus_bg")
+                st.pixels = int(np.prod(np.shape(d))) if d is not None else 0
+                key = self._key(item.kwargs)
+            except BaseException as e:  # noqa: BLE001 -- reported through the future
+                self._finish(item, error=e)
+                continue
+            held = self._acquire(nbytes)
+            st.admitted = time.perf_counter()
+            with self._rcv:
+                self._ready.append(_Admitted(item, plan, held, fb, key))
+                self._rcv.notify()
+        with self._rcv:
+            self._planning -= 1
+            self._rcv.notify_all()
+
+    def _take(self) -> list:
+        """Every admitted request sharing the oldest one's key, oldest first
+        (called with the ready lock held)."""
+        key = self._ready[0].key
+        pack, rest = [], []
+        for a in self._ready:
+            if a.key == key and len(pack) < self.max_pack:
+                pack.append(a)
+            else:
+                rest.append(a)
+        self._ready = rest
+        return pack
+
+    def _engine_loop(self, ei: int):
+        state = self._init(ei)
+        while True:
+            with self._rcv:
+                while not self._ready and self._planning > 0:
+                    self._rcv.wait()
+                if not self._ready:
+                    break
+                pack = self._take()
+            with self._lock:
+                pid = self._npack
+                self._npack += 1
+                self.packs.append(len(pack))
+            for a in pack:
+                a.item.stats.worker, a.item.stats.pack = ei, pid
+                a.item.stats.pack_size = len(pack)
+            try:
+                outs = list(self._pack(state, [(a.item.kwargs, a.plan) for a in pack]))
+                if len(outs) != len(pack):
+                    raise RuntimeError(f"pack_fn returned {len(outs)} results for "
+                                       f"{len(pack)} requests")
+            except BaseException as e:  # noqa: BLE001 -- every request of the pack
+                outs = [e] * len(pack)
+            # the context keeps the last uploaded field between packs: at
+            # most the largest field seen stays charged to the budget
+            new_res = max([self.resident[ei]] + [a.field_bytes for a in pack])
+            growth = new_res - self.resident[ei]
+            self.resident[ei] = new_res
+            with self._cv:
+                self.in_use -= sum(a.charged for a in pack) - growth
+                self._cv.notify_all()
+            for a, r in zip(pack, outs):
+                if isinstance(r, BaseException):
+                    self._finish(a.item, error=r)
+                else:
+                    self._finish(a.item, result=r)
+
+
+def default_pack(state: dict, reqs: list) -> list:
+    """Solve planned requests as one job on the engine's context: every
+    request's field and PSF uploaded (a field bound by the job's chunks stays
+    allocated while later fields are uploaded), all chunks added to one job,
+    one solve, then each request's rows unpacked.  Returns one result or
+    exception per request.  If the packed solve itself fails, each request
+    is solved alone so that one bad request does not fail the others."""
+    from . import _lib
+    from .solver import DeviceField, IslandFitJob, giant_only_result
+    if "ctx" not in state:
+        state["ctx"] = _lib.Context(state["device"])
+    ctx = state["ctx"]
+    out: list = [None] * len(reqs)
+    fits = []
+    job = _lib.Job(ctx)
+    try:
+        job.set_engine(state.get("engine", "queue"), int(state.get("lanes", 0)))
+        for i, (kw, plan) in enumerate(reqs):
+            try:
+                if plan is None:
+                    out[i] = giant_only_result(**kw)
+                    continue
+                kw = dict(kw)
+                kw.setdefault("precision", state["precision"])
+                fld = DeviceField.from_unpadded(kw["data_minus_bg"], kw["invvar"], plan.PAD,
+                                                device=state["device"], context=ctx)
+                fits.append((i, IslandFitJob(**kw, device=state["device"], field=fld,
+                                             plan=plan, job=job)))
+            except BaseException as e:  # noqa: BLE001 -- this request only
+                out[i] = e
+        if fits:
+            try:
+                job.solve(max(f.max_steps for _, f in fits))
+            except BaseException:  # noqa: BLE001 -- retried one by one below
+                fits_alone, fits = fits, []
+                job.close()
+                for i, _ in fits_alone:
+                    try:
+                        out[i] = default_solve(state, reqs[i][0], reqs[i][1])
+                    except BaseException as e:  # noqa: BLE001
+                        out[i] = e
+            for i, f in fits:
+                try:
+                    out[i] = f.result()
+                except BaseException as e:  # noqa: BLE001
+                    out[i] = e
+    finally:
+        job.close()
+    return out
 
 
 def default_plan(kwargs: dict):

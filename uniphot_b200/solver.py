@@ -121,12 +121,16 @@ def _fingerprint(*arrays) -> str:
 class DeviceField:
     """The padded field stacks resident on one device (a library context).
 
-    Plays the role of the reference's ``dstack_dev``/``wstack_dev``."""
+    Plays the role of the reference's ``dstack_dev``/``wstack_dev``.  A
+    context holds one field at a time for new chunks: uploading another field
+    to the same context supersedes this one (:meth:`check_current` raises),
+    while the chunks already added from it keep reading it."""
 
     def __init__(self, data_pad: np.ndarray, invvar_pad: np.ndarray, pad: int,
                  device: int = 0, context: Optional[_lib.Context] = None):
         self.ctx = context if context is not None else _lib.Context(device)
         self.ctx.upload_field(data_pad, invvar_pad, pad)
+        self.gen = self.ctx.field_gen
         self.pad = int(pad)
         self.n_bands = int(data_pad.shape[0])
         self.shape = tuple(data_pad.shape)
@@ -142,6 +146,7 @@ class DeviceField:
         self = cls.__new__(cls)
         self.ctx = context if context is not None else _lib.Context(device)
         self.ctx.upload_field_unpadded(data_minus_bg, invvar, pad)
+        self.gen = self.ctx.field_gen
         nb, H, W = np.shape(data_minus_bg)
         self.pad = int(pad)
         self.n_bands = int(nb)
@@ -150,6 +155,12 @@ class DeviceField:
         self._mog_key = None
         self._table = False
         return self
+
+    def check_current(self):
+        """Raise unless this is still the field its context holds."""
+        if self.ctx.field_gen != self.gen:
+            raise ValueError("the DeviceField was superseded by a later field upload "
+                             "to its context; upload it again")
 
     def ensure_psf(self, tree: PsfTree):
         # keyed by content: object ids can be reused once a tree is freed
@@ -464,7 +475,10 @@ class IslandFitJob:
     ``engine`` picks the LM loop's scheduling: "queue" (every chunk's
     iteration as one persistent work-queue kernel per kernel kind, islands
     retired on the device) or "chunks" (each chunk's iterations as its own
-    graph on a stream pool); the results are the same bit for bit."""
+    graph on a stream pool); the results are the same bit for bit.
+    ``job``: add the chunks to this (shared) library job instead of a job of
+    their own -- the packed server puts several requests' fields into one
+    job this way; the job's owner solves and closes it."""
 
     def __init__(self, *, bandnames: list, data_minus_bg: np.ndarray,
                  invvar: np.ndarray, psfs: list, island_set, buckets, pos_x, pos_y,
@@ -495,7 +509,8 @@ class IslandFitJob:
                  field: DeviceField | None = None,
                  chunk_budget_bytes: float = 16e9, precision: str = "plain",
                  plan: "FieldPlan | None" = None, bg_mode: str = "frozen",
-                 engine: str = "chunks", lanes: int = 0):
+                 engine: str = "chunks", lanes: int = 0,
+                 job: "_lib.Job | None" = None):
         self.log_fn = log_fn
         if render_mode is None:
             render_mode = "analytic" if _is_mog(psfs[0]) else "reference"
@@ -520,11 +535,19 @@ class IslandFitJob:
             field = DeviceField.from_unpadded(
                 data_minus_bg, invvar, PAD, device=device,
                 context=field.ctx if field is not None else None)
+        field.check_current()
         self.field, self.PAD = field, PAD
         plans = [p for p, _ in fp.classes]
         capped = fp.capped
-        self.job = _lib.Job(field.ctx)
-        self.job.set_engine(engine, lanes)
+        if job is not None:
+            # chunks added to a job shared with other fields (packed
+            # serving): its owner solves and closes it
+            if job.ctx is not field.ctx:
+                raise ValueError("a shared job must belong to the field's context")
+            self.job, self._own_job = job, False
+        else:
+            self.job, self._own_job = _lib.Job(field.ctx), True
+            self.job.set_engine(engine, lanes)
         self.tuning = None
         self.classes = []
         trees = {}
@@ -656,7 +679,8 @@ class IslandFitJob:
         return _assemble_result(self.bandnames, out_rows, bucket_stats)
 
     def close(self):
-        self.job.close()
+        if self._own_job:
+            self.job.close()
 
 
 def _assemble_result(bandnames, out_rows, bucket_stats) -> IslandFitResult:
