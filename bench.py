@@ -429,6 +429,36 @@ def _stress_measure(args, device):
         q["pos_err_px_median"] = float(np.median(dp)) if dp.size else None
         q["pos_err_px_max"] = float(dp.max()) if dp.size else None
         q["frac_pos_within_1e-3_px"] = float(np.mean(dp <= 1e-3)) if dp.size else None
+        nst = np.concatenate([get(ci)["nst"] for ci in range(len(job.classes))])
+        q["lm_iterations"] = {"median": float(np.median(nst)), "p90": float(np.percentile(nst, 90)),
+                              "max": int(nst.max())}
+        if prec == "mixed":
+            # the conditioning indicator of every island (worst band) at the
+            # final parameters, over the whole field, and the sampled fluxes'
+            # pass fraction by its range
+            ac = np.concatenate([np.nanmax(get(ci)["acond"], axis=1)
+                                 for ci in range(len(job.classes))])
+            edges = (1.0, 10.0, 1e3, 1e6, np.inf)
+            q["conditioning"] = {
+                "what": "pivot spread of the f64 elimination of each band's diagonally "
+                        "scaled member normal matrix (worst band), final parameters",
+                "p50": float(np.percentile(ac, 50)), "p90": float(np.percentile(ac, 90)),
+                "p99": float(np.percentile(ac, 99)), "max": float(ac.max()),
+                "frac_above_tc_cond_max_10": float(np.mean(ac > 10.0)),
+                "islands_by_range": {f"{lo:g}-{hi:g}": int(np.sum((ac >= lo) & (ac < hi)))
+                                     for lo, hi in zip(edges[:-1], edges[1:])}}
+            passed = {}
+            for (ci, r), o in ref64:
+                a = float(np.nanmax(get(ci)["acond"][r]))
+                mm = job.classes[ci][1]["mmask"][r]
+                f, f64 = get(ci)["fluxes"][r][:, mm], o["fluxes"][:, mm]
+                d = np.abs(f - f64)
+                ok = (d <= 1e-4 * np.abs(f64)) | (d <= 0.01 * o["ferr"][:, mm])
+                key = next(f"{lo:g}-{hi:g}" for lo, hi in zip(edges[:-1], edges[1:]) if a < hi)
+                n_ok, n_all = passed.get(key, (0, 0))
+                passed[key] = (n_ok + int(ok.sum()), n_all + int(ok.size))
+            q["conditioning"]["sample_flux_pass_by_range"] = {
+                k: {"fluxes": n, "frac_within": ok / n} for k, (ok, n) in sorted(passed.items())}
         out[prec] = q
         job.close()
     return out
@@ -639,7 +669,7 @@ def _class_results(job):
             plan, host, ids = job.classes[ci]
             parts = [job.job.read(i) for i in ids]
             cache[ci] = {k: np.concatenate([q[k] for q in parts], axis=0)
-                         for k in ("fluxes", "p")}
+                         for k in ("fluxes", "p", "nst", "acond")}
         return cache[ci]
     return get
 

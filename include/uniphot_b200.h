@@ -224,6 +224,12 @@ typedef struct uph_chunk_out {
   float* resid;         /* [n*B*B] with residual: sum_b w (d - model)      */
   float* resid_w;       /* [n*B*B] with residual: sum_b w; both NaN-filled
                            without; may be NULL                            */
+  float* acond;         /* [n*nb] mixed precision: conditioning indicator
+                           of each band's member normal matrix at the
+                           final parameters (the spread of the f64
+                           elimination's pivots of the diagonally scaled
+                           matrix, the tensor-core routing test); NaN in
+                           the plain form; may be NULL                     */
 } uph_chunk_out;
 
 /* Context: one per device per process. */

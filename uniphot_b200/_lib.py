@@ -67,7 +67,7 @@ class ChunkOut(C.Structure):
         [("steps_run", C.c_int32), ("bg", _P), ("bg_err", _P), ("n_same", _P),
          ("prej", _P), ("railed", _P), ("perr", _P), ("femarg", _P),
          ("smetrics", _P), ("swin", _P), ("reprof", _P), ("resid", _P),
-         ("resid_w", _P)]
+         ("resid_w", _P), ("acond", _P)]
 
 
 class SparseBand(C.Structure):
@@ -414,7 +414,8 @@ def chunk_out(n: int, N: int, nb: int, B: int = 0):
                railed=np.zeros(n, np.uint8), perr=np.zeros((n, N, 13), np.float32),
                femarg=np.zeros((n, nb, N), np.float32),
                smetrics=np.zeros((n, N, 4), np.float32), swin=np.zeros((n, nb, N), np.float32),
-               reprof=np.zeros((n, N, 12), np.float32))
+               reprof=np.zeros((n, N, 12), np.float32),
+               acond=np.zeros((n, nb), np.float32))
     if B > 0:
         out["resid"] = np.zeros((n, B, B), np.float32)
         out["resid_w"] = np.zeros((n, B, B), np.float32)

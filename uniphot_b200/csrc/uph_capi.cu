@@ -1611,6 +1611,14 @@ int job_read(uph_job* job, int id, uph_chunk_out* out) {
       for (size_t e = 0; e < (size_t)n * N * UPH_REPROF_K; ++e) out->reprof[e] = NAN;
     }
   }
+  if (out->acond) {
+    if (c.acond_cur) {
+      if ((rc = download(ctx, out->acond, c.acond_cur, sizeof(float) * n * nb, "acond")))
+        return rc;
+    } else {
+      for (size_t e = 0; e < (size_t)n * nb; ++e) out->acond[e] = NAN;
+    }
+  }
   for (int q = 0; q < 2; ++q) {
     float* dst = q ? out->resid_w : out->resid;
     const float* src = q ? c.resid_w : c.resid;
