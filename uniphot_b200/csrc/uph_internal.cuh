@@ -518,33 +518,60 @@ __device__ inline void sersic_segment(const double* knots, int nk, double nmin, 
 // ---- Shared-memory radix-2 FFTs for the Fourier-domain galaxy stamps ----
 // In-place decimation-in-time FFTs of nl lines of length P = 2^logP stored
 // contiguously in shared memory; sign -1 forward, +1 inverse (unnormalised);
-// cw/sw hold cos and sin of 2 pi m / P.  Ends with a barrier.
+// cw/sw hold cos and sin of 2 pi m / P.  The callers fill each line in
+// bit-reversed order (fft_brev), so the transform starts at the butterflies.
+// Two consecutive stages (half-lengths h and 2h) run as one pass: a thread
+// takes the four elements j, j+h, j+2h, j+3h of a group of 4h and applies
+// both stages' butterflies with the stages' own twiddles, which halves the
+// barriers and shared-memory round trips; an odd last stage runs alone.
+// Ends with a barrier.
+__device__ inline int fft_brev(int k, int logP) {
+  return (int)(__brev((unsigned)k) >> (32 - logP));
+}
+
+__device__ inline void fft_bfly(float2& u, float2& v, float wr, float wi) {
+  const float tr = wr * v.x - wi * v.y, ti = wr * v.y + wi * v.x;
+  const float2 a = u;
+  u = make_float2(a.x + tr, a.y + ti);
+  v = make_float2(a.x - tr, a.y - ti);
+}
+
 __device__ inline void smem_fft_lines(float2* buf, int nl, int P, int logP, float sign,
                                       const float* cw, const float* sw) {
   const int tid = threadIdx.x, nth = blockDim.x;
-  for (int e = tid; e < nl * P; e += nth) {
-    const int base = (e >> logP) << logP, k = e & (P - 1);
-    const int r = (int)(__brev((unsigned)k) >> (32 - logP));
-    if (k < r) {
-      const float2 a = buf[base + k];
-      buf[base + k] = buf[base + r];
-      buf[base + r] = a;
+  int h = 1;
+  for (; 4 * h <= P; h <<= 2) {
+    const int q = P >> 2;                      // four-element groups per line
+    const int sA = P / (2 * h), sB = P / (4 * h);
+    for (int e = tid; e < nl * q; e += nth) {
+      const int line = e / q, b = e - line * q;
+      const int grp = b / h, j = b - grp * h;
+      const int i0 = (line << logP) + grp * 4 * h + j;
+      float2 x0 = buf[i0], x1 = buf[i0 + h], x2 = buf[i0 + 2 * h], x3 = buf[i0 + 3 * h];
+      const int mA = j * sA;
+      fft_bfly(x0, x1, cw[mA], sign * sw[mA]);
+      fft_bfly(x2, x3, cw[mA], sign * sw[mA]);
+      const int mB0 = j * sB, mB1 = (j + h) * sB;
+      fft_bfly(x0, x2, cw[mB0], sign * sw[mB0]);
+      fft_bfly(x1, x3, cw[mB1], sign * sw[mB1]);
+      buf[i0] = x0;
+      buf[i0 + h] = x1;
+      buf[i0 + 2 * h] = x2;
+      buf[i0 + 3 * h] = x3;
     }
+    __syncthreads();
   }
-  __syncthreads();
-  const int hp = P >> 1;
-  for (int len = 2, step = hp; len <= P; len <<= 1, step >>= 1) {
-    const int half = len >> 1;
+  if (2 * h == P) {
+    const int hp = P >> 1, step = P / (2 * h);
     for (int e = tid; e < nl * hp; e += nth) {
       const int line = e / hp, b = e - line * hp;
-      const int grp = b / half, j = b - grp * half;
-      const int i0 = (line << logP) + grp * len + j, i1 = i0 + half;
+      const int grp = b / h, j = b - grp * h;
+      const int i0 = (line << logP) + grp * 2 * h + j;
+      float2 u = buf[i0], v = buf[i0 + h];
       const int m = j * step;
-      const float wr = cw[m], wi = sign * sw[m];
-      const float2 v = buf[i1], u = buf[i0];
-      const float tr = wr * v.x - wi * v.y, ti = wr * v.y + wi * v.x;
-      buf[i0] = make_float2(u.x + tr, u.y + ti);
-      buf[i1] = make_float2(u.x - tr, u.y - ti);
+      fft_bfly(u, v, cw[m], sign * sw[m]);
+      buf[i0] = u;
+      buf[i0 + h] = v;
     }
     __syncthreads();
   }
@@ -561,7 +588,8 @@ __device__ inline void fft2_forward(const float* img, int Hs, int Ws, int P, int
     const int nl = min(lb, Hs - i0);
     for (int e = tid; e < nl * P; e += nth) {
       const int line = e >> logP, k = e & (P - 1);
-      buf[e] = make_float2(k < Ws ? img[(i0 + line) * Ws + k] : 0.f, 0.f);
+      buf[(line << logP) + fft_brev(k, logP)] =
+          make_float2(k < Ws ? img[(i0 + line) * Ws + k] : 0.f, 0.f);
     }
     __syncthreads();
     smem_fft_lines(buf, nl, P, logP, -1.f, cw, sw);
@@ -575,7 +603,8 @@ __device__ inline void fft2_forward(const float* img, int Hs, int Ws, int P, int
     const int nl = min(lb, Hf - u0);
     for (int e = tid; e < nl * P; e += nth) {
       const int k = e / nl, line = e - k * nl;
-      buf[(line << logP) + k] = k < Hs ? R[(size_t)k * Hf + u0 + line] : make_float2(0.f, 0.f);
+      buf[(line << logP) + fft_brev(k, logP)] =
+          k < Hs ? R[(size_t)k * Hf + u0 + line] : make_float2(0.f, 0.f);
     }
     __syncthreads();
     smem_fft_lines(buf, nl, P, logP, -1.f, cw, sw);
@@ -606,7 +635,7 @@ __device__ inline void fft2_inverse_cols(const float2* Xb, const float* fac, boo
         f *= -(float)UPH_TWO_PI2 * (d0 * nu * nu + d1 * nw * nw + 2.f * d2 * nu * nw);
       }
       const float2 x = Xb[(size_t)w * Hf + u];
-      buf[(line << logP) + w] = make_float2(f * x.x, f * x.y);
+      buf[(line << logP) + fft_brev(w, logP)] = make_float2(f * x.x, f * x.y);
     }
     __syncthreads();
     smem_fft_lines(buf, nl, P, logP, 1.f, cw, sw);
@@ -636,7 +665,7 @@ __device__ inline void fft2_inverse_rows(const float2* C, int Hs, int Ws, int P,
       else if (k == P / 2) v = make_float2(ci[Hf - 1].x, 0.f);
       else if (k < P / 2) v = ci[k];
       else v = make_float2(ci[P - k].x, -ci[P - k].y);
-      buf[e] = v;
+      buf[(line << logP) + fft_brev(k, logP)] = v;
     }
     __syncthreads();
     smem_fft_lines(buf, nl, P, logP, 1.f, cw, sw);
