@@ -582,10 +582,11 @@ def _batched_measure(args, device):
 
 def _serve_measure(args, rates, device):
     """Serving: the same seeded request pool streamed with Poisson arrivals
-    through the packing server (admitted requests solved as one job through
-    the work-queue engine, mixed precision), through the batched+mixed
-    server (worker contexts overlapping on the device) and through one plain
-    FP32 worker (one request at a time)."""
+    through the packing server (admitted requests solved as one job, mixed
+    precision; its LM loop on the per-chunk engine, and on the work-queue
+    engine), through the batched+mixed server (worker contexts overlapping
+    on the device) and through one plain FP32 worker (one request at a
+    time)."""
     from uniphot_b200.serve import PackedServer, Server, latency_summary, poisson_stream
     from uniphot_b200.synth import make_serving_request
     pool = [make_serving_request(i, device="cuda").fit_kwargs("analytic")
@@ -596,15 +597,17 @@ def _serve_measure(args, rates, device):
                              "sources 5-2000 at the production density, PSF "
                              "polynomial coefficients drawn per request",
            "rates": []}
-    def packed(prec):
-        return PackedServer(device=device, planners=2, engines=2, hbm_budget_bytes=160e9,
-                            precision=prec, engine="queue")
+    def packed(engine):
+        return lambda prec: PackedServer(device=device, planners=2, engines=2,
+                                         hbm_budget_bytes=160e9, precision=prec,
+                                         engine=engine)
 
     def workers(n):
         return lambda prec: Server(device=device, workers=n, hbm_budget_bytes=160e9,
                                    precision=prec)
 
-    forms = (("packed_mixed", "mixed", packed, 2),
+    forms = (("packed_mixed", "mixed", packed("chunks"), 2),
+             ("packed_mixed_queue", "mixed", packed("queue"), 2),
              ("batched_mixed", "mixed", workers(args.serve_workers), args.serve_workers),
              ("one_at_a_time_plain", "plain", workers(1), 1))
     for name, prec, make, warm in forms:

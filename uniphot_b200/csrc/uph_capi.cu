@@ -193,7 +193,7 @@ int uph_create(int device, uph_ctx** out) {
   }
   ctx->own_stream = true;
   if (uph_render_setup() != 0 || uph_solve_setup() != 0 || uph_gram_tc_setup() != 0 ||
-      sparse_setup() != 0) {
+      sparse_setup() != 0 || gal_fft_setup() != 0) {
     cudaStreamDestroy(ctx->stream);
     delete ctx;
     return UPH_ERR_CUDA;
@@ -484,6 +484,8 @@ struct uph_job {
   std::vector<cudaStream_t> streams;
   int* h_active = nullptr;  // pinned, one slot per chunk
   int h_active_cap = 0;
+  int* h_stall = nullptr;   // pinned: per chunk, active and stalled islands
+  int h_stall_cap = 0;
   bool profile = false;
   float ktime[WK_KINDS] = {};
   int64_t kcount[WK_KINDS] = {};
@@ -508,6 +510,7 @@ struct uph_job {
     for (auto* c : chunks) delete c;
     for (auto s : streams) cudaStreamDestroy(s);
     if (h_active) cudaFreeHost(h_active);
+    if (h_stall) cudaFreeHost(h_stall);
     if (d_work) cudaFree(d_work);
   }
 };
@@ -785,6 +788,7 @@ int add_chunk(uph_ctx* ctx, Chunk* ch, const uph_class_desc* cls,
     // galaxy stamps by the Fourier-domain convolution with the pixel PSF
     c.fft_P = fft_pad_for(T);
     c.gfft_floats = gal_fft_floats(T, c.fft_P);
+    c.gfft_smem = gal_fft_smem(T, c.fft_P);
     // concurrent chunks each hold a work space: half an SM's worth of CTAs
     // per chunk keeps the device busy without multiplying the memory
     c.gfft_ctas = (int)std::min<long long>((long long)n * nb * N,
@@ -1326,6 +1330,11 @@ int job_solve_queue(uph_job* job, int max_steps) {
     CK(cudaMallocHost((void**)&job->h_active, sizeof(int) * std::max(nch, nl)), "pinned");
     job->h_active_cap = std::max(nch, nl);
   }
+  if (job->h_stall_cap < 2 * nch) {
+    if (job->h_stall) cudaFreeHost(job->h_stall);
+    CK(cudaMallocHost((void**)&job->h_stall, sizeof(int) * 2 * nch), "pinned");
+    job->h_stall_cap = 2 * nch;
+  }
   LaunchRecords rec;
   auto* recp = job->profile ? &rec : nullptr;
   if (job->profile) {
@@ -1519,23 +1528,35 @@ int job_solve_queue(uph_job* job, int max_steps) {
     ln.inflight = true;
     return UPH_OK;
   };
-  auto finish_lane = [&](int l) {
+  auto finish_lane = [&](int l) -> int {
     QueueLane& ln = job->lanes[l];
     cudaStream_t ls = job->streams[l];
     ln.live = false;
+    // which chunks hold stalled islands (the post-loop probes' subjects)
+    const bool counted = max_steps > 0;
+    if (counted) {
+      for (int i : ln.chunks) {
+        launch_count_active(job->chunks[i]->c, ls);
+        CK(cudaMemcpyAsync(job->h_stall + 2 * i, job->chunks[i]->c.n_active, 2 * sizeof(int),
+                           cudaMemcpyDeviceToHost, ls), "count");
+      }
+      ctx->launches += (int64_t)ln.chunks.size();
+      CK(cudaStreamSynchronize(ls), "count");
+    }
     for (int i : ln.chunks) {
       Chunk* ch = job->chunks[i];
       ch->iters = ln.iters;
       ch->done = true;
       Launcher L{job, ls, recp};
-      post_loop(ch, L);
+      post_loop(ch, L, !counted || job->h_stall[2 * i + 1] > 0);
       cudaEventRecord(ch->ev_done, ls);
     }
+    return UPH_OK;
   };
   int live = 0;
   for (int l = 0; l < nl; ++l) {
     if (!job->lanes[l].live) {
-      finish_lane(l);
+      if ((rc = finish_lane(l))) return rc;
       continue;
     }
     if ((rc = enqueue_group(l))) return rc;
@@ -1552,7 +1573,7 @@ int job_solve_queue(uph_job* job, int max_steps) {
       ln.inflight = false;
       progress = true;
       if (job->h_active[l] == 0 || ln.iters >= max_steps) {
-        finish_lane(l);
+        if ((rc = finish_lane(l))) return rc;
         --live;
       } else if ((rc = enqueue_group(l))) {
         return rc;

@@ -14,7 +14,9 @@
 // times a real factor.
 //
 // The transforms are radix-2 FFTs of whole lines in shared memory (a batch
-// of lines per pass, 32 KB): the T non-zero rows of the padded image, then
+// of lines per pass: as many as the larger of the T rows and the P/2 + 1
+// columns, up to FFT_SMEM_MAX bytes, so a P = 128 grid takes one pass per
+// direction): the T non-zero rows of the padded image, then
 // the P/2 + 1 columns of their half spectra; on the way back the columns,
 // keeping the T rows of the crop, then those rows' real inverses.  One CTA per (island, band, galaxy member), looping over the members
 // of a grid sized to the SM count, with its work space in global memory
@@ -27,7 +29,12 @@ namespace {
 
 constexpr int GT = 256;
 constexpr int MAXP = 512;
-constexpr int FFT_SMEM_BYTES = 32768;      // shared line buffer of the FFTs
+// shared line buffer of the FFTs, at most: three CTAs fit an SM beside their
+// static shared memory
+#ifndef UPH_FFT_SMEM_MAX
+#define UPH_FFT_SMEM_MAX (70 * 1024)
+#endif
+constexpr int FFT_SMEM_MAX = UPH_FFT_SMEM_MAX;
 
 __host__ __device__ inline size_t align64(size_t f) { return (f + 63) & ~(size_t)63; }
 
@@ -41,7 +48,7 @@ __global__ void __launch_bounds__(GT) k_gal_fft(ClassDev c, const float* __restr
   const int tid = threadIdx.x;
   const int T = c.T, PP = c.fft_P, H = PP / 2 + 1;
   const int logP = 31 - __clz(PP);
-  const int lb = FFT_SMEM_BYTES / (8 * PP);
+  const int lb = c.gfft_smem / (8 * PP);
   const int TT = T * T;
   for (int m = tid; m < PP; m += GT) {
     double sn, cs;
@@ -155,6 +162,16 @@ int fft_pad_for(int T) {
   return n;
 }
 
+int gal_fft_smem(int T, int P) {
+  const int lines = std::max(P / 2 + 1, T);
+  return 8 * P * std::min(lines, FFT_SMEM_MAX / (8 * P));
+}
+
+int gal_fft_setup() {
+  return (int)cudaFuncSetAttribute(k_gal_fft, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   FFT_SMEM_MAX);
+}
+
 size_t gal_fft_floats(int T, int P) {
   const size_t H = (size_t)P / 2 + 1;
   // img, R (complex), X (3 complex), Fs (3 real), Cc (complex), each aligned
@@ -164,5 +181,5 @@ size_t gal_fft_floats(int T, int P) {
 
 void launch_gal_fft(const ClassDev& c, const float* P, int phase, cudaStream_t s) {
   if (c.gfft_ctas > 0)
-    k_gal_fft<<<(unsigned)c.gfft_ctas, GT, FFT_SMEM_BYTES, s>>>(c, P, phase);
+    k_gal_fft<<<(unsigned)c.gfft_ctas, GT, (size_t)c.gfft_smem, s>>>(c, P, phase);
 }

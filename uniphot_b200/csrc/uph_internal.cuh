@@ -175,9 +175,11 @@ struct ClassDev {
   // reference render mode with galaxies: the unshifted galaxy stamp and its
   // partials (S, Sx, Sy, S_lr, S_e1, S_e2, S_u) per (island, band, member),
   // (n_isl, nb, N, 7, T, T), from the Fourier-domain convolution; its work
-  // space per resident CTA (gfft_ctas of gfft_floats floats); the pad size
+  // space per resident CTA (gfft_ctas of gfft_floats floats); the pad size;
+  // the shared line buffer's bytes (gal_fft_smem)
   int fft_P;
   int gfft_ctas;
+  int gfft_smem;
   size_t gfft_floats;
   float* gstamp;
   float* gfft_ws;
@@ -529,6 +531,13 @@ __device__ inline int fft_brev(int k, int logP) {
   return (int)(__brev((unsigned)k) >> (32 - logP));
 }
 
+// Lines per pass when L lines go through a buffer of lb lines: the passes
+// split L evenly (65 columns in buffers of 64 lines take 33 + 32, not 64 + 1).
+__device__ inline int fft_pass_lines(int L, int lb) {
+  const int np = (L + lb - 1) / lb;
+  return (L + np - 1) / np;
+}
+
 __device__ inline void fft_bfly(float2& u, float2& v, float wr, float wi) {
   const float tr = wr * v.x - wi * v.y, ti = wr * v.y + wi * v.x;
   const float2 a = u;
@@ -584,8 +593,9 @@ __device__ inline void fft2_forward(const float* img, int Hs, int Ws, int P, int
                                     float2* R, float2* X, float2* buf, int lb,
                                     const float* cw, const float* sw) {
   const int tid = threadIdx.x, nth = blockDim.x, Hf = P / 2 + 1;
-  for (int i0 = 0; i0 < Hs; i0 += lb) {
-    const int nl = min(lb, Hs - i0);
+  const int lr = fft_pass_lines(Hs, lb), lc = fft_pass_lines(Hf, lb);
+  for (int i0 = 0; i0 < Hs; i0 += lr) {
+    const int nl = min(lr, Hs - i0);
     for (int e = tid; e < nl * P; e += nth) {
       const int line = e >> logP, k = e & (P - 1);
       buf[(line << logP) + fft_brev(k, logP)] =
@@ -599,8 +609,8 @@ __device__ inline void fft2_forward(const float* img, int Hs, int Ws, int P, int
     }
     __syncthreads();
   }
-  for (int u0 = 0; u0 < Hf; u0 += lb) {
-    const int nl = min(lb, Hf - u0);
+  for (int u0 = 0; u0 < Hf; u0 += lc) {
+    const int nl = min(lc, Hf - u0);
     for (int e = tid; e < nl * P; e += nth) {
       const int k = e / nl, line = e - k * nl;
       buf[(line << logP) + fft_brev(k, logP)] =
@@ -624,8 +634,9 @@ __device__ inline void fft2_inverse_cols(const float2* Xb, const float* fac, boo
                                          float2* C, float2* buf, int lb, const float* cw,
                                          const float* sw) {
   const int tid = threadIdx.x, nth = blockDim.x, Hf = P / 2 + 1;
-  for (int u0 = 0; u0 < Hf; u0 += lb) {
-    const int nl = min(lb, Hf - u0);
+  const int lc = fft_pass_lines(Hf, lb);
+  for (int u0 = 0; u0 < Hf; u0 += lc) {
+    const int nl = min(lc, Hf - u0);
     for (int e = tid; e < nl * P; e += nth) {
       const int w = e / nl, line = e - w * nl, u = u0 + line;
       float f = fac[(size_t)w * Hf + u];
@@ -655,8 +666,9 @@ __device__ inline void fft2_inverse_rows(const float2* C, int Hs, int Ws, int P,
                                          const float* sw) {
   const int tid = threadIdx.x, nth = blockDim.x, Hf = P / 2 + 1;
   const float inv = 1.f / ((float)P * (float)P);
-  for (int i0 = 0; i0 < Hs; i0 += lb) {
-    const int nl = min(lb, Hs - i0);
+  const int lr = fft_pass_lines(Hs, lb);
+  for (int i0 = 0; i0 < Hs; i0 += lr) {
+    const int nl = min(lr, Hs - i0);
     for (int e = tid; e < nl * P; e += nth) {
       const int line = e >> logP, k = e & (P - 1);
       const float2* ci = C + (size_t)(i0 + line) * Hf;
@@ -682,6 +694,8 @@ void launch_render(const ClassDev& c, const float* P, int phase,
                    cudaStream_t s);
 int fft_pad_for(int T);
 size_t gal_fft_floats(int T, int P);
+int gal_fft_smem(int T, int P);
+int gal_fft_setup();
 void launch_gal_fft(const ClassDev& c, const float* P, int phase, cudaStream_t s);
 void launch_gram_lin(const ClassDev& c, cudaStream_t s);
 void launch_assemble(const ClassDev& c, cudaStream_t s);

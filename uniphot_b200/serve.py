@@ -234,7 +234,7 @@ class PackedServer:
 
     def __init__(self, device: int = 0, planners: int = 2, engines: int = 2,
                  hbm_budget_bytes: float = 160e9, precision: str = "mixed",
-                 max_pack: int = 64, engine: str = "queue", lanes: int = 0,
+                 max_pack: int = 64, engine: str = "chunks", lanes: int = 0,
                  plan_fn: Optional[Callable] = None,
                  pack_fn: Optional[Callable] = None,
                  engine_init: Optional[Callable] = None,
@@ -416,7 +416,7 @@ def default_pack(state: dict, reqs: list) -> list:
     fits = []
     job = _lib.Job(ctx)
     try:
-        job.set_engine(state.get("engine", "queue"), int(state.get("lanes", 0)))
+        job.set_engine(state.get("engine", "chunks"), int(state.get("lanes", 0)))
         for i, (kw, plan) in enumerate(reqs):
             try:
                 if plan is None:
