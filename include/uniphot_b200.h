@@ -17,6 +17,8 @@
  *   uph_upload_psf_mog      <- (no reference counterpart: the analytic PSF of
  *                              the north-star render mode)
  *   uph_upload_sersic_table <- sersic_mog.get_table_jax (sersic_mog.py:59-78)
+ *   uph_upload_exp_mog      <- source_model.EXP_AMP / EXP_VAR (source_model.py:
+ *                              56-75), the "direct" backend's mixture
  *   uph_run_chunk           <- run_class_chunk (island_solver.py:2793-3131)
  *                              for the legacy/clip/proposals step protocol
  */
@@ -130,7 +132,19 @@ typedef struct uph_class_desc {
                                (island_solver.py:1795-1818, 2781-2790), in
                                a private copy of the window, before the
                                solve; needs uph_chunk_in.member_s1_flux   */
+  int32_t render_direct;    /* reference render mode: EXP galaxies by the
+                               legacy "direct" backend (source_model.py:
+                               218-256, 298-303): the exponential mixture
+                               of uph_upload_exp_mog at pixel centres, unit
+                               sum, convolved ("same") with the PSF stamp
+                               and renormalised to unit sum, in float64;
+                               position partials through the PSF's spatial
+                               variation, shape partials by float64 central
+                               differences (step 1e-6).  STAR and EXP
+                               members only; tiers up to UPH_DIRECT_MAX_T */
 } uph_class_desc;
+
+#define UPH_DIRECT_MAX_T 111
 
 /* log-radius offsets of the Re profile (the reference's REPROF_DELTAS_LN,
  * island_plan.py:58-60) */
@@ -274,6 +288,10 @@ int uph_upload_psf_poly(uph_ctx* ctx, int32_t tier, const float* coefs,
 int uph_upload_psf_mog(uph_ctx* ctx, const float* params,
                        const float* origin_scale, int32_t n_bands, int32_t K,
                        int32_t nt);
+
+/* The "direct" backend's exponential mixture: k amplitudes and variances
+ * (unit effective radius), float32. */
+int uph_upload_exp_mog(uph_ctx* ctx, const float* amp, const float* var, int32_t k);
 
 /* Sersic MoG table: knots [n_knots], amps/log_vars [n_knots*kmax], core
  * [n_knots], all float64. */

@@ -118,13 +118,22 @@ def test_catalog_errors_propagate_to_the_catalog_frame():
     assert np.isnan(e["sersic_n_prior_frac"][0]) and np.isnan(e["pos_x_prior_frac"][1])
 
 
-def test_direct_backend_galaxies_raise_in_reference_mode():
-    with pytest.raises(ValueError, match="not supported"):
-        solver.make_class_kernels(_plan("mixed"), 3, 1, **dict(KW, render_backend="direct"),
+def test_direct_backend_sets_the_descriptor_in_reference_mode():
+    """render_backend="direct" selects the legacy EXP backend for the
+    pixelised-PSF render (the device checks the members are STAR or EXP);
+    the analytic render has no backend choice."""
+    k = solver.make_class_kernels(_plan("mixed"), 3, 1, **dict(KW, render_backend="direct"),
                                   render_mode="reference")
+    assert k.desc.render_mode == 0 and k.desc.render_direct == 1
     k = solver.make_class_kernels(_plan("star"), 3, 1, **dict(KW, render_backend="direct"),
                                   render_mode="reference")
-    assert k.desc.render_mode == 0
+    assert k.desc.render_mode == 0 and k.desc.render_direct == 1
+    k = solver.make_class_kernels(_plan("mixed"), 3, 1, **dict(KW, render_backend="fft"),
+                                  render_mode="reference")
+    assert k.desc.render_direct == 0
+    k = solver.make_class_kernels(_plan("mixed"), 3, 1, **dict(KW, render_backend="direct"),
+                                  render_mode="analytic")
+    assert k.desc.render_direct == 0
 
 
 def test_scene_subtract_sets_the_descriptor_and_needs_s1_fluxes():

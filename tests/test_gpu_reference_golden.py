@@ -23,16 +23,21 @@ pytestmark = pytest.mark.gpu
 GOLDEN = Path(__file__).parent / "golden"
 
 
-def test_island_fit_matches_the_reference_solver():
+@pytest.mark.parametrize("case,extra", [("small", {}),
+                                        ("small_direct", {"render_backend": "direct"})])
+def test_island_fit_matches_the_reference_solver(case, extra):
+    """The "fft" backend (default) and the legacy EXP "direct" backend
+    (source_model.py:218-256, 298-303; float64 convolution on the device)
+    against the reference's island_fit with the same backend."""
     from test_golden_reference_solver import _digest
     from uniphot_b200.solver import island_fit
     from uniphot_b200.synth import make_small_field
     f = make_small_field(0)
-    ref = dict(np.load(GOLDEN / "solver_small.npz"))
+    ref = dict(np.load(GOLDEN / f"solver_{case}.npz"))
     assert str(ref.pop("digest")) == _digest(f)
     order = np.argsort(ref["source_idx"])
     ref = {k: v[order] for k, v in ref.items()}
-    res = island_fit(**f.fit_kwargs("reference"))
+    res = island_fit(**f.fit_kwargs("reference"), **extra)
     go = np.argsort(res.source_idx)
     np.testing.assert_array_equal(res.source_idx[go], ref["source_idx"])
     np.testing.assert_array_equal(res.n_steps[go], ref["n_steps"])

@@ -30,7 +30,7 @@ EXPORTED = ("uph_create", "uph_destroy", "uph_last_error", "uph_set_stream",
             "uph_job_set_profile", "uph_job_kernel_time", "uph_job_kernel_work",
             "uph_job_chunk_time", "uph_sparse_band_solve", "uph_island_roots",
             "uph_set_island_retry_limit", "uph_job_kernel_exps", "uph_measure_peaks",
-            "uph_job_set_engine")
+            "uph_job_set_engine", "uph_upload_exp_mog")
 KERNEL_KINDS = ("render", "gram", "assemble", "step", "trial_chi2", "accept",
                 "gram_tc")
 
@@ -49,7 +49,8 @@ class ClassDesc(C.Structure):
                 ("tc_cond_max", C.c_float), ("step_tr", C.c_int32),
                 ("param_errors", C.c_int32), ("flux_marg", C.c_int32),
                 ("source_metrics", C.c_int32), ("re_profile", C.c_int32),
-                ("residual", C.c_int32), ("scene_subtract", C.c_int32)]
+                ("residual", C.c_int32), ("scene_subtract", C.c_int32),
+                ("render_direct", C.c_int32)]
 
 
 class ChunkIn(C.Structure):
@@ -145,6 +146,7 @@ def lib():
         L.uph_job_kernel_exps.argtypes = [_P, C.c_int32, C.POINTER(C.c_double)]
         L.uph_job_set_engine.argtypes = [_P, C.c_int32, C.c_int32]
         L.uph_measure_peaks.argtypes = [_P, C.POINTER(C.c_double)]
+        L.uph_upload_exp_mog.argtypes = [_P, _P, _P, C.c_int32]
         _lib = L
     return _lib
 
@@ -317,6 +319,13 @@ class Context:
         self.check(lib().uph_upload_psf_poly(self._h, int(tier), ptr(cf), ptr(os_),
                                              cf.shape[0], cf.shape[-1]),
                    "uph_upload_psf_poly")
+
+    def upload_exp_mog(self, amp: np.ndarray, var: np.ndarray):
+        """The "direct" backend's exponential mixture (uph_upload_exp_mog)."""
+        a = np.ascontiguousarray(amp, np.float32)
+        v = np.ascontiguousarray(var, np.float32)
+        self.check(lib().uph_upload_exp_mog(self._h, ptr(a), ptr(v), int(a.size)),
+                   "uph_upload_exp_mog")
 
     def upload_psf_mog(self, params: np.ndarray, origin_scale: np.ndarray):
         pr = np.ascontiguousarray(params, np.float32)

@@ -91,6 +91,9 @@ struct uph_ctx {
   int mog_k = 0, mog_nt = 0, mog_nb = 0;
   // table
   SBuf tb_knots, tb_amps, tb_lv, tb_core;
+  // the "direct" backend's exponential mixture
+  SBuf exp_amp, exp_var;
+  int exp_k = 0;
   int tb_n = 0, tb_k = 0;
   double tb_nmin = 0, tb_nmax = 0;
   int* h_active = nullptr;  // pinned
@@ -221,6 +224,8 @@ int uph_destroy(uph_ctx* ctx) {
   ctx->tb_amps.reset();
   ctx->tb_lv.reset();
   ctx->tb_core.reset();
+  ctx->exp_amp.reset();
+  ctx->exp_var.reset();
   for (auto& b : ctx->sp) b.release();
   for (auto& b : ctx->isl) b.release();
   for (auto& ev : ctx->ev)
@@ -386,6 +391,23 @@ int uph_upload_sersic_table(uph_ctx* ctx, const double* knots,
   ctx->tb_k = kmax;
   ctx->tb_nmin = nmin;
   ctx->tb_nmax = nmax;
+  return UPH_OK;
+}
+
+int uph_upload_exp_mog(uph_ctx* ctx, const float* amp, const float* var, int32_t k) {
+  if (!ctx) return UPH_ERR_INVALID;
+  if (!amp || !var || k <= 0 || k > UPH_MAXGAL)
+    return set_err(ctx, UPH_ERR_INVALID, "invalid exponential mixture (%d components)", k);
+  cudaSetDevice(ctx->device);
+  int rc = ensure_shared(ctx, ctx->exp_amp, sizeof(float) * k, "exp mixture");
+  if (!rc) rc = ensure_shared(ctx, ctx->exp_var, sizeof(float) * k, "exp mixture");
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(sptr(ctx->exp_amp), amp, sizeof(float) * k, cudaMemcpyHostToDevice,
+                     ctx->stream), "exp mixture");
+  CK(cudaMemcpyAsync(sptr(ctx->exp_var), var, sizeof(float) * k, cudaMemcpyHostToDevice,
+                     ctx->stream), "exp mixture");
+  CK(cudaStreamSynchronize(ctx->stream), "exp mixture");
+  ctx->exp_k = k;
   return UPH_OK;
 }
 
@@ -624,7 +646,22 @@ int add_chunk(uph_ctx* ctx, Chunk* ch, const uph_class_desc* cls,
       return set_err(ctx, UPH_ERR_INVALID, "island %d window outside the padded field", i);
   }
   if (nLmax > UPH_MAXLIVE) return set_err(ctx, UPH_ERR_INVALID, "too many live parameters");
-  if (any_gal && mode == UPH_RENDER_REFERENCE && fft_pad_for(T) > 512)
+  if (cls->render_direct && mode != UPH_RENDER_REFERENCE)
+    return set_err(ctx, UPH_ERR_INVALID, "render_direct needs the reference render mode");
+  const bool direct = cls->render_direct && any_gal;
+  if (direct) {
+    for (int i = 0; i < n; ++i)
+      for (int k = 0; k < nr[i]; ++k)
+        if (in->stype[(size_t)i * N + k] > 1)
+          return set_err(ctx, UPH_ERR_INVALID,
+                         "the direct backend renders STAR and EXP sources only");
+    if (T > UPH_DIRECT_MAX_T)
+      return set_err(ctx, UPH_ERR_INVALID, "the direct backend takes tiers up to %d (tier %d)",
+                     UPH_DIRECT_MAX_T, T);
+    if (!sptr(ctx->exp_amp) || ctx->exp_k <= 0)
+      return set_err(ctx, UPH_ERR_STATE, "no exponential mixture uploaded");
+  }
+  if (any_gal && !direct && mode == UPH_RENDER_REFERENCE && fft_pad_for(T) > 512)
     return set_err(ctx, UPH_ERR_INVALID,
                    "reference-mode galaxies: tier %d needs a Fourier grid above 512", T);
   if (any_gal && !sptr(ctx->tb_knots))
@@ -785,10 +822,19 @@ int add_chunk(uph_ctx* ctx, Chunk* ch, const uph_class_desc* cls,
   if (cls->param_errors || cls->flux_marg || cls->re_profile)
     c.flsave = cbuf<uint8_t>(ctx, ch, "flsave", n, &rc);
   if (any_gal && mode == UPH_RENDER_REFERENCE) {
-    // galaxy stamps by the Fourier-domain convolution with the pixel PSF
+    // galaxy stamps by the Fourier-domain convolution with the pixel PSF,
+    // or by the direct backend's float64 convolution
     c.fft_P = fft_pad_for(T);
-    c.gfft_floats = gal_fft_floats(T, c.fft_P);
-    c.gfft_smem = gal_fft_smem(T, c.fft_P);
+    c.gfft_floats = direct ? gal_direct_floats(T) : gal_fft_floats(T, c.fft_P);
+    c.gfft_smem = direct ? gal_direct_smem(T) : gal_fft_smem(T, c.fft_P);
+    c.gdirect = direct ? 1 : 0;
+    if (direct) {
+      c.exp_k = ctx->exp_k;
+      c.exp_amp = (const float*)sptr(ctx->exp_amp);
+      c.exp_var = (const float*)sptr(ctx->exp_var);
+      ch->bound.push_back(ctx->exp_amp);
+      ch->bound.push_back(ctx->exp_var);
+    }
     // concurrent chunks each hold a work space: half an SM's worth of CTAs
     // per chunk keeps the device busy without multiplying the memory
     c.gfft_ctas = (int)std::min<long long>((long long)n * nb * N,

@@ -181,6 +181,12 @@ struct ClassDev {
   int gfft_ctas;
   int gfft_smem;
   size_t gfft_floats;
+  // the legacy "direct" backend instead of the Fourier-domain convolution
+  // (EXP members only): its exponential mixture
+  int gdirect;
+  int exp_k;
+  const float* exp_amp;
+  const float* exp_var;
   float* gstamp;
   float* gfft_ws;
   float* bgout;            // (n_isl, nb, 3) final background coefficients
@@ -696,6 +702,8 @@ int fft_pad_for(int T);
 size_t gal_fft_floats(int T, int P);
 int gal_fft_smem(int T, int P);
 int gal_fft_setup();
+size_t gal_direct_floats(int T);
+int gal_direct_smem(int T);
 void launch_gal_fft(const ClassDev& c, const float* P, int phase, cudaStream_t s);
 void launch_gram_lin(const ClassDev& c, cudaStream_t s);
 void launch_assemble(const ClassDev& c, cudaStream_t s);

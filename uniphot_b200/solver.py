@@ -174,6 +174,13 @@ class DeviceField:
                 self.ctx.upload_psf_mog(tree.params, tree.origin_scale)
                 self._mog_key = key
 
+    def ensure_exp_mog(self):
+        if not getattr(self, "_exp_mog", False):
+            from .sparse import exp_mixture
+            amp, var = exp_mixture()
+            self.ctx.upload_exp_mog(amp, var)
+            self._exp_mog = True
+
     def ensure_table(self):
         if not self._table:
             self.ctx.upload_sersic_table(load_table())
@@ -234,10 +241,6 @@ def make_class_kernels(plan, n_bands: int, n_terms: int, *, render_backend: str,
     unsupported = []
     # star-only classes keep the clip step (island_solver.py:1910-1912)
     step_eff = str(step_mode) if str(plan.kind) != "star" else "clip"
-    if render_mode == "reference" and render_backend == "direct" and plan.kind != "star":
-        # the legacy EXP-only direct-convolution backend (source_model.py:
-        # 298-303); galaxies render through the "fft" backend here
-        unsupported.append("render_backend='direct' for galaxies")
     if crossband is not None:
         unsupported.append("crossband")
     if unsupported:
@@ -258,7 +261,10 @@ def make_class_kernels(plan, n_bands: int, n_terms: int, *, render_backend: str,
         plateau_dlnp_tol=float(plateau_dlnp_tol),
         bg_joint=int(bg_mode == "joint"), tc_cond_max=float(tc_cond_max),
         scene_subtract=int(bool(scene_subtract)),
-        step_tr=int(step_eff == "trust_region"))
+        step_tr=int(step_eff == "trust_region"),
+        # the legacy EXP-only direct-convolution backend (source_model.py:
+        # 218-256, 298-303); STAR renders the same in both backends
+        render_direct=int(render_mode == "reference" and render_backend == "direct"))
     return ClassKernels(desc, render_mode, int(n_bands), str(plan.kind),
                         step_protocol="dlnp" if convergence == "dlnp"
                         else str(stall_count_mode), step_mode=step_eff)
@@ -296,6 +302,8 @@ def run_class_chunk(kernels: ClassKernels, psf_tree: PsfTree, host: dict,
     dstack_dev.ensure_psf(psf_tree)
     if np.any(np.asarray(host["st"])[rows] != SOURCE_STAR):
         dstack_dev.ensure_table()
+        if kernels.desc.render_direct:
+            dstack_dev.ensure_exp_mog()
     N = int(host["mmask"].shape[1])
     arrays = _slice_host(host, rows, bool(kernels.desc.scene_subtract))
     init = None
@@ -559,6 +567,8 @@ class IslandFitJob:
             field.ensure_psf(tree)
             if np.any(np.asarray(host["st"]) != SOURCE_STAR):
                 field.ensure_table()
+                if render_backend == "direct" and render_mode == "reference":
+                    field.ensure_exp_mog()
             kern = make_class_kernels(
                 plan, n_bands, n_terms, render_backend=render_backend, reg=reg,
                 pos_step_max_pix=pos_step_max_pix, chi2_ftol_rel=chi2_ftol_rel,
