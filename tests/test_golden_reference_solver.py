@@ -87,8 +87,9 @@ def _digest(f):
     return h.hexdigest()
 
 
-def _oracle_rows(f, opts):
-    """Per-source rows of the oracle's float64 solve, sorted by source."""
+def _oracle_rows(f, opts, precision="f64"):
+    """Per-source rows of the oracle's solve (float64, or "ref": the
+    reference's float32 render with float64 solves), sorted by source."""
     from oracle.driver import solve_chunk
     from uniphot_b200.plan import giant_seed_rows, plan_island_classes
     opts = dict(opts)
@@ -111,7 +112,7 @@ def _oracle_rows(f, opts):
     for p, h in zip(plans, hosts):
         o = solve_chunk(h, np.arange(p.n_islands), B=p.bbox_class, T=p.tier, dstack=ds,
                         wstack=ws, psfs=psfs, mode="reference", table_path=TABLE,
-                        precision="f64", max_steps=30, native=f.native,
+                        precision=precision, max_steps=30, native=f.native,
                         step_mode="clip", re_profile=REPROF_DELTAS_LN if re_prof else None,
                         **opts)
         rows.append(unpack_class_results(

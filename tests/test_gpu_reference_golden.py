@@ -23,21 +23,16 @@ pytestmark = pytest.mark.gpu
 GOLDEN = Path(__file__).parent / "golden"
 
 
-@pytest.mark.parametrize("case,extra", [("small", {}),
-                                        ("small_direct", {"render_backend": "direct"})])
-def test_island_fit_matches_the_reference_solver(case, extra):
-    """The "fft" backend (default) and the legacy EXP "direct" backend
-    (source_model.py:218-256, 298-303; float64 convolution on the device)
-    against the reference's island_fit with the same backend."""
+def test_island_fit_matches_the_reference_solver():
     from test_golden_reference_solver import _digest
     from uniphot_b200.solver import island_fit
     from uniphot_b200.synth import make_small_field
     f = make_small_field(0)
-    ref = dict(np.load(GOLDEN / f"solver_{case}.npz"))
+    ref = dict(np.load(GOLDEN / "solver_small.npz"))
     assert str(ref.pop("digest")) == _digest(f)
     order = np.argsort(ref["source_idx"])
     ref = {k: v[order] for k, v in ref.items()}
-    res = island_fit(**f.fit_kwargs("reference"), **extra)
+    res = island_fit(**f.fit_kwargs("reference"))
     go = np.argsort(res.source_idx)
     np.testing.assert_array_equal(res.source_idx[go], ref["source_idx"])
     np.testing.assert_array_equal(res.n_steps[go], ref["n_steps"])
@@ -111,3 +106,55 @@ def test_island_fit_free_sersic_index_matches_the_reference_solver(case, extra):
     df = np.abs(fl - ref["fluxes"])
     assert np.all((df <= 2e-4 * np.abs(ref["fluxes"])) | (df <= 0.02 * ref["flux_err"])), \
         f"worst {np.max(df / ref['flux_err']):.3g} sigma"
+
+
+def test_island_fit_direct_backend_matches_the_oracle_and_the_reference():
+    """The legacy EXP "direct" render backend (source_model.py:218-256,
+    298-303: the exponential mixture at pixel centres convolved with the PSF
+    stamp, renormalised; float64 convolution on the device) on the small
+    field.  Against the oracle at the reference's precision (float32 render,
+    float64 solves; its direct stamps in float64 as here): identical LM
+    iteration counts and converged / stalled / diverged flags on every
+    source, fluxes within 1e-4 relative or 0.01 sigma, positions within
+    1e-3 px.  Against the reference's own island_fit(render_backend=
+    "direct") (float64): the small-field bar, except on the one singleton EXP
+    galaxy where float32 and float64 part at the optimum (the float32
+    oracle and the device stop stalled after 7 steps, float64 converges
+    after 4, at the same chi2, 39410.04): there chi2 must agree within 1e-6
+    relative."""
+    from test_golden_reference_solver import _digest, _oracle_rows
+    from uniphot_b200.solver import island_fit
+    from uniphot_b200.synth import make_small_field
+    f = make_small_field(0)
+    ref = dict(np.load(GOLDEN / "solver_small_direct.npz"))
+    assert str(ref.pop("digest")) == _digest(f)
+    order = np.argsort(ref["source_idx"])
+    ref = {k: v[order] for k, v in ref.items()}
+    res = island_fit(**f.fit_kwargs("reference"), render_backend="direct")
+    go = np.argsort(res.source_idx)
+    np.testing.assert_array_equal(res.source_idx[go], ref["source_idx"])
+    assert np.any(f.source_type == 1)
+    # the oracle at the reference's precision
+    orc = _oracle_rows(f, dict(render_backend="direct"), precision="ref")
+    np.testing.assert_array_equal(orc["src"], ref["source_idx"])
+    np.testing.assert_array_equal(res.n_steps[go], orc["n_steps"])
+    for k in ("converged", "stalled", "diverged"):
+        np.testing.assert_array_equal(getattr(res, k)[go], orc[k], err_msg=k)
+    np.testing.assert_allclose(res.pos_x[go], orc["pos_x"], atol=1e-3)
+    np.testing.assert_allclose(res.pos_y[go], orc["pos_y"], atol=1e-3)
+    d = np.abs(res.fluxes[go].astype(np.float64) - orc["fluxes"])
+    assert np.all((d <= 1e-4 * np.abs(orc["fluxes"])) | (d <= 0.01 * orc["flux_err"])), \
+        f"worst {np.max(d / orc['flux_err']):.3g} sigma vs the oracle"
+    # the reference (float64)
+    diff = res.n_steps[go] != ref["n_steps"]
+    for k in ("converged", "stalled", "diverged"):
+        diff |= getattr(res, k)[go] != ref[k]
+    assert diff.sum() <= 1, f"{diff.sum()} sources differ from the reference"
+    assert np.all(ref["island_nsrc"][diff] == 1)
+    np.testing.assert_allclose(res.chi2[go][diff], ref["chi2"][diff], rtol=1e-6)
+    np.testing.assert_allclose(res.pos_x[go], ref["pos_x"], atol=2e-3)
+    np.testing.assert_allclose(res.pos_y[go], ref["pos_y"], atol=2e-3)
+    df = np.abs(res.fluxes[go].astype(np.float64) - ref["fluxes"])
+    assert np.all((df <= 2e-4 * np.abs(ref["fluxes"])) | (df <= 0.02 * ref["flux_err"])), \
+        f"worst {np.max(df / ref['flux_err']):.3g} sigma"
+    np.testing.assert_allclose(res.flux_err[go], ref["flux_err"], rtol=1e-3)
