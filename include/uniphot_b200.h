@@ -17,6 +17,8 @@
  *   uph_upload_psf_mog      <- (no reference counterpart: the analytic PSF of
  *                              the north-star render mode)
  *   uph_upload_sersic_table <- sersic_mog.get_table_jax (sersic_mog.py:59-78)
+ *   uph_subtract_tile_backgrounds <- the padded field stacks' frozen per-tile
+ *                              background subtraction (island_stage.py:1728-1751)
  *   uph_upload_exp_mog      <- source_model.EXP_AMP / EXP_VAR (source_model.py:
  *                              56-75), the "direct" backend's mixture
  *   uph_run_chunk           <- run_class_chunk (island_solver.py:2793-3131)
@@ -288,6 +290,23 @@ int uph_upload_psf_poly(uph_ctx* ctx, int32_t tier, const float* coefs,
 int uph_upload_psf_mog(uph_ctx* ctx, const float* params,
                        const float* origin_scale, int32_t n_bands, int32_t K,
                        int32_t nt);
+
+/* Field-stack build: subtract each pass-1 tile's frozen planar background
+ * from the context's uploaded data stack, on the device (the reference does
+ * it on the host, island_stage.py:1728-1751).  tiles: n_tiles x (x0, y0,
+ * x1, y1) core rectangles in unpadded pixels, applied in order; coefs:
+ * (n_tiles, n_bands, M) float32 with M = 1, 3, 6 for order 0, 1, 2 and the
+ * terms of make_bg_basis (bg_polynomial.py:125-178): 1, X, Y, X^2, XY,
+ * Y^2 with X = (x - x_origin) / x_scale, Y = (y - y_origin) / y_scale in
+ * float64, each term rounded to float32, the sum in float32; norm =
+ * (x_origin, x_scale, y_origin, y_scale).  The field must not be held by a
+ * live job (UPH_ERR_STATE): upload it, subtract, then add chunks. */
+int uph_subtract_tile_backgrounds(uph_ctx* ctx, int32_t n_tiles, const int32_t* tiles,
+                                  const float* coefs, int32_t order, const double* norm);
+
+/* Copy the context's padded field stacks (n_bands, Hp, Wp) float32 to host
+ * buffers (either may be NULL). */
+int uph_download_field(uph_ctx* ctx, float* data, float* invvar);
 
 /* The "direct" backend's exponential mixture: k amplitudes and variances
  * (unit effective radius), float32. */

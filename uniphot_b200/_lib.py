@@ -30,7 +30,8 @@ EXPORTED = ("uph_create", "uph_destroy", "uph_last_error", "uph_set_stream",
             "uph_job_set_profile", "uph_job_kernel_time", "uph_job_kernel_work",
             "uph_job_chunk_time", "uph_sparse_band_solve", "uph_island_roots",
             "uph_set_island_retry_limit", "uph_job_kernel_exps", "uph_measure_peaks",
-            "uph_job_set_engine", "uph_upload_exp_mog")
+            "uph_job_set_engine", "uph_upload_exp_mog", "uph_subtract_tile_backgrounds",
+            "uph_download_field")
 KERNEL_KINDS = ("render", "gram", "assemble", "step", "trial_chi2", "accept",
                 "gram_tc")
 
@@ -147,6 +148,8 @@ def lib():
         L.uph_job_set_engine.argtypes = [_P, C.c_int32, C.c_int32]
         L.uph_measure_peaks.argtypes = [_P, C.POINTER(C.c_double)]
         L.uph_upload_exp_mog.argtypes = [_P, _P, _P, C.c_int32]
+        L.uph_subtract_tile_backgrounds.argtypes = [_P, C.c_int32, _P, _P, C.c_int32, _P]
+        L.uph_download_field.argtypes = [_P, _P, _P]
         _lib = L
     return _lib
 
@@ -319,6 +322,28 @@ class Context:
         self.check(lib().uph_upload_psf_poly(self._h, int(tier), ptr(cf), ptr(os_),
                                              cf.shape[0], cf.shape[-1]),
                    "uph_upload_psf_poly")
+
+    def subtract_tile_backgrounds(self, tiles, coefs, order: int, norm):
+        """Subtract each tile's planar background from the uploaded data
+        stack (uph_subtract_tile_backgrounds): tiles (n, 4) = (x0, y0, x1,
+        y1) cores, coefs (n, n_bands, M), norm = (x_origin, x_scale,
+        y_origin, y_scale)."""
+        t = np.ascontiguousarray(np.asarray(tiles, np.int32).reshape(-1, 4))
+        c = np.ascontiguousarray(coefs, np.float32)
+        nm = np.ascontiguousarray(np.asarray(norm, np.float64).reshape(4))
+        if c.shape[0] != t.shape[0]:
+            raise ValueError(f"{t.shape[0]} tiles but coefficients for {c.shape[0]}")
+        self.check(lib().uph_subtract_tile_backgrounds(self._h, int(t.shape[0]), ptr(t), ptr(c),
+                                                       int(order), ptr(nm)),
+                   "uph_subtract_tile_backgrounds")
+
+    def download_field(self, shape) -> tuple:
+        """The padded (data, invvar) stacks of the given (n_bands, Hp, Wp)
+        shape, copied to the host."""
+        d = np.empty(shape, np.float32)
+        w = np.empty(shape, np.float32)
+        self.check(lib().uph_download_field(self._h, ptr(d), ptr(w)), "uph_download_field")
+        return d, w
 
     def upload_exp_mog(self, amp: np.ndarray, var: np.ndarray):
         """The "direct" backend's exponential mixture (uph_upload_exp_mog)."""

@@ -14,7 +14,7 @@ PKG = HERE.parent
 LIB = PKG / "libuniphot_b200.so"
 SOURCES = ["uph_render.cu", "uph_solve.cu", "uph_gram_tc.cu", "uph_capi.cu",
            "uph_noalloc.cu", "uph_galfft.cu", "uph_sparse.cu", "uph_islands.cu",
-           "uph_peaks.cu"]
+           "uph_peaks.cu", "uph_stacks.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo",
          "-std=c++17", "-Xcompiler", "-fPIC", "-shared",

@@ -97,6 +97,7 @@ struct uph_ctx {
   int tb_n = 0, tb_k = 0;
   double tb_nmin = 0, tb_nmax = 0;
   int* h_active = nullptr;  // pinned
+  DevBuf bgc;               // per-tile background coefficients (stack build)
   cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
   float timing[4] = {0, 0, 0, 0};
   int64_t launches = 0;
@@ -227,6 +228,7 @@ int uph_destroy(uph_ctx* ctx) {
   ctx->exp_amp.reset();
   ctx->exp_var.reset();
   for (auto& b : ctx->sp) b.release();
+  ctx->bgc.release();
   for (auto& b : ctx->isl) b.release();
   for (auto& ev : ctx->ev)
     if (ev) cudaEventDestroy(ev);
@@ -391,6 +393,57 @@ int uph_upload_sersic_table(uph_ctx* ctx, const double* knots,
   ctx->tb_k = kmax;
   ctx->tb_nmin = nmin;
   ctx->tb_nmax = nmax;
+  return UPH_OK;
+}
+
+int uph_subtract_tile_backgrounds(uph_ctx* ctx, int32_t n_tiles, const int32_t* tiles,
+                                  const float* coefs, int32_t order, const double* norm) {
+  if (!ctx) return UPH_ERR_INVALID;
+  if (!sptr(ctx->dstack)) return set_err(ctx, UPH_ERR_STATE, "no field uploaded");
+  if (ctx->dstack.use_count() > 1)
+    return set_err(ctx, UPH_ERR_STATE,
+                   "the field is held by a live job's chunks: upload it again to change it");
+  if (n_tiles < 0 || (n_tiles > 0 && (!tiles || !coefs)) || !norm || order < 0 || order > 2)
+    return set_err(ctx, UPH_ERR_INVALID, "invalid tile backgrounds (%d tiles, order %d)",
+                   n_tiles, order);
+  if (norm[1] == 0.0 || norm[3] == 0.0)
+    return set_err(ctx, UPH_ERR_INVALID, "zero background normalisation scale");
+  const int M = order == 0 ? 1 : (order == 1 ? 3 : 6);
+  const int H = ctx->Hp - 2 * ctx->pad, W = ctx->Wp - 2 * ctx->pad;
+  for (int t = 0; t < n_tiles; ++t) {
+    const int* r = tiles + 4 * (size_t)t;
+    if (r[0] < 0 || r[1] < 0 || r[2] < r[0] || r[3] < r[1] || r[2] > W || r[3] > H)
+      return set_err(ctx, UPH_ERR_INVALID, "tile %d core (%d, %d, %d, %d) outside the %d x %d field",
+                     t, r[0], r[1], r[2], r[3], W, H);
+  }
+  if (n_tiles == 0) return UPH_OK;
+  cudaSetDevice(ctx->device);
+  const size_t bytes = sizeof(float) * (size_t)n_tiles * ctx->nb * M;
+  int rc = ensure(ctx, ctx->bgc, bytes, "tile backgrounds");
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(ctx->bgc.ptr, coefs, bytes, cudaMemcpyHostToDevice, ctx->stream),
+     "tile backgrounds");
+  for (int t = 0; t < n_tiles; ++t) {
+    const int* r = tiles + 4 * (size_t)t;
+    launch_tile_bg_subtract((float*)sptr(ctx->dstack), ctx->nb, ctx->Hp, ctx->Wp, ctx->pad, r[0],
+                            r[1], r[2] - r[0], r[3] - r[1],
+                            (const float*)ctx->bgc.ptr + (size_t)t * ctx->nb * M, M, norm,
+                            ctx->sm_count, ctx->stream);
+  }
+  CK(cudaGetLastError(), "tile backgrounds");
+  CK(cudaStreamSynchronize(ctx->stream), "tile backgrounds");
+  return UPH_OK;
+}
+
+int uph_download_field(uph_ctx* ctx, float* data, float* invvar) {
+  if (!ctx) return UPH_ERR_INVALID;
+  if (!sptr(ctx->dstack)) return set_err(ctx, UPH_ERR_STATE, "no field uploaded");
+  cudaSetDevice(ctx->device);
+  const size_t bytes = sizeof(float) * (size_t)ctx->nb * ctx->Hp * ctx->Wp;
+  int rc = download(ctx, data, sptr(ctx->dstack), bytes, "field");
+  if (!rc) rc = download(ctx, invvar, sptr(ctx->wstack), bytes, "field");
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(ctx->stream), "field");
   return UPH_OK;
 }
 

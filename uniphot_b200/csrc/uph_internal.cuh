@@ -703,6 +703,9 @@ size_t gal_fft_floats(int T, int P);
 int gal_fft_smem(int T, int P);
 int gal_fft_setup();
 size_t gal_direct_floats(int T);
+void launch_tile_bg_subtract(float* stack, int nb, int Hp, int Wp, int pad, int x0, int y0,
+                             int w, int h, const float* coefs, int M, const double* norm,
+                             int sms, cudaStream_t s);
 int gal_direct_smem(int T);
 void launch_gal_fft(const ClassDev& c, const float* P, int phase, cudaStream_t s);
 void launch_gram_lin(const ClassDev& c, cudaStream_t s);

@@ -1,0 +1,62 @@
+// Field-stack build on the device: the frozen per-tile planar background of
+// pass 1 subtracted from the padded data stack (island_stage.py:1728-1751,
+// there numpy on the host).  Over each tile's core rectangle [x0, x1) x
+// [y0, y1) (unpadded pixels) and every band,
+//
+//   stack[b, pad + y, pad + x] -= sum_m basis_m(x, y) * coefs[t, b, m],
+//
+// with basis_m = X^i Y^j in the term order of make_bg_basis
+// (bg_polynomial.py:125-178): X = (x - x_origin) / x_scale and Y likewise in
+// float64, each product rounded once to float32, the sum over m in float32
+// in term order.  Tiles are applied one launch after another, so
+// overlapping cores subtract in tile order as the host loop does.
+// Elementwise and HBM-bound: a grid-stride loop over (band, row, column) of
+// the tile, consecutive threads on consecutive columns.
+
+#include <algorithm>
+
+#include "uph_internal.cuh"
+
+namespace {
+
+constexpr int ST = 256;
+
+// (i, j) exponents of X and Y per term, orders 0, 1, 2
+__constant__ int kTermX[6] = {0, 1, 0, 2, 1, 0};
+__constant__ int kTermY[6] = {0, 0, 1, 0, 1, 2};
+
+__device__ inline double ipow(double v, int e) { return e == 0 ? 1.0 : (e == 1 ? v : v * v); }
+
+__global__ void __launch_bounds__(ST) k_tile_bg_subtract(float* __restrict__ stack, int nb, int Hp,
+                                                         int Wp, int pad, int x0, int y0, int w,
+                                                         int h, const float* __restrict__ coefs,
+                                                         int M, double xo, double xs, double yo,
+                                                         double ys) {
+  const size_t n = (size_t)nb * h * w;
+  for (size_t e = (size_t)blockIdx.x * ST + threadIdx.x; e < n; e += (size_t)gridDim.x * ST) {
+    const int c = (int)(e % w);
+    const int r = (int)((e / w) % h);
+    const int b = (int)(e / ((size_t)w * h));
+    const double X = ((double)(x0 + c) - xo) / xs;
+    const double Y = ((double)(y0 + r) - yo) / ys;
+    float bg = 0.f;
+    for (int m = 0; m < M; ++m) {
+      const float basis = (float)(ipow(X, kTermX[m]) * ipow(Y, kTermY[m]));
+      bg = __fadd_rn(bg, __fmul_rn(basis, coefs[(size_t)b * M + m]));
+    }
+    float* px = stack + ((size_t)b * Hp + pad + y0 + r) * Wp + pad + x0 + c;
+    *px = __fsub_rn(*px, bg);
+  }
+}
+
+}  // namespace
+
+void launch_tile_bg_subtract(float* stack, int nb, int Hp, int Wp, int pad, int x0, int y0,
+                             int w, int h, const float* coefs, int M, const double* norm,
+                             int sms, cudaStream_t s) {
+  const size_t n = (size_t)nb * h * w;
+  if (n == 0) return;
+  const unsigned grid = (unsigned)std::min<size_t>((n + ST - 1) / ST, (size_t)sms * 8);
+  k_tile_bg_subtract<<<grid, ST, 0, s>>>(stack, nb, Hp, Wp, pad, x0, y0, w, h, coefs, M, norm[0],
+                                         norm[1], norm[2], norm[3]);
+}

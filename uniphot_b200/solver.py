@@ -156,6 +156,25 @@ class DeviceField:
         self._table = False
         return self
 
+    @classmethod
+    def from_tiles(cls, data: np.ndarray, invvar: np.ndarray, pad: int, tiles, coefs,
+                   order: int, norm, device: int = 0,
+                   context: Optional[_lib.Context] = None):
+        """The island stage's padded stacks built on the device from the raw
+        (n_bands, H, W) band data: a border of ``pad`` zeros and each pass-1
+        tile's frozen planar background subtracted over its core
+        (island_stage.py:1728-1751; ``tiles`` (n, 4) = (x0, y0, x1, y1),
+        ``coefs`` (n, n_bands, M), ``norm`` = (x_origin, x_scale, y_origin,
+        y_scale), M = 1, 3, 6 for ``order`` 0, 1, 2)."""
+        self = cls.from_unpadded(data, invvar, pad, device=device, context=context)
+        self.ctx.subtract_tile_backgrounds(tiles, coefs, order, norm)
+        return self
+
+    def download(self) -> tuple:
+        """The padded (data, invvar) stacks on the host."""
+        self.check_current()
+        return self.ctx.download_field(self.shape)
+
     def check_current(self):
         """Raise unless this is still the field its context holds."""
         if self.ctx.field_gen != self.gen:
