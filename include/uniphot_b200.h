@@ -298,7 +298,8 @@ int uph_upload_psf_mog(uph_ctx* ctx, const float* params,
  * (n_tiles, n_bands, M) float32 with M = 1, 3, 6 for order 0, 1, 2 and the
  * terms of make_bg_basis (bg_polynomial.py:125-178): 1, X, Y, X^2, XY,
  * Y^2 with X = (x - x_origin) / x_scale, Y = (y - y_origin) / y_scale in
- * float64, each term rounded to float32, the sum in float32; norm =
+ * float64, each term rounded to float32, summed by float32 fused
+ * multiply-adds in term order; norm =
  * (x_origin, x_scale, y_origin, y_scale).  The field must not be held by a
  * live job (UPH_ERR_STATE): upload it, subtract, then add chunks. */
 int uph_subtract_tile_backgrounds(uph_ctx* ctx, int32_t n_tiles, const int32_t* tiles,
