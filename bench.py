@@ -598,7 +598,7 @@ def _serve_measure(args, rates, device):
                              "polynomial coefficients drawn per request",
            "rates": []}
     def packed(engine):
-        return lambda prec: PackedServer(device=device, planners=2, engines=2,
+        return lambda prec: PackedServer(device=device, planners=4, engines=4,
                                          hbm_budget_bytes=160e9, precision=prec,
                                          engine=engine)
 
@@ -606,8 +606,8 @@ def _serve_measure(args, rates, device):
         return lambda prec: Server(device=device, workers=n, hbm_budget_bytes=160e9,
                                    precision=prec)
 
-    forms = (("packed_mixed", "mixed", packed("chunks"), 2),
-             ("packed_mixed_queue", "mixed", packed("queue"), 2),
+    forms = (("packed_mixed", "mixed", packed("chunks"), 4),
+             ("packed_mixed_queue", "mixed", packed("queue"), 4),
              ("batched_mixed", "mixed", workers(args.serve_workers), args.serve_workers),
              ("one_at_a_time_plain", "plain", workers(1), 1))
     for name, prec, make, warm in forms:
