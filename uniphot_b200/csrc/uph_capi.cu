@@ -98,6 +98,11 @@ struct uph_ctx {
   double tb_nmin = 0, tb_nmax = 0;
   int* h_active = nullptr;  // pinned
   DevBuf bgc;               // per-tile background coefficients (stack build)
+  // pinned staging of the unpadded field upload: two slots of one band's
+  // data and inverse variance, and the events that free them
+  float* h_stage = nullptr;
+  size_t h_stage_floats = 0;
+  cudaEvent_t stage_ev[2] = {nullptr, nullptr};
   cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
   float timing[4] = {0, 0, 0, 0};
   int64_t launches = 0;
@@ -229,6 +234,9 @@ int uph_destroy(uph_ctx* ctx) {
   ctx->exp_var.reset();
   for (auto& b : ctx->sp) b.release();
   ctx->bgc.release();
+  if (ctx->h_stage) cudaFreeHost(ctx->h_stage);
+  for (auto& e : ctx->stage_ev)
+    if (e) cudaEventDestroy(e);
   for (auto& b : ctx->isl) b.release();
   for (auto& ev : ctx->ev)
     if (ev) cudaEventDestroy(ev);
@@ -292,6 +300,23 @@ int uph_upload_field(uph_ctx* ctx, const float* d, const float* w,
   return upload_field_impl(ctx, d, w, nb, Hp, Wp, pad, cudaMemcpyHostToDevice);
 }
 
+// Copy n floats from pageable src to pinned dst with up to `threads` host
+// threads (contiguous slices).
+static void parallel_copy(float* dst, const float* src, size_t n, int threads) {
+  if (threads <= 1 || n < (size_t)1 << 20) {
+    std::memcpy(dst, src, n * sizeof(float));
+    return;
+  }
+  std::vector<std::thread> pool;
+  const size_t per = (n + threads - 1) / threads;
+  for (int t = 0; t < threads; ++t) {
+    const size_t lo = (size_t)t * per, hi = std::min(n, lo + per);
+    if (lo >= hi) break;
+    pool.emplace_back([=] { std::memcpy(dst + lo, src + lo, (hi - lo) * sizeof(float)); });
+  }
+  for (auto& th : pool) th.join();
+}
+
 int uph_upload_field_unpadded(uph_ctx* ctx, const float* d, const float* w,
                               int32_t nb, int32_t H, int32_t W, int32_t pad) {
   if (!ctx) return UPH_ERR_INVALID;
@@ -306,15 +331,36 @@ int uph_upload_field_unpadded(uph_ctx* ctx, const float* d, const float* w,
   if (rc) return rc;
   CK(cudaMemsetAsync(sptr(ctx->dstack), 0, bytes, ctx->stream), "field pad");
   CK(cudaMemsetAsync(sptr(ctx->wstack), 0, bytes, ctx->stream), "field pad");
+  // The pageable host arrays go through two pinned slots of one band each:
+  // host threads fill one slot while the copy engine drains the other, so
+  // the upload runs at the multi-threaded host-copy rate instead of the
+  // driver's single-threaded pageable staging.
+  const size_t band = (size_t)H * W;
+  if (ctx->h_stage_floats < 4 * band) {
+    if (ctx->h_stage) cudaFreeHost(ctx->h_stage);
+    ctx->h_stage = nullptr;
+    ctx->h_stage_floats = 0;
+    CK(cudaMallocHost((void**)&ctx->h_stage, sizeof(float) * 4 * band), "field staging");
+    ctx->h_stage_floats = 4 * band;
+  }
+  for (auto& e : ctx->stage_ev)
+    if (!e) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "field staging");
+  const int threads = (int)std::max(1u, std::min(8u, std::thread::hardware_concurrency()));
   for (int b = 0; b < nb; ++b) {
+    const int slot = b & 1;
+    float* sd = ctx->h_stage + (size_t)slot * 2 * band;
+    float* sw = sd + band;
+    if (b >= 2) CK(cudaEventSynchronize(ctx->stage_ev[slot]), "field staging");
+    parallel_copy(sd, d + (size_t)b * band, band, threads);
+    parallel_copy(sw, w + (size_t)b * band, band, threads);
     const size_t o = ((size_t)b * Hp + pad) * Wp + pad;
-    const size_t so = (size_t)b * H * W;
-    CK(cudaMemcpy2DAsync((float*)sptr(ctx->dstack) + o, sizeof(float) * Wp, d + so,
+    CK(cudaMemcpy2DAsync((float*)sptr(ctx->dstack) + o, sizeof(float) * Wp, sd,
                          sizeof(float) * W, sizeof(float) * W, H,
                          cudaMemcpyHostToDevice, ctx->stream), "field copy");
-    CK(cudaMemcpy2DAsync((float*)sptr(ctx->wstack) + o, sizeof(float) * Wp, w + so,
+    CK(cudaMemcpy2DAsync((float*)sptr(ctx->wstack) + o, sizeof(float) * Wp, sw,
                          sizeof(float) * W, sizeof(float) * W, H,
                          cudaMemcpyHostToDevice, ctx->stream), "field copy");
+    CK(cudaEventRecord(ctx->stage_ev[slot], ctx->stream), "field staging");
   }
   CK(cudaStreamSynchronize(ctx->stream), "field copy");
   ctx->nb = nb;
