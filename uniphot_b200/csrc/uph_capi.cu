@@ -13,6 +13,7 @@
 #include <cstring>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <thread>
 #include <vector>
@@ -98,10 +99,7 @@ struct uph_ctx {
   double tb_nmin = 0, tb_nmax = 0;
   int* h_active = nullptr;  // pinned
   DevBuf bgc;               // per-tile background coefficients (stack build)
-  // pinned staging of the unpadded field upload: two slots of one band's
-  // data and inverse variance, and the events that free them
-  float* h_stage = nullptr;
-  size_t h_stage_floats = 0;
+  // events that free the two pinned staging slots of the field upload
   cudaEvent_t stage_ev[2] = {nullptr, nullptr};
   cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
   float timing[4] = {0, 0, 0, 0};
@@ -234,7 +232,6 @@ int uph_destroy(uph_ctx* ctx) {
   ctx->exp_var.reset();
   for (auto& b : ctx->sp) b.release();
   ctx->bgc.release();
-  if (ctx->h_stage) cudaFreeHost(ctx->h_stage);
   for (auto& e : ctx->stage_ev)
     if (e) cudaEventDestroy(e);
   for (auto& b : ctx->isl) b.release();
@@ -300,6 +297,39 @@ int uph_upload_field(uph_ctx* ctx, const float* d, const float* w,
   return upload_field_impl(ctx, d, w, nb, Hp, Wp, pad, cudaMemcpyHostToDevice);
 }
 
+// Process-wide pool of pinned staging buffers for field uploads (portable
+// across contexts and devices): an upload takes one at least as large as it
+// needs, or allocates one, and gives it back, so contexts created per call
+// do not pay the page-locking each time and concurrent uploads each get
+// their own.
+namespace {
+std::mutex g_stage_mu;
+std::vector<std::pair<float*, size_t>> g_stage_free;
+
+float* stage_take(size_t floats, size_t* got) {
+  {
+    std::lock_guard<std::mutex> lk(g_stage_mu);
+    for (size_t i = 0; i < g_stage_free.size(); ++i)
+      if (g_stage_free[i].second >= floats) {
+        float* p = g_stage_free[i].first;
+        *got = g_stage_free[i].second;
+        g_stage_free.erase(g_stage_free.begin() + (long)i);
+        return p;
+      }
+  }
+  float* p = nullptr;
+  if (cudaHostAlloc((void**)&p, sizeof(float) * floats, cudaHostAllocPortable) != cudaSuccess)
+    return nullptr;
+  *got = floats;
+  return p;
+}
+
+void stage_give(float* p, size_t floats) {
+  std::lock_guard<std::mutex> lk(g_stage_mu);
+  g_stage_free.emplace_back(p, floats);
+}
+}  // namespace
+
 // Copy n floats from pageable src to pinned dst with up to `threads` host
 // threads (contiguous slices).
 static void parallel_copy(float* dst, const float* src, size_t n, int threads) {
@@ -336,33 +366,36 @@ int uph_upload_field_unpadded(uph_ctx* ctx, const float* d, const float* w,
   // the upload runs at the multi-threaded host-copy rate instead of the
   // driver's single-threaded pageable staging.
   const size_t band = (size_t)H * W;
-  if (ctx->h_stage_floats < 4 * band) {
-    if (ctx->h_stage) cudaFreeHost(ctx->h_stage);
-    ctx->h_stage = nullptr;
-    ctx->h_stage_floats = 0;
-    CK(cudaMallocHost((void**)&ctx->h_stage, sizeof(float) * 4 * band), "field staging");
-    ctx->h_stage_floats = 4 * band;
-  }
   for (auto& e : ctx->stage_ev)
     if (!e) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "field staging");
+  size_t got = 0;
+  float* stage = stage_take(4 * band, &got);
+  if (!stage) return set_err(ctx, UPH_ERR_OOM, "RESOURCE_EXHAUSTED: pinned field staging");
   const int threads = (int)std::max(1u, std::min(8u, std::thread::hardware_concurrency()));
-  for (int b = 0; b < nb; ++b) {
+  cudaError_t ce = cudaSuccess;
+  for (int b = 0; b < nb && ce == cudaSuccess; ++b) {
     const int slot = b & 1;
-    float* sd = ctx->h_stage + (size_t)slot * 2 * band;
+    float* sd = stage + (size_t)slot * 2 * band;
     float* sw = sd + band;
-    if (b >= 2) CK(cudaEventSynchronize(ctx->stage_ev[slot]), "field staging");
+    if (b >= 2) ce = cudaEventSynchronize(ctx->stage_ev[slot]);
+    if (ce != cudaSuccess) break;
     parallel_copy(sd, d + (size_t)b * band, band, threads);
     parallel_copy(sw, w + (size_t)b * band, band, threads);
     const size_t o = ((size_t)b * Hp + pad) * Wp + pad;
-    CK(cudaMemcpy2DAsync((float*)sptr(ctx->dstack) + o, sizeof(float) * Wp, sd,
-                         sizeof(float) * W, sizeof(float) * W, H,
-                         cudaMemcpyHostToDevice, ctx->stream), "field copy");
-    CK(cudaMemcpy2DAsync((float*)sptr(ctx->wstack) + o, sizeof(float) * Wp, sw,
-                         sizeof(float) * W, sizeof(float) * W, H,
-                         cudaMemcpyHostToDevice, ctx->stream), "field copy");
-    CK(cudaEventRecord(ctx->stage_ev[slot], ctx->stream), "field staging");
+    ce = cudaMemcpy2DAsync((float*)sptr(ctx->dstack) + o, sizeof(float) * Wp, sd,
+                           sizeof(float) * W, sizeof(float) * W, H, cudaMemcpyHostToDevice,
+                           ctx->stream);
+    if (ce == cudaSuccess)
+      ce = cudaMemcpy2DAsync((float*)sptr(ctx->wstack) + o, sizeof(float) * Wp, sw,
+                             sizeof(float) * W, sizeof(float) * W, H, cudaMemcpyHostToDevice,
+                             ctx->stream);
+    if (ce == cudaSuccess) ce = cudaEventRecord(ctx->stage_ev[slot], ctx->stream);
   }
-  CK(cudaStreamSynchronize(ctx->stream), "field copy");
+  // the staging buffer goes back to the pool only once its copies are done
+  const cudaError_t se = cudaStreamSynchronize(ctx->stream);
+  stage_give(stage, got);
+  if (ce != cudaSuccess) return cuda_err(ctx, ce, "field copy");
+  if (se != cudaSuccess) return cuda_err(ctx, se, "field copy");
   ctx->nb = nb;
   ctx->Hp = Hp;
   ctx->Wp = Wp;
