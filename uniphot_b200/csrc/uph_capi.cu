@@ -1454,6 +1454,44 @@ int job_streams(uph_job* job, int nstreams, std::vector<int>& order) {
   return UPH_OK;
 }
 
+// Lanes of the queue engine by footprint: a queue kernel launches with the
+// largest shared-memory footprint among its lane's chunks, so chunks of like
+// size share a lane -- sorted by window side, Gram rows and stamp tier, then
+// cut into nl runs of about equal cost, every lane non-empty -- instead of
+// the longest-processing-time deal, which puts a heavy chunk in every lane
+// and runs every unit at the heavy chunk's occupancy.
+void queue_lanes(uph_job* job, int nl) {
+  const int nch = (int)job->chunks.size();
+  std::vector<int> byfp(nch);
+  std::vector<double> cost(nch);
+  double total = 0.0;
+  for (int i = 0; i < nch; ++i) {
+    const ClassDev& c = job->chunks[i]->c;
+    byfp[i] = i;
+    cost[i] = (double)c.n_isl * c.nb *
+              ((double)c.B * c.B * c.Kmax + (double)c.N * c.T * c.T * c.R);
+    total += cost[i];
+  }
+  std::stable_sort(byfp.begin(), byfp.end(), [&](int a, int b) {
+    const ClassDev& x = job->chunks[a]->c;
+    const ClassDev& y = job->chunks[b]->c;
+    if (x.B != y.B) return x.B > y.B;
+    if (x.Kmax != y.Kmax) return x.Kmax > y.Kmax;
+    return x.T > y.T;
+  });
+  int lane = 0;
+  double acc = 0.0;
+  for (int j = 0; j < nch; ++j) {
+    // move on when this lane has its share, or when the chunks left are
+    // only enough to give every remaining lane one
+    if (j > 0 && lane < nl - 1 &&
+        (acc >= total * (lane + 1) / nl || nch - j <= nl - 1 - lane))
+      ++lane;
+    job->chunks[byfp[j]]->slot = lane;
+    acc += cost[byfp[j]];
+  }
+}
+
 // Every stream of the job waits for the work enqueued so far on `from`.
 int job_fork(uph_job* job, cudaStream_t from, int nstreams) {
   uph_ctx* ctx = job->ctx;
@@ -1503,6 +1541,7 @@ int job_solve_queue(uph_job* job, int max_steps) {
   std::vector<int> order;
   int rc = job_streams(job, nl, order);
   if (rc) return rc;
+  queue_lanes(job, nl);
   if (job->h_active_cap < std::max(nch, nl)) {
     if (job->h_active) cudaFreeHost(job->h_active);
     CK(cudaMallocHost((void**)&job->h_active, sizeof(int) * std::max(nch, nl)), "pinned");
