@@ -171,3 +171,16 @@ def test_resident_field_bytes_stay_charged_between_requests():
         [f.result(timeout=30) for f in futs]
     assert srv.peak_in_use <= 100
     assert srv.in_use == sum(srv.resident) <= 40
+
+
+def test_a_failing_worker_start_fails_its_requests():
+    def bad_init(i):
+        raise RuntimeError("stand-in: no device")
+    dev = FakeDevice()
+    srv = Server(workers=1, hbm_budget_bytes=100, plan_fn=dev.plan, solve_fn=dev.solve,
+                 worker_init=bad_init)
+    with srv:
+        futs = [srv.submit({"rid": i, "bytes": 1}) for i in range(3)]
+        for f in futs:
+            with pytest.raises(RuntimeError, match="no device"):
+                f.result(timeout=30)

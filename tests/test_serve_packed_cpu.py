@@ -151,3 +151,19 @@ def test_closed_packed_server_rejects_requests():
     srv.close()
     with pytest.raises(RuntimeError):
         srv.submit({"rid": 0})
+
+
+def test_a_failing_engine_start_fails_its_requests():
+    """An engine whose set-up raises (no device, say) answers every request
+    it takes with that error instead of leaving it unanswered."""
+    def bad_init(i):
+        raise RuntimeError("stand-in: no device")
+    dev = FakePacker()
+    srv = PackedServer(planners=1, engines=1, hbm_budget_bytes=100, plan_fn=dev.plan,
+                       pack_fn=dev.pack, engine_init=bad_init)
+    with srv:
+        futs = [srv.submit({"rid": i}) for i in range(3)]
+        for f in futs:
+            with pytest.raises(RuntimeError, match="no device"):
+                f.result(timeout=30)
+    assert srv.in_use == 0

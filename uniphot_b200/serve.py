@@ -165,7 +165,10 @@ class Server:
             self._cv.notify_all()
 
     def _run(self, wi: int):
-        state = self._init(wi)
+        try:
+            state, init_error = self._init(wi), None
+        except BaseException as e:  # noqa: BLE001 -- reported to every request it takes
+            state, init_error = None, e
         while True:
             item = self._q.get()
             if item is None:
@@ -174,6 +177,8 @@ class Server:
             st.worker = wi
             held = 0.0
             try:
+                if init_error is not None:
+                    raise init_error
                 planned = self._plan(item.kwargs)
                 plan, nbytes, n_isl = planned[:3]
                 field_bytes = float(planned[3]) if len(planned) > 3 else 0.0
@@ -364,7 +369,10 @@ class PackedServer:
         return pack
 
     def _engine_loop(self, ei: int):
-        state = self._init(ei)
+        try:
+            state, init_error = self._init(ei), None
+        except BaseException as e:  # noqa: BLE001 -- reported to every request it takes
+            state, init_error = None, e
         while True:
             with self._rcv:
                 while not self._ready and self._planning > 0:
@@ -380,6 +388,8 @@ class PackedServer:
                 a.item.stats.worker, a.item.stats.pack = ei, pid
                 a.item.stats.pack_size = len(pack)
             try:
+                if init_error is not None:
+                    raise init_error
                 outs = list(self._pack(state, [(a.item.kwargs, a.plan) for a in pack]))
                 if len(outs) != len(pack):
                     raise RuntimeError(f"pack_fn returned {len(outs)} results for "
@@ -388,7 +398,8 @@ class PackedServer:
                 outs = [e] * len(pack)
             # the context keeps the last uploaded field between packs: at
             # most the largest field seen stays charged to the budget
-            new_res = max([self.resident[ei]] + [a.field_bytes for a in pack])
+            new_res = max([self.resident[ei]] +
+                          ([a.field_bytes for a in pack] if init_error is None else []))
             growth = new_res - self.resident[ei]
             self.resident[ei] = new_res
             with self._cv:
