@@ -19,6 +19,8 @@
  *   uph_upload_sersic_table <- sersic_mog.get_table_jax (sersic_mog.py:59-78)
  *   uph_subtract_tile_backgrounds <- the padded field stacks' frozen per-tile
  *                              background subtraction (island_stage.py:1728-1751)
+ *   uph_scene_subtract_stars <- the field-wide star scene subtraction
+ *                              (island_stage.py:2024-2118, _star_stamps_jit :99-130)
  *   uph_upload_exp_mog      <- source_model.EXP_AMP / EXP_VAR (source_model.py:
  *                              56-75), the "direct" backend's mixture
  *   uph_run_chunk           <- run_class_chunk (island_solver.py:2793-3131)
@@ -304,6 +306,22 @@ int uph_upload_psf_mog(uph_ctx* ctx, const float* params,
  * live job (UPH_ERR_STATE): upload it, subtract, then add chunks. */
 int uph_subtract_tile_backgrounds(uph_ctx* ctx, int32_t n_tiles, const int32_t* tiles,
                                   const float* coefs, int32_t order, const double* norm);
+
+/* Field-wide scene subtraction of the star models (island_stage.py:
+ * 2024-2118): for every band and every source i with flux[i, b] != 0,
+ * flux[i, b] times its stamp -- the band's polynomial PSF (coefs (n_bands,
+ * T, T, nt), origin_scale (n_bands, 4)) at the float32 position, Lanczos-3
+ * shifted by the position's fractional part, not renormalised -- is
+ * subtracted from the context's padded data stack at the corner
+ * (round(x) - T/2, round(y) - T/2) + pad (round half to even of the
+ * float64 position), clipped to the stack; product and difference each in
+ * float32.  A pixel under several stamps is reduced in source order, as
+ * the reference's loop (disjoint stamps run together).  The caller passes
+ * the sources to subtract (the reference: the STAR members of the fit set;
+ * extended sources stay in).  The field must not be held by a live job. */
+int uph_scene_subtract_stars(uph_ctx* ctx, int32_t n, const double* x, const double* y,
+                             const float* flux, int32_t T, int32_t nt, const float* coefs,
+                             const float* origin_scale);
 
 /* Copy the context's padded field stacks (n_bands, Hp, Wp) float32 to host
  * buffers (either may be NULL). */

@@ -37,3 +37,37 @@ def field_stacks(data, invvar, pad, tiles, coefs, order, norm):
             dmb[b, pad + y0:pad + y1, pad + x0:pad + x1] -= (
                 basis @ np.asarray(coefs[t][b], np.float32)).reshape(h, w)
     return dmb, iv
+
+
+def scene_subtract_stars(dmb, x, y, flux, psfs, native, pad):
+    """The field-wide star scene subtraction (island_stage.py:2024-2118) on a
+    padded data stack (modified in place and returned): per band, per source
+    in index order with a nonzero flux, ``dmb[b, iy:iy + T, ix:ix + T] -=
+    flux * stamp`` over the part inside the stack, with the stamp the band's
+    polynomial PSF at the float32 position, Lanczos-shifted, not
+    renormalised (``_star_stamps_jit``, island_stage.py:99-130; the
+    stamps of ``sparse_oracle.stamps``, pinned to the reference through the
+    per-grid solve's golden fixtures) and the corner ``round(x) - T // 2 +
+    pad`` of the float64 position.  ``psfs``: per-band polynomial PSFs of
+    stamp side ``native``."""
+    from .sparse_oracle import stamps
+    x = np.asarray(x, np.float64)
+    y = np.asarray(y, np.float64)
+    flux = np.asarray(flux, np.float32)
+    T = int(native)
+    nb, Hp, Wp = dmb.shape
+    ixt = np.round(x).astype(np.int64) - T // 2 + pad
+    iyt = np.round(y).astype(np.int64) - T // 2 + pad
+    for b in range(nb):
+        st = stamps(psfs[b], x.astype(np.float32), y.astype(np.float32), 0, 0, renorm=False)
+        for k in range(x.size):
+            f = np.float32(flux[k, b])
+            if f == 0.0:
+                continue
+            ix, iy = int(ixt[k]), int(iyt[k])
+            y0c, x0c = max(0, -iy), max(0, -ix)
+            ye, xe = min(T, Hp - iy), min(T, Wp - ix)
+            if ye <= y0c or xe <= x0c:
+                continue
+            dmb[b, iy + y0c:iy + ye, ix + x0c:ix + xe] -= f * st[k, y0c:ye, x0c:xe]
+    return dmb

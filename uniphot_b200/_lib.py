@@ -31,7 +31,7 @@ EXPORTED = ("uph_create", "uph_destroy", "uph_last_error", "uph_set_stream",
             "uph_job_chunk_time", "uph_sparse_band_solve", "uph_island_roots",
             "uph_set_island_retry_limit", "uph_job_kernel_exps", "uph_measure_peaks",
             "uph_job_set_engine", "uph_upload_exp_mog", "uph_subtract_tile_backgrounds",
-            "uph_download_field")
+            "uph_download_field", "uph_scene_subtract_stars")
 KERNEL_KINDS = ("render", "gram", "assemble", "step", "trial_chi2", "accept",
                 "gram_tc")
 
@@ -150,6 +150,8 @@ def lib():
         L.uph_upload_exp_mog.argtypes = [_P, _P, _P, C.c_int32]
         L.uph_subtract_tile_backgrounds.argtypes = [_P, C.c_int32, _P, _P, C.c_int32, _P]
         L.uph_download_field.argtypes = [_P, _P, _P]
+        L.uph_scene_subtract_stars.argtypes = [_P, C.c_int32, _P, _P, _P, C.c_int32,
+                                               C.c_int32, _P, _P]
         _lib = L
     return _lib
 
@@ -336,6 +338,22 @@ class Context:
         self.check(lib().uph_subtract_tile_backgrounds(self._h, int(t.shape[0]), ptr(t), ptr(c),
                                                        int(order), ptr(nm)),
                    "uph_subtract_tile_backgrounds")
+
+    def scene_subtract_stars(self, x, y, flux, coefs, origin_scale):
+        """Subtract flux x the star stamps from the uploaded data stack
+        (uph_scene_subtract_stars): x, y (n,), flux (n, n_bands), coefs
+        (n_bands, T, T, nt), origin_scale (n_bands, 4)."""
+        xs = np.ascontiguousarray(x, np.float64)
+        ys = np.ascontiguousarray(y, np.float64)
+        fl = np.ascontiguousarray(flux, np.float32)
+        cf = np.ascontiguousarray(coefs, np.float32)
+        os_ = np.ascontiguousarray(origin_scale, np.float32)
+        nb, T, T2, nt = cf.shape
+        if T != T2 or fl.shape != (xs.size, nb) or ys.size != xs.size:
+            raise ValueError("scene_subtract_stars: inconsistent shapes")
+        self.check(lib().uph_scene_subtract_stars(self._h, int(xs.size), ptr(xs), ptr(ys),
+                                                  ptr(fl), int(T), int(nt), ptr(cf),
+                                                  ptr(os_)), "uph_scene_subtract_stars")
 
     def download_field(self, shape) -> tuple:
         """The padded (data, invvar) stacks of the given (n_bands, Hp, Wp)

@@ -514,6 +514,122 @@ int uph_subtract_tile_backgrounds(uph_ctx* ctx, int32_t n_tiles, const int32_t* 
   return UPH_OK;
 }
 
+int uph_scene_subtract_stars(uph_ctx* ctx, int32_t n, const double* x, const double* y,
+                             const float* flux, int32_t T, int32_t nt, const float* coefs,
+                             const float* origin_scale) {
+  if (!ctx) return UPH_ERR_INVALID;
+  if (!sptr(ctx->dstack)) return set_err(ctx, UPH_ERR_STATE, "no field uploaded");
+  if (ctx->dstack.use_count() > 1)
+    return set_err(ctx, UPH_ERR_STATE,
+                   "the field is held by a live job's chunks: upload it again to change it");
+  if (n < 0 || (n > 0 && (!x || !y || !flux || !coefs || !origin_scale)) || T <= 0 ||
+      (T % 2) == 0 || !(nt == 1 || nt == 3 || nt == 6 || nt == 10 || nt == 15 || nt == 21))
+    return set_err(ctx, UPH_ERR_INVALID, "invalid scene subtraction (n %d, T %d, nt %d)", n, T,
+                   nt);
+  if (sparse_stamp_smem(T, T) > 200 * 1024)
+    return set_err(ctx, UPH_ERR_INVALID, "stamp side %d too large", T);
+  if (n == 0) return UPH_OK;
+  for (int i = 0; i < n; ++i)
+    if (!std::isfinite(x[i]) || !std::isfinite(y[i]) || std::fabs(x[i]) > 1e8 ||
+        std::fabs(y[i]) > 1e8)
+      return set_err(ctx, UPH_ERR_INVALID, "source %d position not finite or out of range", i);
+  cudaSetDevice(ctx->device);
+  const int nb = ctx->nb;
+  // stamp corners as the reference computes them (round half to even of
+  // the float64 position, island_stage.py:2000-2001); the stamps render at
+  // the float32 position
+  std::vector<int> ix(n), iy(n);
+  std::vector<float> xf(n), yf(n);
+  for (int i = 0; i < n; ++i) {
+    ix[i] = (int)std::nearbyint(x[i]) - T / 2;
+    iy[i] = (int)std::nearbyint(y[i]) - T / 2;
+    xf[i] = (float)x[i];
+    yf[i] = (float)y[i];
+  }
+  // waves: a source goes one wave after the latest earlier source whose
+  // stamp overlaps its own (corners closer than T on both axes), so each
+  // wave's stamps are disjoint and every pixel sees its sources in index
+  // order; the earlier sources are found in the 3 x 3 cells of pitch T
+  std::vector<int> wave(n, 0);
+  std::map<std::pair<int, int>, std::vector<int>> cells;
+  auto cell_of = [&](int v) { return v >= 0 ? v / T : -((-v + T - 1) / T); };
+  int nwave = 0;
+  for (int i = 0; i < n; ++i) {
+    const int cx = cell_of(ix[i]), cy = cell_of(iy[i]);
+    int w = 0;
+    for (int dy = -1; dy <= 1; ++dy)
+      for (int dx = -1; dx <= 1; ++dx) {
+        auto it = cells.find({cx + dx, cy + dy});
+        if (it == cells.end()) continue;
+        for (int j : it->second)
+          if (std::abs(ix[i] - ix[j]) < T && std::abs(iy[i] - iy[j]) < T)
+            w = std::max(w, wave[j] + 1);
+      }
+    wave[i] = w;
+    nwave = std::max(nwave, w + 1);
+    cells[{cx, cy}].push_back(i);
+  }
+  std::vector<int> srcs(n), off(nwave + 1, 0);
+  for (int i = 0; i < n; ++i) ++off[wave[i] + 1];
+  for (int w = 0; w < nwave; ++w) off[w + 1] += off[w];
+  {
+    std::vector<int> pos(off.begin(), off.end() - 1);
+    for (int i = 0; i < n; ++i) srcs[pos[wave[i]]++] = i;
+  }
+  std::vector<float> fl((size_t)nb * n);
+  for (int i = 0; i < n; ++i)
+    for (int b = 0; b < nb; ++b) fl[(size_t)b * n + i] = flux[(size_t)i * nb + b];
+  DevBuf dx, dy, dfl, dcf, dos, dst, dix, diy, dscr, dsrc;
+  auto release = [&] {
+    for (DevBuf* b : {&dx, &dy, &dfl, &dcf, &dos, &dst, &dix, &diy, &dscr, &dsrc}) b->release();
+  };
+  int rc = UPH_OK;
+  const size_t TT = (size_t)T * T;
+  if (!rc) rc = ensure(ctx, dx, sizeof(float) * n, "scene");
+  if (!rc) rc = ensure(ctx, dy, sizeof(float) * n, "scene");
+  if (!rc) rc = ensure(ctx, dfl, sizeof(float) * nb * (size_t)n, "scene");
+  if (!rc) rc = ensure(ctx, dcf, sizeof(float) * nb * TT * nt, "scene");
+  if (!rc) rc = ensure(ctx, dos, sizeof(float) * 4 * nb, "scene");
+  if (!rc) rc = ensure(ctx, dst, sizeof(float) * TT * n, "scene");
+  if (!rc) rc = ensure(ctx, dix, sizeof(int) * n, "scene");
+  if (!rc) rc = ensure(ctx, diy, sizeof(int) * n, "scene");
+  if (!rc) rc = ensure(ctx, dscr, sizeof(int) * 2 * n, "scene");
+  if (!rc) rc = ensure(ctx, dsrc, sizeof(int) * n, "scene");
+  if (!rc) rc = upload(ctx, dx.ptr, xf.data(), sizeof(float) * n, "scene");
+  if (!rc) rc = upload(ctx, dy.ptr, yf.data(), sizeof(float) * n, "scene");
+  if (!rc) rc = upload(ctx, dfl.ptr, fl.data(), sizeof(float) * nb * (size_t)n, "scene");
+  if (!rc) rc = upload(ctx, dcf.ptr, coefs, sizeof(float) * nb * TT * nt, "scene");
+  if (!rc) rc = upload(ctx, dos.ptr, origin_scale, sizeof(float) * 4 * nb, "scene");
+  if (!rc) rc = upload(ctx, dix.ptr, ix.data(), sizeof(int) * n, "scene");
+  if (!rc) rc = upload(ctx, diy.ptr, iy.data(), sizeof(int) * n, "scene");
+  if (!rc) rc = upload(ctx, dsrc.ptr, srcs.data(), sizeof(int) * n, "scene");
+  if (rc) {
+    cudaStreamSynchronize(ctx->stream);
+    release();
+    return rc;
+  }
+  const size_t plane = (size_t)ctx->Hp * ctx->Wp;
+  for (int b = 0; b < nb; ++b) {
+    // the band's stamps (their own corners go to scratch: the corners above
+    // come from the float64 positions)
+    launch_star_stamps(n, T, T, (const float*)dcf.ptr + (size_t)b * TT * nt, nt,
+                       (const float*)dos.ptr + 4 * b, (const float*)dx.ptr,
+                       (const float*)dy.ptr, (float*)dst.ptr, (int*)dscr.ptr,
+                       (int*)dscr.ptr + n, ctx->stream);
+    for (int w = 0; w < nwave; ++w)
+      launch_scene_sub_wave((float*)sptr(ctx->dstack) + b * plane, ctx->Hp, ctx->Wp, ctx->pad,
+                            T, (const int*)dsrc.ptr + off[w], off[w + 1] - off[w],
+                            (const float*)dst.ptr, (const int*)dix.ptr, (const int*)diy.ptr,
+                            (const float*)dfl.ptr + (size_t)b * n, ctx->stream);
+  }
+  cudaError_t e = cudaGetLastError();
+  const cudaError_t se = cudaStreamSynchronize(ctx->stream);
+  release();
+  if (e != cudaSuccess) return cuda_err(ctx, e, "scene subtraction");
+  if (se != cudaSuccess) return cuda_err(ctx, se, "scene subtraction");
+  return UPH_OK;
+}
+
 int uph_download_field(uph_ctx* ctx, float* data, float* invvar) {
   if (!ctx) return UPH_ERR_INVALID;
   if (!sptr(ctx->dstack)) return set_err(ctx, UPH_ERR_STATE, "no field uploaded");

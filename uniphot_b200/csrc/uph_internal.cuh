@@ -703,6 +703,12 @@ size_t gal_fft_floats(int T, int P);
 int gal_fft_smem(int T, int P);
 int gal_fft_setup();
 size_t gal_direct_floats(int T);
+void launch_star_stamps(int n, int H, int W, const float* coefs, int nt, const float* os,
+                        const float* px, const float* py, float* out, int* ixt, int* iyt,
+                        cudaStream_t s);
+void launch_scene_sub_wave(float* stack, int Hp, int Wp, int pad, int T, const int* srcs,
+                           int count, const float* stamps, const int* ixt, const int* iyt,
+                           const float* flux, cudaStream_t s);
 void launch_tile_bg_subtract(float* stack, int nb, int Hp, int Wp, int pad, int x0, int y0,
                              int w, int h, const float* coefs, int M, const double* norm,
                              int sms, cudaStream_t s);

@@ -583,6 +583,17 @@ int sparse_setup() {
                                    200 * 1024);
 }
 
+// Raw (not renormalised) Lanczos-shifted polynomial-PSF stamps of n point
+// sources at (px, py) in field pixels, H x W each, into out, with their
+// stamp top-left corners (round(x) - W/2, round(y) - H/2) in ixt / iyt.
+void launch_star_stamps(int n, int H, int W, const float* coefs, int nt, const float* os,
+                        const float* px, const float* py, float* out, int* ixt, int* iyt,
+                        cudaStream_t s) {
+  if (n > 0)
+    k_sp_stamps<<<(unsigned)n, ST, sparse_stamp_smem(H, W), s>>>(
+        n, H, W, coefs, nt, os, px, py, 0.f, 0.f, 0, out, ixt, iyt, nullptr, nullptr);
+}
+
 void launch_sparse_band(const SparseDev& d, cudaStream_t s) {
   const int n = d.n, H = d.H, W = d.W, M = d.M, nt = d.n + d.M;
   const size_t npix = (size_t)d.h * d.w;

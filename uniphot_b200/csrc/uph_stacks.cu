@@ -62,3 +62,44 @@ void launch_tile_bg_subtract(float* stack, int nb, int Hp, int Wp, int pad, int 
   k_tile_bg_subtract<<<grid, ST, 0, s>>>(stack, nb, Hp, Wp, pad, x0, y0, w, h, coefs, M, norm[0],
                                          norm[1], norm[2], norm[3]);
 }
+
+// ---- Field-wide scene subtraction of the star models (island_stage.py:
+// 2024-2118): stack[b, pad + iy + r, pad + ix + c] -= flux * stamp[r][c]
+// over the part of each source's T x T stamp inside the padded stack,
+// product and difference each rounded to float32 (the reference's numpy
+// `dmb[...] -= f * st`).  The sources of one launch (a wave) have pairwise
+// disjoint stamps, so no two threads touch a pixel; the host orders the
+// waves so that a pixel covered by several stamps is reduced in source
+// order.  One CTA per source of the wave, threads over its stamp pixels.
+namespace {
+
+__global__ void __launch_bounds__(ST) k_scene_sub(float* __restrict__ stack, int Hp, int Wp,
+                                                  int pad, int T,
+                                                  const int* __restrict__ srcs,
+                                                  const float* __restrict__ stamps,
+                                                  const int* __restrict__ ixt,
+                                                  const int* __restrict__ iyt,
+                                                  const float* __restrict__ flux) {
+  const int s = srcs[blockIdx.x];
+  const float f = flux[s];
+  if (f == 0.f) return;
+  const int ix = ixt[s] + pad, iy = iyt[s] + pad;
+  const float* st = stamps + (size_t)s * T * T;
+  for (int e = threadIdx.x; e < T * T; e += ST) {
+    const int r = e / T, c = e - (e / T) * T;
+    const int y = iy + r, x = ix + c;
+    if (y < 0 || y >= Hp || x < 0 || x >= Wp) continue;
+    float* px = stack + (size_t)y * Wp + x;
+    *px = __fsub_rn(*px, __fmul_rn(f, st[e]));
+  }
+}
+
+}  // namespace
+
+void launch_scene_sub_wave(float* stack, int Hp, int Wp, int pad, int T, const int* srcs,
+                           int count, const float* stamps, const int* ixt, const int* iyt,
+                           const float* flux, cudaStream_t s) {
+  if (count > 0)
+    k_scene_sub<<<(unsigned)count, ST, 0, s>>>(stack, Hp, Wp, pad, T, srcs, stamps, ixt, iyt,
+                                               flux);
+}

@@ -170,6 +170,21 @@ class DeviceField:
         self.ctx.subtract_tile_backgrounds(tiles, coefs, order, norm)
         return self
 
+    def subtract_star_scene(self, psfs: list, x, y, flux, native: int | None = None):
+        """Field-wide scene subtraction of the star models on the device
+        (island_stage.py:2024-2118): every source's pass-1 flux (n,
+        n_bands) times its stamp (the band's polynomial PSF at its position,
+        Lanczos-shifted, on the ``native`` stamp) removed from the data
+        stack, in source order per pixel.  Pass the stars to subtract (the
+        reference subtracts the fit set's STAR members and keeps extended
+        sources)."""
+        self.check_current()
+        T = int(native if native is not None else psfs[0].H_psf)
+        tree, _ = build_psf_tree(psfs, T)
+        if tree.mode != "reference":
+            raise ValueError("the scene subtraction takes pixelised polynomial PSFs")
+        self.ctx.scene_subtract_stars(x, y, flux, tree.params, tree.origin_scale)
+
     def download(self) -> tuple:
         """The padded (data, invvar) stacks on the host."""
         self.check_current()
