@@ -322,6 +322,10 @@ int uph_subtract_tile_backgrounds(uph_ctx* ctx, int32_t n_tiles, const int32_t* 
 int uph_scene_subtract_stars(uph_ctx* ctx, int32_t n, const double* x, const double* y,
                              const float* flux, int32_t T, int32_t nt, const float* coefs,
                              const float* origin_scale);
+/* The wave of each source in that subtraction (host only, no device):
+ * one more than the latest wave among the earlier sources whose T x T
+ * stamps overlap its own; returns the number of waves, -1 on bad input. */
+int uph_scene_waves(int32_t n, const double* x, const double* y, int32_t T, int32_t* wave);
 
 /* Copy the context's padded field stacks (n_bands, Hp, Wp) float32 to host
  * buffers (either may be NULL). */

@@ -44,3 +44,29 @@ def test_oracle_stack_build_matches_the_reference(order):
     dmb, iv = field_stacks(data, invvar, PAD, tiles, coefs, order, norm)
     np.testing.assert_array_equal(dmb, z[f"dmb_order{order}"])
     assert np.all(iv[:, :PAD] == 0) and np.all(iv[:, PAD:PAD + 70, PAD:PAD + 90] == invvar)
+
+
+def test_scene_subtraction_waves_keep_source_order_per_pixel():
+    """The star scene subtraction's schedule (host code of the library, no
+    device): every wave's stamps are pairwise disjoint, and of two
+    overlapping stamps the earlier source is in an earlier wave -- against
+    an all-pairs restatement on clustered positions, stamps off the field's
+    edges and coincident sources."""
+    from uniphot_b200 import _lib
+    rng = np.random.default_rng(3)
+    T = 31
+    cx, cy = rng.uniform(0, 400, 30), rng.uniform(0, 400, 30)
+    x = np.concatenate([cx[k] + rng.normal(0, 12, 8) for k in range(30)] + [[-40.2, -40.2]])
+    y = np.concatenate([cy[k] + rng.normal(0, 12, 8) for k in range(30)] + [[5.5, 5.5]])
+    wave = _lib.scene_waves(x, y, T)
+    ix = np.round(x).astype(int) - T // 2
+    iy = np.round(y).astype(int) - T // 2
+    ref = np.zeros(x.size, int)
+    for i in range(x.size):
+        for j in range(i):
+            if abs(ix[i] - ix[j]) < T and abs(iy[i] - iy[j]) < T:
+                ref[i] = max(ref[i], ref[j] + 1)
+    np.testing.assert_array_equal(wave, ref)
+    assert wave.max() >= 3 and wave[-1] == wave[-2] + 1
+    with pytest.raises(ValueError):
+        _lib.scene_waves([np.nan], [0.0], T)

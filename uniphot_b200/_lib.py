@@ -31,7 +31,7 @@ EXPORTED = ("uph_create", "uph_destroy", "uph_last_error", "uph_set_stream",
             "uph_job_chunk_time", "uph_sparse_band_solve", "uph_island_roots",
             "uph_set_island_retry_limit", "uph_job_kernel_exps", "uph_measure_peaks",
             "uph_job_set_engine", "uph_upload_exp_mog", "uph_subtract_tile_backgrounds",
-            "uph_download_field", "uph_scene_subtract_stars")
+            "uph_download_field", "uph_scene_subtract_stars", "uph_scene_waves")
 KERNEL_KINDS = ("render", "gram", "assemble", "step", "trial_chi2", "accept",
                 "gram_tc")
 
@@ -152,12 +152,24 @@ def lib():
         L.uph_download_field.argtypes = [_P, _P, _P]
         L.uph_scene_subtract_stars.argtypes = [_P, C.c_int32, _P, _P, _P, C.c_int32,
                                                C.c_int32, _P, _P]
+        L.uph_scene_waves.argtypes = [C.c_int32, _P, _P, C.c_int32, _P]
         _lib = L
     return _lib
 
 
 def ptr(a):
     return None if a is None else a.ctypes.data_as(_P)
+
+
+def scene_waves(x, y, T: int) -> np.ndarray:
+    """The wave of each source in the ordered star scene subtraction
+    (uph_scene_waves; host only)."""
+    xs = np.ascontiguousarray(x, np.float64)
+    ys = np.ascontiguousarray(y, np.float64)
+    w = np.zeros(xs.size, np.int32)
+    if lib().uph_scene_waves(int(xs.size), ptr(xs), ptr(ys), int(T), ptr(w)) < 0:
+        raise ValueError("scene_waves: bad positions or stamp side")
+    return w
 
 
 class Context:

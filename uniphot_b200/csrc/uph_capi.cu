@@ -514,6 +514,46 @@ int uph_subtract_tile_backgrounds(uph_ctx* ctx, int32_t n_tiles, const int32_t* 
   return UPH_OK;
 }
 
+// Waves of the ordered stamp subtraction: a source goes one wave after the
+// latest earlier source whose T x T stamp (corner ix, iy) overlaps its own
+// (corners closer than T on both axes), so each wave's stamps are disjoint
+// and every pixel sees its sources in index order; the earlier sources are
+// found in the 3 x 3 cells of pitch T.  Returns the number of waves.
+static int scene_waves(int n, const int* ix, const int* iy, int T, int* wave) {
+  std::map<std::pair<int, int>, std::vector<int>> cells;
+  auto cell_of = [&](int v) { return v >= 0 ? v / T : -((-v + T - 1) / T); };
+  int nwave = 0;
+  for (int i = 0; i < n; ++i) {
+    const int cx = cell_of(ix[i]), cy = cell_of(iy[i]);
+    int w = 0;
+    for (int dy = -1; dy <= 1; ++dy)
+      for (int dx = -1; dx <= 1; ++dx) {
+        auto it = cells.find({cx + dx, cy + dy});
+        if (it == cells.end()) continue;
+        for (int j : it->second)
+          if (std::abs(ix[i] - ix[j]) < T && std::abs(iy[i] - iy[j]) < T)
+            w = std::max(w, wave[j] + 1);
+      }
+    wave[i] = w;
+    nwave = std::max(nwave, w + 1);
+    cells[{cx, cy}].push_back(i);
+  }
+  return nwave;
+}
+
+int uph_scene_waves(int32_t n, const double* x, const double* y, int32_t T, int32_t* wave) {
+  if (n < 0 || (n > 0 && (!x || !y || !wave)) || T <= 0) return -1;
+  std::vector<int> ix(n), iy(n);
+  for (int i = 0; i < n; ++i) {
+    if (!std::isfinite(x[i]) || !std::isfinite(y[i]) || std::fabs(x[i]) > 1e8 ||
+        std::fabs(y[i]) > 1e8)
+      return -1;
+    ix[i] = (int)std::nearbyint(x[i]) - T / 2;
+    iy[i] = (int)std::nearbyint(y[i]) - T / 2;
+  }
+  return scene_waves(n, ix.data(), iy.data(), T, wave);
+}
+
 int uph_scene_subtract_stars(uph_ctx* ctx, int32_t n, const double* x, const double* y,
                              const float* flux, int32_t T, int32_t nt, const float* coefs,
                              const float* origin_scale) {
@@ -546,29 +586,8 @@ int uph_scene_subtract_stars(uph_ctx* ctx, int32_t n, const double* x, const dou
     xf[i] = (float)x[i];
     yf[i] = (float)y[i];
   }
-  // waves: a source goes one wave after the latest earlier source whose
-  // stamp overlaps its own (corners closer than T on both axes), so each
-  // wave's stamps are disjoint and every pixel sees its sources in index
-  // order; the earlier sources are found in the 3 x 3 cells of pitch T
   std::vector<int> wave(n, 0);
-  std::map<std::pair<int, int>, std::vector<int>> cells;
-  auto cell_of = [&](int v) { return v >= 0 ? v / T : -((-v + T - 1) / T); };
-  int nwave = 0;
-  for (int i = 0; i < n; ++i) {
-    const int cx = cell_of(ix[i]), cy = cell_of(iy[i]);
-    int w = 0;
-    for (int dy = -1; dy <= 1; ++dy)
-      for (int dx = -1; dx <= 1; ++dx) {
-        auto it = cells.find({cx + dx, cy + dy});
-        if (it == cells.end()) continue;
-        for (int j : it->second)
-          if (std::abs(ix[i] - ix[j]) < T && std::abs(iy[i] - iy[j]) < T)
-            w = std::max(w, wave[j] + 1);
-      }
-    wave[i] = w;
-    nwave = std::max(nwave, w + 1);
-    cells[{cx, cy}].push_back(i);
-  }
+  const int nwave = scene_waves(n, ix.data(), iy.data(), T, wave.data());
   std::vector<int> srcs(n), off(nwave + 1, 0);
   for (int i = 0; i < n; ++i) ++off[wave[i] + 1];
   for (int w = 0; w < nwave; ++w) off[w + 1] += off[w];
