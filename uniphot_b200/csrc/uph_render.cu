@@ -719,10 +719,18 @@ __device__ __forceinline__ void render_body(const ClassDev& c, const float* __re
   }
 }
 
-template <bool LIN>
-__global__ void __launch_bounds__(256)
-k_render(ClassDev c, const float* __restrict__ P, int phase) {
-  render_body<LIN>(c, P, phase, blockIdx.x);
+// The linearisation render at the compiler's own register choice (61, four
+// CTAs per SM, the shared-memory limit too); the trial render (model row
+// only) held to 48 registers for five CTAs per SM, without spills.
+__global__ void __launch_bounds__(256) k_render_lin(ClassDev c, const float* __restrict__ P,
+                                                    int phase) {
+  render_body<true>(c, P, phase, blockIdx.x);
+}
+
+__global__ void __launch_bounds__(256, 5) k_render_trial(ClassDev c,
+                                                         const float* __restrict__ P,
+                                                         int phase) {
+  render_body<false>(c, P, phase, blockIdx.x);
 }
 
 // Queue kernels of the LM loop: the member set-up and the render of every
@@ -805,13 +813,13 @@ void launch_render(const ClassDev& c, const float* P, int phase,
       c, P, phase);
   if (c.mode == 0 && c.gstamp) launch_gal_fft(c, P, phase, s);
   if (phase == PH_LIN)
-    k_render<true><<<(unsigned)nblk, 256, bytes, s>>>(c, P, phase);
+    k_render_lin<<<(unsigned)nblk, 256, bytes, s>>>(c, P, phase);
   else
-    k_render<false><<<(unsigned)nblk, 256, bytes, s>>>(c, P, phase);
+    k_render_trial<<<(unsigned)nblk, 256, bytes, s>>>(c, P, phase);
 }
 
 int uph_render_setup() {
-  cudaError_t e = cudaFuncSetAttribute(k_render<true>,
+  cudaError_t e = cudaFuncSetAttribute(k_render_lin,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)render_smem_bytes());
   if (e != cudaSuccess) return (int)e;
@@ -821,7 +829,7 @@ int uph_render_setup() {
   e = cudaFuncSetAttribute(kq_render<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)render_smem_bytes());
   if (e != cudaSuccess) return (int)e;
-  return (int)cudaFuncSetAttribute(k_render<false>,
+  return (int)cudaFuncSetAttribute(k_render_trial,
                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)render_smem_bytes());
 }
