@@ -721,13 +721,14 @@ __device__ __forceinline__ void render_body(const ClassDev& c, const float* __re
 
 // The linearisation render at the compiler's own register choice (61, four
 // CTAs per SM, the shared-memory limit too); the trial render (model row
-// only) held to 48 registers for five CTAs per SM, without spills.
+// only) held to 32 registers for eight CTAs per SM (a 20-byte spill; the
+// solve measured faster at each step from four to eight CTAs).
 __global__ void __launch_bounds__(256) k_render_lin(ClassDev c, const float* __restrict__ P,
                                                     int phase) {
   render_body<true>(c, P, phase, blockIdx.x);
 }
 
-__global__ void __launch_bounds__(256, 5) k_render_trial(ClassDev c,
+__global__ void __launch_bounds__(256, 8) k_render_trial(ClassDev c,
                                                          const float* __restrict__ P,
                                                          int phase) {
   render_body<false>(c, P, phase, blockIdx.x);
