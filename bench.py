@@ -612,7 +612,11 @@ def _serve_measure(args, rates, device):
              ("one_at_a_time_plain", "plain", workers(1), 1))
     for name, prec, make, warm in forms:
         with make(prec) as srv:
-            # warm-up: every context, allocations and graphs
+            # warm-up: every request of the pool once (so that every kernel
+            # the stream uses is loaded, whichever form runs first), then one
+            # per worker or engine
+            for f in [srv.submit(dict(kw, precision=prec)) for kw in pool]:
+                f.result()
             for f in [srv.submit(dict(pool[i % len(pool)], precision=prec))
                       for i in range(warm)]:
                 f.result()
