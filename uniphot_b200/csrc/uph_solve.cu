@@ -252,14 +252,16 @@ __device__ __forceinline__ unsigned dynamic_smem_bytes() {
 // a fixed order, and through a small shared buffer when s > 32.
 // sp / nsp: this CTA's share of the window's pixel tiles (contiguous, in
 // order), for a Gram split over nsp CTAs whose partial Grams are summed
-// afterwards; the small path (K <= 8) runs whole in split 0.
-template <bool BG>
+// afterwards; the small path (K <= 8) runs whole in split 0.  SMALL: the
+// caller guarantees K <= 8, and the tiled path (its 8 x 8 register blocks)
+// is not compiled in, so the kernel keeps few registers.
+template <bool BG, bool SMALL = false>
 __device__ void gram_window(const ClassDev& c, int isl, int b, RowSrc rows,
                             const int4* box, float* out, int ld, int part,
                             float* sm, int sp = 0, int nsp = 1) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int K = rows.K;
-  if (K <= 8) {
+  if (SMALL || K <= 8) {
     if (part == 0 && sp == 0) gram_window_small<BG>(c, isl, b, rows, box, out, ld, sm);
     return;
   }
@@ -405,7 +407,7 @@ __device__ void load_boxes(const ClassDev& c, int isl, const float* P,
   }
 }
 
-template <bool BG>
+template <bool BG, bool SMALL = false>
 __device__ __forceinline__ void gram_lin_body(const ClassDev& c, int bx, int by) {
   extern __shared__ float sm[];
   __shared__ int4 box[UPH_MAXN];
@@ -433,8 +435,8 @@ __device__ __forceinline__ void gram_lin_body(const ClassDev& c, int bx, int by)
   const size_t mat = (size_t)c.Kmax * c.Kmax;
   float* out = nsp > 1 ? c.glpart + (size_t)sp * c.n_isl * c.nb * mat
                        : c.gram;
-  gram_window<BG>(c, isl, b, rows, box, out + ((size_t)isl * c.nb + b) * mat, c.Kmax,
-                  part, sm, sp, nsp);
+  gram_window<BG, SMALL>(c, isl, b, rows, box, out + ((size_t)isl * c.nb + b) * mat,
+                         c.Kmax, part, sm, sp, nsp);
 }
 
 // Sum of the gl_split partial FP32 Grams of an (island, band), in split order
@@ -466,6 +468,14 @@ __global__ void __launch_bounds__(NT) k_gram_lin_reduce(ClassDev c) {
 template <bool BG>
 __global__ void __launch_bounds__(NT) k_gram_lin(ClassDev c) {
   gram_lin_body<BG>(c, blockIdx.x, blockIdx.y);
+}
+
+// Chunks whose Grams all have at most 8 rows (most singleton classes): the
+// same work without the tiled path's registers (79 instead of 128: three
+// CTAs per SM instead of two).
+template <bool BG>
+__global__ void __launch_bounds__(NT) k_gram_lin_small(ClassDev c) {
+  gram_lin_body<BG, true>(c, blockIdx.x, blockIdx.y);
 }
 
 // Gauss-Jordan elimination with partial pivoting on M (n x ncol, pitch ld):
@@ -2017,10 +2027,17 @@ size_t step_smem_bytes(int nLmax) {
 
 void launch_gram_lin(const ClassDev& c, cudaStream_t s) {
   dim3 grid((unsigned)(c.n_isl * c.nb), (unsigned)gram_lin_ydim(c));
-  if (c.nbg)
-    k_gram_lin<true><<<grid, NT, gram_lin_smem_bytes(c.Kmax), s>>>(c);
-  else
-    k_gram_lin<false><<<grid, NT, gram_lin_smem_bytes(c.Kmax), s>>>(c);
+  const size_t smem = gram_lin_smem_bytes(c.Kmax);
+  if (c.Kmax <= 8) {
+    if (c.nbg)
+      k_gram_lin_small<true><<<grid, NT, smem, s>>>(c);
+    else
+      k_gram_lin_small<false><<<grid, NT, smem, s>>>(c);
+  } else if (c.nbg) {
+    k_gram_lin<true><<<grid, NT, smem, s>>>(c);
+  } else {
+    k_gram_lin<false><<<grid, NT, smem, s>>>(c);
+  }
   if (c.gl_split > 1) k_gram_lin_reduce<<<(unsigned)(c.n_isl * c.nb), NT, 0, s>>>(c);
 }
 
@@ -2030,12 +2047,13 @@ void launch_assemble(const ClassDev& c, cudaStream_t s) {
 
 void launch_gram_trial(const ClassDev& c, const float* P, int phase,
                        int final_mode, float* fout, float* cout, cudaStream_t s) {
-  if (c.nbg)
-    k_gram_trial<true><<<(unsigned)(c.n_isl * c.nb), NT, gram_trial_smem_bytes(c.N), s>>>(
-      c, P, phase, final_mode, fout, cout);
-  else
-    k_gram_trial<false><<<(unsigned)(c.n_isl * c.nb), NT, gram_trial_smem_bytes(c.N), s>>>(
-      c, P, phase, final_mode, fout, cout);
+  const unsigned grid = (unsigned)(c.n_isl * c.nb);
+  const size_t smem = gram_trial_smem_bytes(c.N);
+  if (c.nbg) {
+    k_gram_trial<true><<<grid, NT, smem, s>>>(c, P, phase, final_mode, fout, cout);
+  } else {
+    k_gram_trial<false><<<grid, NT, smem, s>>>(c, P, phase, final_mode, fout, cout);
+  }
 }
 
 void launch_step(const ClassDev& c, int phase, int probe_j, float probe_lam,
