@@ -349,6 +349,10 @@ __device__ __forceinline__ void member_setup_warp(const ClassDev& c,
 // One warp per member record, four records per CTA (warp-level syncs only:
 // the warps of a CTA are independent).
 constexpr int SETUP_WARPS = 4;
+// CTAs per SM the star-only linearisation render is held to (32 registers)
+#ifndef RENDER_LIN_STAR_CTAS
+#define RENDER_LIN_STAR_CTAS 8
+#endif
 
 __device__ __forceinline__ void member_setup_body(const ClassDev& c,
                                                   const float* __restrict__ P, int phase,
@@ -366,15 +370,17 @@ k_member_setup(ClassDev c, const float* __restrict__ P, int phase) {
   member_setup_body(c, P, phase, (int)r0, (int)std::min<long long>(SETUP_WARPS, nrec - r0));
 }
 
-template <bool LIN>
+template <bool LIN, bool GAL = true>
 __device__ __forceinline__ void render_body(const ClassDev& c, const float* __restrict__ P,
                                             int phase, int bx) {
   // LIN: linearisation render (model and derivative rows); the trial and
   // probe renders (model row only) are a separate instantiation that needs
-  // far fewer registers, hence more CTAs per SM
+  // far fewer registers, hence more CTAs per SM.  GAL = false: the chunk
+  // holds no galaxy (c.has_gal == 0), and the galaxy paths are not compiled
+  // in (the star paths run the same operations in either instantiation).
   extern __shared__ float smem[];
   __shared__ MemberSetup ms;
-  __shared__ float4 trec[MAXCOMP * (LIN ? 7 : 1)];   // per-tile component records
+  __shared__ float4 trec[MAXCOMP * (LIN ? (GAL ? 7 : 3) : 1)];   // per-tile component records
   __shared__ MemberBox mb;
   const int ntile = c.ntile_side * c.ntile_side;
   int t = bx;
@@ -393,7 +399,7 @@ __device__ __forceinline__ void render_body(const ClassDev& c, const float* __re
   const MemberRecord* rec = c.mrec + ((size_t)isl * c.nb + b) * c.N + k;
   if (tid == 0) {
     mb = member_box(c, isl, P, k);
-    ms.is_gal = c.has_gal && c.stype[isl * c.N + k] != 0;
+    ms.is_gal = GAL && c.has_gal && c.stype[isl * c.N + k] != 0;
     ms.support_half = ms.is_gal ? c.T / 2 : c.native / 2;
     const uint8_t* kp = c.keep + ((size_t)isl * c.N + k) * 6;
     int row = 1;
@@ -467,7 +473,8 @@ __device__ __forceinline__ void render_body(const ClassDev& c, const float* __re
   // (galaxies: x, y, three shape rows, and the Sersic-index row only when
   // the index is live)
   int nout = 0;
-  if (lin) nout = ms.is_gal ? (ms.need[6] ? 6 : 5) : ((ms.need[1] || ms.need[2]) ? 2 : 0);
+  const bool is_gal = GAL && ms.is_gal;
+  if (lin) nout = is_gal ? (ms.need[6] ? 6 : 5) : ((ms.need[1] || ms.need[2]) ? 2 : 0);
   if (tid == 0 && c.work) {
     // algorithmic work of this tile: the stamp rows written; on the tile's
     // pixels inside the member's support, per Gaussian term that reaches the
@@ -487,7 +494,7 @@ __device__ __forceinline__ void render_body(const ClassDev& c, const float* __re
       if (c.mode == 1) {
         exps = sup * (unsigned long long)ms.nact;
         flops = exps * 2ull * (4 + 4 * nout);
-      } else if (!ms.is_gal) {
+      } else if (!is_gal) {
         flops = sup * 2ull * c.nt * (unsigned long long)nsarr;
       }
       // shifted arrays: S and its partials, plus the tap derivatives of the
@@ -520,12 +527,12 @@ __device__ __forceinline__ void render_body(const ClassDev& c, const float* __re
       };
       r[1] = comb(o.dAx, o.dCx, o.dBx, o.nrm, o.nx);
       r[2] = comb(o.dAy, o.dCy, o.dBy, o.nrm, o.ny);
-      if (nout >= 5) {
+      if (GAL && nout >= 5) {
         const float nv = o.nrm * o.v;
         for (int q = 0; q < 3; ++q)
           r[3 + q] = comb(ms.dcov[q][0], ms.dcov[q][1], ms.dcov[q][2], nv, 0.f);
       }
-      if (nout == 6) {
+      if (GAL && nout == 6) {
         const float4 u = comb(ms.cg[0], ms.cg[1], ms.cg[2], o.nrm * o.dv, o.nu);
         r[6] = make_float4(ms.dndu * u.x, ms.dndu * u.y, ms.dndu * u.z, ms.dndu * u.w);
       }
@@ -547,7 +554,7 @@ __device__ __forceinline__ void render_body(const ClassDev& c, const float* __re
 
   // ---- un-shifted stamp (and partials) on the halo region ----
   const int nh = hr * hc;
-  if (c.mode == 0 && ms.is_gal) {
+  if (c.mode == 0 && is_gal) {
     // reference-mode galaxy: the unshifted rows from the Fourier-domain
     // convolution (k_gal_fft)
     const float* gs = c.gstamp + (((size_t)isl * c.nb + b) * c.N + k) * 7 * (size_t)(T * T);
@@ -611,9 +618,9 @@ __device__ __forceinline__ void render_body(const ClassDev& c, const float* __re
         y2[h] = yo * yo;
       }
       float va[NS], vb[NS];
-      if (nout == 6)
+      if (GAL && nout == 6)
         mog_pair<6>(trec, ms.nact, x2[0], xy[0], y2[0], x2[1], xy[1], y2[1], va, vb);
-      else if (nout == 5)
+      else if (GAL && nout == 5)
         mog_pair<5>(trec, ms.nact, x2[0], xy[0], y2[0], x2[1], xy[1], y2[1], va, vb);
       else if (nout == 2)
         mog_pair<2>(trec, ms.nact, x2[0], xy[0], y2[0], x2[1], xy[1], y2[1], va, vb);
@@ -659,7 +666,7 @@ __device__ __forceinline__ void render_body(const ClassDev& c, const float* __re
           xv[1] = a1;
         }
 #pragma unroll
-        for (int sa = 2; sa < NS; ++sa) {
+        for (int sa = 2; sa < (GAL ? NS : 3); ++sa) {
           if (!ms.need[sa]) continue;
           const float* sp = S + (sa * UPH_HALO + r) * HP + cc;
           float a = ms.Lx[0] * sp[0];
@@ -672,7 +679,7 @@ __device__ __forceinline__ void render_body(const ClassDev& c, const float* __re
         S[(0 * UPH_HALO + r) * HP + cc] = xv[0];
         if (dox) S[(1 * UPH_HALO + r) * HP + cc] = xv[1];
 #pragma unroll
-        for (int sa = 2; sa < NS; ++sa)
+        for (int sa = 2; sa < (GAL ? NS : 3); ++sa)
           if (ms.need[sa]) S[(sa * UPH_HALO + r) * HP + cc] = xv[sa];
       }
       __syncwarp();
@@ -708,7 +715,7 @@ __device__ __forceinline__ void render_body(const ClassDev& c, const float* __re
       }
       c.stamps[stamp_slot(c, isl, b, k, ms.live_row[1]) + off] = d;
     }
-    for (int j = 2; j < 6; ++j) {
+    for (int j = 2; j < (GAL ? 6 : 2); ++j) {
       if (!ms.live_row[j]) continue;
       const int s = j + 1;  // S arrays 3..6 hold lr, e1, e2, u
       const float* xs = S + (s * UPH_HALO + rr) * HP + cc;
@@ -726,6 +733,13 @@ __device__ __forceinline__ void render_body(const ClassDev& c, const float* __re
 __global__ void __launch_bounds__(256) k_render_lin(ClassDev c, const float* __restrict__ P,
                                                     int phase) {
   render_body<true>(c, P, phase, blockIdx.x);
+}
+
+// The linearisation render of chunks without galaxies: the galaxy paths
+// compiled out, three stamp arrays, and an occupancy bound.
+__global__ void __launch_bounds__(256, RENDER_LIN_STAR_CTAS) k_render_lin_star(
+    ClassDev c, const float* __restrict__ P, int phase) {
+  render_body<true, false>(c, P, phase, blockIdx.x);
 }
 
 __global__ void __launch_bounds__(256, 8) k_render_trial(ClassDev c,
@@ -813,7 +827,9 @@ void launch_render(const ClassDev& c, const float* P, int phase,
   k_member_setup<<<(unsigned)((nrec + SETUP_WARPS - 1) / SETUP_WARPS), 32 * SETUP_WARPS, 0, s>>>(
       c, P, phase);
   if (c.mode == 0 && c.gstamp) launch_gal_fft(c, P, phase, s);
-  if (phase == PH_LIN)
+  if (phase == PH_LIN && !c.has_gal)
+    k_render_lin_star<<<(unsigned)nblk, 256, bytes, s>>>(c, P, phase);
+  else if (phase == PH_LIN)
     k_render_lin<<<(unsigned)nblk, 256, bytes, s>>>(c, P, phase);
   else
     k_render_trial<<<(unsigned)nblk, 256, bytes, s>>>(c, P, phase);
