@@ -177,3 +177,24 @@ def test_catalog_errors_round_source_and_degenerate_variances():
     np.testing.assert_allclose(e["re_err"][0], 0.2, rtol=1e-6)
     assert np.isnan(e["ell_err"][0]) and np.isnan(e["theta_err"][0])
     assert np.isnan(e["sersic_n_err"][0]) and np.isnan(e["pos_x_prior_frac"][0])
+
+
+def test_superseded_device_field_is_refused():
+    """A DeviceField records the upload it came from; after another field is
+    uploaded to the same context it refuses to bind new chunks (the chunks
+    already added keep their own buffers).  A stand-in context holds only
+    the upload counter the check reads."""
+    class Ctx:
+        field_gen = 0
+
+        def upload_field_unpadded(self, d, w, pad):
+            self.field_gen += 1
+    ctx = Ctx()
+    d = np.zeros((2, 8, 8), np.float32)
+    a = solver.DeviceField.from_unpadded(d, d, 3, context=ctx)
+    a.check_current()
+    b = solver.DeviceField.from_unpadded(d, d, 3, context=ctx)
+    b.check_current()
+    with pytest.raises(ValueError, match="superseded"):
+        a.check_current()
+    assert b.shape == (2, 14, 14) and b.pad == 3
