@@ -332,6 +332,8 @@ void stage_give(float* p, size_t floats) {
 
 // Copy n floats from pageable src to pinned dst with up to `threads` host
 // threads (contiguous slices).
+// Nothing throws out of it: if a thread cannot be started, the calling
+// thread copies what no thread took.
 static void parallel_copy(float* dst, const float* src, size_t n, int threads) {
   if (threads <= 1 || n < (size_t)1 << 20) {
     std::memcpy(dst, src, n * sizeof(float));
@@ -339,11 +341,18 @@ static void parallel_copy(float* dst, const float* src, size_t n, int threads) {
   }
   std::vector<std::thread> pool;
   const size_t per = (n + threads - 1) / threads;
-  for (int t = 0; t < threads; ++t) {
-    const size_t lo = (size_t)t * per, hi = std::min(n, lo + per);
-    if (lo >= hi) break;
-    pool.emplace_back([=] { std::memcpy(dst + lo, src + lo, (hi - lo) * sizeof(float)); });
+  size_t taken = 0;   // [0, taken) is handed to started threads
+  try {
+    pool.reserve((size_t)threads);
+    for (int t = 0; t < threads; ++t) {
+      const size_t lo = (size_t)t * per, hi = std::min(n, lo + per);
+      if (lo >= hi) break;
+      pool.emplace_back([=] { std::memcpy(dst + lo, src + lo, (hi - lo) * sizeof(float)); });
+      taken = hi;
+    }
+  } catch (...) {
   }
+  if (taken < n) std::memcpy(dst + taken, src + taken, (n - taken) * sizeof(float));
   for (auto& th : pool) th.join();
 }
 
