@@ -1,8 +1,8 @@
 """The radix-2 shared-memory FFT scheme of the reference-mode galaxy render
 (``smem_fft_lines`` / ``fft2_*`` in uph_internal.cuh, used by k_gal_fft and
 k_sp_gal) restated in numpy with the kernels' index arithmetic -- bit-
-reversed loads, iterative decimation-in-time stages with twiddles j P/len
-from a float32 table, row transforms of the T non-zero rows, column
+reversed loads, decimation-in-time stages fused in pairs with twiddles from
+a float32 table, row transforms of the T non-zero rows, column
 transforms of the P/2 + 1 half-spectrum columns, the inverse columns cropped
 to T rows and the Hermitian real inverse of those rows -- agrees with the
 oracle's numpy FFT render (sersic_mog.py:153-207) on every row the Gauss-
@@ -20,27 +20,48 @@ def brev(k, logP):
         r = (r << 1) | ((k >> b) & 1)
     return r
 
+def _bfly(u, v, wr, wi):
+    """The kernel's butterfly: t = w v, (u + t, u - t)."""
+    w = np.complex64(wr + 1j * wi)
+    t = w * v
+    return u + t, u - t
+
+
 def fft_lines(buf, P, sign, cw, sw):
-    """buf: (nl, P) complex64; in-place iterative DIT as the kernel does."""
+    """buf: (nl, P) complex64; in place, as the kernel does: the lines are
+    filled in bit-reversed order, then the decimation-in-time stages run in
+    pairs -- for half-lengths h and 2h, the four elements j, j+h, j+2h,
+    j+3h of each group of 4h take stage h's butterflies (twiddle j P/(2h))
+    and then stage 2h's (twiddles j P/(4h) and (j+h) P/(4h)) -- with a last
+    single stage when log2 P is odd."""
     logP = P.bit_length() - 1
-    nl = buf.shape[0]
     perm = np.array([brev(k, logP) for k in range(P)])
-    buf[:] = buf[:, perm]
-    length = 2
-    while length <= P:
-        half = length // 2
-        step = P // length
-        for grp in range(P // length):
-            for j in range(half):
-                i0 = grp * length + j
-                i1 = i0 + half
-                m = j * step
-                w = np.complex64(cw[m] + 1j * sign * sw[m])
-                t = w * buf[:, i1]
-                u = buf[:, i0].copy()
-                buf[:, i0] = u + t
-                buf[:, i1] = u - t
-        length <<= 1
+    loaded = np.empty_like(buf)
+    loaded[:, perm] = buf          # element k goes to position brev(k)
+    buf[:] = loaded
+    h = 1
+    while 4 * h <= P:
+        sA, sB = P // (2 * h), P // (4 * h)
+        for grp in range(P // (4 * h)):
+            for j in range(h):
+                i0 = grp * 4 * h + j
+                x0, x1 = buf[:, i0].copy(), buf[:, i0 + h].copy()
+                x2, x3 = buf[:, i0 + 2 * h].copy(), buf[:, i0 + 3 * h].copy()
+                mA = j * sA
+                x0, x1 = _bfly(x0, x1, cw[mA], sign * sw[mA])
+                x2, x3 = _bfly(x2, x3, cw[mA], sign * sw[mA])
+                mB0, mB1 = j * sB, (j + h) * sB
+                x0, x2 = _bfly(x0, x2, cw[mB0], sign * sw[mB0])
+                x1, x3 = _bfly(x1, x3, cw[mB1], sign * sw[mB1])
+                buf[:, i0], buf[:, i0 + h], buf[:, i0 + 2 * h], buf[:, i0 + 3 * h] = \
+                    x0, x1, x2, x3
+        h *= 4
+    if 2 * h == P:
+        step = P // (2 * h)
+        for j in range(h):
+            m = j * step
+            buf[:, j], buf[:, j + h] = _bfly(buf[:, j].copy(), buf[:, j + h].copy(),
+                                             cw[m], sign * sw[m])
     return buf
 
 def _fft_render(psf, gal, T, PP, need, psfx=None, psfy=None):
